@@ -1,0 +1,119 @@
+"""ctypes binding of the C ABI in ``include/dmsc_b200.h``.
+
+The product path has no CPU fallback: if ``libdmsc_b200.so`` is missing or no
+CUDA device is present, loading raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdmsc_b200.so")
+
+DUAL, RETURN_GRADIENT, TRACE_RIDGES, TRACE_VALLEYS, TRACE_PEAKS, TRACE_BASINS = 1, 2, 4, 8, 16, 32
+
+# C-ABI exports, in header order (include/dmsc_b200.h).
+EXPORTS = (
+    "dmsc_b200_create",
+    "dmsc_b200_destroy",
+    "dmsc_b200_extract",
+    "dmsc_b200_fetch",
+    "dmsc_b200_error_string",
+    "dmsc_b200_last_error",
+)
+
+ERR_TOO_LARGE = 2
+
+
+class Sizes(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "max_pts", "min_pts", "sad_pts", "e_max_rows", "e_min_rows", "p_max", "p_min", "ppairs_max", "ppairs_min",
+        "grad_indices", "peaks_h", "peaks_w", "ridges", "ridge_offsets", "ridge_arc_offsets", "basins_h", "basins_w",
+        "valleys", "valley_offsets", "valley_arc_offsets")]
+
+
+class Outputs(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in (
+        "max_pts", "min_pts", "sad_pts", "e_max", "e_min", "p_max", "p_min", "ppairs_max", "ppairs_min", "ridges",
+        "ridge_offsets", "ridge_arc_offsets", "valleys", "valley_offsets", "valley_arc_offsets")]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"dmsc_b200 CUDA library not found at {LIB_PATH}; build it with `python -m dmsc_b200.build`")
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.dmsc_b200_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]
+        lib.dmsc_b200_create.restype = ctypes.c_int
+        lib.dmsc_b200_destroy.argtypes = [ctypes.c_void_p]
+        lib.dmsc_b200_destroy.restype = None
+        lib.dmsc_b200_extract.argtypes = [
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Sizes), ctypes.c_void_p]
+        lib.dmsc_b200_extract.restype = ctypes.c_int
+        lib.dmsc_b200_fetch.argtypes = [ctypes.c_void_p, ctypes.POINTER(Outputs), ctypes.c_void_p]
+        lib.dmsc_b200_fetch.restype = ctypes.c_int
+        lib.dmsc_b200_error_string.argtypes = [ctypes.c_int]
+        lib.dmsc_b200_error_string.restype = ctypes.c_char_p
+        lib.dmsc_b200_last_error.argtypes = [ctypes.c_void_p]
+        lib.dmsc_b200_last_error.restype = ctypes.c_char_p
+        _lib = lib
+        return lib
+
+
+class Context:
+    """Owns one device workspace (a ``dmsc_b200_context``)."""
+
+    def __init__(self, device: int):
+        self.lib = load()
+        self.device = device
+        h = ctypes.c_void_p()
+        rc = self.lib.dmsc_b200_create(ctypes.byref(h), device)
+        if rc != 0:
+            raise RuntimeError(f"dmsc_b200_create failed on cuda:{device}: {self.lib.dmsc_b200_error_string(rc).decode()}")
+        self.h = h
+
+    def check(self, rc: int, what: str):
+        if rc == 0:
+            return
+        msg = self.lib.dmsc_b200_last_error(self.h).decode() or self.lib.dmsc_b200_error_string(rc).decode()
+        raise RuntimeError(f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dmsc_b200_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_tls = threading.local()
+
+
+def context(device: int) -> Context:
+    """Per-thread, per-device context (a context is not thread-safe)."""
+    ctxs = getattr(_tls, "ctxs", None)
+    if ctxs is None:
+        ctxs = _tls.ctxs = {}
+    c = ctxs.get(device)
+    if c is None:
+        c = ctxs[device] = Context(device)
+    return c

@@ -1,0 +1,97 @@
+// Shared device helpers for the dmsc_b200 kernels (sm_100a).
+//
+// Cell encoding follows the reference cell complex (dmsc/csrc/cell_complex.hxx:13-51):
+//   cell id = type + 4 * (y * Nx + x),  Nx = W + 1
+//   type 0 vertex (pixel), 1 H-edge, 2 V-edge, 3 face (pixel corner).
+// The "index" of a cell is y * Nx + x; every index holds 4 slots in the
+// gradient array (16 bytes), which is the layout of the grad_indices output.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dmsc {
+
+// Error codes shared with the C-ABI (include/dmsc_b200.h).
+enum : int {
+  kOk = 0,
+  kErrInvalidArgument = 1,
+  kErrTooLarge = 2,
+  kErrCuda = 3,
+  kErrIterationCap = 4,
+  kErrOverflow = 5,
+  kErrInternal = 6,
+};
+
+// Bits of the device-side status word.
+enum : unsigned {
+  kStatusWalkCap = 1u,      // a V-path walk exceeded its step bound
+  kStatusRoundCap = 2u,     // a round loop exceeded its bound
+  kStatusChainCap = 4u,     // a replay chain walk exceeded its bound
+  kStatusQueueOverflow = 8u,
+  kStatusBadIndex = 16u,
+};
+
+__host__ __device__ __forceinline__ int cell_id(int t, int y, int x, int Nx) { return t + 4 * (y * Nx + x); }
+__host__ __device__ __forceinline__ int cell_type(int id) { return id & 3; }
+__host__ __device__ __forceinline__ int cell_index(int id) { return id >> 2; }
+
+// std::tie(v1, id1) < std::tie(v2, id2) with IEEE '<' (cpu/cell_compare.hxx:10-12):
+// -0 == +0 and NaN compare as ties, broken by id.
+__device__ __forceinline__ bool tie_lt(float v1, int id1, float v2, int id2) {
+  return (v1 < v2) || (!(v2 < v1) && id1 < id2);
+}
+// value_less<IS_DUAL> / value_greater<IS_DUAL> (cpu/cell_compare.hxx:9-21).
+template <bool DUAL>
+__device__ __forceinline__ bool value_less(float v1, int id1, float v2, int id2) {
+  return DUAL ? tie_lt(v2, id2, v1, id1) : tie_lt(v1, id1, v2, id2);
+}
+template <bool DUAL>
+__device__ __forceinline__ bool value_greater(float v1, int id1, float v2, int id2) {
+  return value_less<!DUAL>(v1, id1, v2, id2);
+}
+
+// Monotone float -> uint32 key: ascending key order == ascending IEEE order,
+// with -0 mapped onto +0 and every NaN onto one key (ties, as std::tie sees them).
+__device__ __forceinline__ uint32_t orderable_key(float f) {
+  if (f != f) return 0xFFFFFFFFu;
+  if (f == 0.0f) f = 0.0f;
+  uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// Successor of a face along its V-path: the other face of its paired edge
+// (cpu/arcs_topology.hxx:19-39). Both cofaces of an edge are always valid.
+__device__ __forceinline__ int next_face(int e, int curr, int Nx) {
+  int idx = e >> 2, t = e & 3;
+  int f1 = 3 + 4 * idx;
+  int f2 = (t == 1) ? 3 + 4 * (idx + Nx) : 3 + 4 * (idx + 1);
+  return (f1 == curr) ? f2 : f1;
+}
+
+// Successor of a vertex: the other vertex of its paired edge, or -1 off the
+// image (cpu/arcs_topology.hxx:41-65).
+__device__ __forceinline__ int next_vertex(int e, int curr, int H, int W, int Nx) {
+  int idx = e >> 2, t = e & 3;
+  int ey = idx / Nx, ex = idx - ey * Nx;
+  int v1 = -1, v2 = -1;
+  if (t == 1) {
+    if (ex - 1 >= 0) v1 = 4 * (idx - 1);
+    if (ex < W) v2 = 4 * idx;
+  } else {
+    if (ey - 1 >= 0) v1 = 4 * (idx - Nx);
+    if (ey < H) v2 = 4 * idx;
+  }
+  return (v1 == curr) ? v2 : v1;
+}
+
+__device__ __forceinline__ void set_status(unsigned* status, unsigned bit) { atomicOr(status, bit); }
+
+inline unsigned grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > 2147483647LL) g = 2147483647LL;
+  return (unsigned)g;
+}
+
+}  // namespace dmsc

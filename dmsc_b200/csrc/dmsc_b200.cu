@@ -1,0 +1,780 @@
+// dmsc_b200: host orchestration and C ABI (include/dmsc_b200.h).
+//
+// Replaces the reference CUDA binding and its host-side pipeline
+// (dmsc/csrc/dmsc_gpu.cpp:18-180, dmsc/csrc/gpu/dmsc_cuda.hxx:64-477,
+// dmsc/csrc/gpu/workspace.hxx:91-397): every stage runs on the device, the
+// persistence sweeps and the arc-simplification replay included. The host
+// reads back only sizes and round counters.
+//
+// Internal sides: side 0 = faces (maxima in the primal), side 1 = vertices
+// (minima in the primal); the dual swaps roles at the boundary exactly as the
+// reference does (dmsc_cpu.cpp:34-37, workspace.hxx:322-362).
+#include <cuda_runtime.h>
+
+#include <cub/cub.cuh>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/dmsc_b200.h"
+#include "assemble.cuh"
+#include "common.cuh"
+#include "gradient.cuh"
+#include "pairing.cuh"
+#include "replay.cuh"
+#include "walks.cuh"
+
+using namespace dmsc;
+
+namespace {
+
+enum Slot {
+  S_GRAD, S_MASK, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT,
+  S_CMIN, S_CSAD, S_CMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA, S_ASC,
+  S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS,
+  S_SIDE0,  // per-side slots start here, kSideSlots each
+};
+enum SideSlot {
+  X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
+  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CKEY2, X_CVAL, X_CORD, X_CTIME, X_STAT,
+  X_PAR, X_WLEN, X_SIDE, X_CSAD, X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC,
+  X_EROWO, X_Q0, X_Q1, kSideSlots
+};
+
+struct Buf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct Side {
+  int M = 0;
+  bool faces = true;
+  bool arcs = false;
+  bool groups = false;
+  int* crit = nullptr;
+  float* val = nullptr;
+  int* rank_map = nullptr;
+  int* t = nullptr;
+  int* steps = nullptr;
+  int* sweep = nullptr;
+  int* c1 = nullptr;
+  int* c2 = nullptr;
+  int* dying = nullptr;
+  int* pair_dense = nullptr;
+  float* pers = nullptr;
+  uint8_t* alive = nullptr;
+  int* to_out_excl = nullptr;
+  int* to_out = nullptr;
+  int* ut = nullptr;
+  long long* blen = nullptr;
+  ReplayState R{};
+  int C = 0;
+  long long* arc_len = nullptr;
+  long long* arc_cl = nullptr;
+  int* arc_root = nullptr;
+  long long* arc_pos = nullptr;
+  long long total = 0;
+  int n_alive = 0;
+  int n_erows = 0;
+  int* erow_off = nullptr;
+  int rounds_pair = 0, rounds_replay = 0;
+};
+
+}  // namespace
+
+struct dmsc_b200_context {
+  int device = 0;
+  std::vector<Buf> bufs;
+  Buf cub_tmp;
+  long long* pinned = nullptr;  // host scalars for readbacks
+  std::string err;
+  // state of the last extract()
+  bool valid = false;
+  int H = 0, W = 0;
+  bool dual = false;
+  float thr = 0.f;
+  int nmin = 0, nsad = 0, nmax = 0, nsurv = 0;
+  const int* grad = nullptr;
+  int* crit_sad = nullptr;
+  int* surv = nullptr;
+  unsigned* status = nullptr;
+  Side side[2];
+  dmsc_b200_sizes sizes{};
+};
+
+namespace {
+
+struct Fail {
+  int code;
+};
+
+void set_err(dmsc_b200_context* c, const char* fmt, ...) {
+  char b[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(b, sizeof b, fmt, ap);
+  va_end(ap);
+  c->err = b;
+}
+
+void ck(dmsc_b200_context* c, cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    set_err(c, "%s: %s", what, cudaGetErrorString(e));
+    throw Fail{kErrCuda};
+  }
+}
+#define CK(x) ck(ctx, (x), #x)
+#define LAUNCH_CHECK(name) ck(ctx, cudaGetLastError(), name)
+
+template <class T>
+T* get(dmsc_b200_context* ctx, int slot, size_t n) {
+  size_t bytes = n * sizeof(T);
+  if (bytes == 0) bytes = 16;
+  if ((size_t)slot >= ctx->bufs.size()) ctx->bufs.resize(slot + 1);
+  Buf& b = ctx->bufs[slot];
+  if (b.cap < bytes) {
+    if (b.p) CK(cudaFree(b.p));
+    b.p = nullptr;
+    size_t nb = bytes + bytes / 4 + 256;
+    CK(cudaMalloc(&b.p, nb));
+    b.cap = nb;
+  }
+  return (T*)b.p;
+}
+
+template <class T>
+T* sget(dmsc_b200_context* ctx, int side, int slot, size_t n) {
+  return get<T>(ctx, S_SIDE0 + side * kSideSlots + slot, n);
+}
+
+void* cub_tmp(dmsc_b200_context* ctx, size_t bytes) {
+  if (ctx->cub_tmp.cap < bytes) {
+    if (ctx->cub_tmp.p) CK(cudaFree(ctx->cub_tmp.p));
+    size_t nb = bytes + bytes / 4 + 256;
+    CK(cudaMalloc(&ctx->cub_tmp.p, nb));
+    ctx->cub_tmp.cap = nb;
+  }
+  return ctx->cub_tmp.p;
+}
+
+template <class In, class Out>
+void excl_sum(dmsc_b200_context* ctx, const In* in, Out* out, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  size_t bytes = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, st));
+  void* tmp = cub_tmp(ctx, bytes);
+  CK(cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, n, st));
+}
+
+template <class In, class Out>
+void incl_sum(dmsc_b200_context* ctx, const In* in, Out* out, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  size_t bytes = 0;
+  CK(cub::DeviceScan::InclusiveSum(nullptr, bytes, in, out, n, st));
+  void* tmp = cub_tmp(ctx, bytes);
+  CK(cub::DeviceScan::InclusiveSum(tmp, bytes, in, out, n, st));
+}
+
+template <class K>
+void sort_pairs(dmsc_b200_context* ctx, const K* kin, K* kout, const int* vin, int* vout, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  size_t bytes = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, (int)(8 * sizeof(K)), st));
+  void* tmp = cub_tmp(ctx, bytes);
+  CK(cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, n, 0, (int)(8 * sizeof(K)), st));
+}
+
+__global__ void totals3_kernel(const int* o0, const int* s0, const int* o1, const int* s1, const int* o2,
+                               const int* s2, long long n, long long* out) {
+  out[0] = (long long)o0[n - 1] + s0[n - 1];
+  out[1] = (long long)o1[n - 1] + s1[n - 1];
+  out[2] = (long long)o2[n - 1] + s2[n - 1];
+}
+
+template <class T>
+__global__ void last_plus_kernel(const T* excl, const T* val, int n, long long* out) {
+  *out = n > 0 ? (long long)excl[n - 1] + (long long)val[n - 1] : 0;
+}
+
+template <class T>
+__global__ void last_kernel(const T* a, int n, long long* out) {
+  *out = n > 0 ? (long long)a[n - 1] : 0;
+}
+
+__global__ void u8_last_plus_kernel(const int* excl, const uint8_t* v, int n, long long* out) {
+  *out = n > 0 ? (long long)excl[n - 1] + v[n - 1] : 0;
+}
+
+// Host read of `k` pinned scalars after the stream drains.
+void readback(dmsc_b200_context* ctx, cudaStream_t st, const long long* dev, int k) {
+  CK(cudaMemcpyAsync(ctx->pinned, dev, k * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+}
+
+void check_status(dmsc_b200_context* ctx, cudaStream_t st) {
+  unsigned h = 0;
+  CK(cudaMemcpyAsync(&h, ctx->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (h & (kStatusWalkCap | kStatusRoundCap | kStatusChainCap)) {
+    set_err(ctx, "a bounded device loop reached its cap (status 0x%x)", h);
+    throw Fail{kErrIterationCap};
+  }
+  if (h & kStatusQueueOverflow) {
+    set_err(ctx, "geometry work queue overflow (status 0x%x)", h);
+    throw Fail{kErrOverflow};
+  }
+  if (h) {
+    set_err(ctx, "device status 0x%x", h);
+    throw Fail{kErrInternal};
+  }
+}
+
+constexpr int TB = 256;
+
+// Persistence pairing of one side (see pairing.cuh).
+void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool reverse, cudaStream_t st) {
+  const int nsad = ctx->nsad, M = S.M;
+  S.sweep = sget<int>(ctx, si, X_SWEEP, nsad);
+  S.c1 = sget<int>(ctx, si, X_C1, nsad);
+  S.c2 = sget<int>(ctx, si, X_C2, nsad);
+  S.dying = sget<int>(ctx, si, X_DYING, nsad);
+  int* grp = sget<int>(ctx, si, X_GRP, M + 1);
+  int* link = sget<int>(ctx, si, X_LINK, M + 1);
+  unsigned* minedge = sget<unsigned>(ctx, si, X_MINE, M + 1);
+  int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
+  int* cnt = sget<int>(ctx, si, X_CNT, 4);
+  if (nsad > 0) {
+    sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, reverse, S.t, S.sweep, S.c1, S.c2, S.dying);
+    LAUNCH_CHECK("sweep_edges_kernel");
+  }
+  iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(grp, M + 1);
+  iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(link, M + 1);
+  CK(cudaMemsetAsync(minedge, 0xFF, (M + 1) * sizeof(unsigned), st));
+  if (nsad > 0) iota_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(act[0], nsad);
+  LAUNCH_CHECK("pairing init");
+  // older = value_less<D'> with D' = dual on the vertex side, !dual on the face side
+  const bool older_less = S.faces ? ctx->dual : !ctx->dual;
+  int n_active = nsad, cur = 0, rounds = 0;
+  while (n_active > 0) {
+    if (++rounds > M + 2) {
+      set_err(ctx, "pairing exceeded %d rounds", M + 2);
+      throw Fail{kErrIterationCap};
+    }
+    CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+    pair_edges_kernel<<<grid_for(n_active, TB), TB, 0, st>>>(act[cur], n_active, S.c1, S.c2, M, grp, S.dying,
+                                                             minedge, act[cur ^ 1], cnt);
+    if (older_less)
+      pair_groups_kernel<true><<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, M, S.c1, S.c2, grp, minedge, link,
+                                                                    S.dying, S.val, S.crit);
+    else
+      pair_groups_kernel<false><<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, M, S.c1, S.c2, grp, minedge, link,
+                                                                     S.dying, S.val, S.crit);
+    pair_jump_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, grp, link, ctx->status);
+    LAUNCH_CHECK("pairing round");
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    n_active = h;
+    cur ^= 1;
+  }
+  S.rounds_pair = rounds;
+
+  // persistence, cancellation, alive flags
+  S.pair_dense = sget<int>(ctx, si, X_PAIR, nsad);
+  S.pers = sget<float>(ctx, si, X_PERS, nsad);
+  S.alive = sget<uint8_t>(ctx, si, X_ALIVE, M + 4);
+  CK(cudaMemsetAsync(S.alive, 1, M + 4, st));
+  uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
+  if (nsad > 0) {
+    persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, !S.faces, ctx->dual, ctx->thr, S.sweep, S.dying,
+                                                          get<float>(ctx, S_SVAL, nsad), S.val, S.pair_dense, S.pers,
+                                                          canc, (uint8_t)(S.faces ? 1 : 2), S.alive);
+    LAUNCH_CHECK("persistence_kernel");
+  }
+  // thresholded union-find roots
+  int* uf = sget<int>(ctx, si, X_UF, M + 1);
+  int* croot = sget<int>(ctx, si, X_CROOT, M + 1);
+  S.ut = sget<int>(ctx, si, X_UT, M + 1);
+  iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(uf, M + 1);
+  if (nsad > 0)
+    ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.c1, S.c2, S.pers, ctx->thr, M, uf);
+  ut_flatten_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, uf);
+  ut_mark_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M, uf, S.alive, croot);
+  if (M > 0) ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.ut);
+  LAUNCH_CHECK("thresholded union-find");
+  // output rank of alive extrema
+  int* alive_i = sget<int>(ctx, si, X_ALIVEI, M + 1);
+  S.to_out_excl = sget<int>(ctx, si, X_TOOUTX, M + 1);
+  S.to_out = sget<int>(ctx, si, X_TOOUT, M + 1);
+  if (M > 0) {
+    u8_to_int_kernel<<<grid_for(M, TB), TB, 0, st>>>(S.alive, M, alive_i);
+    excl_sum(ctx, alive_i, S.to_out_excl, M, st);
+    compact_alive_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, S.alive, S.to_out_excl, S.crit, nullptr, S.to_out);
+    LAUNCH_CHECK("compact_alive_kernel");
+  }
+}
+
+// Replay of one side's cancellations and the final arc lengths.
+void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
+  const int nsad = ctx->nsad, M = S.M, nsurv = ctx->nsurv;
+  long long* tot = get<long long>(ctx, S_TOT, 8);
+  S.blen = sget<long long>(ctx, si, X_BLEN, 2 * (size_t)nsad);
+  if (nsad > 0) base_len_kernel<<<grid_for(2LL * nsad, TB), TB, 0, st>>>(2 * nsad, S.t, S.steps, S.blen);
+  unsigned long long* ckey = sget<unsigned long long>(ctx, si, X_CKEY, nsad);
+  unsigned long long* ck2 = sget<unsigned long long>(ctx, si, X_CKEY2, nsad);
+  int* cval = sget<int>(ctx, si, X_CVAL, nsad);
+  int* cord = sget<int>(ctx, si, X_CORD, nsad);
+  int* cnt = sget<int>(ctx, si, X_CNT, 4);
+  CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+  if (nsad > 0)
+    cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->thr,
+                                                             ctx->crit_sad, ckey, cval, cnt);
+  LAUNCH_CHECK("cancel_collect_kernel");
+  int C = 0;
+  CK(cudaMemcpyAsync(&C, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  S.C = C;
+  sort_pairs(ctx, ckey, ck2, cval, cord, C, st);
+
+  ReplayState& R = S.R;
+  R.ctime = sget<int>(ctx, si, X_CTIME, M + 1);
+  R.status = sget<int>(ctx, si, X_STAT, M + 1);
+  R.parent = sget<int>(ctx, si, X_PAR, M + 1);
+  R.wlen = sget<long long>(ctx, si, X_WLEN, M + 1);
+  R.side = sget<int>(ctx, si, X_SIDE, M + 1);
+  R.csad = sget<int>(ctx, si, X_CSAD, M + 1);
+  R.cl_dy = sget<long long>(ctx, si, X_CLDY, M + 1);
+  R.cl_ot = sget<long long>(ctx, si, X_CLOT, M + 1);
+  fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.ctime, M + 1, kNever);
+  fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.status, M + 1, kRootForever);
+  if (C > 0) replay_init_kernel<<<grid_for(C, TB), TB, 0, st>>>(C, cord, S.dying, R);
+  LAUNCH_CHECK("replay init");
+  int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
+  if (C > 0) iota_kernel<<<grid_for(C, TB), TB, 0, st>>>(act[0], C);
+  int n_active = C, cur = 0, rounds = 0;
+  const int max_steps = C + 1;
+  while (n_active > 0) {
+    if (++rounds > C + 2) {
+      set_err(ctx, "replay exceeded %d rounds", C + 2);
+      throw Fail{kErrIterationCap};
+    }
+    CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+    replay_round_kernel<<<grid_for(n_active, TB), TB, 0, st>>>(act[cur], n_active, cord, S.sweep, S.dying, S.c1,
+                                                               S.c2, S.blen, R, max_steps, act[cur ^ 1], cnt,
+                                                               ctx->status);
+    LAUNCH_CHECK("replay_round_kernel");
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h == n_active) {
+      set_err(ctx, "replay made no progress");
+      throw Fail{kErrInternal};
+    }
+    n_active = h;
+    cur ^= 1;
+  }
+  S.rounds_replay = rounds;
+
+  S.arc_len = sget<long long>(ctx, si, X_ALEN, 2 * (size_t)nsurv);
+  S.arc_cl = sget<long long>(ctx, si, X_ACL, 2 * (size_t)nsurv);
+  S.arc_root = sget<int>(ctx, si, X_AROOT, 2 * (size_t)nsurv);
+  S.arc_pos = sget<long long>(ctx, si, X_APOS, 2 * (size_t)nsurv);
+  long long* plen = sget<long long>(ctx, si, X_PLEN, nsurv);
+  long long* send = sget<long long>(ctx, si, X_SEND, nsurv);
+  S.total = 0;
+  if (nsurv > 0) {
+    final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, S.t, S.blen, R, max_steps,
+                                                                S.arc_len, S.arc_cl, S.arc_root, ctx->status);
+    pair_len_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, plen);
+    incl_sum(ctx, plen, send, nsurv, st);
+    arc_pos_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, send, S.arc_pos);
+    last_kernel<long long><<<1, 1, 0, st>>>(send, nsurv, tot);
+    LAUNCH_CHECK("final arcs");
+    readback(ctx, st, tot, 1);
+    S.total = ctx->pinned[0];
+    if (S.total > 2147483647LL) {
+      set_err(ctx, "arc geometry of %lld cells exceeds int32 offsets", S.total);
+      throw Fail{kErrOverflow};
+    }
+  }
+}
+
+int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float thr, unsigned flags, int32_t* grad_out,
+                 int32_t* peaks_out, int32_t* basins_out, dmsc_b200_sizes* sizes, cudaStream_t st) {
+  ctx->valid = false;
+  if (!img || H <= 0 || W <= 0 || !sizes) {
+    set_err(ctx, "invalid argument");
+    return kErrInvalidArgument;
+  }
+  // 32-bit cell ids (input_validation.hxx:24-26)
+  if ((long long)H + 1 > 2147483647LL / 4 / ((long long)W + 1)) {
+    set_err(ctx, "Input is too large for 32-bit cell IDs: %dx%d", H, W);
+    return kErrTooLarge;
+  }
+  const bool dual = flags & DMSC_B200_DUAL;
+  const bool ret_grad = flags & DMSC_B200_RETURN_GRADIENT;
+  const bool f_ridges = flags & DMSC_B200_TRACE_RIDGES, f_valleys = flags & DMSC_B200_TRACE_VALLEYS;
+  const bool f_peaks = flags & DMSC_B200_TRACE_PEAKS, f_basins = flags & DMSC_B200_TRACE_BASINS;
+  if ((ret_grad && !grad_out) || (f_peaks && !peaks_out) || (f_basins && !basins_out)) {
+    set_err(ctx, "missing output buffer for a requested field");
+    return kErrInvalidArgument;
+  }
+  CK(cudaSetDevice(ctx->device));
+  ctx->H = H;
+  ctx->W = W;
+  ctx->dual = dual;
+  ctx->thr = thr;
+  const int Nx = W + 1;
+  const long long nidx = (long long)(H + 1) * Nx;
+  const long long ncells = 4 * nidx;
+  ctx->status = get<unsigned>(ctx, S_STATUS, 4);
+  CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
+
+  // ---- K1 gradient + criticality ----
+  int* grad = ret_grad ? grad_out : get<int>(ctx, S_GRAD, ncells);
+  ctx->grad = grad;
+  const int nsegx = (W + 1 + kTileX - 1) / kTileX;
+  const long long nseg = (long long)(H + 1) * nsegx;
+  uint8_t* mask = get<uint8_t>(ctx, S_MASK, nidx);
+  int* seg[3] = {get<int>(ctx, S_SEG0, nseg), get<int>(ctx, S_SEG1, nseg), get<int>(ctx, S_SEG2, nseg)};
+  int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
+  dim3 g1(nsegx, (H + 1 + kTileY - 1) / kTileY);
+  if (dual)
+    gradient_kernel<true><<<g1, 256, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]);
+  else
+    gradient_kernel<false><<<g1, 256, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]);
+  LAUNCH_CHECK("gradient_kernel");
+  for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);
+  long long* tot = get<long long>(ctx, S_TOT, 8);
+  totals3_kernel<<<1, 1, 0, st>>>(off[0], seg[0], off[1], seg[1], off[2], seg[2], nseg, tot);
+  LAUNCH_CHECK("totals3_kernel");
+  readback(ctx, st, tot, 3);
+  const int nmin = (int)ctx->pinned[0], nsad = (int)ctx->pinned[1], nmax = (int)ctx->pinned[2];
+  ctx->nmin = nmin;
+  ctx->nsad = nsad;
+  ctx->nmax = nmax;
+
+  // ---- K2 ordered compaction ----
+  int* cmin = get<int>(ctx, S_CMIN, nmin);
+  int* csad = get<int>(ctx, S_CSAD, nsad);
+  int* cmax = get<int>(ctx, S_CMAX, nmax);
+  int* rmin = get<int>(ctx, S_RMIN, nidx);
+  int* rmax = get<int>(ctx, S_RMAX, nidx);
+  float* vmin = get<float>(ctx, S_VMIN, nmin);
+  float* vmax = get<float>(ctx, S_VMAX, nmax);
+  float* sval = get<float>(ctx, S_SVAL, nsad);
+  uint32_t* skey = get<uint32_t>(ctx, S_SKEY, nsad);
+  ctx->crit_sad = csad;
+  {
+    unsigned blocks = grid_for(nseg, 8);
+    if (dual)
+      compact_kernel<true><<<blocks, 256, 0, st>>>(img, H, W, nsegx, nseg, mask, off[0], off[1], off[2], cmin, csad,
+                                                   cmax, rmin, rmax, vmin, vmax, sval, skey);
+    else
+      compact_kernel<false><<<blocks, 256, 0, st>>>(img, H, W, nsegx, nseg, mask, off[0], off[1], off[2], cmin, csad,
+                                                    cmax, rmin, rmax, vmin, vmax, sval, skey);
+    LAUNCH_CHECK("compact_kernel");
+  }
+
+  // ---- saddle order: ascending (s_val, cell id) (arcs_topology.hxx:99-102) ----
+  int* iota = get<int>(ctx, S_IOTA, nsad);
+  int* asc = get<int>(ctx, S_ASC, nsad);
+  uint32_t* skey2 = get<uint32_t>(ctx, S_SKEY2, nsad);
+  if (nsad > 0) {
+    iota_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(iota, nsad);
+    sort_pairs(ctx, skey, skey2, iota, asc, nsad, st);
+  }
+
+  // ---- K4 saddle walks ----
+  int* tf = get<int>(ctx, S_TF, 2 * (size_t)nsad);
+  int* lf = get<int>(ctx, S_LF, 2 * (size_t)nsad);
+  int* tv = get<int>(ctx, S_TV, 2 * (size_t)nsad);
+  int* lv = get<int>(ctx, S_LV, 2 * (size_t)nsad);
+  if (nsad > 0) {
+    saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(grad, H, W, nsad, csad, rmax, rmin, tf, lf, tv, lv, ncells,
+                                                          ctx->status);
+    LAUNCH_CHECK("saddle_walk_kernel");
+  }
+
+  // ---- sides ----
+  Side& F = ctx->side[0];
+  Side& V = ctx->side[1];
+  F = Side();
+  V = Side();
+  F.faces = true;
+  V.faces = false;
+  F.M = nmax;
+  V.M = nmin;
+  F.crit = cmax;
+  V.crit = cmin;
+  F.val = vmax;
+  V.val = vmin;
+  F.rank_map = rmax;
+  V.rank_map = rmin;
+  F.t = tf;
+  F.steps = lf;
+  V.t = tv;
+  V.steps = lv;
+  F.arcs = dual ? f_valleys : f_ridges;
+  V.arcs = dual ? f_ridges : f_valleys;
+  F.groups = dual ? f_basins : f_peaks;
+  V.groups = dual ? f_peaks : f_basins;
+
+  uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
+  CK(cudaMemsetAsync(canc, 0, nsad + 4, st));
+  // sweep orders: minima = asc in the primal, reverse in the dual; maxima the reverse of minima
+  run_pairing(ctx, 0, F, asc, !dual, st);
+  run_pairing(ctx, 1, V, asc, dual, st);
+
+  // ---- surviving saddles in minima-sweep order ----
+  int* flag = get<int>(ctx, S_FLAG, nsad);
+  int* fpos = get<int>(ctx, S_FPOS, nsad);
+  ctx->surv = get<int>(ctx, S_SURV, nsad);
+  ctx->nsurv = 0;
+  if (nsad > 0) {
+    survivor_flag_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, V.sweep, canc, flag);
+    excl_sum(ctx, flag, fpos, nsad, st);
+    survivor_list_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, V.sweep, flag, fpos, ctx->surv);
+    last_plus_kernel<int><<<1, 1, 0, st>>>(fpos, flag, nsad, tot);
+    LAUNCH_CHECK("survivors");
+    readback(ctx, st, tot, 1);
+    ctx->nsurv = (int)ctx->pinned[0];
+  }
+  const int nsurv = ctx->nsurv;
+
+  // ---- replay + final arc lengths ----
+  for (int si = 0; si < 2; ++si)
+    if (ctx->side[si].arcs && nsad > 0) run_replay(ctx, si, ctx->side[si], st);
+
+  // ---- labels (region id = rank among alive extrema) ----
+  for (int si = 0; si < 2; ++si) {
+    Side& S = ctx->side[si];
+    if (!S.groups) continue;
+    int32_t* out = S.faces ? (dual ? basins_out : peaks_out) : (dual ? peaks_out : basins_out);
+    long long n = S.faces ? nidx : (long long)H * W;
+    if (S.faces)
+      label_kernel<true><<<grid_for(n, TB), TB, 0, st>>>(grad, H, W, rmax, S.ut, S.to_out, out, ncells, ctx->status);
+    else
+      label_kernel<false><<<grid_for(n, TB), TB, 0, st>>>(grad, H, W, rmin, S.ut, S.to_out, out, ncells,
+                                                           ctx->status);
+    LAUNCH_CHECK("label_kernel");
+  }
+
+  // ---- e rows and alive counts ----
+  for (int si = 0; si < 2; ++si) {
+    Side& S = ctx->side[si];
+    int* ec = sget<int>(ctx, si, X_EROWC, nsurv);
+    S.erow_off = sget<int>(ctx, si, X_EROWO, nsurv);
+    if (nsurv > 0) {
+      erow_count_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, ctx->surv, S.t, S.ut, S.to_out, ec);
+      excl_sum(ctx, ec, S.erow_off, nsurv, st);
+      last_plus_kernel<int><<<1, 1, 0, st>>>(S.erow_off, ec, nsurv, tot + 2 * si);
+    } else {
+      CK(cudaMemsetAsync(tot + 2 * si, 0, sizeof(long long), st));
+    }
+    if (S.M > 0)
+      u8_last_plus_kernel<<<1, 1, 0, st>>>(S.to_out_excl, S.alive, S.M, tot + 2 * si + 1);
+    else
+      CK(cudaMemsetAsync(tot + 2 * si + 1, 0, sizeof(long long), st));
+    LAUNCH_CHECK("e rows");
+  }
+  readback(ctx, st, tot, 4);
+  F.n_erows = (int)ctx->pinned[0];
+  F.n_alive = (int)ctx->pinned[1];
+  V.n_erows = (int)ctx->pinned[2];
+  V.n_alive = (int)ctx->pinned[3];
+  check_status(ctx, st);
+
+  // ---- sizes, public (primal / dual) naming ----
+  Side& PX = dual ? V : F;  // public "max" side
+  Side& PN = dual ? F : V;  // public "min" side
+  dmsc_b200_sizes z{};
+  z.max_pts = PX.n_alive;
+  z.min_pts = PN.n_alive;
+  z.sad_pts = nsurv;
+  z.e_max_rows = PX.n_erows;
+  z.e_min_rows = PN.n_erows;
+  z.p_max = z.p_min = z.ppairs_max = z.ppairs_min = nsurv;
+  z.grad_indices = ret_grad ? ncells : 0;
+  z.peaks_h = f_peaks ? (dual ? H : H + 1) : 0;
+  z.peaks_w = f_peaks ? (dual ? W : W + 1) : 0;
+  z.basins_h = f_basins ? (dual ? H + 1 : H) : 0;
+  z.basins_w = f_basins ? (dual ? W + 1 : W) : 0;
+  z.ridges = f_ridges ? PX.total : 0;
+  z.ridge_offsets = f_ridges ? nsurv + 1 : 0;
+  z.ridge_arc_offsets = f_ridges ? nsurv : 0;
+  z.valleys = f_valleys ? PN.total : 0;
+  z.valley_offsets = f_valleys ? nsurv + 1 : 0;
+  z.valley_arc_offsets = f_valleys ? nsurv : 0;
+  ctx->sizes = z;
+  *sizes = z;
+  ctx->valid = true;
+  return kOk;
+}
+
+void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* offsets, int32_t* arc_offsets,
+               cudaStream_t st) {
+  const int nsurv = ctx->nsurv;
+  long long* send = sget<long long>(ctx, si, X_SEND, nsurv);
+  if (offsets)
+    arc_offsets_kernel<<<grid_for(nsurv + 1LL, TB), TB, 0, st>>>(nsurv, S.arc_len, send, offsets, arc_offsets);
+  LAUNCH_CHECK("arc_offsets_kernel");
+  if (S.total <= 0 || !flat) return;
+  long long cap = S.total;
+  int4* q[2] = {sget<int4>(ctx, si, X_Q0, cap), sget<int4>(ctx, si, X_Q1, cap)};
+  int* cnt = sget<int>(ctx, si, X_CNT, 4);
+  EmitCtx E;
+  E.grad = ctx->grad;
+  E.crit_sad = ctx->crit_sad;
+  E.H = ctx->H;
+  E.W = ctx->W;
+  E.Nx = ctx->W + 1;
+  E.faces = S.faces;
+  E.t = S.t;
+  E.blen = S.blen;
+  E.S = S.R;
+  E.out = flat;
+  E.q_cap = cap;
+  E.max_steps = S.C + 1;
+  E.status = ctx->status;
+  int cur = 0;
+  E.q_out = q[cur];
+  E.n_out = cnt;
+  CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+  emit_roots_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(E, nsurv, ctx->surv, S.arc_pos, S.arc_cl, S.arc_root);
+  LAUNCH_CHECK("emit_roots_kernel");
+  int n = 0, levels = 0;
+  CK(cudaMemcpyAsync(&n, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  while (n > 0) {
+    if (n > cap || ++levels > S.C + 4) {
+      set_err(ctx, "geometry expansion overflow");
+      throw Fail{kErrOverflow};
+    }
+    E.q_out = q[cur ^ 1];
+    CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+    emit_level_kernel<<<grid_for(n, TB), TB, 0, st>>>(E, q[cur], n);
+    LAUNCH_CHECK("emit_level_kernel");
+    CK(cudaMemcpyAsync(&n, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    cur ^= 1;
+  }
+}
+
+int fetch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t st) {
+  if (!ctx->valid || !o) {
+    set_err(ctx, "fetch without a successful extract");
+    return kErrInvalidArgument;
+  }
+  CK(cudaSetDevice(ctx->device));
+  const bool dual = ctx->dual;
+  const int nsurv = ctx->nsurv;
+  Side& F = ctx->side[0];
+  Side& V = ctx->side[1];
+  // extrema lists
+  int32_t* fpts = dual ? o->min_pts : o->max_pts;
+  int32_t* vpts = dual ? o->max_pts : o->min_pts;
+  if (F.M > 0 && fpts)
+    compact_alive_kernel<<<grid_for(F.M, TB), TB, 0, st>>>(F.M, F.alive, F.to_out_excl, F.crit, fpts, F.to_out);
+  if (V.M > 0 && vpts)
+    compact_alive_kernel<<<grid_for(V.M, TB), TB, 0, st>>>(V.M, V.alive, V.to_out_excl, V.crit, vpts, V.to_out);
+  if (nsurv > 0 && o->sad_pts)
+    sad_pts_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->crit_sad, o->sad_pts);
+  LAUNCH_CHECK("point lists");
+  // per-saddle scalars and e rows
+  if (nsurv > 0) {
+    side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(
+        nsurv, true, ctx->surv, F.t, F.ut, F.to_out, F.pers, F.pair_dense, F.erow_off, dual ? o->p_min : o->p_max,
+        dual ? o->ppairs_min : o->ppairs_max, F.n_erows > 0 ? (dual ? o->e_min : o->e_max) : nullptr);
+    side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(
+        nsurv, false, ctx->surv, V.t, V.ut, V.to_out, V.pers, V.pair_dense, V.erow_off, dual ? o->p_max : o->p_min,
+        dual ? o->ppairs_max : o->ppairs_min, V.n_erows > 0 ? (dual ? o->e_max : o->e_min) : nullptr);
+    LAUNCH_CHECK("side_outputs_kernel");
+  }
+  // arc geometry
+  for (int si = 0; si < 2; ++si) {
+    Side& S = ctx->side[si];
+    if (!S.arcs) continue;
+    bool ridges = S.faces != dual;  // faces are ridges in the primal
+    int32_t* flat = ridges ? o->ridges : o->valleys;
+    int32_t* offs = ridges ? o->ridge_offsets : o->valley_offsets;
+    int32_t* aoffs = ridges ? o->ridge_arc_offsets : o->valley_arc_offsets;
+    if (ctx->nsad == 0) {
+      if (offs) CK(cudaMemsetAsync(offs, 0, sizeof(int32_t), st));
+      continue;
+    }
+    emit_side(ctx, si, S, flat, offs, aoffs, st);
+  }
+  check_status(ctx, st);
+  return kOk;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dmsc_b200_create(dmsc_b200_context** out, int device) {
+  if (!out) return kErrInvalidArgument;
+  *out = nullptr;
+  auto* c = new (std::nothrow) dmsc_b200_context();
+  if (!c) return kErrInternal;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaMallocHost(&c->pinned, 64 * sizeof(long long)) != cudaSuccess) {
+    delete c;
+    return kErrCuda;
+  }
+  *out = c;
+  return kOk;
+}
+
+void dmsc_b200_destroy(dmsc_b200_context* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  for (auto& b : c->bufs)
+    if (b.p) cudaFree(b.p);
+  if (c->cub_tmp.p) cudaFree(c->cub_tmp.p);
+  if (c->pinned) cudaFreeHost(c->pinned);
+  delete c;
+}
+
+int dmsc_b200_extract(dmsc_b200_context* ctx, const float* image, int H, int W, float thr, unsigned flags,
+                      int32_t* grad_out, int32_t* peaks_out, int32_t* basins_out, dmsc_b200_sizes* sizes,
+                      void* stream) {
+  if (!ctx) return kErrInvalidArgument;
+  ctx->err.clear();
+  try {
+    return extract_impl(ctx, image, H, W, thr, flags, grad_out, peaks_out, basins_out, sizes, (cudaStream_t)stream);
+  } catch (const Fail& f) {
+    ctx->valid = false;
+    return f.code;
+  }
+}
+
+int dmsc_b200_fetch(dmsc_b200_context* ctx, const dmsc_b200_outputs* out, void* stream) {
+  if (!ctx) return kErrInvalidArgument;
+  ctx->err.clear();
+  try {
+    return fetch_impl(ctx, out, (cudaStream_t)stream);
+  } catch (const Fail& f) {
+    return f.code;
+  }
+}
+
+const char* dmsc_b200_error_string(int code) {
+  switch (code) {
+    case kOk: return "ok";
+    case kErrInvalidArgument: return "invalid argument";
+    case kErrTooLarge: return "input is too large for 32-bit cell ids";
+    case kErrCuda: return "CUDA runtime error";
+    case kErrIterationCap: return "bounded device loop reached its cap";
+    case kErrOverflow: return "output or work queue overflow";
+    default: return "internal error";
+  }
+}
+
+const char* dmsc_b200_last_error(const dmsc_b200_context* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+}  // extern "C"

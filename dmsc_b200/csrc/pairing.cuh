@@ -1,0 +1,236 @@
+// Persistence pairing and cancellation on the device.
+//
+// Reference semantics: cpu/persistence.hxx:16-182. Each side is a sequential
+// union-find sweep over the saddles in sweep order (ascending (s_val, cell id)
+// for minima in the primal, the reverse for maxima; flipped in the dual)
+// with the elder rule: at a saddle joining two components the one whose
+// oldest extremum is younger dies, and the void (-1, one-sided saddles) is
+// older than every extremum.
+//
+// Parallel form (exact). Groups start as single extrema plus the void; a
+// group is named by its oldest member. Every round, each group takes the
+// first (lowest sweep index) saddle leaving it; a group whose partner group
+// has an older oldest member dies at that saddle, which pairs the saddle with
+// the group's oldest member, and joins the partner. Saddles whose ends fall
+// in one group are cycles (pair -1, persistence -1). Why this equals the
+// sweep: a group is always connected, by the time any of its outgoing saddles
+// is swept, to its oldest member, so at its first outgoing saddle the dying
+// side is exactly known; the globally first remaining saddle is always
+// decided, so every round makes progress.
+//
+// The thresholded union-find (the reference's uf_min / uf_max) ends with one
+// component per connected set of cancelled saddles; its root is the unique
+// member not killed by a cancelled saddle, or the void.
+#pragma once
+
+#include <cuda/atomic>
+
+#include "common.cuh"
+
+namespace dmsc {
+
+constexpr uint32_t kNoEdge = 0xFFFFFFFFu;
+constexpr int kUndecided = -2;
+
+// older(a, b) for extremum dense indices; `void_id` is older than all.
+// OLDER_LESS: older = smaller (value, cell) under value_less (minima side in
+// the primal, maxima side in the dual).
+template <bool OLDER_LESS>
+__device__ __forceinline__ bool older(int a, int b, int void_id, const float* __restrict__ val,
+                                      const int* __restrict__ cell) {
+  if (a == void_id) return b != void_id;
+  if (b == void_id) return false;
+  return OLDER_LESS ? tie_lt(val[a], cell[a], val[b], cell[b]) : tie_lt(val[b], cell[b], val[a], cell[a]);
+}
+
+// Round step 1: relabel each active saddle's ends; cycles are decided, the
+// rest offer their sweep index to both groups' minimum.
+__global__ void __launch_bounds__(256) pair_edges_kernel(const int* __restrict__ active, int n_active,
+                                                         const int* __restrict__ c1, const int* __restrict__ c2,
+                                                         int void_id, const int* __restrict__ grp,
+                                                         int* __restrict__ dying, unsigned* __restrict__ minedge,
+                                                         int* __restrict__ next_active, int* __restrict__ n_next) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool keep = false;
+  int e = -1;
+  if (i < n_active) {
+    e = active[i];
+    if (dying[e] == kUndecided) {
+      int a = c1[e], b = c2[e];
+      int ga = grp[a < 0 ? void_id : a], gb = grp[b < 0 ? void_id : b];
+      if (ga == gb) {
+        dying[e] = -1;
+      } else {
+        atomicMin(minedge + ga, (unsigned)e);
+        atomicMin(minedge + gb, (unsigned)e);
+        keep = true;
+      }
+    }
+  }
+  // warp-aggregated append
+  unsigned b = __ballot_sync(0xffffffffu, keep);
+  if (b == 0) return;
+  int lane = threadIdx.x & 31, leader = __ffs(b) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(n_next, __popc(b));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (keep) next_active[base + __popc(b & ((1u << lane) - 1u))] = e;
+}
+
+// Round step 2: each group root with an outgoing saddle decides.
+template <bool OLDER_LESS>
+__global__ void __launch_bounds__(256) pair_groups_kernel(int n_nodes, int void_id, const int* __restrict__ c1,
+                                                          const int* __restrict__ c2, const int* __restrict__ grp,
+                                                          unsigned* __restrict__ minedge, int* __restrict__ link,
+                                                          int* __restrict__ dying, const float* __restrict__ val,
+                                                          const int* __restrict__ cell) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_nodes) return;
+  unsigned me = minedge[g];
+  if (me == kNoEdge) return;
+  minedge[g] = kNoEdge;
+  int e = (int)me;
+  int a = c1[e], b = c2[e];
+  int ga = grp[a < 0 ? void_id : a], gb = grp[b < 0 ? void_id : b];
+  int h = (ga == g) ? gb : ga;
+  if (older<OLDER_LESS>(h, g, void_id, val, cell)) {
+    link[g] = h;
+    dying[e] = g;
+  }
+}
+
+// Round step 3: every node's group becomes the root of its group's link chain.
+__global__ void __launch_bounds__(256) pair_jump_kernel(int n_nodes, int* __restrict__ grp,
+                                                        const int* __restrict__ link, unsigned* status) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_nodes) return;
+  int r = grp[x];
+  int guard = 0;
+  while (link[r] != r) {
+    r = link[r];
+    if (++guard > n_nodes) {
+      set_status(status, kStatusRoundCap);
+      break;
+    }
+  }
+  grp[x] = r;
+}
+
+__global__ void iota_kernel(int* __restrict__ a, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+
+__global__ void fill_kernel(int* __restrict__ a, long long n, int v) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+// Builds the sweep-ordered edge list of one side: edge j is saddle
+// sweep[j] with ends (t[2s], t[2s+1]).
+__global__ void sweep_edges_kernel(int nsad, const int* __restrict__ asc, bool reverse, const int* __restrict__ t,
+                                   int* __restrict__ sweep, int* __restrict__ c1, int* __restrict__ c2,
+                                   int* __restrict__ dying) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nsad) return;
+  int s = reverse ? asc[nsad - 1 - j] : asc[j];
+  sweep[j] = s;
+  c1[j] = t[2 * s];
+  c2[j] = t[2 * s + 1];
+  dying[j] = kUndecided;
+}
+
+// Persistence of each decided saddle and cancellation (persistence.hxx:82-104,
+// 139-161). MIN_SIDE selects the formula; `sbit` marks the side in `cancelled`.
+__global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_side, bool dual, float thr,
+                                                          const int* __restrict__ sweep,
+                                                          const int* __restrict__ dying,
+                                                          const float* __restrict__ sad_val,
+                                                          const float* __restrict__ ext_val,
+                                                          int* __restrict__ pair_dense, float* __restrict__ pers,
+                                                          uint8_t* __restrict__ cancelled, uint8_t sbit,
+                                                          uint8_t* __restrict__ alive) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nsad) return;
+  int s = sweep[j], d = dying[j];
+  if (d < 0) {
+    pair_dense[s] = -1;
+    pers[s] = -1.0f;
+    return;
+  }
+  float sv = sad_val[s], ev = ext_val[d];
+  float p;
+  if (min_side)
+    p = dual ? ev - sv : sv - ev;
+  else
+    p = dual ? sv - ev : ev - sv;
+  pair_dense[s] = d;
+  pers[s] = p;
+  if (p <= thr) {
+    atomicOr((unsigned*)(cancelled + (s & ~3)), (unsigned)sbit << (8 * (s & 3)));
+    alive[d] = 0;
+  }
+}
+
+// Thresholded union-find: lock-free union of the ends of every cancelled
+// saddle (link the larger root under the smaller).
+__device__ __forceinline__ int uf_root(int* p, int x) {
+  while (true) {
+    int px = p[x];
+    if (px == x) return x;
+    int ppx = p[px];
+    if (ppx != px) p[x] = ppx;  // path halving; benign race
+    x = ppx;
+  }
+}
+
+__global__ void __launch_bounds__(256) ut_union_kernel(int nsad, const int* __restrict__ sweep,
+                                                       const int* __restrict__ dying, const int* __restrict__ c1,
+                                                       const int* __restrict__ c2, const float* __restrict__ pers,
+                                                       float thr, int void_id, int* __restrict__ p) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nsad) return;
+  if (dying[j] < 0) return;
+  if (!(pers[sweep[j]] <= thr)) return;
+  int a = c1[j] < 0 ? void_id : c1[j];
+  int b = c2[j] < 0 ? void_id : c2[j];
+  while (true) {
+    a = uf_root(p, a);
+    b = uf_root(p, b);
+    if (a == b) return;
+    if (a > b) {
+      int t = a;
+      a = b;
+      b = t;
+    }
+    if (atomicCAS(p + b, b, a) == b) return;
+  }
+}
+
+__global__ void ut_flatten_kernel(int n, int* __restrict__ p) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n) return;
+  int r = x;
+  while (p[r] != r) r = p[r];
+  p[x] = r;
+}
+
+// Component root = its alive member, or -1 for the void's component.
+__global__ void ut_mark_kernel(int n_ext, const int* __restrict__ p, const uint8_t* __restrict__ alive,
+                               int* __restrict__ comp_root) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x > n_ext) return;
+  if (x == n_ext)
+    comp_root[p[x]] = -1;
+  else if (alive[x])
+    comp_root[p[x]] = x;
+}
+
+__global__ void ut_root_kernel(int n_ext, const int* __restrict__ p, const int* __restrict__ comp_root,
+                               int* __restrict__ ut) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_ext) return;
+  ut[x] = comp_root[p[x]];
+}
+
+}  // namespace dmsc

@@ -1,0 +1,322 @@
+// Arc simplification: replay of the cancellations and emission of the
+// simplified arc geometry.
+//
+// Reference semantics: cpu/arcs_simplification.hxx:310-504. The cancellations
+// of one side are replayed in (persistence, saddle cell, target cell) order on
+// a union-find whose roots are extrema. For a cancellation of saddle s killing
+// extremum d, with arc targets T0 and T1: R0 = Find(T0), R1 = Find(T1); if
+// R0 == d != R1 then d is linked under R1 (symmetric for R1 == d); otherwise
+// the cancellation is skipped. Every link carries a path: the geometry from d
+// back along the dying side's arc through s and on to the other root.
+//
+// Parallel form (exact). Links never move once made and link times increase
+// along every parent chain, so the root of x just before replay step t is the
+// first node on x's parent chain that is not linked before t. Each unresolved
+// cancellation walks its two chains; it can decide as soon as every node it
+// passes has been decided, and decisions are final, so rounds of such walks
+// reproduce the sequential replay (including skips, which arise only from
+// ties in persistence). Path lengths are summed along the same walks.
+//
+// Geometry. A link's path W(d) is
+//   reverse(chain(T_dying -> d)) + reverse(arc_dying) + arc_other + chain(T_other -> R)
+// where chain(x -> R) concatenates W along x's parent chain up to R, and every
+// surviving saddle's final arc is arc + chain(T -> root). These are expanded
+// breadth-first as tasks that each cover a known output range; raw arcs are
+// re-walked from their start cells when written.
+#pragma once
+
+#include <cuda/atomic>
+
+#include "common.cuh"
+#include "walks.cuh"
+
+namespace dmsc {
+
+constexpr int kNever = 0x7FFFFFFF;
+enum : int { kPending = 0, kLinked = 1, kRootForever = 2 };
+
+struct ReplayState {
+  int* ctime;       // [M] replay rank of the cancellation killing the node, kNever if none
+  int* status;      // [M] kPending / kLinked / kRootForever
+  int* parent;      // [M] link target (-1 = void) when kLinked
+  long long* wlen;  // [M] length of W(node)
+  int* side;        // [M] dying side (0/1) of the node's cancellation
+  int* csad;        // [M] saddle of the node's cancellation
+  long long* cl_dy; // [M] chain length T_dying -> node at link time
+  long long* cl_ot; // [M] chain length T_other -> parent at link time
+};
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  return cuda::atomic_ref<const int, cuda::thread_scope_device>(*p).load(cuda::memory_order_acquire);
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  cuda::atomic_ref<int, cuda::thread_scope_device>(*p).store(v, cuda::memory_order_release);
+}
+
+// Root of x just before replay step t, with the summed path length; returns
+// false when a node on the way is still undecided.
+__device__ __forceinline__ bool walk_root(const ReplayState& S, int x, int t, int* root, long long* acc,
+                                          int max_steps, unsigned* status) {
+  long long a = 0;
+  int steps = 0;
+  while (true) {
+    if (x < 0) break;
+    if (S.ctime[x] >= t) break;
+    int st = ld_acquire(S.status + x);
+    if (st == kPending) return false;
+    if (st == kRootForever) break;
+    a += S.wlen[x];
+    x = S.parent[x];
+    if (++steps > max_steps) {
+      set_status(status, kStatusChainCap);
+      break;
+    }
+  }
+  *root = x;
+  *acc = a;
+  return true;
+}
+
+// Cancellation list of one side in sweep order -> (key, sweep index).
+__global__ void cancel_collect_kernel(int nsad, const int* __restrict__ sweep, const int* __restrict__ dying,
+                                      const float* __restrict__ pers, float thr, const int* __restrict__ crit_sad,
+                                      unsigned long long* __restrict__ keys, int* __restrict__ vals,
+                                      int* __restrict__ count) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  bool take = false;
+  unsigned long long key = 0;
+  if (j < nsad && dying[j] >= 0) {
+    float p = pers[sweep[j]];
+    if (p <= thr) {
+      take = true;
+      // CancelEvent::operator< (cpu/persistence_struct.hxx:16-21); a saddle is
+      // cancelled at most once per side, so (persistence, saddle) is unique.
+      key = ((unsigned long long)orderable_key(p) << 32) | (unsigned)crit_sad[sweep[j]];
+    }
+  }
+  unsigned b = __ballot_sync(0xffffffffu, take);
+  if (b == 0) return;
+  int lane = threadIdx.x & 31, leader = __ffs(b) - 1, base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(b));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (take) {
+    int p = base + __popc(b & ((1u << lane) - 1u));
+    keys[p] = key;
+    vals[p] = j;
+  }
+}
+
+// ctime[d] = replay rank of d's cancellation.
+__global__ void replay_init_kernel(int C, const int* __restrict__ order, const int* __restrict__ dying,
+                                   ReplayState S) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= C) return;
+  int d = dying[order[r]];
+  S.ctime[d] = r;
+  S.status[d] = kPending;
+}
+
+// One resolution round over the unresolved cancellations (by replay rank).
+__global__ void __launch_bounds__(256) replay_round_kernel(const int* __restrict__ active, int n_active,
+                                                          const int* __restrict__ order, const int* __restrict__ sweep,
+                                                          const int* __restrict__ dying, const int* __restrict__ c1,
+                                                          const int* __restrict__ c2, const long long* __restrict__ blen,
+                                                          ReplayState S, int max_steps, int* __restrict__ next_active,
+                                                          int* __restrict__ n_next, unsigned* status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool keep = false;
+  int r = -1;
+  if (i < n_active) {
+    r = active[i];
+    int j = order[r];
+    int d = dying[j], s = sweep[j];
+    int T0 = c1[j], T1 = c2[j];
+    int R0, R1;
+    long long a0, a1;
+    bool ok0 = walk_root(S, T0, r, &R0, &a0, max_steps, status);
+    bool ok1 = ok0 && walk_root(S, T1, r, &R1, &a1, max_steps, status);
+    if (!ok0 || !ok1) {
+      keep = true;
+    } else {
+      int k = -1;
+      if (R0 == d && R0 != R1)
+        k = 0;
+      else if (R1 == d && R0 != R1)
+        k = 1;
+      if (k >= 0) {
+        S.parent[d] = k == 0 ? R1 : R0;
+        S.side[d] = k;
+        S.csad[d] = s;
+        S.cl_dy[d] = k == 0 ? a0 : a1;
+        S.cl_ot[d] = k == 0 ? a1 : a0;
+        S.wlen[d] = blen[2 * s] + blen[2 * s + 1] + a0 + a1;
+        st_release(S.status + d, kLinked);
+      } else {
+        st_release(S.status + d, kRootForever);
+      }
+    }
+  }
+  unsigned b = __ballot_sync(0xffffffffu, keep);
+  if (b == 0) return;
+  int lane = threadIdx.x & 31, leader = __ffs(b) - 1, base = 0;
+  if (lane == leader) base = atomicAdd(n_next, __popc(b));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (keep) next_active[base + __popc(b & ((1u << lane) - 1u))] = r;
+}
+
+// Base arc length in cells: steps + 1 for a valid arc, 0 otherwise
+// (cpu/arcs_geometry.hxx:35-49, 83-111).
+__global__ void base_len_kernel(int n2, const int* __restrict__ t, const int* __restrict__ steps,
+                                long long* __restrict__ blen) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n2) return;
+  blen[a] = t[a] >= 0 ? (long long)steps[a] + 1 : 0;
+}
+
+// Final arcs of the surviving saddles: length and the chain root of each
+// (survivor i in output order, arc j). `surv_sad[i]` = dense saddle index.
+__global__ void final_arcs_kernel(int nsurv, const int* __restrict__ surv_sad, const int* __restrict__ t,
+                                  const long long* __restrict__ blen, ReplayState S, int max_steps,
+                                  long long* __restrict__ arc_len, long long* __restrict__ arc_cl,
+                                  int* __restrict__ arc_root, unsigned* status) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 2 * nsurv) return;
+  int i = q >> 1, j = q & 1;
+  int s = surv_sad[i];
+  int T = t[2 * s + j];
+  if (T < 0) {
+    arc_len[q] = 0;
+    arc_cl[q] = 0;
+    arc_root[q] = -1;
+    return;
+  }
+  int R;
+  long long a;
+  walk_root(S, T, kNever, &R, &a, max_steps, status);
+  arc_len[q] = blen[2 * s + j] + a;
+  arc_cl[q] = a;
+  arc_root[q] = R;
+}
+
+// ---------------------------------------------------------------------------
+// geometry emission
+// ---------------------------------------------------------------------------
+enum : int { kTaskBase = 0, kTaskW = 1, kTaskChain = 2 };
+// task = {kind | dir << 2, a, b, pos}; base: a = saddle, b = arc; W: a = node;
+// chain: a = start node, b = stop node (-1 = void).
+__device__ __forceinline__ int4 make_task(int kind, int rev, int a, int b, long long pos) {
+  return make_int4(kind | (rev << 2), a, b, (int)pos);
+}
+
+struct EmitCtx {
+  const int* grad;
+  const int* crit_sad;
+  int H, W, Nx;
+  bool faces;
+  const int* t;            // per arc target
+  const long long* blen;   // per arc length
+  ReplayState S;
+  int* out;
+  int4* q_out;
+  int* n_out;
+  long long q_cap;
+  int max_steps;
+  unsigned* status;
+};
+
+__device__ __forceinline__ void push_task(const EmitCtx& E, int4 task) {
+  int p = atomicAdd(E.n_out, 1);
+  if (p < E.q_cap)
+    E.q_out[p] = task;
+  else
+    set_status(E.status, kStatusQueueOverflow);
+}
+
+// Writes raw arc (s, j): the V-path from its start cell, `len` cells.
+__device__ void emit_base(const EmitCtx& E, int s, int j, int rev, long long pos) {
+  long long len = E.blen[2 * s + j];
+  if (len <= 0) return;
+  int sc = E.crit_sad[s];
+  int curr = E.faces ? face_start(sc, j, E.Nx) : vertex_start(sc, j, E.H, E.W, E.Nx);
+  for (long long k = 0; k < len; ++k) {
+    E.out[rev ? pos + len - 1 - k : pos + k] = curr;
+    if (k + 1 < len) {
+      int e = __ldg(E.grad + curr);
+      curr = E.faces ? next_face(e, curr, E.Nx) : next_vertex(e, curr, E.H, E.W, E.Nx);
+    }
+  }
+}
+
+__device__ void emit_chain(const EmitCtx& E, int x, int stop, int rev, long long pos) {
+  long long total = 0;
+  if (rev) {
+    int z = x, steps = 0;
+    while (z != stop && z >= 0) {
+      total += E.S.wlen[z];
+      z = E.S.parent[z];
+      if (++steps > E.max_steps) break;
+    }
+  }
+  long long p = 0;
+  int z = x, steps = 0;
+  while (z != stop && z >= 0) {
+    long long w = E.S.wlen[z];
+    push_task(E, make_task(kTaskW, rev, z, 0, rev ? pos + total - p - w : pos + p));
+    p += w;
+    z = E.S.parent[z];
+    if (++steps > E.max_steps) {
+      set_status(E.status, kStatusChainCap);
+      break;
+    }
+  }
+}
+
+__device__ void emit_w(const EmitCtx& E, int d, int rev, long long pos) {
+  int k = E.S.side[d], o = 1 - k, s = E.S.csad[d];
+  int Tk = E.t[2 * s + k], To = E.t[2 * s + o];
+  long long la = E.S.cl_dy[d], lb = E.blen[2 * s + k], lc = E.blen[2 * s + o], ld = E.S.cl_ot[d];
+  int R = E.S.parent[d];
+  if (!rev) {
+    // reverse(chain(Tk -> d)) + reverse(arc k) + arc o + chain(To -> R)
+    if (la > 0) push_task(E, make_task(kTaskChain, 1, Tk, d, pos));
+    if (lb > 0) emit_base(E, s, k, 1, pos + la);
+    if (lc > 0) emit_base(E, s, o, 0, pos + la + lb);
+    if (ld > 0) push_task(E, make_task(kTaskChain, 0, To, R, pos + la + lb + lc));
+  } else {
+    if (ld > 0) push_task(E, make_task(kTaskChain, 1, To, R, pos));
+    if (lc > 0) emit_base(E, s, o, 1, pos + ld);
+    if (lb > 0) emit_base(E, s, k, 0, pos + ld + lc);
+    if (la > 0) push_task(E, make_task(kTaskChain, 0, Tk, d, pos + ld + lc + lb));
+  }
+}
+
+// Level 0: every surviving arc's own raw arc, then its chain.
+__global__ void emit_roots_kernel(EmitCtx E, int nsurv, const int* __restrict__ surv_sad,
+                                  const long long* __restrict__ arc_pos, const long long* __restrict__ arc_cl,
+                                  const int* __restrict__ arc_root) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 2 * nsurv) return;
+  int i = q >> 1, j = q & 1;
+  int s = surv_sad[i];
+  int T = E.t[2 * s + j];
+  if (T < 0) return;
+  long long pos = arc_pos[q];
+  long long bl = E.blen[2 * s + j];
+  emit_base(E, s, j, 0, pos);
+  if (arc_cl[q] > 0) push_task(E, make_task(kTaskChain, 0, T, arc_root[q], pos + bl));
+}
+
+__global__ void emit_level_kernel(EmitCtx E, const int4* __restrict__ q_in, int n_in) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_in) return;
+  int4 t = q_in[i];
+  int kind = t.x & 3, rev = (t.x >> 2) & 1;
+  if (kind == kTaskW)
+    emit_w(E, t.y, rev, t.w);
+  else if (kind == kTaskChain)
+    emit_chain(E, t.y, t.z, rev, t.w);
+  else
+    emit_base(E, t.y, t.z, rev, t.w);
+}
+
+}  // namespace dmsc

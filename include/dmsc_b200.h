@@ -1,0 +1,120 @@
+/*
+ * dmsc_b200.h -- C ABI of the B200 (sm_100a) discrete Morse-Smale complex path.
+ *
+ * These entry points replace the reference's CUDA-side native entry
+ *   dmsc_gpu.extract_dmsc(scalar_field, persistence_threshold, return_gradient,
+ *                         is_dual, trace_max_arcs, trace_min_arcs,
+ *                         trace_max_groups, trace_min_groups)
+ * (dmsc/csrc/dmsc_gpu.cpp:128-180, bound at dmsc/csrc/dmsc_gpu.cpp:249-253),
+ * which returns the 19-field DMSComplex (dmsc/csrc/dmsc_struct.hxx:5-30).
+ * Every pointer below is a device pointer unless stated otherwise; the stream
+ * argument is a cudaStream_t passed as void*.
+ *
+ * A call is two phases because most output sizes depend on the data:
+ *   1. dmsc_b200_extract() runs the whole pipeline on the device, writes the
+ *      fixed-size outputs (grad_indices, peaks, basins) into caller buffers and
+ *      returns every variable output size (one device->host read of sizes);
+ *   2. dmsc_b200_fetch() writes the variable-size outputs into caller buffers
+ *      sized from phase 1.
+ * A context keeps the device workspace between the two phases and across
+ * calls; a context is not thread-safe, use one per host thread.
+ */
+#ifndef DMSC_B200_H
+#define DMSC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes. */
+#define DMSC_B200_OK 0
+#define DMSC_B200_ERR_INVALID_ARGUMENT 1 /* bad pointer, size or flag */
+#define DMSC_B200_ERR_TOO_LARGE 2        /* 4*(H+1)*(W+1) exceeds int32 cell ids (input_validation.hxx:24-26) */
+#define DMSC_B200_ERR_CUDA 3             /* a CUDA runtime call failed */
+#define DMSC_B200_ERR_ITERATION_CAP 4    /* a bounded device loop hit its cap */
+#define DMSC_B200_ERR_OVERFLOW 5         /* an output exceeds int32 offsets or a work queue */
+#define DMSC_B200_ERR_INTERNAL 6
+
+/* Flags (the reference keyword arguments, dmsc/dmsc.py:230-239, 262-271). */
+#define DMSC_B200_DUAL 1u           /* is_dual */
+#define DMSC_B200_RETURN_GRADIENT 2u /* return_gradient */
+#define DMSC_B200_TRACE_RIDGES 4u   /* trace_ridges  (native trace_max_arcs) */
+#define DMSC_B200_TRACE_VALLEYS 8u  /* trace_valleys (native trace_min_arcs) */
+#define DMSC_B200_TRACE_PEAKS 16u   /* trace_peaks   (native trace_max_groups) */
+#define DMSC_B200_TRACE_BASINS 32u  /* trace_basins  (native trace_min_groups) */
+
+typedef struct dmsc_b200_context dmsc_b200_context;
+
+/* Element counts of the 19 outputs of one image (DMSComplex field order).
+   2-D outputs give rows and columns. A field that was not requested has
+   count 0 (the reference returns an empty tensor for it). */
+typedef struct {
+  int64_t max_pts, min_pts, sad_pts;
+  int64_t e_max_rows, e_min_rows; /* e_max / e_min are [rows, 2] int32 */
+  int64_t p_max, p_min, ppairs_max, ppairs_min;
+  int64_t grad_indices;
+  int64_t peaks_h, peaks_w;
+  int64_t ridges, ridge_offsets, ridge_arc_offsets;
+  int64_t basins_h, basins_w;
+  int64_t valleys, valley_offsets, valley_arc_offsets;
+} dmsc_b200_sizes;
+
+/* Variable-size outputs of phase 2 (device pointers; NULL when the size is 0).
+   int32 everywhere except p_max / p_min (float32). */
+typedef struct {
+  int32_t* max_pts;
+  int32_t* min_pts;
+  int32_t* sad_pts;
+  int32_t* e_max;
+  int32_t* e_min;
+  float* p_max;
+  float* p_min;
+  int32_t* ppairs_max;
+  int32_t* ppairs_min;
+  int32_t* ridges;
+  int32_t* ridge_offsets;
+  int32_t* ridge_arc_offsets;
+  int32_t* valleys;
+  int32_t* valley_offsets;
+  int32_t* valley_arc_offsets;
+} dmsc_b200_outputs;
+
+/* Creates a context bound to CUDA device `device`. Replaces the per-call
+   gpu::Workspace of the reference (dmsc/csrc/dmsc_gpu.cpp:141-148). */
+int dmsc_b200_create(dmsc_b200_context** ctx, int device);
+
+/* Frees the context and its device workspace. */
+void dmsc_b200_destroy(dmsc_b200_context* ctx);
+
+/* Phase 1 for one H x W float32 image in device memory (row-major,
+   contiguous). Replaces extract_single_dmsc_gpu_t up to output assembly
+   (dmsc/csrc/dmsc_gpu.cpp:53-82) and the size part of gpu::Workspace::complex
+   (dmsc/csrc/gpu/workspace.hxx:91-397).
+   `grad_out`   : int32[4*(H+1)*(W+1)] when DMSC_B200_RETURN_GRADIENT, else NULL.
+   `peaks_out`  : int32[(H+1)*(W+1)] in the primal, int32[H*W] in the dual,
+                  when DMSC_B200_TRACE_PEAKS, else NULL.
+   `basins_out` : int32[H*W] in the primal, int32[(H+1)*(W+1)] in the dual,
+                  when DMSC_B200_TRACE_BASINS, else NULL.
+   `persistence_threshold` is compared as float32, as the reference's C++
+   `float` parameter is. Writes `sizes` (host pointer). */
+int dmsc_b200_extract(dmsc_b200_context* ctx, const float* image, int H, int W, float persistence_threshold,
+                      unsigned flags, int32_t* grad_out, int32_t* peaks_out, int32_t* basins_out,
+                      dmsc_b200_sizes* sizes, void* stream);
+
+/* Phase 2: writes the variable-size outputs of the last extract() on this
+   context. `out` is a host pointer to a struct of device pointers. */
+int dmsc_b200_fetch(dmsc_b200_context* ctx, const dmsc_b200_outputs* out, void* stream);
+
+/* Static description of a return code. */
+const char* dmsc_b200_error_string(int code);
+
+/* Message of the last failure on this context (empty when none). */
+const char* dmsc_b200_last_error(const dmsc_b200_context* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DMSC_B200_H */

@@ -464,7 +464,7 @@ static void write_geom(const dag_t* g, path_ref path, int32_t* out, int64_t star
 /* result object                                                             */
 /* ------------------------------------------------------------------------ */
 #define NF_OUT 19
-#define NF_DBG 16
+#define NF_DBG 23
 #define NF_ALL (NF_OUT + NF_DBG)
 
 typedef struct {
@@ -863,6 +863,28 @@ void* dmsc_oracle_run(const float* img, int H, int W, float thr, int flags) {
       dbg_pair_max[k] = smax[j].pair_id;
       dbg_pers_max[k] = smax[j].persistence;
     }
+  }
+  /* debug: sweep-order events (saddle dense idx, c1, c2) per side */
+  int32_t* dbg_ev_min = (int32_t*)xmalloc(3LL * nsad, sizeof(int32_t));
+  int32_t* dbg_ev_max = (int32_t*)xmalloc(3LL * nsad, sizeof(int32_t));
+  for (int j = 0; j < nsad; ++j) {
+    dbg_ev_min[3 * j] = smin[j].saddle_id >= 0 ? fcm[smin[j].saddle_id] : -1;
+    dbg_ev_min[3 * j + 1] = smin[j].c1;
+    dbg_ev_min[3 * j + 2] = smin[j].c2;
+    dbg_ev_max[3 * j] = smax[j].saddle_id >= 0 ? fcm[smax[j].saddle_id] : -1;
+    dbg_ev_max[3 * j + 1] = smax[j].c1;
+    dbg_ev_max[3 * j + 2] = smax[j].c2;
+  }
+  int32_t* dbg_arcs = (int32_t*)xmalloc(8LL * nsad, sizeof(int32_t));
+  for (int i = 0; i < nsad; ++i) {
+    dbg_arcs[8 * i + 0] = nodes[i].max_arcs[0].target;
+    dbg_arcs[8 * i + 1] = nodes[i].max_arcs[0].length;
+    dbg_arcs[8 * i + 2] = nodes[i].max_arcs[1].target;
+    dbg_arcs[8 * i + 3] = nodes[i].max_arcs[1].length;
+    dbg_arcs[8 * i + 4] = nodes[i].min_arcs[0].target;
+    dbg_arcs[8 * i + 5] = nodes[i].min_arcs[0].length;
+    dbg_arcs[8 * i + 6] = nodes[i].min_arcs[1].target;
+    dbg_arcs[8 * i + 7] = nodes[i].min_arcs[1].length;
   }
   /* erase cancelled saddles from both sorted lists (persistence.hxx:164-181) */
   for (int i = 0; i < n_removed; ++i) fcm[removed[i]] = -1;
@@ -1310,8 +1332,19 @@ void* dmsc_oracle_run(const float* img, int H, int W, float thr, int flags) {
   set_i(R, 32, idup(uf_max, nmax), nmax);
   set_i(R, 33, dbg_rep_par_min, nmin); /* replay parents at link time */
   set_i(R, 34, dbg_rep_par_max, nmax);
-  free(dbg_cancel_max);
-  free(dbg_cancel_min);
+  set_i2(R, 35, dbg_ev_min, nsad, 3);
+  set_i2(R, 36, dbg_ev_max, nsad, 3);
+  set_i2(R, 37, dbg_arcs, nsad, 8);
+  set_i2(R, 38, dbg_cancel_min ? dbg_cancel_min : (int32_t*)xmalloc(0, 4), dbg_cancel_min ? n_min_c : 0, 3);
+  set_i2(R, 39, dbg_cancel_max ? dbg_cancel_max : (int32_t*)xmalloc(0, 4), dbg_cancel_max ? n_max_c : 0, 3);
+  {
+    float* mv = (float*)xmalloc(nmin, sizeof(float));
+    memcpy(mv, min_vals, (size_t)nmin * sizeof(float));
+    set_f(R, 40, mv, nmin);
+    float* xv = (float*)xmalloc(nmax, sizeof(float));
+    memcpy(xv, max_vals, (size_t)nmax * sizeof(float));
+    set_f(R, 41, xv, nmax);
+  }
 
   free(pw);
   free(mins.a);

@@ -30,7 +30,7 @@ FIELDS = (
 DEBUG_FIELDS = (
     "paired_with crit_mins crit_saddles crit_maxes saddle_values saddle_order_desc "
     "pair_min pers_min pair_max pers_max min_alive max_alive uf_min uf_max "
-    "replay_parent_min replay_parent_max"
+    "replay_parent_min replay_parent_max ev_min ev_max raw_arcs cancels_min cancels_max min_vals max_vals"
 ).split()
 
 FL_DUAL, FL_GRAD, FL_RIDGES, FL_VALLEYS, FL_PEAKS, FL_BASINS = 1, 2, 4, 8, 16, 32

@@ -1,0 +1,150 @@
+"""Parity of the CUDA path (through the C ABI) with the reference: bit-exact on
+every output against the golden fixtures and the C oracle."""
+
+import numpy as np
+import pytest
+import torch
+
+from tests.helpers import FIELDS, diff_fields, golden_cases, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_run(img, thr, fl, dual):
+    from dmsc_b200 import extract_dmsc
+
+    return extract_dmsc(img.cuda(), thr, fl[0], dual, fl[1], fl[2], fl[3], fl[4])
+
+
+@pytest.mark.parametrize("name,path", list(golden_cases()))
+def test_golden(name, path):
+    img, thr, dual, fl, expected = load_golden(path)
+    got = gpu_run(img, thr, fl, dual)
+    assert diff_fields(got, expected) == []
+
+
+def _random_field(rng, kind, H, W):
+    if kind == 0:
+        a = rng.standard_normal((H, W))
+    elif kind == 1:
+        a = rng.integers(0, 3, (H, W))
+    elif kind == 2:
+        a = rng.integers(0, 64, (H, W)) / 64.0
+    elif kind == 3:
+        a = rng.random((H, W))
+    else:
+        y, x = np.mgrid[0:H, 0:W]
+        a = np.sin(x / 5.0) * np.cos(y / 7.0) + 0.05 * rng.standard_normal((H, W))
+    return torch.from_numpy(a.astype(np.float32))
+
+
+def test_random_small_vs_oracle(oracle_mod):
+    rng = np.random.default_rng(7)
+    for it in range(250):
+        H, W = int(rng.integers(1, 40)), int(rng.integers(1, 40))
+        img = _random_field(rng, it % 5, H, W)
+        thr = float(rng.choice([-1.0, 0.0, 0.05, 0.1, 0.5, 2.0]))
+        dual = bool(rng.integers(0, 2))
+        fl = [bool(v) for v in rng.integers(0, 2, 5)]
+        exp = oracle_mod.run(img, thr, fl[0], dual, fl[1], fl[2], fl[3], fl[4])
+        got = gpu_run(img, thr, fl, dual)
+        assert diff_fields(got, exp) == [], (it, H, W, thr, dual, fl)
+
+
+@pytest.mark.parametrize("dual", [False, True])
+@pytest.mark.parametrize("thr", [0.0, 0.1])
+def test_bump_256(oracle_mod, dual, thr):
+    from dmsc_b200.synthetic import field_256_bumps
+
+    img = field_256_bumps(seed=3)
+    exp = oracle_mod.run(img, thr, True, dual, True, True, True, True)
+    got = gpu_run(img, thr, [True] * 5, dual)
+    assert diff_fields(got, exp) == []
+
+
+@pytest.mark.parametrize("dual", [False, True])
+@pytest.mark.parametrize("thr", [0.0, 0.05])
+def test_bump_1024(oracle_mod, dual, thr):
+    from dmsc_b200.synthetic import field_4096_bumps
+
+    img = field_4096_bumps(seed=5, size=1024)
+    exp = oracle_mod.run(img, thr, True, dual, True, True, True, True)
+    got = gpu_run(img, thr, [True] * 5, dual)
+    assert diff_fields(got, exp) == []
+
+
+def test_uniform_ties(oracle_mod):
+    """i.i.d. 12-bit uniform values: heavy ties and zero-persistence pairs."""
+    rng = np.random.default_rng(11)
+    for thr, size in ((0.0, 512), (0.5, 96)):
+        img = torch.from_numpy((rng.integers(0, 1 << 12, (size, size)) / (1 << 12)).astype(np.float32))
+        for dual in (False, True):
+            exp = oracle_mod.run(img, thr, True, dual, True, True, True, True)
+            got = gpu_run(img, thr, [True] * 5, dual)
+            assert diff_fields(got, exp) == [], (thr, size, dual)
+
+
+def test_batch_matches_sequential():
+    from dmsc_b200 import compute_dmsc
+
+    fields = torch.randn((3, 9, 7), generator=torch.Generator().manual_seed(8)).cuda()
+    batched = compute_dmsc(fields, 0.15)
+    sequential = [compute_dmsc(f, 0.15) for f in fields]
+    for a, b in zip(batched, sequential):
+        assert diff_fields(list(a), list(b)) == []
+        assert all(x.device == y.device for x, y in zip(a, b))
+
+
+def test_noncontiguous_input():
+    from dmsc_b200 import compute_dmsc
+
+    field = torch.randn((7, 11), generator=torch.Generator().manual_seed(4)).cuda().transpose(0, 1)
+    assert not field.is_contiguous()
+    assert diff_fields(list(compute_dmsc(field, 0.1)), list(compute_dmsc(field.contiguous(), 0.1))) == []
+
+
+def test_cpu_input_returns_cpu_outputs(oracle_mod):
+    from dmsc_b200 import compute_dmsc
+
+    img = torch.randn((13, 10), generator=torch.Generator().manual_seed(2))
+    ms = compute_dmsc(img, 0.1)
+    assert all(t.device.type == "cpu" for t in ms)
+    exp = oracle_mod.compute_dmsc(img, 0.1)
+    assert diff_fields(list(ms), exp) == []
+
+
+def test_output_devices():
+    from dmsc_b200 import compute_dmsc
+
+    ms = compute_dmsc(torch.randn((8, 8), device="cuda"), 0.1)
+    assert ms.shape.device.type == "cpu"
+    assert all(t.device.type == "cuda" for f, t in zip(FIELDS, ms) if f != "shape")
+
+
+@pytest.mark.parametrize("value", [0.0, float("inf"), float("-inf"), float("nan")])
+def test_constant_fields(oracle_mod, value):
+    from dmsc_b200 import compute_dmsc
+
+    field = torch.full((6, 5), value)
+    first = compute_dmsc(field.cuda(), 0.0)
+    second = compute_dmsc(field.cuda(), 0.0)
+    assert diff_fields(list(first), list(second)) == []
+    assert diff_fields(list(first), oracle_mod.compute_dmsc(field, 0.0)) == []
+
+
+def test_too_large_raises():
+    from dmsc_b200 import compute_dmsc
+
+    img = torch.zeros((1, 1), device="cuda").expand(23170, 23170)
+    with pytest.raises(RuntimeError, match="too large"):
+        compute_dmsc(img, 0.0)
+
+
+def test_full_size_4096_primal(oracle_mod):
+    """The headline 4096 x 4096 bump workload, primal, threshold 0.05."""
+    from dmsc_b200.synthetic import field_4096_bumps
+
+    img = field_4096_bumps(seed=1234, device="cuda")
+    got = gpu_run(img, 0.05, [True] * 5, False)
+    exp = oracle_mod.run(img.cpu(), 0.05, True, False, True, True, True, True)
+    assert diff_fields(got, exp) == []
