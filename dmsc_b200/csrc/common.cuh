@@ -85,6 +85,18 @@ __device__ __forceinline__ int next_vertex(int e, int curr, int H, int W, int Nx
   return (v1 == curr) ? v2 : v1;
 }
 
+// a - b with the NaN results of the x86 SSE subtraction the reference CPU
+// path executes: a NaN operand propagates (first operand first, quieted) and
+// an invalid operation (inf - inf) yields the default NaN 0xFFC00000. Non-NaN
+// results are the IEEE difference, identical on both.
+__device__ __forceinline__ float sub_like_host(float a, float b) {
+  float r = a - b;
+  if (r == r) return r;
+  if (a != a) return __uint_as_float(__float_as_uint(a) | 0x00400000u);
+  if (b != b) return __uint_as_float(__float_as_uint(b) | 0x00400000u);
+  return __uint_as_float(0xFFC00000u);
+}
+
 __device__ __forceinline__ void set_status(unsigned* status, unsigned bit) { atomicOr(status, bit); }
 
 inline unsigned grid_for(long long n, int block) {

@@ -161,9 +161,9 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
   float sv = sad_val[s], ev = ext_val[d];
   float p;
   if (min_side)
-    p = dual ? ev - sv : sv - ev;
+    p = dual ? sub_like_host(ev, sv) : sub_like_host(sv, ev);
   else
-    p = dual ? sv - ev : ev - sv;
+    p = dual ? sub_like_host(sv, ev) : sub_like_host(ev, sv);
   pair_dense[s] = d;
   pers[s] = p;
   if (p <= thr) {
