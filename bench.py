@@ -1,0 +1,384 @@
+#!/usr/bin/env python
+"""Throughput of the full compute_dmsc path on B200.
+
+Workload: one 4096 x 4096 float32 field per GPU = 2000 Gaussian bumps
+(amplitude U[-1, 1], sigma U[4, 64] px) + N(0, 0.02^2) noise, seeded; full
+geometry (gradient, ridges, valleys, peaks, basins). The timed steps cycle
+through the four variants (is_dual, threshold) in {False, True} x {0, 0.05}.
+A step is one compute_dmsc call on one field. The field and the gradient
+output (64 MiB + 256 MiB) exceed the 126 MB L2, so no flush is needed.
+
+Metric: Mpixel/s (higher is better). ``value`` is device-timed with the
+input resident in HBM; ``e2e`` is the same metric through the public API
+from pinned host memory with every output read back to the host. N GPUs run
+N independent replicas (one field each, weak scaling), timed as the max over
+ranks.
+
+``--impl reference`` times the reference's own CPU path (compiled from the
+reference sources into oracle/_ref, all host threads) on the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import torch  # noqa: E402
+
+METRIC = "Mpixel/s full compute_dmsc at 4096^2 (bit-exact)"
+UNIT = "Mpixel/s"
+VARIANTS = [(False, 0.0), (False, 0.05), (True, 0.0), (True, 0.05)]
+SEED = 1234
+
+
+def workload_config(size):
+    return {
+        "workload": f"{size}x{size} float32 bump field: {int(round(2000 * (size / 4096) ** 2))} Gaussian bumps "
+                    "(a~U[-1,1], sigma~U[4,64] px) + N(0,0.02^2) noise, full geometry, steps cycle "
+                    "is_dual x threshold in {F,T} x {0,0.05}",
+        "image": [size, size],
+        "variants": [{"is_dual": d, "threshold": t} for d, t in VARIANTS],
+        "l2": "inputs larger than L2 (64 MiB field + 256 MiB gradient per call)",
+        "parallelism": "replicas (one field per GPU, no collective)",
+    }
+
+
+def _json_line(d):
+    print(json.dumps(d), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (oracle/_ref) -- checker and CPU baseline only
+# ---------------------------------------------------------------------------
+def load_reference():
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    if os.path.exists(os.path.join(ref_dir, "dmsc_cpu.so")):
+        sys.path.insert(0, ref_dir)
+        import dmsc_cpu
+
+        def run(img, thr, dual):
+            r = dmsc_cpu.extract_dmsc(img, thr, True, dual, True, True, True, True)
+            return [r[i] for i in range(19)]
+
+        return "reference", run
+    from oracle import oracle
+
+    def run(img, thr, dual):
+        return list(oracle.run(img, thr, True, dual, True, True, True, True))
+
+    return "port", run
+
+
+def same_outputs(a, b):
+    for x, y in zip(a, b):
+        x = x.cpu()
+        y = y.cpu()
+        if x.shape != y.shape or x.dtype != y.dtype:
+            return False
+        if x.is_floating_point():
+            x, y = x.view(torch.int32), y.view(torch.int32)
+        if not torch.equal(x, y):
+            return False
+    return True
+
+
+def cpu_baseline(img_cpu, gpu_outputs, budget_s=30.0):
+    """Reference CPU path on the same field (bounded sample), all host threads."""
+    kind, run = load_reference()
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    pix, t_tot, exact, done = 0, 0.0, True, []
+    for k, (dual, thr) in enumerate([VARIANTS[1], VARIANTS[2]]):
+        t0 = time.perf_counter()
+        out = run(img_cpu, thr, dual)
+        t_tot += time.perf_counter() - t0
+        pix += img_cpu.numel()
+        done.append(f"is_dual={dual},thr={thr}")
+        g = gpu_outputs.get((dual, thr))
+        if g is not None:
+            exact = exact and same_outputs(g, out)
+        if t_tot > budget_s:
+            break
+    return {
+        "value": pix / 1e6 / t_tot,
+        "unit": UNIT,
+        "cores": threads,
+        "kind": kind,
+        "sample": f"{len(done)} full compute_dmsc calls on the same {img_cpu.shape[0]}x{img_cpu.shape[1]} field "
+                  f"({'; '.join(done)}), torch threads={threads}",
+        "seconds": t_tot,
+    }, exact
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from dmsc_b200.synthetic import field_4096_bumps
+
+    size = args.size
+    kind, run = load_reference()
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    img = field_4096_bumps(seed=SEED, size=size)
+    # bound the run to a few minutes: measure one call, shrink to a centred
+    # crop when K + W full calls would not fit
+    t0 = time.perf_counter()
+    run(img, VARIANTS[0][1], VARIANTS[0][0])
+    est = time.perf_counter() - t0
+    sample = img
+    if est * (args.steps + args.warmup) > 240.0:
+        scale = (240.0 / (est * (args.steps + args.warmup))) ** 0.5
+        c = max(256, int(size * scale) // 64 * 64)
+        o = (size - c) // 2
+        sample = img[o:o + c, o:o + c].contiguous()
+    for w in range(max(0, args.warmup - 1)):
+        d, t = VARIANTS[w % 4]
+        run(sample, t, d)
+    times = []
+    for k in range(args.steps):
+        d, t = VARIANTS[k % 4]
+        t0 = time.perf_counter()
+        run(sample, t, d)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = sample.numel() * args.steps / 1e6 / total
+    sample_desc = (f"{'full field' if sample is img else f'centred {sample.shape[0]}x{sample.shape[1]} crop'} of the "
+                   f"{size}x{size} workload per step, cycling the 4 variants")
+    _json_line({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/i32",
+        "data": "synthetic", "config": workload_config(size),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample_desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    })
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key, size):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    e = d.get(kernel_key)
+    if not e:
+        return None
+    return e["bytes_per_launch_per_pixel"] * size * size
+
+
+def b200_arm(args):
+    from dmsc_b200 import _lib, compute_dmsc
+    from dmsc_b200.synthetic import field_4096_bumps
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    size = args.size
+    dev = torch.device("cuda", local)
+    img = field_4096_bumps(seed=SEED + rank, size=size, device=dev)
+    torch.cuda.synchronize()
+    ctx = _lib.context(local)
+    st = torch.cuda.current_stream(dev)
+
+    def step(k):
+        d, t = VARIANTS[k % 4]
+        return compute_dmsc(img, t, is_dual=d)
+
+    gpu_out = {}
+    for w in range(max(3, args.warmup)):
+        ms = step(w)
+        if rank == 0 and world == 1:
+            gpu_out[VARIANTS[w % 4]] = [x.cpu() for x in ms]
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident input ----
+    ctx.set_profiling(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    stage_sum = {}
+    launches = 0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for k in range(args.steps):
+        step(k)
+        for name, v in ctx.stage_times().items():
+            stage_sum[name] = stage_sum.get(name, 0.0) + v
+        launches += ctx.launch_count()
+    e1.record(st)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms_total = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ctx.set_profiling(False)
+    t = torch.tensor([ms_total], device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps * size * size / 1e6 / (ms_max / 1000.0)
+
+    # ---- end to end through the public API from pinned host memory ----
+    host = img.cpu().pin_memory()
+    h2d = host.numel() * host.element_size()
+    d2h = 0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(st)
+    for k in range(args.steps):
+        d, th = VARIANTS[k % 4]
+        ms = compute_dmsc(host, th, is_dual=d)  # H2D, compute, every output back to the host
+        d2h += sum(x.numel() * x.element_size() for x in ms)
+    f1.record(st)
+    torch.cuda.synchronize()
+    te = torch.tensor([f0.elapsed_time(f1)], device=dev)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e = world * args.steps * size * size / 1e6 / (float(te.item()) / 1000.0)
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind = measured_peak()
+    # roofline of the gradient kernel: 4 B/pixel read + 16 B/index written
+    grad_bytes = 4.0 * size * size + 16.0 * (size + 1) * (size + 1)
+    grad_ms = stage_sum.get("gradient", 0.0) / args.steps
+    achieved = grad_bytes / (grad_ms / 1000.0) / 1e9 if grad_ms > 0 else None
+    traffic = ncu_traffic("gradient_kernel", size)
+    # segmentation (basins + peaks) kernels
+    seg_bytes = 8.0 * (size + 1) ** 2 + 4.0 * size * size + 4.0 * (size + 1) ** 2
+    lab_ms = stage_sum.get("labels", 0.0) / args.steps
+    seg = seg_bytes / (lab_ms / 1000.0) / 1e9 if lab_ms > 0 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/i32", "data": "synthetic",
+        "config": workload_config(size),
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h // args.steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "gradient_kernel", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "algorithmic_bytes": grad_bytes, "avg_ms": grad_ms,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6.65 TB/s"},
+        "roofline_segmentation": {"bound": "hbm", "kernel": "label_kernel x2", "achieved": seg, "peak": peak,
+                                  "unit": "GB/s", "frac": (seg / peak) if seg else None,
+                                  "algorithmic_bytes": seg_bytes, "avg_ms": lab_ms},
+        "stage_ms_per_step": {k: v / args.steps for k, v in stage_sum.items()},
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        cb, exact = cpu_baseline(img.cpu(), gpu_out)
+        line["cpu_baseline"] = cb
+        line["bit_exact_vs_reference"] = exact
+    _json_line(line)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

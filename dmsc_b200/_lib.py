@@ -23,7 +23,13 @@ EXPORTS = (
     "dmsc_b200_fetch",
     "dmsc_b200_error_string",
     "dmsc_b200_last_error",
+    "dmsc_b200_set_profiling",
+    "dmsc_b200_stage_times",
+    "dmsc_b200_launch_count",
 )
+
+STAGES = ("gradient", "compaction", "saddle_sort", "saddle_walks", "pairing_faces", "pairing_vertices", "survivors",
+          "replay_faces", "replay_vertices", "labels", "sizes", "fetch_lists", "fetch_geometry")
 
 ERR_TOO_LARGE = 2
 
@@ -71,6 +77,12 @@ def load():
         lib.dmsc_b200_error_string.restype = ctypes.c_char_p
         lib.dmsc_b200_last_error.argtypes = [ctypes.c_void_p]
         lib.dmsc_b200_last_error.restype = ctypes.c_char_p
+        lib.dmsc_b200_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.dmsc_b200_set_profiling.restype = ctypes.c_int
+        lib.dmsc_b200_stage_times.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
+        lib.dmsc_b200_stage_times.restype = ctypes.c_int
+        lib.dmsc_b200_launch_count.argtypes = [ctypes.c_void_p]
+        lib.dmsc_b200_launch_count.restype = ctypes.c_longlong
         _lib = lib
         return lib
 
@@ -92,6 +104,19 @@ class Context:
             return
         msg = self.lib.dmsc_b200_last_error(self.h).decode() or self.lib.dmsc_b200_error_string(rc).decode()
         raise RuntimeError(f"{what}: {msg}")
+
+    def set_profiling(self, on: bool):
+        self.check(self.lib.dmsc_b200_set_profiling(self.h, 1 if on else 0), "dmsc_b200_set_profiling")
+
+    def stage_times(self) -> dict:
+        buf = (ctypes.c_float * 32)()
+        n = self.lib.dmsc_b200_stage_times(self.h, buf, 32)
+        if n < 0:
+            raise RuntimeError("stage times unavailable (profiling off or no call)")
+        return {STAGES[k]: float(buf[k]) for k in range(min(n, len(STAGES)))}
+
+    def launch_count(self) -> int:
+        return int(self.lib.dmsc_b200_launch_count(self.h))
 
     def close(self):
         if getattr(self, "h", None):

@@ -85,6 +85,8 @@ struct Side {
 
 }  // namespace
 
+constexpr int kStageMarks = 16;
+
 struct dmsc_b200_context {
   int device = 0;
   std::vector<Buf> bufs;
@@ -103,6 +105,10 @@ struct dmsc_b200_context {
   unsigned* status = nullptr;
   Side side[2];
   dmsc_b200_sizes sizes{};
+  // profiling: launch counter and stage boundary events
+  long long launches = 0;
+  bool profile = false;
+  cudaEvent_t ev[kStageMarks] = {};
 };
 
 namespace {
@@ -128,6 +134,13 @@ void ck(dmsc_b200_context* c, cudaError_t e, const char* what) {
 }
 #define CK(x) ck(ctx, (x), #x)
 #define LAUNCH_CHECK(name) ck(ctx, cudaGetLastError(), name)
+// every kernel launch of this library goes through LK so the context can
+// report how many kernels one call issued (CUB scans/sorts count once each)
+#define LK(...)      \
+  do {                \
+    __VA_ARGS__;      \
+    ++ctx->launches;  \
+  } while (0)
 
 template <class T>
 T* get(dmsc_b200_context* ctx, int slot, size_t n) {
@@ -167,6 +180,7 @@ void excl_sum(dmsc_b200_context* ctx, const In* in, Out* out, int n, cudaStream_
   CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, st));
   void* tmp = cub_tmp(ctx, bytes);
   CK(cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, n, st));
+  ++ctx->launches;
 }
 
 template <class In, class Out>
@@ -176,6 +190,7 @@ void incl_sum(dmsc_b200_context* ctx, const In* in, Out* out, int n, cudaStream_
   CK(cub::DeviceScan::InclusiveSum(nullptr, bytes, in, out, n, st));
   void* tmp = cub_tmp(ctx, bytes);
   CK(cub::DeviceScan::InclusiveSum(tmp, bytes, in, out, n, st));
+  ++ctx->launches;
 }
 
 template <class K>
@@ -185,6 +200,7 @@ void sort_pairs(dmsc_b200_context* ctx, const K* kin, K* kout, const int* vin, i
   CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, (int)(8 * sizeof(K)), st));
   void* tmp = cub_tmp(ctx, bytes);
   CK(cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, n, 0, (int)(8 * sizeof(K)), st));
+  ++ctx->launches;
 }
 
 __global__ void totals3_kernel(const int* o0, const int* s0, const int* o1, const int* s1, const int* o2,
@@ -206,6 +222,11 @@ __global__ void last_kernel(const T* a, int n, long long* out) {
 
 __global__ void u8_last_plus_kernel(const int* excl, const uint8_t* v, int n, long long* out) {
   *out = n > 0 ? (long long)excl[n - 1] + v[n - 1] : 0;
+}
+
+// Records stage boundary `k` when profiling.
+void mark(dmsc_b200_context* ctx, int k, cudaStream_t st) {
+  if (ctx->profile) CK(cudaEventRecord(ctx->ev[k], st));
 }
 
 // Host read of `k` pinned scalars after the stream drains.
@@ -247,13 +268,13 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
   int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
   int* cnt = sget<int>(ctx, si, X_CNT, 4);
   if (nsad > 0) {
-    sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, reverse, S.t, S.sweep, S.c1, S.c2, S.dying);
+    LK(sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, reverse, S.t, S.sweep, S.c1, S.c2, S.dying));
     LAUNCH_CHECK("sweep_edges_kernel");
   }
-  iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(grp, M + 1);
-  iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(link, M + 1);
+  LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(grp, M + 1));
+  LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(link, M + 1));
   CK(cudaMemsetAsync(minedge, 0xFF, (M + 1) * sizeof(unsigned), st));
-  if (nsad > 0) iota_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(act[0], nsad);
+  if (nsad > 0) LK(iota_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(act[0], nsad));
   LAUNCH_CHECK("pairing init");
   // older = value_less<D'> with D' = dual on the vertex side, !dual on the face side
   const bool older_less = S.faces ? ctx->dual : !ctx->dual;
@@ -264,15 +285,15 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
       throw Fail{kErrIterationCap};
     }
     CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
-    pair_edges_kernel<<<grid_for(n_active, TB), TB, 0, st>>>(act[cur], n_active, S.c1, S.c2, M, grp, S.dying,
-                                                             minedge, act[cur ^ 1], cnt);
+    LK(pair_edges_kernel<<<grid_for(n_active, TB), TB, 0, st>>>(act[cur], n_active, S.c1, S.c2, M, grp, S.dying,
+                                                             minedge, act[cur ^ 1], cnt));
     if (older_less)
-      pair_groups_kernel<true><<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, M, S.c1, S.c2, grp, minedge, link,
-                                                                    S.dying, S.val, S.crit);
+      LK(pair_groups_kernel<true><<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, M, S.c1, S.c2, grp, minedge, link,
+                                                                    S.dying, S.val, S.crit));
     else
-      pair_groups_kernel<false><<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, M, S.c1, S.c2, grp, minedge, link,
-                                                                     S.dying, S.val, S.crit);
-    pair_jump_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, grp, link, ctx->status);
+      LK(pair_groups_kernel<false><<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, M, S.c1, S.c2, grp, minedge, link,
+                                                                     S.dying, S.val, S.crit));
+    LK(pair_jump_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, grp, link, ctx->status));
     LAUNCH_CHECK("pairing round");
     int h = 0;
     CK(cudaMemcpyAsync(&h, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -289,30 +310,30 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
   CK(cudaMemsetAsync(S.alive, 1, M + 4, st));
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
   if (nsad > 0) {
-    persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, !S.faces, ctx->dual, ctx->thr, S.sweep, S.dying,
+    LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, !S.faces, ctx->dual, ctx->thr, S.sweep, S.dying,
                                                           get<float>(ctx, S_SVAL, nsad), S.val, S.pair_dense, S.pers,
-                                                          canc, (uint8_t)(S.faces ? 1 : 2), S.alive);
+                                                          canc, (uint8_t)(S.faces ? 1 : 2), S.alive));
     LAUNCH_CHECK("persistence_kernel");
   }
   // thresholded union-find roots
   int* uf = sget<int>(ctx, si, X_UF, M + 1);
   int* croot = sget<int>(ctx, si, X_CROOT, M + 1);
   S.ut = sget<int>(ctx, si, X_UT, M + 1);
-  iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(uf, M + 1);
+  LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(uf, M + 1));
   if (nsad > 0)
-    ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.c1, S.c2, S.pers, ctx->thr, M, uf);
-  ut_flatten_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, uf);
-  ut_mark_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M, uf, S.alive, croot);
-  if (M > 0) ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.ut);
+    LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.c1, S.c2, S.pers, ctx->thr, M, uf));
+  LK(ut_flatten_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, uf));
+  LK(ut_mark_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M, uf, S.alive, croot));
+  if (M > 0) LK(ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.ut));
   LAUNCH_CHECK("thresholded union-find");
   // output rank of alive extrema
   int* alive_i = sget<int>(ctx, si, X_ALIVEI, M + 1);
   S.to_out_excl = sget<int>(ctx, si, X_TOOUTX, M + 1);
   S.to_out = sget<int>(ctx, si, X_TOOUT, M + 1);
   if (M > 0) {
-    u8_to_int_kernel<<<grid_for(M, TB), TB, 0, st>>>(S.alive, M, alive_i);
+    LK(u8_to_int_kernel<<<grid_for(M, TB), TB, 0, st>>>(S.alive, M, alive_i));
     excl_sum(ctx, alive_i, S.to_out_excl, M, st);
-    compact_alive_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, S.alive, S.to_out_excl, S.crit, nullptr, S.to_out);
+    LK(compact_alive_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, S.alive, S.to_out_excl, S.crit, nullptr, S.to_out));
     LAUNCH_CHECK("compact_alive_kernel");
   }
 }
@@ -322,7 +343,7 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   const int nsad = ctx->nsad, M = S.M, nsurv = ctx->nsurv;
   long long* tot = get<long long>(ctx, S_TOT, 8);
   S.blen = sget<long long>(ctx, si, X_BLEN, 2 * (size_t)nsad);
-  if (nsad > 0) base_len_kernel<<<grid_for(2LL * nsad, TB), TB, 0, st>>>(2 * nsad, S.t, S.steps, S.blen);
+  if (nsad > 0) LK(base_len_kernel<<<grid_for(2LL * nsad, TB), TB, 0, st>>>(2 * nsad, S.t, S.steps, S.blen));
   unsigned long long* ckey = sget<unsigned long long>(ctx, si, X_CKEY, nsad);
   unsigned long long* ck2 = sget<unsigned long long>(ctx, si, X_CKEY2, nsad);
   int* cval = sget<int>(ctx, si, X_CVAL, nsad);
@@ -330,8 +351,8 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   int* cnt = sget<int>(ctx, si, X_CNT, 4);
   CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
   if (nsad > 0)
-    cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->thr,
-                                                             ctx->crit_sad, ckey, cval, cnt);
+    LK(cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->thr,
+                                                             ctx->crit_sad, ckey, cval, cnt));
   LAUNCH_CHECK("cancel_collect_kernel");
   int C = 0;
   CK(cudaMemcpyAsync(&C, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -348,12 +369,12 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   R.csad = sget<int>(ctx, si, X_CSAD, M + 1);
   R.cl_dy = sget<long long>(ctx, si, X_CLDY, M + 1);
   R.cl_ot = sget<long long>(ctx, si, X_CLOT, M + 1);
-  fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.ctime, M + 1, kNever);
-  fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.status, M + 1, kRootForever);
-  if (C > 0) replay_init_kernel<<<grid_for(C, TB), TB, 0, st>>>(C, cord, S.dying, R);
+  LK(fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.ctime, M + 1, kNever));
+  LK(fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.status, M + 1, kRootForever));
+  if (C > 0) LK(replay_init_kernel<<<grid_for(C, TB), TB, 0, st>>>(C, cord, S.dying, R));
   LAUNCH_CHECK("replay init");
   int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
-  if (C > 0) iota_kernel<<<grid_for(C, TB), TB, 0, st>>>(act[0], C);
+  if (C > 0) LK(iota_kernel<<<grid_for(C, TB), TB, 0, st>>>(act[0], C));
   int n_active = C, cur = 0, rounds = 0;
   const int max_steps = C + 1;
   while (n_active > 0) {
@@ -362,9 +383,9 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
       throw Fail{kErrIterationCap};
     }
     CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
-    replay_round_kernel<<<grid_for(n_active, TB), TB, 0, st>>>(act[cur], n_active, cord, S.sweep, S.dying, S.c1,
+    LK(replay_round_kernel<<<grid_for(n_active, TB), TB, 0, st>>>(act[cur], n_active, cord, S.sweep, S.dying, S.c1,
                                                                S.c2, S.blen, R, max_steps, act[cur ^ 1], cnt,
-                                                               ctx->status);
+                                                               ctx->status));
     LAUNCH_CHECK("replay_round_kernel");
     int h = 0;
     CK(cudaMemcpyAsync(&h, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -386,12 +407,12 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   long long* send = sget<long long>(ctx, si, X_SEND, nsurv);
   S.total = 0;
   if (nsurv > 0) {
-    final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, S.t, S.blen, R, max_steps,
-                                                                S.arc_len, S.arc_cl, S.arc_root, ctx->status);
-    pair_len_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, plen);
+    LK(final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, S.t, S.blen, R, max_steps,
+                                                                S.arc_len, S.arc_cl, S.arc_root, ctx->status));
+    LK(pair_len_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, plen));
     incl_sum(ctx, plen, send, nsurv, st);
-    arc_pos_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, send, S.arc_pos);
-    last_kernel<long long><<<1, 1, 0, st>>>(send, nsurv, tot);
+    LK(arc_pos_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, send, S.arc_pos));
+    LK(last_kernel<long long><<<1, 1, 0, st>>>(send, nsurv, tot));
     LAUNCH_CHECK("final arcs");
     readback(ctx, st, tot, 1);
     S.total = ctx->pinned[0];
@@ -431,6 +452,8 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   const long long nidx = (long long)(H + 1) * Nx;
   const long long ncells = 4 * nidx;
   ctx->status = get<unsigned>(ctx, S_STATUS, 4);
+  ctx->launches = 0;
+  mark(ctx, 0, st);
   CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
 
   // ---- K1 gradient + criticality ----
@@ -443,13 +466,14 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
   dim3 g1(nsegx, (H + 1 + kTileY - 1) / kTileY);
   if (dual)
-    gradient_kernel<true><<<g1, 256, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]);
+    LK(gradient_kernel<true><<<g1, 256, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]));
   else
-    gradient_kernel<false><<<g1, 256, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]);
+    LK(gradient_kernel<false><<<g1, 256, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]));
   LAUNCH_CHECK("gradient_kernel");
+  mark(ctx, 1, st);
   for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);
   long long* tot = get<long long>(ctx, S_TOT, 8);
-  totals3_kernel<<<1, 1, 0, st>>>(off[0], seg[0], off[1], seg[1], off[2], seg[2], nseg, tot);
+  LK(totals3_kernel<<<1, 1, 0, st>>>(off[0], seg[0], off[1], seg[1], off[2], seg[2], nseg, tot));
   LAUNCH_CHECK("totals3_kernel");
   readback(ctx, st, tot, 3);
   const int nmin = (int)ctx->pinned[0], nsad = (int)ctx->pinned[1], nmax = (int)ctx->pinned[2];
@@ -471,31 +495,33 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   {
     unsigned blocks = grid_for(nseg, 8);
     if (dual)
-      compact_kernel<true><<<blocks, 256, 0, st>>>(img, H, W, nsegx, nseg, mask, off[0], off[1], off[2], cmin, csad,
-                                                   cmax, rmin, rmax, vmin, vmax, sval, skey);
+      LK(compact_kernel<true><<<blocks, 256, 0, st>>>(img, H, W, nsegx, nseg, mask, off[0], off[1], off[2], cmin, csad,
+                                                   cmax, rmin, rmax, vmin, vmax, sval, skey));
     else
-      compact_kernel<false><<<blocks, 256, 0, st>>>(img, H, W, nsegx, nseg, mask, off[0], off[1], off[2], cmin, csad,
-                                                    cmax, rmin, rmax, vmin, vmax, sval, skey);
+      LK(compact_kernel<false><<<blocks, 256, 0, st>>>(img, H, W, nsegx, nseg, mask, off[0], off[1], off[2], cmin, csad,
+                                                    cmax, rmin, rmax, vmin, vmax, sval, skey));
     LAUNCH_CHECK("compact_kernel");
   }
+  mark(ctx, 2, st);
 
   // ---- saddle order: ascending (s_val, cell id) (arcs_topology.hxx:99-102) ----
   int* iota = get<int>(ctx, S_IOTA, nsad);
   int* asc = get<int>(ctx, S_ASC, nsad);
   uint32_t* skey2 = get<uint32_t>(ctx, S_SKEY2, nsad);
   if (nsad > 0) {
-    iota_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(iota, nsad);
+    LK(iota_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(iota, nsad));
     sort_pairs(ctx, skey, skey2, iota, asc, nsad, st);
   }
 
+  mark(ctx, 3, st);
   // ---- K4 saddle walks ----
   int* tf = get<int>(ctx, S_TF, 2 * (size_t)nsad);
   int* lf = get<int>(ctx, S_LF, 2 * (size_t)nsad);
   int* tv = get<int>(ctx, S_TV, 2 * (size_t)nsad);
   int* lv = get<int>(ctx, S_LV, 2 * (size_t)nsad);
   if (nsad > 0) {
-    saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(grad, H, W, nsad, csad, rmax, rmin, tf, lf, tv, lv, ncells,
-                                                          ctx->status);
+    LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(grad, H, W, nsad, csad, rmax, rmin, tf, lf, tv, lv, ncells,
+                                                          ctx->status));
     LAUNCH_CHECK("saddle_walk_kernel");
   }
 
@@ -524,10 +550,13 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   V.groups = dual ? f_peaks : f_basins;
 
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
+  mark(ctx, 4, st);
   CK(cudaMemsetAsync(canc, 0, nsad + 4, st));
   // sweep orders: minima = asc in the primal, reverse in the dual; maxima the reverse of minima
   run_pairing(ctx, 0, F, asc, !dual, st);
+  mark(ctx, 5, st);
   run_pairing(ctx, 1, V, asc, dual, st);
+  mark(ctx, 6, st);
 
   // ---- surviving saddles in minima-sweep order ----
   int* flag = get<int>(ctx, S_FLAG, nsad);
@@ -535,19 +564,22 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   ctx->surv = get<int>(ctx, S_SURV, nsad);
   ctx->nsurv = 0;
   if (nsad > 0) {
-    survivor_flag_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, V.sweep, canc, flag);
+    LK(survivor_flag_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, V.sweep, canc, flag));
     excl_sum(ctx, flag, fpos, nsad, st);
-    survivor_list_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, V.sweep, flag, fpos, ctx->surv);
-    last_plus_kernel<int><<<1, 1, 0, st>>>(fpos, flag, nsad, tot);
+    LK(survivor_list_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, V.sweep, flag, fpos, ctx->surv));
+    LK(last_plus_kernel<int><<<1, 1, 0, st>>>(fpos, flag, nsad, tot));
     LAUNCH_CHECK("survivors");
     readback(ctx, st, tot, 1);
     ctx->nsurv = (int)ctx->pinned[0];
   }
   const int nsurv = ctx->nsurv;
+  mark(ctx, 7, st);
 
   // ---- replay + final arc lengths ----
-  for (int si = 0; si < 2; ++si)
+  for (int si = 0; si < 2; ++si) {
     if (ctx->side[si].arcs && nsad > 0) run_replay(ctx, si, ctx->side[si], st);
+    mark(ctx, 8 + si, st);
+  }
 
   // ---- labels (region id = rank among alive extrema) ----
   for (int si = 0; si < 2; ++si) {
@@ -556,27 +588,28 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
     int32_t* out = S.faces ? (dual ? basins_out : peaks_out) : (dual ? peaks_out : basins_out);
     long long n = S.faces ? nidx : (long long)H * W;
     if (S.faces)
-      label_kernel<true><<<grid_for(n, TB), TB, 0, st>>>(grad, H, W, rmax, S.ut, S.to_out, out, ncells, ctx->status);
+      LK(label_kernel<true><<<grid_for(n, TB), TB, 0, st>>>(grad, H, W, rmax, S.ut, S.to_out, out, ncells, ctx->status));
     else
-      label_kernel<false><<<grid_for(n, TB), TB, 0, st>>>(grad, H, W, rmin, S.ut, S.to_out, out, ncells,
-                                                           ctx->status);
+      LK(label_kernel<false><<<grid_for(n, TB), TB, 0, st>>>(grad, H, W, rmin, S.ut, S.to_out, out, ncells,
+                                                           ctx->status));
     LAUNCH_CHECK("label_kernel");
   }
 
+  mark(ctx, 10, st);
   // ---- e rows and alive counts ----
   for (int si = 0; si < 2; ++si) {
     Side& S = ctx->side[si];
     int* ec = sget<int>(ctx, si, X_EROWC, nsurv);
     S.erow_off = sget<int>(ctx, si, X_EROWO, nsurv);
     if (nsurv > 0) {
-      erow_count_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, ctx->surv, S.t, S.ut, S.to_out, ec);
+      LK(erow_count_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, ctx->surv, S.t, S.ut, S.to_out, ec));
       excl_sum(ctx, ec, S.erow_off, nsurv, st);
-      last_plus_kernel<int><<<1, 1, 0, st>>>(S.erow_off, ec, nsurv, tot + 2 * si);
+      LK(last_plus_kernel<int><<<1, 1, 0, st>>>(S.erow_off, ec, nsurv, tot + 2 * si));
     } else {
       CK(cudaMemsetAsync(tot + 2 * si, 0, sizeof(long long), st));
     }
     if (S.M > 0)
-      u8_last_plus_kernel<<<1, 1, 0, st>>>(S.to_out_excl, S.alive, S.M, tot + 2 * si + 1);
+      LK(u8_last_plus_kernel<<<1, 1, 0, st>>>(S.to_out_excl, S.alive, S.M, tot + 2 * si + 1));
     else
       CK(cudaMemsetAsync(tot + 2 * si + 1, 0, sizeof(long long), st));
     LAUNCH_CHECK("e rows");
@@ -586,6 +619,7 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   F.n_alive = (int)ctx->pinned[1];
   V.n_erows = (int)ctx->pinned[2];
   V.n_alive = (int)ctx->pinned[3];
+  mark(ctx, 11, st);
   check_status(ctx, st);
 
   // ---- sizes, public (primal / dual) naming ----
@@ -620,7 +654,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   const int nsurv = ctx->nsurv;
   long long* send = sget<long long>(ctx, si, X_SEND, nsurv);
   if (offsets)
-    arc_offsets_kernel<<<grid_for(nsurv + 1LL, TB), TB, 0, st>>>(nsurv, S.arc_len, send, offsets, arc_offsets);
+    LK(arc_offsets_kernel<<<grid_for(nsurv + 1LL, TB), TB, 0, st>>>(nsurv, S.arc_len, send, offsets, arc_offsets));
   LAUNCH_CHECK("arc_offsets_kernel");
   if (S.total <= 0 || !flat) return;
   long long cap = S.total;
@@ -644,7 +678,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   E.q_out = q[cur];
   E.n_out = cnt;
   CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
-  emit_roots_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(E, nsurv, ctx->surv, S.arc_pos, S.arc_cl, S.arc_root);
+  LK(emit_roots_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(E, nsurv, ctx->surv, S.arc_pos, S.arc_cl, S.arc_root));
   LAUNCH_CHECK("emit_roots_kernel");
   int n = 0, levels = 0;
   CK(cudaMemcpyAsync(&n, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -656,7 +690,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
     }
     E.q_out = q[cur ^ 1];
     CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
-    emit_level_kernel<<<grid_for(n, TB), TB, 0, st>>>(E, q[cur], n);
+    LK(emit_level_kernel<<<grid_for(n, TB), TB, 0, st>>>(E, q[cur], n));
     LAUNCH_CHECK("emit_level_kernel");
     CK(cudaMemcpyAsync(&n, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -670,6 +704,7 @@ int fetch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t 
     return kErrInvalidArgument;
   }
   CK(cudaSetDevice(ctx->device));
+  mark(ctx, 12, st);
   const bool dual = ctx->dual;
   const int nsurv = ctx->nsurv;
   Side& F = ctx->side[0];
@@ -678,22 +713,23 @@ int fetch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t 
   int32_t* fpts = dual ? o->min_pts : o->max_pts;
   int32_t* vpts = dual ? o->max_pts : o->min_pts;
   if (F.M > 0 && fpts)
-    compact_alive_kernel<<<grid_for(F.M, TB), TB, 0, st>>>(F.M, F.alive, F.to_out_excl, F.crit, fpts, F.to_out);
+    LK(compact_alive_kernel<<<grid_for(F.M, TB), TB, 0, st>>>(F.M, F.alive, F.to_out_excl, F.crit, fpts, F.to_out));
   if (V.M > 0 && vpts)
-    compact_alive_kernel<<<grid_for(V.M, TB), TB, 0, st>>>(V.M, V.alive, V.to_out_excl, V.crit, vpts, V.to_out);
+    LK(compact_alive_kernel<<<grid_for(V.M, TB), TB, 0, st>>>(V.M, V.alive, V.to_out_excl, V.crit, vpts, V.to_out));
   if (nsurv > 0 && o->sad_pts)
-    sad_pts_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->crit_sad, o->sad_pts);
+    LK(sad_pts_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->crit_sad, o->sad_pts));
   LAUNCH_CHECK("point lists");
   // per-saddle scalars and e rows
   if (nsurv > 0) {
-    side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(
+    LK(side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(
         nsurv, true, ctx->surv, F.t, F.ut, F.to_out, F.pers, F.pair_dense, F.erow_off, dual ? o->p_min : o->p_max,
-        dual ? o->ppairs_min : o->ppairs_max, F.n_erows > 0 ? (dual ? o->e_min : o->e_max) : nullptr);
-    side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(
+        dual ? o->ppairs_min : o->ppairs_max, F.n_erows > 0 ? (dual ? o->e_min : o->e_max) : nullptr));
+    LK(side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(
         nsurv, false, ctx->surv, V.t, V.ut, V.to_out, V.pers, V.pair_dense, V.erow_off, dual ? o->p_max : o->p_min,
-        dual ? o->ppairs_max : o->ppairs_min, V.n_erows > 0 ? (dual ? o->e_max : o->e_min) : nullptr);
+        dual ? o->ppairs_max : o->ppairs_min, V.n_erows > 0 ? (dual ? o->e_max : o->e_min) : nullptr));
     LAUNCH_CHECK("side_outputs_kernel");
   }
+  mark(ctx, 13, st);
   // arc geometry
   for (int si = 0; si < 2; ++si) {
     Side& S = ctx->side[si];
@@ -708,6 +744,7 @@ int fetch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t 
     }
     emit_side(ctx, si, S, flat, offs, aoffs, st);
   }
+  mark(ctx, 14, st);
   check_status(ctx, st);
   return kOk;
 }
@@ -737,6 +774,8 @@ void dmsc_b200_destroy(dmsc_b200_context* c) {
     if (b.p) cudaFree(b.p);
   if (c->cub_tmp.p) cudaFree(c->cub_tmp.p);
   if (c->pinned) cudaFreeHost(c->pinned);
+  for (int k = 0; k < kStageMarks; ++k)
+    if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   delete c;
 }
 
@@ -776,5 +815,33 @@ const char* dmsc_b200_error_string(int code) {
 }
 
 const char* dmsc_b200_last_error(const dmsc_b200_context* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int dmsc_b200_set_profiling(dmsc_b200_context* ctx, int enable) {
+  if (!ctx) return kErrInvalidArgument;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return kErrCuda;
+  if (enable && !ctx->ev[0]) {
+    for (int k = 0; k < kStageMarks; ++k)
+      if (cudaEventCreate(&ctx->ev[k]) != cudaSuccess) return kErrCuda;
+  }
+  ctx->profile = enable != 0;
+  return kOk;
+}
+
+int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n) {
+  if (!ctx || !ms || !ctx->profile) return -1;
+  // extract stages are marks 0..11, fetch stages marks 12..14
+  static const int from[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 13};
+  static const int to[] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 13, 14};
+  const int ns = (int)(sizeof(from) / sizeof(from[0]));
+  if (cudaEventSynchronize(ctx->ev[14]) != cudaSuccess) return -1;
+  for (int k = 0; k < ns && k < n; ++k) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, ctx->ev[from[k]], ctx->ev[to[k]]) != cudaSuccess) t = -1.f;
+    ms[k] = t;
+  }
+  return ns;
+}
+
+long long dmsc_b200_launch_count(const dmsc_b200_context* ctx) { return ctx ? ctx->launches : -1; }
 
 }  // extern "C"

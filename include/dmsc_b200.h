@@ -113,6 +113,22 @@ const char* dmsc_b200_error_string(int code);
 /* Message of the last failure on this context (empty when none). */
 const char* dmsc_b200_last_error(const dmsc_b200_context* ctx);
 
+/* Instrumentation (no reference counterpart; the reference exposes its stage
+   timings only as RECORD_FUNCTION ranges, e.g. cpu/gradient.hxx:24).
+   When enabled, extract() and fetch() record a CUDA event on the call's stream
+   at every stage boundary. dmsc_b200_stage_times() writes up to `n` stage
+   durations in milliseconds of the last extract()+fetch() pair (host pointer)
+   and returns the number of stages: 0 gradient, 1 compaction, 2 saddle sort,
+   3 saddle walks, 4 pairing (faces), 5 pairing (vertices), 6 survivors,
+   7 replay (faces), 8 replay (vertices), 9 labels, 10 sizes,
+   11 fetch lists, 12 fetch geometry. */
+int dmsc_b200_set_profiling(dmsc_b200_context* ctx, int enable);
+int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n);
+
+/* Kernel launches issued by the last extract()+fetch() pair (each CUB scan or
+   sort call counts once). */
+long long dmsc_b200_launch_count(const dmsc_b200_context* ctx);
+
 #ifdef __cplusplus
 }
 #endif

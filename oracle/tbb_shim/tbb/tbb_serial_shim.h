@@ -1,10 +1,13 @@
-// Serial stand-in for the handful of oneTBB facilities the reference CPU path
-// uses. TBB is not installed in this image. Every construct runs in program
+// Stand-in for the handful of oneTBB facilities the reference CPU path uses. TBB is not installed in this image. Every construct runs in program
 // order on the calling thread, which reproduces the reference's canonical
 // single-thread output order (ascending cell ids in the critical lists).
 // Test infrastructure only: used to compile the reference checker.
 #pragma once
 #include <algorithm>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <vector>
 #include <cstddef>
 #include <utility>
 
@@ -49,17 +52,31 @@ void parallel_sort(It first, It last) {
   std::sort(first, last);
 }
 
+// One slot per calling thread. Serial TBB constructs only ever touch the
+// first slot (so the reference's per-thread lists concatenate in program
+// order), while the reference also calls local() from ATen's parallel_for,
+// which does run on several OpenMP threads.
 template <typename T>
 class enumerable_thread_specific {
  public:
-  T& local() { return slot_; }
-  T* begin() { return &slot_; }
-  T* end() { return &slot_ + 1; }
-  const T* begin() const { return &slot_; }
-  const T* end() const { return &slot_ + 1; }
+  T& local() {
+    std::lock_guard<std::mutex> g(m_);
+    auto id = std::this_thread::get_id();
+    for (std::size_t i = 0; i < ids_.size(); ++i)
+      if (ids_[i] == id) return slots_[i];
+    ids_.push_back(id);
+    slots_.emplace_back();
+    return slots_.back();
+  }
+  typename std::deque<T>::iterator begin() { return slots_.begin(); }
+  typename std::deque<T>::iterator end() { return slots_.end(); }
+  typename std::deque<T>::const_iterator begin() const { return slots_.begin(); }
+  typename std::deque<T>::const_iterator end() const { return slots_.end(); }
 
  private:
-  T slot_{};
+  std::mutex m_;
+  std::vector<std::thread::id> ids_;
+  std::deque<T> slots_;
 };
 
 class global_control {

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def header_functions():
     src = open(os.path.join(ROOT, "include", "dmsc_b200.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:int|void|const char\*)\s+(dmsc_b200_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void|long long|const char\*)\s+(dmsc_b200_\w+)\s*\(", src, re.M)))
 
 
 def test_library_exports_header_symbols():
