@@ -73,7 +73,7 @@ class ClockSampler:
         try:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -276,6 +276,7 @@ def b200_arm(args):
     ctx.set_profiling(True)
     clocks = ClockSampler(local)
     clocks.start()
+    time.sleep(0.3)
     stage_sum = {}
     launches = 0
     if dist:
@@ -294,7 +295,6 @@ def b200_arm(args):
     if dist:
         dist.barrier()
     ms_total = e0.elapsed_time(e1)
-    clk = clocks.stop()
     ctx.set_profiling(False)
     t = torch.tensor([ms_total], device=dev)
     if dist:
@@ -322,6 +322,7 @@ def b200_arm(args):
     if dist:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e = world * args.steps * size * size / 1e6 / (float(te.item()) / 1000.0)
+    clk = clocks.stop()
 
     if rank != 0:
         if dist:

@@ -111,6 +111,31 @@ struct dmsc_b200_context {
   cudaEvent_t ev[kStageMarks] = {};
 };
 
+namespace dmsc {
+
+__global__ void totals3_kernel(const int* o0, const int* s0, const int* o1, const int* s1, const int* o2,
+                               const int* s2, long long n, long long* out) {
+  out[0] = (long long)o0[n - 1] + s0[n - 1];
+  out[1] = (long long)o1[n - 1] + s1[n - 1];
+  out[2] = (long long)o2[n - 1] + s2[n - 1];
+}
+
+template <class T>
+__global__ void last_plus_kernel(const T* excl, const T* val, int n, long long* out) {
+  *out = n > 0 ? (long long)excl[n - 1] + (long long)val[n - 1] : 0;
+}
+
+template <class T>
+__global__ void last_kernel(const T* a, int n, long long* out) {
+  *out = n > 0 ? (long long)a[n - 1] : 0;
+}
+
+__global__ void u8_last_plus_kernel(const int* excl, const uint8_t* v, int n, long long* out) {
+  *out = n > 0 ? (long long)excl[n - 1] + v[n - 1] : 0;
+}
+
+}  // namespace dmsc
+
 namespace {
 
 struct Fail {
@@ -201,27 +226,6 @@ void sort_pairs(dmsc_b200_context* ctx, const K* kin, K* kout, const int* vin, i
   void* tmp = cub_tmp(ctx, bytes);
   CK(cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, n, 0, (int)(8 * sizeof(K)), st));
   ++ctx->launches;
-}
-
-__global__ void totals3_kernel(const int* o0, const int* s0, const int* o1, const int* s1, const int* o2,
-                               const int* s2, long long n, long long* out) {
-  out[0] = (long long)o0[n - 1] + s0[n - 1];
-  out[1] = (long long)o1[n - 1] + s1[n - 1];
-  out[2] = (long long)o2[n - 1] + s2[n - 1];
-}
-
-template <class T>
-__global__ void last_plus_kernel(const T* excl, const T* val, int n, long long* out) {
-  *out = n > 0 ? (long long)excl[n - 1] + (long long)val[n - 1] : 0;
-}
-
-template <class T>
-__global__ void last_kernel(const T* a, int n, long long* out) {
-  *out = n > 0 ? (long long)a[n - 1] : 0;
-}
-
-__global__ void u8_last_plus_kernel(const int* excl, const uint8_t* v, int n, long long* out) {
-  *out = n > 0 ? (long long)excl[n - 1] + v[n - 1] : 0;
 }
 
 // Records stage boundary `k` when profiling.
@@ -466,9 +470,9 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
   dim3 g1(nsegx, (H + 1 + kTileY - 1) / kTileY);
   if (dual)
-    LK(gradient_kernel<true><<<g1, 256, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]));
+    LK(gradient_kernel<true><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]));
   else
-    LK(gradient_kernel<false><<<g1, 256, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]));
+    LK(gradient_kernel<false><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]));
   LAUNCH_CHECK("gradient_kernel");
   mark(ctx, 1, st);
   for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);

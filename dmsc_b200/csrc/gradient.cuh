@@ -29,85 +29,116 @@ constexpr int kTileY = 8;   // tile rows (one warp each)
 constexpr int kValX = kTileX + 3;
 constexpr int kValY = kTileY + 3;
 
-template <bool DUAL>
-struct PixelTile {
-  const float (*v)[kValX];
-  int oy, ox, W;  // tile value origin = (y0 - 2, x0 - 2)
-  __device__ __forceinline__ float val(int y, int x) const { return v[y - oy][x - ox]; }
-  // v_greater (cpu/cell_compare.hxx:23-31): pixels ordered by (value, y*W+x)
-  __device__ __forceinline__ bool gt(int ay, int ax, int by, int bx) const {
-    return value_greater<DUAL>(val(ay, ax), ay * W + ax, val(by, bx), by * W + bx);
-  }
-};
+constexpr int kGradThreads = 320;  // >= (kTileY + 1) * (kTileX + 1) = 297 lower stars per tile
 
-// get_highest_vertex_yx scan over a face's candidates in the reference order
-// (cpu/cell_compare.hxx:33-63); returns true when pixel (py, px) wins.
+// One pixel value with its linear id; gt() is v_greater (cpu/cell_compare.hxx:23-31):
+// pixels ordered by (value, y*W+x), flipped in the dual.
+struct Px {
+  float v;
+  int id;
+};
 template <bool DUAL>
-__device__ __forceinline__ bool face_top_is(const PixelTile<DUAL>& T, int fy, int fx, int H, int W, int py,
-                                            int px) {
-  int by = -1, bx = -1;
-  int cy[4] = {fy - 1, fy - 1, fy, fy};
-  int cx[4] = {fx - 1, fx, fx - 1, fx};
-  bool ok[4] = {fy >= 1 && fx >= 1, fy >= 1 && fx < W, fy < H && fx >= 1, fy < H && fx < W};
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (!ok[k]) continue;
-    if (by < 0 || T.gt(cy[k], cx[k], by, bx)) {
-      by = cy[k];
-      bx = cx[k];
-    }
-  }
-  return by == py && bx == px;
+__device__ __forceinline__ bool gt(const Px& a, const Px& b) {
+  return value_greater<DUAL>(a.v, a.id, b.v, b.id);
 }
 
-// Lower star of pixel (y, x) and its pairing (cpu/gradient.hxx:48-192).
-// Edge slots: e0 = H(y,x), e1 = H(y,x+1), e2 = V(y,x), e3 = V(y+1,x).
-// Face slots: f0 = F(y,x), f1 = F(y,x+1), f2 = F(y+1,x), f3 = F(y+1,x+1).
-// The owned cells' gradient values are written into the shared index tile.
+// Lower star of pixel (y, x) and its pairing (cpu/gradient.hxx:48-192), all in
+// registers. The highest-vertex scans keep the reference's candidate order
+// (cpu/cell_compare.hxx:33-63), so ties and non-finite values resolve the same
+// way. Edge slots: e0 = H(y,x), e1 = H(y,x+1), e2 = V(y,x), e3 = V(y+1,x);
+// face slots: f0 = F(y,x), f1 = F(y,x+1), f2 = F(y+1,x), f3 = F(y+1,x+1).
+// Writes the gradient values of the owned cells into the shared index tile.
 template <bool DUAL>
-__device__ __forceinline__ void lower_star(const PixelTile<DUAL>& T, int y, int x, int H, int W, int Nx, int ty0,
+__device__ __forceinline__ void lower_star(const float (*sv)[kValX], int y, int x, int H, int W, int Nx, int ty0,
                                            int tx0, int (*tile)[kTileX][4]) {
-  // --- lower-star membership, with the reference's candidate scan order ---
-  unsigned eL = 0, fL = 0;
-  if (x - 1 < 0 || T.gt(y, x, y, x - 1)) eL |= 1u;
-  if (!(x + 1 < W && T.gt(y, x + 1, y, x))) eL |= 2u;
-  if (y - 1 < 0 || T.gt(y, x, y - 1, x)) eL |= 4u;
-  if (!(y + 1 < H && T.gt(y + 1, x, y, x))) eL |= 8u;
-  if (face_top_is<DUAL>(T, y, x, H, W, y, x)) fL |= 1u;
-  if (face_top_is<DUAL>(T, y, x + 1, H, W, y, x)) fL |= 2u;
-  if (face_top_is<DUAL>(T, y + 1, x, H, W, y, x)) fL |= 4u;
-  if (face_top_is<DUAL>(T, y + 1, x + 1, H, W, y, x)) fL |= 8u;
+  // 3x3 neighbourhood; r, c index the value tile (origin y0-2, x0-2)
+  const int r = y - (ty0 - 2), c = x - (tx0 - 2);
+  const bool lv = x >= 1, rv = x + 1 < W, uv = y >= 1, dv = y + 1 < H;
+  const Px P{sv[r][c], y * W + x};
+  const Px L{sv[r][c - 1], P.id - 1}, R{sv[r][c + 1], P.id + 1};
+  const Px U{sv[r - 1][c], P.id - W}, D{sv[r + 1][c], P.id + W};
+  const Px UL{sv[r - 1][c - 1], P.id - W - 1}, UR{sv[r - 1][c + 1], P.id - W + 1};
+  const Px DL{sv[r + 1][c - 1], P.id + W - 1}, DR{sv[r + 1][c + 1], P.id + W + 1};
 
-  // --- vertex pairing: the lower-star edge whose other vertex is lowest ---
-  int ov_y[4] = {y, y, y - 1, y + 1};
-  int ov_x[4] = {x - 1, x + 1, x, x};
-  bool ov_ok[4] = {x - 1 >= 0, x + 1 < W, y - 1 >= 0, y + 1 < H};
-  int best = -1, bo_y = 0, bo_x = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (!((eL >> k) & 1u) || !ov_ok[k]) continue;
-    if (best == -1 || T.gt(bo_y, bo_x, ov_y[k], ov_x[k])) {
-      best = k;
-      bo_y = ov_y[k];
-      bo_x = ov_x[k];
+  const bool p_gt_l = lv && gt<DUAL>(P, L);
+  const bool r_gt_p = rv && gt<DUAL>(R, P);
+  const bool p_gt_u = uv && gt<DUAL>(P, U);
+  const bool d_gt_p = dv && gt<DUAL>(D, P);
+
+  unsigned eL = 0, fL = 0;
+  if (!lv || p_gt_l) eL |= 1u;
+  if (!r_gt_p) eL |= 2u;
+  if (!uv || p_gt_u) eL |= 4u;
+  if (!d_gt_p) eL |= 8u;
+  {  // f0 = F(y,x): scan UL, U, L, then P
+    bool have = false;
+    Px b = P;
+    if (uv && lv) {
+      b = UL;
+      have = true;
     }
+    if (uv) {
+      if (!have || gt<DUAL>(U, b)) b = U;
+      have = true;
+    }
+    if (lv) {
+      if (!have || gt<DUAL>(L, b)) b = L;
+      have = true;
+    }
+    if (!have || gt<DUAL>(P, b)) fL |= 1u;
   }
-  // pairing state: epair[k] = -1 none, 4 vertex, 0..3 face slot; fpair[f] = edge slot or -1
-  int epair[4] = {-1, -1, -1, -1};
-  int fpair[4] = {-1, -1, -1, -1};
+  {  // f1 = F(y,x+1): scan U, UR, P, R
+    bool have = false;
+    Px b = P;
+    if (uv) {
+      b = U;
+      have = true;
+    }
+    if (uv && rv) {
+      if (!have || gt<DUAL>(UR, b)) b = UR;
+      have = true;
+    }
+    if ((!have || gt<DUAL>(P, b)) && !r_gt_p) fL |= 2u;
+  }
+  {  // f2 = F(y+1,x): scan L, P, DL, D
+    bool p_best = !lv || p_gt_l;
+    if (p_best && dv && lv && gt<DUAL>(DL, P)) p_best = false;
+    if (p_best && d_gt_p) p_best = false;
+    if (p_best) fL |= 4u;
+  }
+  {  // f3 = F(y+1,x+1): scan P, R, D, DR
+    bool p_best = !r_gt_p && !d_gt_p && !(dv && rv && gt<DUAL>(DR, P));
+    if (p_best) fL |= 8u;
+  }
+
+  // vertex pairing: the lower-star edge whose other vertex is lowest
+  int best = -1;
+  Px bo = P;
+  if ((eL & 1u) && lv) {
+    best = 0;
+    bo = L;
+  }
+  if ((eL & 2u) && rv && (best < 0 || gt<DUAL>(bo, R))) {
+    best = 1;
+    bo = R;
+  }
+  if ((eL & 4u) && uv && (best < 0 || gt<DUAL>(bo, U))) {
+    best = 2;
+    bo = U;
+  }
+  if ((eL & 8u) && dv && (best < 0 || gt<DUAL>(bo, D))) {
+    best = 3;
+    bo = D;
+  }
+
+  // face pairing by FIFO. Pair state packed 4 bits per slot: epk (edge ->
+  // 4 vertex, 0..3 face, 15 none), fpk (face -> edge slot, 15 none).
+  unsigned epk = 0xFFFFu, fpk = 0xFFFFu;
   unsigned epaired = 0, fpaired = 0;
   if (best >= 0) {
-    epair[best] = 4;
-    epaired |= 1u << best;
+    epk = (epk & ~(0xFu << (4 * best))) | (4u << (4 * best));
+    epaired = 1u << best;
   }
-
-  // --- face pairing by FIFO (cpu/gradient.hxx:115-191) ---
-  // face f's lower-star-candidate edges in the reference visiting order
-  const int fe_a[4] = {0, 1, 0, 1};
-  const int fe_b[4] = {2, 2, 3, 3};
-  // faces bounding edge slot k, in check_and_push order
-  const int ef_a[4] = {0, 1, 0, 2};
-  const int ef_b[4] = {2, 3, 1, 3};
   unsigned long long q = 0;  // queue of face slots, 4 bits per entry
   int head = 0, tail = 0;
 #pragma unroll
@@ -117,28 +148,24 @@ __device__ __forceinline__ void lower_star(const PixelTile<DUAL>& T, int y, int 
       tail++;
     }
   while (head < tail) {
-    int f = (int)((q >> (4 * head)) & 0xFull);
+    const int f = (int)((q >> (4 * head)) & 0xFull);
     head++;
     if ((fpaired >> f) & 1u) continue;
-    int unp_e = -1, unp_n = 0;
-    int ea = fe_a[f], eb = fe_b[f];
-    if (((eL >> ea) & 1u) && !((epaired >> ea) & 1u)) {
-      unp_n++;
-      unp_e = ea;
-    }
-    if (((eL >> eb) & 1u) && !((epaired >> eb) & 1u)) {
-      unp_n++;
-      unp_e = eb;
-    }
-    if (unp_n != 1) continue;
-    fpair[f] = unp_e;
+    const int ea = f & 1, eb = 2 + (f >> 1);  // the face's lower-star-candidate edges, reference order
+    const bool ua = ((eL >> ea) & 1u) && !((epaired >> ea) & 1u);
+    const bool ub = ((eL >> eb) & 1u) && !((epaired >> eb) & 1u);
+    if (ua == ub) continue;  // zero or two unpaired lower-star edges
+    const int e = ua ? ea : eb;
+    fpk = (fpk & ~(0xFu << (4 * f))) | ((unsigned)e << (4 * f));
     fpaired |= 1u << f;
-    epair[unp_e] = f;
-    epaired |= 1u << unp_e;
-    int cand[2] = {ef_a[unp_e], ef_b[unp_e]};
+    epk = (epk & ~(0xFu << (4 * e))) | ((unsigned)f << (4 * e));
+    epaired |= 1u << e;
+    // faces bounding edge e, in check_and_push order
+    const int na = e < 2 ? e : 2 * (e - 2);
+    const int nb = e < 2 ? e + 2 : 2 * (e - 2) + 1;
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      int nf = cand[c];
+    for (int k = 0; k < 2; ++k) {
+      const int nf = k == 0 ? na : nb;
       if (nf == f || !((fL >> nf) & 1u) || ((fpaired >> nf) & 1u)) continue;
       bool already = false;
       for (int qi = head; qi < tail; ++qi)
@@ -150,73 +177,68 @@ __device__ __forceinline__ void lower_star(const PixelTile<DUAL>& T, int y, int 
     }
   }
 
-  // --- write owned cells into the index tile ---
-  const int e_iy[4] = {y, y, y, y + 1};
-  const int e_ix[4] = {x, x + 1, x, x};
-  const int e_t[4] = {1, 1, 2, 2};
-  const int f_iy[4] = {y, y, y + 1, y + 1};
-  const int f_ix[4] = {x, x + 1, x, x + 1};
-  auto put = [&](int iy, int ix, int t, int v) {
-    int r = iy - ty0, c = ix - tx0;
-    if (r >= 0 && r < kTileY && c >= 0 && c < kTileX) tile[r][c][t] = v;
+  // owned cells -> index tile (slot index arithmetic: edge k at index
+  // (y + (k == 3), x + (k == 1)), type 1 + (k >> 1); face f at (y + (f >> 1), x + (f & 1)))
+  const int tr = y - ty0, tc = x - tx0;
+  auto put = [&](int dr, int dc, int t, int v) {
+    const int rr = tr + dr, cc = tc + dc;
+    if (rr >= 0 && rr < kTileY && cc >= 0 && cc < kTileX) tile[rr][cc][t] = v;
   };
-  put(y, x, 0, best >= 0 ? cell_id(e_t[best], e_iy[best], e_ix[best], Nx) : -1);
+  const int base = y * Nx + x;
+  auto edge_cell = [&](int k) { return (1 + (k >> 1)) + 4 * (base + (k == 3 ? Nx : 0) + (k == 1 ? 1 : 0)); };
+  auto face_cell = [&](int f) { return 3 + 4 * (base + (f >> 1) * Nx + (f & 1)); };
+  put(0, 0, 0, best >= 0 ? edge_cell(best) : -1);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     if (!((eL >> k) & 1u)) continue;
-    int v = -1;
-    if (epair[k] == 4)
-      v = cell_id(0, y, x, Nx);
-    else if (epair[k] >= 0)
-      v = cell_id(3, f_iy[epair[k]], f_ix[epair[k]], Nx);
-    put(e_iy[k], e_ix[k], e_t[k], v);
+    const unsigned pk = (epk >> (4 * k)) & 0xFu;
+    const int v = pk == 4u ? 4 * base : (pk < 4u ? face_cell((int)pk) : -1);
+    put(k == 3 ? 1 : 0, k == 1 ? 1 : 0, 1 + (k >> 1), v);
   }
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
     if (!((fL >> f) & 1u)) continue;
-    int k = fpair[f];
-    put(f_iy[f], f_ix[f], 3, k >= 0 ? cell_id(e_t[k], e_iy[k], e_ix[k], Nx) : -1);
+    const unsigned pk = (fpk >> (4 * f)) & 0xFu;
+    put(f >> 1, f & 1, 3, pk < 4u ? edge_cell((int)pk) : -1);
   }
 }
 
-// K1: gradient over one 32 x 8 index tile per CTA (256 threads).
+// K1: gradient over one 32 x 8 index tile per CTA (320 threads).
 template <bool DUAL>
-__global__ void __launch_bounds__(256) gradient_kernel(const float* __restrict__ img, int H, int W,
-                                                       int4* __restrict__ grad, uint8_t* __restrict__ crit_mask,
-                                                       int* __restrict__ seg_min, int* __restrict__ seg_sad,
-                                                       int* __restrict__ seg_max) {
+__global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __restrict__ img, int H, int W,
+                                                               int4* __restrict__ grad,
+                                                               uint8_t* __restrict__ crit_mask,
+                                                               int* __restrict__ seg_min, int* __restrict__ seg_sad,
+                                                               int* __restrict__ seg_max) {
   __shared__ float sv[kValY][kValX];
   __shared__ int tile[kTileY][kTileX][4];
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY;
   const int Nx = W + 1;
 
-  for (int i = tid; i < kValY * kValX; i += 256) {
+  for (int i = tid; i < kValY * kValX; i += kGradThreads) {
     int r = i / kValX, c = i - r * kValX;
     int gy = y0 - 2 + r, gx = x0 - 2 + c;
     sv[r][c] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(img + (size_t)gy * W + gx) : 0.0f;
   }
-  for (int i = tid; i < kTileY * kTileX; i += 256) {
-    int r = i / kTileX, c = i - r * kTileX;
-    tile[r][c][0] = tile[r][c][1] = tile[r][c][2] = tile[r][c][3] = -1;
-  }
+  for (int i = tid; i < kTileY * kTileX; i += kGradThreads)
+    reinterpret_cast<int4*>(&tile[0][0][0])[i] = make_int4(-1, -1, -1, -1);
   __syncthreads();
 
-  PixelTile<DUAL> T{sv, y0 - 2, x0 - 2, W};
-  for (int i = tid; i < (kTileY + 1) * (kTileX + 1); i += 256) {
-    int r = i / (kTileX + 1), c = i - r * (kTileX + 1);
+  if (tid < (kTileY + 1) * (kTileX + 1)) {
+    int r = tid / (kTileX + 1), c = tid - r * (kTileX + 1);
     int y = y0 - 1 + r, x = x0 - 1 + c;
-    if (y < 0 || y >= H || x < 0 || x >= W) continue;
-    lower_star<DUAL>(T, y, x, H, W, Nx, y0, x0, tile);
+    if (y >= 0 && y < H && x >= 0 && x < W) lower_star<DUAL>(sv, y, x, H, W, Nx, y0, x0, tile);
   }
   __syncthreads();
 
   // one warp per tile row: coalesced int4 stores, criticality mask and counts
   const int warp = tid >> 5, lane = tid & 31;
+  if (warp >= kTileY) return;
   const int iy = y0 + warp, ix = x0 + lane;
   if (iy > H) return;
   bool in = ix <= W;
-  int4 v = make_int4(tile[warp][lane][0], tile[warp][lane][1], tile[warp][lane][2], tile[warp][lane][3]);
+  int4 v = reinterpret_cast<const int4*>(&tile[warp][lane][0])[0];
   unsigned m = 0;
   if (in) {
     size_t idx = (size_t)iy * Nx + ix;
