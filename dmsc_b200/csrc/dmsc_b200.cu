@@ -447,6 +447,10 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
     set_err(ctx, "missing output buffer for a requested field");
     return kErrInvalidArgument;
   }
+  if (ret_grad && ((uintptr_t)grad_out & 15u)) {  // written with 16-byte stores
+    set_err(ctx, "grad_out must be 16-byte aligned");
+    return kErrInvalidArgument;
+  }
   CK(cudaSetDevice(ctx->device));
   ctx->H = H;
   ctx->W = W;

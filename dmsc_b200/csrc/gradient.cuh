@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __r
                                                                int* __restrict__ seg_min, int* __restrict__ seg_sad,
                                                                int* __restrict__ seg_max) {
   __shared__ float sv[kValY][kValX];
-  __shared__ int tile[kTileY][kTileX][4];
+  __shared__ __align__(16) int tile[kTileY][kTileX][4];  // read and written as int4
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY;
   const int Nx = W + 1;

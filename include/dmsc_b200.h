@@ -92,7 +92,8 @@ void dmsc_b200_destroy(dmsc_b200_context* ctx);
    contiguous). Replaces extract_single_dmsc_gpu_t up to output assembly
    (dmsc/csrc/dmsc_gpu.cpp:53-82) and the size part of gpu::Workspace::complex
    (dmsc/csrc/gpu/workspace.hxx:91-397).
-   `grad_out`   : int32[4*(H+1)*(W+1)] when DMSC_B200_RETURN_GRADIENT, else NULL.
+   `grad_out`   : int32[4*(H+1)*(W+1)], 16-byte aligned, when DMSC_B200_RETURN_GRADIENT,
+                  else NULL.
    `peaks_out`  : int32[(H+1)*(W+1)] in the primal, int32[H*W] in the dual,
                   when DMSC_B200_TRACE_PEAKS, else NULL.
    `basins_out` : int32[H*W] in the primal, int32[(H+1)*(W+1)] in the dual,
