@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "gradient.cuh"
 #include "pairing.cuh"
+#include "persistent.cuh"
 #include "replay.cuh"
 #include "walks.cuh"
 
@@ -108,6 +109,8 @@ struct dmsc_b200_context {
   // profiling: launch counter and stage boundary events
   long long launches = 0;
   bool profile = false;
+  uint32_t* fifo_lut = nullptr;  // face-pairing FIFO table (device)
+  int num_sms = 0;
   cudaEvent_t ev[kStageMarks] = {};
 };
 
@@ -233,6 +236,22 @@ void mark(dmsc_b200_context* ctx, int k, cudaStream_t st) {
   if (ctx->profile) CK(cudaEventRecord(ctx->ev[k], st));
 }
 
+// Cooperative launch of a persistent kernel: all blocks co-resident (at most
+// 4 per SM), so grid-wide barriers are safe.
+template <class T>
+void coop_launch(dmsc_b200_context* ctx, void (*kernel)(T), T args, cudaStream_t st, const char* name) {
+  int per = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, 0));
+  if (per < 1) {
+    set_err(ctx, "%s cannot be made resident", name);
+    throw Fail{kErrInternal};
+  }
+  if (per > 4) per = 4;
+  void* a[] = {&args};
+  CK(cudaLaunchCooperativeKernel((void*)kernel, dim3(per * ctx->num_sms), dim3(256), a, 0, st));
+  ++ctx->launches;
+}
+
 // Host read of `k` pinned scalars after the stream drains.
 void readback(dmsc_b200_context* ctx, cudaStream_t st, const long long* dev, int k) {
   CK(cudaMemcpyAsync(ctx->pinned, dev, k * sizeof(long long), cudaMemcpyDeviceToHost, st));
@@ -275,36 +294,32 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
     LK(sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, reverse, S.t, S.sweep, S.c1, S.c2, S.dying));
     LAUNCH_CHECK("sweep_edges_kernel");
   }
-  LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(grp, M + 1));
-  LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(link, M + 1));
-  CK(cudaMemsetAsync(minedge, 0xFF, (M + 1) * sizeof(unsigned), st));
-  if (nsad > 0) LK(iota_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(act[0], nsad));
-  LAUNCH_CHECK("pairing init");
-  // older = value_less<D'> with D' = dual on the vertex side, !dual on the face side
-  const bool older_less = S.faces ? ctx->dual : !ctx->dual;
-  int n_active = nsad, cur = 0, rounds = 0;
-  while (n_active > 0) {
-    if (++rounds > M + 2) {
-      set_err(ctx, "pairing exceeded %d rounds", M + 2);
-      throw Fail{kErrIterationCap};
-    }
-    CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
-    LK(pair_edges_kernel<<<grid_for(n_active, TB), TB, 0, st>>>(act[cur], n_active, S.c1, S.c2, M, grp, S.dying,
-                                                             minedge, act[cur ^ 1], cnt));
+  {
+    PairArgs A;
+    A.nsad = nsad;
+    A.M = M;
+    A.c1 = S.c1;
+    A.c2 = S.c2;
+    A.dying = S.dying;
+    A.link = link;
+    A.minedge = minedge;
+    A.act0 = act[0];
+    A.act1 = act[1];
+    A.touched = grp;  // reuses the group buffer: [M+1]
+    A.hdec = sget<int>(ctx, si, X_CROOT, M + 1);
+    A.cnt = cnt;
+    A.val = S.val;
+    A.cell = S.crit;
+    A.status = ctx->status;
+    A.max_rounds = M + 2;
+    // older = value_less<D'> with D' = dual on the vertex side, !dual on the face side
+    const bool older_less = S.faces ? ctx->dual : !ctx->dual;
     if (older_less)
-      LK(pair_groups_kernel<true><<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, M, S.c1, S.c2, grp, minedge, link,
-                                                                    S.dying, S.val, S.crit));
+      coop_launch(ctx, pairing_persistent_kernel<true>, A, st, "pairing_persistent_kernel");
     else
-      LK(pair_groups_kernel<false><<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, M, S.c1, S.c2, grp, minedge, link,
-                                                                     S.dying, S.val, S.crit));
-    LK(pair_jump_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, grp, link, ctx->status));
-    LAUNCH_CHECK("pairing round");
-    int h = 0;
-    CK(cudaMemcpyAsync(&h, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    n_active = h;
-    cur ^= 1;
+      coop_launch(ctx, pairing_persistent_kernel<false>, A, st, "pairing_persistent_kernel");
   }
+  int rounds = 0;
   S.rounds_pair = rounds;
 
   // persistence, cancellation, alive flags
@@ -353,16 +368,14 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   int* cval = sget<int>(ctx, si, X_CVAL, nsad);
   int* cord = sget<int>(ctx, si, X_CORD, nsad);
   int* cnt = sget<int>(ctx, si, X_CNT, 4);
-  CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), st));
   if (nsad > 0)
-    LK(cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->thr,
-                                                             ctx->crit_sad, ckey, cval, cnt));
-  LAUNCH_CHECK("cancel_collect_kernel");
-  int C = 0;
-  CK(cudaMemcpyAsync(&C, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  S.C = C;
-  sort_pairs(ctx, ckey, ck2, cval, cord, C, st);
+    LK(cancel_keys_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->thr, ctx->crit_sad,
+                                                            ckey, cval, cnt + 3));
+  LAUNCH_CHECK("cancel_keys_kernel");
+  // every saddle is sorted; the non-cancelled ones carry the largest key and
+  // land after the C cancellations, so C never needs to reach the host
+  sort_pairs(ctx, ckey, ck2, cval, cord, nsad, st);
 
   ReplayState& R = S.R;
   R.ctime = sget<int>(ctx, si, X_CTIME, M + 1);
@@ -375,32 +388,28 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   R.cl_ot = sget<long long>(ctx, si, X_CLOT, M + 1);
   LK(fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.ctime, M + 1, kNever));
   LK(fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.status, M + 1, kRootForever));
-  if (C > 0) LK(replay_init_kernel<<<grid_for(C, TB), TB, 0, st>>>(C, cord, S.dying, R));
   LAUNCH_CHECK("replay init");
   int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
-  if (C > 0) LK(iota_kernel<<<grid_for(C, TB), TB, 0, st>>>(act[0], C));
-  int n_active = C, cur = 0, rounds = 0;
-  const int max_steps = C + 1;
-  while (n_active > 0) {
-    if (++rounds > C + 2) {
-      set_err(ctx, "replay exceeded %d rounds", C + 2);
-      throw Fail{kErrIterationCap};
-    }
-    CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
-    LK(replay_round_kernel<<<grid_for(n_active, TB), TB, 0, st>>>(act[cur], n_active, cord, S.sweep, S.dying, S.c1,
-                                                               S.c2, S.blen, R, max_steps, act[cur ^ 1], cnt,
-                                                               ctx->status));
-    LAUNCH_CHECK("replay_round_kernel");
-    int h = 0;
-    CK(cudaMemcpyAsync(&h, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (h == n_active) {
-      set_err(ctx, "replay made no progress");
-      throw Fail{kErrInternal};
-    }
-    n_active = h;
-    cur ^= 1;
+  const int max_steps = nsad + 1;
+  {
+    ReplayArgs A;
+    A.n_cancel = cnt + 3;
+    A.order = cord;
+    A.sweep = S.sweep;
+    A.dying = S.dying;
+    A.c1 = S.c1;
+    A.c2 = S.c2;
+    A.blen = S.blen;
+    A.S = R;
+    A.max_steps = max_steps;
+    A.act0 = act[0];
+    A.act1 = act[1];
+    A.cnt = cnt;
+    A.status = ctx->status;
+    A.max_rounds = nsad + 2;
+    coop_launch(ctx, replay_persistent_kernel, A, st, "replay_persistent_kernel");
   }
+  int rounds = 0;
   S.rounds_replay = rounds;
 
   S.arc_len = sget<long long>(ctx, si, X_ALEN, 2 * (size_t)nsurv);
@@ -474,9 +483,9 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
   dim3 g1(nsegx, (H + 1 + kTileY - 1) / kTileY);
   if (dual)
-    LK(gradient_kernel<true><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]));
+    LK(gradient_kernel<true><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2], ctx->fifo_lut));
   else
-    LK(gradient_kernel<false><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2]));
+    LK(gradient_kernel<false><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2], ctx->fifo_lut));
   LAUNCH_CHECK("gradient_kernel");
   mark(ctx, 1, st);
   for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);
@@ -666,9 +675,8 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   LAUNCH_CHECK("arc_offsets_kernel");
   if (S.total <= 0 || !flat) return;
   long long cap = S.total;
-  int4* q[2] = {sget<int4>(ctx, si, X_Q0, cap), sget<int4>(ctx, si, X_Q1, cap)};
-  int* cnt = sget<int>(ctx, si, X_CNT, 4);
-  EmitCtx E;
+  EmitArgs A;
+  EmitCtx& E = A.E;
   E.grad = ctx->grad;
   E.crit_sad = ctx->crit_sad;
   E.H = ctx->H;
@@ -679,31 +687,21 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   E.blen = S.blen;
   E.S = S.R;
   E.out = flat;
+  E.q_out = nullptr;
+  E.n_out = nullptr;
   E.q_cap = cap;
-  E.max_steps = S.C + 1;
+  E.max_steps = ctx->nsad + 1;
   E.status = ctx->status;
-  int cur = 0;
-  E.q_out = q[cur];
-  E.n_out = cnt;
-  CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
-  LK(emit_roots_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(E, nsurv, ctx->surv, S.arc_pos, S.arc_cl, S.arc_root));
-  LAUNCH_CHECK("emit_roots_kernel");
-  int n = 0, levels = 0;
-  CK(cudaMemcpyAsync(&n, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  while (n > 0) {
-    if (n > cap || ++levels > S.C + 4) {
-      set_err(ctx, "geometry expansion overflow");
-      throw Fail{kErrOverflow};
-    }
-    E.q_out = q[cur ^ 1];
-    CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
-    LK(emit_level_kernel<<<grid_for(n, TB), TB, 0, st>>>(E, q[cur], n));
-    LAUNCH_CHECK("emit_level_kernel");
-    CK(cudaMemcpyAsync(&n, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    cur ^= 1;
-  }
+  A.nsurv = nsurv;
+  A.surv_sad = ctx->surv;
+  A.arc_pos = S.arc_pos;
+  A.arc_cl = S.arc_cl;
+  A.arc_root = S.arc_root;
+  A.q0 = sget<int4>(ctx, si, X_Q0, cap);
+  A.q1 = sget<int4>(ctx, si, X_Q1, cap);
+  A.cnt = sget<int>(ctx, si, X_CNT, 4);
+  A.max_levels = ctx->nsad + 4;
+  coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel");
 }
 
 int fetch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t st) {
@@ -771,6 +769,17 @@ int dmsc_b200_create(dmsc_b200_context** out, int device) {
     delete c;
     return kErrCuda;
   }
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  {
+    std::vector<uint32_t> lut(kFifoTable);
+    face_fifo_table(lut.data());
+    if (cudaMalloc(&c->fifo_lut, kFifoTable * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMemcpy(c->fifo_lut, lut.data(), kFifoTable * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaFreeHost(c->pinned);
+      delete c;
+      return kErrCuda;
+    }
+  }
   *out = c;
   return kOk;
 }
@@ -781,6 +790,7 @@ void dmsc_b200_destroy(dmsc_b200_context* c) {
   for (auto& b : c->bufs)
     if (b.p) cudaFree(b.p);
   if (c->cub_tmp.p) cudaFree(c->cub_tmp.p);
+  if (c->fifo_lut) cudaFree(c->fifo_lut);
   if (c->pinned) cudaFreeHost(c->pinned);
   for (int k = 0; k < kStageMarks; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);

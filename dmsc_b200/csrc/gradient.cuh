@@ -29,6 +29,57 @@ constexpr int kTileY = 8;   // tile rows (one warp each)
 constexpr int kValX = kTileX + 3;
 constexpr int kValY = kTileY + 3;
 
+// Face-edge pairing FIFO of one lower star (cpu/gradient.hxx:115-191) as a
+// pure function of eL (lower-star edge slots), fL (lower-star face slots) and
+// `best` (edge slot paired with the vertex, -1 for none). Result: 4 bits per
+// edge slot (4 = vertex, 0..3 = face slot, 15 = unpaired) in the low half and
+// 4 bits per face slot (edge slot or 15) in the high half. Edge slots
+// e0 = H(y,x), e1 = H(y,x+1), e2 = V(y,x), e3 = V(y+1,x); face slots
+// f0 = F(y,x), f1 = F(y,x+1), f2 = F(y+1,x), f3 = F(y+1,x+1). Face f's
+// candidate edges in the reference visiting order are (f & 1, 2 + (f >> 1));
+// edge e bounds faces (e, e+2) for e < 2 and (2(e-2), 2(e-2)+1) otherwise.
+inline uint32_t face_fifo_entry(unsigned eL, unsigned fL, int best) {
+  unsigned epk = 0xFFFFu, fpk = 0xFFFFu, epaired = 0, fpaired = 0;
+  if (best >= 0) {
+    epk = (epk & ~(0xFu << (4 * best))) | (4u << (4 * best));
+    epaired = 1u << best;
+  }
+  int q[16], head = 0, tail = 0;
+  for (int f = 0; f < 4; ++f)
+    if ((fL >> f) & 1u) q[tail++] = f;
+  while (head < tail) {
+    const int f = q[head++];
+    if ((fpaired >> f) & 1u) continue;
+    const int ea = f & 1, eb = 2 + (f >> 1);
+    const bool ua = ((eL >> ea) & 1u) && !((epaired >> ea) & 1u);
+    const bool ub = ((eL >> eb) & 1u) && !((epaired >> eb) & 1u);
+    if (ua == ub) continue;  // zero or two unpaired lower-star edges
+    const int e = ua ? ea : eb;
+    fpk = (fpk & ~(0xFu << (4 * f))) | ((unsigned)e << (4 * f));
+    fpaired |= 1u << f;
+    epk = (epk & ~(0xFu << (4 * e))) | ((unsigned)f << (4 * e));
+    epaired |= 1u << e;
+    const int nb[2] = {e < 2 ? e : 2 * (e - 2), e < 2 ? e + 2 : 2 * (e - 2) + 1};
+    for (int k = 0; k < 2; ++k) {
+      const int nf = nb[k];
+      if (nf == f || !((fL >> nf) & 1u) || ((fpaired >> nf) & 1u)) continue;
+      bool already = false;
+      for (int qi = head; qi < tail; ++qi)
+        if (q[qi] == nf) already = true;
+      if (!already && tail < 16) q[tail++] = nf;
+    }
+  }
+  return (fpk << 16) | epk;
+}
+
+// All 16 x 16 x 5 entries, indexed ((eL << 4) | fL) * 5 + best + 1.
+inline void face_fifo_table(uint32_t* out) {
+  for (unsigned eL = 0; eL < 16; ++eL)
+    for (unsigned fL = 0; fL < 16; ++fL)
+      for (int b = -1; b < 4; ++b) out[((eL << 4) | fL) * 5 + (b + 1)] = face_fifo_entry(eL, fL, b);
+}
+constexpr int kFifoTable = 16 * 16 * 5;
+
 constexpr int kGradThreads = 320;  // >= (kTileY + 1) * (kTileX + 1) = 297 lower stars per tile
 
 // One pixel value with its linear id; gt() is v_greater (cpu/cell_compare.hxx:23-31):
@@ -50,7 +101,7 @@ __device__ __forceinline__ bool gt(const Px& a, const Px& b) {
 // Writes the gradient values of the owned cells into the shared index tile.
 template <bool DUAL>
 __device__ __forceinline__ void lower_star(const float (*sv)[kValX], int y, int x, int H, int W, int Nx, int ty0,
-                                           int tx0, int (*tile)[kTileX][4]) {
+                                           int tx0, int (*tile)[kTileY][kTileX], const uint32_t* __restrict__ fifo_lut) {
   // 3x3 neighbourhood; r, c index the value tile (origin y0-2, x0-2)
   const int r = y - (ty0 - 2), c = x - (tx0 - 2);
   const bool lv = x >= 1, rv = x + 1 < W, uv = y >= 1, dv = y + 1 < H;
@@ -131,58 +182,18 @@ __device__ __forceinline__ void lower_star(const float (*sv)[kValX], int y, int 
     bo = D;
   }
 
-  // face pairing by FIFO. Pair state packed 4 bits per slot: epk (edge ->
-  // 4 vertex, 0..3 face, 15 none), fpk (face -> edge slot, 15 none).
-  unsigned epk = 0xFFFFu, fpk = 0xFFFFu;
-  unsigned epaired = 0, fpaired = 0;
-  if (best >= 0) {
-    epk = (epk & ~(0xFu << (4 * best))) | (4u << (4 * best));
-    epaired = 1u << best;
-  }
-  unsigned long long q = 0;  // queue of face slots, 4 bits per entry
-  int head = 0, tail = 0;
-#pragma unroll
-  for (int f = 0; f < 4; ++f)
-    if ((fL >> f) & 1u) {
-      q |= (unsigned long long)f << (4 * tail);
-      tail++;
-    }
-  while (head < tail) {
-    const int f = (int)((q >> (4 * head)) & 0xFull);
-    head++;
-    if ((fpaired >> f) & 1u) continue;
-    const int ea = f & 1, eb = 2 + (f >> 1);  // the face's lower-star-candidate edges, reference order
-    const bool ua = ((eL >> ea) & 1u) && !((epaired >> ea) & 1u);
-    const bool ub = ((eL >> eb) & 1u) && !((epaired >> eb) & 1u);
-    if (ua == ub) continue;  // zero or two unpaired lower-star edges
-    const int e = ua ? ea : eb;
-    fpk = (fpk & ~(0xFu << (4 * f))) | ((unsigned)e << (4 * f));
-    fpaired |= 1u << f;
-    epk = (epk & ~(0xFu << (4 * e))) | ((unsigned)f << (4 * e));
-    epaired |= 1u << e;
-    // faces bounding edge e, in check_and_push order
-    const int na = e < 2 ? e : 2 * (e - 2);
-    const int nb = e < 2 ? e + 2 : 2 * (e - 2) + 1;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int nf = k == 0 ? na : nb;
-      if (nf == f || !((fL >> nf) & 1u) || ((fpaired >> nf) & 1u)) continue;
-      bool already = false;
-      for (int qi = head; qi < tail; ++qi)
-        if ((int)((q >> (4 * qi)) & 0xFull) == nf) already = true;
-      if (!already && tail < 16) {
-        q |= (unsigned long long)nf << (4 * tail);
-        tail++;
-      }
-    }
-  }
+  // face pairing: the FIFO of cpu/gradient.hxx:115-191 depends only on the
+  // lower-star masks and the vertex-paired edge, so its result is looked up
+  // (face_fifo_table() builds the 1280 entries with the same procedure).
+  const uint32_t pr = __ldg(fifo_lut + (((eL << 4) | fL) * 5 + (best + 1)));
+  const unsigned epk = pr & 0xFFFFu, fpk = pr >> 16;
 
   // owned cells -> index tile (slot index arithmetic: edge k at index
   // (y + (k == 3), x + (k == 1)), type 1 + (k >> 1); face f at (y + (f >> 1), x + (f & 1)))
   const int tr = y - ty0, tc = x - tx0;
   auto put = [&](int dr, int dc, int t, int v) {
     const int rr = tr + dr, cc = tc + dc;
-    if (rr >= 0 && rr < kTileY && cc >= 0 && cc < kTileX) tile[rr][cc][t] = v;
+    if (rr >= 0 && rr < kTileY && cc >= 0 && cc < kTileX) tile[t][rr][cc] = v;
   };
   const int base = y * Nx + x;
   auto edge_cell = [&](int k) { return (1 + (k >> 1)) + 4 * (base + (k == 3 ? Nx : 0) + (k == 1 ? 1 : 0)); };
@@ -209,9 +220,10 @@ __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __r
                                                                int4* __restrict__ grad,
                                                                uint8_t* __restrict__ crit_mask,
                                                                int* __restrict__ seg_min, int* __restrict__ seg_sad,
-                                                               int* __restrict__ seg_max) {
+                                                               int* __restrict__ seg_max,
+                                                               const uint32_t* __restrict__ fifo_lut) {
   __shared__ float sv[kValY][kValX];
-  __shared__ __align__(16) int tile[kTileY][kTileX][4];  // read and written as int4
+  __shared__ int tile[4][kTileY][kTileX];  // slot-major: conflict-free per-slot writes
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY;
   const int Nx = W + 1;
@@ -221,14 +233,13 @@ __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __r
     int gy = y0 - 2 + r, gx = x0 - 2 + c;
     sv[r][c] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(img + (size_t)gy * W + gx) : 0.0f;
   }
-  for (int i = tid; i < kTileY * kTileX; i += kGradThreads)
-    reinterpret_cast<int4*>(&tile[0][0][0])[i] = make_int4(-1, -1, -1, -1);
+  for (int i = tid; i < 4 * kTileY * kTileX; i += kGradThreads) (&tile[0][0][0])[i] = -1;
   __syncthreads();
 
   if (tid < (kTileY + 1) * (kTileX + 1)) {
     int r = tid / (kTileX + 1), c = tid - r * (kTileX + 1);
     int y = y0 - 1 + r, x = x0 - 1 + c;
-    if (y >= 0 && y < H && x >= 0 && x < W) lower_star<DUAL>(sv, y, x, H, W, Nx, y0, x0, tile);
+    if (y >= 0 && y < H && x >= 0 && x < W) lower_star<DUAL>(sv, y, x, H, W, Nx, y0, x0, tile, fifo_lut);
   }
   __syncthreads();
 
@@ -238,7 +249,7 @@ __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __r
   const int iy = y0 + warp, ix = x0 + lane;
   if (iy > H) return;
   bool in = ix <= W;
-  int4 v = reinterpret_cast<const int4*>(&tile[warp][lane][0])[0];
+  int4 v = make_int4(tile[0][warp][lane], tile[1][warp][lane], tile[2][warp][lane], tile[3][warp][lane]);
   unsigned m = 0;
   if (in) {
     size_t idx = (size_t)iy * Nx + ix;

@@ -43,79 +43,6 @@ __device__ __forceinline__ bool older(int a, int b, int void_id, const float* __
   return OLDER_LESS ? tie_lt(val[a], cell[a], val[b], cell[b]) : tie_lt(val[b], cell[b], val[a], cell[a]);
 }
 
-// Round step 1: relabel each active saddle's ends; cycles are decided, the
-// rest offer their sweep index to both groups' minimum.
-__global__ void __launch_bounds__(256) pair_edges_kernel(const int* __restrict__ active, int n_active,
-                                                         const int* __restrict__ c1, const int* __restrict__ c2,
-                                                         int void_id, const int* __restrict__ grp,
-                                                         int* __restrict__ dying, unsigned* __restrict__ minedge,
-                                                         int* __restrict__ next_active, int* __restrict__ n_next) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool keep = false;
-  int e = -1;
-  if (i < n_active) {
-    e = active[i];
-    if (dying[e] == kUndecided) {
-      int a = c1[e], b = c2[e];
-      int ga = grp[a < 0 ? void_id : a], gb = grp[b < 0 ? void_id : b];
-      if (ga == gb) {
-        dying[e] = -1;
-      } else {
-        atomicMin(minedge + ga, (unsigned)e);
-        atomicMin(minedge + gb, (unsigned)e);
-        keep = true;
-      }
-    }
-  }
-  // warp-aggregated append
-  unsigned b = __ballot_sync(0xffffffffu, keep);
-  if (b == 0) return;
-  int lane = threadIdx.x & 31, leader = __ffs(b) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(n_next, __popc(b));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (keep) next_active[base + __popc(b & ((1u << lane) - 1u))] = e;
-}
-
-// Round step 2: each group root with an outgoing saddle decides.
-template <bool OLDER_LESS>
-__global__ void __launch_bounds__(256) pair_groups_kernel(int n_nodes, int void_id, const int* __restrict__ c1,
-                                                          const int* __restrict__ c2, const int* __restrict__ grp,
-                                                          unsigned* __restrict__ minedge, int* __restrict__ link,
-                                                          int* __restrict__ dying, const float* __restrict__ val,
-                                                          const int* __restrict__ cell) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n_nodes) return;
-  unsigned me = minedge[g];
-  if (me == kNoEdge) return;
-  minedge[g] = kNoEdge;
-  int e = (int)me;
-  int a = c1[e], b = c2[e];
-  int ga = grp[a < 0 ? void_id : a], gb = grp[b < 0 ? void_id : b];
-  int h = (ga == g) ? gb : ga;
-  if (older<OLDER_LESS>(h, g, void_id, val, cell)) {
-    link[g] = h;
-    dying[e] = g;
-  }
-}
-
-// Round step 3: every node's group becomes the root of its group's link chain.
-__global__ void __launch_bounds__(256) pair_jump_kernel(int n_nodes, int* __restrict__ grp,
-                                                        const int* __restrict__ link, unsigned* status) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= n_nodes) return;
-  int r = grp[x];
-  int guard = 0;
-  while (link[r] != r) {
-    r = link[r];
-    if (++guard > n_nodes) {
-      set_status(status, kStatusRoundCap);
-      break;
-    }
-  }
-  grp[x] = r;
-}
-
 __global__ void iota_kernel(int* __restrict__ a, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = i;
@@ -127,7 +54,8 @@ __global__ void fill_kernel(int* __restrict__ a, long long n, int v) {
 }
 
 // Builds the sweep-ordered edge list of one side: edge j is saddle
-// sweep[j] with ends (t[2s], t[2s+1]).
+// sweep[j] with ends (t[2s], t[2s+1]). The round loop itself is
+// pairing_persistent_kernel (persistent.cuh).
 __global__ void sweep_edges_kernel(int nsad, const int* __restrict__ asc, bool reverse, const int* __restrict__ t,
                                    int* __restrict__ sweep, int* __restrict__ c1, int* __restrict__ c2,
                                    int* __restrict__ dying) {

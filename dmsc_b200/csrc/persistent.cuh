@@ -1,0 +1,293 @@
+// Persistent cooperative kernels: the round loops of the pairing, the replay
+// and the geometry expansion run entirely on the device, separated by
+// grid-wide barriers, with no host round trip per round.
+//
+// Counters rotate over three slots: round r reads its input count from
+// cnt[r % 3], appends its output to cnt[(r + 1) % 3] and clears
+// cnt[(r + 2) % 3], which was last read at the top of round r - 1 (before the
+// barrier that ended that round). Every loop is capped; hitting a cap sets a
+// status bit the host turns into an error, and every thread leaves the loop at
+// the same round because the loop condition reads the same counters.
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "pairing.cuh"
+#include "replay.cuh"
+
+namespace dmsc {
+
+namespace cg = cooperative_groups;
+
+__device__ __forceinline__ int find_halving(int* link, int x) {
+  while (true) {
+    int p = link[x];
+    if (p == x) return x;
+    int pp = link[p];
+    if (pp != p) link[x] = pp;  // path halving: replaces a pointer with an ancestor
+    x = pp;
+  }
+}
+
+__device__ __forceinline__ int warp_append(int* counter, bool take) {
+  unsigned b = __ballot_sync(0xffffffffu, take);
+  if (b == 0) return -1;
+  int lane = threadIdx.x & 31, leader = __ffs(b) - 1, base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(b));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return take ? base + __popc(b & ((1u << lane) - 1u)) : -1;
+}
+
+// ---------------------------------------------------------------------------
+// pairing rounds (see pairing.cuh for the algorithm)
+// ---------------------------------------------------------------------------
+struct PairArgs {
+  int nsad, M;  // void group = M
+  const int* c1;
+  const int* c2;
+  int* dying;
+  int* link;          // [M+1] group union-find
+  unsigned* minedge;  // [M+1]
+  int* act0;
+  int* act1;
+  int* touched;  // [M+1]
+  int* hdec;     // [M+1]
+  int* cnt;      // [0..2] rotating active counts, [3] touched count
+  const float* val;
+  const int* cell;
+  unsigned* status;
+  int max_rounds;
+};
+
+template <bool OLDER_LESS>
+__global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
+  cg::grid_group grid = cg::this_grid();
+  const long long tid = grid.thread_rank(), nth = grid.size();
+  const int M = A.M;
+  for (long long i = tid; i <= M; i += nth) {
+    A.link[i] = (int)i;
+    A.minedge[i] = kNoEdge;
+  }
+  for (long long i = tid; i < A.nsad; i += nth) {
+    A.act0[i] = (int)i;
+    A.dying[i] = kUndecided;
+  }
+  if (tid == 0) {
+    A.cnt[0] = A.nsad;
+    A.cnt[1] = 0;
+    A.cnt[2] = 0;
+    A.cnt[3] = 0;
+  }
+  grid.sync();
+  for (int r = 0;; ++r) {
+    const int n = *(volatile int*)(A.cnt + r % 3);
+    if (n == 0) break;
+    if (r >= A.max_rounds) {
+      if (tid == 0) set_status(A.status, kStatusRoundCap);
+      break;
+    }
+    const int* in = (r & 1) ? A.act1 : A.act0;
+    int* out = (r & 1) ? A.act0 : A.act1;
+    int* ocnt = A.cnt + (r + 1) % 3;
+    if (tid == 0) A.cnt[(r + 2) % 3] = 0;
+    // phase A: relabel ends; cycles decided; offer to both groups' minimum
+    for (long long base = 0; base < n; base += nth) {
+      long long i = base + tid;
+      bool keep = false;
+      int e = -1;
+      if (i < n) {
+        e = in[i];
+        if (A.dying[e] == kUndecided) {
+          int a = A.c1[e], b = A.c2[e];
+          int ga = find_halving(A.link, a < 0 ? M : a), gb = find_halving(A.link, b < 0 ? M : b);
+          if (ga == gb) {
+            A.dying[e] = -1;
+          } else {
+            if (atomicMin(A.minedge + ga, (unsigned)e) == kNoEdge) A.touched[atomicAdd(A.cnt + 3, 1)] = ga;
+            if (atomicMin(A.minedge + gb, (unsigned)e) == kNoEdge) A.touched[atomicAdd(A.cnt + 3, 1)] = gb;
+            keep = true;
+          }
+        }
+      }
+      int p = warp_append(ocnt, keep);
+      if (keep) out[p] = e;
+    }
+    grid.sync();
+    // phase B1: every touched group decides on its first outgoing saddle
+    const int nt = *(volatile int*)(A.cnt + 3);
+    for (long long k = tid; k < nt; k += nth) {
+      int g = A.touched[k];
+      int e = (int)A.minedge[g];
+      A.minedge[g] = kNoEdge;
+      int a = A.c1[e], b = A.c2[e];
+      int ga = find_halving(A.link, a < 0 ? M : a), gb = find_halving(A.link, b < 0 ? M : b);
+      int h = (ga == g) ? gb : ga;
+      if (older<OLDER_LESS>(h, g, M, A.val, A.cell)) {
+        A.hdec[k] = h;
+        A.dying[e] = g;
+      } else {
+        A.hdec[k] = -1;
+      }
+    }
+    grid.sync();
+    // phase B2: apply the links
+    for (long long k = tid; k < nt; k += nth)
+      if (A.hdec[k] >= 0) A.link[A.touched[k]] = A.hdec[k];
+    if (tid == 0) A.cnt[3] = 0;
+    grid.sync();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// replay rounds (see replay.cuh)
+// ---------------------------------------------------------------------------
+struct ReplayArgs {
+  const int* n_cancel;  // device count of cancellations
+  const int* order;     // sweep index of the r-th cancellation in replay order
+  const int* sweep;
+  const int* dying;
+  const int* c1;
+  const int* c2;
+  const long long* blen;
+  ReplayState S;
+  int max_steps;
+  int* act0;
+  int* act1;
+  int* cnt;  // [0..2]
+  unsigned* status;
+  int max_rounds;
+};
+
+__global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs A) {
+  cg::grid_group grid = cg::this_grid();
+  const long long tid = grid.thread_rank(), nth = grid.size();
+  const int C = *A.n_cancel;
+  for (long long r = tid; r < C; r += nth) {
+    A.act0[r] = (int)r;
+    int d = A.dying[A.order[r]];
+    A.S.ctime[d] = (int)r;
+    A.S.status[d] = kPending;
+  }
+  if (tid == 0) {
+    A.cnt[0] = C;
+    A.cnt[1] = 0;
+    A.cnt[2] = 0;
+  }
+  grid.sync();
+  for (int rd = 0;; ++rd) {
+    const int n = *(volatile int*)(A.cnt + rd % 3);
+    if (n == 0) break;
+    if (rd >= A.max_rounds) {
+      if (tid == 0) set_status(A.status, kStatusRoundCap);
+      break;
+    }
+    const int* in = (rd & 1) ? A.act1 : A.act0;
+    int* out = (rd & 1) ? A.act0 : A.act1;
+    int* ocnt = A.cnt + (rd + 1) % 3;
+    if (tid == 0) A.cnt[(rd + 2) % 3] = 0;
+    for (long long base = 0; base < n; base += nth) {
+      long long i = base + tid;
+      bool keep = false;
+      int r = -1;
+      if (i < n) {
+        r = in[i];
+        int j = A.order[r];
+        int d = A.dying[j], s = A.sweep[j];
+        int T0 = A.c1[j], T1 = A.c2[j];
+        int R0 = -1, R1 = -1;
+        long long a0 = 0, a1 = 0;
+        bool ok = walk_root(A.S, T0, r, &R0, &a0, A.max_steps, A.status) &&
+                  walk_root(A.S, T1, r, &R1, &a1, A.max_steps, A.status);
+        if (!ok) {
+          keep = true;
+        } else {
+          int k = -1;
+          if (R0 == d && R0 != R1)
+            k = 0;
+          else if (R1 == d && R0 != R1)
+            k = 1;
+          if (k >= 0) {
+            A.S.parent[d] = k == 0 ? R1 : R0;
+            A.S.side[d] = k;
+            A.S.csad[d] = s;
+            A.S.cl_dy[d] = k == 0 ? a0 : a1;
+            A.S.cl_ot[d] = k == 0 ? a1 : a0;
+            A.S.wlen[d] = A.blen[2 * s] + A.blen[2 * s + 1] + a0 + a1;
+            st_release(A.S.status + d, kLinked);
+          } else {
+            st_release(A.S.status + d, kRootForever);
+          }
+        }
+      }
+      int p = warp_append(ocnt, keep);
+      if (keep) out[p] = r;
+    }
+    grid.sync();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// geometry expansion levels (see replay.cuh)
+// ---------------------------------------------------------------------------
+struct EmitArgs {
+  EmitCtx E;
+  int nsurv;
+  const int* surv_sad;
+  const long long* arc_pos;
+  const long long* arc_cl;
+  const int* arc_root;
+  int4* q0;
+  int4* q1;
+  int* cnt;  // [0..2]
+  int max_levels;
+};
+
+__global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
+  cg::grid_group grid = cg::this_grid();
+  const long long tid = grid.thread_rank(), nth = grid.size();
+  if (tid == 0) {
+    A.cnt[0] = 0;
+    A.cnt[1] = 0;
+    A.cnt[2] = 0;
+  }
+  grid.sync();
+  EmitCtx E = A.E;
+  // level 0: each surviving arc's own raw arc, then its chain
+  E.q_out = A.q0;
+  E.n_out = A.cnt;
+  for (long long q = tid; q < 2LL * A.nsurv; q += nth) {
+    int i = (int)(q >> 1), j = (int)(q & 1);
+    int s = A.surv_sad[i];
+    if (E.t[2 * s + j] < 0) continue;
+    long long pos = A.arc_pos[q];
+    emit_base(E, s, j, 0, pos);
+    if (A.arc_cl[q] > 0) push_task(E, make_task(kTaskChain, 0, E.t[2 * s + j], A.arc_root[q], pos + E.blen[2 * s + j]));
+  }
+  grid.sync();
+  for (int lv = 0;; ++lv) {
+    int n = *(volatile int*)(A.cnt + lv % 3);
+    if (n == 0) break;
+    if (lv >= A.max_levels || n > E.q_cap) {
+      if (tid == 0) set_status(E.status, kStatusQueueOverflow);
+      break;
+    }
+    const int4* in = (lv & 1) ? A.q1 : A.q0;
+    E.q_out = (lv & 1) ? A.q0 : A.q1;
+    E.n_out = A.cnt + (lv + 1) % 3;
+    if (tid == 0) A.cnt[(lv + 2) % 3] = 0;
+    for (long long i = tid; i < n; i += nth) {
+      int4 t = in[i];
+      int kind = t.x & 3, rev = (t.x >> 2) & 1;
+      if (kind == kTaskW)
+        emit_w(E, t.y, rev, t.w);
+      else if (kind == kTaskChain)
+        emit_chain(E, t.y, t.z, rev, t.w);
+      else
+        emit_base(E, t.y, t.z, rev, t.w);
+    }
+    grid.sync();
+  }
+}
+
+}  // namespace dmsc

@@ -77,91 +77,31 @@ __device__ __forceinline__ bool walk_root(const ReplayState& S, int x, int t, in
   return true;
 }
 
-// Cancellation list of one side in sweep order -> (key, sweep index).
-__global__ void cancel_collect_kernel(int nsad, const int* __restrict__ sweep, const int* __restrict__ dying,
-                                      const float* __restrict__ pers, float thr, const int* __restrict__ crit_sad,
-                                      unsigned long long* __restrict__ keys, int* __restrict__ vals,
-                                      int* __restrict__ count) {
+// Sort keys of one side's saddles in sweep order: a cancelled saddle gets
+// (persistence, saddle cell) -- CancelEvent::operator<
+// (cpu/persistence_struct.hxx:16-21); a saddle is cancelled at most once per
+// side, so this pair is unique -- and every other saddle the largest key, so
+// the C cancellations come first after sorting. `count` receives C.
+__global__ void cancel_keys_kernel(int nsad, const int* __restrict__ sweep, const int* __restrict__ dying,
+                                   const float* __restrict__ pers, float thr, const int* __restrict__ crit_sad,
+                                   unsigned long long* __restrict__ keys, int* __restrict__ vals,
+                                   int* __restrict__ count) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   bool take = false;
-  unsigned long long key = 0;
-  if (j < nsad && dying[j] >= 0) {
-    float p = pers[sweep[j]];
-    if (p <= thr) {
-      take = true;
-      // CancelEvent::operator< (cpu/persistence_struct.hxx:16-21); a saddle is
-      // cancelled at most once per side, so (persistence, saddle) is unique.
-      key = ((unsigned long long)orderable_key(p) << 32) | (unsigned)crit_sad[sweep[j]];
-    }
-  }
-  unsigned b = __ballot_sync(0xffffffffu, take);
-  if (b == 0) return;
-  int lane = threadIdx.x & 31, leader = __ffs(b) - 1, base = 0;
-  if (lane == leader) base = atomicAdd(count, __popc(b));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (take) {
-    int p = base + __popc(b & ((1u << lane) - 1u));
-    keys[p] = key;
-    vals[p] = j;
-  }
-}
-
-// ctime[d] = replay rank of d's cancellation.
-__global__ void replay_init_kernel(int C, const int* __restrict__ order, const int* __restrict__ dying,
-                                   ReplayState S) {
-  int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= C) return;
-  int d = dying[order[r]];
-  S.ctime[d] = r;
-  S.status[d] = kPending;
-}
-
-// One resolution round over the unresolved cancellations (by replay rank).
-__global__ void __launch_bounds__(256) replay_round_kernel(const int* __restrict__ active, int n_active,
-                                                          const int* __restrict__ order, const int* __restrict__ sweep,
-                                                          const int* __restrict__ dying, const int* __restrict__ c1,
-                                                          const int* __restrict__ c2, const long long* __restrict__ blen,
-                                                          ReplayState S, int max_steps, int* __restrict__ next_active,
-                                                          int* __restrict__ n_next, unsigned* status) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool keep = false;
-  int r = -1;
-  if (i < n_active) {
-    r = active[i];
-    int j = order[r];
-    int d = dying[j], s = sweep[j];
-    int T0 = c1[j], T1 = c2[j];
-    int R0, R1;
-    long long a0, a1;
-    bool ok0 = walk_root(S, T0, r, &R0, &a0, max_steps, status);
-    bool ok1 = ok0 && walk_root(S, T1, r, &R1, &a1, max_steps, status);
-    if (!ok0 || !ok1) {
-      keep = true;
-    } else {
-      int k = -1;
-      if (R0 == d && R0 != R1)
-        k = 0;
-      else if (R1 == d && R0 != R1)
-        k = 1;
-      if (k >= 0) {
-        S.parent[d] = k == 0 ? R1 : R0;
-        S.side[d] = k;
-        S.csad[d] = s;
-        S.cl_dy[d] = k == 0 ? a0 : a1;
-        S.cl_ot[d] = k == 0 ? a1 : a0;
-        S.wlen[d] = blen[2 * s] + blen[2 * s + 1] + a0 + a1;
-        st_release(S.status + d, kLinked);
-      } else {
-        st_release(S.status + d, kRootForever);
+  unsigned long long key = ~0ull;
+  if (j < nsad) {
+    if (dying[j] >= 0) {
+      float p = pers[sweep[j]];
+      if (p <= thr) {
+        take = true;
+        key = ((unsigned long long)orderable_key(p) << 32) | (unsigned)crit_sad[sweep[j]];
       }
     }
+    keys[j] = key;
+    vals[j] = j;
   }
-  unsigned b = __ballot_sync(0xffffffffu, keep);
-  if (b == 0) return;
-  int lane = threadIdx.x & 31, leader = __ffs(b) - 1, base = 0;
-  if (lane == leader) base = atomicAdd(n_next, __popc(b));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (keep) next_active[base + __popc(b & ((1u << lane) - 1u))] = r;
+  unsigned b = __ballot_sync(0xffffffffu, take);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, __popc(b));
 }
 
 // Base arc length in cells: steps + 1 for a valid arc, 0 otherwise
@@ -288,35 +228,6 @@ __device__ void emit_w(const EmitCtx& E, int d, int rev, long long pos) {
     if (lb > 0) emit_base(E, s, k, 0, pos + ld + lc);
     if (la > 0) push_task(E, make_task(kTaskChain, 0, Tk, d, pos + ld + lc + lb));
   }
-}
-
-// Level 0: every surviving arc's own raw arc, then its chain.
-__global__ void emit_roots_kernel(EmitCtx E, int nsurv, const int* __restrict__ surv_sad,
-                                  const long long* __restrict__ arc_pos, const long long* __restrict__ arc_cl,
-                                  const int* __restrict__ arc_root) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= 2 * nsurv) return;
-  int i = q >> 1, j = q & 1;
-  int s = surv_sad[i];
-  int T = E.t[2 * s + j];
-  if (T < 0) return;
-  long long pos = arc_pos[q];
-  long long bl = E.blen[2 * s + j];
-  emit_base(E, s, j, 0, pos);
-  if (arc_cl[q] > 0) push_task(E, make_task(kTaskChain, 0, T, arc_root[q], pos + bl));
-}
-
-__global__ void emit_level_kernel(EmitCtx E, const int4* __restrict__ q_in, int n_in) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_in) return;
-  int4 t = q_in[i];
-  int kind = t.x & 3, rev = (t.x >> 2) & 1;
-  if (kind == kTaskW)
-    emit_w(E, t.y, rev, t.w);
-  else if (kind == kTaskChain)
-    emit_chain(E, t.y, t.z, rev, t.w);
-  else
-    emit_base(E, t.y, t.z, rev, t.w);
 }
 
 }  // namespace dmsc
