@@ -279,6 +279,7 @@ def b200_arm(args):
     time.sleep(0.3)
     stage_sum = {}
     launches = 0
+    loops = []
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -290,6 +291,7 @@ def b200_arm(args):
         for name, v in ctx.stage_times().items():
             stage_sum[name] = stage_sum.get(name, 0.0) + v
         launches += ctx.launch_count()
+        loops.append(ctx.loop_counts())
     e1.record(st)
     torch.cuda.synchronize()
     if dist:
@@ -355,6 +357,7 @@ def b200_arm(args):
                                   "unit": "GB/s", "frac": (seg / peak) if seg else None,
                                   "algorithmic_bytes": seg_bytes, "avg_ms": lab_ms},
         "stage_ms_per_step": {k: v / args.steps for k, v in stage_sum.items()},
+        "device_loops_per_variant": {f"dual={d},thr={t}": loops[k] for k, (d, t) in enumerate(VARIANTS) if k < len(loops)},
         "clocks": clk,
     }
     if world == 1 and not args.no_cpu_baseline:

@@ -26,6 +26,7 @@ EXPORTS = (
     "dmsc_b200_set_profiling",
     "dmsc_b200_stage_times",
     "dmsc_b200_launch_count",
+    "dmsc_b200_loop_counts",
 )
 
 STAGES = ("gradient", "compaction", "saddle_sort", "saddle_walks", "pairing_faces", "pairing_vertices", "survivors",
@@ -83,6 +84,8 @@ def load():
         lib.dmsc_b200_stage_times.restype = ctypes.c_int
         lib.dmsc_b200_launch_count.argtypes = [ctypes.c_void_p]
         lib.dmsc_b200_launch_count.restype = ctypes.c_longlong
+        lib.dmsc_b200_loop_counts.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        lib.dmsc_b200_loop_counts.restype = ctypes.c_int
         _lib = lib
         return lib
 
@@ -117,6 +120,13 @@ class Context:
 
     def launch_count(self) -> int:
         return int(self.lib.dmsc_b200_launch_count(self.h))
+
+    def loop_counts(self) -> dict:
+        buf = (ctypes.c_int * 6)()
+        n = self.lib.dmsc_b200_loop_counts(self.h, buf, 6)
+        names = ("pair_rounds_faces", "pair_rounds_vertices", "replay_rounds_faces", "replay_rounds_vertices",
+                 "emit_levels_faces", "emit_levels_vertices")
+        return {names[k]: int(buf[k]) for k in range(max(n, 0))}
 
     def close(self):
         if getattr(self, "h", None):

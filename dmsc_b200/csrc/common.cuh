@@ -99,6 +99,29 @@ __device__ __forceinline__ float sub_like_host(float a, float b) {
 
 __device__ __forceinline__ void set_status(unsigned* status, unsigned bit) { atomicOr(status, bit); }
 
+// Block-aggregated append: one global atomic per block. Every thread of the
+// block must call it (with blockDim.x a multiple of 32, at most 1024).
+// Returns the slot of this thread's item, or -1 when `take` is false.
+__device__ __forceinline__ int block_append(int* counter, bool take) {
+  __shared__ int wcount[32], wbase[32], bbase;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  unsigned b = __ballot_sync(0xffffffffu, take);
+  if (lane == 0) wcount[warp] = __popc(b);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int w = 0; w < nw; ++w) {
+      wbase[w] = s;
+      s += wcount[w];
+    }
+    bbase = s ? atomicAdd(counter, s) : 0;
+  }
+  __syncthreads();
+  int r = take ? bbase + wbase[warp] + __popc(b & ((1u << lane) - 1u)) : -1;
+  __syncthreads();
+  return r;
+}
+
 inline unsigned grid_for(long long n, int block) {
   long long g = (n + block - 1) / block;
   if (g < 1) g = 1;

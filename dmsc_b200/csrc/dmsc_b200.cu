@@ -35,7 +35,7 @@ namespace {
 enum Slot {
   S_GRAD, S_MASK, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT,
   S_CMIN, S_CSAD, S_CMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA, S_ASC,
-  S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS,
+  S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
@@ -126,6 +126,11 @@ __global__ void totals3_kernel(const int* o0, const int* s0, const int* o1, cons
 template <class T>
 __global__ void last_plus_kernel(const T* excl, const T* val, int n, long long* out) {
   *out = n > 0 ? (long long)excl[n - 1] + (long long)val[n - 1] : 0;
+}
+
+__global__ void copy2_kernel(const int* a, long long* out) {
+  out[0] = a[0];
+  out[1] = a[1];
 }
 
 template <class T>
@@ -312,6 +317,7 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
     A.cell = S.crit;
     A.status = ctx->status;
     A.max_rounds = M + 2;
+    A.rounds = get<int>(ctx, S_STATS, 8) + 0 + si;
     // older = value_less<D'> with D' = dual on the vertex side, !dual on the face side
     const bool older_less = S.faces ? ctx->dual : !ctx->dual;
     if (older_less)
@@ -328,10 +334,12 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
   S.alive = sget<uint8_t>(ctx, si, X_ALIVE, M + 4);
   CK(cudaMemsetAsync(S.alive, 1, M + 4, st));
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
+  int* ncanc = get<int>(ctx, S_NCANC, 4) + si;
+  CK(cudaMemsetAsync(ncanc, 0, sizeof(int), st));
   if (nsad > 0) {
     LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, !S.faces, ctx->dual, ctx->thr, S.sweep, S.dying,
                                                           get<float>(ctx, S_SVAL, nsad), S.val, S.pair_dense, S.pers,
-                                                          canc, (uint8_t)(S.faces ? 1 : 2), S.alive));
+                                                          canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc));
     LAUNCH_CHECK("persistence_kernel");
   }
   // thresholded union-find roots
@@ -370,12 +378,10 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   int* cnt = sget<int>(ctx, si, X_CNT, 4);
   CK(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), st));
   if (nsad > 0)
-    LK(cancel_keys_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->thr, ctx->crit_sad,
-                                                            ckey, cval, cnt + 3));
-  LAUNCH_CHECK("cancel_keys_kernel");
-  // every saddle is sorted; the non-cancelled ones carry the largest key and
-  // land after the C cancellations, so C never needs to reach the host
-  sort_pairs(ctx, ckey, ck2, cval, cord, nsad, st);
+    LK(cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->thr,
+                                                               ctx->crit_sad, ckey, cval, cnt + 3));
+  LAUNCH_CHECK("cancel_collect_kernel");
+  sort_pairs(ctx, ckey, ck2, cval, cord, S.C, st);
 
   ReplayState& R = S.R;
   R.ctime = sget<int>(ctx, si, X_CTIME, M + 1);
@@ -407,6 +413,7 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
     A.cnt = cnt;
     A.status = ctx->status;
     A.max_rounds = nsad + 2;
+    A.rounds = get<int>(ctx, S_STATS, 8) + 2 + si;
     coop_launch(ctx, replay_persistent_kernel, A, st, "replay_persistent_kernel");
   }
   int rounds = 0;
@@ -471,6 +478,7 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   ctx->status = get<unsigned>(ctx, S_STATUS, 4);
   ctx->launches = 0;
   mark(ctx, 0, st);
+  CK(cudaMemsetAsync(get<int>(ctx, S_STATS, 8), 0, 8 * sizeof(int), st));
   CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
 
   // ---- K1 gradient + criticality ----
@@ -585,9 +593,12 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
     excl_sum(ctx, flag, fpos, nsad, st);
     LK(survivor_list_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, V.sweep, flag, fpos, ctx->surv));
     LK(last_plus_kernel<int><<<1, 1, 0, st>>>(fpos, flag, nsad, tot));
+    LK(copy2_kernel<<<1, 1, 0, st>>>(get<int>(ctx, S_NCANC, 4), tot + 1));
     LAUNCH_CHECK("survivors");
-    readback(ctx, st, tot, 1);
+    readback(ctx, st, tot, 3);
     ctx->nsurv = (int)ctx->pinned[0];
+    F.C = (int)ctx->pinned[1];
+    V.C = (int)ctx->pinned[2];
   }
   const int nsurv = ctx->nsurv;
   mark(ctx, 7, st);
@@ -701,6 +712,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   A.q1 = sget<int4>(ctx, si, X_Q1, cap);
   A.cnt = sget<int>(ctx, si, X_CNT, 4);
   A.max_levels = ctx->nsad + 4;
+  A.levels = get<int>(ctx, S_STATS, 8) + 4 + si;
   coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel");
 }
 
@@ -861,5 +873,15 @@ int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n) {
 }
 
 long long dmsc_b200_launch_count(const dmsc_b200_context* ctx) { return ctx ? ctx->launches : -1; }
+
+int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n) {
+  if (!ctx || !out || ctx->bufs.size() <= (size_t)S_STATS || !ctx->bufs[S_STATS].p) return -1;
+  int h[6] = {0};
+  if (cudaSetDevice(ctx->device) != cudaSuccess ||
+      cudaMemcpy(h, ctx->bufs[S_STATS].p, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  for (int k = 0; k < 6 && k < n; ++k) out[k] = h[k];
+  return 6;
+}
 
 }  // extern "C"

@@ -25,7 +25,7 @@
 namespace dmsc {
 
 constexpr int kTileX = 32;  // indices per tile row (one warp)
-constexpr int kTileY = 8;   // tile rows (one warp each)
+constexpr int kTileY = 16;  // tile rows (one warp each)
 constexpr int kValX = kTileX + 3;
 constexpr int kValY = kTileY + 3;
 
@@ -80,17 +80,19 @@ inline void face_fifo_table(uint32_t* out) {
 }
 constexpr int kFifoTable = 16 * 16 * 5;
 
-constexpr int kGradThreads = 320;  // >= (kTileY + 1) * (kTileX + 1) = 297 lower stars per tile
+constexpr int kGradThreads = 576;  // >= (kTileY + 1) * (kTileX + 1) = 561 lower stars per tile
 
-// One pixel value with its linear id; gt() is v_greater (cpu/cell_compare.hxx:23-31):
-// pixels ordered by (value, y*W+x), flipped in the dual.
-struct Px {
-  float v;
-  int id;
-};
+// v_greater (cpu/cell_compare.hxx:23-31) orders pixels by (value, y*W+x),
+// flipped in the dual. gt(a, b) when a's linear id is known to be larger (a "after" b) or smaller:
+// the (value, id) tie rule then reduces to one float compare.
+//   primal: after -> !(a < b), before -> (b < a); dual: after -> (a < b), before -> !(b < a)
 template <bool DUAL>
-__device__ __forceinline__ bool gt(const Px& a, const Px& b) {
-  return value_greater<DUAL>(a.v, a.id, b.v, b.id);
+__device__ __forceinline__ bool gt_after(float a, float b) {
+  return DUAL ? (a < b) : !(a < b);
+}
+template <bool DUAL>
+__device__ __forceinline__ bool gt_before(float a, float b) {
+  return DUAL ? !(b < a) : (b < a);
 }
 
 // Lower star of pixel (y, x) and its pairing (cpu/gradient.hxx:48-192), all in
@@ -105,82 +107,87 @@ __device__ __forceinline__ void lower_star(const float (*sv)[kValX], int y, int 
   // 3x3 neighbourhood; r, c index the value tile (origin y0-2, x0-2)
   const int r = y - (ty0 - 2), c = x - (tx0 - 2);
   const bool lv = x >= 1, rv = x + 1 < W, uv = y >= 1, dv = y + 1 < H;
-  const Px P{sv[r][c], y * W + x};
-  const Px L{sv[r][c - 1], P.id - 1}, R{sv[r][c + 1], P.id + 1};
-  const Px U{sv[r - 1][c], P.id - W}, D{sv[r + 1][c], P.id + W};
-  const Px UL{sv[r - 1][c - 1], P.id - W - 1}, UR{sv[r - 1][c + 1], P.id - W + 1};
-  const Px DL{sv[r + 1][c - 1], P.id + W - 1}, DR{sv[r + 1][c + 1], P.id + W + 1};
+  // row-major linear order of the 3x3 neighbourhood: UL < U < UR < L < P < R < DL < D < DR
+  const float P = sv[r][c];
+  const float L = sv[r][c - 1], R = sv[r][c + 1];
+  const float U = sv[r - 1][c], D = sv[r + 1][c];
+  const float UL = sv[r - 1][c - 1], UR = sv[r - 1][c + 1];
+  const float DL = sv[r + 1][c - 1], DR = sv[r + 1][c + 1];
+#define GT_A(a, b) gt_after<DUAL>(a, b)   /* a after b */
+#define GT_B(a, b) gt_before<DUAL>(a, b)  /* a before b */
 
-  const bool p_gt_l = lv && gt<DUAL>(P, L);
-  const bool r_gt_p = rv && gt<DUAL>(R, P);
-  const bool p_gt_u = uv && gt<DUAL>(P, U);
-  const bool d_gt_p = dv && gt<DUAL>(D, P);
+  const bool p_gt_l = lv && GT_A(P, L);
+  const bool r_gt_p = rv && GT_A(R, P);
+  const bool p_gt_u = uv && GT_A(P, U);
+  const bool d_gt_p = dv && GT_A(D, P);
 
   unsigned eL = 0, fL = 0;
   if (!lv || p_gt_l) eL |= 1u;
   if (!r_gt_p) eL |= 2u;
   if (!uv || p_gt_u) eL |= 4u;
   if (!d_gt_p) eL |= 8u;
-  {  // f0 = F(y,x): scan UL, U, L, then P
-    bool have = false;
-    Px b = P;
+  {  // f0 = F(y,x): scan UL, U, L, then P (each later candidate is after the earlier ones)
+    bool p_top;
     if (uv && lv) {
-      b = UL;
-      have = true;
+      // best of UL, U, L
+      int b = GT_A(U, UL) ? 1 : 0;  // 0 = UL, 1 = U
+      float bv = b ? U : UL;
+      if (GT_A(L, bv)) {
+        bv = L;
+      }
+      p_top = GT_A(P, bv);
+    } else if (uv) {
+      p_top = GT_A(P, U);
+    } else if (lv) {
+      p_top = GT_A(P, L);
+    } else {
+      p_top = true;
     }
-    if (uv) {
-      if (!have || gt<DUAL>(U, b)) b = U;
-      have = true;
-    }
-    if (lv) {
-      if (!have || gt<DUAL>(L, b)) b = L;
-      have = true;
-    }
-    if (!have || gt<DUAL>(P, b)) fL |= 1u;
+    if (p_top) fL |= 1u;
   }
   {  // f1 = F(y,x+1): scan U, UR, P, R
-    bool have = false;
-    Px b = P;
+    bool p_best;
     if (uv) {
-      b = U;
-      have = true;
+      float bv = (rv && GT_A(UR, U)) ? UR : U;  // U, UR both before P
+      p_best = GT_A(P, bv);
+    } else {
+      p_best = true;
     }
-    if (uv && rv) {
-      if (!have || gt<DUAL>(UR, b)) b = UR;
-      have = true;
-    }
-    if ((!have || gt<DUAL>(P, b)) && !r_gt_p) fL |= 2u;
+    if (p_best && !r_gt_p) fL |= 2u;
   }
   {  // f2 = F(y+1,x): scan L, P, DL, D
     bool p_best = !lv || p_gt_l;
-    if (p_best && dv && lv && gt<DUAL>(DL, P)) p_best = false;
+    if (p_best && dv && lv && GT_A(DL, P)) p_best = false;
     if (p_best && d_gt_p) p_best = false;
     if (p_best) fL |= 4u;
   }
   {  // f3 = F(y+1,x+1): scan P, R, D, DR
-    bool p_best = !r_gt_p && !d_gt_p && !(dv && rv && gt<DUAL>(DR, P));
+    bool p_best = !r_gt_p && !d_gt_p && !(dv && rv && GT_A(DR, P));
     if (p_best) fL |= 8u;
   }
 
   // vertex pairing: the lower-star edge whose other vertex is lowest
+  // (candidates visited L, R, U, D; "bo greater than the new one" decides)
   int best = -1;
-  Px bo = P;
+  float bo = 0.0f;
   if ((eL & 1u) && lv) {
     best = 0;
     bo = L;
   }
-  if ((eL & 2u) && rv && (best < 0 || gt<DUAL>(bo, R))) {
+  if ((eL & 2u) && rv && (best < 0 || GT_B(bo, R))) {  // L before R
     best = 1;
     bo = R;
   }
-  if ((eL & 4u) && uv && (best < 0 || gt<DUAL>(bo, U))) {
+  if ((eL & 4u) && uv && (best < 0 || GT_A(bo, U))) {  // L, R after U
     best = 2;
     bo = U;
   }
-  if ((eL & 8u) && dv && (best < 0 || gt<DUAL>(bo, D))) {
+  if ((eL & 8u) && dv && (best < 0 || GT_B(bo, D))) {  // L, R, U before D
     best = 3;
     bo = D;
   }
+#undef GT_A
+#undef GT_B
 
   // face pairing: the FIFO of cpu/gradient.hxx:115-191 depends only on the
   // lower-star masks and the vertex-paired edge, so its result is looked up

@@ -77,27 +77,31 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
                                                           const float* __restrict__ ext_val,
                                                           int* __restrict__ pair_dense, float* __restrict__ pers,
                                                           uint8_t* __restrict__ cancelled, uint8_t sbit,
-                                                          uint8_t* __restrict__ alive) {
+                                                          uint8_t* __restrict__ alive, int* __restrict__ n_cancel) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nsad) return;
-  int s = sweep[j], d = dying[j];
-  if (d < 0) {
-    pair_dense[s] = -1;
-    pers[s] = -1.0f;
-    return;
+  bool canc = false;
+  if (j < nsad) {
+    int s = sweep[j], d = dying[j];
+    if (d < 0) {
+      pair_dense[s] = -1;
+      pers[s] = -1.0f;
+    } else {
+      float sv = sad_val[s], ev = ext_val[d];
+      float p;
+      if (min_side)
+        p = dual ? sub_like_host(ev, sv) : sub_like_host(sv, ev);
+      else
+        p = dual ? sub_like_host(sv, ev) : sub_like_host(ev, sv);
+      pair_dense[s] = d;
+      pers[s] = p;
+      if (p <= thr) {
+        canc = true;
+        atomicOr((unsigned*)(cancelled + (s & ~3)), (unsigned)sbit << (8 * (s & 3)));
+        alive[d] = 0;
+      }
+    }
   }
-  float sv = sad_val[s], ev = ext_val[d];
-  float p;
-  if (min_side)
-    p = dual ? sub_like_host(ev, sv) : sub_like_host(sv, ev);
-  else
-    p = dual ? sub_like_host(sv, ev) : sub_like_host(ev, sv);
-  pair_dense[s] = d;
-  pers[s] = p;
-  if (p <= thr) {
-    atomicOr((unsigned*)(cancelled + (s & ~3)), (unsigned)sbit << (8 * (s & 3)));
-    alive[d] = 0;
-  }
+  block_append(n_cancel, canc);
 }
 
 // Thresholded union-find: lock-free union of the ends of every cancelled

@@ -58,6 +58,7 @@ struct PairArgs {
   const int* cell;
   unsigned* status;
   int max_rounds;
+  int* rounds;  // receives the number of rounds (statistics)
 };
 
 template <bool OLDER_LESS>
@@ -82,7 +83,10 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
   grid.sync();
   for (int r = 0;; ++r) {
     const int n = *(volatile int*)(A.cnt + r % 3);
-    if (n == 0) break;
+    if (n == 0) {
+      if (tid == 0 && A.rounds) *A.rounds = r;
+      break;
+    }
     if (r >= A.max_rounds) {
       if (tid == 0) set_status(A.status, kStatusRoundCap);
       break;
@@ -94,24 +98,29 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
     // phase A: relabel ends; cycles decided; offer to both groups' minimum
     for (long long base = 0; base < n; base += nth) {
       long long i = base + tid;
-      bool keep = false;
-      int e = -1;
+      bool keep = false, ta = false, tb = false;
+      int e = -1, ga = -1, gb = -1;
       if (i < n) {
         e = in[i];
         if (A.dying[e] == kUndecided) {
           int a = A.c1[e], b = A.c2[e];
-          int ga = find_halving(A.link, a < 0 ? M : a), gb = find_halving(A.link, b < 0 ? M : b);
+          ga = find_halving(A.link, a < 0 ? M : a);
+          gb = find_halving(A.link, b < 0 ? M : b);
           if (ga == gb) {
             A.dying[e] = -1;
           } else {
-            if (atomicMin(A.minedge + ga, (unsigned)e) == kNoEdge) A.touched[atomicAdd(A.cnt + 3, 1)] = ga;
-            if (atomicMin(A.minedge + gb, (unsigned)e) == kNoEdge) A.touched[atomicAdd(A.cnt + 3, 1)] = gb;
+            ta = atomicMin(A.minedge + ga, (unsigned)e) == kNoEdge;
+            tb = atomicMin(A.minedge + gb, (unsigned)e) == kNoEdge;
             keep = true;
           }
         }
       }
       int p = warp_append(ocnt, keep);
       if (keep) out[p] = e;
+      int pa = warp_append(A.cnt + 3, ta);
+      if (ta) A.touched[pa] = ga;
+      int pb = warp_append(A.cnt + 3, tb);
+      if (tb) A.touched[pb] = gb;
     }
     grid.sync();
     // phase B1: every touched group decides on its first outgoing saddle
@@ -157,6 +166,7 @@ struct ReplayArgs {
   int* cnt;  // [0..2]
   unsigned* status;
   int max_rounds;
+  int* rounds;
 };
 
 __global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs A) {
@@ -177,7 +187,10 @@ __global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs A) {
   grid.sync();
   for (int rd = 0;; ++rd) {
     const int n = *(volatile int*)(A.cnt + rd % 3);
-    if (n == 0) break;
+    if (n == 0) {
+      if (tid == 0 && A.rounds) *A.rounds = rd;
+      break;
+    }
     if (rd >= A.max_rounds) {
       if (tid == 0) set_status(A.status, kStatusRoundCap);
       break;
@@ -241,6 +254,7 @@ struct EmitArgs {
   int4* q1;
   int* cnt;  // [0..2]
   int max_levels;
+  int* levels;  // receives the number of levels (statistics)
 };
 
 __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
@@ -256,18 +270,37 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
   // level 0: each surviving arc's own raw arc, then its chain
   E.q_out = A.q0;
   E.n_out = A.cnt;
-  for (long long q = tid; q < 2LL * A.nsurv; q += nth) {
-    int i = (int)(q >> 1), j = (int)(q & 1);
-    int s = A.surv_sad[i];
-    if (E.t[2 * s + j] < 0) continue;
-    long long pos = A.arc_pos[q];
-    emit_base(E, s, j, 0, pos);
-    if (A.arc_cl[q] > 0) push_task(E, make_task(kTaskChain, 0, E.t[2 * s + j], A.arc_root[q], pos + E.blen[2 * s + j]));
+  for (long long base = 0; base < 2LL * A.nsurv; base += nth) {
+    long long q = base + tid;
+    bool push = false;
+    int4 task = make_int4(0, 0, 0, 0);
+    if (q < 2LL * A.nsurv) {
+      int i = (int)(q >> 1), j = (int)(q & 1);
+      int s = A.surv_sad[i];
+      if (E.t[2 * s + j] >= 0) {
+        long long pos = A.arc_pos[q];
+        emit_base(E, s, j, 0, pos);
+        if (A.arc_cl[q] > 0) {
+          push = true;
+          task = make_task(kTaskChain, 0, E.t[2 * s + j], A.arc_root[q], pos + E.blen[2 * s + j]);
+        }
+      }
+    }
+    int p = warp_append(A.cnt, push);
+    if (push) {
+      if (p < E.q_cap)
+        A.q0[p] = task;
+      else
+        set_status(E.status, kStatusQueueOverflow);
+    }
   }
   grid.sync();
   for (int lv = 0;; ++lv) {
     int n = *(volatile int*)(A.cnt + lv % 3);
-    if (n == 0) break;
+    if (n == 0) {
+      if (tid == 0 && A.levels) *A.levels = lv;
+      break;
+    }
     if (lv >= A.max_levels || n > E.q_cap) {
       if (tid == 0) set_status(E.status, kStatusQueueOverflow);
       break;

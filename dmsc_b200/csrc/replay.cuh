@@ -77,31 +77,31 @@ __device__ __forceinline__ bool walk_root(const ReplayState& S, int x, int t, in
   return true;
 }
 
-// Sort keys of one side's saddles in sweep order: a cancelled saddle gets
-// (persistence, saddle cell) -- CancelEvent::operator<
-// (cpu/persistence_struct.hxx:16-21); a saddle is cancelled at most once per
-// side, so this pair is unique -- and every other saddle the largest key, so
-// the C cancellations come first after sorting. `count` receives C.
-__global__ void cancel_keys_kernel(int nsad, const int* __restrict__ sweep, const int* __restrict__ dying,
-                                   const float* __restrict__ pers, float thr, const int* __restrict__ crit_sad,
-                                   unsigned long long* __restrict__ keys, int* __restrict__ vals,
-                                   int* __restrict__ count) {
+// Cancellations of one side, compacted in any order with their sort keys
+// (CancelEvent::operator<, cpu/persistence_struct.hxx:16-21): (persistence,
+// saddle cell); a saddle is cancelled at most once per side, so the pair is
+// unique and the target cell never breaks a tie.
+__global__ void __launch_bounds__(256) cancel_collect_kernel(int nsad, const int* __restrict__ sweep,
+                                                             const int* __restrict__ dying,
+                                                             const float* __restrict__ pers, float thr,
+                                                             const int* __restrict__ crit_sad,
+                                                             unsigned long long* __restrict__ keys,
+                                                             int* __restrict__ vals, int* __restrict__ count) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   bool take = false;
-  unsigned long long key = ~0ull;
-  if (j < nsad) {
-    if (dying[j] >= 0) {
-      float p = pers[sweep[j]];
-      if (p <= thr) {
-        take = true;
-        key = ((unsigned long long)orderable_key(p) << 32) | (unsigned)crit_sad[sweep[j]];
-      }
+  unsigned long long key = 0;
+  if (j < nsad && dying[j] >= 0) {
+    float p = pers[sweep[j]];
+    if (p <= thr) {
+      take = true;
+      key = ((unsigned long long)orderable_key(p) << 32) | (unsigned)crit_sad[sweep[j]];
     }
-    keys[j] = key;
-    vals[j] = j;
   }
-  unsigned b = __ballot_sync(0xffffffffu, take);
-  if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, __popc(b));
+  int pos = block_append(count, take);
+  if (take) {
+    keys[pos] = key;
+    vals[pos] = j;
+  }
 }
 
 // Base arc length in cells: steps + 1 for a valid arc, 0 otherwise
@@ -187,27 +187,36 @@ __device__ void emit_base(const EmitCtx& E, int s, int j, int rev, long long pos
   }
 }
 
+// Reserves `k` consecutive queue slots with one atomic.
+__device__ __forceinline__ int reserve_tasks(const EmitCtx& E, int k) {
+  int p = atomicAdd(E.n_out, k);
+  if (p + (long long)k > E.q_cap) {
+    set_status(E.status, kStatusQueueOverflow);
+    return -1;
+  }
+  return p;
+}
+
 __device__ void emit_chain(const EmitCtx& E, int x, int stop, int rev, long long pos) {
   long long total = 0;
-  if (rev) {
-    int z = x, steps = 0;
-    while (z != stop && z >= 0) {
-      total += E.S.wlen[z];
-      z = E.S.parent[z];
-      if (++steps > E.max_steps) break;
+  int k = 0, z = x;
+  while (z != stop && z >= 0) {
+    total += E.S.wlen[z];
+    z = E.S.parent[z];
+    if (++k > E.max_steps) {
+      set_status(E.status, kStatusChainCap);
+      return;
     }
   }
-  long long p = 0;
-  int z = x, steps = 0;
-  while (z != stop && z >= 0) {
+  int p = reserve_tasks(E, k);
+  if (p < 0) return;
+  long long off = 0;
+  z = x;
+  for (int i = 0; i < k; ++i) {
     long long w = E.S.wlen[z];
-    push_task(E, make_task(kTaskW, rev, z, 0, rev ? pos + total - p - w : pos + p));
-    p += w;
+    E.q_out[p + i] = make_task(kTaskW, rev, z, 0, rev ? pos + total - off - w : pos + off);
+    off += w;
     z = E.S.parent[z];
-    if (++steps > E.max_steps) {
-      set_status(E.status, kStatusChainCap);
-      break;
-    }
   }
 }
 
@@ -216,17 +225,20 @@ __device__ void emit_w(const EmitCtx& E, int d, int rev, long long pos) {
   int Tk = E.t[2 * s + k], To = E.t[2 * s + o];
   long long la = E.S.cl_dy[d], lb = E.blen[2 * s + k], lc = E.blen[2 * s + o], ld = E.S.cl_ot[d];
   int R = E.S.parent[d];
+  int nq = (la > 0) + (ld > 0);
+  int p = nq ? reserve_tasks(E, nq) : 0;
+  if (p < 0) return;
   if (!rev) {
     // reverse(chain(Tk -> d)) + reverse(arc k) + arc o + chain(To -> R)
-    if (la > 0) push_task(E, make_task(kTaskChain, 1, Tk, d, pos));
+    if (la > 0) E.q_out[p++] = make_task(kTaskChain, 1, Tk, d, pos);
     if (lb > 0) emit_base(E, s, k, 1, pos + la);
     if (lc > 0) emit_base(E, s, o, 0, pos + la + lb);
-    if (ld > 0) push_task(E, make_task(kTaskChain, 0, To, R, pos + la + lb + lc));
+    if (ld > 0) E.q_out[p++] = make_task(kTaskChain, 0, To, R, pos + la + lb + lc);
   } else {
-    if (ld > 0) push_task(E, make_task(kTaskChain, 1, To, R, pos));
+    if (ld > 0) E.q_out[p++] = make_task(kTaskChain, 1, To, R, pos);
     if (lc > 0) emit_base(E, s, o, 1, pos + ld);
     if (lb > 0) emit_base(E, s, k, 0, pos + ld + lc);
-    if (la > 0) push_task(E, make_task(kTaskChain, 0, Tk, d, pos + ld + lc + lb));
+    if (la > 0) E.q_out[p++] = make_task(kTaskChain, 0, Tk, d, pos + ld + lc + lb);
   }
 }
 

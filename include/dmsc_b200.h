@@ -130,6 +130,11 @@ int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n);
    sort call counts once). */
 long long dmsc_b200_launch_count(const dmsc_b200_context* ctx);
 
+/* Device loop counts of the last call (host pointer, up to `n` values):
+   pairing rounds (faces, vertices), replay rounds (faces, vertices), geometry
+   expansion levels (faces, vertices). Returns the number written or -1. */
+int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n);
+
 #ifdef __cplusplus
 }
 #endif
