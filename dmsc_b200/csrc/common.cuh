@@ -99,6 +99,35 @@ __device__ __forceinline__ float sub_like_host(float a, float b) {
 
 __device__ __forceinline__ void set_status(unsigned* status, unsigned bit) { atomicOr(status, bit); }
 
+// Block-aggregated reservation of `cnt` consecutive slots per thread: one
+// global atomic per block. Every thread of the block must call it (blockDim.x
+// a multiple of 32, at most 1024). Returns this thread's first slot.
+__device__ __forceinline__ int block_reserve(int* counter, int cnt) {
+  __shared__ int wsum[32], bbase_r;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int x = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int w = 0; w < nw; ++w) {
+      int t = wsum[w];
+      wsum[w] = s;
+      s += t;
+    }
+    bbase_r = s ? atomicAdd(counter, s) : 0;
+  }
+  __syncthreads();
+  int r = bbase_r + wsum[warp] + x - cnt;
+  __syncthreads();
+  return r;
+}
+
 // Block-aggregated append: one global atomic per block. Every thread of the
 // block must call it (with blockDim.x a multiple of 32, at most 1024).
 // Returns the slot of this thread's item, or -1 when `take` is false.

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
     if (tid == 0) A.cnt[(r + 2) % 3] = 0;
     // phase A: relabel ends; cycles decided; offer to both groups' minimum
     for (long long base = 0; base < n; base += nth) {
-      long long i = base + tid;
+      long long i = base + tid;  // block-uniform trip count (tid = block offset + threadIdx.x)
       bool keep = false, ta = false, tb = false;
       int e = -1, ga = -1, gb = -1;
       if (i < n) {
@@ -115,12 +115,11 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
           }
         }
       }
-      int p = warp_append(ocnt, keep);
+      int p = block_reserve(ocnt, keep ? 1 : 0);
       if (keep) out[p] = e;
-      int pa = warp_append(A.cnt + 3, ta);
-      if (ta) A.touched[pa] = ga;
-      int pb = warp_append(A.cnt + 3, tb);
-      if (tb) A.touched[pb] = gb;
+      int pt = block_reserve(A.cnt + 3, (ta ? 1 : 0) + (tb ? 1 : 0));
+      if (ta) A.touched[pt++] = ga;
+      if (tb) A.touched[pt] = gb;
     }
     grid.sync();
     // phase B1: every touched group decides on its first outgoing saddle
@@ -233,7 +232,7 @@ __global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs A) {
           }
         }
       }
-      int p = warp_append(ocnt, keep);
+      int p = block_reserve(ocnt, keep ? 1 : 0);
       if (keep) out[p] = r;
     }
     grid.sync();
@@ -286,7 +285,7 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
         }
       }
     }
-    int p = warp_append(A.cnt, push);
+    int p = block_reserve(A.cnt, push ? 1 : 0);
     if (push) {
       if (p < E.q_cap)
         A.q0[p] = task;
@@ -309,14 +308,29 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
     E.q_out = (lv & 1) ? A.q0 : A.q1;
     E.n_out = A.cnt + (lv + 1) % 3;
     if (tid == 0) A.cnt[(lv + 2) % 3] = 0;
-    for (long long i = tid; i < n; i += nth) {
-      int4 t = in[i];
-      int kind = t.x & 3, rev = (t.x >> 2) & 1;
+    for (long long base = 0; base < n; base += nth) {
+      long long i = base + tid;
+      int4 t = make_int4(-1, 0, 0, 0);
+      int kind = -1, rev = 0, need = 0;
+      long long total = 0;
+      if (i < n) {
+        t = in[i];
+        kind = t.x & 3;
+        rev = (t.x >> 2) & 1;
+        if (kind == kTaskW) need = w_task_count(E, t.y);
+        else if (kind == kTaskChain) need = chain_task_count(E, t.y, t.z, &total);
+      }
+      int p = block_reserve(E.n_out, need);
+      if (p + (long long)need > E.q_cap) {
+        set_status(E.status, kStatusQueueOverflow);
+        need = 0;
+        kind = -1;
+      }
       if (kind == kTaskW)
-        emit_w(E, t.y, rev, t.w);
+        emit_w(E, t.y, rev, t.w, p);
       else if (kind == kTaskChain)
-        emit_chain(E, t.y, t.z, rev, t.w);
-      else
+        emit_chain(E, t.y, t.z, rev, t.w, need, total, p);
+      else if (kind == kTaskBase)
         emit_base(E, t.y, t.z, rev, t.w);
     }
     grid.sync();

@@ -164,14 +164,6 @@ struct EmitCtx {
   unsigned* status;
 };
 
-__device__ __forceinline__ void push_task(const EmitCtx& E, int4 task) {
-  int p = atomicAdd(E.n_out, 1);
-  if (p < E.q_cap)
-    E.q_out[p] = task;
-  else
-    set_status(E.status, kStatusQueueOverflow);
-}
-
 // Writes raw arc (s, j): the V-path from its start cell, `len` cells.
 __device__ void emit_base(const EmitCtx& E, int s, int j, int rev, long long pos) {
   long long len = E.blen[2 * s + j];
@@ -187,31 +179,29 @@ __device__ void emit_base(const EmitCtx& E, int s, int j, int rev, long long pos
   }
 }
 
-// Reserves `k` consecutive queue slots with one atomic.
-__device__ __forceinline__ int reserve_tasks(const EmitCtx& E, int k) {
-  int p = atomicAdd(E.n_out, k);
-  if (p + (long long)k > E.q_cap) {
-    set_status(E.status, kStatusQueueOverflow);
-    return -1;
-  }
-  return p;
-}
-
-__device__ void emit_chain(const EmitCtx& E, int x, int stop, int rev, long long pos) {
-  long long total = 0;
+// Number of W tasks of chain(x -> stop) and its total length; the chain is
+// walked once here and once when written.
+__device__ __forceinline__ int chain_task_count(const EmitCtx& E, int x, int stop, long long* total) {
+  long long tot = 0;
   int k = 0, z = x;
   while (z != stop && z >= 0) {
-    total += E.S.wlen[z];
+    tot += E.S.wlen[z];
     z = E.S.parent[z];
     if (++k > E.max_steps) {
       set_status(E.status, kStatusChainCap);
-      return;
+      *total = 0;
+      return 0;
     }
   }
-  int p = reserve_tasks(E, k);
-  if (p < 0) return;
+  *total = tot;
+  return k;
+}
+
+// Writes the k W tasks of chain(x -> stop) into queue slots p .. p+k-1.
+__device__ void emit_chain(const EmitCtx& E, int x, int stop, int rev, long long pos, int k, long long total,
+                           int p) {
   long long off = 0;
-  z = x;
+  int z = x;
   for (int i = 0; i < k; ++i) {
     long long w = E.S.wlen[z];
     E.q_out[p + i] = make_task(kTaskW, rev, z, 0, rev ? pos + total - off - w : pos + off);
@@ -220,14 +210,17 @@ __device__ void emit_chain(const EmitCtx& E, int x, int stop, int rev, long long
   }
 }
 
-__device__ void emit_w(const EmitCtx& E, int d, int rev, long long pos) {
+// Number of chain tasks W(d) produces (its two chains, when non-empty).
+__device__ __forceinline__ int w_task_count(const EmitCtx& E, int d) {
+  return (E.S.cl_dy[d] > 0) + (E.S.cl_ot[d] > 0);
+}
+
+// Expands W(d): writes its two raw arcs and queues its two chains at slot p.
+__device__ void emit_w(const EmitCtx& E, int d, int rev, long long pos, int p) {
   int k = E.S.side[d], o = 1 - k, s = E.S.csad[d];
   int Tk = E.t[2 * s + k], To = E.t[2 * s + o];
   long long la = E.S.cl_dy[d], lb = E.blen[2 * s + k], lc = E.blen[2 * s + o], ld = E.S.cl_ot[d];
   int R = E.S.parent[d];
-  int nq = (la > 0) + (ld > 0);
-  int p = nq ? reserve_tasks(E, nq) : 0;
-  if (p < 0) return;
   if (!rev) {
     // reverse(chain(Tk -> d)) + reverse(arc k) + arc o + chain(To -> R)
     if (la > 0) E.q_out[p++] = make_task(kTaskChain, 1, Tk, d, pos);
