@@ -27,6 +27,7 @@ EXPORTS = (
     "dmsc_b200_stage_times",
     "dmsc_b200_launch_count",
     "dmsc_b200_loop_counts",
+    "dmsc_b200_pairing_timeline",
 )
 
 STAGES = ("gradient", "compaction", "saddle_sort", "saddle_walks", "pairing_faces", "pairing_vertices", "survivors",
@@ -86,6 +87,8 @@ def load():
         lib.dmsc_b200_launch_count.restype = ctypes.c_longlong
         lib.dmsc_b200_loop_counts.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         lib.dmsc_b200_loop_counts.restype = ctypes.c_int
+        lib.dmsc_b200_pairing_timeline.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+        lib.dmsc_b200_pairing_timeline.restype = ctypes.c_int
         _lib = lib
         return lib
 
@@ -127,6 +130,18 @@ class Context:
         names = ("pair_rounds_faces", "pair_rounds_vertices", "replay_rounds_faces", "replay_rounds_vertices",
                  "emit_levels_faces", "emit_levels_vertices")
         return {names[k]: int(buf[k]) for k in range(max(n, 0))}
+
+    def pairing_timeline(self) -> tuple:
+        """Per-round durations (us) of the pairing loops of the last call: (faces, vertices)."""
+        buf = (ctypes.c_longlong * 128)()
+        if self.lib.dmsc_b200_pairing_timeline(self.h, buf, 128) < 0:
+            return (), ()
+        out = []
+        for side in range(2):
+            t = [buf[side * 64 + k] for k in range(64)]
+            t = [x for x in t if x > 0]
+            out.append(tuple((b - a) / 1000.0 for a, b in zip(t, t[1:])))
+        return tuple(out)
 
     def close(self):
         if getattr(self, "h", None):

@@ -35,7 +35,7 @@ namespace {
 enum Slot {
   S_GRAD, S_MASK, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT,
   S_CMIN, S_CSAD, S_CMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA, S_ASC,
-  S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS,
+  S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
@@ -241,8 +241,8 @@ void mark(dmsc_b200_context* ctx, int k, cudaStream_t st) {
   if (ctx->profile) CK(cudaEventRecord(ctx->ev[k], st));
 }
 
-// Cooperative launch of a persistent kernel: all blocks co-resident (at most
-// 4 per SM), so grid-wide barriers are safe.
+// Cooperative launch of a persistent kernel: as many blocks as can be
+// co-resident, so grid-wide barriers are safe.
 template <class T>
 void coop_launch(dmsc_b200_context* ctx, void (*kernel)(T), T args, cudaStream_t st, const char* name) {
   int per = 0;
@@ -251,7 +251,6 @@ void coop_launch(dmsc_b200_context* ctx, void (*kernel)(T), T args, cudaStream_t
     set_err(ctx, "%s cannot be made resident", name);
     throw Fail{kErrInternal};
   }
-  if (per > 4) per = 4;
   void* a[] = {&args};
   CK(cudaLaunchCooperativeKernel((void*)kernel, dim3(per * ctx->num_sms), dim3(256), a, 0, st));
   ++ctx->launches;
@@ -294,7 +293,7 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
   int* link = sget<int>(ctx, si, X_LINK, M + 1);
   unsigned* minedge = sget<unsigned>(ctx, si, X_MINE, M + 1);
   int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
-  int* cnt = sget<int>(ctx, si, X_CNT, 4);
+  int* cnt = sget<int>(ctx, si, X_CNT, 8);
   if (nsad > 0) {
     LK(sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, reverse, S.t, S.sweep, S.c1, S.c2, S.dying));
     LAUNCH_CHECK("sweep_edges_kernel");
@@ -310,7 +309,8 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
     A.minedge = minedge;
     A.act0 = act[0];
     A.act1 = act[1];
-    A.touched = grp;  // reuses the group buffer: [M+1]
+    A.roots0 = grp;  // [M+1]
+    A.roots1 = sget<int>(ctx, si, X_UF, M + 1);
     A.hdec = sget<int>(ctx, si, X_CROOT, M + 1);
     A.cnt = cnt;
     A.val = S.val;
@@ -318,6 +318,7 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
     A.status = ctx->status;
     A.max_rounds = M + 2;
     A.rounds = get<int>(ctx, S_STATS, 8) + 0 + si;
+    A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 2 * kTimeline) + si * kTimeline;
     // older = value_less<D'> with D' = dual on the vertex side, !dual on the face side
     const bool older_less = S.faces ? ctx->dual : !ctx->dual;
     if (older_less)
@@ -375,7 +376,7 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   unsigned long long* ck2 = sget<unsigned long long>(ctx, si, X_CKEY2, nsad);
   int* cval = sget<int>(ctx, si, X_CVAL, nsad);
   int* cord = sget<int>(ctx, si, X_CORD, nsad);
-  int* cnt = sget<int>(ctx, si, X_CNT, 4);
+  int* cnt = sget<int>(ctx, si, X_CNT, 8);
   CK(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), st));
   if (nsad > 0)
     LK(cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->thr,
@@ -479,6 +480,8 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   ctx->launches = 0;
   mark(ctx, 0, st);
   CK(cudaMemsetAsync(get<int>(ctx, S_STATS, 8), 0, 8 * sizeof(int), st));
+  CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, 2 * kTimeline), 0,
+                     2 * kTimeline * sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
 
   // ---- K1 gradient + criticality ----
@@ -710,7 +713,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   A.arc_root = S.arc_root;
   A.q0 = sget<int4>(ctx, si, X_Q0, cap);
   A.q1 = sget<int4>(ctx, si, X_Q1, cap);
-  A.cnt = sget<int>(ctx, si, X_CNT, 4);
+  A.cnt = sget<int>(ctx, si, X_CNT, 8);
   A.max_levels = ctx->nsad + 4;
   A.levels = get<int>(ctx, S_STATS, 8) + 4 + si;
   coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel");
@@ -873,6 +876,15 @@ int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n) {
 }
 
 long long dmsc_b200_launch_count(const dmsc_b200_context* ctx) { return ctx ? ctx->launches : -1; }
+
+int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n) {
+  if (!ctx || !out || ctx->bufs.size() <= (size_t)S_TIMELINE || !ctx->bufs[S_TIMELINE].p) return -1;
+  int k = n < 2 * kTimeline ? n : 2 * kTimeline;
+  if (cudaSetDevice(ctx->device) != cudaSuccess ||
+      cudaMemcpy(out, ctx->bufs[S_TIMELINE].p, k * sizeof(long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  return k;
+}
 
 int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n) {
   if (!ctx || !out || ctx->bufs.size() <= (size_t)S_STATS || !ctx->bufs[S_STATS].p) return -1;

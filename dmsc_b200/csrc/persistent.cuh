@@ -20,6 +20,13 @@ namespace dmsc {
 
 namespace cg = cooperative_groups;
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+constexpr int kTimeline = 64;  // timestamps kept per loop (round starts)
+
 __device__ __forceinline__ int find_halving(int* link, int x) {
   while (true) {
     int p = link[x];
@@ -49,18 +56,27 @@ struct PairArgs {
   int* dying;
   int* link;          // [M+1] group union-find
   unsigned* minedge;  // [M+1]
-  int* act0;
+  int* act0;          // active saddles (ping-pong)
   int* act1;
-  int* touched;  // [M+1]
-  int* hdec;     // [M+1]
-  int* cnt;      // [0..2] rotating active counts, [3] touched count
+  int* roots0;        // live group roots (ping-pong), [M+1] each
+  int* roots1;
+  int* hdec;          // [M+1] decision per root-list slot
+  int* cnt;           // [0..2] rotating active counts, [3..5] rotating root counts
   const float* val;
   const int* cell;
   unsigned* status;
   int max_rounds;
-  int* rounds;  // receives the number of rounds (statistics)
+  int* rounds;                   // receives the number of rounds (statistics)
+  unsigned long long* timeline;  // [kTimeline] round start times (ns), optional
 };
 
+// One side's persistence pairing. Per round: (A) every active saddle finds its
+// ends' groups, cycles are decided, the rest reduce their sweep index into
+// both groups' minimum (no returned value needed) and stay active; (B1) every
+// live root with an outgoing saddle decides whether it dies there and stays
+// live otherwise; roots without outgoing saddles leave the list for good;
+// (B2) the links are applied. Round 0 skips the lookups: all groups are
+// single extrema.
 template <bool OLDER_LESS>
 __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
   cg::grid_group grid = cg::this_grid();
@@ -69,6 +85,7 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
   for (long long i = tid; i <= M; i += nth) {
     A.link[i] = (int)i;
     A.minedge[i] = kNoEdge;
+    A.roots0[i] = (int)i;
   }
   for (long long i = tid; i < A.nsad; i += nth) {
     A.act0[i] = (int)i;
@@ -78,11 +95,15 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
     A.cnt[0] = A.nsad;
     A.cnt[1] = 0;
     A.cnt[2] = 0;
-    A.cnt[3] = 0;
+    A.cnt[3] = M + 1;
+    A.cnt[4] = 0;
+    A.cnt[5] = 0;
   }
   grid.sync();
   for (int r = 0;; ++r) {
     const int n = *(volatile int*)(A.cnt + r % 3);
+    const int nr = *(volatile int*)(A.cnt + 3 + r % 3);
+    if (tid == 0 && A.timeline && r < kTimeline) A.timeline[r] = global_ns();
     if (n == 0) {
       if (tid == 0 && A.rounds) *A.rounds = r;
       break;
@@ -93,56 +114,72 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
     }
     const int* in = (r & 1) ? A.act1 : A.act0;
     int* out = (r & 1) ? A.act0 : A.act1;
+    const int* rin = (r & 1) ? A.roots1 : A.roots0;
+    int* rout = (r & 1) ? A.roots0 : A.roots1;
     int* ocnt = A.cnt + (r + 1) % 3;
-    if (tid == 0) A.cnt[(r + 2) % 3] = 0;
-    // phase A: relabel ends; cycles decided; offer to both groups' minimum
+    int* rcnt = A.cnt + 3 + (r + 1) % 3;
+    if (tid == 0) {
+      A.cnt[(r + 2) % 3] = 0;
+      A.cnt[3 + (r + 2) % 3] = 0;
+    }
+    // phase A (block-uniform trip count: tid = block offset + threadIdx.x)
     for (long long base = 0; base < n; base += nth) {
-      long long i = base + tid;  // block-uniform trip count (tid = block offset + threadIdx.x)
-      bool keep = false, ta = false, tb = false;
-      int e = -1, ga = -1, gb = -1;
+      long long i = base + tid;
+      bool keep = false;
+      int e = -1;
       if (i < n) {
         e = in[i];
-        if (A.dying[e] == kUndecided) {
+        if (r == 0 || A.dying[e] == kUndecided) {
           int a = A.c1[e], b = A.c2[e];
-          ga = find_halving(A.link, a < 0 ? M : a);
-          gb = find_halving(A.link, b < 0 ? M : b);
+          a = a < 0 ? M : a;
+          b = b < 0 ? M : b;
+          int ga = r == 0 ? a : find_halving(A.link, a);
+          int gb = r == 0 ? b : find_halving(A.link, b);
           if (ga == gb) {
             A.dying[e] = -1;
           } else {
-            ta = atomicMin(A.minedge + ga, (unsigned)e) == kNoEdge;
-            tb = atomicMin(A.minedge + gb, (unsigned)e) == kNoEdge;
+            atomicMin(A.minedge + ga, (unsigned)e);  // result unused: a reduction
+            atomicMin(A.minedge + gb, (unsigned)e);
             keep = true;
           }
         }
       }
       int p = block_reserve(ocnt, keep ? 1 : 0);
       if (keep) out[p] = e;
-      int pt = block_reserve(A.cnt + 3, (ta ? 1 : 0) + (tb ? 1 : 0));
-      if (ta) A.touched[pt++] = ga;
-      if (tb) A.touched[pt] = gb;
     }
     grid.sync();
-    // phase B1: every touched group decides on its first outgoing saddle
-    const int nt = *(volatile int*)(A.cnt + 3);
-    for (long long k = tid; k < nt; k += nth) {
-      int g = A.touched[k];
-      int e = (int)A.minedge[g];
-      A.minedge[g] = kNoEdge;
-      int a = A.c1[e], b = A.c2[e];
-      int ga = find_halving(A.link, a < 0 ? M : a), gb = find_halving(A.link, b < 0 ? M : b);
-      int h = (ga == g) ? gb : ga;
-      if (older<OLDER_LESS>(h, g, M, A.val, A.cell)) {
+    // phase B1: live roots decide on their first outgoing saddle
+    for (long long base = 0; base < nr; base += nth) {
+      long long k = base + tid;
+      bool live = false;
+      int g = -1, h = -1;
+      if (k < nr) {
+        g = rin[k];
+        unsigned me = A.minedge[g];
+        if (me != kNoEdge) {
+          A.minedge[g] = kNoEdge;
+          int e = (int)me;
+          int a = A.c1[e], b = A.c2[e];
+          int ga = find_halving(A.link, a < 0 ? M : a), gb = find_halving(A.link, b < 0 ? M : b);
+          h = (ga == g) ? gb : ga;
+          if (older<OLDER_LESS>(h, g, M, A.val, A.cell)) {
+            A.dying[e] = g;
+          } else {
+            h = -1;
+            live = true;
+          }
+        }
         A.hdec[k] = h;
-        A.dying[e] = g;
-      } else {
-        A.hdec[k] = -1;
       }
+      int p = block_reserve(rcnt, live ? 1 : 0);
+      if (live) rout[p] = g;
     }
     grid.sync();
     // phase B2: apply the links
-    for (long long k = tid; k < nt; k += nth)
-      if (A.hdec[k] >= 0) A.link[A.touched[k]] = A.hdec[k];
-    if (tid == 0) A.cnt[3] = 0;
+    for (long long k = tid; k < nr; k += nth) {
+      int h = A.hdec[k];
+      if (h >= 0) A.link[rin[k]] = h;
+    }
     grid.sync();
   }
 }

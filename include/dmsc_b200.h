@@ -135,6 +135,11 @@ long long dmsc_b200_launch_count(const dmsc_b200_context* ctx);
    expansion levels (faces, vertices). Returns the number written or -1. */
 int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n);
 
+/* Start times (ns, device global timer) of the pairing rounds of the last
+   call: 64 slots for the faces, then 64 for the vertices; unused slots are 0.
+   Writes up to `n` values to `out` (host pointer), returns the number written. */
+int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n);
+
 #ifdef __cplusplus
 }
 #endif
