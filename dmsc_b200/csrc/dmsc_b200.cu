@@ -40,9 +40,9 @@ enum Slot {
 };
 enum SideSlot {
   X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
-  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CKEY2, X_CVAL, X_CORD, X_CTIME, X_STAT,
+  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_CTIME, X_STAT,
   X_PAR, X_WLEN, X_SIDE, X_CSAD, X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC,
-  X_EROWO, X_Q0, X_Q1, kSideSlots
+  X_EROWO, X_Q0, X_Q1, X_QB, kSideSlots
 };
 
 struct Buf {
@@ -373,19 +373,16 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   S.blen = sget<long long>(ctx, si, X_BLEN, 2 * (size_t)nsad);
   if (nsad > 0) LK(base_len_kernel<<<grid_for(2LL * nsad, TB), TB, 0, st>>>(2 * nsad, S.t, S.steps, S.blen));
   unsigned long long* ckey = sget<unsigned long long>(ctx, si, X_CKEY, nsad);
-  unsigned long long* ck2 = sget<unsigned long long>(ctx, si, X_CKEY2, nsad);
   int* cval = sget<int>(ctx, si, X_CVAL, nsad);
-  int* cord = sget<int>(ctx, si, X_CORD, nsad);
   int* cnt = sget<int>(ctx, si, X_CNT, 8);
   CK(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), st));
   if (nsad > 0)
     LK(cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->thr,
                                                                ctx->crit_sad, ckey, cval, cnt + 3));
   LAUNCH_CHECK("cancel_collect_kernel");
-  sort_pairs(ctx, ckey, ck2, cval, cord, S.C, st);
 
   ReplayState& R = S.R;
-  R.ctime = sget<int>(ctx, si, X_CTIME, M + 1);
+  R.ctime = sget<unsigned long long>(ctx, si, X_CTIME, M + 1);
   R.status = sget<int>(ctx, si, X_STAT, M + 1);
   R.parent = sget<int>(ctx, si, X_PAR, M + 1);
   R.wlen = sget<long long>(ctx, si, X_WLEN, M + 1);
@@ -393,7 +390,7 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   R.csad = sget<int>(ctx, si, X_CSAD, M + 1);
   R.cl_dy = sget<long long>(ctx, si, X_CLDY, M + 1);
   R.cl_ot = sget<long long>(ctx, si, X_CLOT, M + 1);
-  LK(fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.ctime, M + 1, kNever));
+  LK(fill_u64_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.ctime, M + 1, kNever));
   LK(fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.status, M + 1, kRootForever));
   LAUNCH_CHECK("replay init");
   int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
@@ -401,7 +398,8 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   {
     ReplayArgs A;
     A.n_cancel = cnt + 3;
-    A.order = cord;
+    A.key = ckey;
+    A.cj = cval;
     A.sweep = S.sweep;
     A.dying = S.dying;
     A.c1 = S.c1;
@@ -714,6 +712,9 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   A.q0 = sget<int4>(ctx, si, X_Q0, cap);
   A.q1 = sget<int4>(ctx, si, X_Q1, cap);
   A.cnt = sget<int>(ctx, si, X_CNT, 8);
+  E.base_q = sget<int4>(ctx, si, X_QB, cap);
+  E.base_cap = cap;
+  E.n_base = nullptr;
   A.max_levels = ctx->nsad + 4;
   A.levels = get<int>(ctx, S_STATS, 8) + 4 + si;
   coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel");

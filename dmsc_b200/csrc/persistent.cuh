@@ -188,8 +188,9 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
 // replay rounds (see replay.cuh)
 // ---------------------------------------------------------------------------
 struct ReplayArgs {
-  const int* n_cancel;  // device count of cancellations
-  const int* order;     // sweep index of the r-th cancellation in replay order
+  const int* n_cancel;               // device count of cancellations
+  const unsigned long long* key;     // [C] replay key of each cancellation
+  const int* cj;                     // [C] sweep index of each cancellation
   const int* sweep;
   const int* dying;
   const int* c1;
@@ -205,14 +206,16 @@ struct ReplayArgs {
   int* rounds;
 };
 
+// Rounds of cancellation resolution (replay.cuh). The cancellations are in
+// collection order; their keys order the replay.
 __global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs A) {
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
   const int C = *A.n_cancel;
   for (long long r = tid; r < C; r += nth) {
     A.act0[r] = (int)r;
-    int d = A.dying[A.order[r]];
-    A.S.ctime[d] = (int)r;
+    int d = A.dying[A.cj[r]];
+    A.S.ctime[d] = A.key[r];
     A.S.status[d] = kPending;
   }
   if (tid == 0) {
@@ -241,13 +244,14 @@ __global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs A) {
       int r = -1;
       if (i < n) {
         r = in[i];
-        int j = A.order[r];
+        const unsigned long long t = A.key[r];
+        int j = A.cj[r];
         int d = A.dying[j], s = A.sweep[j];
         int T0 = A.c1[j], T1 = A.c2[j];
         int R0 = -1, R1 = -1;
         long long a0 = 0, a1 = 0;
-        bool ok = walk_root(A.S, T0, r, &R0, &a0, A.max_steps, A.status) &&
-                  walk_root(A.S, T1, r, &R1, &a1, A.max_steps, A.status);
+        bool ok = walk_root(A.S, T0, t, &R0, &a0, A.max_steps, A.status) &&
+                  walk_root(A.S, T1, t, &R1, &a1, A.max_steps, A.status);
         if (!ok) {
           keep = true;
         } else {
@@ -288,11 +292,14 @@ struct EmitArgs {
   const int* arc_root;
   int4* q0;
   int4* q1;
-  int* cnt;  // [0..2]
+  int* cnt;  // [0..2] rotating level counts, [3] raw-arc segment count
   int max_levels;
   int* levels;  // receives the number of levels (statistics)
 };
 
+// Geometry of one side: breadth-first expansion of the chain and W tasks
+// (replay.cuh), collecting the raw-arc segments with their output positions,
+// then one parallel pass that walks and writes every segment.
 __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
@@ -300,22 +307,23 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
     A.cnt[0] = 0;
     A.cnt[1] = 0;
     A.cnt[2] = 0;
+    A.cnt[3] = 0;
   }
   grid.sync();
   EmitCtx E = A.E;
+  E.n_base = A.cnt + 3;
   // level 0: each surviving arc's own raw arc, then its chain
-  E.q_out = A.q0;
-  E.n_out = A.cnt;
   for (long long base = 0; base < 2LL * A.nsurv; base += nth) {
     long long q = base + tid;
-    bool push = false;
-    int4 task = make_int4(0, 0, 0, 0);
+    bool push = false, seg = false;
+    int4 task = make_int4(0, 0, 0, 0), btask = make_int4(0, 0, 0, 0);
     if (q < 2LL * A.nsurv) {
       int i = (int)(q >> 1), j = (int)(q & 1);
       int s = A.surv_sad[i];
       if (E.t[2 * s + j] >= 0) {
         long long pos = A.arc_pos[q];
-        emit_base(E, s, j, 0, pos);
+        seg = E.blen[2 * s + j] > 0;
+        btask = make_task(kTaskBase, 0, s, j, pos);
         if (A.arc_cl[q] > 0) {
           push = true;
           task = make_task(kTaskChain, 0, E.t[2 * s + j], A.arc_root[q], pos + E.blen[2 * s + j]);
@@ -323,9 +331,16 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
       }
     }
     int p = block_reserve(A.cnt, push ? 1 : 0);
+    int pb = block_reserve(E.n_base, seg ? 1 : 0);
     if (push) {
       if (p < E.q_cap)
         A.q0[p] = task;
+      else
+        set_status(E.status, kStatusQueueOverflow);
+    }
+    if (seg) {
+      if (pb < E.base_cap)
+        E.base_q[pb] = btask;
       else
         set_status(E.status, kStatusQueueOverflow);
     }
@@ -348,29 +363,37 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
     for (long long base = 0; base < n; base += nth) {
       long long i = base + tid;
       int4 t = make_int4(-1, 0, 0, 0);
-      int kind = -1, rev = 0, need = 0;
+      int kind = -1, rev = 0, need = 0, nb = 0;
       long long total = 0;
       if (i < n) {
         t = in[i];
         kind = t.x & 3;
         rev = (t.x >> 2) & 1;
-        if (kind == kTaskW) need = w_task_count(E, t.y);
-        else if (kind == kTaskChain) need = chain_task_count(E, t.y, t.z, &total);
+        if (kind == kTaskW) {
+          need = w_task_count(E, t.y);
+          nb = w_base_count(E, t.y);
+        } else if (kind == kTaskChain) {
+          need = chain_task_count(E, t.y, t.z, &total);
+        }
       }
       int p = block_reserve(E.n_out, need);
-      if (p + (long long)need > E.q_cap) {
+      int pb = block_reserve(E.n_base, nb);
+      if (p + (long long)need > E.q_cap || pb + (long long)nb > E.base_cap) {
         set_status(E.status, kStatusQueueOverflow);
-        need = 0;
         kind = -1;
       }
       if (kind == kTaskW)
-        emit_w(E, t.y, rev, t.w, p);
+        emit_w(E, t.y, rev, t.w, p, pb);
       else if (kind == kTaskChain)
         emit_chain(E, t.y, t.z, rev, t.w, need, total, p);
-      else if (kind == kTaskBase)
-        emit_base(E, t.y, t.z, rev, t.w);
     }
     grid.sync();
+  }
+  // every raw-arc segment, in parallel
+  const int nb = *(volatile int*)(A.cnt + 3);
+  for (long long i = tid; i < nb && i < E.base_cap; i += nth) {
+    int4 t = E.base_q[i];
+    emit_base(E, t.y, t.z, (t.x >> 2) & 1, t.w);
   }
 }
 

@@ -32,11 +32,11 @@
 
 namespace dmsc {
 
-constexpr int kNever = 0x7FFFFFFF;
+constexpr unsigned long long kNever = ~0ull;  // replay key of a node that is never cancelled
 enum : int { kPending = 0, kLinked = 1, kRootForever = 2 };
 
 struct ReplayState {
-  int* ctime;       // [M] replay rank of the cancellation killing the node, kNever if none
+  unsigned long long* ctime;  // [M] replay key of the cancellation killing the node, kNever if none
   int* status;      // [M] kPending / kLinked / kRootForever
   int* parent;      // [M] link target (-1 = void) when kLinked
   long long* wlen;  // [M] length of W(node)
@@ -53,10 +53,12 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   cuda::atomic_ref<int, cuda::thread_scope_device>(*p).store(v, cuda::memory_order_release);
 }
 
-// Root of x just before replay step t, with the summed path length; returns
-// false when a node on the way is still undecided.
-__device__ __forceinline__ bool walk_root(const ReplayState& S, int x, int t, int* root, long long* acc,
-                                          int max_steps, unsigned* status) {
+// Root of x just before the replay step with key t, with the summed path
+// length; returns false when a node on the way is still undecided. Replay
+// steps are compared by their (persistence, saddle cell) keys, which are
+// unique, so no ranks are needed.
+__device__ __forceinline__ bool walk_root(const ReplayState& S, int x, unsigned long long t, int* root,
+                                          long long* acc, int max_steps, unsigned* status) {
   long long a = 0;
   int steps = 0;
   while (true) {
@@ -160,6 +162,9 @@ struct EmitCtx {
   int4* q_out;
   int* n_out;
   long long q_cap;
+  int4* base_q;  // raw-arc segments, written after the expansion
+  int* n_base;
+  long long base_cap;
   int max_steps;
   unsigned* status;
 };
@@ -177,6 +182,12 @@ __device__ void emit_base(const EmitCtx& E, int s, int j, int rev, long long pos
       curr = E.faces ? next_face(e, curr, E.Nx) : next_vertex(e, curr, E.H, E.W, E.Nx);
     }
   }
+}
+
+// Number of raw-arc segments W(d) contributes.
+__device__ __forceinline__ int w_base_count(const EmitCtx& E, int d) {
+  int k = E.S.side[d], s = E.S.csad[d];
+  return (E.blen[2 * s + k] > 0) + (E.blen[2 * s + 1 - k] > 0);
 }
 
 // Number of W tasks of chain(x -> stop) and its total length; the chain is
@@ -215,8 +226,9 @@ __device__ __forceinline__ int w_task_count(const EmitCtx& E, int d) {
   return (E.S.cl_dy[d] > 0) + (E.S.cl_ot[d] > 0);
 }
 
-// Expands W(d): writes its two raw arcs and queues its two chains at slot p.
-__device__ void emit_w(const EmitCtx& E, int d, int rev, long long pos, int p) {
+// Expands W(d): queues its two chains at slot p and its two raw-arc segments
+// at base slot pb.
+__device__ void emit_w(const EmitCtx& E, int d, int rev, long long pos, int p, int pb) {
   int k = E.S.side[d], o = 1 - k, s = E.S.csad[d];
   int Tk = E.t[2 * s + k], To = E.t[2 * s + o];
   long long la = E.S.cl_dy[d], lb = E.blen[2 * s + k], lc = E.blen[2 * s + o], ld = E.S.cl_ot[d];
@@ -224,13 +236,13 @@ __device__ void emit_w(const EmitCtx& E, int d, int rev, long long pos, int p) {
   if (!rev) {
     // reverse(chain(Tk -> d)) + reverse(arc k) + arc o + chain(To -> R)
     if (la > 0) E.q_out[p++] = make_task(kTaskChain, 1, Tk, d, pos);
-    if (lb > 0) emit_base(E, s, k, 1, pos + la);
-    if (lc > 0) emit_base(E, s, o, 0, pos + la + lb);
+    if (lb > 0) E.base_q[pb++] = make_task(kTaskBase, 1, s, k, pos + la);
+    if (lc > 0) E.base_q[pb++] = make_task(kTaskBase, 0, s, o, pos + la + lb);
     if (ld > 0) E.q_out[p++] = make_task(kTaskChain, 0, To, R, pos + la + lb + lc);
   } else {
     if (ld > 0) E.q_out[p++] = make_task(kTaskChain, 1, To, R, pos);
-    if (lc > 0) emit_base(E, s, o, 1, pos + ld);
-    if (lb > 0) emit_base(E, s, k, 0, pos + ld + lc);
+    if (lc > 0) E.base_q[pb++] = make_task(kTaskBase, 1, s, o, pos + ld);
+    if (lb > 0) E.base_q[pb++] = make_task(kTaskBase, 0, s, k, pos + ld + lc);
     if (la > 0) E.q_out[p++] = make_task(kTaskChain, 0, Tk, d, pos + ld + lc + lb);
   }
 }

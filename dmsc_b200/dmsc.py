@@ -211,18 +211,33 @@ def extract_dmsc(scalar_field, persistence_threshold, return_gradient=False, is_
     if not torch.cuda.is_available():
         raise RuntimeError("dmsc_b200 requires a CUDA device; there is no CPU compute path")
     on_cpu = scalar_field.device.type != "cuda"
-    x = scalar_field.to("cuda", non_blocking=False) if on_cpu else scalar_field
-    x = x.contiguous()
     flags = _flags(return_gradient, is_dual, trace_max_arcs, trace_min_arcs, trace_max_groups, trace_min_groups)
+    if on_cpu:
+        x = scalar_field.contiguous().to("cuda", non_blocking=True)
+    else:
+        x = scalar_field.contiguous()
     with torch.cuda.device(x.device):
         if x.dim() == 2:
             res = extract_single(x, persistence_threshold, flags)
-            return tuple(t.cpu() for t in res) if on_cpu else res
-        outs = []
-        for b in range(x.shape[0]):
-            res = extract_single(x[b], persistence_threshold, flags)
-            outs.append(tuple(t.cpu() for t in res) if on_cpu else res)
-        return outs
+            return _to_host(res) if on_cpu else res
+        outs = [extract_single(x[b], persistence_threshold, flags) for b in range(x.shape[0])]
+        return [_to_host(r) for r in outs] if on_cpu else outs
+
+
+def _to_host(res: tuple) -> tuple:
+    """Device outputs -> CPU tensors for a CPU caller: asynchronous copies into
+    pinned (cached) host buffers on the current stream, one synchronisation."""
+    out = []
+    for t in res:
+        if t.device.type == "cpu":
+            out.append(t)
+            continue
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        if t.numel():
+            h.copy_(t, non_blocking=True)
+        out.append(h)
+    torch.cuda.current_stream().synchronize()
+    return tuple(out)
 
 
 def compute_dmsc(img, persistence_threshold, return_gradient=True, is_dual=False, trace_valleys=True,
