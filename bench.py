@@ -266,7 +266,9 @@ def b200_arm(args):
         return compute_dmsc(img, t, is_dual=d)
 
     gpu_out = {}
-    for w in range(max(3, args.warmup)):
+    # warm-up covers every variant once, so workspace growth happens here
+    warm = max(args.warmup, len(VARIANTS))
+    for w in range(warm):
         ms = step(w)
         if rank == 0 and world == 1:
             gpu_out[VARIANTS[w % 4]] = [x.cpu() for x in ms]
@@ -308,6 +310,10 @@ def b200_arm(args):
     host = img.cpu().pin_memory()
     h2d = host.numel() * host.element_size()
     d2h = 0
+    ms = None
+    for w in range(2 * warm):  # warm the pinned host buffers exactly as the timed loop uses them
+        d, th = VARIANTS[w % 4]
+        ms = compute_dmsc(host, th, is_dual=d)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -343,7 +349,7 @@ def b200_arm(args):
     seg = seg_bytes / (lab_ms / 1000.0) / 1e9 if lab_ms > 0 else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "warmup": warm, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32/i32", "data": "synthetic",
         "config": workload_config(size),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h // args.steps},

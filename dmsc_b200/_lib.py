@@ -131,17 +131,18 @@ class Context:
                  "emit_levels_faces", "emit_levels_vertices")
         return {names[k]: int(buf[k]) for k in range(max(n, 0))}
 
-    def pairing_timeline(self) -> tuple:
-        """Per-round durations (us) of the pairing loops of the last call: (faces, vertices)."""
-        buf = (ctypes.c_longlong * 128)()
-        if self.lib.dmsc_b200_pairing_timeline(self.h, buf, 128) < 0:
-            return (), ()
-        out = []
-        for side in range(2):
-            t = [buf[side * 64 + k] for k in range(64)]
-            t = [x for x in t if x > 0]
-            out.append(tuple((b - a) / 1000.0 for a, b in zip(t, t[1:])))
-        return tuple(out)
+    def timelines(self) -> dict:
+        """Per-round / per-level durations (us) of the device loops of the last call."""
+        buf = (ctypes.c_longlong * 256)()
+        if self.lib.dmsc_b200_pairing_timeline(self.h, buf, 256) < 0:
+            return {}
+        out = {}
+        for blk, name in enumerate(("pairing_faces", "pairing_vertices", "emit_faces", "emit_vertices")):
+            t = [buf[blk * 64 + k] for k in range(64)]
+            tail = t[63] if blk >= 2 else 0
+            t = [x for x in t[:62] if x > 0] + ([tail] if tail > 0 else [])
+            out[name] = tuple((b - a) / 1000.0 for a, b in zip(t, t[1:]))
+        return out
 
     def close(self):
         if getattr(self, "h", None):

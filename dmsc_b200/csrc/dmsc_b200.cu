@@ -35,7 +35,7 @@ namespace {
 enum Slot {
   S_GRAD, S_MASK, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT,
   S_CMIN, S_CSAD, S_CMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA, S_ASC,
-  S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE,
+  S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_FLOW,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
@@ -101,6 +101,7 @@ struct dmsc_b200_context {
   float thr = 0.f;
   int nmin = 0, nsad = 0, nmax = 0, nsurv = 0;
   const int* grad = nullptr;
+  const uint8_t* flow = nullptr;
   int* crit_sad = nullptr;
   int* surv = nullptr;
   unsigned* status = nullptr;
@@ -318,7 +319,7 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
     A.status = ctx->status;
     A.max_rounds = M + 2;
     A.rounds = get<int>(ctx, S_STATS, 8) + 0 + si;
-    A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 2 * kTimeline) + si * kTimeline;
+    A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline) + si * kTimeline;
     // older = value_less<D'> with D' = dual on the vertex side, !dual on the face side
     const bool older_less = S.faces ? ctx->dual : !ctx->dual;
     if (older_less)
@@ -478,8 +479,8 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   ctx->launches = 0;
   mark(ctx, 0, st);
   CK(cudaMemsetAsync(get<int>(ctx, S_STATS, 8), 0, 8 * sizeof(int), st));
-  CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, 2 * kTimeline), 0,
-                     2 * kTimeline * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline), 0,
+                     4 * kTimeline * sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
 
   // ---- K1 gradient + criticality ----
@@ -488,13 +489,15 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   const int nsegx = (W + 1 + kTileX - 1) / kTileX;
   const long long nseg = (long long)(H + 1) * nsegx;
   uint8_t* mask = get<uint8_t>(ctx, S_MASK, nidx);
+  uint8_t* flow = get<uint8_t>(ctx, S_FLOW, nidx);
+  ctx->flow = flow;
   int* seg[3] = {get<int>(ctx, S_SEG0, nseg), get<int>(ctx, S_SEG1, nseg), get<int>(ctx, S_SEG2, nseg)};
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
   dim3 g1(nsegx, (H + 1 + kTileY - 1) / kTileY);
   if (dual)
-    LK(gradient_kernel<true><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2], ctx->fifo_lut));
+    LK(gradient_kernel<true><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2], ctx->fifo_lut, flow));
   else
-    LK(gradient_kernel<false><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2], ctx->fifo_lut));
+    LK(gradient_kernel<false><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2], ctx->fifo_lut, flow));
   LAUNCH_CHECK("gradient_kernel");
   mark(ctx, 1, st);
   for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);
@@ -546,7 +549,7 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   int* tv = get<int>(ctx, S_TV, 2 * (size_t)nsad);
   int* lv = get<int>(ctx, S_LV, 2 * (size_t)nsad);
   if (nsad > 0) {
-    LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(grad, H, W, nsad, csad, rmax, rmin, tf, lf, tv, lv, ncells,
+    LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(flow, H, W, nsad, csad, rmax, rmin, tf, lf, tv, lv, ncells,
                                                           ctx->status));
     LAUNCH_CHECK("saddle_walk_kernel");
   }
@@ -617,9 +620,9 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
     int32_t* out = S.faces ? (dual ? basins_out : peaks_out) : (dual ? peaks_out : basins_out);
     long long n = S.faces ? nidx : (long long)H * W;
     if (S.faces)
-      LK(label_kernel<true><<<grid_for(n, TB), TB, 0, st>>>(grad, H, W, rmax, S.ut, S.to_out, out, ncells, ctx->status));
+      LK(label_kernel<true><<<grid_for(n, TB), TB, 0, st>>>(flow, H, W, rmax, S.ut, S.to_out, out, ncells, ctx->status));
     else
-      LK(label_kernel<false><<<grid_for(n, TB), TB, 0, st>>>(grad, H, W, rmin, S.ut, S.to_out, out, ncells,
+      LK(label_kernel<false><<<grid_for(n, TB), TB, 0, st>>>(flow, H, W, rmin, S.ut, S.to_out, out, ncells,
                                                            ctx->status));
     LAUNCH_CHECK("label_kernel");
   }
@@ -689,7 +692,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   long long cap = S.total;
   EmitArgs A;
   EmitCtx& E = A.E;
-  E.grad = ctx->grad;
+  E.flow = ctx->flow;
   E.crit_sad = ctx->crit_sad;
   E.H = ctx->H;
   E.W = ctx->W;
@@ -717,6 +720,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   E.n_base = nullptr;
   A.max_levels = ctx->nsad + 4;
   A.levels = get<int>(ctx, S_STATS, 8) + 4 + si;
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline) + (2 + si) * kTimeline;
   coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel");
 }
 
@@ -880,7 +884,7 @@ long long dmsc_b200_launch_count(const dmsc_b200_context* ctx) { return ctx ? ct
 
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n) {
   if (!ctx || !out || ctx->bufs.size() <= (size_t)S_TIMELINE || !ctx->bufs[S_TIMELINE].p) return -1;
-  int k = n < 2 * kTimeline ? n : 2 * kTimeline;
+  int k = n < 4 * kTimeline ? n : 4 * kTimeline;
   if (cudaSetDevice(ctx->device) != cudaSuccess ||
       cudaMemcpy(out, ctx->bufs[S_TIMELINE].p, k * sizeof(long long), cudaMemcpyDeviceToHost) != cudaSuccess)
     return -1;

@@ -228,7 +228,8 @@ __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __r
                                                                uint8_t* __restrict__ crit_mask,
                                                                int* __restrict__ seg_min, int* __restrict__ seg_sad,
                                                                int* __restrict__ seg_max,
-                                                               const uint32_t* __restrict__ fifo_lut) {
+                                                               const uint32_t* __restrict__ fifo_lut,
+                                                               uint8_t* __restrict__ flow) {
   __shared__ float sv[kValY][kValX];
   __shared__ int tile[4][kTileY][kTileX];  // slot-major: conflict-free per-slot writes
   const int tid = threadIdx.x;
@@ -266,6 +267,7 @@ __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __r
     if (v.z == -1 && ix < W) m |= 4u;
     if (v.w == -1) m |= 8u;
     crit_mask[idx] = (uint8_t)m;
+    flow[idx] = (uint8_t)(vertex_flow(v.x, (int)idx) | (face_flow(v.w, (int)idx) << 4));
   }
   unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
   unsigned bs1 = __ballot_sync(0xffffffffu, m & 2u);

@@ -294,7 +294,8 @@ struct EmitArgs {
   int4* q1;
   int* cnt;  // [0..2] rotating level counts, [3] raw-arc segment count
   int max_levels;
-  int* levels;  // receives the number of levels (statistics)
+  int* levels;                   // receives the number of levels (statistics)
+  unsigned long long* timeline;  // [kTimeline] level start times (ns), optional; last slot = segment pass
 };
 
 // Geometry of one side: breadth-first expansion of the chain and W tasks
@@ -348,6 +349,7 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
   grid.sync();
   for (int lv = 0;; ++lv) {
     int n = *(volatile int*)(A.cnt + lv % 3);
+    if (tid == 0 && A.timeline && lv < kTimeline - 2) A.timeline[lv] = global_ns();
     if (n == 0) {
       if (tid == 0 && A.levels) *A.levels = lv;
       break;
@@ -394,6 +396,10 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
   for (long long i = tid; i < nb && i < E.base_cap; i += nth) {
     int4 t = E.base_q[i];
     emit_base(E, t.y, t.z, (t.x >> 2) & 1, t.w);
+  }
+  if (A.timeline) {
+    grid.sync();
+    if (tid == 0) A.timeline[kTimeline - 1] = global_ns();
   }
 }
 

@@ -151,7 +151,7 @@ __device__ __forceinline__ int4 make_task(int kind, int rev, int a, int b, long 
 }
 
 struct EmitCtx {
-  const int* grad;
+  const uint8_t* flow;
   const int* crit_sad;
   int H, W, Nx;
   bool faces;
@@ -169,18 +169,18 @@ struct EmitCtx {
   unsigned* status;
 };
 
-// Writes raw arc (s, j): the V-path from its start cell, `len` cells.
+// Writes raw arc (s, j): the V-path from its start cell, `len` cells
+// (cpu/arcs_geometry.hxx:83-111, 133-161), following the flow codes.
 __device__ void emit_base(const EmitCtx& E, int s, int j, int rev, long long pos) {
   long long len = E.blen[2 * s + j];
   if (len <= 0) return;
   int sc = E.crit_sad[s];
-  int curr = E.faces ? face_start(sc, j, E.Nx) : vertex_start(sc, j, E.H, E.W, E.Nx);
+  int cell = E.faces ? face_start(sc, j, E.Nx) : vertex_start(sc, j, E.H, E.W, E.Nx);
+  const int type = cell & 3, shift = E.faces ? 4 : 0;
+  int idx = cell >> 2;
   for (long long k = 0; k < len; ++k) {
-    E.out[rev ? pos + len - 1 - k : pos + k] = curr;
-    if (k + 1 < len) {
-      int e = __ldg(E.grad + curr);
-      curr = E.faces ? next_face(e, curr, E.Nx) : next_vertex(e, curr, E.H, E.W, E.Nx);
-    }
+    E.out[rev ? pos + len - 1 - k : pos + k] = type + 4 * idx;
+    if (k + 1 < len) idx += flow_step((__ldg(E.flow + idx) >> shift) & 0xFu, E.Nx);
   }
 }
 

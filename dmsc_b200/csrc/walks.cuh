@@ -36,9 +36,27 @@ __device__ __forceinline__ int vertex_start(int s_cell, int j, int H, int W, int
   return j < n ? v[j] : -1;
 }
 
+// Walks from index `idx` along the flow codes (nibble shift 0 = vertices,
+// 4 = faces) to the index of the critical cell; counts the steps.
+template <int SHIFT>
+__device__ __forceinline__ int flow_walk(const uint8_t* __restrict__ flow, int idx, int Nx, long long cap,
+                                         long long* steps, unsigned* status) {
+  long long n = 0;
+  unsigned c;
+  while ((c = (__ldg(flow + idx) >> SHIFT) & 0xFu) != kFlowNone) {
+    idx += flow_step(c, Nx);
+    if (++n > cap) {
+      set_status(status, kStatusWalkCap);
+      break;
+    }
+  }
+  *steps = n;
+  return idx;
+}
+
 // K4: per saddle, both face walks and the vertex walks. Writes per arc
 // (2 per saddle and side): dense target index (or -1) and step count.
-__global__ void __launch_bounds__(256) saddle_walk_kernel(const int* __restrict__ grad, int H, int W, int nsad,
+__global__ void __launch_bounds__(256) saddle_walk_kernel(const uint8_t* __restrict__ flow, int H, int W, int nsad,
                                                           const int* __restrict__ crit_sad,
                                                           const int* __restrict__ max_rank,
                                                           const int* __restrict__ min_rank, int* __restrict__ tf,
@@ -50,33 +68,18 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(const int* __restrict_
   int sc = crit_sad[s];
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
-    int curr = face_start(sc, j, Nx);
-    long long steps = 0;
-    int e;
-    while ((e = __ldg(grad + curr)) != -1) {
-      curr = next_face(e, curr, Nx);
-      if (++steps > cap) {
-        set_status(status, kStatusWalkCap);
-        break;
-      }
-    }
-    tf[2 * s + j] = max_rank[curr >> 2];
+    long long steps;
+    int end = flow_walk<4>(flow, face_start(sc, j, Nx) >> 2, Nx, cap, &steps, status);
+    tf[2 * s + j] = max_rank[end];
     lf[2 * s + j] = (int)steps;
   }
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
-    int curr = vertex_start(sc, j, H, W, Nx);
+    int start = vertex_start(sc, j, H, W, Nx);
     long long steps = 0;
-    if (curr >= 0) {
-      int e;
-      while (curr != -1 && (e = __ldg(grad + curr)) != -1) {
-        curr = next_vertex(e, curr, H, W, Nx);
-        if (++steps > cap) {
-          set_status(status, kStatusWalkCap);
-          break;
-        }
-      }
-      tv[2 * s + j] = curr >= 0 ? min_rank[curr >> 2] : -1;
+    if (start >= 0) {
+      int end = flow_walk<0>(flow, start >> 2, Nx, cap, &steps, status);
+      tv[2 * s + j] = min_rank[end];
     } else {
       tv[2 * s + j] = -1;
     }
@@ -88,7 +91,7 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(const int* __restrict_
 // walk to the critical cell, map it through the flattened thresholded
 // union-find root to the rank of the surviving extremum.
 template <bool FACES>
-__global__ void __launch_bounds__(256) label_kernel(const int* __restrict__ grad, int H, int W,
+__global__ void __launch_bounds__(256) label_kernel(const uint8_t* __restrict__ flow, int H, int W,
                                                     const int* __restrict__ rank_map, const int* __restrict__ ut_root,
                                                     const int* __restrict__ region, int* __restrict__ out, long long cap,
                                                     unsigned* status) {
@@ -96,26 +99,18 @@ __global__ void __launch_bounds__(256) label_kernel(const int* __restrict__ grad
   const int Nx = W + 1;
   long long n = FACES ? (long long)(H + 1) * Nx : (long long)H * W;
   if (i >= n) return;
-  int curr;
+  int idx;
   if (FACES) {
-    curr = (int)(4 * i + 3);
+    idx = (int)i;
   } else {
     int y = (int)(i / W), x = (int)(i - (long long)y * W);
-    curr = 4 * (y * Nx + x);
+    idx = y * Nx + x;
   }
-  long long steps = 0;
-  int e;
-  while (curr != -1 && (e = __ldg(grad + curr)) != -1) {
-    curr = FACES ? next_face(e, curr, Nx) : next_vertex(e, curr, H, W, Nx);
-    if (++steps > cap) {
-      set_status(status, kStatusWalkCap);
-      curr = -1;
-      break;
-    }
-  }
+  long long steps;
+  int end = flow_walk<FACES ? 4 : 0>(flow, idx, Nx, cap, &steps, status);
   int lab = -1;
-  if (curr != -1) {
-    int r = ut_root[rank_map[curr >> 2]];
+  if (steps <= cap) {
+    int r = ut_root[rank_map[end]];
     if (r != -1) lab = region[r];
   }
   out[i] = lab;

@@ -135,9 +135,11 @@ long long dmsc_b200_launch_count(const dmsc_b200_context* ctx);
    expansion levels (faces, vertices). Returns the number written or -1. */
 int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n);
 
-/* Start times (ns, device global timer) of the pairing rounds of the last
-   call: 64 slots for the faces, then 64 for the vertices; unused slots are 0.
-   Writes up to `n` values to `out` (host pointer), returns the number written. */
+/* Device loop timelines of the last call (ns, device global timer), four
+   blocks of 64 slots: pairing round starts (faces, vertices), then geometry
+   expansion level starts (faces, vertices) whose last slot is the end of the
+   raw-arc pass. Unused slots are 0. Writes up to `n` values to `out` (host
+   pointer), returns the number written. */
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n);
 
 #ifdef __cplusplus
