@@ -138,9 +138,7 @@ class Context:
             return {}
         out = {}
         for blk, name in enumerate(("pairing_faces", "pairing_vertices", "emit_faces", "emit_vertices")):
-            t = [buf[blk * 64 + k] for k in range(64)]
-            tail = t[63] if blk >= 2 else 0
-            t = [x for x in t[:62] if x > 0] + ([tail] if tail > 0 else [])
+            t = [x for x in (buf[blk * 64 + k] for k in range(64)) if x > 0]
             out[name] = tuple((b - a) / 1000.0 for a, b in zip(t, t[1:]))
         return out
 

@@ -42,7 +42,7 @@ enum SideSlot {
   X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
   X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_CTIME, X_STAT,
   X_PAR, X_WLEN, X_SIDE, X_CSAD, X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC,
-  X_EROWO, X_Q0, X_Q1, X_QB, kSideSlots
+  X_EROWO, X_Q0, X_Q1, X_QB, X_G1, X_G2, kSideSlots
 };
 
 struct Buf {
@@ -305,6 +305,8 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
     A.M = M;
     A.c1 = S.c1;
     A.c2 = S.c2;
+    A.g1 = sget<int>(ctx, si, X_G1, nsad);
+    A.g2 = sget<int>(ctx, si, X_G2, nsad);
     A.dying = S.dying;
     A.link = link;
     A.minedge = minedge;
@@ -619,11 +621,12 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
     if (!S.groups) continue;
     int32_t* out = S.faces ? (dual ? basins_out : peaks_out) : (dual ? peaks_out : basins_out);
     long long n = S.faces ? nidx : (long long)H * W;
+    int* map = S.rank_map;  // dense ranks are no longer needed: reuse as the label map
+    if (S.M > 0) LK(label_map_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.crit, S.ut, S.to_out, map));
     if (S.faces)
-      LK(label_kernel<true><<<grid_for(n, TB), TB, 0, st>>>(flow, H, W, rmax, S.ut, S.to_out, out, ncells, ctx->status));
+      LK(label_kernel<true><<<grid_for(n, TB), TB, 0, st>>>(flow, H, W, map, out, ncells, ctx->status));
     else
-      LK(label_kernel<false><<<grid_for(n, TB), TB, 0, st>>>(flow, H, W, rmin, S.ut, S.to_out, out, ncells,
-                                                           ctx->status));
+      LK(label_kernel<false><<<grid_for(n, TB), TB, 0, st>>>(flow, H, W, map, out, ncells, ctx->status));
     LAUNCH_CHECK("label_kernel");
   }
 
@@ -722,6 +725,13 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   A.levels = get<int>(ctx, S_STATS, 8) + 4 + si;
   A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline) + (2 + si) * kTimeline;
   coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel");
+  {
+    int per = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel, 256, 0));
+    E.n_base = A.cnt + 3;
+    LK(emit_segments_kernel<<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3, nullptr));
+    LAUNCH_CHECK("emit_segments_kernel");
+  }
 }
 
 int fetch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t st) {

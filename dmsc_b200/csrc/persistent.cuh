@@ -53,6 +53,8 @@ struct PairArgs {
   int nsad, M;  // void group = M
   const int* c1;
   const int* c2;
+  int* g1;            // [nsad] group of each end, as of the saddle's last active round
+  int* g2;
   int* dying;
   int* link;          // [M+1] group union-find
   unsigned* minedge;  // [M+1]
@@ -130,14 +132,20 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
       if (i < n) {
         e = in[i];
         if (r == 0 || A.dying[e] == kUndecided) {
-          int a = A.c1[e], b = A.c2[e];
-          a = a < 0 ? M : a;
-          b = b < 0 ? M : b;
-          int ga = r == 0 ? a : find_halving(A.link, a);
-          int gb = r == 0 ? b : find_halving(A.link, b);
+          int ga, gb;
+          if (r == 0) {
+            int a = A.c1[e], b = A.c2[e];
+            ga = a < 0 ? M : a;
+            gb = b < 0 ? M : b;
+          } else {  // the ends' groups of the previous round, followed to their roots
+            ga = find_halving(A.link, A.g1[e]);
+            gb = find_halving(A.link, A.g2[e]);
+          }
           if (ga == gb) {
             A.dying[e] = -1;
           } else {
+            A.g1[e] = ga;
+            A.g2[e] = gb;
             atomicMin(A.minedge + ga, (unsigned)e);  // result unused: a reduction
             atomicMin(A.minedge + gb, (unsigned)e);
             keep = true;
@@ -159,8 +167,7 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
         if (me != kNoEdge) {
           A.minedge[g] = kNoEdge;
           int e = (int)me;
-          int a = A.c1[e], b = A.c2[e];
-          int ga = find_halving(A.link, a < 0 ? M : a), gb = find_halving(A.link, b < 0 ? M : b);
+          int ga = A.g1[e], gb = A.g2[e];  // roots as of phase A; links change only in B2
           h = (ga == g) ? gb : ga;
           if (older<OLDER_LESS>(h, g, M, A.val, A.cell)) {
             A.dying[e] = g;
@@ -295,7 +302,7 @@ struct EmitArgs {
   int* cnt;  // [0..2] rotating level counts, [3] raw-arc segment count
   int max_levels;
   int* levels;                   // receives the number of levels (statistics)
-  unsigned long long* timeline;  // [kTimeline] level start times (ns), optional; last slot = segment pass
+  unsigned long long* timeline;  // [kTimeline] level start times (ns), optional
 };
 
 // Geometry of one side: breadth-first expansion of the chain and W tasks
@@ -391,16 +398,19 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
     }
     grid.sync();
   }
-  // every raw-arc segment, in parallel
-  const int nb = *(volatile int*)(A.cnt + 3);
-  for (long long i = tid; i < nb && i < E.base_cap; i += nth) {
+}
+
+// Every raw-arc segment collected by emit_persistent_kernel, one thread per
+// segment at full occupancy (grid-stride over the device-side count).
+__global__ void __launch_bounds__(256) emit_segments_kernel(EmitCtx E, const int* __restrict__ count,
+                                                            unsigned long long* timeline_end) {
+  const int nb = *count;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nb && i < E.base_cap; i += nth) {
     int4 t = E.base_q[i];
     emit_base(E, t.y, t.z, (t.x >> 2) & 1, t.w);
   }
-  if (A.timeline) {
-    grid.sync();
-    if (tid == 0) A.timeline[kTimeline - 1] = global_ns();
-  }
+  (void)timeline_end;
 }
 
 }  // namespace dmsc

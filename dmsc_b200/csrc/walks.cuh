@@ -87,14 +87,24 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(const uint8_t* __restr
   }
 }
 
+// Label of every extremum, stored at its index in `map` (which held the
+// extremum's dense rank): the rank among surviving extrema of its
+// thresholded union-find root, or -1 when the root is the void
+// (cpu/cell_groups.hxx:128-146, 168-173).
+__global__ void label_map_kernel(int M, const int* __restrict__ crit, const int* __restrict__ ut_root,
+                                 const int* __restrict__ region, int* __restrict__ map) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= M) return;
+  int u = ut_root[r];
+  map[crit[r] >> 2] = u < 0 ? -1 : region[u];
+}
+
 // K9: labels. One thread per face index (FACES) or per pixel (vertices):
-// walk to the critical cell, map it through the flattened thresholded
-// union-find root to the rank of the surviving extremum.
+// walk to the critical cell and read its label from the map.
 template <bool FACES>
 __global__ void __launch_bounds__(256) label_kernel(const uint8_t* __restrict__ flow, int H, int W,
-                                                    const int* __restrict__ rank_map, const int* __restrict__ ut_root,
-                                                    const int* __restrict__ region, int* __restrict__ out, long long cap,
-                                                    unsigned* status) {
+                                                    const int* __restrict__ label_map, int* __restrict__ out,
+                                                    long long cap, unsigned* status) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int Nx = W + 1;
   long long n = FACES ? (long long)(H + 1) * Nx : (long long)H * W;
@@ -108,12 +118,7 @@ __global__ void __launch_bounds__(256) label_kernel(const uint8_t* __restrict__ 
   }
   long long steps;
   int end = flow_walk<FACES ? 4 : 0>(flow, idx, Nx, cap, &steps, status);
-  int lab = -1;
-  if (steps <= cap) {
-    int r = ut_root[rank_map[end]];
-    if (r != -1) lab = region[r];
-  }
-  out[i] = lab;
+  out[i] = steps <= cap ? __ldg(label_map + end) : -1;
 }
 
 }  // namespace dmsc

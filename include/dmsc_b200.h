@@ -137,8 +137,7 @@ int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n);
 
 /* Device loop timelines of the last call (ns, device global timer), four
    blocks of 64 slots: pairing round starts (faces, vertices), then geometry
-   expansion level starts (faces, vertices) whose last slot is the end of the
-   raw-arc pass. Unused slots are 0. Writes up to `n` values to `out` (host
+   expansion level starts (faces, vertices). Unused slots are 0. Writes up to `n` values to `out` (host
    pointer), returns the number written. */
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n);
 
