@@ -12,7 +12,7 @@ from __future__ import annotations
 
 import ctypes
 import time
-from dataclasses import astuple, dataclass, fields
+from dataclasses import dataclass, fields
 
 import torch
 
@@ -114,13 +114,15 @@ class MSComplex:
         return pts
 
     def __iter__(self):
-        return iter(astuple(self))
+        # The 19 tensors in field order, as the reference's astuple-based
+        # iteration yields them (dmsc/dmsc.py:158-159), without its deep copies.
+        return iter(tuple(getattr(self, f.name) for f in fields(self)))
 
     def __len__(self):
         return 19
 
     def __getitem__(self, i):
-        return astuple(self)[i]
+        return getattr(self, fields(self)[i].name)
 
     def _no_plots(self, *a, **k):
         raise NotImplementedError("visualisation (matplotlib dashboards) is not part of dmsc_b200")
