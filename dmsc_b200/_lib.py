@@ -28,6 +28,7 @@ EXPORTS = (
     "dmsc_b200_launch_count",
     "dmsc_b200_loop_counts",
     "dmsc_b200_pairing_timeline",
+    "dmsc_b200_critical_cells_static",
 )
 
 STAGES = ("gradient", "compaction", "saddle_sort", "saddle_walks", "pairing_faces", "pairing_vertices", "survivors",
@@ -89,6 +90,10 @@ def load():
         lib.dmsc_b200_loop_counts.restype = ctypes.c_int
         lib.dmsc_b200_pairing_timeline.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
         lib.dmsc_b200_pairing_timeline.restype = ctypes.c_int
+        lib.dmsc_b200_critical_cells_static.argtypes = [
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.dmsc_b200_critical_cells_static.restype = ctypes.c_int
         _lib = lib
         return lib
 

@@ -1,8 +1,8 @@
 """Builds the CUDA library ``dmsc_b200/libdmsc_b200.so`` for sm_100a.
 
 One nvcc invocation compiles ``csrc/dmsc_b200.cu`` (which includes the other
-kernel sources) into a position-independent shared library exporting the C ABI
-declared in ``include/dmsc_b200.h``. The library is built in-tree so that it
+kernel sources) and ``csrc/noalloc.cu`` into a position-independent shared
+library exporting the C ABI declared in ``include/dmsc_b200.h``. The library is built in-tree so that it
 travels with the repository snapshot; it is loaded with ctypes.
 """
 
@@ -18,6 +18,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libdmsc_b200.so")
 SRC_DIR = os.path.join(HERE, "csrc")
 MAIN = os.path.join(SRC_DIR, "dmsc_b200.cu")
+UNITS = [MAIN, os.path.join(SRC_DIR, "noalloc.cu")]  # translation units of the library
 HEADER = os.path.join(ROOT, "include", "dmsc_b200.h")
 
 NVCC_FLAGS = [
@@ -47,7 +48,7 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
     if not force and not needs_build():
         return LIB
-    cmd = [_nvcc(), *NVCC_FLAGS, *(extra or []), "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp", MAIN]
+    cmd = [_nvcc(), *NVCC_FLAGS, *(extra or []), "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp", *UNITS]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.check_call(cmd)

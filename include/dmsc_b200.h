@@ -141,6 +141,29 @@ int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n);
    pointer), returns the number written. */
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n);
 
+/* No counterpart in the reference. For callers that cannot allocate device
+   memory at call time -- code running while a stream is captured into a CUDA
+   graph, fixed-memory real-time hosts, or plugins whose framework hands out
+   only input and output buffers -- this computes the discrete gradient
+   (grad_indices) and the ascending lists of critical minima (vertices),
+   saddles (edges) and maxima (faces) of one H x W image without allocating:
+   its scratch is a fixed 8 MiB static device array of the library (about
+   2 bytes per index (H+1)*(W+1) plus 24 bytes per 32-index row segment, so
+   up to roughly 1900 x 1900 images); larger images return
+   DMSC_B200_ERR_TOO_LARGE.
+   `grad_out`    : int32[4*(H+1)*(W+1)], 16-byte aligned.
+   `mins_out`    : int32[H*W] capacity; `saddles_out`: int32[H*(W+1)+(H+1)*W];
+   `maxes_out`   : int32[(H+1)*(W+1)]; `counts_out`: int32[3] = (#mins,
+                   #saddles, #maxima). All device pointers; only DMSC_B200_DUAL
+                   is read from `flags`.
+   The first call on a device looks up the static array's device address and
+   uploads a table; make it before any stream capture. Every call shares the
+   one scratch array (which keeps the last call's contents), so calls that
+   overlap on the GPU race: serialise them. */
+int dmsc_b200_critical_cells_static(const float* image, int H, int W, unsigned flags, int32_t* grad_out,
+                                    int32_t* mins_out, int32_t* saddles_out, int32_t* maxes_out,
+                                    int32_t* counts_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
