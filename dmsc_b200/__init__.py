@@ -7,7 +7,7 @@ replay and basin/peak labels all run as CUDA kernels (sm_100a) behind the C ABI
 in ``include/dmsc_b200.h``.
 """
 
-from .dmsc import MSComplex, compute_dmsc, extract_dmsc
+from .dmsc import MSComplex, compute_dmsc, compute_dmsc_batched, extract_dmsc
 from .synthetic import generate_noisy_landscape
 
-__all__ = ["compute_dmsc", "generate_noisy_landscape", "MSComplex", "extract_dmsc"]
+__all__ = ["compute_dmsc", "compute_dmsc_batched", "generate_noisy_landscape", "MSComplex", "extract_dmsc"]

@@ -21,6 +21,7 @@ EXPORTS = (
     "dmsc_b200_destroy",
     "dmsc_b200_extract",
     "dmsc_b200_fetch",
+    "dmsc_b200_extract_batch",
     "dmsc_b200_error_string",
     "dmsc_b200_last_error",
     "dmsc_b200_set_profiling",
@@ -76,6 +77,11 @@ def load():
         lib.dmsc_b200_extract.restype = ctypes.c_int
         lib.dmsc_b200_fetch.argtypes = [ctypes.c_void_p, ctypes.POINTER(Outputs), ctypes.c_void_p]
         lib.dmsc_b200_fetch.restype = ctypes.c_int
+        lib.dmsc_b200_extract_batch.argtypes = [
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+            ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_ubyte), ctypes.c_uint, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Sizes), ctypes.c_void_p]
+        lib.dmsc_b200_extract_batch.restype = ctypes.c_int
         lib.dmsc_b200_error_string.argtypes = [ctypes.c_int]
         lib.dmsc_b200_error_string.restype = ctypes.c_char_p
         lib.dmsc_b200_last_error.argtypes = [ctypes.c_void_p]

@@ -1,31 +1,61 @@
-// Output assembly on the device (cpu/workspace.hxx:86-365).
+// Output assembly on the device (cpu/workspace.hxx:86-365), for a batch.
 //
-// Surviving extrema keep their ascending-cell-id order; surviving saddles are
-// listed in minima-sweep order; e_min rows follow the minima sweep and e_max
-// rows the maxima sweep, which is the reverse of the minima sweep for the
-// same saddles (cpu/arcs_topology.hxx:142).
+// Per image: surviving extrema keep their ascending-cell-id order; surviving
+// saddles are listed in minima-sweep order; e_min rows follow the minima sweep
+// and e_max rows the maxima sweep, which is the reverse of the minima sweep
+// for the same saddles (cpu/arcs_topology.hxx:142). Internal side 0 is the
+// faces, side 1 the vertices; in the primal the faces are the maxima, in the
+// dual the minima (workspace.hxx:322-362), so every side's per-image output
+// goes to the array that image's orientation selects, at an offset the host
+// computed from the per-image sizes. All written ids are image-local.
 #pragma once
 
 #include "common.cuh"
 
 namespace dmsc {
 
+// Destination of one side's per-image output: the array picked by the
+// image's orientation, at the image's offset in it.
+struct Route {
+  int* primal;
+  int* dual;
+  const int* off;  // [B]
+  __device__ __forceinline__ int* at(bool d, int b) const {
+    int* p = d ? dual : primal;
+    return p ? p + off[b] : nullptr;
+  }
+};
+struct RouteF {
+  float* primal;
+  float* dual;
+  const int* off;
+  __device__ __forceinline__ float* at(bool d, int b) const {
+    float* p = d ? dual : primal;
+    return p ? p + off[b] : nullptr;
+  }
+};
+
 __global__ void u8_to_int_kernel(const uint8_t* __restrict__ a, int n, int* __restrict__ b) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = a[i];
 }
 
-// pts[to_out[x]] = cell[x] for alive x.
-__global__ void compact_alive_kernel(int n, const uint8_t* __restrict__ alive, const int* __restrict__ to_out_excl,
-                                     const int* __restrict__ cell, int* __restrict__ pts, int* __restrict__ to_out) {
+// to_out[x] = batch-wide output rank of alive extremum x (-1 otherwise).
+__global__ void to_out_kernel(int n, const uint8_t* __restrict__ alive, const int* __restrict__ to_out_excl,
+                              int* __restrict__ to_out) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= n) return;
-  if (alive[x]) {
-    to_out[x] = to_out_excl[x];
-    if (pts) pts[to_out_excl[x]] = cell[x];
-  } else {
-    to_out[x] = -1;
-  }
+  if (x < n) to_out[x] = alive[x] ? to_out_excl[x] : -1;
+}
+
+// Surviving extrema, image-local cell ids, into the routed point lists.
+__global__ void points_kernel(int n, const uint8_t* __restrict__ alive, const int* __restrict__ to_out_excl,
+                              const int* __restrict__ alive_base, const int* __restrict__ cell,
+                              const int* __restrict__ ext_img, Imgs I, Route R) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n || !alive[x]) return;
+  int b = ext_img[x];
+  int* dst = R.at(I.dual[b], b);
+  if (dst) dst[to_out_excl[x] - alive_base[b]] = cell[x] - 4 * I.idx_base[b];
 }
 
 // flag[j] = 1 when the saddle at minima-sweep position j survives both sides.
@@ -43,8 +73,37 @@ __global__ void survivor_list_kernel(int nsad, const int* __restrict__ sweep_min
   if (flag[j]) surv_sad[pos[j]] = sweep_min[j];
 }
 
-// Per survivor, in iteration order (minima: i; maxima: nsurv-1-i): number of
-// e rows (0..2) (cpu/workspace.hxx:175-195, 197-219).
+// Per-image first positions (B + 1 entries, the last one the total):
+// base[b] = excl[first[b]] where first[] are the image's first items.
+__global__ void image_base_kernel(int B, const int* __restrict__ first, int n_items, const int* __restrict__ excl,
+                                  int total, int* __restrict__ base) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > B) return;
+  int f = b < B ? first[b] : n_items;
+  base[b] = f < n_items ? excl[f] : total;
+}
+
+// The same with the total read from the device.
+__global__ void image_base_dev_kernel(int B, const int* __restrict__ first, int n_items, const int* __restrict__ excl,
+                                      const long long* __restrict__ total, int* __restrict__ base) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > B) return;
+  int f = b < B ? first[b] : n_items;
+  base[b] = f < n_items ? excl[f] : (int)*total;
+}
+
+// The survivor of output position q when an image's survivors are visited in
+// reverse (maxima sweep) or forward (minima sweep) order.
+__device__ __forceinline__ int visit(int q, bool reversed, const int* __restrict__ surv_base, int B, int* b_out) {
+  int b = find_image(surv_base, B, q);
+  *b_out = b;
+  if (!reversed) return q;
+  int base = surv_base[b], n = surv_base[b + 1] - base;
+  return base + n - 1 - (q - base);
+}
+
+// e rows of one survivor (cpu/workspace.hxx:175-195, 197-219): (0..2) ends
+// as batch-wide output ranks.
 __device__ __forceinline__ int erow_ends(int s, const int* __restrict__ t, const int* __restrict__ ut,
                                          const int* __restrict__ to_out, int* o1, int* o2) {
   int c1 = t[2 * s], c2 = t[2 * s + 1];
@@ -65,81 +124,116 @@ __device__ __forceinline__ int erow_ends(int s, const int* __restrict__ t, const
   return n;
 }
 
-__global__ void erow_count_kernel(int nsurv, bool reversed, const int* __restrict__ surv_sad,
-                                  const int* __restrict__ t, const int* __restrict__ ut,
-                                  const int* __restrict__ to_out, int* __restrict__ cnt) {
+__global__ void erow_count_kernel(int nsurv, bool reversed, const int* __restrict__ surv_base, int B,
+                                  const int* __restrict__ surv_sad, const int* __restrict__ t,
+                                  const int* __restrict__ ut, const int* __restrict__ to_out, int* __restrict__ cnt) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nsurv) return;
-  int i = reversed ? nsurv - 1 - q : q;
-  int a, b;
-  cnt[q] = erow_ends(surv_sad[i], t, ut, to_out, &a, &b);
+  int b;
+  int i = visit(q, reversed, surv_base, B, &b);
+  int a, c;
+  cnt[q] = erow_ends(surv_sad[i], t, ut, to_out, &a, &c);
 }
 
-// Per-survivor scalar outputs and e rows of one side.
-__global__ void side_outputs_kernel(int nsurv, bool reversed, const int* __restrict__ surv_sad,
-                                    const int* __restrict__ t, const int* __restrict__ ut,
-                                    const int* __restrict__ to_out, const float* __restrict__ pers,
+// Per-survivor scalars and e rows of one side. `row_off` is the batch-wide
+// exclusive scan of the row counts in visiting order; `row_base[b]` its value
+// at image b's first survivor.
+__global__ void side_outputs_kernel(int nsurv, bool reversed, const int* __restrict__ surv_base, Imgs I,
+                                    const int* __restrict__ surv_sad, const int* __restrict__ t,
+                                    const int* __restrict__ ut, const int* __restrict__ to_out,
+                                    const int* __restrict__ alive_base, const float* __restrict__ pers,
                                     const int* __restrict__ pair_dense, const int* __restrict__ row_off,
-                                    float* __restrict__ p_out, int* __restrict__ pp_out, int* __restrict__ e_out) {
+                                    const int* __restrict__ row_base, RouteF P, Route PP, Route E) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nsurv) return;
-  int i = reversed ? nsurv - 1 - q : q;
+  int b;
+  int i = visit(q, reversed, surv_base, I.B, &b);
+  const bool d = I.dual[b];
+  const int li = i - surv_base[b];
   int s = surv_sad[i];
-  if (p_out) p_out[i] = pers[s];
-  if (pp_out) {
+  if (float* p = P.at(d, b)) p[li] = pers[s];
+  if (int* pp = PP.at(d, b)) {
     int pd = pair_dense[s];
     int r = pd >= 0 ? ut[pd] : -1;
-    pp_out[i] = r >= 0 ? to_out[r] : -1;
+    pp[li] = r >= 0 ? to_out[r] - alive_base[b] : -1;
   }
-  if (e_out) {
-    int a = 0, b = 0;
-    int n = erow_ends(s, t, ut, to_out, &a, &b);
-    int o = row_off[q];
+  if (int* e = E.at(d, b)) {
+    int a = 0, c = 0;
+    int n = erow_ends(s, t, ut, to_out, &a, &c);
+    int o = row_off[q] - row_base[b];
     if (n >= 1) {
-      e_out[2 * o] = i;
-      e_out[2 * o + 1] = a;
+      e[2 * o] = li;
+      e[2 * o + 1] = a - alive_base[b];
     }
     if (n == 2) {
-      e_out[2 * o + 2] = i;
-      e_out[2 * o + 3] = b;
+      e[2 * o + 2] = li;
+      e[2 * o + 3] = c - alive_base[b];
     }
   }
 }
 
 __global__ void sad_pts_kernel(int nsurv, const int* __restrict__ surv_sad, const int* __restrict__ crit_sad,
-                               int* __restrict__ out) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nsurv) out[i] = crit_sad[surv_sad[i]];
-}
-
-// CSR offsets of one side's arcs (cpu/workspace.hxx:247-287):
-// offsets[i+1] = end of survivor i, arc_offsets[i] = end of its first arc.
-__global__ void arc_offsets_kernel(int nsurv, const long long* __restrict__ arc_len,
-                                   const long long* __restrict__ saddle_end_incl, int* __restrict__ offsets,
-                                   int* __restrict__ arc_offsets) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > nsurv) return;
-  if (i == 0) offsets[0] = 0;
-  if (i < nsurv) {
-    long long end = saddle_end_incl[i];
-    long long start = end - arc_len[2 * i] - arc_len[2 * i + 1];
-    offsets[i + 1] = (int)end;
-    arc_offsets[i] = (int)(start + arc_len[2 * i]);
-  }
-}
-
-__global__ void arc_pos_kernel(int nsurv, const long long* __restrict__ arc_len,
-                               const long long* __restrict__ saddle_end_incl, long long* __restrict__ arc_pos) {
+                               const int* __restrict__ sad_img, const int* __restrict__ surv_base, Imgs I,
+                               int* __restrict__ out, const int* __restrict__ out_off) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsurv) return;
-  long long start = saddle_end_incl[i] - arc_len[2 * i] - arc_len[2 * i + 1];
-  arc_pos[2 * i] = start;
-  arc_pos[2 * i + 1] = start + arc_len[2 * i];
+  int s = surv_sad[i];
+  int b = sad_img[s];
+  out[out_off[b] + (i - surv_base[b])] = crit_sad[s] - 4 * I.idx_base[b];
 }
 
 __global__ void pair_len_kernel(int nsurv, const long long* __restrict__ arc_len, long long* __restrict__ out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nsurv) out[i] = arc_len[2 * i] + arc_len[2 * i + 1];
+}
+
+// Geometry start of every image on one side (B + 1 entries).
+__global__ void geom_base_kernel(int B, const int* __restrict__ surv_base, int nsurv,
+                                 const long long* __restrict__ saddle_end_incl, const long long* __restrict__ plen,
+                                 long long total, long long* __restrict__ gbase) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > B) return;
+  int f = b < B ? surv_base[b] : nsurv;
+  gbase[b] = f < nsurv ? saddle_end_incl[f] - plen[f] : total;
+}
+
+// Output position of every arc: the image's destination offset plus the
+// arc's position inside the image's geometry.
+__global__ void arc_pos_kernel(int nsurv, const long long* __restrict__ arc_len,
+                               const long long* __restrict__ saddle_end_incl, const int* __restrict__ surv_sad,
+                               const int* __restrict__ sad_img, const long long* __restrict__ gbase,
+                               const int* __restrict__ dst_off, long long* __restrict__ arc_pos) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsurv) return;
+  long long start = saddle_end_incl[i] - arc_len[2 * i] - arc_len[2 * i + 1];
+  const int b = sad_img[surv_sad[i]];
+  start += (long long)dst_off[b] - gbase[b];
+  arc_pos[2 * i] = start;
+  arc_pos[2 * i + 1] = start + arc_len[2 * i];
+}
+
+// CSR offsets of one side's arcs, per image (cpu/workspace.hxx:247-287):
+// offsets[0] = 0, offsets[k+1] = end of survivor k, arc_offsets[k] = end of
+// its first arc, image-local. `off_off[b]` / `arc_off[b]` place image b's
+// block (n_b + 1 and n_b entries) in the routed arrays.
+__global__ void arc_offsets_kernel(int nsurv, int B, const int* __restrict__ surv_base, const uint8_t* __restrict__ dual,
+                                   const long long* __restrict__ arc_len,
+                                   const long long* __restrict__ saddle_end_incl, const long long* __restrict__ gbase,
+                                   Route OFF, Route AOFF) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsurv + B) return;
+  if (i >= nsurv) {  // one leading zero per image
+    int b = i - nsurv;
+    if (int* o = OFF.at(dual[b], b)) o[0] = 0;
+    return;
+  }
+  int b = find_image(surv_base, B, i);
+  const bool d = dual[b];
+  long long end = saddle_end_incl[i] - gbase[b];
+  long long start = end - arc_len[2 * i] - arc_len[2 * i + 1];
+  int li = i - surv_base[b];
+  if (int* o = OFF.at(d, b)) o[li + 1] = (int)end;
+  if (int* a = AOFF.at(d, b)) a[li] = (int)(start + arc_len[2 * i]);
 }
 
 }  // namespace dmsc

@@ -128,6 +128,36 @@ __device__ __forceinline__ float sub_like_host(float a, float b) {
 
 __device__ __forceinline__ void set_status(unsigned* status, unsigned bit) { atomicOr(status, bit); }
 
+// Per-image tables of a batch. The images' index grids ((H+1) x (W+1) each)
+// are concatenated into one global index space, so a global cell id is
+// type + 4 * (idx_base[b] + y * (W+1) + x); every per-image quantity is
+// looked up from the image id b. Bases are exclusive prefix sums with B+1
+// entries. Cell ids stay int32: the batch's total index count is < 2^29.
+struct Imgs {
+  int B;
+  const int* H;
+  const int* W;
+  const int* idx_base;   // indices
+  const int* px_base;    // pixels
+  const int* tile_base;  // 32 x 16 gradient tiles
+  const int* seg_base;   // 32-index row segments
+  const uint8_t* dual;
+  const float* thr;
+};
+
+// Largest b with base[b] <= g (the image holding global item g).
+__device__ __forceinline__ int find_image(const int* __restrict__ base, int B, long long g) {
+  int lo = 0, hi = B - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= g)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
 // Block-aggregated reservation of `cnt` consecutive slots per thread: one
 // global atomic per block. Every thread of the block must call it (blockDim.x
 // a multiple of 32, at most 1024). Returns this thread's first slot.

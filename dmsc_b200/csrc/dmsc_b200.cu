@@ -32,17 +32,18 @@ using namespace dmsc;
 
 namespace {
 
+
 enum Slot {
-  S_GRAD, S_MASK, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT,
-  S_CMIN, S_CSAD, S_CMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA, S_ASC,
-  S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_FLOW,
+  S_GRAD, S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
+  S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
+  S_ASC, S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
   X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
-  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_CTIME, X_STAT,
-  X_PAR, X_WLEN, X_SIDE, X_CSAD, X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC,
-  X_EROWO, X_Q0, X_Q1, X_QB, X_G1, X_G2, kSideSlots
+  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_CTIME, X_STAT, X_PAR, X_WLEN, X_SIDE,
+  X_CSAD, X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G1,
+  X_G2, X_GBASE, kSideSlots
 };
 
 struct Buf {
@@ -50,12 +51,25 @@ struct Buf {
   size_t cap = 0;
 };
 
+// Device-side per-image bases (B + 1 entries each) of the last extract.
+struct Bases {
+  int* min;       // first minimum (vertex extremum) of each image
+  int* sad;       // first saddle
+  int* max;       // first maximum (face extremum)
+  int* surv;      // first surviving saddle
+  int* alive[2];  // first output rank of each side's surviving extrema
+  int* erow[2];   // first e row of each side
+};
+
 struct Side {
   int M = 0;
   bool faces = true;
-  bool arcs = false;
-  bool groups = false;
+  bool arcs = false;    // some image takes this side's arcs
+  bool groups = false;  // some image takes this side's labels
+  bool arcs_primal = false, arcs_dual = false;      // by orientation
+  bool groups_primal = false, groups_dual = false;
   int* crit = nullptr;
+  int* ext_img = nullptr;
   float* val = nullptr;
   int* rank_map = nullptr;
   int* t = nullptr;
@@ -76,12 +90,13 @@ struct Side {
   long long* arc_len = nullptr;
   long long* arc_cl = nullptr;
   int* arc_root = nullptr;
-  long long* arc_pos = nullptr;
+  long long* send = nullptr;
+  long long* plen = nullptr;
+  long long* gbase = nullptr;  // [B+1] geometry start of each image
   long long total = 0;
   int n_alive = 0;
   int n_erows = 0;
   int* erow_off = nullptr;
-  int rounds_pair = 0, rounds_replay = 0;
 };
 
 }  // namespace
@@ -92,21 +107,28 @@ struct dmsc_b200_context {
   int device = 0;
   std::vector<Buf> bufs;
   Buf cub_tmp;
-  long long* pinned = nullptr;  // host scalars for readbacks
+  long long* pinned = nullptr;  // host staging for readbacks and tables
+  size_t pinned_cap = 0;
   std::string err;
-  // state of the last extract()
+  // state of the last extract
   bool valid = false;
-  int H = 0, W = 0;
-  bool dual = false;
-  float thr = 0.f;
+  int B = 0;
+  unsigned flags = 0;
   int nmin = 0, nsad = 0, nmax = 0, nsurv = 0;
+  long long nidx = 0;
+  Imgs I{};
+  std::vector<int> hH, hW;
+  std::vector<uint8_t> hdual;
+  Bases bases{};
   const int* grad = nullptr;
   const uint8_t* flow = nullptr;
   int* crit_sad = nullptr;
+  int* sad_img = nullptr;
   int* surv = nullptr;
   unsigned* status = nullptr;
   Side side[2];
-  dmsc_b200_sizes sizes{};
+  std::vector<dmsc_b200_sizes> sizes;
+  std::vector<long long> geom[2];  // per-image geometry lengths of each side
   // profiling: launch counter and stage boundary events
   long long launches = 0;
   bool profile = false;
@@ -114,6 +136,8 @@ struct dmsc_b200_context {
   int num_sms = 0;
   cudaEvent_t ev[kStageMarks] = {};
 };
+
+
 
 namespace dmsc {
 
@@ -228,12 +252,13 @@ void incl_sum(dmsc_b200_context* ctx, const In* in, Out* out, int n, cudaStream_
 }
 
 template <class K>
-void sort_pairs(dmsc_b200_context* ctx, const K* kin, K* kout, const int* vin, int* vout, int n, cudaStream_t st) {
+void sort_pairs(dmsc_b200_context* ctx, const K* kin, K* kout, const int* vin, int* vout, int n, cudaStream_t st,
+                int end_bit = (int)(8 * sizeof(K))) {
   if (n <= 0) return;
   size_t bytes = 0;
-  CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, (int)(8 * sizeof(K)), st));
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, end_bit, st));
   void* tmp = cub_tmp(ctx, bytes);
-  CK(cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, n, 0, (int)(8 * sizeof(K)), st));
+  CK(cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, n, 0, end_bit, st));
   ++ctx->launches;
 }
 
@@ -281,10 +306,24 @@ void check_status(dmsc_b200_context* ctx, cudaStream_t st) {
   }
 }
 
+
+
 constexpr int TB = 256;
 
-// Persistence pairing of one side (see pairing.cuh).
-void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool reverse, cudaStream_t st) {
+// Pinned host staging of at least `bytes`.
+void* staging(dmsc_b200_context* ctx, size_t bytes) {
+  if (ctx->pinned_cap < bytes) {
+    if (ctx->pinned) CK(cudaFreeHost(ctx->pinned));
+    ctx->pinned = nullptr;
+    size_t nb = bytes + bytes / 2 + 1024;
+    CK(cudaMallocHost(&ctx->pinned, nb));
+    ctx->pinned_cap = nb;
+  }
+  return ctx->pinned;
+}
+
+// Persistence pairing of one side over the whole batch (see pairing.cuh).
+void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, cudaStream_t st) {
   const int nsad = ctx->nsad, M = S.M;
   S.sweep = sget<int>(ctx, si, X_SWEEP, nsad);
   S.c1 = sget<int>(ctx, si, X_C1, nsad);
@@ -296,10 +335,9 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
   int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
   int* cnt = sget<int>(ctx, si, X_CNT, 8);
   if (nsad > 0) {
-    LK(sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, reverse, S.t, S.sweep, S.c1, S.c2, S.dying));
+    LK(sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, ctx->sad_img, ctx->bases.sad, ctx->I.dual,
+                                                             S.faces, S.t, S.sweep, S.c1, S.c2));
     LAUNCH_CHECK("sweep_edges_kernel");
-  }
-  {
     PairArgs A;
     A.nsad = nsad;
     A.M = M;
@@ -318,19 +356,15 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
     A.cnt = cnt;
     A.val = S.val;
     A.cell = S.crit;
+    A.ext_img = S.ext_img;
+    A.dual = ctx->I.dual;
+    A.faces = S.faces;
     A.status = ctx->status;
     A.max_rounds = M + 2;
     A.rounds = get<int>(ctx, S_STATS, 8) + 0 + si;
     A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline) + si * kTimeline;
-    // older = value_less<D'> with D' = dual on the vertex side, !dual on the face side
-    const bool older_less = S.faces ? ctx->dual : !ctx->dual;
-    if (older_less)
-      coop_launch(ctx, pairing_persistent_kernel<true>, A, st, "pairing_persistent_kernel");
-    else
-      coop_launch(ctx, pairing_persistent_kernel<false>, A, st, "pairing_persistent_kernel");
+    coop_launch(ctx, pairing_persistent_kernel, A, st, "pairing_persistent_kernel");
   }
-  int rounds = 0;
-  S.rounds_pair = rounds;
 
   // persistence, cancellation, alive flags
   S.pair_dense = sget<int>(ctx, si, X_PAIR, nsad);
@@ -341,9 +375,9 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
   int* ncanc = get<int>(ctx, S_NCANC, 4) + si;
   CK(cudaMemsetAsync(ncanc, 0, sizeof(int), st));
   if (nsad > 0) {
-    LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, !S.faces, ctx->dual, ctx->thr, S.sweep, S.dying,
-                                                          get<float>(ctx, S_SVAL, nsad), S.val, S.pair_dense, S.pers,
-                                                          canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc));
+    LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(
+        nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.sweep, S.dying, get<float>(ctx, S_SVAL, nsad), S.val,
+        S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc));
     LAUNCH_CHECK("persistence_kernel");
   }
   // thresholded union-find roots
@@ -352,27 +386,27 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, bool r
   S.ut = sget<int>(ctx, si, X_UT, M + 1);
   LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(uf, M + 1));
   if (nsad > 0)
-    LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.c1, S.c2, S.pers, ctx->thr, M, uf));
+    LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.c1, S.c2, S.pers, ctx->I.thr,
+                                                          ctx->sad_img, M, uf));
   LK(ut_flatten_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, uf));
   LK(ut_mark_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M, uf, S.alive, croot));
   if (M > 0) LK(ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.ut));
   LAUNCH_CHECK("thresholded union-find");
-  // output rank of alive extrema
+  // batch-wide output rank of alive extrema
   int* alive_i = sget<int>(ctx, si, X_ALIVEI, M + 1);
   S.to_out_excl = sget<int>(ctx, si, X_TOOUTX, M + 1);
   S.to_out = sget<int>(ctx, si, X_TOOUT, M + 1);
   if (M > 0) {
     LK(u8_to_int_kernel<<<grid_for(M, TB), TB, 0, st>>>(S.alive, M, alive_i));
     excl_sum(ctx, alive_i, S.to_out_excl, M, st);
-    LK(compact_alive_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, S.alive, S.to_out_excl, S.crit, nullptr, S.to_out));
-    LAUNCH_CHECK("compact_alive_kernel");
+    LK(to_out_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, S.alive, S.to_out_excl, S.to_out));
+    LAUNCH_CHECK("to_out_kernel");
   }
 }
 
-// Replay of one side's cancellations and the final arc lengths.
+// Replay of one side's cancellations and the final arc lengths (batch).
 void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   const int nsad = ctx->nsad, M = S.M, nsurv = ctx->nsurv;
-  long long* tot = get<long long>(ctx, S_TOT, 8);
   S.blen = sget<long long>(ctx, si, X_BLEN, 2 * (size_t)nsad);
   if (nsad > 0) LK(base_len_kernel<<<grid_for(2LL * nsad, TB), TB, 0, st>>>(2 * nsad, S.t, S.steps, S.blen));
   unsigned long long* ckey = sget<unsigned long long>(ctx, si, X_CKEY, nsad);
@@ -380,8 +414,8 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   int* cnt = sget<int>(ctx, si, X_CNT, 8);
   CK(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), st));
   if (nsad > 0)
-    LK(cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->thr,
-                                                               ctx->crit_sad, ckey, cval, cnt + 3));
+    LK(cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->I.thr,
+                                                               ctx->sad_img, ctx->crit_sad, ckey, cval, cnt + 3));
   LAUNCH_CHECK("cancel_collect_kernel");
 
   ReplayState& R = S.R;
@@ -398,7 +432,7 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   LAUNCH_CHECK("replay init");
   int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
   const int max_steps = nsad + 1;
-  {
+  if (S.C > 0) {
     ReplayArgs A;
     A.n_cancel = cnt + 3;
     A.key = ckey;
@@ -418,23 +452,23 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
     A.rounds = get<int>(ctx, S_STATS, 8) + 2 + si;
     coop_launch(ctx, replay_persistent_kernel, A, st, "replay_persistent_kernel");
   }
-  int rounds = 0;
-  S.rounds_replay = rounds;
 
   S.arc_len = sget<long long>(ctx, si, X_ALEN, 2 * (size_t)nsurv);
   S.arc_cl = sget<long long>(ctx, si, X_ACL, 2 * (size_t)nsurv);
   S.arc_root = sget<int>(ctx, si, X_AROOT, 2 * (size_t)nsurv);
-  S.arc_pos = sget<long long>(ctx, si, X_APOS, 2 * (size_t)nsurv);
-  long long* plen = sget<long long>(ctx, si, X_PLEN, nsurv);
-  long long* send = sget<long long>(ctx, si, X_SEND, nsurv);
+  S.plen = sget<long long>(ctx, si, X_PLEN, nsurv);
+  S.send = sget<long long>(ctx, si, X_SEND, nsurv);
+  S.gbase = sget<long long>(ctx, si, X_GBASE, ctx->B + 1);
   S.total = 0;
   if (nsurv > 0) {
-    LK(final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, S.t, S.blen, R, max_steps,
-                                                                S.arc_len, S.arc_cl, S.arc_root, ctx->status));
-    LK(pair_len_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, plen));
-    incl_sum(ctx, plen, send, nsurv, st);
-    LK(arc_pos_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, send, S.arc_pos));
-    LK(last_kernel<long long><<<1, 1, 0, st>>>(send, nsurv, tot));
+    long long* tot = get<long long>(ctx, S_TOT, 8);
+    LK(final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->sad_img, ctx->I.dual,
+                                                                   S.arcs_primal, S.arcs_dual, S.t, S.blen, R,
+                                                                   max_steps, S.arc_len, S.arc_cl, S.arc_root,
+                                                                   ctx->status));
+    LK(pair_len_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.plen));
+    incl_sum(ctx, S.plen, S.send, nsurv, st);
+    LK(last_kernel<long long><<<1, 1, 0, st>>>(S.send, nsurv, tot));
     LAUNCH_CHECK("final arcs");
     readback(ctx, st, tot, 1);
     S.total = ctx->pinned[0];
@@ -443,21 +477,26 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
       throw Fail{kErrOverflow};
     }
   }
+  LK(geom_base_kernel<<<grid_for(ctx->B + 1LL, TB), TB, 0, st>>>(ctx->B, ctx->bases.surv, nsurv, S.send, S.plen,
+                                                                 S.total, S.gbase));
+  LAUNCH_CHECK("geom_base_kernel");
 }
 
-int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float thr, unsigned flags, int32_t* grad_out,
-                 int32_t* peaks_out, int32_t* basins_out, dmsc_b200_sizes* sizes, cudaStream_t st) {
+// Number of bits needed for values 0 .. n-1 (at least 1).
+int bits_for(int n) {
+  int b = 1;
+  while ((1LL << b) < n) ++b;
+  return b;
+}
+
+int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const int* hH, const int* hW,
+                       const float* hthr, const unsigned char* hdual, unsigned flags, int32_t* grad_out,
+                       int32_t* peaks_out, int32_t* basins_out, dmsc_b200_sizes* sizes_out, cudaStream_t st) {
   ctx->valid = false;
-  if (!img || H <= 0 || W <= 0 || !sizes) {
+  if (!img || B <= 0 || !hH || !hW || !hthr || !hdual || !sizes_out) {
     set_err(ctx, "invalid argument");
     return kErrInvalidArgument;
   }
-  // 32-bit cell ids (input_validation.hxx:24-26)
-  if ((long long)H + 1 > 2147483647LL / 4 / ((long long)W + 1)) {
-    set_err(ctx, "Input is too large for 32-bit cell IDs: %dx%d", H, W);
-    return kErrTooLarge;
-  }
-  const bool dual = flags & DMSC_B200_DUAL;
   const bool ret_grad = flags & DMSC_B200_RETURN_GRADIENT;
   const bool f_ridges = flags & DMSC_B200_TRACE_RIDGES, f_valleys = flags & DMSC_B200_TRACE_VALLEYS;
   const bool f_peaks = flags & DMSC_B200_TRACE_PEAKS, f_basins = flags & DMSC_B200_TRACE_BASINS;
@@ -469,38 +508,105 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
     set_err(ctx, "grad_out must be 16-byte aligned");
     return kErrInvalidArgument;
   }
+  // per-image tables (host): 32-bit cell ids per image (input_validation.hxx:24-26) and for the batch
+  std::vector<int> tab(8 * (size_t)(B + 1), 0);
+  int* tH = tab.data();
+  int* tW = tH + (B + 1);
+  int* idx_base = tW + (B + 1);
+  int* px_base = idx_base + (B + 1);
+  int* tile_base = px_base + (B + 1);
+  int* seg_base = tile_base + (B + 1);
+  int* peaks_off = seg_base + (B + 1);
+  int* basins_off = peaks_off + (B + 1);
+  long long nidx = 0, npx = 0, ntile = 0, nseg = 0, npk = 0, nbs = 0;
+  bool any_primal = false, any_dual = false;
+  for (int b = 0; b < B; ++b) {
+    const long long H = hH[b], W = hW[b];
+    if (H <= 0 || W <= 0) {
+      set_err(ctx, "image %d has an empty dimension", b);
+      return kErrInvalidArgument;
+    }
+    if (H + 1 > 2147483647LL / 4 / (W + 1)) {
+      set_err(ctx, "Input is too large for 32-bit cell IDs: %lldx%lld", H, W);
+      return kErrTooLarge;
+    }
+    tH[b] = (int)H;
+    tW[b] = (int)W;
+    idx_base[b] = (int)nidx;
+    px_base[b] = (int)npx;
+    tile_base[b] = (int)ntile;
+    seg_base[b] = (int)nseg;
+    peaks_off[b] = (int)npk;
+    basins_off[b] = (int)nbs;
+    const long long ntx = (W + 1 + kTileX - 1) / kTileX, nty = (H + 1 + kTileY - 1) / kTileY;
+    nidx += (H + 1) * (W + 1);
+    npx += H * W;
+    ntile += ntx * nty;
+    nseg += (H + 1) * ntx;
+    npk += hdual[b] ? H * W : (H + 1) * (W + 1);
+    nbs += hdual[b] ? (H + 1) * (W + 1) : H * W;
+    (hdual[b] ? any_dual : any_primal) = true;
+    if (4 * nidx > 2147483647LL || npx > 2147483647LL || npk > 2147483647LL || nbs > 2147483647LL) {
+      set_err(ctx, "batch too large for 32-bit cell ids; split it");
+      return kErrTooLarge;
+    }
+  }
+  idx_base[B] = (int)nidx;
+  px_base[B] = (int)npx;
+  tile_base[B] = (int)ntile;
+  seg_base[B] = (int)nseg;
+  peaks_off[B] = (int)npk;
+  basins_off[B] = (int)nbs;
   CK(cudaSetDevice(ctx->device));
-  ctx->H = H;
-  ctx->W = W;
-  ctx->dual = dual;
-  ctx->thr = thr;
-  const int Nx = W + 1;
-  const long long nidx = (long long)(H + 1) * Nx;
-  const long long ncells = 4 * nidx;
+  ctx->B = B;
+  ctx->flags = flags;
+  ctx->nidx = nidx;
+  ctx->hH.assign(hH, hH + B);
+  ctx->hW.assign(hW, hW + B);
+  ctx->hdual.assign(hdual, hdual + B);
   ctx->status = get<unsigned>(ctx, S_STATUS, 4);
   ctx->launches = 0;
   mark(ctx, 0, st);
+  CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
   CK(cudaMemsetAsync(get<int>(ctx, S_STATS, 8), 0, 8 * sizeof(int), st));
   CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline), 0,
                      4 * kTimeline * sizeof(unsigned long long), st));
-  CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
+  {  // upload the tables: 8 int arrays, then thr (float) and dual (u8)
+    size_t ib = tab.size() * sizeof(int), fb = (size_t)B * sizeof(float);
+    size_t total = ib + fb + B + 16;
+    char* h = (char*)staging(ctx, total);
+    memcpy(h, tab.data(), ib);
+    memcpy(h + ib, hthr, fb);
+    memcpy(h + ib + fb, hdual, B);
+    char* d = get<char>(ctx, S_TAB, total);
+    CK(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, st));
+    int* di = (int*)d;
+    ctx->I.B = B;
+    ctx->I.H = di;
+    ctx->I.W = di + (B + 1);
+    ctx->I.idx_base = di + 2 * (B + 1);
+    ctx->I.px_base = di + 3 * (B + 1);
+    ctx->I.tile_base = di + 4 * (B + 1);
+    ctx->I.seg_base = di + 5 * (B + 1);
+    ctx->I.thr = (const float*)(d + ib);
+    ctx->I.dual = (const uint8_t*)(d + ib + fb);
+  }
+  const int* d_peaks_off = ctx->I.H + 6 * (B + 1);
+  const int* d_basins_off = ctx->I.H + 7 * (B + 1);
+  const Imgs I = ctx->I;
+  const long long ncells = 4 * nidx;
 
-  // ---- K1 gradient + criticality ----
+  // ---- K1 gradient + criticality (all images, one grid) ----
   int* grad = ret_grad ? grad_out : get<int>(ctx, S_GRAD, ncells);
   ctx->grad = grad;
-  const int nsegx = (W + 1 + kTileX - 1) / kTileX;
-  const long long nseg = (long long)(H + 1) * nsegx;
   uint8_t* mask = get<uint8_t>(ctx, S_MASK, nidx);
   uint8_t* flow = get<uint8_t>(ctx, S_FLOW, nidx);
   ctx->flow = flow;
   int* seg[3] = {get<int>(ctx, S_SEG0, nseg), get<int>(ctx, S_SEG1, nseg), get<int>(ctx, S_SEG2, nseg)};
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
-  dim3 g1(nsegx, (H + 1 + kTileY - 1) / kTileY);
-  if (dual)
-    LK(gradient_kernel<true><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2], ctx->fifo_lut, flow));
-  else
-    LK(gradient_kernel<false><<<g1, kGradThreads, 0, st>>>(img, H, W, (int4*)grad, mask, seg[0], seg[1], seg[2], ctx->fifo_lut, flow));
-  LAUNCH_CHECK("gradient_kernel");
+  LK(gradient_batch_kernel<<<(unsigned)ntile, kGradThreads, 0, st>>>(I, img, (int4*)grad, mask, seg[0], seg[1], seg[2],
+                                                                     ctx->fifo_lut, flow));
+  LAUNCH_CHECK("gradient_batch_kernel");
   mark(ctx, 1, st);
   for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);
   long long* tot = get<long long>(ctx, S_TOT, 8);
@@ -516,43 +622,55 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   int* cmin = get<int>(ctx, S_CMIN, nmin);
   int* csad = get<int>(ctx, S_CSAD, nsad);
   int* cmax = get<int>(ctx, S_CMAX, nmax);
+  int* imin = get<int>(ctx, S_IMIN, nmin);
+  int* isad = get<int>(ctx, S_ISAD, nsad);
+  int* imax = get<int>(ctx, S_IMAX, nmax);
   int* rmin = get<int>(ctx, S_RMIN, nidx);
   int* rmax = get<int>(ctx, S_RMAX, nidx);
   float* vmin = get<float>(ctx, S_VMIN, nmin);
   float* vmax = get<float>(ctx, S_VMAX, nmax);
   float* sval = get<float>(ctx, S_SVAL, nsad);
-  uint32_t* skey = get<uint32_t>(ctx, S_SKEY, nsad);
+  unsigned long long* skey = get<unsigned long long>(ctx, S_SKEY, nsad);
   ctx->crit_sad = csad;
-  {
-    unsigned blocks = grid_for(nseg, 8);
-    if (dual)
-      LK(compact_kernel<true><<<blocks, 256, 0, st>>>(img, H, W, nsegx, nseg, mask, off[0], off[1], off[2], cmin, csad,
-                                                   cmax, rmin, rmax, vmin, vmax, sval, skey));
-    else
-      LK(compact_kernel<false><<<blocks, 256, 0, st>>>(img, H, W, nsegx, nseg, mask, off[0], off[1], off[2], cmin, csad,
-                                                    cmax, rmin, rmax, vmin, vmax, sval, skey));
-    LAUNCH_CHECK("compact_kernel");
-  }
+  ctx->sad_img = isad;
+  LK(compact_kernel<<<grid_for(nseg, 8), 256, 0, st>>>(I, img, nseg, mask, off[0], off[1], off[2], cmin, csad, cmax,
+                                                       imin, isad, imax, rmin, rmax, vmin, vmax, sval, skey));
+  LAUNCH_CHECK("compact_kernel");
+  // per-image bases of the critical lists (B + 1 entries each)
+  int* bases = get<int>(ctx, S_BASES, 9 * (size_t)(B + 1));
+  Bases& BS = ctx->bases;
+  BS.min = bases;
+  BS.sad = bases + (B + 1);
+  BS.max = bases + 2 * (B + 1);
+  BS.surv = bases + 3 * (B + 1);
+  BS.alive[0] = bases + 4 * (B + 1);
+  BS.alive[1] = bases + 5 * (B + 1);
+  BS.erow[0] = bases + 6 * (B + 1);
+  BS.erow[1] = bases + 7 * (B + 1);
+  LK(image_base_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, I.seg_base, (int)nseg, off[0], nmin, BS.min));
+  LK(image_base_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, I.seg_base, (int)nseg, off[1], nsad, BS.sad));
+  LK(image_base_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, I.seg_base, (int)nseg, off[2], nmax, BS.max));
+  LAUNCH_CHECK("image_base_kernel");
   mark(ctx, 2, st);
 
-  // ---- saddle order: ascending (s_val, cell id) (arcs_topology.hxx:99-102) ----
+  // ---- saddle order: per image ascending (s_val, cell id) (arcs_topology.hxx:99-102) ----
   int* iota = get<int>(ctx, S_IOTA, nsad);
   int* asc = get<int>(ctx, S_ASC, nsad);
-  uint32_t* skey2 = get<uint32_t>(ctx, S_SKEY2, nsad);
+  unsigned long long* skey2 = get<unsigned long long>(ctx, S_SKEY2, nsad);
   if (nsad > 0) {
     LK(iota_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(iota, nsad));
-    sort_pairs(ctx, skey, skey2, iota, asc, nsad, st);
+    sort_pairs(ctx, skey, skey2, iota, asc, nsad, st, 32 + (B > 1 ? bits_for(B) : 0));
   }
-
   mark(ctx, 3, st);
+
   // ---- K4 saddle walks ----
   int* tf = get<int>(ctx, S_TF, 2 * (size_t)nsad);
   int* lf = get<int>(ctx, S_LF, 2 * (size_t)nsad);
   int* tv = get<int>(ctx, S_TV, 2 * (size_t)nsad);
   int* lv = get<int>(ctx, S_LV, 2 * (size_t)nsad);
   if (nsad > 0) {
-    LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(flow, H, W, nsad, csad, rmax, rmin, tf, lf, tv, lv, ncells,
-                                                          ctx->status));
+    LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(I, flow, nsad, csad, isad, rmax, rmin, tf, lf, tv, lv,
+                                                             ncells, ctx->status));
     LAUNCH_CHECK("saddle_walk_kernel");
   }
 
@@ -567,6 +685,8 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   V.M = nmin;
   F.crit = cmax;
   V.crit = cmin;
+  F.ext_img = imax;
+  V.ext_img = imin;
   F.val = vmax;
   V.val = vmin;
   F.rank_map = rmax;
@@ -575,21 +695,29 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
   F.steps = lf;
   V.t = tv;
   V.steps = lv;
-  F.arcs = dual ? f_valleys : f_ridges;
-  V.arcs = dual ? f_ridges : f_valleys;
-  F.groups = dual ? f_basins : f_peaks;
-  V.groups = dual ? f_peaks : f_basins;
+  // faces: ridges/peaks in the primal, valleys/basins in the dual (workspace.hxx:322-362)
+  F.arcs_primal = f_ridges;
+  F.arcs_dual = f_valleys;
+  V.arcs_primal = f_valleys;
+  V.arcs_dual = f_ridges;
+  F.groups_primal = f_peaks;
+  F.groups_dual = f_basins;
+  V.groups_primal = f_basins;
+  V.groups_dual = f_peaks;
+  for (Side* S : {&F, &V}) {
+    S->arcs = (S->arcs_primal && any_primal) || (S->arcs_dual && any_dual);
+    S->groups = (S->groups_primal && any_primal) || (S->groups_dual && any_dual);
+  }
 
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
   mark(ctx, 4, st);
   CK(cudaMemsetAsync(canc, 0, nsad + 4, st));
-  // sweep orders: minima = asc in the primal, reverse in the dual; maxima the reverse of minima
-  run_pairing(ctx, 0, F, asc, !dual, st);
+  run_pairing(ctx, 0, F, asc, st);
   mark(ctx, 5, st);
-  run_pairing(ctx, 1, V, asc, dual, st);
+  run_pairing(ctx, 1, V, asc, st);
   mark(ctx, 6, st);
 
-  // ---- surviving saddles in minima-sweep order ----
+  // ---- surviving saddles in minima-sweep (vertex side) order ----
   int* flag = get<int>(ctx, S_FLAG, nsad);
   int* fpos = get<int>(ctx, S_FPOS, nsad);
   ctx->surv = get<int>(ctx, S_SURV, nsad);
@@ -607,104 +735,156 @@ int extract_impl(dmsc_b200_context* ctx, const float* img, int H, int W, float t
     V.C = (int)ctx->pinned[2];
   }
   const int nsurv = ctx->nsurv;
+  LK(image_base_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, BS.sad, nsad, fpos, nsurv, BS.surv));
+  LAUNCH_CHECK("survivor bases");
   mark(ctx, 7, st);
 
   // ---- replay + final arc lengths ----
   for (int si = 0; si < 2; ++si) {
-    if (ctx->side[si].arcs && nsad > 0) run_replay(ctx, si, ctx->side[si], st);
+    Side& S = ctx->side[si];
+    if (S.arcs && nsad > 0) {
+      run_replay(ctx, si, S, st);
+    } else {
+      S.gbase = sget<long long>(ctx, si, X_GBASE, B + 1);
+      CK(cudaMemsetAsync(S.gbase, 0, (B + 1) * sizeof(long long), st));
+    }
     mark(ctx, 8 + si, st);
   }
 
-  // ---- labels (region id = rank among alive extrema) ----
+  // ---- labels (region id = rank among the image's alive extrema) ----
   for (int si = 0; si < 2; ++si) {
     Side& S = ctx->side[si];
-    if (!S.groups) continue;
-    int32_t* out = S.faces ? (dual ? basins_out : peaks_out) : (dual ? peaks_out : basins_out);
-    long long n = S.faces ? nidx : (long long)H * W;
     int* map = S.rank_map;  // dense ranks are no longer needed: reuse as the label map
-    if (S.M > 0) LK(label_map_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.crit, S.ut, S.to_out, map));
-    if (S.faces)
-      LK(label_kernel<true><<<grid_for(n, TB), TB, 0, st>>>(flow, H, W, map, out, ncells, ctx->status));
+    // alive bases first (needed by the labels and the outputs)
+    long long* at = get<long long>(ctx, S_TOT, 8) + 4 + si;
+    if (S.M > 0)
+      LK(u8_last_plus_kernel<<<1, 1, 0, st>>>(S.to_out_excl, S.alive, S.M, at));
     else
-      LK(label_kernel<false><<<grid_for(n, TB), TB, 0, st>>>(flow, H, W, map, out, ncells, ctx->status));
+      CK(cudaMemsetAsync(at, 0, sizeof(long long), st));
+    LK(image_base_dev_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, S.faces ? BS.max : BS.min, S.M, S.to_out_excl,
+                                                                   at, BS.alive[si]));
+    LAUNCH_CHECK("alive bases");
+    if (!S.groups) continue;
+    LabelOut O;
+    if (S.faces) {
+      O.primal = f_peaks ? peaks_out : nullptr;
+      O.dual = f_basins ? basins_out : nullptr;
+      O.primal_off = d_peaks_off;
+      O.dual_off = d_basins_off;
+    } else {
+      O.primal = f_basins ? basins_out : nullptr;
+      O.dual = f_peaks ? peaks_out : nullptr;
+      O.primal_off = d_basins_off;
+      O.dual_off = d_peaks_off;
+    }
+    if (S.M > 0)
+      LK(label_map_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.crit, S.ext_img, S.ut, S.to_out, BS.alive[si], map));
+    long long n = S.faces ? nidx : npx;
+    if (S.faces)
+      LK(label_kernel<true><<<grid_for(n, TB), TB, 0, st>>>(I, flow, n, map, O, ncells, ctx->status));
+    else
+      LK(label_kernel<false><<<grid_for(n, TB), TB, 0, st>>>(I, flow, n, map, O, ncells, ctx->status));
     LAUNCH_CHECK("label_kernel");
   }
-
   mark(ctx, 10, st);
-  // ---- e rows and alive counts ----
+
+  // ---- e rows ----
   for (int si = 0; si < 2; ++si) {
     Side& S = ctx->side[si];
     int* ec = sget<int>(ctx, si, X_EROWC, nsurv);
     S.erow_off = sget<int>(ctx, si, X_EROWO, nsurv);
+    long long* et = get<long long>(ctx, S_TOT, 8) + 6 + si;
     if (nsurv > 0) {
-      LK(erow_count_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, ctx->surv, S.t, S.ut, S.to_out, ec));
+      LK(erow_count_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, BS.surv, B, ctx->surv, S.t, S.ut,
+                                                               S.to_out, ec));
       excl_sum(ctx, ec, S.erow_off, nsurv, st);
-      LK(last_plus_kernel<int><<<1, 1, 0, st>>>(S.erow_off, ec, nsurv, tot + 2 * si));
+      LK(last_plus_kernel<int><<<1, 1, 0, st>>>(S.erow_off, ec, nsurv, et));
     } else {
-      CK(cudaMemsetAsync(tot + 2 * si, 0, sizeof(long long), st));
+      CK(cudaMemsetAsync(et, 0, sizeof(long long), st));
     }
-    if (S.M > 0)
-      LK(u8_last_plus_kernel<<<1, 1, 0, st>>>(S.to_out_excl, S.alive, S.M, tot + 2 * si + 1));
-    else
-      CK(cudaMemsetAsync(tot + 2 * si + 1, 0, sizeof(long long), st));
+    LK(image_base_dev_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, BS.surv, nsurv, S.erow_off, et, BS.erow[si]));
     LAUNCH_CHECK("e rows");
   }
-  readback(ctx, st, tot, 4);
-  F.n_erows = (int)ctx->pinned[0];
-  F.n_alive = (int)ctx->pinned[1];
-  V.n_erows = (int)ctx->pinned[2];
-  V.n_alive = (int)ctx->pinned[3];
-  mark(ctx, 11, st);
-  check_status(ctx, st);
 
-  // ---- sizes, public (primal / dual) naming ----
-  Side& PX = dual ? V : F;  // public "max" side
-  Side& PN = dual ? F : V;  // public "min" side
-  dmsc_b200_sizes z{};
-  z.max_pts = PX.n_alive;
-  z.min_pts = PN.n_alive;
-  z.sad_pts = nsurv;
-  z.e_max_rows = PX.n_erows;
-  z.e_min_rows = PN.n_erows;
-  z.p_max = z.p_min = z.ppairs_max = z.ppairs_min = nsurv;
-  z.grad_indices = ret_grad ? ncells : 0;
-  z.peaks_h = f_peaks ? (dual ? H : H + 1) : 0;
-  z.peaks_w = f_peaks ? (dual ? W : W + 1) : 0;
-  z.basins_h = f_basins ? (dual ? H + 1 : H) : 0;
-  z.basins_w = f_basins ? (dual ? W + 1 : W) : 0;
-  z.ridges = f_ridges ? PX.total : 0;
-  z.ridge_offsets = f_ridges ? nsurv + 1 : 0;
-  z.ridge_arc_offsets = f_ridges ? nsurv : 0;
-  z.valleys = f_valleys ? PN.total : 0;
-  z.valley_offsets = f_valleys ? nsurv + 1 : 0;
-  z.valley_arc_offsets = f_valleys ? nsurv : 0;
-  ctx->sizes = z;
-  *sizes = z;
+  // ---- per-image sizes: one read of the bases ----
+  {
+    size_t ib = 9 * (size_t)(B + 1) * sizeof(int), lb = 2 * (size_t)(B + 1) * sizeof(long long);
+    char* h = (char*)staging(ctx, ib + lb + 64);
+    CK(cudaMemcpyAsync(h, bases, ib, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h + ib, F.gbase, (B + 1) * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h + ib + (B + 1) * sizeof(long long), V.gbase, (B + 1) * sizeof(long long),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    mark(ctx, 11, st);
+    const int* hb = (const int*)h;
+    const int* hsurv = hb + 3 * (B + 1);
+    const int* hal[2] = {hb + 4 * (B + 1), hb + 5 * (B + 1)};
+    const int* her[2] = {hb + 6 * (B + 1), hb + 7 * (B + 1)};
+    const long long* hg[2] = {(const long long*)(h + ib), (const long long*)(h + ib) + (B + 1)};
+    ctx->sizes.assign(B, dmsc_b200_sizes{});
+    ctx->geom[0].assign(B, 0);
+    ctx->geom[1].assign(B, 0);
+    for (int b = 0; b < B; ++b) {
+      const bool dual = hdual[b];
+      const int PX = dual ? 1 : 0, PN = dual ? 0 : 1;  // public max / min side
+      const long long ns = hsurv[b + 1] - hsurv[b];
+      const long long H = hH[b], W = hW[b];
+      for (int si = 0; si < 2; ++si) ctx->geom[si][b] = hg[si][b + 1] - hg[si][b];
+      dmsc_b200_sizes z{};
+      z.max_pts = hal[PX][b + 1] - hal[PX][b];
+      z.min_pts = hal[PN][b + 1] - hal[PN][b];
+      z.sad_pts = ns;
+      z.e_max_rows = her[PX][b + 1] - her[PX][b];
+      z.e_min_rows = her[PN][b + 1] - her[PN][b];
+      z.p_max = z.p_min = z.ppairs_max = z.ppairs_min = ns;
+      z.grad_indices = ret_grad ? 4 * (H + 1) * (W + 1) : 0;
+      z.peaks_h = f_peaks ? (dual ? H : H + 1) : 0;
+      z.peaks_w = f_peaks ? (dual ? W : W + 1) : 0;
+      z.basins_h = f_basins ? (dual ? H + 1 : H) : 0;
+      z.basins_w = f_basins ? (dual ? W + 1 : W) : 0;
+      z.ridges = f_ridges ? ctx->geom[PX][b] : 0;
+      z.ridge_offsets = f_ridges ? ns + 1 : 0;
+      z.ridge_arc_offsets = f_ridges ? ns : 0;
+      z.valleys = f_valleys ? ctx->geom[PN][b] : 0;
+      z.valley_offsets = f_valleys ? ns + 1 : 0;
+      z.valley_arc_offsets = f_valleys ? ns : 0;
+      ctx->sizes[b] = z;
+      sizes_out[b] = z;
+    }
+  }
+  check_status(ctx, st);
   ctx->valid = true;
   return kOk;
 }
 
-void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* offsets, int32_t* arc_offsets,
-               cudaStream_t st) {
-  const int nsurv = ctx->nsurv;
-  long long* send = sget<long long>(ctx, si, X_SEND, nsurv);
-  if (offsets)
-    LK(arc_offsets_kernel<<<grid_for(nsurv + 1LL, TB), TB, 0, st>>>(nsurv, S.arc_len, send, offsets, arc_offsets));
+// Geometry of one side: positions, CSR offsets and the expansion kernels.
+void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, int32_t* flat_dual, const int* dst_off,
+               Route OFF, Route AOFF, cudaStream_t st) {
+  const int nsurv = ctx->nsurv, B = ctx->B;
+  if (nsurv > 0)
+    LK(arc_offsets_kernel<<<grid_for(nsurv + (long long)B, TB), TB, 0, st>>>(
+        nsurv, B, ctx->bases.surv, ctx->I.dual, S.arc_len, S.send, S.gbase, OFF, AOFF));
+  else
+    LK(arc_offsets_kernel<<<grid_for((long long)B, TB), TB, 0, st>>>(0, B, ctx->bases.surv, ctx->I.dual, S.arc_len,
+                                                                     S.send, S.gbase, OFF, AOFF));
   LAUNCH_CHECK("arc_offsets_kernel");
-  if (S.total <= 0 || !flat) return;
+  if (S.total <= 0 || (!flat_primal && !flat_dual)) return;
+  long long* arc_pos = sget<long long>(ctx, si, X_APOS, 2 * (size_t)nsurv);
+  LK(arc_pos_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.send, ctx->surv, ctx->sad_img, S.gbase,
+                                                        dst_off, arc_pos));
   long long cap = S.total;
   EmitArgs A;
   EmitCtx& E = A.E;
   E.flow = ctx->flow;
   E.crit_sad = ctx->crit_sad;
-  E.H = ctx->H;
-  E.W = ctx->W;
-  E.Nx = ctx->W + 1;
+  E.I = ctx->I;
+  E.sad_img = ctx->sad_img;
   E.faces = S.faces;
   E.t = S.t;
   E.blen = S.blen;
   E.S = S.R;
-  E.out = flat;
+  E.out_primal = flat_primal;
+  E.out_dual = flat_dual;
   E.q_out = nullptr;
   E.n_out = nullptr;
   E.q_cap = cap;
@@ -712,7 +892,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   E.status = ctx->status;
   A.nsurv = nsurv;
   A.surv_sad = ctx->surv;
-  A.arc_pos = S.arc_pos;
+  A.arc_pos = arc_pos;
   A.arc_cl = S.arc_cl;
   A.arc_root = S.arc_root;
   A.q0 = sget<int4>(ctx, si, X_Q0, cap);
@@ -734,35 +914,76 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat, int32_t* 
   }
 }
 
-int fetch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t st) {
+int fetch_batch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t st) {
   if (!ctx->valid || !o) {
     set_err(ctx, "fetch without a successful extract");
     return kErrInvalidArgument;
   }
   CK(cudaSetDevice(ctx->device));
   mark(ctx, 12, st);
-  const bool dual = ctx->dual;
-  const int nsurv = ctx->nsurv;
-  Side& F = ctx->side[0];
-  Side& V = ctx->side[1];
+  const int B = ctx->B, nsurv = ctx->nsurv;
+  const Imgs I = ctx->I;
+  // per-image offsets of every output, and their per-side routes
+  enum { R_PTS0, R_PTS1, R_E0, R_E1, R_G0, R_G1, R_OFF0, R_OFF1, R_AOFF0, R_AOFF1, R_N };
+  std::vector<int> route((size_t)R_N * B);
+  {
+    long long mx = 0, mn = 0, ex = 0, en = 0, rg = 0, vl = 0, ro = 0, vo = 0, ra = 0, va = 0;
+    for (int b = 0; b < B; ++b) {
+      const dmsc_b200_sizes& z = ctx->sizes[b];
+      const bool d = ctx->hdual[b];
+      // side 0 (faces) is the public max side in the primal, min side in the dual
+      route[R_PTS0 * B + b] = (int)(d ? mn : mx);
+      route[R_PTS1 * B + b] = (int)(d ? mx : mn);
+      route[R_E0 * B + b] = (int)(2 * (d ? en : ex));
+      route[R_E1 * B + b] = (int)(2 * (d ? ex : en));
+      route[R_G0 * B + b] = (int)(d ? vl : rg);
+      route[R_G1 * B + b] = (int)(d ? rg : vl);
+      route[R_OFF0 * B + b] = (int)(d ? vo : ro);
+      route[R_OFF1 * B + b] = (int)(d ? ro : vo);
+      route[R_AOFF0 * B + b] = (int)(d ? va : ra);
+      route[R_AOFF1 * B + b] = (int)(d ? ra : va);
+      mx += z.max_pts;
+      mn += z.min_pts;
+      ex += z.e_max_rows;
+      en += z.e_min_rows;
+      rg += z.ridges;
+      vl += z.valleys;
+      ro += z.ridge_offsets;
+      vo += z.valley_offsets;
+      ra += z.ridge_arc_offsets;
+      va += z.valley_arc_offsets;
+    }
+    size_t bytes = route.size() * sizeof(int);
+    void* h = staging(ctx, bytes);
+    memcpy(h, route.data(), bytes);
+    int* d = get<int>(ctx, S_ROUTE, route.size());
+    CK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+  }
+  const int* rt = (const int*)ctx->bufs[S_ROUTE].p;
+  auto rt_of = [&](int k) { return rt + (size_t)k * B; };
   // extrema lists
-  int32_t* fpts = dual ? o->min_pts : o->max_pts;
-  int32_t* vpts = dual ? o->max_pts : o->min_pts;
-  if (F.M > 0 && fpts)
-    LK(compact_alive_kernel<<<grid_for(F.M, TB), TB, 0, st>>>(F.M, F.alive, F.to_out_excl, F.crit, fpts, F.to_out));
-  if (V.M > 0 && vpts)
-    LK(compact_alive_kernel<<<grid_for(V.M, TB), TB, 0, st>>>(V.M, V.alive, V.to_out_excl, V.crit, vpts, V.to_out));
+  for (int si = 0; si < 2; ++si) {
+    Side& S = ctx->side[si];
+    Route R{S.faces ? o->max_pts : o->min_pts, S.faces ? o->min_pts : o->max_pts, rt_of(si == 0 ? R_PTS0 : R_PTS1)};
+    if (S.M > 0)
+      LK(points_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.alive, S.to_out_excl, ctx->bases.alive[si], S.crit,
+                                                         S.ext_img, I, R));
+  }
   if (nsurv > 0 && o->sad_pts)
-    LK(sad_pts_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->crit_sad, o->sad_pts));
+    LK(sad_pts_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->crit_sad, ctx->sad_img,
+                                                          ctx->bases.surv, I, o->sad_pts, ctx->bases.surv));
   LAUNCH_CHECK("point lists");
   // per-saddle scalars and e rows
   if (nsurv > 0) {
-    LK(side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(
-        nsurv, true, ctx->surv, F.t, F.ut, F.to_out, F.pers, F.pair_dense, F.erow_off, dual ? o->p_min : o->p_max,
-        dual ? o->ppairs_min : o->ppairs_max, F.n_erows > 0 ? (dual ? o->e_min : o->e_max) : nullptr));
-    LK(side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(
-        nsurv, false, ctx->surv, V.t, V.ut, V.to_out, V.pers, V.pair_dense, V.erow_off, dual ? o->p_max : o->p_min,
-        dual ? o->ppairs_max : o->ppairs_min, V.n_erows > 0 ? (dual ? o->e_max : o->e_min) : nullptr));
+    for (int si = 0; si < 2; ++si) {
+      Side& S = ctx->side[si];
+      RouteF P{S.faces ? o->p_max : o->p_min, S.faces ? o->p_min : o->p_max, ctx->bases.surv};
+      Route PP{S.faces ? o->ppairs_max : o->ppairs_min, S.faces ? o->ppairs_min : o->ppairs_max, ctx->bases.surv};
+      Route E{S.faces ? o->e_max : o->e_min, S.faces ? o->e_min : o->e_max, rt_of(si == 0 ? R_E0 : R_E1)};
+      LK(side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(
+          nsurv, S.faces, ctx->bases.surv, I, ctx->surv, S.t, S.ut, S.to_out, ctx->bases.alive[si], S.pers,
+          S.pair_dense, S.erow_off, ctx->bases.erow[si], P, PP, E));
+    }
     LAUNCH_CHECK("side_outputs_kernel");
   }
   mark(ctx, 13, st);
@@ -770,15 +991,24 @@ int fetch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t 
   for (int si = 0; si < 2; ++si) {
     Side& S = ctx->side[si];
     if (!S.arcs) continue;
-    bool ridges = S.faces != dual;  // faces are ridges in the primal
-    int32_t* flat = ridges ? o->ridges : o->valleys;
-    int32_t* offs = ridges ? o->ridge_offsets : o->valley_offsets;
-    int32_t* aoffs = ridges ? o->ridge_arc_offsets : o->valley_arc_offsets;
-    if (ctx->nsad == 0) {
-      if (offs) CK(cudaMemsetAsync(offs, 0, sizeof(int32_t), st));
-      continue;
+    // faces: ridges in the primal, valleys in the dual
+    int32_t* gp = S.faces ? o->ridges : o->valleys;
+    int32_t* gd = S.faces ? o->valleys : o->ridges;
+    Route OFF{S.faces ? o->ridge_offsets : o->valley_offsets, S.faces ? o->valley_offsets : o->ridge_offsets,
+              rt_of(si == 0 ? R_OFF0 : R_OFF1)};
+    Route AOFF{S.faces ? o->ridge_arc_offsets : o->valley_arc_offsets,
+               S.faces ? o->valley_arc_offsets : o->ridge_arc_offsets, rt_of(si == 0 ? R_AOFF0 : R_AOFF1)};
+    if (!S.arcs_primal) {
+      gp = nullptr;
+      OFF.primal = nullptr;
+      AOFF.primal = nullptr;
     }
-    emit_side(ctx, si, S, flat, offs, aoffs, st);
+    if (!S.arcs_dual) {
+      gd = nullptr;
+      OFF.dual = nullptr;
+      AOFF.dual = nullptr;
+    }
+    emit_side(ctx, si, S, gp, gd, rt_of(si == 0 ? R_G0 : R_G1), OFF, AOFF, st);
   }
   mark(ctx, 14, st);
   check_status(ctx, st);
@@ -786,6 +1016,7 @@ int fetch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t 
 }
 
 }  // namespace
+
 
 extern "C" {
 
@@ -799,6 +1030,7 @@ int dmsc_b200_create(dmsc_b200_context** out, int device) {
     delete c;
     return kErrCuda;
   }
+  c->pinned_cap = 64 * sizeof(long long);
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
   {
     std::vector<uint32_t> lut(kFifoTable);
@@ -833,7 +1065,9 @@ int dmsc_b200_extract(dmsc_b200_context* ctx, const float* image, int H, int W, 
   if (!ctx) return kErrInvalidArgument;
   ctx->err.clear();
   try {
-    return extract_impl(ctx, image, H, W, thr, flags, grad_out, peaks_out, basins_out, sizes, (cudaStream_t)stream);
+    const unsigned char dual = (flags & DMSC_B200_DUAL) ? 1 : 0;
+    return extract_batch_impl(ctx, 1, image, &H, &W, &thr, &dual, flags, grad_out, peaks_out, basins_out, sizes,
+                              (cudaStream_t)stream);
   } catch (const Fail& f) {
     ctx->valid = false;
     return f.code;
@@ -844,8 +1078,22 @@ int dmsc_b200_fetch(dmsc_b200_context* ctx, const dmsc_b200_outputs* out, void* 
   if (!ctx) return kErrInvalidArgument;
   ctx->err.clear();
   try {
-    return fetch_impl(ctx, out, (cudaStream_t)stream);
+    return fetch_batch_impl(ctx, out, (cudaStream_t)stream);
   } catch (const Fail& f) {
+    return f.code;
+  }
+}
+
+int dmsc_b200_extract_batch(dmsc_b200_context* ctx, const float* images, int B, const int* H, const int* W,
+                            const float* thresholds, const unsigned char* is_dual, unsigned flags, int32_t* grad_out,
+                            int32_t* peaks_out, int32_t* basins_out, dmsc_b200_sizes* sizes, void* stream) {
+  if (!ctx) return kErrInvalidArgument;
+  ctx->err.clear();
+  try {
+    return extract_batch_impl(ctx, B, images, H, W, thresholds, is_dual, flags, grad_out, peaks_out, basins_out,
+                              sizes, (cudaStream_t)stream);
+  } catch (const Fail& f) {
+    ctx->valid = false;
     return f.code;
   }
 }

@@ -221,7 +221,61 @@ __device__ __forceinline__ void lower_star(const float (*sv)[kValX], int y, int 
   }
 }
 
-// K1: gradient over one 32 x 8 index tile per CTA (320 threads).
+// Lower stars of one 32 x 16 index tile into the slot-major shared tile.
+template <bool DUAL>
+__device__ __forceinline__ void gradient_tile(const float* __restrict__ img, int H, int W, int y0, int x0, int tid,
+                                              float (*sv)[kValX], int (*tile)[kTileY][kTileX],
+                                              const uint32_t* __restrict__ fifo_lut) {
+  for (int i = tid; i < kValY * kValX; i += kGradThreads) {
+    int r = i / kValX, c = i - r * kValX;
+    int gy = y0 - 2 + r, gx = x0 - 2 + c;
+    sv[r][c] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(img + (size_t)gy * W + gx) : 0.0f;
+  }
+  for (int i = tid; i < 4 * kTileY * kTileX; i += kGradThreads) (&tile[0][0][0])[i] = -1;
+  __syncthreads();
+  if (tid < (kTileY + 1) * (kTileX + 1)) {
+    int r = tid / (kTileX + 1), c = tid - r * (kTileX + 1);
+    int y = y0 - 1 + r, x = x0 - 1 + c;
+    if (y >= 0 && y < H && x >= 0 && x < W) lower_star<DUAL>(sv, y, x, H, W, W + 1, y0, x0, tile, fifo_lut);
+  }
+  __syncthreads();
+}
+
+// Write-out of one tile row by one warp: coalesced int4 gradient stores at
+// global index base `gbase`, criticality mask, flow codes and the row
+// segment's counts (segment id `seg`).
+__device__ __forceinline__ void gradient_store_row(const int (*tile)[kTileY][kTileX], int warp, int lane, int H,
+                                                   int W, int iy, int ix, long long gbase, int seg,
+                                                   int4* __restrict__ grad, uint8_t* __restrict__ crit_mask,
+                                                   uint8_t* __restrict__ flow, int* __restrict__ seg_min,
+                                                   int* __restrict__ seg_sad, int* __restrict__ seg_max) {
+  const int Nx = W + 1;
+  bool in = ix <= W;
+  int4 v = make_int4(tile[0][warp][lane], tile[1][warp][lane], tile[2][warp][lane], tile[3][warp][lane]);
+  unsigned m = 0;
+  if (in) {
+    const int lidx = iy * Nx + ix;  // image-local index: the cell ids in v are local
+    const size_t gidx = (size_t)(gbase + lidx);
+    grad[gidx] = v;
+    if (v.x == -1 && iy < H && ix < W) m |= 1u;
+    if (v.y == -1 && iy < H) m |= 2u;
+    if (v.z == -1 && ix < W) m |= 4u;
+    if (v.w == -1) m |= 8u;
+    crit_mask[gidx] = (uint8_t)m;
+    flow[gidx] = (uint8_t)(vertex_flow(v.x, lidx) | (face_flow(v.w, lidx) << 4));
+  }
+  unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
+  unsigned bs1 = __ballot_sync(0xffffffffu, m & 2u);
+  unsigned bs2 = __ballot_sync(0xffffffffu, m & 4u);
+  unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
+  if (lane == 0) {
+    seg_min[seg] = __popc(bmin);
+    seg_sad[seg] = __popc(bs1) + __popc(bs2);
+    seg_max[seg] = __popc(bmax);
+  }
+}
+
+// K1 (one image): gradient over one 32 x 16 index tile per CTA.
 template <bool DUAL>
 __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __restrict__ img, int H, int W,
                                                                int4* __restrict__ grad,
@@ -234,51 +288,45 @@ __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __r
   __shared__ int tile[4][kTileY][kTileX];  // slot-major: conflict-free per-slot writes
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY;
-  const int Nx = W + 1;
-
-  for (int i = tid; i < kValY * kValX; i += kGradThreads) {
-    int r = i / kValX, c = i - r * kValX;
-    int gy = y0 - 2 + r, gx = x0 - 2 + c;
-    sv[r][c] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(img + (size_t)gy * W + gx) : 0.0f;
-  }
-  for (int i = tid; i < 4 * kTileY * kTileX; i += kGradThreads) (&tile[0][0][0])[i] = -1;
-  __syncthreads();
-
-  if (tid < (kTileY + 1) * (kTileX + 1)) {
-    int r = tid / (kTileX + 1), c = tid - r * (kTileX + 1);
-    int y = y0 - 1 + r, x = x0 - 1 + c;
-    if (y >= 0 && y < H && x >= 0 && x < W) lower_star<DUAL>(sv, y, x, H, W, Nx, y0, x0, tile, fifo_lut);
-  }
-  __syncthreads();
-
-  // one warp per tile row: coalesced int4 stores, criticality mask and counts
+  gradient_tile<DUAL>(img, H, W, y0, x0, tid, sv, tile, fifo_lut);
   const int warp = tid >> 5, lane = tid & 31;
   if (warp >= kTileY) return;
   const int iy = y0 + warp, ix = x0 + lane;
   if (iy > H) return;
-  bool in = ix <= W;
-  int4 v = make_int4(tile[0][warp][lane], tile[1][warp][lane], tile[2][warp][lane], tile[3][warp][lane]);
-  unsigned m = 0;
-  if (in) {
-    size_t idx = (size_t)iy * Nx + ix;
-    grad[idx] = v;
-    if (v.x == -1 && iy < H && ix < W) m |= 1u;
-    if (v.y == -1 && iy < H) m |= 2u;
-    if (v.z == -1 && ix < W) m |= 4u;
-    if (v.w == -1) m |= 8u;
-    crit_mask[idx] = (uint8_t)m;
-    flow[idx] = (uint8_t)(vertex_flow(v.x, (int)idx) | (face_flow(v.w, (int)idx) << 4));
-  }
-  unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
-  unsigned bs1 = __ballot_sync(0xffffffffu, m & 2u);
-  unsigned bs2 = __ballot_sync(0xffffffffu, m & 4u);
-  unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
-  if (lane == 0) {
-    int seg = iy * gridDim.x + blockIdx.x;
-    seg_min[seg] = __popc(bmin);
-    seg_sad[seg] = __popc(bs1) + __popc(bs2);
-    seg_max[seg] = __popc(bmax);
-  }
+  gradient_store_row(tile, warp, lane, H, W, iy, ix, 0, iy * gridDim.x + blockIdx.x, grad, crit_mask, flow,
+                     seg_min, seg_sad, seg_max);
+}
+
+// K1 (batch): the tiles of every image of a batch in one 1-D grid; each CTA
+// finds its image from the tile bases.
+static __global__ void __launch_bounds__(kGradThreads) gradient_batch_kernel(Imgs I, const float* __restrict__ img_all,
+                                                                     int4* __restrict__ grad,
+                                                                     uint8_t* __restrict__ crit_mask,
+                                                                     int* __restrict__ seg_min,
+                                                                     int* __restrict__ seg_sad,
+                                                                     int* __restrict__ seg_max,
+                                                                     const uint32_t* __restrict__ fifo_lut,
+                                                                     uint8_t* __restrict__ flow) {
+  __shared__ float sv[kValY][kValX];
+  __shared__ int tile[4][kTileY][kTileX];
+  const int tid = threadIdx.x;
+  const int b = find_image(I.tile_base, I.B, blockIdx.x);
+  const int H = I.H[b], W = I.W[b];
+  const int ntx = (W + 1 + kTileX - 1) / kTileX;
+  const int t = blockIdx.x - I.tile_base[b];
+  const int ty = t / ntx, tx = t - ty * ntx;
+  const int x0 = tx * kTileX, y0 = ty * kTileY;
+  const float* img = img_all + I.px_base[b];
+  if (I.dual[b])
+    gradient_tile<true>(img, H, W, y0, x0, tid, sv, tile, fifo_lut);
+  else
+    gradient_tile<false>(img, H, W, y0, x0, tid, sv, tile, fifo_lut);
+  const int warp = tid >> 5, lane = tid & 31;
+  if (warp >= kTileY) return;
+  const int iy = y0 + warp, ix = x0 + lane;
+  if (iy > H) return;
+  gradient_store_row(tile, warp, lane, H, W, iy, ix, I.idx_base[b], I.seg_base[b] + iy * ntx + tx, grad, crit_mask,
+                     flow, seg_min, seg_sad, seg_max);
 }
 
 // cell_value (cpu/cell_compare.hxx:82-87): value of the highest (dual: lowest)
@@ -339,26 +387,34 @@ __device__ __forceinline__ float cell_value_g(const float* __restrict__ img, int
   return bv;
 }
 
-// K2: ordered compaction. One warp per (row, 32-column) segment; segment
-// offsets are exclusive scans of the per-segment counts. Writes the three
-// ascending-cell-id lists, the index -> dense-rank maps of the extrema, the
-// extremum values and the saddle values with their radix-sort keys.
-template <bool DUAL>
-__global__ void __launch_bounds__(256) compact_kernel(
-    const float* __restrict__ img, int H, int W, int nsegx, long long nseg, const uint8_t* __restrict__ crit_mask,
+// K2: ordered compaction. One warp per (row, 32-column) segment of an image;
+// segment offsets are exclusive scans of the per-segment counts over the
+// whole batch (images in order, rows in order), so each image's lists are a
+// contiguous slice in ascending cell-id order. Writes the three lists as
+// global cell ids, each critical cell's image, the index -> dense-rank maps of
+// the extrema, the extremum values and the saddle values with their sort keys
+// (image id above the orderable value, so one sort orders every image).
+static __global__ void __launch_bounds__(256) compact_kernel(
+    Imgs I, const float* __restrict__ img_all, long long nseg, const uint8_t* __restrict__ crit_mask,
     const int* __restrict__ off_min, const int* __restrict__ off_sad, const int* __restrict__ off_max,
-    int* __restrict__ crit_min, int* __restrict__ crit_sad, int* __restrict__ crit_max, int* __restrict__ min_rank,
-    int* __restrict__ max_rank, float* __restrict__ min_val, float* __restrict__ max_val, float* __restrict__ sad_val,
-    uint32_t* __restrict__ sad_key) {
+    int* __restrict__ crit_min, int* __restrict__ crit_sad, int* __restrict__ crit_max, int* __restrict__ min_img,
+    int* __restrict__ sad_img, int* __restrict__ max_img, int* __restrict__ min_rank, int* __restrict__ max_rank,
+    float* __restrict__ min_val, float* __restrict__ max_val, float* __restrict__ sad_val,
+    unsigned long long* __restrict__ sad_key) {
   const int lane = threadIdx.x & 31;
   long long seg = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (seg >= nseg) return;
-  const int Nx = W + 1;
-  int iy = (int)(seg / nsegx), sx = (int)(seg - (long long)iy * nsegx);
+  const int b = find_image(I.seg_base, I.B, seg);
+  const int H = I.H[b], W = I.W[b], Nx = W + 1;
+  const bool dual = I.dual[b];
+  const int nsegx = (W + 1 + kTileX - 1) / kTileX;
+  const long long lseg = seg - I.seg_base[b];
+  int iy = (int)(lseg / nsegx), sx = (int)(lseg - (long long)iy * nsegx);
   int ix = sx * kTileX + lane;
   unsigned m = 0;
-  size_t idx = (size_t)iy * Nx + ix;
-  if (ix <= W) m = crit_mask[idx];
+  const long long gidx = (long long)I.idx_base[b] + (long long)iy * Nx + ix;
+  const float* img = img_all + I.px_base[b];
+  if (ix <= W) m = crit_mask[gidx];
   unsigned lt = (1u << lane) - 1u;
   unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
   unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
@@ -372,29 +428,28 @@ __global__ void __launch_bounds__(256) compact_kernel(
   int excl = incl - ns;
   if (m & 1u) {
     int p = off_min[seg] + __popc(bmin & lt);
-    crit_min[p] = (int)(4 * idx);
-    min_rank[idx] = p;
+    crit_min[p] = (int)(4 * gidx);
+    min_img[p] = b;
+    min_rank[gidx] = p;
     min_val[p] = __ldg(img + (size_t)iy * W + ix);
   }
   if (m & 8u) {
     int p = off_max[seg] + __popc(bmax & lt);
-    crit_max[p] = (int)(4 * idx + 3);
-    max_rank[idx] = p;
-    max_val[p] = cell_value_g<DUAL>(img, 3, iy, ix, H, W);
+    crit_max[p] = (int)(4 * gidx + 3);
+    max_img[p] = b;
+    max_rank[gidx] = p;
+    max_val[p] = dual ? cell_value_g<true>(img, 3, iy, ix, H, W) : cell_value_g<false>(img, 3, iy, ix, H, W);
   }
   int p = off_sad[seg] + excl;
-  if (m & 2u) {
-    crit_sad[p] = (int)(4 * idx + 1);
-    float v = cell_value_g<DUAL>(img, 1, iy, ix, H, W);
+#pragma unroll
+  for (int t = 1; t <= 2; ++t) {
+    if (!(m & (1u << t))) continue;
+    crit_sad[p] = (int)(4 * gidx + t);
+    sad_img[p] = b;
+    float v = dual ? cell_value_g<true>(img, t, iy, ix, H, W) : cell_value_g<false>(img, t, iy, ix, H, W);
     sad_val[p] = v;
-    sad_key[p] = orderable_key(v);
+    sad_key[p] = ((unsigned long long)b << 32) | orderable_key(v);
     p++;
-  }
-  if (m & 4u) {
-    crit_sad[p] = (int)(4 * idx + 2);
-    float v = cell_value_g<DUAL>(img, 2, iy, ix, H, W);
-    sad_val[p] = v;
-    sad_key[p] = orderable_key(v);
   }
 }
 

@@ -32,15 +32,14 @@ namespace dmsc {
 constexpr uint32_t kNoEdge = 0xFFFFFFFFu;
 constexpr int kUndecided = -2;
 
-// older(a, b) for extremum dense indices; `void_id` is older than all.
-// OLDER_LESS: older = smaller (value, cell) under value_less (minima side in
-// the primal, maxima side in the dual).
-template <bool OLDER_LESS>
+// older(a, b) for extremum dense indices of one image; `void_id` is older
+// than all. Older = smaller (value, cell) under value_less on the vertex side
+// in the primal and the face side in the dual, larger otherwise.
 __device__ __forceinline__ bool older(int a, int b, int void_id, const float* __restrict__ val,
-                                      const int* __restrict__ cell) {
+                                      const int* __restrict__ cell, bool older_less) {
   if (a == void_id) return b != void_id;
   if (b == void_id) return false;
-  return OLDER_LESS ? tie_lt(val[a], cell[a], val[b], cell[b]) : tie_lt(val[b], cell[b], val[a], cell[a]);
+  return older_less ? tie_lt(val[a], cell[a], val[b], cell[b]) : tie_lt(val[b], cell[b], val[a], cell[a]);
 }
 
 __global__ void iota_kernel(int* __restrict__ a, int n) {
@@ -58,24 +57,33 @@ __global__ void fill_kernel(int* __restrict__ a, long long n, int v) {
   if (i < n) a[i] = v;
 }
 
-// Builds the sweep-ordered edge list of one side: edge j is saddle
-// sweep[j] with ends (t[2s], t[2s+1]). The round loop itself is
-// pairing_persistent_kernel (persistent.cuh).
-__global__ void sweep_edges_kernel(int nsad, const int* __restrict__ asc, bool reverse, const int* __restrict__ t,
-                                   int* __restrict__ sweep, int* __restrict__ c1, int* __restrict__ c2,
-                                   int* __restrict__ dying) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nsad) return;
-  int s = reverse ? asc[nsad - 1 - j] : asc[j];
-  sweep[j] = s;
-  c1[j] = t[2 * s];
-  c2[j] = t[2 * s + 1];
-  dying[j] = kUndecided;
+// Sweep-ordered edge list of one side for a batch. `asc` lists every image's
+// saddles in ascending (s_val, cell id), images in order; the face side sweeps
+// each image descending in the primal and ascending in the dual, the vertex
+// side the reverse (cpu/arcs_topology.hxx:99-102, 142). Edge q is saddle
+// sweep[q] with ends (t[2s], t[2s+1]); an image's edges stay contiguous.
+__global__ void sweep_edges_kernel(int nsad, const int* __restrict__ asc, const int* __restrict__ sad_img,
+                                   const int* __restrict__ sad_base, const uint8_t* __restrict__ dual, bool faces,
+                                   const int* __restrict__ t, int* __restrict__ sweep, int* __restrict__ c1,
+                                   int* __restrict__ c2) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nsad) return;
+  int s = asc[p];
+  int b = sad_img[s];
+  int base = sad_base[b], n = sad_base[b + 1] - base;
+  bool rev = faces ? !dual[b] : dual[b];
+  int q = rev ? base + n - 1 - (p - base) : p;
+  sweep[q] = s;
+  c1[q] = t[2 * s];
+  c2[q] = t[2 * s + 1];
 }
 
 // Persistence of each decided saddle and cancellation (persistence.hxx:82-104,
-// 139-161). MIN_SIDE selects the formula; `sbit` marks the side in `cancelled`.
-__global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_side, bool dual, float thr,
+// 139-161), with the saddle's image's orientation and threshold; `sbit` marks
+// the side in `cancelled`.
+__global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_side, const uint8_t* __restrict__ dual,
+                                                          const float* __restrict__ thr,
+                                                          const int* __restrict__ sad_img,
                                                           const int* __restrict__ sweep,
                                                           const int* __restrict__ dying,
                                                           const float* __restrict__ sad_val,
@@ -91,15 +99,17 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
       pair_dense[s] = -1;
       pers[s] = -1.0f;
     } else {
+      const int b = sad_img[s];
+      const bool du = dual[b];
       float sv = sad_val[s], ev = ext_val[d];
       float p;
       if (min_side)
-        p = dual ? sub_like_host(ev, sv) : sub_like_host(sv, ev);
+        p = du ? sub_like_host(ev, sv) : sub_like_host(sv, ev);
       else
-        p = dual ? sub_like_host(sv, ev) : sub_like_host(ev, sv);
+        p = du ? sub_like_host(sv, ev) : sub_like_host(ev, sv);
       pair_dense[s] = d;
       pers[s] = p;
-      if (p <= thr) {
+      if (p <= thr[b]) {
         canc = true;
         atomicOr((unsigned*)(cancelled + (s & ~3)), (unsigned)sbit << (8 * (s & 3)));
         alive[d] = 0;
@@ -124,11 +134,14 @@ __device__ __forceinline__ int uf_root(int* p, int x) {
 __global__ void __launch_bounds__(256) ut_union_kernel(int nsad, const int* __restrict__ sweep,
                                                        const int* __restrict__ dying, const int* __restrict__ c1,
                                                        const int* __restrict__ c2, const float* __restrict__ pers,
-                                                       float thr, int void_id, int* __restrict__ p) {
+                                                       const float* __restrict__ thr,
+                                                       const int* __restrict__ sad_img, int void_id,
+                                                       int* __restrict__ p) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nsad) return;
   if (dying[j] < 0) return;
-  if (!(pers[sweep[j]] <= thr)) return;
+  const int s = sweep[j];
+  if (!(pers[s] <= thr[sad_img[s]])) return;
   int a = c1[j] < 0 ? void_id : c1[j];
   int b = c2[j] < 0 ? void_id : c2[j];
   while (true) {

@@ -66,6 +66,9 @@ struct PairArgs {
   int* cnt;           // [0..2] rotating active counts, [3..5] rotating root counts
   const float* val;
   const int* cell;
+  const int* ext_img;    // [M] image of each extremum
+  const uint8_t* dual;   // [B] orientation of each image
+  bool faces;            // face side (maxima in the primal) or vertex side
   unsigned* status;
   int max_rounds;
   int* rounds;                   // receives the number of rounds (statistics)
@@ -79,7 +82,6 @@ struct PairArgs {
 // live otherwise; roots without outgoing saddles leave the list for good;
 // (B2) the links are applied. Round 0 skips the lookups: all groups are
 // single extrema.
-template <bool OLDER_LESS>
 __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
@@ -169,7 +171,10 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
           int e = (int)me;
           int ga = A.g1[e], gb = A.g2[e];  // roots as of phase A; links change only in B2
           h = (ga == g) ? gb : ga;
-          if (older<OLDER_LESS>(h, g, M, A.val, A.cell)) {
+          // g is an extremum of one image (the void never dies); older = value_less
+          // order on the vertex side in the primal and the face side in the dual
+          const bool du = g < M && A.dual[A.ext_img[g]];
+          if (older(h, g, M, A.val, A.cell, A.faces ? du : !du)) {
             A.dying[e] = g;
           } else {
             h = -1;
@@ -328,7 +333,10 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
     if (q < 2LL * A.nsurv) {
       int i = (int)(q >> 1), j = (int)(q & 1);
       int s = A.surv_sad[i];
-      if (E.t[2 * s + j] >= 0) {
+      // images whose output takes none of this side's arcs emit nothing
+      const int b = E.sad_img[s];
+      const bool takes = (E.I.dual[b] ? E.out_dual : E.out_primal) != nullptr;
+      if (takes && E.t[2 * s + j] >= 0) {
         long long pos = A.arc_pos[q];
         seg = E.blen[2 * s + j] > 0;
         btask = make_task(kTaskBase, 0, s, j, pos);

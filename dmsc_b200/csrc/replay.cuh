@@ -85,7 +85,9 @@ __device__ __forceinline__ bool walk_root(const ReplayState& S, int x, unsigned 
 // unique and the target cell never breaks a tie.
 __global__ void __launch_bounds__(256) cancel_collect_kernel(int nsad, const int* __restrict__ sweep,
                                                              const int* __restrict__ dying,
-                                                             const float* __restrict__ pers, float thr,
+                                                             const float* __restrict__ pers,
+                                                             const float* __restrict__ thr,
+                                                             const int* __restrict__ sad_img,
                                                              const int* __restrict__ crit_sad,
                                                              unsigned long long* __restrict__ keys,
                                                              int* __restrict__ vals, int* __restrict__ count) {
@@ -94,7 +96,7 @@ __global__ void __launch_bounds__(256) cancel_collect_kernel(int nsad, const int
   unsigned long long key = 0;
   if (j < nsad && dying[j] >= 0) {
     float p = pers[sweep[j]];
-    if (p <= thr) {
+    if (p <= thr[sad_img[sweep[j]]]) {
       take = true;
       key = ((unsigned long long)orderable_key(p) << 32) | (unsigned)crit_sad[sweep[j]];
     }
@@ -117,16 +119,19 @@ __global__ void base_len_kernel(int n2, const int* __restrict__ t, const int* __
 
 // Final arcs of the surviving saddles: length and the chain root of each
 // (survivor i in output order, arc j). `surv_sad[i]` = dense saddle index.
-__global__ void final_arcs_kernel(int nsurv, const int* __restrict__ surv_sad, const int* __restrict__ t,
-                                  const long long* __restrict__ blen, ReplayState S, int max_steps,
-                                  long long* __restrict__ arc_len, long long* __restrict__ arc_cl,
+// Images whose output does not take this side's arcs (`arcs_primal` /
+// `arcs_dual` by orientation) get empty arcs.
+__global__ void final_arcs_kernel(int nsurv, const int* __restrict__ surv_sad, const int* __restrict__ sad_img,
+                                  const uint8_t* __restrict__ dual, bool arcs_primal, bool arcs_dual,
+                                  const int* __restrict__ t, const long long* __restrict__ blen, ReplayState S,
+                                  int max_steps, long long* __restrict__ arc_len, long long* __restrict__ arc_cl,
                                   int* __restrict__ arc_root, unsigned* status) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= 2 * nsurv) return;
   int i = q >> 1, j = q & 1;
   int s = surv_sad[i];
   int T = t[2 * s + j];
-  if (T < 0) {
+  if (T < 0 || !(dual[sad_img[s]] ? arcs_dual : arcs_primal)) {
     arc_len[q] = 0;
     arc_cl[q] = 0;
     arc_root[q] = -1;
@@ -153,12 +158,14 @@ __device__ __forceinline__ int4 make_task(int kind, int rev, int a, int b, long 
 struct EmitCtx {
   const uint8_t* flow;
   const int* crit_sad;
-  int H, W, Nx;
+  Imgs I;
+  const int* sad_img;
   bool faces;
   const int* t;            // per arc target
   const long long* blen;   // per arc length
   ReplayState S;
-  int* out;
+  int* out_primal;  // destination of primal images' arcs of this side
+  int* out_dual;    // destination of dual images' arcs
   int4* q_out;
   int* n_out;
   long long q_cap;
@@ -174,13 +181,17 @@ struct EmitCtx {
 __device__ void emit_base(const EmitCtx& E, int s, int j, int rev, long long pos) {
   long long len = E.blen[2 * s + j];
   if (len <= 0) return;
+  const int b = E.sad_img[s];
+  const int W = E.I.W[b], Nx = W + 1, ibase = E.I.idx_base[b];
+  int* out = E.I.dual[b] ? E.out_dual : E.out_primal;
+  if (!out) return;
   int sc = E.crit_sad[s];
-  int cell = E.faces ? face_start(sc, j, E.Nx) : vertex_start(sc, j, E.H, E.W, E.Nx);
+  int cell = E.faces ? face_start(sc, j, Nx) : vertex_start(sc, j, E.I.H[b], W, Nx, ibase);
   const int type = cell & 3, shift = E.faces ? 4 : 0;
   int idx = cell >> 2;
   for (long long k = 0; k < len; ++k) {
-    E.out[rev ? pos + len - 1 - k : pos + k] = type + 4 * idx;
-    if (k + 1 < len) idx += flow_step((__ldg(E.flow + idx) >> shift) & 0xFu, E.Nx);
+    out[rev ? pos + len - 1 - k : pos + k] = type + 4 * (idx - ibase);  // image-local cell id
+    if (k + 1 < len) idx += flow_step((__ldg(E.flow + idx) >> shift) & 0xFu, Nx);
   }
 }
 

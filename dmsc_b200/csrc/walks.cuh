@@ -21,10 +21,12 @@ __device__ __forceinline__ int face_start(int s_cell, int j, int Nx) {
   return (cell_type(s_cell) == 1) ? 3 + 4 * (idx + Nx) : 3 + 4 * (idx + 1);
 }
 
-// The j-th valid start cell on the vertex side, or -1.
-__device__ __forceinline__ int vertex_start(int s_cell, int j, int H, int W, int Nx) {
+// The j-th valid start cell on the vertex side, or -1. `s_cell` may be a
+// global cell id of a batch whose image starts at index `ibase`.
+__device__ __forceinline__ int vertex_start(int s_cell, int j, int H, int W, int Nx, int ibase = 0) {
   int idx = s_cell >> 2, t = cell_type(s_cell);
-  int ey = idx / Nx, ex = idx - ey * Nx;
+  int lidx = idx - ibase;
+  int ey = lidx / Nx, ex = lidx - ey * Nx;
   int v[2], n = 0;
   if (t == 1) {
     if (ex - 1 >= 0) v[n++] = 4 * (idx - 1);
@@ -56,15 +58,17 @@ __device__ __forceinline__ int flow_walk(const uint8_t* __restrict__ flow, int i
 
 // K4: per saddle, both face walks and the vertex walks. Writes per arc
 // (2 per saddle and side): dense target index (or -1) and step count.
-__global__ void __launch_bounds__(256) saddle_walk_kernel(const uint8_t* __restrict__ flow, int H, int W, int nsad,
+__global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t* __restrict__ flow, int nsad,
                                                           const int* __restrict__ crit_sad,
+                                                          const int* __restrict__ sad_img,
                                                           const int* __restrict__ max_rank,
                                                           const int* __restrict__ min_rank, int* __restrict__ tf,
                                                           int* __restrict__ lf, int* __restrict__ tv,
                                                           int* __restrict__ lv, long long cap, unsigned* status) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsad) return;
-  const int Nx = W + 1;
+  const int b = sad_img[s];
+  const int H = I.H[b], W = I.W[b], Nx = W + 1;
   int sc = crit_sad[s];
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
@@ -75,7 +79,7 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(const uint8_t* __restr
   }
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
-    int start = vertex_start(sc, j, H, W, Nx);
+    int start = vertex_start(sc, j, H, W, Nx, I.idx_base[b]);
     long long steps = 0;
     if (start >= 0) {
       int end = flow_walk<0>(flow, start >> 2, Nx, cap, &steps, status);
@@ -88,37 +92,54 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(const uint8_t* __restr
 }
 
 // Label of every extremum, stored at its index in `map` (which held the
-// extremum's dense rank): the rank among surviving extrema of its
+// extremum's dense rank): the rank among its image's surviving extrema of its
 // thresholded union-find root, or -1 when the root is the void
-// (cpu/cell_groups.hxx:128-146, 168-173).
-__global__ void label_map_kernel(int M, const int* __restrict__ crit, const int* __restrict__ ut_root,
-                                 const int* __restrict__ region, int* __restrict__ map) {
+// (cpu/cell_groups.hxx:128-146, 168-173). `alive_base[b]` is the first output
+// rank of image b's extrema.
+__global__ void label_map_kernel(int M, const int* __restrict__ crit, const int* __restrict__ ext_img,
+                                 const int* __restrict__ ut_root, const int* __restrict__ region,
+                                 const int* __restrict__ alive_base, int* __restrict__ map) {
   int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= M) return;
   int u = ut_root[r];
-  map[crit[r] >> 2] = u < 0 ? -1 : region[u];
+  map[crit[r] >> 2] = u < 0 ? -1 : region[u] - alive_base[ext_img[r]];
 }
 
-// K9: labels. One thread per face index (FACES) or per pixel (vertices):
-// walk to the critical cell and read its label from the map.
+// Where the labels of one side go: image b's block of the output array picked
+// by its orientation (faces are peaks in the primal, basins in the dual).
+struct LabelOut {
+  int* primal;            // output for primal images (nullptr: not requested)
+  int* dual;              // output for dual images
+  const int* primal_off;  // [B] block offset of image b in `primal`
+  const int* dual_off;
+};
+
+// K9: labels. One thread per face index (FACES) or per pixel (vertices) of
+// the batch: walk to the critical cell and read its label from the map.
 template <bool FACES>
-__global__ void __launch_bounds__(256) label_kernel(const uint8_t* __restrict__ flow, int H, int W,
-                                                    const int* __restrict__ label_map, int* __restrict__ out,
-                                                    long long cap, unsigned* status) {
+__global__ void __launch_bounds__(256) label_kernel(Imgs I, const uint8_t* __restrict__ flow, long long n,
+                                                    const int* __restrict__ label_map, LabelOut O, long long cap,
+                                                    unsigned* status) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int Nx = W + 1;
-  long long n = FACES ? (long long)(H + 1) * Nx : (long long)H * W;
   if (i >= n) return;
+  const int b = find_image(FACES ? I.idx_base : I.px_base, I.B, i);
+  const bool d = I.dual[b];
+  int* out = d ? O.dual : O.primal;
+  if (!out) return;
+  const int W = I.W[b], Nx = W + 1;
+  long long local;
   int idx;
   if (FACES) {
+    local = i - I.idx_base[b];
     idx = (int)i;
   } else {
-    int y = (int)(i / W), x = (int)(i - (long long)y * W);
-    idx = y * Nx + x;
+    local = i - I.px_base[b];
+    int y = (int)(local / W), x = (int)(local - (long long)y * W);
+    idx = I.idx_base[b] + y * Nx + x;
   }
   long long steps;
   int end = flow_walk<FACES ? 4 : 0>(flow, idx, Nx, cap, &steps, status);
-  out[i] = steps <= cap ? __ldg(label_map + end) : -1;
+  out[(d ? O.dual_off : O.primal_off)[b] + local] = steps <= cap ? __ldg(label_map + end) : -1;
 }
 
 }  // namespace dmsc

@@ -200,11 +200,113 @@ def extract_single(img: torch.Tensor, persistence_threshold: float, flags: int, 
             out["valley_arc_offsets"])
 
 
+# Indices (H+1)*(W+1) summed over the images of one device batch. The library
+# takes up to 2^29 - 1 (int32 cell ids over the batch); smaller batches keep the
+# workspace a few GB.
+BATCH_INDEX_CAP = 1 << 27
+
+_FIELDS = ("max_pts", "min_pts", "sad_pts", "e_max", "e_min", "p_max", "p_min", "ppairs_max", "ppairs_min", "ridges",
+           "ridge_offsets", "ridge_arc_offsets", "valleys", "valley_offsets", "valley_arc_offsets")
+_SIZE_OF = dict(max_pts="max_pts", min_pts="min_pts", sad_pts="sad_pts", e_max="e_max_rows", e_min="e_min_rows",
+                p_max="p_max", p_min="p_min", ppairs_max="ppairs_max", ppairs_min="ppairs_min", ridges="ridges",
+                ridge_offsets="ridge_offsets", ridge_arc_offsets="ridge_arc_offsets", valleys="valleys",
+                valley_offsets="valley_offsets", valley_arc_offsets="valley_arc_offsets")
+
+
+def extract_batch(images, thresholds, is_dual, flags: int, to_host: bool = False, stream=None) -> list:
+    """Contiguous float32 2-D CUDA images of any sizes (one device), each with
+    its own threshold and orientation, through one batched extract and one
+    fetch (``dmsc_b200_extract_batch``). Returns one 19-tuple per image; each
+    tensor is a view of one batch-wide output tensor (on the CPU when
+    ``to_host``). ``flags``' DUAL bit is ignored in favour of ``is_dual``."""
+    B = len(images)
+    dev = images[0].device
+    ctx = _lib.context(dev.index if dev.index is not None else torch.cuda.current_device())
+    s = stream if stream is not None else torch.cuda.current_stream(dev)
+    i32 = dict(dtype=torch.int32, device=dev)
+    Hs = [int(x.shape[0]) for x in images]
+    Ws = [int(x.shape[1]) for x in images]
+    duals = [bool(d) for d in is_dual]
+    flat = images[0].reshape(-1) if B == 1 else torch.cat([x.reshape(-1) for x in images])
+    nidx = [(h + 1) * (w + 1) for h, w in zip(Hs, Ws)]
+    npx = [h * w for h, w in zip(Hs, Ws)]
+    pk_n = [p if d else n for p, n, d in zip(npx, nidx, duals)]
+    bs_n = [n if d else p for p, n, d in zip(npx, nidx, duals)]
+    grad = torch.empty(4 * sum(nidx), **i32) if flags & _lib.RETURN_GRADIENT else None
+    peaks = torch.empty(sum(pk_n), **i32) if flags & _lib.TRACE_PEAKS else None
+    basins = torch.empty(sum(bs_n), **i32) if flags & _lib.TRACE_BASINS else None
+    sz = (_lib.Sizes * B)()
+    rc = ctx.lib.dmsc_b200_extract_batch(
+        ctx.h, ctypes.c_void_p(flat.data_ptr()), B, (ctypes.c_int * B)(*Hs), (ctypes.c_int * B)(*Ws),
+        (ctypes.c_float * B)(*[float(t) for t in thresholds]), (ctypes.c_ubyte * B)(*[int(d) for d in duals]), flags,
+        _ptr(grad), _ptr(peaks), _ptr(basins), sz, ctypes.c_void_p(s.cuda_stream))
+    if rc == _lib.ERR_TOO_LARGE and B == 1:
+        raise RuntimeError(f"Input is too large for 32-bit cell IDs: {Hs[0]}x{Ws[0]}")
+    ctx.check(rc, "dmsc_b200_extract_batch")
+    lens = {f: [int(getattr(sz[b], _SIZE_OF[f])) for b in range(B)] for f in _FIELDS}
+    out = {}
+    for f in _FIELDS:
+        n = sum(lens[f])
+        dt = torch.float32 if f in ("p_max", "p_min") else torch.int32
+        out[f] = torch.empty((n, 2) if f in ("e_max", "e_min") else n, dtype=dt, device=dev)
+    o = _lib.Outputs(**{k: _ptr(v) for k, v in out.items()})
+    ctx.check(ctx.lib.dmsc_b200_fetch(ctx.h, ctypes.byref(o), ctypes.c_void_p(s.cuda_stream)), "dmsc_b200_fetch")
+    if grad is not None:
+        out["grad_indices"] = grad
+        lens["grad_indices"] = [4 * n for n in nidx]
+    if peaks is not None:
+        out["peaks"] = peaks
+        lens["peaks"] = pk_n
+    if basins is not None:
+        out["basins"] = basins
+        lens["basins"] = bs_n
+    if to_host:
+        with torch.cuda.stream(s):
+            out = dict(zip(out.keys(), _to_host(tuple(out.values()))))
+    parts = {k: torch.split(v, lens[k]) for k, v in out.items()}
+    odev = torch.device("cpu") if to_host else dev
+    empty = torch.empty(0, dtype=torch.int32, device=odev)
+    empty2 = torch.empty((0, 0), dtype=torch.int32, device=odev)
+    res = []
+    for b in range(B):
+        H, W, d = Hs[b], Ws[b], duals[b]
+        g = parts["grad_indices"][b] if grad is not None else empty
+        pk = parts["peaks"][b].view((H, W) if d else (H + 1, W + 1)) if peaks is not None else empty2
+        bs = parts["basins"][b].view((H + 1, W + 1) if d else (H, W)) if basins is not None else empty2
+        q = {f: parts[f][b] for f in _FIELDS}
+        res.append((torch.tensor([H, W], dtype=torch.int32), q["max_pts"], q["min_pts"], q["sad_pts"], q["e_max"],
+                    q["e_min"], q["p_max"], q["p_min"], q["ppairs_max"], q["ppairs_min"], g, pk, q["ridges"],
+                    q["ridge_offsets"], q["ridge_arc_offsets"], bs, q["valleys"], q["valley_offsets"],
+                    q["valley_arc_offsets"]))
+    return res
+
+
+def _chunks(shapes):
+    """Consecutive image ranges whose index counts fit one device batch."""
+    start, acc = 0, 0
+    for b, (h, w) in enumerate(shapes):
+        n = (h + 1) * (w + 1)
+        if b > start and acc + n > BATCH_INDEX_CAP:
+            yield start, b
+            start, acc = b, 0
+        acc += n
+    if start < len(shapes):
+        yield start, len(shapes)
+
+
+def _extract_many(xs, thresholds, duals, flags, to_host) -> list:
+    out = []
+    for a, b in _chunks([tuple(x.shape) for x in xs]):
+        out.extend(extract_batch(xs[a:b], thresholds[a:b], duals[a:b], flags, to_host=to_host))
+    return out
+
+
 def extract_dmsc(scalar_field, persistence_threshold, return_gradient=False, is_dual=False, trace_max_arcs=False,
                  trace_min_arcs=False, trace_max_groups=False, trace_min_groups=False):
     """Mirror of the reference native entry ``dmsc_gpu.extract_dmsc``
     (dmsc/csrc/dmsc_gpu.cpp:128-180, 249-253): 19-tuple for 2-D input, a list
-    of 19-tuples for a 3-D batch (one image after another)."""
+    of 19-tuples for a 3-D batch (computed as device batches, each image's
+    outputs identical to a call on it alone)."""
     if scalar_field.dim() not in (2, 3) or scalar_field.dtype != torch.float32 or scalar_field.numel() == 0:
         raise RuntimeError("Input tensor must be a non-empty float32 2D [H, W] or 3D [B, H, W] tensor")
     H, W = int(scalar_field.shape[-2]), int(scalar_field.shape[-1])
@@ -222,8 +324,58 @@ def extract_dmsc(scalar_field, persistence_threshold, return_gradient=False, is_
         if x.dim() == 2:
             res = extract_single(x, persistence_threshold, flags)
             return _to_host(res) if on_cpu else res
-        outs = [extract_single(x[b], persistence_threshold, flags) for b in range(x.shape[0])]
-        return [_to_host(r) for r in outs] if on_cpu else outs
+        n = x.shape[0]
+        return _extract_many(list(x.unbind(0)), [persistence_threshold] * n, [is_dual] * n, flags, on_cpu)
+
+
+def compute_dmsc_batched(images, persistence_thresholds, is_dual=False, return_gradient=True, trace_valleys=True,
+                         trace_ridges=True, trace_peaks=True, trace_basins=True, verbose=False) -> list:
+    """Many images of uneven sizes, each with its own threshold and orientation.
+
+    ``images`` is a sequence of 2-D float32 tensors (all CUDA on one device, or
+    all CPU); ``persistence_thresholds`` and ``is_dual`` are scalars or one
+    value per image. Returns one ``MSComplex`` per image, equal field by field
+    to ``compute_dmsc(images[b], persistence_thresholds[b], is_dual=is_dual[b],
+    ...)``, computed as device batches (one pass of every stage over the
+    union of a batch's images). The reference has no counterpart beyond its
+    loop over a 3-D batch of one size and threshold (dmsc/dmsc.py:230-276,
+    dmsc/csrc/dmsc_gpu.cpp:84-126).
+    """
+    images = list(images)
+    if not images:
+        return []
+    n = len(images)
+    for x in images:
+        if x.dim() != 2:
+            raise ValueError(f"Each image must be 2D [H, W]. Got {x.dim()}D.")
+        _validate(x)
+    thr = list(persistence_thresholds) if hasattr(persistence_thresholds, "__len__") else [persistence_thresholds] * n
+    duals = list(is_dual) if hasattr(is_dual, "__len__") else [is_dual] * n
+    if len(thr) != n or len(duals) != n:
+        raise ValueError("persistence_thresholds and is_dual need one value per image")
+    for x in images:
+        H, W = int(x.shape[0]), int(x.shape[1])
+        if H + 1 > (2**31 - 1) // 4 // (W + 1):
+            raise RuntimeError(f"Input is too large for 32-bit cell IDs: {H}x{W}")
+    if not torch.cuda.is_available():
+        raise RuntimeError("dmsc_b200 requires a CUDA device; there is no CPU compute path")
+    devs = {x.device for x in images}
+    if len(devs) != 1:
+        raise ValueError(f"All images must be on one device. Got {sorted(str(d) for d in devs)}.")
+    on_cpu = images[0].device.type != "cuda"
+    start = time.perf_counter()
+    if on_cpu:
+        flat = torch.cat([x.contiguous().reshape(-1) for x in images]).pin_memory().to("cuda", non_blocking=True)
+        xs = list(torch.split(flat, [x.numel() for x in images]))
+        xs = [v.view(x.shape) for v, x in zip(xs, images)]
+    else:
+        xs = [x.contiguous() for x in images]
+    flags = _flags(return_gradient, False, trace_ridges, trace_valleys, trace_peaks, trace_basins)
+    with torch.cuda.device(xs[0].device):
+        outs = _extract_many(xs, thr, duals, flags, on_cpu)
+    if verbose:
+        print(f"Time for MS-complex computation ({n} images): {(time.perf_counter() - start) * 1000:.3f} ms")
+    return [MSComplex(*r) for r in outs]
 
 
 def _to_host(res: tuple) -> tuple:

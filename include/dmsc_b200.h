@@ -104,9 +104,34 @@ int dmsc_b200_extract(dmsc_b200_context* ctx, const float* image, int H, int W, 
                       unsigned flags, int32_t* grad_out, int32_t* peaks_out, int32_t* basins_out,
                       dmsc_b200_sizes* sizes, void* stream);
 
-/* Phase 2: writes the variable-size outputs of the last extract() on this
-   context. `out` is a host pointer to a struct of device pointers. */
+/* Phase 2: writes the variable-size outputs of the last extract() or
+   extract_batch() on this context. `out` is a host pointer to a struct of
+   device pointers. After extract_batch(), every array holds the images'
+   parts back to back in image order, each part sized by that image's sizes
+   entry (offset arrays too: ridge_offsets holds ridge_offsets[b] + 1 entries
+   of image b, and so on); all values are image-local. */
 int dmsc_b200_fetch(dmsc_b200_context* ctx, const dmsc_b200_outputs* out, void* stream);
+
+/* Phase 1 for a batch of B images of independent sizes, thresholds and
+   orientations, computed together (one pass of every stage over the union
+   of the images). Replaces the reference's per-image loop over a 3-D batch
+   (dmsc/csrc/dmsc_gpu.cpp:84-126, dmsc/csrc/dmsc_cpu.cpp:80-106), which only
+   takes images of one size and one threshold; each image's outputs are
+   exactly those of dmsc_b200_extract() on it alone.
+   `images`     : device float32, the images back to back, image b H[b] x W[b]
+                  row-major, starting at element sum_{c<b} H[c]*W[c].
+   `H`, `W`, `thresholds`, `is_dual` : host arrays of B entries (is_dual 0/1);
+                  DMSC_B200_DUAL in `flags` is ignored, the other flags apply
+                  to every image.
+   `grad_out`, `peaks_out`, `basins_out` : the per-image arrays of
+                  dmsc_b200_extract() back to back in image order.
+   `sizes`      : host array of B entries, written per image.
+   The cell ids of the whole batch must fit int32 (sum over images of
+   4*(H+1)*(W+1)), else DMSC_B200_ERR_TOO_LARGE: split the batch. */
+int dmsc_b200_extract_batch(dmsc_b200_context* ctx, const float* images, int B, const int* H, const int* W,
+                            const float* thresholds, const unsigned char* is_dual, unsigned flags,
+                            int32_t* grad_out, int32_t* peaks_out, int32_t* basins_out, dmsc_b200_sizes* sizes,
+                            void* stream);
 
 /* Static description of a return code. */
 const char* dmsc_b200_error_string(int code);
