@@ -201,9 +201,9 @@ def extract_single(img: torch.Tensor, persistence_threshold: float, flags: int, 
 
 
 # Indices (H+1)*(W+1) summed over the images of one device batch. The library
-# takes up to 2^29 - 1 (int32 cell ids over the batch); smaller batches keep the
-# workspace a few GB.
-BATCH_INDEX_CAP = 1 << 27
+# takes up to 2^29 - 1 (int32 cell ids over the batch); 2^28 keeps one device
+# batch's workspace to a few tens of GB of HBM.
+BATCH_INDEX_CAP = 1 << 28
 
 _FIELDS = ("max_pts", "min_pts", "sad_pts", "e_max", "e_min", "p_max", "p_min", "ppairs_max", "ppairs_min", "ridges",
            "ridge_offsets", "ridge_arc_offsets", "valleys", "valley_offsets", "valley_arc_offsets")
@@ -213,12 +213,13 @@ _SIZE_OF = dict(max_pts="max_pts", min_pts="min_pts", sad_pts="sad_pts", e_max="
                 valley_offsets="valley_offsets", valley_arc_offsets="valley_arc_offsets")
 
 
-def extract_batch(images, thresholds, is_dual, flags: int, to_host: bool = False, stream=None) -> list:
-    """Contiguous float32 2-D CUDA images of any sizes (one device), each with
-    its own threshold and orientation, through one batched extract and one
-    fetch (``dmsc_b200_extract_batch``). Returns one 19-tuple per image; each
-    tensor is a view of one batch-wide output tensor (on the CPU when
-    ``to_host``). ``flags``' DUAL bit is ignored in favour of ``is_dual``."""
+def _batch_raw(images, thresholds, is_dual, flags: int, stream=None, flat=None, pair_pixels=False):
+    """Both C-ABI phases of one device batch. Returns the batch-wide output
+    tensors (``out``, field -> tensor, images back to back), the per-image
+    lengths of each (``lens``), the image shapes and orientations and the
+    stream. ``flat`` may hold the images already back to back; with
+    ``pair_pixels`` the pixel pairs of every p_max / p_min entry are fetched
+    too (``plus_max``, ``minus_max``, ``plus_min``, ``minus_min``)."""
     B = len(images)
     dev = images[0].device
     ctx = _lib.context(dev.index if dev.index is not None else torch.cuda.current_device())
@@ -227,7 +228,8 @@ def extract_batch(images, thresholds, is_dual, flags: int, to_host: bool = False
     Hs = [int(x.shape[0]) for x in images]
     Ws = [int(x.shape[1]) for x in images]
     duals = [bool(d) for d in is_dual]
-    flat = images[0].reshape(-1) if B == 1 else torch.cat([x.reshape(-1) for x in images])
+    if flat is None:
+        flat = images[0].reshape(-1) if B == 1 else torch.cat([x.reshape(-1) for x in images])
     nidx = [(h + 1) * (w + 1) for h, w in zip(Hs, Ws)]
     npx = [h * w for h, w in zip(Hs, Ws)]
     pk_n = [p if d else n for p, n, d in zip(npx, nidx, duals)]
@@ -251,6 +253,14 @@ def extract_batch(images, thresholds, is_dual, flags: int, to_host: bool = False
         out[f] = torch.empty((n, 2) if f in ("e_max", "e_min") else n, dtype=dt, device=dev)
     o = _lib.Outputs(**{k: _ptr(v) for k, v in out.items()})
     ctx.check(ctx.lib.dmsc_b200_fetch(ctx.h, ctypes.byref(o), ctypes.c_void_p(s.cuda_stream)), "dmsc_b200_fetch")
+    if pair_pixels:
+        for f in ("plus_max", "minus_max", "plus_min", "minus_min"):
+            side = f.split("_")[1]
+            out[f] = torch.empty(out["p_" + side].numel(), **i32)
+            lens[f] = lens["p_" + side]
+        ctx.check(ctx.lib.dmsc_b200_fetch_pair_pixels(
+            ctx.h, _ptr(out["plus_max"]), _ptr(out["minus_max"]), _ptr(out["plus_min"]), _ptr(out["minus_min"]),
+            ctypes.c_void_p(s.cuda_stream)), "dmsc_b200_fetch_pair_pixels")
     if grad is not None:
         out["grad_indices"] = grad
         lens["grad_indices"] = [4 * n for n in nidx]
@@ -260,6 +270,19 @@ def extract_batch(images, thresholds, is_dual, flags: int, to_host: bool = False
     if basins is not None:
         out["basins"] = basins
         lens["basins"] = bs_n
+    return out, lens, Hs, Ws, duals, s
+
+
+def extract_batch(images, thresholds, is_dual, flags: int, to_host: bool = False, stream=None) -> list:
+    """Contiguous float32 2-D CUDA images of any sizes (one device), each with
+    its own threshold and orientation, through one batched extract and one
+    fetch (``dmsc_b200_extract_batch``). Returns one 19-tuple per image; each
+    tensor is a view of one batch-wide output tensor (on the CPU when
+    ``to_host``). ``flags``' DUAL bit is ignored in favour of ``is_dual``."""
+    B = len(images)
+    dev = images[0].device
+    out, lens, Hs, Ws, duals, s = _batch_raw(images, thresholds, is_dual, flags, stream)
+    grad, peaks, basins = out.get("grad_indices"), out.get("peaks"), out.get("basins")
     if to_host:
         with torch.cuda.stream(s):
             out = dict(zip(out.keys(), _to_host(tuple(out.values()))))

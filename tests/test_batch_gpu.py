@@ -123,3 +123,15 @@ def test_batch_argument_errors():
     with pytest.raises(TypeError):
         compute_dmsc_batched([x.double()], 0.1)
     assert compute_dmsc_batched([], 0.1) == []
+
+
+def test_sharded_single_rank_matches_plain_calls():
+    """The sharded driver on one rank (no process group) equals plain calls."""
+    from dmsc_b200 import compute_dmsc
+    from dmsc_b200.sharding import compute_dmsc_sharded
+
+    imgs, thr, dual = _batch(31, 12, 2, 64)
+    full = compute_dmsc_sharded(imgs, thr, dual, device="cuda:0", gather=True)
+    for b, ms in enumerate(full):
+        ref = compute_dmsc(imgs[b], thr[b], is_dual=dual[b])
+        assert diff_fields(tuple(ms), tuple(ref)) == [], b
