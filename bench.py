@@ -332,6 +332,7 @@ def b200_arm(args):
     e2e = world * args.steps * size * size / 1e6 / (float(te.item()) / 1000.0)
 
     batched = None if args.batch_images <= 0 else batched_section(args, dev, ctx, dist, world, rank)
+    diff = None if args.no_diff else diff_section(args, dev, dist)
 
     if rank != 0:
         if dist:
@@ -370,6 +371,8 @@ def b200_arm(args):
     }
     if batched is not None:
         line["batched"] = batched
+    if diff is not None:
+        line["differentiation"] = diff
     if world == 1 and not args.no_cpu_baseline:
         cb, exact = cpu_baseline(img.cpu(), gpu_out)
         line["cpu_baseline"] = cb
@@ -454,6 +457,74 @@ def batched_section(args, dev, ctx, dist, world, rank):
     }
 
 
+def diff_section(args, dev, dist):
+    """Differentiation workload: 64 float32 512 x 512 fields (200 bumps,
+    sigma U[4,32], noise N(0,0.05^2), plus 1e-6 * permutation rank / N), loss
+    = sum of p^2 over pairs with ppairs != -1 and 0 <= p < 0.1. A step is the
+    forward (persistence pairs of the batch) and the backward (the
+    deterministic scatter kernel) of that loss; host wall clock around K
+    steps ending with a device synchronisation, max over ranks. The backward
+    kernel alone is timed with CUDA events."""
+    from dmsc_b200.autograd import persistence_pairs, scatter_pair_grads
+    from dmsc_b200.synthetic import bump_field
+
+    n, size = 64, 512
+    fields = []
+    for i in range(n):
+        f = bump_field(size, size, 200, 4.0, 32.0, 0.05, SEED + 101 * i, device=dev)
+        g = torch.Generator().manual_seed(SEED + 101 * i + 1)
+        rank = torch.randperm(size * size, generator=g).reshape(size, size).float().to(dev)
+        fields.append(f + 1e-6 * rank / (size * size))
+    x0 = torch.stack(fields).contiguous()
+
+    def step():
+        x = x0.detach().requires_grad_(True)
+        pp = persistence_pairs(x, -1.0)
+        p = pp.persistence
+        keep = (pp.ppairs != -1) & (p >= 0) & (p < 0.1)
+        (p * p * keep).sum().backward()
+        return x.grad, pp
+
+    g1, pp = step()
+    g2, _ = step()
+    deterministic = bool(torch.equal(g1.view(torch.int32), g2.view(torch.int32)))
+    steps = max(3, args.steps)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    torch.cuda.synchronize()
+    t = torch.tensor([(time.perf_counter() - t0) / steps], device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    # the backward kernel alone, on this batch's pairs
+    base = (pp.image * (size * size)).to(torch.int32)
+    plus = torch.where(pp.plus_pixel >= 0, pp.plus_pixel + base, pp.plus_pixel)
+    minus = torch.where(pp.minus_pixel >= 0, pp.minus_pixel + base, pp.minus_pixel)
+    gp = torch.ones_like(pp.persistence)
+    st = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        scatter_pair_grads(plus, minus, gp, x0.shape)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(10):
+        scatter_pair_grads(plus, minus, gp, x0.shape)
+    e1.record(st)
+    torch.cuda.synchronize()
+    return {
+        "workload": "64 x 512^2 float32 bump fields (200 bumps, sigma U[4,32], noise N(0,0.05^2)) + 1e-6*rank/N; "
+                    "loss = sum p^2 over pairs with ppairs != -1 and 0 <= p < 0.1",
+        "ms_per_forward_backward": 1000.0 * float(t.item()),
+        "images_per_s": n / float(t.item()),
+        "pairs": int(pp.persistence.numel()),
+        "backward_kernel_ms": e0.elapsed_time(e1) / 10,
+        "backward_deterministic": deterministic,
+        "timing": "host wall clock around K forward+backward steps, inputs resident in HBM",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -463,6 +534,7 @@ def main():
     ap.add_argument("--size", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-images", type=int, default=512, help="uneven-batch images per GPU (0: skip)")
+    ap.add_argument("--no-diff", action="store_true", help="skip the differentiation workload")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

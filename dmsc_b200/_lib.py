@@ -22,6 +22,8 @@ EXPORTS = (
     "dmsc_b200_extract",
     "dmsc_b200_fetch",
     "dmsc_b200_extract_batch",
+    "dmsc_b200_fetch_pair_pixels",
+    "dmsc_b200_scatter_pair_grads",
     "dmsc_b200_error_string",
     "dmsc_b200_last_error",
     "dmsc_b200_set_profiling",
@@ -82,6 +84,12 @@ def load():
             ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_ubyte), ctypes.c_uint, ctypes.c_void_p,
             ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Sizes), ctypes.c_void_p]
         lib.dmsc_b200_extract_batch.restype = ctypes.c_int
+        lib.dmsc_b200_fetch_pair_pixels.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 5
+        lib.dmsc_b200_fetch_pair_pixels.restype = ctypes.c_int
+        lib.dmsc_b200_scatter_pair_grads.argtypes = [
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+            ctypes.c_int64, ctypes.c_void_p]
+        lib.dmsc_b200_scatter_pair_grads.restype = ctypes.c_int
         lib.dmsc_b200_error_string.argtypes = [ctypes.c_int]
         lib.dmsc_b200_error_string.restype = ctypes.c_char_p
         lib.dmsc_b200_last_error.argtypes = [ctypes.c_void_p]

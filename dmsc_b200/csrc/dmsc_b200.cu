@@ -26,6 +26,7 @@
 #include "pairing.cuh"
 #include "persistent.cuh"
 #include "replay.cuh"
+#include "pairs.cuh"
 #include "walks.cuh"
 
 using namespace dmsc;
@@ -37,6 +38,7 @@ enum Slot {
   S_GRAD, S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
   S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
   S_ASC, S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
+  S_BKEY, S_BIDX, S_BKEY2, S_BIDX2,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
@@ -122,6 +124,7 @@ struct dmsc_b200_context {
   Bases bases{};
   const int* grad = nullptr;
   const uint8_t* flow = nullptr;
+  const float* img = nullptr;  // input of the last extract (read again by fetch_pair_pixels)
   int* crit_sad = nullptr;
   int* sad_img = nullptr;
   int* surv = nullptr;
@@ -602,6 +605,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   uint8_t* mask = get<uint8_t>(ctx, S_MASK, nidx);
   uint8_t* flow = get<uint8_t>(ctx, S_FLOW, nidx);
   ctx->flow = flow;
+  ctx->img = img;
   int* seg[3] = {get<int>(ctx, S_SEG0, nseg), get<int>(ctx, S_SEG1, nseg), get<int>(ctx, S_SEG2, nseg)};
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
   LK(gradient_batch_kernel<<<(unsigned)ntile, kGradThreads, 0, st>>>(I, img, (int4*)grad, mask, seg[0], seg[1], seg[2],
@@ -1015,6 +1019,56 @@ int fetch_batch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStr
   return kOk;
 }
 
+// Pixel pairs of the surviving saddles of the last extract (pairs.cuh).
+int fetch_pair_pixels_impl(dmsc_b200_context* ctx, int32_t* plus_max, int32_t* minus_max, int32_t* plus_min,
+                           int32_t* minus_min, cudaStream_t st) {
+  if (!ctx->valid) {
+    set_err(ctx, "fetch_pair_pixels without a successful extract");
+    return kErrInvalidArgument;
+  }
+  CK(cudaSetDevice(ctx->device));
+  const int nsurv = ctx->nsurv;
+  if (nsurv == 0) return kOk;
+  for (int si = 0; si < 2; ++si) {
+    Side& S = ctx->side[si];
+    // faces: the max side in the primal, the min side in the dual
+    Route PLUS{S.faces ? plus_max : plus_min, S.faces ? plus_min : plus_max, ctx->bases.surv};
+    Route MINUS{S.faces ? minus_max : minus_min, S.faces ? minus_min : minus_max, ctx->bases.surv};
+    LK(pair_pixels_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, ctx->bases.surv, ctx->I, ctx->img,
+                                                              ctx->surv, ctx->crit_sad, S.pair_dense, S.crit, PLUS,
+                                                              MINUS));
+  }
+  LAUNCH_CHECK("pair_pixels_kernel");
+  return kOk;
+}
+
+// grad_img[0, npx) = deterministic scatter of +-grad[i] onto (plus[i], minus[i]).
+int scatter_pair_grads_impl(dmsc_b200_context* ctx, const int32_t* plus, const int32_t* minus, const float* grad,
+                            long long n, float* grad_img, long long npx, cudaStream_t st) {
+  if (n < 0 || npx < 0 || (n > 0 && (!plus || !minus || !grad)) || (npx > 0 && !grad_img)) {
+    set_err(ctx, "invalid argument");
+    return kErrInvalidArgument;
+  }
+  if (npx >= 2147483647LL || 2 * n >= 2147483647LL) {
+    set_err(ctx, "scatter of %lld pairs onto %lld pixels exceeds int32 indexing", n, npx);
+    return kErrTooLarge;
+  }
+  CK(cudaSetDevice(ctx->device));
+  if (npx > 0) CK(cudaMemsetAsync(grad_img, 0, npx * sizeof(float), st));
+  if (n == 0 || npx == 0) return kOk;
+  const int m = (int)(2 * n);
+  int* key = get<int>(ctx, S_BKEY, m);
+  int* idx = get<int>(ctx, S_BIDX, m);
+  int* key2 = get<int>(ctx, S_BKEY2, m);
+  int* idx2 = get<int>(ctx, S_BIDX2, m);
+  LK(pair_entries_kernel<<<grid_for(m, TB), TB, 0, st>>>(n, plus, minus, (int)npx, key, idx));
+  LAUNCH_CHECK("pair_entries_kernel");
+  sort_pairs(ctx, key, key2, idx, idx2, m, st, bits_for((int)npx + 1));
+  LK(pair_segments_kernel<<<grid_for(m, TB), TB, 0, st>>>(m, key2, idx2, grad, (int)npx, grad_img));
+  LAUNCH_CHECK("pair_segments_kernel");
+  return kOk;
+}
+
 }  // namespace
 
 
@@ -1094,6 +1148,28 @@ int dmsc_b200_extract_batch(dmsc_b200_context* ctx, const float* images, int B, 
                               sizes, (cudaStream_t)stream);
   } catch (const Fail& f) {
     ctx->valid = false;
+    return f.code;
+  }
+}
+
+int dmsc_b200_fetch_pair_pixels(dmsc_b200_context* ctx, int32_t* plus_max, int32_t* minus_max, int32_t* plus_min,
+                                int32_t* minus_min, void* stream) {
+  if (!ctx) return kErrInvalidArgument;
+  ctx->err.clear();
+  try {
+    return fetch_pair_pixels_impl(ctx, plus_max, minus_max, plus_min, minus_min, (cudaStream_t)stream);
+  } catch (const Fail& f) {
+    return f.code;
+  }
+}
+
+int dmsc_b200_scatter_pair_grads(dmsc_b200_context* ctx, const int32_t* plus, const int32_t* minus, const float* grad,
+                                 int64_t n, float* grad_img, int64_t npx, void* stream) {
+  if (!ctx) return kErrInvalidArgument;
+  ctx->err.clear();
+  try {
+    return scatter_pair_grads_impl(ctx, plus, minus, grad, n, grad_img, npx, (cudaStream_t)stream);
+  } catch (const Fail& f) {
     return f.code;
   }
 }

@@ -133,6 +133,30 @@ int dmsc_b200_extract_batch(dmsc_b200_context* ctx, const float* images, int B, 
                             int32_t* grad_out, int32_t* peaks_out, int32_t* basins_out, dmsc_b200_sizes* sizes,
                             void* stream);
 
+/* Differentiation support (no counterpart in the reference, whose outputs
+   carry no gradient). A persistence value p (p_max / p_min, computed as the
+   float32 difference of two input pixels, dmsc/csrc/cpu/persistence.hxx:82-104,
+   139-161) has d p / d image = +1 at one pixel and -1 at another on a field
+   without ties.
+   dmsc_b200_fetch_pair_pixels() writes, for the last extract() or
+   extract_batch() on this context, those two image-local pixel ids
+   (y * W + x) of every entry of p_max and p_min: `plus_*` and `minus_*` are
+   device int32 arrays laid out exactly like p_max / p_min (per image, back
+   to back for a batch); -1 in both for a cycle (persistence -1, constant).
+   Any pointer may be NULL. It reads the input image again: the image passed
+   to extract must be unchanged. */
+int dmsc_b200_fetch_pair_pixels(dmsc_b200_context* ctx, int32_t* plus_max, int32_t* minus_max, int32_t* plus_min,
+                                int32_t* minus_min, void* stream);
+
+/* Backward scatter: grad_img[0 .. npx) = 0, then for every i < n,
+   grad_img[plus[i]] += grad[i] and grad_img[minus[i]] -= grad[i] (ends
+   outside [0, npx), such as -1, are skipped). Deterministic: the terms of
+   each pixel are summed in ascending order of i, + end before - end, by a
+   stable sort and a segmented sum; no float atomics. Device pointers; `plus`
+   and `minus` are pixel ids in the caller's flat pixel array. */
+int dmsc_b200_scatter_pair_grads(dmsc_b200_context* ctx, const int32_t* plus, const int32_t* minus,
+                                 const float* grad, int64_t n, float* grad_img, int64_t npx, void* stream);
+
 /* Static description of a return code. */
 const char* dmsc_b200_error_string(int code);
 
