@@ -7,12 +7,14 @@
 //
 // Layout. The gradient array holds 4 int32 slots per index (y, x) of the
 // (H+1) x (W+1) index grid, i.e. 16 bytes per index; it is the grad_indices
-// output. One CTA owns a 32 x 8 tile of indices and writes it with one int4
+// output. One CTA owns a 32 x 16 tile of indices and writes it with one int4
 // store per index, so every warp writes 512 contiguous bytes. The cells at a
 // tile's indices are owned (have their highest vertex) in the pixels of the
 // tile plus one halo row above and one halo column to the left, so the CTA
-// evaluates the lower star of (8+1) x (32+1) pixels from a (8+3) x (32+3)
-// value tile in shared memory. Slots of invalid cells stay -1.
+// evaluates the lower star of (16+1) x (32+1) pixels from a (16+3) x (32+3)
+// value tile in shared memory, one 32-bit pairing word per pixel, and every
+// index then gathers its four slots from the words of their owners. Slots of
+// invalid cells are -1.
 //
 // The same pass writes one criticality byte per index (bit t = slot t is an
 // unpaired valid cell) and per-(row, 32-column segment) counts of minima,
@@ -72,11 +74,28 @@ inline uint32_t face_fifo_entry(unsigned eL, unsigned fL, int best) {
   return (fpk << 16) | epk;
 }
 
-// All 16 x 16 x 5 entries, indexed ((eL << 4) | fL) * 5 + best + 1.
+// Nibble value of a slot whose cell is not in this pixel's lower star (the
+// cell belongs to a neighbour, or does not exist).
+constexpr unsigned kNotMine = 14u;
+// Word of a pixel outside the image: it owns no cell.
+constexpr uint32_t kNoPixel = 0xEEEEEEEEu;
+
+// All 16 x 16 x 5 entries, indexed ((eL << 4) | fL) * 5 + best + 1: the
+// pairing word of a pixel. Nibbles 0-3 describe edge slots 0-3 (4 = paired
+// with the vertex, 0..3 = paired with that face slot, 15 = critical, 14 = not
+// in the lower star), nibbles 4-7 face slots 0-3 (0..3 = paired with that
+// edge slot, 15 = critical, 14 = not in the lower star).
 inline void face_fifo_table(uint32_t* out) {
   for (unsigned eL = 0; eL < 16; ++eL)
     for (unsigned fL = 0; fL < 16; ++fL)
-      for (int b = -1; b < 4; ++b) out[((eL << 4) | fL) * 5 + (b + 1)] = face_fifo_entry(eL, fL, b);
+      for (int b = -1; b < 4; ++b) {
+        uint32_t w = face_fifo_entry(eL, fL, b);
+        for (int k = 0; k < 4; ++k) {
+          if (!((eL >> k) & 1u)) w = (w & ~(0xFu << (4 * k))) | (kNotMine << (4 * k));
+          if (!((fL >> k) & 1u)) w = (w & ~(0xFu << (16 + 4 * k))) | (kNotMine << (16 + 4 * k));
+        }
+        out[((eL << 4) | fL) * 5 + (b + 1)] = w;
+      }
 }
 constexpr int kFifoTable = 16 * 16 * 5;
 
@@ -100,10 +119,10 @@ __device__ __forceinline__ bool gt_before(float a, float b) {
 // (cpu/cell_compare.hxx:33-63), so ties and non-finite values resolve the same
 // way. Edge slots: e0 = H(y,x), e1 = H(y,x+1), e2 = V(y,x), e3 = V(y+1,x);
 // face slots: f0 = F(y,x), f1 = F(y,x+1), f2 = F(y+1,x), f3 = F(y+1,x+1).
-// Writes the gradient values of the owned cells into the shared index tile.
+// Returns the pixel's pairing word (face_fifo_table).
 template <bool DUAL>
-__device__ __forceinline__ void lower_star(const float (*sv)[kValX], int y, int x, int H, int W, int Nx, int ty0,
-                                           int tx0, int (*tile)[kTileY][kTileX], const uint32_t* __restrict__ fifo_lut) {
+__device__ __forceinline__ uint32_t lower_star(const float (*sv)[kValX], int y, int x, int H, int W, int ty0, int tx0,
+                                               const uint32_t* __restrict__ fifo_lut) {
   // 3x3 neighbourhood; r, c index the value tile (origin y0-2, x0-2)
   const int r = y - (ty0 - 2), c = x - (tx0 - 2);
   const bool lv = x >= 1, rv = x + 1 < W, uv = y >= 1, dv = y + 1 < H;
@@ -192,77 +211,86 @@ __device__ __forceinline__ void lower_star(const float (*sv)[kValX], int y, int 
   // face pairing: the FIFO of cpu/gradient.hxx:115-191 depends only on the
   // lower-star masks and the vertex-paired edge, so its result is looked up
   // (face_fifo_table() builds the 1280 entries with the same procedure).
-  const uint32_t pr = __ldg(fifo_lut + (((eL << 4) | fL) * 5 + (best + 1)));
-  const unsigned epk = pr & 0xFFFFu, fpk = pr >> 16;
-
-  // owned cells -> index tile (slot index arithmetic: edge k at index
-  // (y + (k == 3), x + (k == 1)), type 1 + (k >> 1); face f at (y + (f >> 1), x + (f & 1)))
-  const int tr = y - ty0, tc = x - tx0;
-  auto put = [&](int dr, int dc, int t, int v) {
-    const int rr = tr + dr, cc = tc + dc;
-    if (rr >= 0 && rr < kTileY && cc >= 0 && cc < kTileX) tile[t][rr][cc] = v;
-  };
-  const int base = y * Nx + x;
-  auto edge_cell = [&](int k) { return (1 + (k >> 1)) + 4 * (base + (k == 3 ? Nx : 0) + (k == 1 ? 1 : 0)); };
-  auto face_cell = [&](int f) { return 3 + 4 * (base + (f >> 1) * Nx + (f & 1)); };
-  put(0, 0, 0, best >= 0 ? edge_cell(best) : -1);
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (!((eL >> k) & 1u)) continue;
-    const unsigned pk = (epk >> (4 * k)) & 0xFu;
-    const int v = pk == 4u ? 4 * base : (pk < 4u ? face_cell((int)pk) : -1);
-    put(k == 3 ? 1 : 0, k == 1 ? 1 : 0, 1 + (k >> 1), v);
-  }
-#pragma unroll
-  for (int f = 0; f < 4; ++f) {
-    if (!((fL >> f) & 1u)) continue;
-    const unsigned pk = (fpk >> (4 * f)) & 0xFu;
-    put(f >> 1, f & 1, 3, pk < 4u ? edge_cell((int)pk) : -1);
-  }
+  return __ldg(fifo_lut + (((eL << 4) | fL) * 5 + (best + 1)));
 }
 
-// Lower stars of one 32 x 16 index tile into the slot-major shared tile.
+// Pairing words of the (kTileY + 1) x (kTileX + 1) pixels whose lower stars
+// hold the cells of one 32 x 16 index tile (origin pixel (y0 - 1, x0 - 1)).
 template <bool DUAL>
 __device__ __forceinline__ void gradient_tile(const float* __restrict__ img, int H, int W, int y0, int x0, int tid,
-                                              float (*sv)[kValX], int (*tile)[kTileY][kTileX],
+                                              float (*sv)[kValX], uint32_t (*word)[kTileX + 1],
                                               const uint32_t* __restrict__ fifo_lut) {
   for (int i = tid; i < kValY * kValX; i += kGradThreads) {
     int r = i / kValX, c = i - r * kValX;
     int gy = y0 - 2 + r, gx = x0 - 2 + c;
     sv[r][c] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(img + (size_t)gy * W + gx) : 0.0f;
   }
-  for (int i = tid; i < 4 * kTileY * kTileX; i += kGradThreads) (&tile[0][0][0])[i] = -1;
   __syncthreads();
   if (tid < (kTileY + 1) * (kTileX + 1)) {
     int r = tid / (kTileX + 1), c = tid - r * (kTileX + 1);
     int y = y0 - 1 + r, x = x0 - 1 + c;
-    if (y >= 0 && y < H && x >= 0 && x < W) lower_star<DUAL>(sv, y, x, H, W, W + 1, y0, x0, tile, fifo_lut);
+    uint32_t w = kNoPixel;
+    if (y >= 0 && y < H && x >= 0 && x < W) w = lower_star<DUAL>(sv, y, x, H, W, y0, x0, fifo_lut);
+    word[r][c] = w;
   }
   __syncthreads();
 }
 
-// Write-out of one tile row by one warp: coalesced int4 gradient stores at
+// Cell of edge slot k / face slot f of the pixel at index `b`.
+__device__ __forceinline__ int slot_edge_cell(int k, int b, int Nx) {
+  return (1 + (k >> 1)) + 4 * (b + (k == 3 ? Nx : 0) + (k == 1 ? 1 : 0));
+}
+__device__ __forceinline__ int slot_face_cell(int f, int b, int Nx) { return 3 + 4 * (b + (f >> 1) * Nx + (f & 1)); }
+
+// Write-out of one tile row by one warp. Index (iy, ix) gathers its four
+// slots from the pairing words of the pixels owning them: its vertex and
+// (when owned there) its H edge, V edge and face from pixel (iy, ix), else
+// the H edge from (iy, ix-1), the V edge from (iy-1, ix) and the face from
+// (iy, ix-1), (iy-1, ix) or (iy-1, ix-1). Coalesced int4 gradient stores at
 // global index base `gbase`, criticality mask, flow codes and the row
 // segment's counts (segment id `seg`).
-__device__ __forceinline__ void gradient_store_row(const int (*tile)[kTileY][kTileX], int warp, int lane, int H,
+__device__ __forceinline__ void gradient_store_row(const uint32_t (*word)[kTileX + 1], int warp, int lane, int H,
                                                    int W, int iy, int ix, long long gbase, int seg,
                                                    int4* __restrict__ grad, uint8_t* __restrict__ crit_mask,
                                                    uint8_t* __restrict__ flow, int* __restrict__ seg_min,
                                                    int* __restrict__ seg_sad, int* __restrict__ seg_max) {
   const int Nx = W + 1;
-  bool in = ix <= W;
-  int4 v = make_int4(tile[0][warp][lane], tile[1][warp][lane], tile[2][warp][lane], tile[3][warp][lane]);
+  const bool in = ix <= W;
   unsigned m = 0;
   if (in) {
-    const int lidx = iy * Nx + ix;  // image-local index: the cell ids in v are local
-    const size_t gidx = (size_t)(gbase + lidx);
-    grad[gidx] = v;
-    if (v.x == -1 && iy < H && ix < W) m |= 1u;
-    if (v.y == -1 && iy < H) m |= 2u;
-    if (v.z == -1 && ix < W) m |= 4u;
-    if (v.w == -1) m |= 8u;
+    const uint32_t wP = word[warp + 1][lane + 1], wL = word[warp + 1][lane];
+    const uint32_t wU = word[warp][lane + 1], wUL = word[warp][lane];
+    const int b = iy * Nx + ix;  // image-local index: the cell ids written are local
+    // vertex: the edge slot of its own pixel marked 4
+    const unsigned e = wP & 0xFFFFu;
+    const int vk = ((e & 0xFu) == 4u) ? 0 : (((e >> 4) & 0xFu) == 4u) ? 1 : (((e >> 8) & 0xFu) == 4u) ? 2
+                 : (((e >> 12) & 0xFu) == 4u) ? 3 : -1;
+    const int s0 = vk >= 0 ? slot_edge_cell(vk, b, Nx) : -1;
+    // H edge (iy, ix): slot 0 of (iy, ix) or slot 1 of (iy, ix-1)
+    const unsigned h0 = wP & 0xFu;
+    const bool hown = h0 != kNotMine;
+    const unsigned hn = hown ? h0 : ((wL >> 4) & 0xFu);
+    const int hb = hown ? b : b - 1;
+    const int s1 = hn == 4u ? 4 * hb : (hn < 4u ? slot_face_cell((int)hn, hb, Nx) : -1);
+    // V edge (iy, ix): slot 2 of (iy, ix) or slot 3 of (iy-1, ix)
+    const unsigned v0 = (wP >> 8) & 0xFu;
+    const bool vown = v0 != kNotMine;
+    const unsigned vn = vown ? v0 : ((wU >> 12) & 0xFu);
+    const int vb = vown ? b : b - Nx;
+    const int s2 = vn == 4u ? 4 * vb : (vn < 4u ? slot_face_cell((int)vn, vb, Nx) : -1);
+    // face (iy, ix): face slot 0 of (iy, ix), 1 of (iy, ix-1), 2 of (iy-1, ix), 3 of (iy-1, ix-1)
+    const unsigned f0 = (wP >> 16) & 0xFu, f1 = (wL >> 20) & 0xFu, f2 = (wU >> 24) & 0xFu, f3 = wUL >> 28;
+    const unsigned fn = f0 != kNotMine ? f0 : f1 != kNotMine ? f1 : f2 != kNotMine ? f2 : f3;
+    const int fb = f0 != kNotMine ? b : f1 != kNotMine ? b - 1 : f2 != kNotMine ? b - Nx : b - Nx - 1;
+    const int s3 = fn < 4u ? slot_edge_cell((int)fn, fb, Nx) : -1;
+    const size_t gidx = (size_t)(gbase + b);
+    grad[gidx] = make_int4(s0, s1, s2, s3);
+    if (vk < 0 && iy < H && ix < W) m |= 1u;
+    if (hn == 15u) m |= 2u;
+    if (vn == 15u) m |= 4u;
+    if (fn == 15u) m |= 8u;
     crit_mask[gidx] = (uint8_t)m;
-    flow[gidx] = (uint8_t)(vertex_flow(v.x, lidx) | (face_flow(v.w, lidx) << 4));
+    flow[gidx] = (uint8_t)((unsigned)(vk + 1) | (face_flow(s3, b) << 4));
   }
   unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
   unsigned bs1 = __ballot_sync(0xffffffffu, m & 2u);
@@ -285,15 +313,15 @@ __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __r
                                                                const uint32_t* __restrict__ fifo_lut,
                                                                uint8_t* __restrict__ flow) {
   __shared__ float sv[kValY][kValX];
-  __shared__ int tile[4][kTileY][kTileX];  // slot-major: conflict-free per-slot writes
+  __shared__ uint32_t word[kTileY + 1][kTileX + 1];
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY;
-  gradient_tile<DUAL>(img, H, W, y0, x0, tid, sv, tile, fifo_lut);
+  gradient_tile<DUAL>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
   const int warp = tid >> 5, lane = tid & 31;
   if (warp >= kTileY) return;
   const int iy = y0 + warp, ix = x0 + lane;
   if (iy > H) return;
-  gradient_store_row(tile, warp, lane, H, W, iy, ix, 0, iy * gridDim.x + blockIdx.x, grad, crit_mask, flow,
+  gradient_store_row(word, warp, lane, H, W, iy, ix, 0, iy * gridDim.x + blockIdx.x, grad, crit_mask, flow,
                      seg_min, seg_sad, seg_max);
 }
 
@@ -308,7 +336,7 @@ static __global__ void __launch_bounds__(kGradThreads) gradient_batch_kernel(Img
                                                                      const uint32_t* __restrict__ fifo_lut,
                                                                      uint8_t* __restrict__ flow) {
   __shared__ float sv[kValY][kValX];
-  __shared__ int tile[4][kTileY][kTileX];
+  __shared__ uint32_t word[kTileY + 1][kTileX + 1];
   const int tid = threadIdx.x;
   const int b = find_image(I.tile_base, I.B, blockIdx.x);
   const int H = I.H[b], W = I.W[b];
@@ -318,14 +346,14 @@ static __global__ void __launch_bounds__(kGradThreads) gradient_batch_kernel(Img
   const int x0 = tx * kTileX, y0 = ty * kTileY;
   const float* img = img_all + I.px_base[b];
   if (I.dual[b])
-    gradient_tile<true>(img, H, W, y0, x0, tid, sv, tile, fifo_lut);
+    gradient_tile<true>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
   else
-    gradient_tile<false>(img, H, W, y0, x0, tid, sv, tile, fifo_lut);
+    gradient_tile<false>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
   const int warp = tid >> 5, lane = tid & 31;
   if (warp >= kTileY) return;
   const int iy = y0 + warp, ix = x0 + lane;
   if (iy > H) return;
-  gradient_store_row(tile, warp, lane, H, W, iy, ix, I.idx_base[b], I.seg_base[b] + iy * ntx + tx, grad, crit_mask,
+  gradient_store_row(word, warp, lane, H, W, iy, ix, I.idx_base[b], I.seg_base[b] + iy * ntx + tx, grad, crit_mask,
                      flow, seg_min, seg_sad, seg_max);
 }
 
