@@ -7,11 +7,11 @@
 //
 // Layout. The gradient array holds 4 int32 slots per index (y, x) of the
 // (H+1) x (W+1) index grid, i.e. 16 bytes per index; it is the grad_indices
-// output. One CTA owns a 32 x 16 tile of indices and writes it with one int4
-// store per index, so every warp writes 512 contiguous bytes. The cells at a
-// tile's indices are owned (have their highest vertex) in the pixels of the
-// tile plus one halo row above and one halo column to the left, so the CTA
-// evaluates the lower star of (16+1) x (32+1) pixels from a (16+3) x (32+3)
+// output. One CTA owns a 32 x 64 tile of indices and writes it with one int4
+// store per index, so every warp writes 512 contiguous bytes per row. The
+// cells at a tile's indices are owned (have their highest vertex) in the
+// pixels of the tile plus one halo row above and one halo column to the left,
+// so the CTA evaluates the lower star of (64+1) x (32+1) pixels from a (64+3) x (32+3)
 // value tile in shared memory, one 32-bit pairing word per pixel, and every
 // index then gathers its four slots from the words of their owners. Slots of
 // invalid cells are -1.
@@ -27,7 +27,7 @@
 namespace dmsc {
 
 constexpr int kTileX = 32;  // indices per tile row (one warp)
-constexpr int kTileY = 16;  // tile rows (one warp each)
+constexpr int kTileY = 64;  // tile rows
 constexpr int kValX = kTileX + 3;
 constexpr int kValY = kTileY + 3;
 
@@ -99,7 +99,12 @@ inline void face_fifo_table(uint32_t* out) {
 }
 constexpr int kFifoTable = 16 * 16 * 5;
 
-constexpr int kGradThreads = 576;  // >= (kTileY + 1) * (kTileX + 1) = 561 lower stars per tile
+// 16 warps; each thread evaluates about 4 of the (kTileY + 1) x (kTileX + 1)
+// lower stars of a tile and each warp writes kTileY / 16 of its rows, so one
+// CTA's global loads (all issued before their first use) are amortised over
+// 2048 indices.
+constexpr int kGradThreads = 512;
+constexpr int kGradWarps = kGradThreads / 32;
 
 // v_greater (cpu/cell_compare.hxx:23-31) orders pixels by (value, y*W+x),
 // flipped in the dual. gt(a, b) when a's linear id is known to be larger (a "after" b) or smaller:
@@ -215,20 +220,31 @@ __device__ __forceinline__ uint32_t lower_star(const float (*sv)[kValX], int y, 
 }
 
 // Pairing words of the (kTileY + 1) x (kTileX + 1) pixels whose lower stars
-// hold the cells of one 32 x 16 index tile (origin pixel (y0 - 1, x0 - 1)).
+// hold the cells of one 32 x kTileY index tile (origin pixel (y0 - 1, x0 - 1)).
 template <bool DUAL>
 __device__ __forceinline__ void gradient_tile(const float* __restrict__ img, int H, int W, int y0, int x0, int tid,
                                               float (*sv)[kValX], uint32_t (*word)[kTileX + 1],
                                               const uint32_t* __restrict__ fifo_lut) {
-  for (int i = tid; i < kValY * kValX; i += kGradThreads) {
-    int r = i / kValX, c = i - r * kValX;
-    int gy = y0 - 2 + r, gx = x0 - 2 + c;
-    sv[r][c] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(img + (size_t)gy * W + gx) : 0.0f;
+  constexpr int kValN = kValY * kValX;
+  constexpr int kLoads = (kValN + kGradThreads - 1) / kGradThreads;
+  float v[kLoads];
+#pragma unroll
+  for (int k = 0; k < kLoads; ++k) {  // every load in flight before the first shared store
+    const int i = tid + k * kGradThreads;
+    const int r = i / kValX, c = i - r * kValX;
+    const int gy = y0 - 2 + r, gx = x0 - 2 + c;
+    v[k] = (i < kValN && gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(img + (size_t)gy * W + gx) : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < kLoads; ++k) {
+    const int i = tid + k * kGradThreads;
+    if (i < kValN) (&sv[0][0])[i] = v[k];
   }
   __syncthreads();
-  if (tid < (kTileY + 1) * (kTileX + 1)) {
-    int r = tid / (kTileX + 1), c = tid - r * (kTileX + 1);
-    int y = y0 - 1 + r, x = x0 - 1 + c;
+  constexpr int kWordN = (kTileY + 1) * (kTileX + 1);
+  for (int p = tid; p < kWordN; p += kGradThreads) {
+    const int r = p / (kTileX + 1), c = p - r * (kTileX + 1);
+    const int y = y0 - 1 + r, x = x0 - 1 + c;
     uint32_t w = kNoPixel;
     if (y >= 0 && y < H && x >= 0 && x < W) w = lower_star<DUAL>(sv, y, x, H, W, y0, x0, fifo_lut);
     word[r][c] = w;
@@ -242,7 +258,7 @@ __device__ __forceinline__ int slot_edge_cell(int k, int b, int Nx) {
 }
 __device__ __forceinline__ int slot_face_cell(int f, int b, int Nx) { return 3 + 4 * (b + (f >> 1) * Nx + (f & 1)); }
 
-// Write-out of one tile row by one warp. Index (iy, ix) gathers its four
+// Write-out of tile row `warp` by one warp. Index (iy, ix) gathers its four
 // slots from the pairing words of the pixels owning them: its vertex and
 // (when owned there) its H edge, V edge and face from pixel (iy, ix), else
 // the H edge from (iy, ix-1), the V edge from (iy-1, ix) and the face from
@@ -303,7 +319,7 @@ __device__ __forceinline__ void gradient_store_row(const uint32_t (*word)[kTileX
   }
 }
 
-// K1 (one image): gradient over one 32 x 16 index tile per CTA.
+// K1 (one image): gradient over one 32 x 64 index tile per CTA.
 template <bool DUAL>
 __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __restrict__ img, int H, int W,
                                                                int4* __restrict__ grad,
@@ -318,11 +334,12 @@ __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __r
   const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY;
   gradient_tile<DUAL>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
   const int warp = tid >> 5, lane = tid & 31;
-  if (warp >= kTileY) return;
-  const int iy = y0 + warp, ix = x0 + lane;
-  if (iy > H) return;
-  gradient_store_row(word, warp, lane, H, W, iy, ix, 0, iy * gridDim.x + blockIdx.x, grad, crit_mask, flow,
-                     seg_min, seg_sad, seg_max);
+  for (int rr = warp; rr < kTileY; rr += kGradWarps) {
+    const int iy = y0 + rr, ix = x0 + lane;
+    if (iy > H) break;  // uniform per warp
+    gradient_store_row(word, rr, lane, H, W, iy, ix, 0, iy * gridDim.x + blockIdx.x, grad, crit_mask, flow, seg_min,
+                       seg_sad, seg_max);
+  }
 }
 
 // K1 (batch): the tiles of every image of a batch in one 1-D grid; each CTA
@@ -350,11 +367,14 @@ static __global__ void __launch_bounds__(kGradThreads) gradient_batch_kernel(Img
   else
     gradient_tile<false>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
   const int warp = tid >> 5, lane = tid & 31;
-  if (warp >= kTileY) return;
-  const int iy = y0 + warp, ix = x0 + lane;
-  if (iy > H) return;
-  gradient_store_row(word, warp, lane, H, W, iy, ix, I.idx_base[b], I.seg_base[b] + iy * ntx + tx, grad, crit_mask,
-                     flow, seg_min, seg_sad, seg_max);
+  const long long gbase = I.idx_base[b];
+  const int sbase = I.seg_base[b];
+  for (int rr = warp; rr < kTileY; rr += kGradWarps) {
+    const int iy = y0 + rr, ix = x0 + lane;
+    if (iy > H) break;  // uniform per warp
+    gradient_store_row(word, rr, lane, H, W, iy, ix, gbase, sbase + iy * ntx + tx, grad, crit_mask, flow, seg_min,
+                       seg_sad, seg_max);
+  }
 }
 
 // cell_value (cpu/cell_compare.hxx:82-87): value of the highest (dual: lowest)
