@@ -362,7 +362,7 @@ def b200_arm(args):
                      "algorithmic_bytes": grad_bytes, "avg_ms": grad_ms,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6.65 TB/s"},
-        "roofline_segmentation": {"bound": "hbm", "kernel": "label_kernel x2", "achieved": seg, "peak": peak,
+        "roofline_segmentation": {"bound": "hbm", "kernel": "label stage (label_tile_kernel + label_exit_kernel x2)", "achieved": seg, "peak": peak,
                                   "unit": "GB/s", "frac": (seg / peak) if seg else None,
                                   "algorithmic_bytes": seg_bytes, "avg_ms": lab_ms},
         "stage_ms_per_step": {k: v / args.steps for k, v in stage_sum.items()},

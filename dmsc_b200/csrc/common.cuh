@@ -141,6 +141,7 @@ struct Imgs {
   const int* px_base;    // pixels
   const int* tile_base;  // 32 x 16 gradient tiles
   const int* seg_base;   // 32-index row segments
+  const int* ltile_base;  // 64 x 64 label tiles
   const uint8_t* dual;
   const float* thr;
 };

@@ -11,6 +11,7 @@
 // reference does (dmsc_cpu.cpp:34-37, workspace.hxx:322-362).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cub/cub.cuh>
 #include <cstdarg>
 #include <cstdio>
@@ -38,14 +39,14 @@ enum Slot {
   S_GRAD, S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
   S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
   S_ASC, S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
-  S_BKEY, S_BIDX, S_BKEY2, S_BIDX2,
+  S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
   X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
   X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_CTIME, X_STAT, X_PAR, X_WLEN, X_SIDE,
   X_CSAD, X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G1,
-  X_G2, X_GBASE, kSideSlots
+  X_G2, X_GBASE, X_LAB, kSideSlots
 };
 
 struct Buf {
@@ -512,7 +513,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     return kErrInvalidArgument;
   }
   // per-image tables (host): 32-bit cell ids per image (input_validation.hxx:24-26) and for the batch
-  std::vector<int> tab(8 * (size_t)(B + 1), 0);
+  std::vector<int> tab(9 * (size_t)(B + 1), 0);
   int* tH = tab.data();
   int* tW = tH + (B + 1);
   int* idx_base = tW + (B + 1);
@@ -521,7 +522,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   int* seg_base = tile_base + (B + 1);
   int* peaks_off = seg_base + (B + 1);
   int* basins_off = peaks_off + (B + 1);
-  long long nidx = 0, npx = 0, ntile = 0, nseg = 0, npk = 0, nbs = 0;
+  int* ltile_base = basins_off + (B + 1);
+  long long nidx = 0, npx = 0, ntile = 0, nseg = 0, npk = 0, nbs = 0, nltile = 0;
   bool any_primal = false, any_dual = false;
   for (int b = 0; b < B; ++b) {
     const long long H = hH[b], W = hW[b];
@@ -541,6 +543,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     seg_base[b] = (int)nseg;
     peaks_off[b] = (int)npk;
     basins_off[b] = (int)nbs;
+    ltile_base[b] = (int)nltile;
+    nltile += ((W + kLT) / kLT) * ((H + kLT) / kLT);
     const long long ntx = (W + 1 + kTileX - 1) / kTileX, nty = (H + 1 + kTileY - 1) / kTileY;
     nidx += (H + 1) * (W + 1);
     npx += H * W;
@@ -560,6 +564,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   seg_base[B] = (int)nseg;
   peaks_off[B] = (int)npk;
   basins_off[B] = (int)nbs;
+  ltile_base[B] = (int)nltile;
   CK(cudaSetDevice(ctx->device));
   ctx->B = B;
   ctx->flags = flags;
@@ -574,7 +579,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   CK(cudaMemsetAsync(get<int>(ctx, S_STATS, 8), 0, 8 * sizeof(int), st));
   CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline), 0,
                      4 * kTimeline * sizeof(unsigned long long), st));
-  {  // upload the tables: 8 int arrays, then thr (float) and dual (u8)
+  {  // upload the tables: 9 int arrays, then thr (float) and dual (u8)
     size_t ib = tab.size() * sizeof(int), fb = (size_t)B * sizeof(float);
     size_t total = ib + fb + B + 16;
     char* h = (char*)staging(ctx, total);
@@ -591,6 +596,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     ctx->I.px_base = di + 3 * (B + 1);
     ctx->I.tile_base = di + 4 * (B + 1);
     ctx->I.seg_base = di + 5 * (B + 1);
+    ctx->I.ltile_base = di + 8 * (B + 1);
     ctx->I.thr = (const float*)(d + ib);
     ctx->I.dual = (const uint8_t*)(d + ib + fb);
   }
@@ -756,9 +762,10 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   }
 
   // ---- labels (region id = rank among the image's alive extrema) ----
+  LabelOut OF{}, OV{};
+  LabelSide LF{}, LV{};
   for (int si = 0; si < 2; ++si) {
     Side& S = ctx->side[si];
-    int* map = S.rank_map;  // dense ranks are no longer needed: reuse as the label map
     // alive bases first (needed by the labels and the outputs)
     long long* at = get<long long>(ctx, S_TOT, 8) + 4 + si;
     if (S.M > 0)
@@ -769,7 +776,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
                                                                    at, BS.alive[si]));
     LAUNCH_CHECK("alive bases");
     if (!S.groups) continue;
-    LabelOut O;
+    LabelOut& O = S.faces ? OF : OV;
     if (S.faces) {
       O.primal = f_peaks ? peaks_out : nullptr;
       O.dual = f_basins ? basins_out : nullptr;
@@ -781,14 +788,29 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
       O.primal_off = d_basins_off;
       O.dual_off = d_peaks_off;
     }
+    LabelSide& L = S.faces ? LF : LV;
+    int* lab = sget<int>(ctx, si, X_LAB, S.M + 1);
+    L.off = S.faces ? off[2] : off[0];
+    L.lab = lab;
+    L.perim = get<int>(ctx, S.faces ? S_PERF : S_PERV, (size_t)nltile * kPerim);
     if (S.M > 0)
-      LK(label_map_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.crit, S.ext_img, S.ut, S.to_out, BS.alive[si], map));
-    long long n = S.faces ? nidx : npx;
-    if (S.faces)
-      LK(label_kernel<true><<<grid_for(n, TB), TB, 0, st>>>(I, flow, n, map, O, ncells, ctx->status));
-    else
-      LK(label_kernel<false><<<grid_for(n, TB), TB, 0, st>>>(I, flow, n, map, O, ncells, ctx->status));
-    LAUNCH_CHECK("label_kernel");
+      LK(label_map_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.ext_img, S.ut, S.to_out, BS.alive[si], lab));
+    LAUNCH_CHECK("label_map_kernel");
+  }
+  if (F.groups || V.groups) {
+    int2* exf = F.groups ? get<int2>(ctx, S_EXF, nidx) : nullptr;
+    int2* exv = V.groups ? get<int2>(ctx, S_EXV, nidx) : nullptr;
+    int* nex = get<int>(ctx, S_NEX, 2);
+    CK(cudaMemsetAsync(nex, 0, 2 * sizeof(int), st));
+    LK(label_tile_kernel<<<(unsigned)nltile, kLabelThreads, 0, st>>>(I, flow, LF, LV, OF, OV, exf, exv, nex,
+                                                                    ctx->status));
+    LAUNCH_CHECK("label_tile_kernel");
+    int per = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, label_exit_kernel<true>, 256, 0));
+    const unsigned eg = (unsigned)std::max(1, per) * ctx->num_sms;
+    if (F.groups) LK(label_exit_kernel<true><<<eg, 256, 0, st>>>(I, exf, nex + 0, LF.perim, OF, (int)nltile + 2, ctx->status));
+    if (V.groups) LK(label_exit_kernel<false><<<eg, 256, 0, st>>>(I, exv, nex + 1, LV.perim, OV, (int)nltile + 2, ctx->status));
+    LAUNCH_CHECK("label_exit_kernel");
   }
   mark(ctx, 10, st);
 
