@@ -73,7 +73,7 @@ class ClockSampler:
         try:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -274,14 +274,25 @@ def b200_arm(args):
             gpu_out[VARIANTS[w % 4]] = [x.cpu() for x in ms]
     torch.cuda.synchronize()
 
-    # ---- timed region: device-resident input ----
+    # ---- profiling pass (untimed): per-stage device times, loop counts and
+    # the library's own kernel launches of the same K steps ----
     ctx.set_profiling(True)
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
     stage_sum = {}
     launches = 0
     loops = []
+    for k in range(args.steps):
+        step(k)
+        for name, v in ctx.stage_times().items():
+            stage_sum[name] = stage_sum.get(name, 0.0) + v
+        launches += ctx.launch_count()
+        loops.append(ctx.loop_counts())
+    ctx.set_profiling(False)
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident input, K plain calls ----
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -290,17 +301,12 @@ def b200_arm(args):
     e0.record(st)
     for k in range(args.steps):
         step(k)
-        for name, v in ctx.stage_times().items():
-            stage_sum[name] = stage_sum.get(name, 0.0) + v
-        launches += ctx.launch_count()
-        loops.append(ctx.loop_counts())
     e1.record(st)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     ms_total = e0.elapsed_time(e1)
     clk = clocks.stop()  # clocks cover the device-timed region
-    ctx.set_profiling(False)
     t = torch.tensor([ms_total], device=dev)
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

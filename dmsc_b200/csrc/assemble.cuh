@@ -190,11 +190,11 @@ __global__ void pair_len_kernel(int nsurv, const long long* __restrict__ arc_len
 // Geometry start of every image on one side (B + 1 entries).
 __global__ void geom_base_kernel(int B, const int* __restrict__ surv_base, int nsurv,
                                  const long long* __restrict__ saddle_end_incl, const long long* __restrict__ plen,
-                                 long long total, long long* __restrict__ gbase) {
+                                 const long long* __restrict__ total, long long* __restrict__ gbase) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b > B) return;
   int f = b < B ? surv_base[b] : nsurv;
-  gbase[b] = f < nsurv ? saddle_end_incl[f] - plen[f] : total;
+  gbase[b] = f < nsurv ? saddle_end_incl[f] - plen[f] : *total;
 }
 
 // Output position of every arc: the image's destination offset plus the

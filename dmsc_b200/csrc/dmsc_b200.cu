@@ -139,6 +139,8 @@ struct dmsc_b200_context {
   uint32_t* fifo_lut = nullptr;  // face-pairing FIFO table (device)
   int num_sms = 0;
   cudaEvent_t ev[kStageMarks] = {};
+  cudaEvent_t sync_ev = nullptr;   // polled by wait_stream
+  unsigned* pstatus = nullptr;     // pinned copy of the device status word
 };
 
 
@@ -286,16 +288,27 @@ void coop_launch(dmsc_b200_context* ctx, void (*kernel)(T), T args, cudaStream_t
   ++ctx->launches;
 }
 
+// Waits until the stream has drained by polling an event: the host thread
+// spins instead of sleeping in the driver, so the next launches follow the
+// readback without an operating-system wake-up delay (the few host round
+// trips of a call are on its critical path).
+void wait_stream(dmsc_b200_context* ctx, cudaStream_t st) {
+  CK(cudaEventRecord(ctx->sync_ev, st));
+  while (true) {
+    const cudaError_t e = cudaEventQuery(ctx->sync_ev);
+    if (e == cudaSuccess) return;
+    if (e != cudaErrorNotReady) CK(e);
+  }
+}
+
 // Host read of `k` pinned scalars after the stream drains.
 void readback(dmsc_b200_context* ctx, cudaStream_t st, const long long* dev, int k) {
   CK(cudaMemcpyAsync(ctx->pinned, dev, k * sizeof(long long), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  wait_stream(ctx, st);
 }
 
-void check_status(dmsc_b200_context* ctx, cudaStream_t st) {
-  unsigned h = 0;
-  CK(cudaMemcpyAsync(&h, ctx->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+// Error of a device status word (0: none).
+void raise_status(dmsc_b200_context* ctx, unsigned h) {
   if (h & (kStatusWalkCap | kStatusRoundCap | kStatusChainCap)) {
     set_err(ctx, "a bounded device loop reached its cap (status 0x%x)", h);
     throw Fail{kErrIterationCap};
@@ -308,6 +321,12 @@ void check_status(dmsc_b200_context* ctx, cudaStream_t st) {
     set_err(ctx, "device status 0x%x", h);
     throw Fail{kErrInternal};
   }
+}
+
+void check_status(dmsc_b200_context* ctx, cudaStream_t st) {
+  CK(cudaMemcpyAsync(ctx->pstatus, ctx->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  wait_stream(ctx, st);
+  raise_status(ctx, *ctx->pstatus);
 }
 
 
@@ -326,50 +345,56 @@ void* staging(dmsc_b200_context* ctx, size_t bytes) {
   return ctx->pinned;
 }
 
-// Persistence pairing of one side over the whole batch (see pairing.cuh).
-void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, cudaStream_t st) {
+// Sweep-ordered edges and the pairing arguments of one side (see pairing.cuh).
+PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, cudaStream_t st) {
   const int nsad = ctx->nsad, M = S.M;
   S.sweep = sget<int>(ctx, si, X_SWEEP, nsad);
   S.c1 = sget<int>(ctx, si, X_C1, nsad);
   S.c2 = sget<int>(ctx, si, X_C2, nsad);
   S.dying = sget<int>(ctx, si, X_DYING, nsad);
-  int* grp = sget<int>(ctx, si, X_GRP, M + 1);
-  int* link = sget<int>(ctx, si, X_LINK, M + 1);
-  unsigned* minedge = sget<unsigned>(ctx, si, X_MINE, M + 1);
-  int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
-  int* cnt = sget<int>(ctx, si, X_CNT, 8);
   if (nsad > 0) {
     LK(sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, ctx->sad_img, ctx->bases.sad, ctx->I.dual,
                                                              S.faces, S.t, S.sweep, S.c1, S.c2));
     LAUNCH_CHECK("sweep_edges_kernel");
-    PairArgs A;
-    A.nsad = nsad;
-    A.M = M;
-    A.c1 = S.c1;
-    A.c2 = S.c2;
-    A.g1 = sget<int>(ctx, si, X_G1, nsad);
-    A.g2 = sget<int>(ctx, si, X_G2, nsad);
-    A.dying = S.dying;
-    A.link = link;
-    A.minedge = minedge;
-    A.act0 = act[0];
-    A.act1 = act[1];
-    A.roots0 = grp;  // [M+1]
-    A.roots1 = sget<int>(ctx, si, X_UF, M + 1);
-    A.hdec = sget<int>(ctx, si, X_CROOT, M + 1);
-    A.cnt = cnt;
-    A.val = S.val;
-    A.cell = S.crit;
-    A.ext_img = S.ext_img;
-    A.dual = ctx->I.dual;
-    A.faces = S.faces;
-    A.status = ctx->status;
-    A.max_rounds = M + 2;
-    A.rounds = get<int>(ctx, S_STATS, 8) + 0 + si;
-    A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline) + si * kTimeline;
-    coop_launch(ctx, pairing_persistent_kernel, A, st, "pairing_persistent_kernel");
   }
+  PairArgs A;
+  A.nsad = nsad;
+  A.M = M;
+  A.c1 = S.c1;
+  A.c2 = S.c2;
+  A.g1 = sget<int>(ctx, si, X_G1, nsad);
+  A.g2 = sget<int>(ctx, si, X_G2, nsad);
+  A.dying = S.dying;
+  A.link = sget<int>(ctx, si, X_LINK, M + 1);
+  A.minedge = sget<unsigned>(ctx, si, X_MINE, M + 1);
+  A.act0 = sget<int>(ctx, si, X_ACT0, nsad);
+  A.act1 = sget<int>(ctx, si, X_ACT1, nsad);
+  A.roots0 = sget<int>(ctx, si, X_GRP, M + 1);
+  A.roots1 = sget<int>(ctx, si, X_UF, M + 1);
+  A.hdec = sget<int>(ctx, si, X_CROOT, M + 1);
+  A.cnt = sget<int>(ctx, si, X_CNT, 8);
+  A.val = S.val;
+  A.cell = S.crit;
+  A.ext_img = S.ext_img;
+  A.dual = ctx->I.dual;
+  A.faces = S.faces;
+  A.status = ctx->status;
+  A.max_rounds = M + 2;
+  A.rounds = get<int>(ctx, S_STATS, 8) + 0 + si;
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline) + si * kTimeline;
+  return A;
+}
 
+// Both sides' pairing rounds in one cooperative launch.
+void run_pairing(dmsc_b200_context* ctx, const int* asc, cudaStream_t st) {
+  PairArgs2 P;
+  for (int si = 0; si < 2; ++si) P.s[si] = pairing_args(ctx, si, ctx->side[si], asc, st);
+  if (ctx->nsad > 0) coop_launch(ctx, pairing_persistent_kernel, P, st, "pairing_persistent_kernel");
+}
+
+// Persistence, cancellation, thresholded union-find and output ranks of one side.
+void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
+  const int nsad = ctx->nsad, M = S.M;
   // persistence, cancellation, alive flags
   S.pair_dense = sget<int>(ctx, si, X_PAIR, nsad);
   S.pers = sget<float>(ctx, si, X_PERS, nsad);
@@ -408,9 +433,10 @@ void run_pairing(dmsc_b200_context* ctx, int si, Side& S, const int* asc, cudaSt
   }
 }
 
-// Replay of one side's cancellations and the final arc lengths (batch).
-void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
-  const int nsad = ctx->nsad, M = S.M, nsurv = ctx->nsurv;
+// Replay inputs of one side (batch); returns the replay kernel's arguments,
+// with n_cancel == nullptr when the side has no cancellation to replay.
+ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
+  const int nsad = ctx->nsad, M = S.M;
   S.blen = sget<long long>(ctx, si, X_BLEN, 2 * (size_t)nsad);
   if (nsad > 0) LK(base_len_kernel<<<grid_for(2LL * nsad, TB), TB, 0, st>>>(2 * nsad, S.t, S.steps, S.blen));
   unsigned long long* ckey = sget<unsigned long long>(ctx, si, X_CKEY, nsad);
@@ -434,56 +460,43 @@ void run_replay(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   LK(fill_u64_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.ctime, M + 1, kNever));
   LK(fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.status, M + 1, kRootForever));
   LAUNCH_CHECK("replay init");
-  int* act[2] = {sget<int>(ctx, si, X_ACT0, nsad), sget<int>(ctx, si, X_ACT1, nsad)};
-  const int max_steps = nsad + 1;
-  if (S.C > 0) {
-    ReplayArgs A;
-    A.n_cancel = cnt + 3;
-    A.key = ckey;
-    A.cj = cval;
-    A.sweep = S.sweep;
-    A.dying = S.dying;
-    A.c1 = S.c1;
-    A.c2 = S.c2;
-    A.blen = S.blen;
-    A.S = R;
-    A.max_steps = max_steps;
-    A.act0 = act[0];
-    A.act1 = act[1];
-    A.cnt = cnt;
-    A.status = ctx->status;
-    A.max_rounds = nsad + 2;
-    A.rounds = get<int>(ctx, S_STATS, 8) + 2 + si;
-    coop_launch(ctx, replay_persistent_kernel, A, st, "replay_persistent_kernel");
-  }
+  ReplayArgs A{};
+  A.n_cancel = S.C > 0 ? cnt + 3 : nullptr;
+  A.key = ckey;
+  A.cj = cval;
+  A.sweep = S.sweep;
+  A.dying = S.dying;
+  A.c1 = S.c1;
+  A.c2 = S.c2;
+  A.blen = S.blen;
+  A.S = R;
+  A.max_steps = nsad + 1;
+  A.act0 = sget<int>(ctx, si, X_ACT0, nsad);
+  A.act1 = sget<int>(ctx, si, X_ACT1, nsad);
+  A.cnt = cnt;
+  A.status = ctx->status;
+  A.max_rounds = nsad + 2;
+  A.rounds = get<int>(ctx, S_STATS, 8) + 2 + si;
+  return A;
+}
 
+// Final arcs of one side's survivors after the replay: lengths, chain roots
+// and the side's geometry total (device, into *total).
+void replay_final(dmsc_b200_context* ctx, int si, Side& S, long long* total, cudaStream_t st) {
+  const int nsurv = ctx->nsurv;
   S.arc_len = sget<long long>(ctx, si, X_ALEN, 2 * (size_t)nsurv);
   S.arc_cl = sget<long long>(ctx, si, X_ACL, 2 * (size_t)nsurv);
   S.arc_root = sget<int>(ctx, si, X_AROOT, 2 * (size_t)nsurv);
   S.plen = sget<long long>(ctx, si, X_PLEN, nsurv);
   S.send = sget<long long>(ctx, si, X_SEND, nsurv);
-  S.gbase = sget<long long>(ctx, si, X_GBASE, ctx->B + 1);
-  S.total = 0;
-  if (nsurv > 0) {
-    long long* tot = get<long long>(ctx, S_TOT, 8);
-    LK(final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->sad_img, ctx->I.dual,
-                                                                   S.arcs_primal, S.arcs_dual, S.t, S.blen, R,
-                                                                   max_steps, S.arc_len, S.arc_cl, S.arc_root,
-                                                                   ctx->status));
-    LK(pair_len_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.plen));
-    incl_sum(ctx, S.plen, S.send, nsurv, st);
-    LK(last_kernel<long long><<<1, 1, 0, st>>>(S.send, nsurv, tot));
-    LAUNCH_CHECK("final arcs");
-    readback(ctx, st, tot, 1);
-    S.total = ctx->pinned[0];
-    if (S.total > 2147483647LL) {
-      set_err(ctx, "arc geometry of %lld cells exceeds int32 offsets", S.total);
-      throw Fail{kErrOverflow};
-    }
-  }
-  LK(geom_base_kernel<<<grid_for(ctx->B + 1LL, TB), TB, 0, st>>>(ctx->B, ctx->bases.surv, nsurv, S.send, S.plen,
-                                                                 S.total, S.gbase));
-  LAUNCH_CHECK("geom_base_kernel");
+  LK(final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->sad_img, ctx->I.dual,
+                                                                 S.arcs_primal, S.arcs_dual, S.t, S.blen, S.R,
+                                                                 ctx->nsad + 1, S.arc_len, S.arc_cl, S.arc_root,
+                                                                 ctx->status));
+  LK(pair_len_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.plen));
+  incl_sum(ctx, S.plen, S.send, nsurv, st);
+  LK(last_kernel<long long><<<1, 1, 0, st>>>(S.send, nsurv, total));
+  LAUNCH_CHECK("final arcs");
 }
 
 // Number of bits needed for values 0 .. n-1 (at least 1).
@@ -722,9 +735,10 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
   mark(ctx, 4, st);
   CK(cudaMemsetAsync(canc, 0, nsad + 4, st));
-  run_pairing(ctx, 0, F, asc, st);
+  run_pairing(ctx, asc, st);
   mark(ctx, 5, st);
-  run_pairing(ctx, 1, V, asc, st);
+  finish_pairing(ctx, 0, F, st);
+  finish_pairing(ctx, 1, V, st);
   mark(ctx, 6, st);
 
   // ---- surviving saddles in minima-sweep (vertex side) order ----
@@ -749,16 +763,37 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   LAUNCH_CHECK("survivor bases");
   mark(ctx, 7, st);
 
-  // ---- replay + final arc lengths ----
-  for (int si = 0; si < 2; ++si) {
-    Side& S = ctx->side[si];
-    if (S.arcs && nsad > 0) {
-      run_replay(ctx, si, S, st);
-    } else {
-      S.gbase = sget<long long>(ctx, si, X_GBASE, B + 1);
-      CK(cudaMemsetAsync(S.gbase, 0, (B + 1) * sizeof(long long), st));
+  // ---- replay (both sides in one cooperative launch) + final arc lengths ----
+  {
+    ReplayArgs2 RA{};
+    bool any = false;
+    for (int si = 0; si < 2; ++si) {
+      Side& S = ctx->side[si];
+      RA.s[si].status = ctx->status;
+      if (S.arcs && nsad > 0) {
+        RA.s[si] = replay_prepare(ctx, si, S, st);
+        any = any || RA.s[si].n_cancel != nullptr;
+      }
     }
-    mark(ctx, 8 + si, st);
+    if (any) coop_launch(ctx, replay_persistent_kernel, RA, st, "replay_persistent_kernel");
+    mark(ctx, 8, st);
+    // geometry totals stay on the device (read back with the sizes)
+    long long* tot = get<long long>(ctx, S_TOT, 8);
+    CK(cudaMemsetAsync(tot, 0, 2 * sizeof(long long), st));
+    for (int si = 0; si < 2; ++si) {
+      Side& S = ctx->side[si];
+      S.gbase = sget<long long>(ctx, si, X_GBASE, B + 1);
+      S.total = 0;
+      if (S.arcs && nsad > 0) {
+        if (nsurv > 0) replay_final(ctx, si, S, tot + si, st);
+        LK(geom_base_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, BS.surv, nsurv, S.send, S.plen, tot + si,
+                                                                  S.gbase));
+        LAUNCH_CHECK("geom_base_kernel");
+      } else {
+        CK(cudaMemsetAsync(S.gbase, 0, (B + 1) * sizeof(long long), st));
+      }
+    }
+    mark(ctx, 9, st);
   }
 
   // ---- labels (region id = rank among the image's alive extrema) ----
@@ -840,13 +875,22 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     CK(cudaMemcpyAsync(h + ib, F.gbase, (B + 1) * sizeof(long long), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(h + ib + (B + 1) * sizeof(long long), V.gbase, (B + 1) * sizeof(long long),
                        cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpyAsync(ctx->pstatus, ctx->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    wait_stream(ctx, st);
     mark(ctx, 11, st);
+    raise_status(ctx, *ctx->pstatus);
     const int* hb = (const int*)h;
     const int* hsurv = hb + 3 * (B + 1);
     const int* hal[2] = {hb + 4 * (B + 1), hb + 5 * (B + 1)};
     const int* her[2] = {hb + 6 * (B + 1), hb + 7 * (B + 1)};
     const long long* hg[2] = {(const long long*)(h + ib), (const long long*)(h + ib) + (B + 1)};
+    for (int si = 0; si < 2; ++si) {
+      ctx->side[si].total = hg[si][B];
+      if (hg[si][B] > 2147483647LL) {
+        set_err(ctx, "arc geometry of %lld cells exceeds int32 offsets", hg[si][B]);
+        throw Fail{kErrOverflow};
+      }
+    }
     ctx->sizes.assign(B, dmsc_b200_sizes{});
     ctx->geom[0].assign(B, 0);
     ctx->geom[1].assign(B, 0);
@@ -878,7 +922,6 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
       sizes_out[b] = z;
     }
   }
-  check_status(ctx, st);
   ctx->valid = true;
   return kOk;
 }
@@ -1107,6 +1150,13 @@ int dmsc_b200_create(dmsc_b200_context** out, int device) {
     return kErrCuda;
   }
   c->pinned_cap = 64 * sizeof(long long);
+  if (cudaEventCreateWithFlags(&c->sync_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost(&c->pstatus, sizeof(unsigned)) != cudaSuccess) {
+    if (c->sync_ev) cudaEventDestroy(c->sync_ev);
+    cudaFreeHost(c->pinned);
+    delete c;
+    return kErrCuda;
+  }
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
   {
     std::vector<uint32_t> lut(kFifoTable);
@@ -1130,6 +1180,8 @@ void dmsc_b200_destroy(dmsc_b200_context* c) {
   if (c->cub_tmp.p) cudaFree(c->cub_tmp.p);
   if (c->fifo_lut) cudaFree(c->fifo_lut);
   if (c->pinned) cudaFreeHost(c->pinned);
+  if (c->pstatus) cudaFreeHost(c->pstatus);
+  if (c->sync_ev) cudaEventDestroy(c->sync_ev);
   for (int k = 0; k < kStageMarks; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   delete c;

@@ -75,122 +75,159 @@ struct PairArgs {
   unsigned long long* timeline;  // [kTimeline] round start times (ns), optional
 };
 
-// One side's persistence pairing. Per round: (A) every active saddle finds its
+// Both sides' persistence pairing in one cooperative launch; each round
+// processes both sides' active saddles and live roots, so the two sides share
+// their grid barriers. Per round and side: (A) every active saddle finds its
 // ends' groups, cycles are decided, the rest reduce their sweep index into
 // both groups' minimum (no returned value needed) and stay active; (B1) every
 // live root with an outgoing saddle decides whether it dies there and stays
 // live otherwise; roots without outgoing saddles leave the list for good;
 // (B2) the links are applied. Round 0 skips the lookups: all groups are
-// single extrema.
-__global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs A) {
+// single extrema. A side whose active list is empty just idles.
+struct PairArgs2 {
+  PairArgs s[2];
+};
+
+__device__ __forceinline__ void pair_phase_a(const PairArgs& A, int r, long long i, int n, bool& keep, int& e) {
+  keep = false;
+  e = -1;
+  if (i < 0 || i >= n) return;
+  const int* in = (r & 1) ? A.act1 : A.act0;
+  const int M = A.M;
+  e = in[i];
+  if (r == 0 || A.dying[e] == kUndecided) {
+    int ga, gb;
+    if (r == 0) {
+      int a = A.c1[e], b = A.c2[e];
+      ga = a < 0 ? M : a;
+      gb = b < 0 ? M : b;
+    } else {  // the ends' groups of the previous round, followed to their roots
+      ga = find_halving(A.link, A.g1[e]);
+      gb = find_halving(A.link, A.g2[e]);
+    }
+    if (ga == gb) {
+      A.dying[e] = -1;
+    } else {
+      A.g1[e] = ga;
+      A.g2[e] = gb;
+      atomicMin(A.minedge + ga, (unsigned)e);  // result unused: a reduction
+      atomicMin(A.minedge + gb, (unsigned)e);
+      keep = true;
+    }
+  }
+}
+
+__device__ __forceinline__ void pair_phase_b1(const PairArgs& A, int r, long long k, int nr, bool& live, int& g) {
+  live = false;
+  g = -1;
+  if (k < 0 || k >= nr) return;
+  const int* rin = (r & 1) ? A.roots1 : A.roots0;
+  const int M = A.M;
+  int h = -1;
+  g = rin[k];
+  unsigned me = A.minedge[g];
+  if (me != kNoEdge) {
+    A.minedge[g] = kNoEdge;
+    int e = (int)me;
+    int ga = A.g1[e], gb = A.g2[e];  // roots as of phase A; links change only in B2
+    h = (ga == g) ? gb : ga;
+    // g is an extremum of one image (the void never dies); older = value_less
+    // order on the vertex side in the primal and the face side in the dual
+    const bool du = g < M && A.dual[A.ext_img[g]];
+    if (older(h, g, M, A.val, A.cell, A.faces ? du : !du)) {
+      A.dying[e] = g;
+    } else {
+      h = -1;
+      live = true;
+    }
+  }
+  A.hdec[k] = h;
+}
+
+__global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs2 P) {
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
-  const int M = A.M;
-  for (long long i = tid; i <= M; i += nth) {
-    A.link[i] = (int)i;
-    A.minedge[i] = kNoEdge;
-    A.roots0[i] = (int)i;
-  }
-  for (long long i = tid; i < A.nsad; i += nth) {
-    A.act0[i] = (int)i;
-    A.dying[i] = kUndecided;
-  }
-  if (tid == 0) {
-    A.cnt[0] = A.nsad;
-    A.cnt[1] = 0;
-    A.cnt[2] = 0;
-    A.cnt[3] = M + 1;
-    A.cnt[4] = 0;
-    A.cnt[5] = 0;
+  for (int sd = 0; sd < 2; ++sd) {
+    const PairArgs& A = P.s[sd];
+    for (long long i = tid; i <= A.M; i += nth) {
+      A.link[i] = (int)i;
+      A.minedge[i] = kNoEdge;
+      A.roots0[i] = (int)i;
+    }
+    for (long long i = tid; i < A.nsad; i += nth) {
+      A.act0[i] = (int)i;
+      A.dying[i] = kUndecided;
+    }
+    if (tid == 0) {
+      A.cnt[0] = A.nsad;
+      A.cnt[1] = 0;
+      A.cnt[2] = 0;
+      A.cnt[3] = A.M + 1;
+      A.cnt[4] = 0;
+      A.cnt[5] = 0;
+    }
   }
   grid.sync();
+  bool done0 = false, done1 = false;
   for (int r = 0;; ++r) {
-    const int n = *(volatile int*)(A.cnt + r % 3);
-    const int nr = *(volatile int*)(A.cnt + 3 + r % 3);
-    if (tid == 0 && A.timeline && r < kTimeline) A.timeline[r] = global_ns();
-    if (n == 0) {
-      if (tid == 0 && A.rounds) *A.rounds = r;
-      break;
-    }
-    if (r >= A.max_rounds) {
-      if (tid == 0) set_status(A.status, kStatusRoundCap);
-      break;
-    }
-    const int* in = (r & 1) ? A.act1 : A.act0;
-    int* out = (r & 1) ? A.act0 : A.act1;
-    const int* rin = (r & 1) ? A.roots1 : A.roots0;
-    int* rout = (r & 1) ? A.roots0 : A.roots1;
-    int* ocnt = A.cnt + (r + 1) % 3;
-    int* rcnt = A.cnt + 3 + (r + 1) % 3;
+    const int n0 = *(volatile int*)(P.s[0].cnt + r % 3), n1 = *(volatile int*)(P.s[1].cnt + r % 3);
+    // a side whose active list is empty is finished: its roots are not visited
+    const int nr0 = n0 ? *(volatile int*)(P.s[0].cnt + 3 + r % 3) : 0;
+    const int nr1 = n1 ? *(volatile int*)(P.s[1].cnt + 3 + r % 3) : 0;
     if (tid == 0) {
-      A.cnt[(r + 2) % 3] = 0;
-      A.cnt[3 + (r + 2) % 3] = 0;
-    }
-    // phase A (block-uniform trip count: tid = block offset + threadIdx.x)
-    for (long long base = 0; base < n; base += nth) {
-      long long i = base + tid;
-      bool keep = false;
-      int e = -1;
-      if (i < n) {
-        e = in[i];
-        if (r == 0 || A.dying[e] == kUndecided) {
-          int ga, gb;
-          if (r == 0) {
-            int a = A.c1[e], b = A.c2[e];
-            ga = a < 0 ? M : a;
-            gb = b < 0 ? M : b;
-          } else {  // the ends' groups of the previous round, followed to their roots
-            ga = find_halving(A.link, A.g1[e]);
-            gb = find_halving(A.link, A.g2[e]);
-          }
-          if (ga == gb) {
-            A.dying[e] = -1;
-          } else {
-            A.g1[e] = ga;
-            A.g2[e] = gb;
-            atomicMin(A.minedge + ga, (unsigned)e);  // result unused: a reduction
-            atomicMin(A.minedge + gb, (unsigned)e);
-            keep = true;
-          }
-        }
+      for (int sd = 0; sd < 2; ++sd) {
+        const PairArgs& A = P.s[sd];
+        const int n = sd ? n1 : n0;
+        bool& done = sd ? done1 : done0;
+        if (A.timeline && r < kTimeline && !done) A.timeline[r] = global_ns();
+        if (n == 0 && !done && A.rounds) *A.rounds = r;
+        done = done || n == 0;
       }
-      int p = block_reserve(ocnt, keep ? 1 : 0);
-      if (keep) out[p] = e;
+    }
+    if (n0 == 0 && n1 == 0) break;
+    if (r >= max(P.s[0].max_rounds, P.s[1].max_rounds)) {
+      if (tid == 0) set_status(P.s[0].status, kStatusRoundCap);
+      break;
+    }
+    if (tid == 0) {
+      for (int sd = 0; sd < 2; ++sd) {
+        P.s[sd].cnt[(r + 2) % 3] = 0;
+        P.s[sd].cnt[3 + (r + 2) % 3] = 0;
+      }
+    }
+    // phase A over both sides' active saddles (block-uniform trip count)
+    for (long long base = 0; base < (long long)n0 + n1; base += nth) {
+      const long long i = base + tid;
+      bool k0, k1;
+      int e0, e1;
+      pair_phase_a(P.s[0], r, i, n0, k0, e0);
+      pair_phase_a(P.s[1], r, i - n0, i >= n0 ? n1 : 0, k1, e1);
+      const int p0 = block_reserve(P.s[0].cnt + (r + 1) % 3, k0 ? 1 : 0);
+      const int p1 = block_reserve(P.s[1].cnt + (r + 1) % 3, k1 ? 1 : 0);
+      if (k0) ((r & 1) ? P.s[0].act0 : P.s[0].act1)[p0] = e0;
+      if (k1) ((r & 1) ? P.s[1].act0 : P.s[1].act1)[p1] = e1;
     }
     grid.sync();
     // phase B1: live roots decide on their first outgoing saddle
-    for (long long base = 0; base < nr; base += nth) {
-      long long k = base + tid;
-      bool live = false;
-      int g = -1, h = -1;
-      if (k < nr) {
-        g = rin[k];
-        unsigned me = A.minedge[g];
-        if (me != kNoEdge) {
-          A.minedge[g] = kNoEdge;
-          int e = (int)me;
-          int ga = A.g1[e], gb = A.g2[e];  // roots as of phase A; links change only in B2
-          h = (ga == g) ? gb : ga;
-          // g is an extremum of one image (the void never dies); older = value_less
-          // order on the vertex side in the primal and the face side in the dual
-          const bool du = g < M && A.dual[A.ext_img[g]];
-          if (older(h, g, M, A.val, A.cell, A.faces ? du : !du)) {
-            A.dying[e] = g;
-          } else {
-            h = -1;
-            live = true;
-          }
-        }
-        A.hdec[k] = h;
-      }
-      int p = block_reserve(rcnt, live ? 1 : 0);
-      if (live) rout[p] = g;
+    for (long long base = 0; base < (long long)nr0 + nr1; base += nth) {
+      const long long k = base + tid;
+      bool l0, l1;
+      int g0, g1;
+      pair_phase_b1(P.s[0], r, k, nr0, l0, g0);
+      pair_phase_b1(P.s[1], r, k - nr0, k >= nr0 ? nr1 : 0, l1, g1);
+      const int p0 = block_reserve(P.s[0].cnt + 3 + (r + 1) % 3, l0 ? 1 : 0);
+      const int p1 = block_reserve(P.s[1].cnt + 3 + (r + 1) % 3, l1 ? 1 : 0);
+      if (l0) ((r & 1) ? P.s[0].roots0 : P.s[0].roots1)[p0] = g0;
+      if (l1) ((r & 1) ? P.s[1].roots0 : P.s[1].roots1)[p1] = g1;
     }
     grid.sync();
     // phase B2: apply the links
-    for (long long k = tid; k < nr; k += nth) {
-      int h = A.hdec[k];
-      if (h >= 0) A.link[rin[k]] = h;
+    for (long long k = tid; k < (long long)nr0 + nr1; k += nth) {
+      const int sd = k < nr0 ? 0 : 1;
+      const PairArgs& A = P.s[sd];
+      const long long kk = sd ? k - nr0 : k;
+      const int h = A.hdec[kk];
+      if (h >= 0) A.link[((r & 1) ? A.roots1 : A.roots0)[kk]] = h;
     }
     grid.sync();
   }
@@ -218,75 +255,97 @@ struct ReplayArgs {
   int* rounds;
 };
 
-// Rounds of cancellation resolution (replay.cuh). The cancellations are in
-// collection order; their keys order the replay.
-__global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs A) {
+// Rounds of cancellation resolution (replay.cuh) for both sides in one
+// cooperative launch (a side with n_cancel == nullptr takes no part). The
+// cancellations are in collection order; their keys order the replay.
+struct ReplayArgs2 {
+  ReplayArgs s[2];
+};
+
+__device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r) {
+  const unsigned long long t = A.key[r];
+  int j = A.cj[r];
+  int d = A.dying[j], s = A.sweep[j];
+  int T0 = A.c1[j], T1 = A.c2[j];
+  int R0 = -1, R1 = -1;
+  long long a0 = 0, a1 = 0;
+  bool ok = walk_root(A.S, T0, t, &R0, &a0, A.max_steps, A.status) &&
+            walk_root(A.S, T1, t, &R1, &a1, A.max_steps, A.status);
+  if (!ok) return true;  // still waiting on an earlier cancellation
+  int k = -1;
+  if (R0 == d && R0 != R1)
+    k = 0;
+  else if (R1 == d && R0 != R1)
+    k = 1;
+  if (k >= 0) {
+    A.S.parent[d] = k == 0 ? R1 : R0;
+    A.S.side[d] = k;
+    A.S.csad[d] = s;
+    A.S.cl_dy[d] = k == 0 ? a0 : a1;
+    A.S.cl_ot[d] = k == 0 ? a1 : a0;
+    A.S.wlen[d] = A.blen[2 * s] + A.blen[2 * s + 1] + a0 + a1;
+    st_release(A.S.status + d, kLinked);
+  } else {
+    st_release(A.S.status + d, kRootForever);
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs2 P) {
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
-  const int C = *A.n_cancel;
-  for (long long r = tid; r < C; r += nth) {
-    A.act0[r] = (int)r;
-    int d = A.dying[A.cj[r]];
-    A.S.ctime[d] = A.key[r];
-    A.S.status[d] = kPending;
-  }
-  if (tid == 0) {
-    A.cnt[0] = C;
-    A.cnt[1] = 0;
-    A.cnt[2] = 0;
+  for (int sd = 0; sd < 2; ++sd) {
+    const ReplayArgs& A = P.s[sd];
+    if (!A.n_cancel) continue;
+    const int C = *A.n_cancel;
+    for (long long r = tid; r < C; r += nth) {
+      A.act0[r] = (int)r;
+      int d = A.dying[A.cj[r]];
+      A.S.ctime[d] = A.key[r];
+      A.S.status[d] = kPending;
+    }
+    if (tid == 0) {
+      A.cnt[0] = C;
+      A.cnt[1] = 0;
+      A.cnt[2] = 0;
+    }
   }
   grid.sync();
+  bool done[2] = {false, false};
   for (int rd = 0;; ++rd) {
-    const int n = *(volatile int*)(A.cnt + rd % 3);
-    if (n == 0) {
-      if (tid == 0 && A.rounds) *A.rounds = rd;
+    int n[2];
+    for (int sd = 0; sd < 2; ++sd) {
+      const ReplayArgs& A = P.s[sd];
+      n[sd] = A.n_cancel ? *(volatile int*)(A.cnt + rd % 3) : 0;
+      if (tid == 0 && A.n_cancel && !done[sd] && n[sd] == 0 && A.rounds) *A.rounds = rd;
+      done[sd] = done[sd] || n[sd] == 0;
+    }
+    if (n[0] == 0 && n[1] == 0) break;
+    if (rd >= max(P.s[0].max_rounds, P.s[1].max_rounds)) {
+      if (tid == 0) set_status(P.s[0].n_cancel ? P.s[0].status : P.s[1].status, kStatusRoundCap);
       break;
     }
-    if (rd >= A.max_rounds) {
-      if (tid == 0) set_status(A.status, kStatusRoundCap);
-      break;
-    }
-    const int* in = (rd & 1) ? A.act1 : A.act0;
-    int* out = (rd & 1) ? A.act0 : A.act1;
-    int* ocnt = A.cnt + (rd + 1) % 3;
-    if (tid == 0) A.cnt[(rd + 2) % 3] = 0;
-    for (long long base = 0; base < n; base += nth) {
-      long long i = base + tid;
-      bool keep = false;
-      int r = -1;
-      if (i < n) {
-        r = in[i];
-        const unsigned long long t = A.key[r];
-        int j = A.cj[r];
-        int d = A.dying[j], s = A.sweep[j];
-        int T0 = A.c1[j], T1 = A.c2[j];
-        int R0 = -1, R1 = -1;
-        long long a0 = 0, a1 = 0;
-        bool ok = walk_root(A.S, T0, t, &R0, &a0, A.max_steps, A.status) &&
-                  walk_root(A.S, T1, t, &R1, &a1, A.max_steps, A.status);
-        if (!ok) {
-          keep = true;
-        } else {
-          int k = -1;
-          if (R0 == d && R0 != R1)
-            k = 0;
-          else if (R1 == d && R0 != R1)
-            k = 1;
-          if (k >= 0) {
-            A.S.parent[d] = k == 0 ? R1 : R0;
-            A.S.side[d] = k;
-            A.S.csad[d] = s;
-            A.S.cl_dy[d] = k == 0 ? a0 : a1;
-            A.S.cl_ot[d] = k == 0 ? a1 : a0;
-            A.S.wlen[d] = A.blen[2 * s] + A.blen[2 * s + 1] + a0 + a1;
-            st_release(A.S.status + d, kLinked);
-          } else {
-            st_release(A.S.status + d, kRootForever);
-          }
-        }
+    if (tid == 0)
+      for (int sd = 0; sd < 2; ++sd)
+        if (P.s[sd].n_cancel) P.s[sd].cnt[(rd + 2) % 3] = 0;
+    for (long long base = 0; base < (long long)n[0] + n[1]; base += nth) {
+      const long long i = base + tid;
+      bool keep[2] = {false, false};
+      int r[2] = {-1, -1};
+      if (i < n[0]) {
+        r[0] = ((rd & 1) ? P.s[0].act1 : P.s[0].act0)[i];
+        keep[0] = replay_step(P.s[0], r[0]);
+      } else if (i < (long long)n[0] + n[1]) {
+        r[1] = ((rd & 1) ? P.s[1].act1 : P.s[1].act0)[i - n[0]];
+        keep[1] = replay_step(P.s[1], r[1]);
       }
-      int p = block_reserve(ocnt, keep ? 1 : 0);
-      if (keep) out[p] = r;
+#pragma unroll
+      for (int sd = 0; sd < 2; ++sd) {
+        int* cnt = P.s[sd].n_cancel ? P.s[sd].cnt + (rd + 1) % 3 : nullptr;
+        // every thread of the block takes part in the reservation
+        const int p = cnt ? block_reserve(cnt, keep[sd] ? 1 : 0) : 0;
+        if (keep[sd]) ((rd & 1) ? P.s[sd].act0 : P.s[sd].act1)[p] = r[sd];
+      }
     }
     grid.sync();
   }

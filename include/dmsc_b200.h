@@ -169,9 +169,9 @@ const char* dmsc_b200_last_error(const dmsc_b200_context* ctx);
    at every stage boundary. dmsc_b200_stage_times() writes up to `n` stage
    durations in milliseconds of the last extract()+fetch() pair (host pointer)
    and returns the number of stages: 0 gradient, 1 compaction, 2 saddle sort,
-   3 saddle walks, 4 pairing (faces), 5 pairing (vertices), 6 survivors,
-   7 replay (faces), 8 replay (vertices), 9 labels, 10 sizes,
-   11 fetch lists, 12 fetch geometry. */
+   3 saddle walks, 4 pairing (both sides), 5 persistence, cancellation and
+   output ranks, 6 survivors, 7 replay (both sides), 8 final arcs, 9 labels,
+   10 sizes, 11 fetch lists, 12 fetch geometry. */
 int dmsc_b200_set_profiling(dmsc_b200_context* ctx, int enable);
 int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n);
 
