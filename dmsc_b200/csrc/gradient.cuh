@@ -125,12 +125,13 @@ __device__ __forceinline__ bool gt_before(float a, float b) {
 // way. Edge slots: e0 = H(y,x), e1 = H(y,x+1), e2 = V(y,x), e3 = V(y+1,x);
 // face slots: f0 = F(y,x), f1 = F(y,x+1), f2 = F(y+1,x), f3 = F(y+1,x+1).
 // Returns the pixel's pairing word (face_fifo_table).
-template <bool DUAL>
+template <bool DUAL, bool INTERIOR = false>
 __device__ __forceinline__ uint32_t lower_star(const float (*sv)[kValX], int y, int x, int H, int W, int ty0, int tx0,
                                                const uint32_t* __restrict__ fifo_lut) {
   // 3x3 neighbourhood; r, c index the value tile (origin y0-2, x0-2)
   const int r = y - (ty0 - 2), c = x - (tx0 - 2);
-  const bool lv = x >= 1, rv = x + 1 < W, uv = y >= 1, dv = y + 1 < H;
+  // INTERIOR: every neighbour of the pixel is in the image
+  const bool lv = INTERIOR || x >= 1, rv = INTERIOR || x + 1 < W, uv = INTERIOR || y >= 1, dv = INTERIOR || y + 1 < H;
   // row-major linear order of the 3x3 neighbourhood: UL < U < UR < L < P < R < DL < D < DR
   const float P = sv[r][c];
   const float L = sv[r][c - 1], R = sv[r][c + 1];
@@ -221,7 +222,8 @@ __device__ __forceinline__ uint32_t lower_star(const float (*sv)[kValX], int y, 
 
 // Pairing words of the (kTileY + 1) x (kTileX + 1) pixels whose lower stars
 // hold the cells of one 32 x kTileY index tile (origin pixel (y0 - 1, x0 - 1)).
-template <bool DUAL>
+// INTERIOR: the tile's value window lies inside the image, so no bound is tested.
+template <bool DUAL, bool INTERIOR>
 __device__ __forceinline__ void gradient_tile(const float* __restrict__ img, int H, int W, int y0, int x0, int tid,
                                               float (*sv)[kValX], uint32_t (*word)[kTileX + 1],
                                               const uint32_t* __restrict__ fifo_lut) {
@@ -233,7 +235,8 @@ __device__ __forceinline__ void gradient_tile(const float* __restrict__ img, int
     const int i = tid + k * kGradThreads;
     const int r = i / kValX, c = i - r * kValX;
     const int gy = y0 - 2 + r, gx = x0 - 2 + c;
-    v[k] = (i < kValN && gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(img + (size_t)gy * W + gx) : 0.0f;
+    v[k] = (i < kValN && (INTERIOR || (gy >= 0 && gy < H && gx >= 0 && gx < W))) ? __ldg(img + (size_t)gy * W + gx)
+                                                                                  : 0.0f;
   }
 #pragma unroll
   for (int k = 0; k < kLoads; ++k) {
@@ -246,7 +249,7 @@ __device__ __forceinline__ void gradient_tile(const float* __restrict__ img, int
     const int r = p / (kTileX + 1), c = p - r * (kTileX + 1);
     const int y = y0 - 1 + r, x = x0 - 1 + c;
     uint32_t w = kNoPixel;
-    if (y >= 0 && y < H && x >= 0 && x < W) w = lower_star<DUAL>(sv, y, x, H, W, y0, x0, fifo_lut);
+    if (INTERIOR || (y >= 0 && y < H && x >= 0 && x < W)) w = lower_star<DUAL, INTERIOR>(sv, y, x, H, W, y0, x0, fifo_lut);
     word[r][c] = w;
   }
   __syncthreads();
@@ -265,13 +268,14 @@ __device__ __forceinline__ int slot_face_cell(int f, int b, int Nx) { return 3 +
 // (iy, ix-1), (iy-1, ix) or (iy-1, ix-1). Coalesced int4 gradient stores at
 // global index base `gbase`, criticality mask, flow codes and the row
 // segment's counts (segment id `seg`).
+template <bool INTERIOR>
 __device__ __forceinline__ void gradient_store_row(const uint32_t (*word)[kTileX + 1], int warp, int lane, int H,
                                                    int W, int iy, int ix, long long gbase, int seg,
                                                    int4* __restrict__ grad, uint8_t* __restrict__ crit_mask,
                                                    uint8_t* __restrict__ flow, int* __restrict__ seg_min,
                                                    int* __restrict__ seg_sad, int* __restrict__ seg_max) {
   const int Nx = W + 1;
-  const bool in = ix <= W;
+  const bool in = INTERIOR || ix <= W;
   unsigned m = 0;
   if (in) {
     const uint32_t wP = word[warp + 1][lane + 1], wL = word[warp + 1][lane];
@@ -301,7 +305,7 @@ __device__ __forceinline__ void gradient_store_row(const uint32_t (*word)[kTileX
     const int s3 = fn < 4u ? slot_edge_cell((int)fn, fb, Nx) : -1;
     const size_t gidx = (size_t)(gbase + b);
     grad[gidx] = make_int4(s0, s1, s2, s3);
-    if (vk < 0 && iy < H && ix < W) m |= 1u;
+    if (vk < 0 && (INTERIOR || (iy < H && ix < W))) m |= 1u;
     if (hn == 15u) m |= 2u;
     if (vn == 15u) m |= 4u;
     if (fn == 15u) m |= 8u;
@@ -332,13 +336,13 @@ __global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __r
   __shared__ uint32_t word[kTileY + 1][kTileX + 1];
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY;
-  gradient_tile<DUAL>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
+  gradient_tile<DUAL, false>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
   const int warp = tid >> 5, lane = tid & 31;
   for (int rr = warp; rr < kTileY; rr += kGradWarps) {
     const int iy = y0 + rr, ix = x0 + lane;
     if (iy > H) break;  // uniform per warp
-    gradient_store_row(word, rr, lane, H, W, iy, ix, 0, iy * gridDim.x + blockIdx.x, grad, crit_mask, flow, seg_min,
-                       seg_sad, seg_max);
+    gradient_store_row<false>(word, rr, lane, H, W, iy, ix, 0, iy * gridDim.x + blockIdx.x, grad, crit_mask, flow,
+                              seg_min, seg_sad, seg_max);
   }
 }
 
@@ -362,18 +366,32 @@ static __global__ void __launch_bounds__(kGradThreads) gradient_batch_kernel(Img
   const int ty = t / ntx, tx = t - ty * ntx;
   const int x0 = tx * kTileX, y0 = ty * kTileY;
   const float* img = img_all + I.px_base[b];
-  if (I.dual[b])
-    gradient_tile<true>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
-  else
-    gradient_tile<false>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
+  // tiles whose value window [y0-2, y0+kTileY] x [x0-2, x0+kTileX] lies inside
+  // the image (almost all of them) run without bound tests
+  const bool interior = y0 >= 2 && x0 >= 2 && y0 + kTileY <= H - 1 && x0 + kTileX <= W - 1;
+  if (I.dual[b]) {
+    if (interior)
+      gradient_tile<true, true>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
+    else
+      gradient_tile<true, false>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
+  } else {
+    if (interior)
+      gradient_tile<false, true>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
+    else
+      gradient_tile<false, false>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
+  }
   const int warp = tid >> 5, lane = tid & 31;
   const long long gbase = I.idx_base[b];
   const int sbase = I.seg_base[b];
   for (int rr = warp; rr < kTileY; rr += kGradWarps) {
     const int iy = y0 + rr, ix = x0 + lane;
     if (iy > H) break;  // uniform per warp
-    gradient_store_row(word, rr, lane, H, W, iy, ix, gbase, sbase + iy * ntx + tx, grad, crit_mask, flow, seg_min,
-                       seg_sad, seg_max);
+    if (interior)
+      gradient_store_row<true>(word, rr, lane, H, W, iy, ix, gbase, sbase + iy * ntx + tx, grad, crit_mask, flow,
+                               seg_min, seg_sad, seg_max);
+    else
+      gradient_store_row<false>(word, rr, lane, H, W, iy, ix, gbase, sbase + iy * ntx + tx, grad, crit_mask, flow,
+                                seg_min, seg_sad, seg_max);
   }
 }
 
