@@ -152,11 +152,12 @@ class Context:
 
     def timelines(self) -> dict:
         """Per-round / per-level durations (us) of the device loops of the last call."""
-        buf = (ctypes.c_longlong * 256)()
-        if self.lib.dmsc_b200_pairing_timeline(self.h, buf, 256) < 0:
+        buf = (ctypes.c_longlong * 384)()
+        if self.lib.dmsc_b200_pairing_timeline(self.h, buf, 384) < 0:
             return {}
         out = {}
-        for blk, name in enumerate(("pairing_faces", "pairing_vertices", "emit_faces", "emit_vertices")):
+        for blk, name in enumerate(("pairing_faces", "pairing_vertices", "emit_faces", "emit_vertices",
+                                    "replay_faces", "replay_vertices")):
             t = [x for x in (buf[blk * 64 + k] for k in range(64)) if x > 0]
             out[name] = tuple((b - a) / 1000.0 for a, b in zip(t, t[1:]))
         return out

@@ -46,7 +46,7 @@ enum SideSlot {
   X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
   X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_CTIME, X_STAT, X_PAR, X_WLEN, X_SIDE,
   X_CSAD, X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G1,
-  X_G2, X_GBASE, X_LAB, kSideSlots
+  X_G2, X_GBASE, X_LAB, X_WX, X_WA, kSideSlots
 };
 
 struct Buf {
@@ -381,7 +381,7 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
   A.status = ctx->status;
   A.max_rounds = M + 2;
   A.rounds = get<int>(ctx, S_STATS, 8) + 0 + si;
-  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline) + si * kTimeline;
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline) + si * kTimeline;
   return A;
 }
 
@@ -474,9 +474,12 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   A.act0 = sget<int>(ctx, si, X_ACT0, nsad);
   A.act1 = sget<int>(ctx, si, X_ACT1, nsad);
   A.cnt = cnt;
+  A.wx = sget<int>(ctx, si, X_WX, 2 * (size_t)nsad);
+  A.wa = sget<long long>(ctx, si, X_WA, 2 * (size_t)nsad);
   A.status = ctx->status;
   A.max_rounds = nsad + 2;
   A.rounds = get<int>(ctx, S_STATS, 8) + 2 + si;
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline) + (4 + si) * kTimeline;
   return A;
 }
 
@@ -590,8 +593,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   mark(ctx, 0, st);
   CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
   CK(cudaMemsetAsync(get<int>(ctx, S_STATS, 8), 0, 8 * sizeof(int), st));
-  CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline), 0,
-                     4 * kTimeline * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline), 0,
+                     6 * kTimeline * sizeof(unsigned long long), st));
   {  // upload the tables: 9 int arrays, then thr (float) and dual (u8)
     size_t ib = tab.size() * sizeof(int), fb = (size_t)B * sizeof(float);
     size_t total = ib + fb + B + 16;
@@ -972,7 +975,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   E.n_base = nullptr;
   A.max_levels = ctx->nsad + 4;
   A.levels = get<int>(ctx, S_STATS, 8) + 4 + si;
-  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 4 * kTimeline) + (2 + si) * kTimeline;
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline) + (2 + si) * kTimeline;
   coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel");
   {
     int per = 0;
@@ -1292,7 +1295,7 @@ long long dmsc_b200_launch_count(const dmsc_b200_context* ctx) { return ctx ? ct
 
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n) {
   if (!ctx || !out || ctx->bufs.size() <= (size_t)S_TIMELINE || !ctx->bufs[S_TIMELINE].p) return -1;
-  int k = n < 4 * kTimeline ? n : 4 * kTimeline;
+  int k = n < 6 * kTimeline ? n : 6 * kTimeline;
   if (cudaSetDevice(ctx->device) != cudaSuccess ||
       cudaMemcpy(out, ctx->bufs[S_TIMELINE].p, k * sizeof(long long), cudaMemcpyDeviceToHost) != cudaSuccess)
     return -1;

@@ -46,6 +46,45 @@ __device__ __forceinline__ int warp_append(int* counter, bool take) {
   return take ? base + __popc(b & ((1u << lane) - 1u)) : -1;
 }
 
+
+// Chunked processing with two output lists: each block takes contiguous
+// chunks of items (up to kChunkPer per thread, fewer when there are few
+// items, so small rounds still spread over the whole grid; no barrier between
+// a thread's items); kept items are gathered in shared memory with shared
+// atomics and written out once per chunk with one global reservation per
+// list, so a block meets at a barrier a few times per chunk instead of after
+// every item.
+constexpr int kChunkPer = 8;
+constexpr int kChunk = 256 * kChunkPer;  // blocks of 256 threads
+
+struct ChunkLists {
+  int n[2];
+  int base[2];
+  int buf[2][kChunk];
+};
+
+__device__ __forceinline__ long long chunk_size(long long n) {
+  const long long lanes = (long long)gridDim.x * 256;
+  return 256LL * max(1LL, min((long long)kChunkPer, (n + lanes - 1) / lanes));
+}
+
+__device__ __forceinline__ void chunk_start(ChunkLists& L) {
+  if (threadIdx.x < 2) L.n[threadIdx.x] = 0;
+  __syncthreads();
+}
+
+__device__ __forceinline__ void chunk_keep(ChunkLists& L, int side, int v) { L.buf[side][atomicAdd(&L.n[side], 1)] = v; }
+
+__device__ __forceinline__ void chunk_flush(ChunkLists& L, int* cnt0, int* out0, int* cnt1, int* out1) {
+  const int t = threadIdx.x;
+  __syncthreads();
+  if (t < 2 && L.n[t] > 0) L.base[t] = atomicAdd(t == 0 ? cnt0 : cnt1, L.n[t]);
+  __syncthreads();
+  for (int k = t; k < L.n[0]; k += 256) out0[L.base[0] + k] = L.buf[0][k];
+  for (int k = t; k < L.n[1]; k += 256) out1[L.base[1] + k] = L.buf[1][k];
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // pairing rounds (see pairing.cuh for the algorithm)
 // ---------------------------------------------------------------------------
@@ -145,6 +184,7 @@ __device__ __forceinline__ void pair_phase_b1(const PairArgs& A, int r, long lon
 }
 
 __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs2 P) {
+  __shared__ ChunkLists L;
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
   for (int sd = 0; sd < 2; ++sd) {
@@ -195,30 +235,46 @@ __global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs2 P) {
         P.s[sd].cnt[3 + (r + 2) % 3] = 0;
       }
     }
-    // phase A over both sides' active saddles (block-uniform trip count)
-    for (long long base = 0; base < (long long)n0 + n1; base += nth) {
-      const long long i = base + tid;
-      bool k0, k1;
-      int e0, e1;
-      pair_phase_a(P.s[0], r, i, n0, k0, e0);
-      pair_phase_a(P.s[1], r, i - n0, i >= n0 ? n1 : 0, k1, e1);
-      const int p0 = block_reserve(P.s[0].cnt + (r + 1) % 3, k0 ? 1 : 0);
-      const int p1 = block_reserve(P.s[1].cnt + (r + 1) % 3, k1 ? 1 : 0);
-      if (k0) ((r & 1) ? P.s[0].act0 : P.s[0].act1)[p0] = e0;
-      if (k1) ((r & 1) ? P.s[1].act0 : P.s[1].act1)[p1] = e1;
+    // phase A over both sides' active saddles
+    {
+      const long long n = (long long)n0 + n1, chunk = chunk_size(n);
+      for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
+        chunk_start(L);
+        for (long long i = c0 + threadIdx.x; i < min(n, c0 + chunk); i += 256) {
+          bool keep;
+          int v;
+          if (i < n0) {
+            pair_phase_a(P.s[0], r, i, n0, keep, v);
+            if (keep) chunk_keep(L, 0, v);
+          } else {
+            pair_phase_a(P.s[1], r, i - n0, n1, keep, v);
+            if (keep) chunk_keep(L, 1, v);
+          }
+        }
+        chunk_flush(L, P.s[0].cnt + (r + 1) % 3, (r & 1) ? P.s[0].act0 : P.s[0].act1, P.s[1].cnt + (r + 1) % 3,
+                    (r & 1) ? P.s[1].act0 : P.s[1].act1);
+      }
     }
     grid.sync();
     // phase B1: live roots decide on their first outgoing saddle
-    for (long long base = 0; base < (long long)nr0 + nr1; base += nth) {
-      const long long k = base + tid;
-      bool l0, l1;
-      int g0, g1;
-      pair_phase_b1(P.s[0], r, k, nr0, l0, g0);
-      pair_phase_b1(P.s[1], r, k - nr0, k >= nr0 ? nr1 : 0, l1, g1);
-      const int p0 = block_reserve(P.s[0].cnt + 3 + (r + 1) % 3, l0 ? 1 : 0);
-      const int p1 = block_reserve(P.s[1].cnt + 3 + (r + 1) % 3, l1 ? 1 : 0);
-      if (l0) ((r & 1) ? P.s[0].roots0 : P.s[0].roots1)[p0] = g0;
-      if (l1) ((r & 1) ? P.s[1].roots0 : P.s[1].roots1)[p1] = g1;
+    {
+      const long long n = (long long)nr0 + nr1, chunk = chunk_size(n);
+      for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
+        chunk_start(L);
+        for (long long k = c0 + threadIdx.x; k < min(n, c0 + chunk); k += 256) {
+          bool live;
+          int g;
+          if (k < nr0) {
+            pair_phase_b1(P.s[0], r, k, nr0, live, g);
+            if (live) chunk_keep(L, 0, g);
+          } else {
+            pair_phase_b1(P.s[1], r, k - nr0, nr1, live, g);
+            if (live) chunk_keep(L, 1, g);
+          }
+        }
+        chunk_flush(L, P.s[0].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[0].roots0 : P.s[0].roots1,
+                    P.s[1].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[1].roots0 : P.s[1].roots1);
+      }
     }
     grid.sync();
     // phase B2: apply the links
@@ -250,9 +306,12 @@ struct ReplayArgs {
   int* act0;
   int* act1;
   int* cnt;  // [0..2]
+  int* wx;         // [2C] position of each cancellation's two walks
+  long long* wa;   // [2C] path length summed so far by each walk
   unsigned* status;
   int max_rounds;
   int* rounds;
+  unsigned long long* timeline;  // [kTimeline] round start times (ns), optional
 };
 
 // Rounds of cancellation resolution (replay.cuh) for both sides in one
@@ -266,12 +325,18 @@ __device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r) {
   const unsigned long long t = A.key[r];
   int j = A.cj[r];
   int d = A.dying[j], s = A.sweep[j];
-  int T0 = A.c1[j], T1 = A.c2[j];
-  int R0 = -1, R1 = -1;
-  long long a0 = 0, a1 = 0;
-  bool ok = walk_root(A.S, T0, t, &R0, &a0, A.max_steps, A.status) &&
-            walk_root(A.S, T1, t, &R1, &a1, A.max_steps, A.status);
-  if (!ok) return true;  // still waiting on an earlier cancellation
+  // both walks resume where the previous round left them
+  int R0 = A.wx[2 * r], R1 = A.wx[2 * r + 1];
+  long long a0 = A.wa[2 * r], a1 = A.wa[2 * r + 1];
+  const bool ok0 = walk_resume(A.S, &R0, t, &a0, A.max_steps, A.status);
+  const bool ok1 = walk_resume(A.S, &R1, t, &a1, A.max_steps, A.status);
+  if (!(ok0 && ok1)) {  // still waiting on an earlier cancellation
+    A.wx[2 * r] = R0;
+    A.wx[2 * r + 1] = R1;
+    A.wa[2 * r] = a0;
+    A.wa[2 * r + 1] = a1;
+    return true;
+  }
   int k = -1;
   if (R0 == d && R0 != R1)
     k = 0;
@@ -291,7 +356,7 @@ __device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r) {
   return false;
 }
 
-__global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs2 P) {
+__global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P) {
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
   for (int sd = 0; sd < 2; ++sd) {
@@ -300,9 +365,14 @@ __global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs2 P) {
     const int C = *A.n_cancel;
     for (long long r = tid; r < C; r += nth) {
       A.act0[r] = (int)r;
-      int d = A.dying[A.cj[r]];
+      const int j = A.cj[r];
+      int d = A.dying[j];
       A.S.ctime[d] = A.key[r];
       A.S.status[d] = kPending;
+      A.wx[2 * r] = A.c1[j];
+      A.wx[2 * r + 1] = A.c2[j];
+      A.wa[2 * r] = 0;
+      A.wa[2 * r + 1] = 0;
     }
     if (tid == 0) {
       A.cnt[0] = C;
@@ -311,16 +381,23 @@ __global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs2 P) {
     }
   }
   grid.sync();
-  bool done[2] = {false, false};
+  bool done0 = false, done1 = false;
   for (int rd = 0;; ++rd) {
-    int n[2];
-    for (int sd = 0; sd < 2; ++sd) {
-      const ReplayArgs& A = P.s[sd];
-      n[sd] = A.n_cancel ? *(volatile int*)(A.cnt + rd % 3) : 0;
-      if (tid == 0 && A.n_cancel && !done[sd] && n[sd] == 0 && A.rounds) *A.rounds = rd;
-      done[sd] = done[sd] || n[sd] == 0;
+    const int na = P.s[0].n_cancel ? *(volatile int*)(P.s[0].cnt + rd % 3) : 0;
+    const int nb = P.s[1].n_cancel ? *(volatile int*)(P.s[1].cnt + rd % 3) : 0;
+    if (tid == 0) {
+      if (P.s[0].n_cancel && !done0) {
+        if (P.s[0].timeline && rd < kTimeline) P.s[0].timeline[rd] = global_ns();
+        if (na == 0 && P.s[0].rounds) *P.s[0].rounds = rd;
+      }
+      if (P.s[1].n_cancel && !done1) {
+        if (P.s[1].timeline && rd < kTimeline) P.s[1].timeline[rd] = global_ns();
+        if (nb == 0 && P.s[1].rounds) *P.s[1].rounds = rd;
+      }
     }
-    if (n[0] == 0 && n[1] == 0) break;
+    done0 = done0 || na == 0;
+    done1 = done1 || nb == 0;
+    if (na == 0 && nb == 0) break;
     if (rd >= max(P.s[0].max_rounds, P.s[1].max_rounds)) {
       if (tid == 0) set_status(P.s[0].n_cancel ? P.s[0].status : P.s[1].status, kStatusRoundCap);
       break;
@@ -328,24 +405,24 @@ __global__ void __launch_bounds__(256) replay_persistent_kernel(ReplayArgs2 P) {
     if (tid == 0)
       for (int sd = 0; sd < 2; ++sd)
         if (P.s[sd].n_cancel) P.s[sd].cnt[(rd + 2) % 3] = 0;
-    for (long long base = 0; base < (long long)n[0] + n[1]; base += nth) {
+    // grid-stride over both sides' pending cancellations (a cancellation
+    // decided earlier in the same round is visible to later walks)
+    for (long long base = 0; base < (long long)na + nb; base += nth) {
       const long long i = base + tid;
-      bool keep[2] = {false, false};
-      int r[2] = {-1, -1};
-      if (i < n[0]) {
-        r[0] = ((rd & 1) ? P.s[0].act1 : P.s[0].act0)[i];
-        keep[0] = replay_step(P.s[0], r[0]);
-      } else if (i < (long long)n[0] + n[1]) {
-        r[1] = ((rd & 1) ? P.s[1].act1 : P.s[1].act0)[i - n[0]];
-        keep[1] = replay_step(P.s[1], r[1]);
+      bool k0 = false, k1 = false;
+      int r0 = -1, r1 = -1;
+      if (i < na) {
+        r0 = ((rd & 1) ? P.s[0].act1 : P.s[0].act0)[i];
+        k0 = replay_step(P.s[0], r0);
+      } else if (i < (long long)na + nb) {
+        r1 = ((rd & 1) ? P.s[1].act1 : P.s[1].act0)[i - na];
+        k1 = replay_step(P.s[1], r1);
       }
-#pragma unroll
-      for (int sd = 0; sd < 2; ++sd) {
-        int* cnt = P.s[sd].n_cancel ? P.s[sd].cnt + (rd + 1) % 3 : nullptr;
-        // every thread of the block takes part in the reservation
-        const int p = cnt ? block_reserve(cnt, keep[sd] ? 1 : 0) : 0;
-        if (keep[sd]) ((rd & 1) ? P.s[sd].act0 : P.s[sd].act1)[p] = r[sd];
-      }
+      // every thread of the block takes part in the reservations
+      const int p0 = P.s[0].n_cancel ? block_reserve(P.s[0].cnt + (rd + 1) % 3, k0 ? 1 : 0) : 0;
+      const int p1 = P.s[1].n_cancel ? block_reserve(P.s[1].cnt + (rd + 1) % 3, k1 ? 1 : 0) : 0;
+      if (k0) ((rd & 1) ? P.s[0].act0 : P.s[0].act1)[p0] = r0;
+      if (k1) ((rd & 1) ? P.s[1].act0 : P.s[1].act1)[p1] = r1;
     }
     grid.sync();
   }

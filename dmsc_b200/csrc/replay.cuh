@@ -79,6 +79,37 @@ __device__ __forceinline__ bool walk_root(const ReplayState& S, int x, unsigned 
   return true;
 }
 
+// The same walk resumed from (*x, *acc) and left there: returns false, with
+// *x the first undecided node and *acc the length summed before it, when the
+// walk has to wait; the prefix already walked is final (decisions never
+// change), so a later round continues from that node.
+__device__ __forceinline__ bool walk_resume(const ReplayState& S, int* x_io, unsigned long long t, long long* acc_io,
+                                            int max_steps, unsigned* status) {
+  int x = *x_io;
+  long long a = *acc_io;
+  int steps = 0;
+  bool done = true;
+  while (true) {
+    if (x < 0) break;
+    if (S.ctime[x] >= t) break;
+    int st = ld_acquire(S.status + x);
+    if (st == kPending) {
+      done = false;
+      break;
+    }
+    if (st == kRootForever) break;
+    a += S.wlen[x];
+    x = S.parent[x];
+    if (++steps > max_steps) {
+      set_status(status, kStatusChainCap);
+      break;
+    }
+  }
+  *x_io = x;
+  *acc_io = a;
+  return done;
+}
+
 // Cancellations of one side, compacted in any order with their sort keys
 // (CancelEvent::operator<, cpu/persistence_struct.hxx:16-21): (persistence,
 // saddle cell); a saddle is cancelled at most once per side, so the pair is

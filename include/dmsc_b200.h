@@ -184,9 +184,10 @@ long long dmsc_b200_launch_count(const dmsc_b200_context* ctx);
    expansion levels (faces, vertices). Returns the number written or -1. */
 int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n);
 
-/* Device loop timelines of the last call (ns, device global timer), four
-   blocks of 64 slots: pairing round starts (faces, vertices), then geometry
-   expansion level starts (faces, vertices). Unused slots are 0. Writes up to `n` values to `out` (host
+/* Device loop timelines of the last call (ns, device global timer), six
+   blocks of 64 slots: pairing round starts (faces, vertices), geometry
+   expansion level starts (faces, vertices), then replay round starts (faces,
+   vertices). Unused slots are 0. Writes up to `n` values to `out` (host
    pointer), returns the number written. */
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n);
 
