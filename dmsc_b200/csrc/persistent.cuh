@@ -518,16 +518,11 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
       int4 t = make_int4(-1, 0, 0, 0);
       int kind = -1, rev = 0, need = 0, nb = 0;
       long long total = 0;
-      if (i < n) {
+      if (i < n) {  // every queued task is a chain task
         t = in[i];
         kind = t.x & 3;
         rev = (t.x >> 2) & 1;
-        if (kind == kTaskW) {
-          need = w_task_count(E, t.y);
-          nb = w_base_count(E, t.y);
-        } else if (kind == kTaskChain) {
-          need = chain_task_count(E, t.y, t.z, &total);
-        }
+        if (kind == kTaskChain && !chain_expand_counts(E, t.y, t.z, &need, &nb, &total)) kind = -1;
       }
       int p = block_reserve(E.n_out, need);
       int pb = block_reserve(E.n_base, nb);
@@ -535,10 +530,7 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
         set_status(E.status, kStatusQueueOverflow);
         kind = -1;
       }
-      if (kind == kTaskW)
-        emit_w(E, t.y, rev, t.w, p, pb);
-      else if (kind == kTaskChain)
-        emit_chain(E, t.y, t.z, rev, t.w, need, total, p);
+      if (kind == kTaskChain) chain_expand(E, t.y, t.z, rev, t.w, total, p, pb);
     }
     grid.sync();
   }

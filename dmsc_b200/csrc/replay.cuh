@@ -21,8 +21,10 @@
 //   reverse(chain(T_dying -> d)) + reverse(arc_dying) + arc_other + chain(T_other -> R)
 // where chain(x -> R) concatenates W along x's parent chain up to R, and every
 // surviving saddle's final arc is arc + chain(T -> root). These are expanded
-// breadth-first as tasks that each cover a known output range; raw arcs are
-// re-walked from their start cells when written.
+// breadth-first as chain tasks that each cover a known output range (a chain
+// task writes every W along its chain at once: their raw-arc segments and
+// their own chains as the next level's tasks); raw arcs are re-walked from
+// their start cells when written.
 #pragma once
 
 #include <cuda/atomic>
@@ -179,8 +181,8 @@ __global__ void final_arcs_kernel(int nsurv, const int* __restrict__ surv_sad, c
 // ---------------------------------------------------------------------------
 // geometry emission
 // ---------------------------------------------------------------------------
-enum : int { kTaskBase = 0, kTaskW = 1, kTaskChain = 2 };
-// task = {kind | dir << 2, a, b, pos}; base: a = saddle, b = arc; W: a = node;
+enum : int { kTaskBase = 0, kTaskChain = 2 };
+// task = {kind | dir << 2, a, b, pos}; base: a = saddle, b = arc;
 // chain: a = start node, b = stop node (-1 = void).
 __device__ __forceinline__ int4 make_task(int kind, int rev, int a, int b, long long pos) {
   return make_int4(kind | (rev << 2), a, b, (int)pos);
@@ -232,45 +234,14 @@ __device__ __forceinline__ int w_base_count(const EmitCtx& E, int d) {
   return (E.blen[2 * s + k] > 0) + (E.blen[2 * s + 1 - k] > 0);
 }
 
-// Number of W tasks of chain(x -> stop) and its total length; the chain is
-// walked once here and once when written.
-__device__ __forceinline__ int chain_task_count(const EmitCtx& E, int x, int stop, long long* total) {
-  long long tot = 0;
-  int k = 0, z = x;
-  while (z != stop && z >= 0) {
-    tot += E.S.wlen[z];
-    z = E.S.parent[z];
-    if (++k > E.max_steps) {
-      set_status(E.status, kStatusChainCap);
-      *total = 0;
-      return 0;
-    }
-  }
-  *total = tot;
-  return k;
-}
-
-// Writes the k W tasks of chain(x -> stop) into queue slots p .. p+k-1.
-__device__ void emit_chain(const EmitCtx& E, int x, int stop, int rev, long long pos, int k, long long total,
-                           int p) {
-  long long off = 0;
-  int z = x;
-  for (int i = 0; i < k; ++i) {
-    long long w = E.S.wlen[z];
-    E.q_out[p + i] = make_task(kTaskW, rev, z, 0, rev ? pos + total - off - w : pos + off);
-    off += w;
-    z = E.S.parent[z];
-  }
-}
-
 // Number of chain tasks W(d) produces (its two chains, when non-empty).
 __device__ __forceinline__ int w_task_count(const EmitCtx& E, int d) {
   return (E.S.cl_dy[d] > 0) + (E.S.cl_ot[d] > 0);
 }
 
 // Expands W(d): queues its two chains at slot p and its two raw-arc segments
-// at base slot pb.
-__device__ void emit_w(const EmitCtx& E, int d, int rev, long long pos, int p, int pb) {
+// at base slot pb, advancing both.
+__device__ __forceinline__ void emit_w(const EmitCtx& E, int d, int rev, long long pos, int& p, int& pb) {
   int k = E.S.side[d], o = 1 - k, s = E.S.csad[d];
   int Tk = E.t[2 * s + k], To = E.t[2 * s + o];
   long long la = E.S.cl_dy[d], lb = E.blen[2 * s + k], lc = E.blen[2 * s + o], ld = E.S.cl_ot[d];
@@ -286,6 +257,50 @@ __device__ void emit_w(const EmitCtx& E, int d, int rev, long long pos, int p, i
     if (lc > 0) E.base_q[pb++] = make_task(kTaskBase, 1, s, o, pos + ld);
     if (lb > 0) E.base_q[pb++] = make_task(kTaskBase, 0, s, k, pos + ld + lc);
     if (la > 0) E.q_out[p++] = make_task(kTaskChain, 0, Tk, d, pos + ld + lc + lb);
+  }
+}
+
+// A chain task expanded in one step: chain(x -> stop) is the concatenation
+// of W(z) for the nodes z on x's parent chain up to stop; every W(z) is
+// expanded in place (its raw-arc segments and its own two chains), so the
+// breadth-first expansion needs one level per chain depth instead of two.
+// Counts of the chain tasks and raw-arc segments the expansion writes, and
+// the chain's total length.
+// Returns false (with zero counts) when the chain exceeds its step cap; the
+// task is then dropped and the status reports the cap.
+__device__ __forceinline__ bool chain_expand_counts(const EmitCtx& E, int x, int stop, int* n_chain, int* n_base,
+                                                    long long* total) {
+  long long tot = 0;
+  int nc = 0, nb = 0, k = 0, z = x;
+  *n_chain = 0;
+  *n_base = 0;
+  *total = 0;
+  while (z != stop && z >= 0) {
+    tot += E.S.wlen[z];
+    nc += w_task_count(E, z);
+    nb += w_base_count(E, z);
+    z = E.S.parent[z];
+    if (++k > E.max_steps) {
+      set_status(E.status, kStatusChainCap);
+      return false;
+    }
+  }
+  *n_chain = nc;
+  *n_base = nb;
+  *total = tot;
+  return true;
+}
+
+// Writes the expansion counted by chain_expand_counts at slots p and pb.
+__device__ void chain_expand(const EmitCtx& E, int x, int stop, int rev, long long pos, long long total, int p,
+                             int pb) {
+  long long off = 0;
+  int k = 0;
+  for (int z = x; z != stop && z >= 0; z = E.S.parent[z]) {
+    if (++k > E.max_steps) break;
+    const long long w = E.S.wlen[z];
+    emit_w(E, z, rev, rev ? pos + total - off - w : pos + off, p, pb);
+    off += w;
   }
 }
 
