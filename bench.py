@@ -363,13 +363,14 @@ def b200_arm(args):
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h // args.steps,
                 "timing": "host wall clock around K public-API calls from pinned host memory, max over ranks"},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "gradient_kernel", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "gradient_batch_kernel", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "algorithmic_bytes": grad_bytes, "avg_ms": grad_ms,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6.65 TB/s"},
         "roofline_segmentation": {"bound": "hbm", "kernel": "label stage (label_tile_kernel + label_exit_kernel x2)", "achieved": seg, "peak": peak,
                                   "unit": "GB/s", "frac": (seg / peak) if seg else None,
+                                  "traffic_label_tile_kernel": ncu_traffic("label_tile_kernel", size),
                                   "algorithmic_bytes": seg_bytes, "avg_ms": lab_ms},
         "stage_ms_per_step": {k: v / args.steps for k, v in stage_sum.items()},
         "device_loops_per_variant": {f"dual={d},thr={t}": loops[k] for k, (d, t) in enumerate(VARIANTS) if k < len(loops)},
