@@ -321,15 +321,15 @@ struct ReplayArgs2 {
   ReplayArgs s[2];
 };
 
-__device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r) {
+__device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r, int round) {
   const unsigned long long t = A.key[r];
   int j = A.cj[r];
   int d = A.dying[j], s = A.sweep[j];
   // both walks resume where the previous round left them
   int R0 = A.wx[2 * r], R1 = A.wx[2 * r + 1];
   long long a0 = A.wa[2 * r], a1 = A.wa[2 * r + 1];
-  const bool ok0 = walk_resume(A.S, &R0, t, &a0, A.max_steps, A.status);
-  const bool ok1 = walk_resume(A.S, &R1, t, &a1, A.max_steps, A.status);
+  const bool ok0 = walk_resume(A.S, &R0, t, &a0, A.max_steps, A.status, round);
+  const bool ok1 = walk_resume(A.S, &R1, t, &a1, A.max_steps, A.status, round);
   if (!(ok0 && ok1)) {  // still waiting on an earlier cancellation
     A.wx[2 * r] = R0;
     A.wx[2 * r + 1] = R1;
@@ -349,9 +349,9 @@ __device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r) {
     A.S.cl_dy[d] = k == 0 ? a0 : a1;
     A.S.cl_ot[d] = k == 0 ? a1 : a0;
     A.S.wlen[d] = A.blen[2 * s] + A.blen[2 * s + 1] + a0 + a1;
-    st_release(A.S.status + d, kLinked);
+    A.S.status[d] = status_word(kLinked, round);
   } else {
-    st_release(A.S.status + d, kRootForever);
+    A.S.status[d] = status_word(kRootForever, round);
   }
   return false;
 }
@@ -413,10 +413,10 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
       int r0 = -1, r1 = -1;
       if (i < na) {
         r0 = ((rd & 1) ? P.s[0].act1 : P.s[0].act0)[i];
-        k0 = replay_step(P.s[0], r0);
+        k0 = replay_step(P.s[0], r0, rd);
       } else if (i < (long long)na + nb) {
         r1 = ((rd & 1) ? P.s[1].act1 : P.s[1].act0)[i - na];
-        k1 = replay_step(P.s[1], r1);
+        k1 = replay_step(P.s[1], r1, rd);
       }
       // every thread of the block takes part in the reservations
       const int p0 = P.s[0].n_cancel ? block_reserve(P.s[0].cnt + (rd + 1) % 3, k0 ? 1 : 0) : 0;

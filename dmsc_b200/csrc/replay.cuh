@@ -27,8 +27,6 @@
 // their start cells when written.
 #pragma once
 
-#include <cuda/atomic>
-
 #include "common.cuh"
 #include "walks.cuh"
 
@@ -36,10 +34,17 @@ namespace dmsc {
 
 constexpr unsigned long long kNever = ~0ull;  // replay key of a node that is never cancelled
 enum : int { kPending = 0, kLinked = 1, kRootForever = 2 };
+// A replay status word is kind | tag << 2; a decision made in replay round r
+// carries tag r + 1 (the initial kRootForever of never-cancelled nodes has
+// tag 0). Walks in round r use only decisions with tag <= r: those were
+// written before the grid barrier that opened round r, which orders them, so
+// plain (L2) loads see them complete and no acquire/release is needed.
+__device__ __forceinline__ int status_kind(int st) { return st & 3; }
+__device__ __forceinline__ int status_word(int kind, int round) { return kind | ((round + 1) << 2); }
 
 struct ReplayState {
   unsigned long long* ctime;  // [M] replay key of the cancellation killing the node, kNever if none
-  int* status;      // [M] kPending / kLinked / kRootForever
+  int* status;      // [M] kPending / kLinked / kRootForever, with the deciding round's tag
   int* parent;      // [M] link target (-1 = void) when kLinked
   long long* wlen;  // [M] length of W(node)
   int* side;        // [M] dying side (0/1) of the node's cancellation
@@ -47,13 +52,6 @@ struct ReplayState {
   long long* cl_dy; // [M] chain length T_dying -> node at link time
   long long* cl_ot; // [M] chain length T_other -> parent at link time
 };
-
-__device__ __forceinline__ int ld_acquire(const int* p) {
-  return cuda::atomic_ref<const int, cuda::thread_scope_device>(*p).load(cuda::memory_order_acquire);
-}
-__device__ __forceinline__ void st_release(int* p, int v) {
-  cuda::atomic_ref<int, cuda::thread_scope_device>(*p).store(v, cuda::memory_order_release);
-}
 
 // Root of x just before the replay step with key t, with the summed path
 // length; returns false when a node on the way is still undecided. Replay
@@ -66,7 +64,7 @@ __device__ __forceinline__ bool walk_root(const ReplayState& S, int x, unsigned 
   while (true) {
     if (x < 0) break;
     if (S.ctime[x] >= t) break;
-    int st = ld_acquire(S.status + x);
+    int st = status_kind(S.status[x]);
     if (st == kPending) return false;
     if (st == kRootForever) break;
     a += S.wlen[x];
@@ -86,22 +84,22 @@ __device__ __forceinline__ bool walk_root(const ReplayState& S, int x, unsigned 
 // walk has to wait; the prefix already walked is final (decisions never
 // change), so a later round continues from that node.
 __device__ __forceinline__ bool walk_resume(const ReplayState& S, int* x_io, unsigned long long t, long long* acc_io,
-                                            int max_steps, unsigned* status) {
+                                            int max_steps, unsigned* status, int round) {
   int x = *x_io;
   long long a = *acc_io;
   int steps = 0;
   bool done = true;
   while (true) {
     if (x < 0) break;
-    if (S.ctime[x] >= t) break;
-    int st = ld_acquire(S.status + x);
-    if (st == kPending) {
+    if (__ldcg(S.ctime + x) >= t) break;
+    const int st = __ldcg(S.status + x);
+    if (status_kind(st) == kPending || (st >> 2) > round) {  // undecided, or decided in this round
       done = false;
       break;
     }
-    if (st == kRootForever) break;
-    a += S.wlen[x];
-    x = S.parent[x];
+    if (status_kind(st) == kRootForever) break;
+    a += __ldcg(S.wlen + x);
+    x = __ldcg(S.parent + x);
     if (++steps > max_steps) {
       set_status(status, kStatusChainCap);
       break;
