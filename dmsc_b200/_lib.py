@@ -21,6 +21,7 @@ EXPORTS = (
     "dmsc_b200_destroy",
     "dmsc_b200_extract",
     "dmsc_b200_fetch",
+    "dmsc_b200_set_host_outputs",
     "dmsc_b200_extract_batch",
     "dmsc_b200_fetch_pair_pixels",
     "dmsc_b200_scatter_pair_grads",
@@ -79,6 +80,8 @@ def load():
         lib.dmsc_b200_extract.restype = ctypes.c_int
         lib.dmsc_b200_fetch.argtypes = [ctypes.c_void_p, ctypes.POINTER(Outputs), ctypes.c_void_p]
         lib.dmsc_b200_fetch.restype = ctypes.c_int
+        lib.dmsc_b200_set_host_outputs.argtypes = [ctypes.c_void_p] * 4
+        lib.dmsc_b200_set_host_outputs.restype = ctypes.c_int
         lib.dmsc_b200_extract_batch.argtypes = [
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
             ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_ubyte), ctypes.c_uint, ctypes.c_void_p,

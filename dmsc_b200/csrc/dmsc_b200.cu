@@ -140,7 +140,20 @@ struct dmsc_b200_context {
   int num_sms = 0;
   cudaEvent_t ev[kStageMarks] = {};
   cudaEvent_t sync_ev = nullptr;   // polled by wait_stream
-  unsigned* pstatus = nullptr;     // pinned copy of the device status word
+  // host destinations of the fixed-size outputs for the next extract (copied
+  // on copy_st as soon as each is produced; see dmsc_b200_set_host_outputs)
+  int32_t* host_grad = nullptr;
+  int32_t* host_peaks = nullptr;
+  int32_t* host_basins = nullptr;
+  bool copies_pending = false;
+  cudaStream_t copy_st = nullptr;
+  cudaEvent_t copy_ev = nullptr;
+  // readback area: pinned host memory mapped into the device address space;
+  // a small kernel writes the values, so readbacks never queue behind bulk
+  // device-to-host copies on the copy engines
+  char* rb_h = nullptr;
+  char* rb_d = nullptr;
+  size_t rb_cap = 0;
 };
 
 
@@ -171,6 +184,11 @@ __global__ void last_kernel(const T* a, int n, long long* out) {
 
 __global__ void u8_last_plus_kernel(const int* excl, const uint8_t* v, int n, long long* out) {
   *out = n > 0 ? (long long)excl[n - 1] + v[n - 1] : 0;
+}
+
+// 32-bit words from device memory into the mapped readback area.
+__global__ void copy_words_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
 }
 
 }  // namespace dmsc
@@ -301,11 +319,61 @@ void wait_stream(dmsc_b200_context* ctx, cudaStream_t st) {
   }
 }
 
-// Host read of `k` pinned scalars after the stream drains.
+// Device -> host copy of a finished output on the context's copy stream,
+// ordered after the work enqueued on `st` so far.
+void copy_out_async(dmsc_b200_context* ctx, void* host, const void* dev, size_t bytes, cudaStream_t st) {
+  if (!host || !dev || !bytes) return;
+  CK(cudaEventRecord(ctx->copy_ev, st));
+  CK(cudaStreamWaitEvent(ctx->copy_st, ctx->copy_ev, 0));
+  CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ctx->copy_st));
+  ctx->copies_pending = true;
+}
+
+// Makes `st` wait for every copy issued on the copy stream.
+void join_copies(dmsc_b200_context* ctx, cudaStream_t st) {
+  if (!ctx->copies_pending) return;
+  CK(cudaEventRecord(ctx->copy_ev, ctx->copy_st));
+  CK(cudaStreamWaitEvent(st, ctx->copy_ev, 0));
+  ctx->copies_pending = false;
+}
+
+// After a failure: wait for the copies already issued, so no host buffer is
+// written after the call returns, and forget the registered destinations.
+void abandon_copies(dmsc_b200_context* ctx) {
+  if (ctx->copy_st) cudaStreamSynchronize(ctx->copy_st);
+  ctx->copies_pending = false;
+  ctx->host_grad = ctx->host_peaks = ctx->host_basins = nullptr;
+}
+
+// Mapped readback area of at least `bytes` (grown only between readbacks).
+void rb_reserve(dmsc_b200_context* ctx, size_t bytes) {
+  if (ctx->rb_cap >= bytes) return;
+  if (ctx->rb_h) CK(cudaFreeHost(ctx->rb_h));
+  ctx->rb_h = ctx->rb_d = nullptr;
+  ctx->rb_cap = 0;
+  const size_t nb = ((bytes + bytes / 2 + 4096) + 255) & ~(size_t)255;
+  CK(cudaHostAlloc((void**)&ctx->rb_h, nb, cudaHostAllocMapped));
+  CK(cudaHostGetDevicePointer((void**)&ctx->rb_d, ctx->rb_h, 0));
+  ctx->rb_cap = nb;
+}
+
+// Enqueues the copy of `bytes` (a multiple of 4) from device `src` to offset
+// `off` of the readback area.
+void rb_copy(dmsc_b200_context* ctx, cudaStream_t st, size_t off, const void* src, size_t bytes) {
+  const int n = (int)(bytes / 4);
+  if (n <= 0) return;
+  LK(copy_words_kernel<<<grid_for(n, 256) < 64 ? grid_for(n, 256) : 64, 256, 0, st>>>(
+      (const uint32_t*)src, (uint32_t*)(ctx->rb_d + off), n));
+  LAUNCH_CHECK("copy_words_kernel");
+}
+
+// Host read of `k` device scalars (into rb, as long long) after the stream drains.
 void readback(dmsc_b200_context* ctx, cudaStream_t st, const long long* dev, int k) {
-  CK(cudaMemcpyAsync(ctx->pinned, dev, k * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  rb_reserve(ctx, k * sizeof(long long));
+  rb_copy(ctx, st, 0, dev, k * sizeof(long long));
   wait_stream(ctx, st);
 }
+const long long* rb_ll(dmsc_b200_context* ctx) { return (const long long*)ctx->rb_h; }
 
 // Error of a device status word (0: none).
 void raise_status(dmsc_b200_context* ctx, unsigned h) {
@@ -324,9 +392,10 @@ void raise_status(dmsc_b200_context* ctx, unsigned h) {
 }
 
 void check_status(dmsc_b200_context* ctx, cudaStream_t st) {
-  CK(cudaMemcpyAsync(ctx->pstatus, ctx->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  rb_reserve(ctx, 64);
+  rb_copy(ctx, st, 0, ctx->status, sizeof(unsigned));
   wait_stream(ctx, st);
-  raise_status(ctx, *ctx->pstatus);
+  raise_status(ctx, *(const unsigned*)ctx->rb_h);
 }
 
 
@@ -590,6 +659,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   ctx->hdual.assign(hdual, hdual + B);
   ctx->status = get<unsigned>(ctx, S_STATUS, 4);
   ctx->launches = 0;
+  join_copies(ctx, st);  // host copies of an earlier call still reading its outputs
   mark(ctx, 0, st);
   CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
   CK(cudaMemsetAsync(get<int>(ctx, S_STATS, 8), 0, 8 * sizeof(int), st));
@@ -634,12 +704,13 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
                                                                      ctx->fifo_lut, flow));
   LAUNCH_CHECK("gradient_batch_kernel");
   mark(ctx, 1, st);
+  if (ret_grad) copy_out_async(ctx, ctx->host_grad, grad, 16 * (size_t)nidx, st);
   for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);
   long long* tot = get<long long>(ctx, S_TOT, 8);
   LK(totals3_kernel<<<1, 1, 0, st>>>(off[0], seg[0], off[1], seg[1], off[2], seg[2], nseg, tot));
   LAUNCH_CHECK("totals3_kernel");
   readback(ctx, st, tot, 3);
-  const int nmin = (int)ctx->pinned[0], nsad = (int)ctx->pinned[1], nmax = (int)ctx->pinned[2];
+  const int nmin = (int)rb_ll(ctx)[0], nsad = (int)rb_ll(ctx)[1], nmax = (int)rb_ll(ctx)[2];
   ctx->nmin = nmin;
   ctx->nsad = nsad;
   ctx->nmax = nmax;
@@ -757,9 +828,9 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     LK(copy2_kernel<<<1, 1, 0, st>>>(get<int>(ctx, S_NCANC, 4), tot + 1));
     LAUNCH_CHECK("survivors");
     readback(ctx, st, tot, 3);
-    ctx->nsurv = (int)ctx->pinned[0];
-    F.C = (int)ctx->pinned[1];
-    V.C = (int)ctx->pinned[2];
+    ctx->nsurv = (int)rb_ll(ctx)[0];
+    F.C = (int)rb_ll(ctx)[1];
+    V.C = (int)rb_ll(ctx)[2];
   }
   const int nsurv = ctx->nsurv;
   LK(image_base_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, BS.sad, nsad, fpos, nsurv, BS.surv));
@@ -851,6 +922,9 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     LAUNCH_CHECK("label_exit_kernel");
   }
   mark(ctx, 10, st);
+  if (f_peaks) copy_out_async(ctx, ctx->host_peaks, peaks_out, 4 * (size_t)npk, st);
+  if (f_basins) copy_out_async(ctx, ctx->host_basins, basins_out, 4 * (size_t)nbs, st);
+  ctx->host_grad = ctx->host_peaks = ctx->host_basins = nullptr;  // one extract only
 
   // ---- e rows ----
   for (int si = 0; si < 2; ++si) {
@@ -872,16 +946,17 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
 
   // ---- per-image sizes: one read of the bases ----
   {
-    size_t ib = 9 * (size_t)(B + 1) * sizeof(int), lb = 2 * (size_t)(B + 1) * sizeof(long long);
-    char* h = (char*)staging(ctx, ib + lb + 64);
-    CK(cudaMemcpyAsync(h, bases, ib, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(h + ib, F.gbase, (B + 1) * sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(h + ib + (B + 1) * sizeof(long long), V.gbase, (B + 1) * sizeof(long long),
-                       cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(ctx->pstatus, ctx->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    // int bases, then (8-byte aligned) the two geometry bases, then the status word
+    size_t ib = (9 * (size_t)(B + 1) * sizeof(int) + 7) & ~(size_t)7, lb = 2 * (size_t)(B + 1) * sizeof(long long);
+    rb_reserve(ctx, ib + lb + 64);
+    rb_copy(ctx, st, 0, bases, 9 * (size_t)(B + 1) * sizeof(int));
+    rb_copy(ctx, st, ib, F.gbase, (B + 1) * sizeof(long long));
+    rb_copy(ctx, st, ib + (B + 1) * sizeof(long long), V.gbase, (B + 1) * sizeof(long long));
+    rb_copy(ctx, st, ib + lb, ctx->status, sizeof(unsigned));
     wait_stream(ctx, st);
     mark(ctx, 11, st);
-    raise_status(ctx, *ctx->pstatus);
+    const char* h = ctx->rb_h;
+    raise_status(ctx, *(const unsigned*)(h + ib + lb));
     const int* hb = (const int*)h;
     const int* hsurv = hb + 3 * (B + 1);
     const int* hal[2] = {hb + 4 * (B + 1), hb + 5 * (B + 1)};
@@ -1084,6 +1159,7 @@ int fetch_batch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStr
   }
   mark(ctx, 14, st);
   check_status(ctx, st);
+  join_copies(ctx, st);  // the caller's stream passes here only once the host copies are done
   return kOk;
 }
 
@@ -1154,8 +1230,14 @@ int dmsc_b200_create(dmsc_b200_context** out, int device) {
   }
   c->pinned_cap = 64 * sizeof(long long);
   if (cudaEventCreateWithFlags(&c->sync_ev, cudaEventDisableTiming) != cudaSuccess ||
-      cudaMallocHost(&c->pstatus, sizeof(unsigned)) != cudaSuccess) {
+      cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking) != cudaSuccess) {
     if (c->sync_ev) cudaEventDestroy(c->sync_ev);
+  if (c->copy_st) {
+    cudaStreamSynchronize(c->copy_st);
+    cudaStreamDestroy(c->copy_st);
+  }
+  if (c->copy_ev) cudaEventDestroy(c->copy_ev);
     cudaFreeHost(c->pinned);
     delete c;
     return kErrCuda;
@@ -1183,7 +1265,7 @@ void dmsc_b200_destroy(dmsc_b200_context* c) {
   if (c->cub_tmp.p) cudaFree(c->cub_tmp.p);
   if (c->fifo_lut) cudaFree(c->fifo_lut);
   if (c->pinned) cudaFreeHost(c->pinned);
-  if (c->pstatus) cudaFreeHost(c->pstatus);
+  if (c->rb_h) cudaFreeHost(c->rb_h);
   if (c->sync_ev) cudaEventDestroy(c->sync_ev);
   for (int k = 0; k < kStageMarks; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
@@ -1201,6 +1283,7 @@ int dmsc_b200_extract(dmsc_b200_context* ctx, const float* image, int H, int W, 
                               (cudaStream_t)stream);
   } catch (const Fail& f) {
     ctx->valid = false;
+    abandon_copies(ctx);
     return f.code;
   }
 }
@@ -1211,8 +1294,18 @@ int dmsc_b200_fetch(dmsc_b200_context* ctx, const dmsc_b200_outputs* out, void* 
   try {
     return fetch_batch_impl(ctx, out, (cudaStream_t)stream);
   } catch (const Fail& f) {
+    abandon_copies(ctx);
     return f.code;
   }
+}
+
+int dmsc_b200_set_host_outputs(dmsc_b200_context* ctx, int32_t* grad_host, int32_t* peaks_host,
+                               int32_t* basins_host) {
+  if (!ctx) return kErrInvalidArgument;
+  ctx->host_grad = grad_host;
+  ctx->host_peaks = peaks_host;
+  ctx->host_basins = basins_host;
+  return kOk;
 }
 
 int dmsc_b200_extract_batch(dmsc_b200_context* ctx, const float* images, int B, const int* H, const int* W,
@@ -1225,6 +1318,7 @@ int dmsc_b200_extract_batch(dmsc_b200_context* ctx, const float* images, int B, 
                               sizes, (cudaStream_t)stream);
   } catch (const Fail& f) {
     ctx->valid = false;
+    abandon_copies(ctx);
     return f.code;
   }
 }

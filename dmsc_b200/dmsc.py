@@ -159,9 +159,27 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
 
 
-def extract_single(img: torch.Tensor, persistence_threshold: float, flags: int, stream=None) -> tuple:
+def _keep_alive(stream, tensors):
+    """Marks device tensors as used by ``stream`` (the caching allocator does
+    not hand their memory out again before the stream passes this point)."""
+    for t in tensors:
+        if t is not None:
+            t.record_stream(stream)
+
+
+def _host_like(t):
+    """Pinned host tensor shaped like ``t`` (None stays None)."""
+    return None if t is None else torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+
+
+def extract_single(img: torch.Tensor, persistence_threshold: float, flags: int, stream=None,
+                   host_fixed: bool = False) -> tuple:
     """One contiguous float32 [H, W] CUDA image through both C-ABI phases;
-    returns the 19 output tensors on the image's device (shape on the CPU)."""
+    returns the 19 output tensors on the image's device (shape on the CPU).
+    With ``host_fixed`` the gradient and label maps are returned in pinned
+    host tensors that the library fills while the rest of the call runs
+    (``dmsc_b200_set_host_outputs``); they are complete once the stream has
+    passed the call."""
     H, W = int(img.shape[0]), int(img.shape[1])
     dev = img.device
     ctx = _lib.context(dev.index if dev.index is not None else torch.cuda.current_device())
@@ -172,6 +190,10 @@ def extract_single(img: torch.Tensor, persistence_threshold: float, flags: int, 
     grad = torch.empty(4 * nidx, **i32) if flags & _lib.RETURN_GRADIENT else None
     peaks = torch.empty((H, W) if dual else (H + 1, W + 1), **i32) if flags & _lib.TRACE_PEAKS else None
     basins = torch.empty((H + 1, W + 1) if dual else (H, W), **i32) if flags & _lib.TRACE_BASINS else None
+    if host_fixed:
+        hg, hp, hb = _host_like(grad), _host_like(peaks), _host_like(basins)
+        ctx.check(ctx.lib.dmsc_b200_set_host_outputs(ctx.h, _ptr(hg), _ptr(hp), _ptr(hb)),
+                  "dmsc_b200_set_host_outputs")
     sz = _lib.Sizes()
     rc = ctx.lib.dmsc_b200_extract(ctx.h, ctypes.c_void_p(img.data_ptr()), H, W, ctypes.c_float(persistence_threshold),
                                    flags, _ptr(grad), _ptr(peaks), _ptr(basins), ctypes.byref(sz),
@@ -193,6 +215,9 @@ def extract_single(img: torch.Tensor, persistence_threshold: float, flags: int, 
     empty = torch.empty(0, **i32)
     empty2 = torch.empty((0, 0), **i32)
     shape = torch.tensor([H, W], dtype=torch.int32)
+    if host_fixed:  # the device copies are the sources of the library's transfers; keep them alive until then
+        _keep_alive(s, (grad, peaks, basins))
+        grad, peaks, basins = hg, hp, hb
     return (shape, out["max_pts"], out["min_pts"], out["sad_pts"], out["e_max"], out["e_min"], out["p_max"],
             out["p_min"], out["ppairs_max"], out["ppairs_min"], grad if grad is not None else empty,
             peaks if peaks is not None else empty2, out["ridges"], out["ridge_offsets"], out["ridge_arc_offsets"],
@@ -213,7 +238,7 @@ _SIZE_OF = dict(max_pts="max_pts", min_pts="min_pts", sad_pts="sad_pts", e_max="
                 valley_offsets="valley_offsets", valley_arc_offsets="valley_arc_offsets")
 
 
-def _batch_raw(images, thresholds, is_dual, flags: int, stream=None, flat=None, pair_pixels=False):
+def _batch_raw(images, thresholds, is_dual, flags: int, stream=None, flat=None, pair_pixels=False, host_fixed=False):
     """Both C-ABI phases of one device batch. Returns the batch-wide output
     tensors (``out``, field -> tensor, images back to back), the per-image
     lengths of each (``lens``), the image shapes and orientations and the
@@ -237,6 +262,10 @@ def _batch_raw(images, thresholds, is_dual, flags: int, stream=None, flat=None, 
     grad = torch.empty(4 * sum(nidx), **i32) if flags & _lib.RETURN_GRADIENT else None
     peaks = torch.empty(sum(pk_n), **i32) if flags & _lib.TRACE_PEAKS else None
     basins = torch.empty(sum(bs_n), **i32) if flags & _lib.TRACE_BASINS else None
+    if host_fixed:  # gradient and labels copied to pinned host memory while the call runs
+        hg, hp, hb = _host_like(grad), _host_like(peaks), _host_like(basins)
+        ctx.check(ctx.lib.dmsc_b200_set_host_outputs(ctx.h, _ptr(hg), _ptr(hp), _ptr(hb)),
+                  "dmsc_b200_set_host_outputs")
     sz = (_lib.Sizes * B)()
     rc = ctx.lib.dmsc_b200_extract_batch(
         ctx.h, ctypes.c_void_p(flat.data_ptr()), B, (ctypes.c_int * B)(*Hs), (ctypes.c_int * B)(*Ws),
@@ -261,6 +290,8 @@ def _batch_raw(images, thresholds, is_dual, flags: int, stream=None, flat=None, 
         ctx.check(ctx.lib.dmsc_b200_fetch_pair_pixels(
             ctx.h, _ptr(out["plus_max"]), _ptr(out["minus_max"]), _ptr(out["plus_min"]), _ptr(out["minus_min"]),
             ctypes.c_void_p(s.cuda_stream)), "dmsc_b200_fetch_pair_pixels")
+    if host_fixed:
+        grad, peaks, basins = hg, hp, hb
     if grad is not None:
         out["grad_indices"] = grad
         lens["grad_indices"] = [4 * n for n in nidx]
@@ -281,7 +312,7 @@ def extract_batch(images, thresholds, is_dual, flags: int, to_host: bool = False
     ``to_host``). ``flags``' DUAL bit is ignored in favour of ``is_dual``."""
     B = len(images)
     dev = images[0].device
-    out, lens, Hs, Ws, duals, s = _batch_raw(images, thresholds, is_dual, flags, stream)
+    out, lens, Hs, Ws, duals, s = _batch_raw(images, thresholds, is_dual, flags, stream, host_fixed=to_host)
     grad, peaks, basins = out.get("grad_indices"), out.get("peaks"), out.get("basins")
     if to_host:
         with torch.cuda.stream(s):
@@ -345,7 +376,7 @@ def extract_dmsc(scalar_field, persistence_threshold, return_gradient=False, is_
         x = scalar_field.contiguous()
     with torch.cuda.device(x.device):
         if x.dim() == 2:
-            res = extract_single(x, persistence_threshold, flags)
+            res = extract_single(x, persistence_threshold, flags, host_fixed=on_cpu)
             return _to_host(res) if on_cpu else res
         n = x.shape[0]
         return _extract_many(list(x.unbind(0)), [persistence_threshold] * n, [is_dual] * n, flags, on_cpu)

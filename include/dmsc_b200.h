@@ -112,6 +112,19 @@ int dmsc_b200_extract(dmsc_b200_context* ctx, const float* image, int H, int W, 
    of image b, and so on); all values are image-local. */
 int dmsc_b200_fetch(dmsc_b200_context* ctx, const dmsc_b200_outputs* out, void* stream);
 
+/* Optional host destinations for the fixed-size outputs of the next
+   extract() / extract_batch() on this context (no counterpart in the
+   reference, whose CPU callers get host tensors only after the whole call).
+   Pinned host buffers laid out like grad_out / peaks_out / basins_out (any
+   may be NULL). Each output is copied on an internal stream as soon as it
+   is produced (the gradient right after the first kernel, the labels after
+   the label stage), overlapping the transfer with the rest of the pipeline.
+   The caller's stream waits for these copies at the end of the following
+   dmsc_b200_fetch(): read the host buffers only after that fetch's work on
+   the stream has completed. The registration covers one extract call. */
+int dmsc_b200_set_host_outputs(dmsc_b200_context* ctx, int32_t* grad_host, int32_t* peaks_host,
+                               int32_t* basins_host);
+
 /* Phase 1 for a batch of B images of independent sizes, thresholds and
    orientations, computed together (one pass of every stage over the union
    of the images). Replaces the reference's per-image loop over a 3-D batch
