@@ -22,6 +22,7 @@ EXPORTS = (
     "dmsc_b200_extract",
     "dmsc_b200_fetch",
     "dmsc_b200_set_host_outputs",
+    "dmsc_b200_set_host_fetch_outputs",
     "dmsc_b200_extract_batch",
     "dmsc_b200_fetch_pair_pixels",
     "dmsc_b200_scatter_pair_grads",
@@ -82,6 +83,8 @@ def load():
         lib.dmsc_b200_fetch.restype = ctypes.c_int
         lib.dmsc_b200_set_host_outputs.argtypes = [ctypes.c_void_p] * 4
         lib.dmsc_b200_set_host_outputs.restype = ctypes.c_int
+        lib.dmsc_b200_set_host_fetch_outputs.argtypes = [ctypes.c_void_p, ctypes.POINTER(Outputs)]
+        lib.dmsc_b200_set_host_fetch_outputs.restype = ctypes.c_int
         lib.dmsc_b200_extract_batch.argtypes = [
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
             ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_ubyte), ctypes.c_uint, ctypes.c_void_p,

@@ -46,7 +46,7 @@ enum SideSlot {
   X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
   X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_CTIME, X_STAT, X_PAR, X_WLEN, X_SIDE,
   X_CSAD, X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G1,
-  X_G2, X_GBASE, X_LAB, X_WX, X_WA, kSideSlots
+  X_G2, X_GBASE, X_LAB, X_WX, X_WA, X_CENDS, kSideSlots
 };
 
 struct Buf {
@@ -145,6 +145,8 @@ struct dmsc_b200_context {
   int32_t* host_grad = nullptr;
   int32_t* host_peaks = nullptr;
   int32_t* host_basins = nullptr;
+  dmsc_b200_outputs host_fetch{};  // host destinations of the next fetch's outputs
+  bool host_fetch_set = false;
   bool copies_pending = false;
   cudaStream_t copy_st = nullptr;
   cudaEvent_t copy_ev = nullptr;
@@ -343,6 +345,7 @@ void abandon_copies(dmsc_b200_context* ctx) {
   if (ctx->copy_st) cudaStreamSynchronize(ctx->copy_st);
   ctx->copies_pending = false;
   ctx->host_grad = ctx->host_peaks = ctx->host_basins = nullptr;
+  ctx->host_fetch_set = false;
 }
 
 // Mapped readback area of at least `bytes` (grown only between readbacks).
@@ -471,11 +474,12 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   CK(cudaMemsetAsync(S.alive, 1, M + 4, st));
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
   int* ncanc = get<int>(ctx, S_NCANC, 4) + si;
+  int2* cends = sget<int2>(ctx, si, X_CENDS, nsad);
   CK(cudaMemsetAsync(ncanc, 0, sizeof(int), st));
   if (nsad > 0) {
     LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(
         nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.sweep, S.dying, get<float>(ctx, S_SVAL, nsad), S.val,
-        S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc));
+        S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.c1, S.c2, cends));
     LAUNCH_CHECK("persistence_kernel");
   }
   // thresholded union-find roots
@@ -484,8 +488,7 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   S.ut = sget<int>(ctx, si, X_UT, M + 1);
   LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(uf, M + 1));
   if (nsad > 0)
-    LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.c1, S.c2, S.pers, ctx->I.thr,
-                                                          ctx->sad_img, M, uf));
+    LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(cends, ncanc, M, uf));
   LK(ut_flatten_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, uf));
   LK(ut_mark_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M, uf, S.alive, croot));
   if (M > 0) LK(ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.ut));
@@ -1134,6 +1137,24 @@ int fetch_batch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStr
     LAUNCH_CHECK("side_outputs_kernel");
   }
   mark(ctx, 13, st);
+  // per-field totals over the batch (elements)
+  long long tot_n[15] = {0};
+  for (int b = 0; b < B; ++b) {
+    const dmsc_b200_sizes& z = ctx->sizes[b];
+    const long long v[15] = {z.max_pts, z.min_pts, z.sad_pts, 2 * z.e_max_rows, 2 * z.e_min_rows, z.p_max, z.p_min,
+                             z.ppairs_max, z.ppairs_min, z.ridges, z.ridge_offsets, z.ridge_arc_offsets, z.valleys,
+                             z.valley_offsets, z.valley_arc_offsets};
+    for (int k = 0; k < 15; ++k) tot_n[k] += v[k];
+  }
+  const dmsc_b200_outputs& HO = ctx->host_fetch;
+  void* const dev_f[15] = {o->max_pts, o->min_pts, o->sad_pts, o->e_max, o->e_min, o->p_max, o->p_min,
+                           o->ppairs_max, o->ppairs_min, o->ridges, o->ridge_offsets, o->ridge_arc_offsets,
+                           o->valleys, o->valley_offsets, o->valley_arc_offsets};
+  void* const host_f[15] = {HO.max_pts, HO.min_pts, HO.sad_pts, HO.e_max, HO.e_min, HO.p_max, HO.p_min,
+                            HO.ppairs_max, HO.ppairs_min, HO.ridges, HO.ridge_offsets, HO.ridge_arc_offsets,
+                            HO.valleys, HO.valley_offsets, HO.valley_arc_offsets};
+  if (ctx->host_fetch_set)  // lists and per-saddle outputs are final: copy them while the geometry is built
+    for (int k = 0; k < 9; ++k) copy_out_async(ctx, host_f[k], dev_f[k], 4 * (size_t)tot_n[k], st);
   // arc geometry
   for (int si = 0; si < 2; ++si) {
     Side& S = ctx->side[si];
@@ -1158,6 +1179,9 @@ int fetch_batch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStr
     emit_side(ctx, si, S, gp, gd, rt_of(si == 0 ? R_G0 : R_G1), OFF, AOFF, st);
   }
   mark(ctx, 14, st);
+  if (ctx->host_fetch_set)
+    for (int k = 9; k < 15; ++k) copy_out_async(ctx, host_f[k], dev_f[k], 4 * (size_t)tot_n[k], st);
+  ctx->host_fetch_set = false;  // one fetch only
   check_status(ctx, st);
   join_copies(ctx, st);  // the caller's stream passes here only once the host copies are done
   return kOk;
@@ -1297,6 +1321,13 @@ int dmsc_b200_fetch(dmsc_b200_context* ctx, const dmsc_b200_outputs* out, void* 
     abandon_copies(ctx);
     return f.code;
   }
+}
+
+int dmsc_b200_set_host_fetch_outputs(dmsc_b200_context* ctx, const dmsc_b200_outputs* host) {
+  if (!ctx) return kErrInvalidArgument;
+  ctx->host_fetch_set = host != nullptr;
+  if (host) ctx->host_fetch = *host;
+  return kOk;
 }
 
 int dmsc_b200_set_host_outputs(dmsc_b200_context* ctx, int32_t* grad_host, int32_t* peaks_host,

@@ -90,7 +90,9 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
                                                           const float* __restrict__ ext_val,
                                                           int* __restrict__ pair_dense, float* __restrict__ pers,
                                                           uint8_t* __restrict__ cancelled, uint8_t sbit,
-                                                          uint8_t* __restrict__ alive, int* __restrict__ n_cancel) {
+                                                          uint8_t* __restrict__ alive, int* __restrict__ n_cancel,
+                                                          const int* __restrict__ c1, const int* __restrict__ c2,
+                                                          int2* __restrict__ canc_ends) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   bool canc = false;
   if (j < nsad) {
@@ -116,11 +118,14 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
       }
     }
   }
-  block_append(n_cancel, canc);
+  // cancelled edges' ends, compacted for the thresholded union-find
+  const int slot = block_append(n_cancel, canc);
+  if (canc) canc_ends[slot] = make_int2(c1[j], c2[j]);
 }
 
 // Thresholded union-find: lock-free union of the ends of every cancelled
-// saddle (link the larger root under the smaller).
+// saddle (link the larger root under the smaller), over the compact list of
+// cancelled edges written by persistence_kernel.
 __device__ __forceinline__ int uf_root(int* p, int x) {
   while (true) {
     int px = p[x];
@@ -131,29 +136,24 @@ __device__ __forceinline__ int uf_root(int* p, int x) {
   }
 }
 
-__global__ void __launch_bounds__(256) ut_union_kernel(int nsad, const int* __restrict__ sweep,
-                                                       const int* __restrict__ dying, const int* __restrict__ c1,
-                                                       const int* __restrict__ c2, const float* __restrict__ pers,
-                                                       const float* __restrict__ thr,
-                                                       const int* __restrict__ sad_img, int void_id,
-                                                       int* __restrict__ p) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nsad) return;
-  if (dying[j] < 0) return;
-  const int s = sweep[j];
-  if (!(pers[s] <= thr[sad_img[s]])) return;
-  int a = c1[j] < 0 ? void_id : c1[j];
-  int b = c2[j] < 0 ? void_id : c2[j];
-  while (true) {
-    a = uf_root(p, a);
-    b = uf_root(p, b);
-    if (a == b) return;
-    if (a > b) {
-      int t = a;
-      a = b;
-      b = t;
+__global__ void __launch_bounds__(256) ut_union_kernel(const int2* __restrict__ ends, const int* __restrict__ count,
+                                                       int void_id, int* __restrict__ p) {
+  const int n = *count;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int2 e = ends[q];
+    int a = e.x < 0 ? void_id : e.x;
+    int b = e.y < 0 ? void_id : e.y;
+    while (true) {
+      a = uf_root(p, a);
+      b = uf_root(p, b);
+      if (a == b) break;
+      if (a > b) {
+        int t = a;
+        a = b;
+        b = t;
+      }
+      if (atomicCAS(p + b, b, a) == b) break;
     }
-    if (atomicCAS(p + b, b, a) == b) return;
   }
 }
 

@@ -159,14 +159,6 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
 
 
-def _keep_alive(stream, tensors):
-    """Marks device tensors as used by ``stream`` (the caching allocator does
-    not hand their memory out again before the stream passes this point)."""
-    for t in tensors:
-        if t is not None:
-            t.record_stream(stream)
-
-
 def _host_like(t):
     """Pinned host tensor shaped like ``t`` (None stays None)."""
     return None if t is None else torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
@@ -211,13 +203,19 @@ def extract_single(img: torch.Tensor, persistence_threshold: float, flags: int, 
         valleys=torch.empty(sz.valleys, **i32), valley_offsets=torch.empty(sz.valley_offsets, **i32),
         valley_arc_offsets=torch.empty(sz.valley_arc_offsets, **i32))
     o = _lib.Outputs(**{k: _ptr(v) for k, v in out.items()})
+    if host_fixed:  # variable outputs copied to pinned host memory as the fetch writes them
+        hout = {k: _host_like(v) for k, v in out.items()}
+        ho = _lib.Outputs(**{k: _ptr(v) for k, v in hout.items()})
+        ctx.check(ctx.lib.dmsc_b200_set_host_fetch_outputs(ctx.h, ctypes.byref(ho)), "dmsc_b200_set_host_fetch_outputs")
     ctx.check(ctx.lib.dmsc_b200_fetch(ctx.h, ctypes.byref(o), ctypes.c_void_p(s.cuda_stream)), "dmsc_b200_fetch")
     empty = torch.empty(0, **i32)
     empty2 = torch.empty((0, 0), **i32)
     shape = torch.tensor([H, W], dtype=torch.int32)
-    if host_fixed:  # the device copies are the sources of the library's transfers; keep them alive until then
-        _keep_alive(s, (grad, peaks, basins))
+    if host_fixed:  # host tensors, complete once the stream has passed the fetch
         grad, peaks, basins = hg, hp, hb
+        out = hout
+        empty = torch.empty(0, dtype=torch.int32)
+        empty2 = torch.empty((0, 0), dtype=torch.int32)
     return (shape, out["max_pts"], out["min_pts"], out["sad_pts"], out["e_max"], out["e_min"], out["p_max"],
             out["p_min"], out["ppairs_max"], out["ppairs_min"], grad if grad is not None else empty,
             peaks if peaks is not None else empty2, out["ridges"], out["ridge_offsets"], out["ridge_arc_offsets"],
@@ -281,7 +279,13 @@ def _batch_raw(images, thresholds, is_dual, flags: int, stream=None, flat=None, 
         dt = torch.float32 if f in ("p_max", "p_min") else torch.int32
         out[f] = torch.empty((n, 2) if f in ("e_max", "e_min") else n, dtype=dt, device=dev)
     o = _lib.Outputs(**{k: _ptr(v) for k, v in out.items()})
+    if host_fixed:  # variable outputs copied to pinned host memory as the fetch writes them
+        hout = {k: _host_like(v) for k, v in out.items()}
+        ho = _lib.Outputs(**{k: _ptr(v) for k, v in hout.items()})
+        ctx.check(ctx.lib.dmsc_b200_set_host_fetch_outputs(ctx.h, ctypes.byref(ho)), "dmsc_b200_set_host_fetch_outputs")
     ctx.check(ctx.lib.dmsc_b200_fetch(ctx.h, ctypes.byref(o), ctypes.c_void_p(s.cuda_stream)), "dmsc_b200_fetch")
+    if host_fixed:
+        out = hout
     if pair_pixels:
         for f in ("plus_max", "minus_max", "plus_min", "minus_min"):
             side = f.split("_")[1]

@@ -125,6 +125,14 @@ int dmsc_b200_fetch(dmsc_b200_context* ctx, const dmsc_b200_outputs* out, void* 
 int dmsc_b200_set_host_outputs(dmsc_b200_context* ctx, int32_t* grad_host, int32_t* peaks_host,
                                int32_t* basins_host);
 
+/* The same for the variable-size outputs of the next dmsc_b200_fetch():
+   `host` (host pointer) holds pinned host buffers laid out like that fetch's
+   device outputs (NULL fields are skipped). The lists and per-saddle outputs
+   are copied as soon as they are written, while the arc geometry is built;
+   the geometry when it is done. They are complete once the caller's stream
+   has passed that fetch. The registration covers one fetch call. */
+int dmsc_b200_set_host_fetch_outputs(dmsc_b200_context* ctx, const dmsc_b200_outputs* host);
+
 /* Phase 1 for a batch of B images of independent sizes, thresholds and
    orientations, computed together (one pass of every stage over the union
    of the images). Replaces the reference's per-image loop over a 3-D batch
