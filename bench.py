@@ -338,6 +338,7 @@ def b200_arm(args):
     e2e = world * args.steps * size * size / 1e6 / (float(te.item()) / 1000.0)
 
     batched = None if args.batch_images <= 0 else batched_section(args, dev, ctx, dist, world, rank)
+    seg_only = segmentation_only_section(args, img, dev, ctx, dist, size)
     diff = None if args.no_diff else diff_section(args, dev, dist)
 
     if rank != 0:
@@ -378,6 +379,7 @@ def b200_arm(args):
     }
     if batched is not None:
         line["batched"] = batched
+    line["segmentation_only"] = seg_only
     if diff is not None:
         line["differentiation"] = diff
     if world == 1 and not args.no_cpu_baseline:
@@ -461,6 +463,49 @@ def batched_section(args, dev, ctx, dist, world, rank):
         "device_batch_stage_ms": stages, "device_batch_launches": launches,
         "form": "one device batch per pass (every stage once over the union of the images); "
                 "host wall clock, inputs resident in HBM",
+    }
+
+
+def segmentation_only_section(args, img, dev, ctx, dist, size):
+    """Segmentation-only preset (the reference's basins/peaks use:
+    return_gradient=False, no ridges or valleys): the same field and variant
+    cycle, K device-timed calls. Its label stage reads the 1-byte flow codes
+    and writes the two label maps; no gradient is written and no arc is
+    traced."""
+    from dmsc_b200 import compute_dmsc
+
+    def step(k):
+        d, t = VARIANTS[k % 4]
+        return compute_dmsc(img, t, return_gradient=False, is_dual=d, trace_valleys=False, trace_ridges=False)
+
+    for w in range(max(args.warmup, len(VARIANTS))):
+        step(w)
+    ctx.set_profiling(True)
+    stage_sum = {}
+    for k in range(args.steps):
+        step(k)
+        for name, v in ctx.stage_times().items():
+            stage_sum[name] = stage_sum.get(name, 0.0) + v
+    ctx.set_profiling(False)
+    st = torch.cuda.current_stream(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for k in range(args.steps):
+        step(k)
+    e1.record(st)
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item()) / args.steps
+    world = dist.get_world_size() if dist else 1
+    return {
+        "workload": "same field and variants; return_gradient=False, trace_ridges=False, trace_valleys=False",
+        "value": world * size * size / 1e6 / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms,
+        "stage_ms_per_step": {k: v / args.steps for k, v in stage_sum.items()},
     }
 
 

@@ -39,7 +39,7 @@ enum Slot {
   S_GRAD, S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
   S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
   S_ASC, S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
-  S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX,
+  S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX, S_SKEY32, S_SKEY32B,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
@@ -730,11 +730,13 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   float* vmin = get<float>(ctx, S_VMIN, nmin);
   float* vmax = get<float>(ctx, S_VMAX, nmax);
   float* sval = get<float>(ctx, S_SVAL, nsad);
-  unsigned long long* skey = get<unsigned long long>(ctx, S_SKEY, nsad);
+  // sort keys: (image id << 32) | orderable(s_val), or the 32-bit value key alone for one image
+  unsigned long long* skey = B > 1 ? get<unsigned long long>(ctx, S_SKEY, nsad) : nullptr;
+  uint32_t* skey32 = B > 1 ? nullptr : get<uint32_t>(ctx, S_SKEY32, nsad);
   ctx->crit_sad = csad;
   ctx->sad_img = isad;
   LK(compact_kernel<<<grid_for(nseg, 8), 256, 0, st>>>(I, img, nseg, mask, off[0], off[1], off[2], cmin, csad, cmax,
-                                                       imin, isad, imax, rmin, rmax, vmin, vmax, sval, skey));
+                                                       imin, isad, imax, rmin, rmax, vmin, vmax, sval, skey, skey32));
   LAUNCH_CHECK("compact_kernel");
   // per-image bases of the critical lists (B + 1 entries each)
   int* bases = get<int>(ctx, S_BASES, 9 * (size_t)(B + 1));
@@ -756,10 +758,13 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   // ---- saddle order: per image ascending (s_val, cell id) (arcs_topology.hxx:99-102) ----
   int* iota = get<int>(ctx, S_IOTA, nsad);
   int* asc = get<int>(ctx, S_ASC, nsad);
-  unsigned long long* skey2 = get<unsigned long long>(ctx, S_SKEY2, nsad);
+
   if (nsad > 0) {
     LK(iota_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(iota, nsad));
-    sort_pairs(ctx, skey, skey2, iota, asc, nsad, st, 32 + (B > 1 ? bits_for(B) : 0));
+    if (B > 1)
+      sort_pairs(ctx, skey, get<unsigned long long>(ctx, S_SKEY2, nsad), iota, asc, nsad, st, 32 + bits_for(B));
+    else
+      sort_pairs(ctx, skey32, get<uint32_t>(ctx, S_SKEY32B, nsad), iota, asc, nsad, st, 32);
   }
   mark(ctx, 3, st);
 

@@ -466,7 +466,7 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     int* __restrict__ crit_min, int* __restrict__ crit_sad, int* __restrict__ crit_max, int* __restrict__ min_img,
     int* __restrict__ sad_img, int* __restrict__ max_img, int* __restrict__ min_rank, int* __restrict__ max_rank,
     float* __restrict__ min_val, float* __restrict__ max_val, float* __restrict__ sad_val,
-    unsigned long long* __restrict__ sad_key) {
+    unsigned long long* __restrict__ sad_key, uint32_t* __restrict__ sad_key32) {
   const int lane = threadIdx.x & 31;
   long long seg = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (seg >= nseg) return;
@@ -514,7 +514,10 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     sad_img[p] = b;
     float v = dual ? cell_value_g<true>(img, t, iy, ix, H, W) : cell_value_g<false>(img, t, iy, ix, H, W);
     sad_val[p] = v;
-    sad_key[p] = ((unsigned long long)b << 32) | orderable_key(v);
+    if (sad_key32)  // one image: the image id is 0, a 32-bit key suffices
+      sad_key32[p] = orderable_key(v);
+    else
+      sad_key[p] = ((unsigned long long)b << 32) | orderable_key(v);
     p++;
   }
 }
