@@ -36,7 +36,7 @@ namespace {
 
 
 enum Slot {
-  S_GRAD, S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
+  S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
   S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
   S_ASC, S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
   S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX, S_SKEY32, S_SKEY32B,
@@ -123,7 +123,6 @@ struct dmsc_b200_context {
   std::vector<int> hH, hW;
   std::vector<uint8_t> hdual;
   Bases bases{};
-  const int* grad = nullptr;
   const uint8_t* flow = nullptr;
   const float* img = nullptr;  // input of the last extract (read again by fetch_pair_pixels)
   int* crit_sad = nullptr;
@@ -695,8 +694,9 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   const long long ncells = 4 * nidx;
 
   // ---- K1 gradient + criticality (all images, one grid) ----
-  int* grad = ret_grad ? grad_out : get<int>(ctx, S_GRAD, ncells);
-  ctx->grad = grad;
+  // the 16 B/index gradient is written only when returned; every later stage
+  // works from the mask and the flow codes
+  int* grad = ret_grad ? grad_out : nullptr;
   uint8_t* mask = get<uint8_t>(ctx, S_MASK, nidx);
   uint8_t* flow = get<uint8_t>(ctx, S_FLOW, nidx);
   ctx->flow = flow;

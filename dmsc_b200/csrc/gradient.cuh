@@ -266,8 +266,9 @@ __device__ __forceinline__ int slot_face_cell(int f, int b, int Nx) { return 3 +
 // (when owned there) its H edge, V edge and face from pixel (iy, ix), else
 // the H edge from (iy, ix-1), the V edge from (iy-1, ix) and the face from
 // (iy, ix-1), (iy-1, ix) or (iy-1, ix-1). Coalesced int4 gradient stores at
-// global index base `gbase`, criticality mask, flow codes and the row
-// segment's counts (segment id `seg`).
+// global index base `gbase` (skipped when `grad` is null: the later stages
+// read only the mask and flow codes), criticality mask, flow codes and the
+// row segment's counts (segment id `seg`).
 template <bool INTERIOR>
 __device__ __forceinline__ void gradient_store_row(const uint32_t (*word)[kTileX + 1], int warp, int lane, int H,
                                                    int W, int iy, int ix, long long gbase, int seg,
@@ -304,7 +305,7 @@ __device__ __forceinline__ void gradient_store_row(const uint32_t (*word)[kTileX
     const int fb = f0 != kNotMine ? b : f1 != kNotMine ? b - 1 : f2 != kNotMine ? b - Nx : b - Nx - 1;
     const int s3 = fn < 4u ? slot_edge_cell((int)fn, fb, Nx) : -1;
     const size_t gidx = (size_t)(gbase + b);
-    grad[gidx] = make_int4(s0, s1, s2, s3);
+    if (grad) grad[gidx] = make_int4(s0, s1, s2, s3);  // null when the gradient is not returned
     if (vk < 0 && (INTERIOR || (iy < H && ix < W))) m |= 1u;
     if (hn == 15u) m |= 2u;
     if (vn == 15u) m |= 4u;
