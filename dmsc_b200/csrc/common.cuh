@@ -188,6 +188,47 @@ __device__ __forceinline__ int block_reserve(int* counter, int cnt) {
   return r;
 }
 
+// Block-aggregated reservation on two counters at once (n0 slots on c0 and
+// n1 on c1 per thread), with one pair of barriers for both and the warp
+// totals scanned by warp 0. The two counts share one 32-bit scan, so each
+// block total must stay below 65536. Every thread of the block must call it
+// (blockDim.x a multiple of 32, at most 1024). p0 and p1 receive this
+// thread's first slots.
+__device__ __forceinline__ void block_reserve2(int* c0, int n0, int* c1, int n1, int& p0, int& p1) {
+  __shared__ unsigned wsum2[32];
+  __shared__ int bbase2[2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned mine = (unsigned)n0 | ((unsigned)n1 << 16);
+  unsigned x = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum2[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const unsigned s = lane < nw ? wsum2[lane] : 0u;
+    unsigned incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane < nw) wsum2[lane] = incl - s;
+    if (lane == 31) {  // block totals
+      const unsigned t0 = incl & 0xFFFFu, t1 = incl >> 16;
+      bbase2[0] = t0 ? atomicAdd(c0, (int)t0) : 0;
+      bbase2[1] = t1 ? atomicAdd(c1, (int)t1) : 0;
+    }
+  }
+  __syncthreads();
+  const unsigned e = wsum2[warp] + x - mine;  // exclusive prefix of this thread
+  p0 = bbase2[0] + (int)(e & 0xFFFFu);
+  p1 = bbase2[1] + (int)(e >> 16);
+  __syncthreads();
+}
+
 // Block-aggregated append: one global atomic per block. Every thread of the
 // block must call it (with blockDim.x a multiple of 32, at most 1024).
 // Returns the slot of this thread's item, or -1 when `take` is false.

@@ -113,42 +113,15 @@ struct LabelOut {
   const int* dual_off;
 };
 
-// K9: labels. One thread per face index (FACES) or per pixel (vertices) of
-// the batch: walk to the critical cell and read its label from the map.
-template <bool FACES>
-__global__ void __launch_bounds__(256) label_kernel(Imgs I, const uint8_t* __restrict__ flow, long long n,
-                                                    const int* __restrict__ label_map, LabelOut O, long long cap,
-                                                    unsigned* status) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int b = find_image(FACES ? I.idx_base : I.px_base, I.B, i);
-  const bool d = I.dual[b];
-  int* out = d ? O.dual : O.primal;
-  if (!out) return;
-  const int W = I.W[b], Nx = W + 1;
-  long long local;
-  int idx;
-  if (FACES) {
-    local = i - I.idx_base[b];
-    idx = (int)i;
-  } else {
-    local = i - I.px_base[b];
-    int y = (int)(local / W), x = (int)(local - (long long)y * W);
-    idx = I.idx_base[b] + y * Nx + x;
-  }
-  long long steps;
-  int end = flow_walk<FACES ? 4 : 0>(flow, idx, Nx, cap, &steps, status);
-  out[(d ? O.dual_off : O.primal_off)[b] + local] = steps <= cap ? __ldg(label_map + end) : -1;
-}
-
 // ---------------------------------------------------------------------------
 // K9 (tiled): labels of both sides through 64 x 64 index tiles. A tile's flow
 // codes are staged in shared memory, so every step of a V-path inside the
 // tile is a shared-memory read. A path that leaves the tile continues from
 // the first cell outside it, which lies on the border of the neighbouring
-// tile; label_perimeter_kernel resolves every border cell of every tile
-// first (to its critical cell, or to its own exit), so label_tile_kernel
-// crosses each further tile with one lookup in that map.
+// tile: label_tile_kernel writes, for every border cell of every tile, its
+// label or the border-map entry of the cell its path next enters, and lists
+// the cells whose paths leave their tile; label_exit_kernel then crosses each
+// further tile of such a path with one lookup in that border map.
 constexpr int kLT = 64;
 constexpr int kLTN = kLT * kLT;
 constexpr int kPerim = 4 * kLT;  // border slots per tile: top row, bottom row, left column, right column
@@ -364,30 +337,39 @@ __global__ void __launch_bounds__(kLabelThreads, 2) label_tile_kernel(Imgs I, co
   const int c = threadIdx.x % kLT, rb = threadIdx.x / kLT;
   const int ntx = label_ntx(g);
   const bool border_c = c == 0 || c == kLT - 1;
+  // cells of this thread whose path leaves the tile, on a side whose labels
+  // this image outputs: bit 2k (faces) and 2k + 1 (vertices); all of them are
+  // reserved in the exit lists at once
+  unsigned xm = 0;
 #pragma unroll
+  for (int k = 0; k < kTileCells; ++k) {
+    const int r = rb + 16 * k, i = r * kLT + c;
+    const int y = g.y0 + r, x = g.x0 + c;
+    if (F.perim && of && y <= g.H && x <= g.W && (st[0][i] & kExit)) xm |= 1u << (2 * k);
+    if (V.perim && ov && y < g.H && x < g.W && (st[1][i] & kExit)) xm |= 2u << (2 * k);
+  }
+  int pf, pv;
+  block_reserve2(n_exits + 0, __popc(xm & 0x55u), n_exits + 1, __popc(xm & 0xAAu), pf, pv);
+#pragma unroll 1
   for (int k = 0; k < kTileCells; ++k) {
     const int r = rb + 16 * k, i = r * kLT + c;
     const int y = g.y0 + r, x = g.x0 + c;
     const long long gidx = g.base + (long long)r * g.Nx + c;
     const bool border = border_c || r == 0 || r == kLT - 1;
     const long long po = (long long)blockIdx.x * kPerim + perim_slot(r, c);
-    int ef = 1, ev = 1;  // odd: nothing to append
     if (F.perim && y <= g.H && x <= g.W) {
-      ef = state_entry<true>(st[0][i], fl, R, F.lab, blockIdx.x, ntx);
+      // odd: (label << 1) | 1 of a path ending in the tile; even: exit entry
+      const int ef = state_entry<true>(st[0][i], fl, R, F.lab, blockIdx.x, ntx);
       if (border) F.perim[po] = ef;
       if (of && (ef & 1)) of[(long long)y * g.Nx + x] = ef >> 1;
-      if (!of) ef = 1;
+      if ((xm >> (2 * k)) & 1u) exits_f[pf++] = make_int2((int)gidx, ef);
     }
     if (V.perim && y < g.H && x < g.W) {
-      ev = state_entry<false>(st[1][i], fl, R, V.lab, blockIdx.x, ntx);
+      const int ev = state_entry<false>(st[1][i], fl, R, V.lab, blockIdx.x, ntx);
       if (border) V.perim[po] = ev;
       if (ov && (ev & 1)) ov[(long long)y * g.W + x] = ev >> 1;
-      if (!ov) ev = 1;
+      if ((xm >> (2 * k + 1)) & 1u) exits_v[pv++] = make_int2((int)gidx, ev);
     }
-    const int pf = block_append(n_exits + 0, !(ef & 1));
-    const int pv = block_append(n_exits + 1, !(ev & 1));
-    if (!(ef & 1)) exits_f[pf] = make_int2((int)gidx, ef);
-    if (!(ev & 1)) exits_v[pv] = make_int2((int)gidx, ev);
   }
 }
 
