@@ -139,7 +139,7 @@ struct Imgs {
   const int* W;
   const int* idx_base;   // indices
   const int* px_base;    // pixels
-  const int* tile_base;  // 32 x 16 gradient tiles
+  const int* tile_base;  // 32 x 64 gradient index tiles
   const int* seg_base;   // 32-index row segments
   const int* ltile_base;  // 64 x 64 label tiles
   const uint8_t* dual;
@@ -160,72 +160,80 @@ __device__ __forceinline__ int find_image(const int* __restrict__ base, int B, l
 }
 
 // Block-aggregated reservation of `cnt` consecutive slots per thread: one
-// global atomic per block. Every thread of the block must call it (blockDim.x
-// a multiple of 32, at most 1024). Returns this thread's first slot.
+// global atomic per block, the warp totals scanned by warp 0. Every thread of
+// the block must call it (blockDim.x a multiple of 32, at most 1024). Returns
+// this thread's first slot.
 __device__ __forceinline__ int block_reserve(int* counter, int cnt) {
   __shared__ int wsum[32], bbase_r;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int x = cnt;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, x, o);
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
     if (lane >= o) x += y;
   }
   if (lane == 31) wsum[warp] = x;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int s = 0;
-    for (int w = 0; w < nw; ++w) {
-      int t = wsum[w];
-      wsum[w] = s;
-      s += t;
+  if (warp == 0) {
+    const int s = lane < nw ? wsum[lane] : 0;
+    int incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
     }
-    bbase_r = s ? atomicAdd(counter, s) : 0;
+    if (lane < nw) wsum[lane] = incl - s;
+    if (lane == 31) bbase_r = incl ? atomicAdd(counter, incl) : 0;  // block total
   }
   __syncthreads();
-  int r = bbase_r + wsum[warp] + x - cnt;
+  const int r = bbase_r + wsum[warp] + x - cnt;
   __syncthreads();
   return r;
 }
 
-// Block-aggregated reservation on two counters at once (n0 slots on c0 and
-// n1 on c1 per thread), with one pair of barriers for both and the warp
-// totals scanned by warp 0. The two counts share one 32-bit scan, so each
-// block total must stay below 65536. Every thread of the block must call it
-// (blockDim.x a multiple of 32, at most 1024). p0 and p1 receive this
-// thread's first slots.
+// The same on two counters at once (n0 slots on c0 and n1 on c1 per thread),
+// with one set of barriers for both. A counter that receives no slots from
+// the block is not touched. p0 and p1 receive this thread's first slots.
 __device__ __forceinline__ void block_reserve2(int* c0, int n0, int* c1, int n1, int& p0, int& p1) {
-  __shared__ unsigned wsum2[32];
-  __shared__ int bbase2[2];
+  __shared__ int wsum2[2][32], bbase2[2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const unsigned mine = (unsigned)n0 | ((unsigned)n1 << 16);
-  unsigned x = mine;
+  int x0 = n0, x1 = n1;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
+    const int y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
+    if (lane >= o) {
+      x0 += y0;
+      x1 += y1;
+    }
   }
-  if (lane == 31) wsum2[warp] = x;
+  if (lane == 31) {
+    wsum2[0][warp] = x0;
+    wsum2[1][warp] = x1;
+  }
   __syncthreads();
   if (warp == 0) {
-    const unsigned s = lane < nw ? wsum2[lane] : 0u;
-    unsigned incl = s;
+    const int s0 = lane < nw ? wsum2[0][lane] : 0, s1 = lane < nw ? wsum2[1][lane] : 0;
+    int i0 = s0, i1 = s1;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
+      const int y0 = __shfl_up_sync(0xffffffffu, i0, o), y1 = __shfl_up_sync(0xffffffffu, i1, o);
+      if (lane >= o) {
+        i0 += y0;
+        i1 += y1;
+      }
     }
-    if (lane < nw) wsum2[lane] = incl - s;
+    if (lane < nw) {
+      wsum2[0][lane] = i0 - s0;
+      wsum2[1][lane] = i1 - s1;
+    }
     if (lane == 31) {  // block totals
-      const unsigned t0 = incl & 0xFFFFu, t1 = incl >> 16;
-      bbase2[0] = t0 ? atomicAdd(c0, (int)t0) : 0;
-      bbase2[1] = t1 ? atomicAdd(c1, (int)t1) : 0;
+      bbase2[0] = i0 ? atomicAdd(c0, i0) : 0;
+      bbase2[1] = i1 ? atomicAdd(c1, i1) : 0;
     }
   }
   __syncthreads();
-  const unsigned e = wsum2[warp] + x - mine;  // exclusive prefix of this thread
-  p0 = bbase2[0] + (int)(e & 0xFFFFu);
-  p1 = bbase2[1] + (int)(e >> 16);
+  p0 = bbase2[0] + wsum2[0][warp] + x0 - n0;
+  p1 = bbase2[1] + wsum2[1][warp] + x1 - n1;
   __syncthreads();
 }
 
@@ -233,21 +241,24 @@ __device__ __forceinline__ void block_reserve2(int* c0, int n0, int* c1, int n1,
 // block must call it (with blockDim.x a multiple of 32, at most 1024).
 // Returns the slot of this thread's item, or -1 when `take` is false.
 __device__ __forceinline__ int block_append(int* counter, bool take) {
-  __shared__ int wcount[32], wbase[32], bbase;
+  __shared__ int wbase[32], bbase;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  unsigned b = __ballot_sync(0xffffffffu, take);
-  if (lane == 0) wcount[warp] = __popc(b);
+  const unsigned b = __ballot_sync(0xffffffffu, take);
+  if (lane == 0) wbase[warp] = __popc(b);
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int s = 0;
-    for (int w = 0; w < nw; ++w) {
-      wbase[w] = s;
-      s += wcount[w];
+  if (warp == 0) {
+    const int s = lane < nw ? wbase[lane] : 0;
+    int incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
     }
-    bbase = s ? atomicAdd(counter, s) : 0;
+    if (lane < nw) wbase[lane] = incl - s;
+    if (lane == 31) bbase = incl ? atomicAdd(counter, incl) : 0;  // block total
   }
   __syncthreads();
-  int r = take ? bbase + wbase[warp] + __popc(b & ((1u << lane) - 1u)) : -1;
+  const int r = take ? bbase + wbase[warp] + __popc(b & ((1u << lane) - 1u)) : -1;
   __syncthreads();
   return r;
 }

@@ -418,9 +418,10 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
         r1 = ((rd & 1) ? P.s[1].act1 : P.s[1].act0)[i - na];
         k1 = replay_step(P.s[1], r1, rd);
       }
-      // every thread of the block takes part in the reservations
-      const int p0 = P.s[0].n_cancel ? block_reserve(P.s[0].cnt + (rd + 1) % 3, k0 ? 1 : 0) : 0;
-      const int p1 = P.s[1].n_cancel ? block_reserve(P.s[1].cnt + (rd + 1) % 3, k1 ? 1 : 0) : 0;
+      // every thread of the block takes part in the reservation (a side
+      // without cancellations reserves nothing and its counter is not touched)
+      int p0, p1;
+      block_reserve2(P.s[0].cnt + (rd + 1) % 3, k0 ? 1 : 0, P.s[1].cnt + (rd + 1) % 3, k1 ? 1 : 0, p0, p1);
       if (k0) ((rd & 1) ? P.s[0].act0 : P.s[0].act1)[p0] = r0;
       if (k1) ((rd & 1) ? P.s[1].act0 : P.s[1].act1)[p1] = r1;
     }
@@ -482,8 +483,8 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
         }
       }
     }
-    int p = block_reserve(A.cnt, push ? 1 : 0);
-    int pb = block_reserve(E.n_base, seg ? 1 : 0);
+    int p, pb;
+    block_reserve2(A.cnt, push ? 1 : 0, E.n_base, seg ? 1 : 0, p, pb);
     if (push) {
       if (p < E.q_cap)
         A.q0[p] = task;
@@ -524,8 +525,8 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
         rev = (t.x >> 2) & 1;
         if (kind == kTaskChain && !chain_expand_counts(E, t.y, t.z, &need, &nb, &total)) kind = -1;
       }
-      int p = block_reserve(E.n_out, need);
-      int pb = block_reserve(E.n_base, nb);
+      int p, pb;
+      block_reserve2(E.n_out, need, E.n_base, nb, p, pb);
       if (p + (long long)need > E.q_cap || pb + (long long)nb > E.base_cap) {
         set_status(E.status, kStatusQueueOverflow);
         kind = -1;
