@@ -183,7 +183,7 @@ __device__ __forceinline__ void pair_phase_b1(const PairArgs& A, int r, long lon
   A.hdec[k] = h;
 }
 
-__global__ void __launch_bounds__(256) pairing_persistent_kernel(PairArgs2 P) {
+__global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P) {
   __shared__ ChunkLists L;
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
