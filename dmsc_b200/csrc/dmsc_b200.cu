@@ -442,7 +442,6 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
   A.act1 = sget<int>(ctx, si, X_ACT1, nsad);
   A.roots0 = sget<int>(ctx, si, X_GRP, M + 1);
   A.roots1 = sget<int>(ctx, si, X_UF, M + 1);
-  A.hdec = sget<int>(ctx, si, X_CROOT, M + 1);
   A.cnt = sget<int>(ctx, si, X_CNT, 8);
   A.val = S.val;
   A.cell = S.crit;

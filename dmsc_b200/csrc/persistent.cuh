@@ -101,7 +101,6 @@ struct PairArgs {
   int* act1;
   int* roots0;        // live group roots (ping-pong), [M+1] each
   int* roots1;
-  int* hdec;          // [M+1] decision per root-list slot
   int* cnt;           // [0..2] rotating active counts, [3..5] rotating root counts
   const float* val;
   const int* cell;
@@ -119,10 +118,12 @@ struct PairArgs {
 // their grid barriers. Per round and side: (A) every active saddle finds its
 // ends' groups, cycles are decided, the rest reduce their sweep index into
 // both groups' minimum (no returned value needed) and stay active; (B1) every
-// live root with an outgoing saddle decides whether it dies there and stays
-// live otherwise; roots without outgoing saddles leave the list for good;
-// (B2) the links are applied. Round 0 skips the lookups: all groups are
-// single extrema. A side whose active list is empty just idles.
+// live root with an outgoing saddle decides whether it dies there, and a
+// root that dies links itself under the other group's root at once (phase B1
+// reads no link, and the next reader is the next round's phase A, behind the
+// round's barrier); the others stay live; roots without outgoing saddles
+// leave the list for good. Round 0 skips the lookups: all groups are single
+// extrema. A side whose active list is empty just idles.
 struct PairArgs2 {
   PairArgs s[2];
 };
@@ -168,19 +169,18 @@ __device__ __forceinline__ void pair_phase_b1(const PairArgs& A, int r, long lon
   if (me != kNoEdge) {
     A.minedge[g] = kNoEdge;
     int e = (int)me;
-    int ga = A.g1[e], gb = A.g2[e];  // roots as of phase A; links change only in B2
+    int ga = A.g1[e], gb = A.g2[e];  // roots as of phase A
     h = (ga == g) ? gb : ga;
     // g is an extremum of one image (the void never dies); older = value_less
     // order on the vertex side in the primal and the face side in the dual
     const bool du = g < M && A.dual[A.ext_img[g]];
     if (older(h, g, M, A.val, A.cell, A.faces ? du : !du)) {
       A.dying[e] = g;
+      A.link[g] = h;
     } else {
-      h = -1;
       live = true;
     }
   }
-  A.hdec[k] = h;
 }
 
 __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P) {
@@ -275,15 +275,6 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
         chunk_flush(L, P.s[0].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[0].roots0 : P.s[0].roots1,
                     P.s[1].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[1].roots0 : P.s[1].roots1);
       }
-    }
-    grid.sync();
-    // phase B2: apply the links
-    for (long long k = tid; k < (long long)nr0 + nr1; k += nth) {
-      const int sd = k < nr0 ? 0 : 1;
-      const PairArgs& A = P.s[sd];
-      const long long kk = sd ? k - nr0 : k;
-      const int h = A.hdec[kk];
-      if (h >= 0) A.link[((r & 1) ? A.roots1 : A.roots0)[kk]] = h;
     }
     grid.sync();
   }
