@@ -1063,7 +1063,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
     int per = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel, 256, 0));
     E.n_base = A.cnt + 3;
-    LK(emit_segments_kernel<<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3, nullptr));
+    LK(emit_segments_kernel<<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3));
     LAUNCH_CHECK("emit_segments_kernel");
   }
 }

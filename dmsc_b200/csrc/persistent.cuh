@@ -528,17 +528,42 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
   }
 }
 
-// Every raw-arc segment collected by emit_persistent_kernel, one thread per
-// segment at full occupancy (grid-stride over the device-side count).
-__global__ void __launch_bounds__(256) emit_segments_kernel(EmitCtx E, const int* __restrict__ count,
-                                                            unsigned long long* timeline_end) {
-  const int nb = *count;
-  const long long nth = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nb && i < E.base_cap; i += nth) {
-    int4 t = E.base_q[i];
-    emit_base(E, t.y, t.z, (t.x >> 2) & 1, t.w);
+// Every raw-arc segment collected by emit_persistent_kernel. Segment
+// lengths are very uneven, so a lane that finishes its segment takes the next
+// one instead of idling until the warp's longest is done: each warp owns
+// ranges of kSegRange consecutive segments (grid-stride over the ranges) and,
+// every kSegSteps cells, hands the next unstarted segments of its range to its
+// idle lanes by ballot (warp-local, no atomics).
+constexpr int kSegRange = 256;
+constexpr int kSegSteps = 8;
+
+__global__ void __launch_bounds__(256) emit_segments_kernel(EmitCtx E, const int* __restrict__ count) {
+  const long long nb = min((long long)*count, E.base_cap);
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r0 = warp * kSegRange; r0 < nb; r0 += nwarps * kSegRange) {
+    const long long r1 = min(nb, r0 + kSegRange);
+    long long next = r0;  // first segment of the range not yet handed out (same in every lane)
+    SegCursor c;
+    c.rem = 0;
+    while (true) {
+      const unsigned idle = __ballot_sync(0xffffffffu, c.rem <= 0);
+      if (c.rem <= 0) {
+        const long long my = next + __popc(idle & lt);
+        if (my < r1) {
+          const int4 t = E.base_q[my];
+          seg_start(E, t.y, t.z, (t.x >> 2) & 1, t.w, c);
+        }
+      }
+      next += __popc(idle);
+      if (next >= r1 && __ballot_sync(0xffffffffu, c.rem > 0) == 0) break;
+#pragma unroll 1
+      for (int k = 0; k < kSegSteps; ++k)
+        if (c.rem > 0) seg_step(E, c);
+    }
   }
-  (void)timeline_end;
 }
 
 }  // namespace dmsc

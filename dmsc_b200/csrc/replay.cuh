@@ -207,23 +207,43 @@ struct EmitCtx {
   unsigned* status;
 };
 
-// Writes raw arc (s, j): the V-path from its start cell, `len` cells
-// (cpu/arcs_geometry.hxx:83-111, 133-161), following the flow codes.
-__device__ void emit_base(const EmitCtx& E, int s, int j, int rev, long long pos) {
-  long long len = E.blen[2 * s + j];
+// A raw arc (s, j) being written by one lane: the V-path from its start cell,
+// `len` cells (cpu/arcs_geometry.hxx:83-111, 133-161), following the flow
+// codes. dst is the next output slot, step its stride (-1 for a reversed
+// arc), rem the cells left and idx the current index.
+struct SegCursor {
+  int* dst;
+  int step;
+  long long rem;
+  int idx, ibase, Nx;
+};
+
+// Starts raw arc (s, j) at output position pos; rem = 0 when it writes
+// nothing (no arc, or its image's output does not take this side's arcs).
+__device__ __forceinline__ void seg_start(const EmitCtx& E, int s, int j, int rev, long long pos, SegCursor& c) {
+  c.rem = 0;
+  const long long len = E.blen[2 * s + j];
   if (len <= 0) return;
   const int b = E.sad_img[s];
-  const int W = E.I.W[b], Nx = W + 1, ibase = E.I.idx_base[b];
   int* out = E.I.dual[b] ? E.out_dual : E.out_primal;
   if (!out) return;
-  int sc = E.crit_sad[s];
-  int cell = E.faces ? face_start(sc, j, Nx) : vertex_start(sc, j, E.I.H[b], W, Nx, ibase);
-  const int type = cell & 3, shift = E.faces ? 4 : 0;
-  int idx = cell >> 2;
-  for (long long k = 0; k < len; ++k) {
-    out[rev ? pos + len - 1 - k : pos + k] = type + 4 * (idx - ibase);  // image-local cell id
-    if (k + 1 < len) idx += flow_step((__ldg(E.flow + idx) >> shift) & 0xFu, Nx);
-  }
+  const int W = E.I.W[b];
+  c.Nx = W + 1;
+  c.ibase = E.I.idx_base[b];
+  const int sc = E.crit_sad[s];
+  const int cell = E.faces ? face_start(sc, j, c.Nx) : vertex_start(sc, j, E.I.H[b], W, c.Nx, c.ibase);
+  c.idx = cell >> 2;
+  c.dst = out + (rev ? pos + len - 1 : pos);
+  c.step = rev ? -1 : 1;
+  c.rem = len;
+}
+
+// Writes the cursor's cell (image-local id: faces are type 3, vertices type 0)
+// and moves to the next one.
+__device__ __forceinline__ void seg_step(const EmitCtx& E, SegCursor& c) {
+  *c.dst = (E.faces ? 3 : 0) + 4 * (c.idx - c.ibase);
+  c.dst += c.step;
+  if (--c.rem > 0) c.idx += flow_step((__ldg(E.flow + c.idx) >> (E.faces ? 4 : 0)) & 0xFu, c.Nx);
 }
 
 // Number of raw-arc segments W(d) contributes.
