@@ -37,7 +37,7 @@ namespace {
 
 enum Slot {
   S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
-  S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_RMIN, S_RMAX, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
+  S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_MINBITS, S_MAXBITS, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
   S_ASC, S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
   S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX, S_SKEY32, S_SKEY32B,
   S_SIDE0,  // per-side slots start here, kSideSlots each
@@ -74,7 +74,6 @@ struct Side {
   int* crit = nullptr;
   int* ext_img = nullptr;
   float* val = nullptr;
-  int* rank_map = nullptr;
   int* t = nullptr;
   int* steps = nullptr;
   int* sweep = nullptr;
@@ -724,8 +723,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   int* imin = get<int>(ctx, S_IMIN, nmin);
   int* isad = get<int>(ctx, S_ISAD, nsad);
   int* imax = get<int>(ctx, S_IMAX, nmax);
-  int* rmin = get<int>(ctx, S_RMIN, nidx);
-  int* rmax = get<int>(ctx, S_RMAX, nidx);
+  uint32_t* bmin = get<uint32_t>(ctx, S_MINBITS, nseg);  // per-segment bit masks of the extrema
+  uint32_t* bmax = get<uint32_t>(ctx, S_MAXBITS, nseg);
   float* vmin = get<float>(ctx, S_VMIN, nmin);
   float* vmax = get<float>(ctx, S_VMAX, nmax);
   float* sval = get<float>(ctx, S_SVAL, nsad);
@@ -735,7 +734,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   ctx->crit_sad = csad;
   ctx->sad_img = isad;
   LK(compact_kernel<<<grid_for(nseg, 8), 256, 0, st>>>(I, img, nseg, mask, off[0], off[1], off[2], cmin, csad, cmax,
-                                                       imin, isad, imax, rmin, rmax, vmin, vmax, sval, skey, skey32));
+                                                       imin, isad, imax, bmin, bmax, vmin, vmax, sval, skey, skey32));
   LAUNCH_CHECK("compact_kernel");
   // per-image bases of the critical lists (B + 1 entries each)
   int* bases = get<int>(ctx, S_BASES, 9 * (size_t)(B + 1));
@@ -773,7 +772,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   int* tv = get<int>(ctx, S_TV, 2 * (size_t)nsad);
   int* lv = get<int>(ctx, S_LV, 2 * (size_t)nsad);
   if (nsad > 0) {
-    LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(I, flow, nsad, csad, isad, rmax, rmin, tf, lf, tv, lv,
+    LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(I, flow, nsad, csad, isad, off[2], bmax, off[0], bmin, tf,
+                                                             lf, tv, lv,
                                                              ncells, ctx->status));
     LAUNCH_CHECK("saddle_walk_kernel");
   }
@@ -793,8 +793,6 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   V.ext_img = imin;
   F.val = vmax;
   V.val = vmin;
-  F.rank_map = rmax;
-  V.rank_map = rmin;
   F.t = tf;
   F.steps = lf;
   V.t = tv;

@@ -458,14 +458,17 @@ __device__ __forceinline__ float cell_value_g(const float* __restrict__ img, int
 // segment offsets are exclusive scans of the per-segment counts over the
 // whole batch (images in order, rows in order), so each image's lists are a
 // contiguous slice in ascending cell-id order. Writes the three lists as
-// global cell ids, each critical cell's image, the index -> dense-rank maps of
-// the extrema, the extremum values and the saddle values with their sort keys
-// (image id above the orderable value, so one sort orders every image).
+// global cell ids, each critical cell's image, the per-segment bit masks of
+// the minima and maxima (an extremum's list rank is its segment's offset plus
+// the extrema before it in the mask), the extremum values and the saddle
+// values with their sort keys (image id above the orderable value, so one
+// sort orders every image).
 static __global__ void __launch_bounds__(256) compact_kernel(
     Imgs I, const float* __restrict__ img_all, long long nseg, const uint8_t* __restrict__ crit_mask,
     const int* __restrict__ off_min, const int* __restrict__ off_sad, const int* __restrict__ off_max,
     int* __restrict__ crit_min, int* __restrict__ crit_sad, int* __restrict__ crit_max, int* __restrict__ min_img,
-    int* __restrict__ sad_img, int* __restrict__ max_img, int* __restrict__ min_rank, int* __restrict__ max_rank,
+    int* __restrict__ sad_img, int* __restrict__ max_img, uint32_t* __restrict__ min_bits,
+    uint32_t* __restrict__ max_bits,
     float* __restrict__ min_val, float* __restrict__ max_val, float* __restrict__ sad_val,
     unsigned long long* __restrict__ sad_key, uint32_t* __restrict__ sad_key32) {
   const int lane = threadIdx.x & 31;
@@ -485,6 +488,10 @@ static __global__ void __launch_bounds__(256) compact_kernel(
   unsigned lt = (1u << lane) - 1u;
   unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
   unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
+  if (lane == 0) {
+    min_bits[seg] = bmin;
+    max_bits[seg] = bmax;
+  }
   int ns = ((m >> 1) & 1u) + ((m >> 2) & 1u);
   int incl = ns;
 #pragma unroll
@@ -497,14 +504,12 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     int p = off_min[seg] + __popc(bmin & lt);
     crit_min[p] = (int)(4 * gidx);
     min_img[p] = b;
-    min_rank[gidx] = p;
     min_val[p] = __ldg(img + (size_t)iy * W + ix);
   }
   if (m & 8u) {
     int p = off_max[seg] + __popc(bmax & lt);
     crit_max[p] = (int)(4 * gidx + 3);
     max_img[p] = b;
-    max_rank[gidx] = p;
     max_val[p] = dual ? cell_value_g<true>(img, 3, iy, ix, H, W) : cell_value_g<false>(img, 3, iy, ix, H, W);
   }
   int p = off_sad[seg] + excl;

@@ -56,13 +56,26 @@ __device__ __forceinline__ int flow_walk(const uint8_t* __restrict__ flow, int i
   return idx;
 }
 
+// Dense rank in its critical list of the extremum at global index g of image
+// b: its 32-index row segment's first rank (the compaction's exclusive scan)
+// plus the extrema before it in the segment's bit mask.
+__device__ __forceinline__ int seg_rank(const Imgs& I, int b, int g, int Nx, const int* __restrict__ off,
+                                        const uint32_t* __restrict__ bits) {
+  const int l = g - I.idx_base[b];
+  const int y = l / Nx, x = l - y * Nx;
+  const int seg = I.seg_base[b] + y * ((Nx + 31) >> 5) + (x >> 5);
+  return __ldg(off + seg) + __popc(__ldg(bits + seg) & ((1u << (x & 31)) - 1u));
+}
+
 // K4: per saddle, both face walks and the vertex walks. Writes per arc
 // (2 per saddle and side): dense target index (or -1) and step count.
 __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t* __restrict__ flow, int nsad,
                                                           const int* __restrict__ crit_sad,
                                                           const int* __restrict__ sad_img,
-                                                          const int* __restrict__ max_rank,
-                                                          const int* __restrict__ min_rank, int* __restrict__ tf,
+                                                          const int* __restrict__ off_max,
+                                                          const uint32_t* __restrict__ max_bits,
+                                                          const int* __restrict__ off_min,
+                                                          const uint32_t* __restrict__ min_bits, int* __restrict__ tf,
                                                           int* __restrict__ lf, int* __restrict__ tv,
                                                           int* __restrict__ lv, long long cap, unsigned* status) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -74,7 +87,7 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
   for (int j = 0; j < 2; ++j) {
     long long steps;
     int end = flow_walk<4>(flow, face_start(sc, j, Nx) >> 2, Nx, cap, &steps, status);
-    tf[2 * s + j] = max_rank[end];
+    tf[2 * s + j] = seg_rank(I, b, end, Nx, off_max, max_bits);
     lf[2 * s + j] = (int)steps;
   }
 #pragma unroll
@@ -83,7 +96,7 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
     long long steps = 0;
     if (start >= 0) {
       int end = flow_walk<0>(flow, start >> 2, Nx, cap, &steps, status);
-      tv[2 * s + j] = min_rank[end];
+      tv[2 * s + j] = seg_rank(I, b, end, Nx, off_min, min_bits);
     } else {
       tv[2 * s + j] = -1;
     }
