@@ -334,12 +334,14 @@ __device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r, int roun
   else if (R1 == d && R0 != R1)
     k = 1;
   if (k >= 0) {
+    const long long b0 = A.blen[2 * s], b1 = A.blen[2 * s + 1];
     A.S.parent[d] = k == 0 ? R1 : R0;
-    A.S.side[d] = k;
+    // the dying side, and what W(d) expands to: its non-empty chains and raw-arc segments
+    A.S.side[d] = side_word(k, (a0 > 0) + (a1 > 0), (b0 > 0) + (b1 > 0));
     A.S.csad[d] = s;
     A.S.cl_dy[d] = k == 0 ? a0 : a1;
     A.S.cl_ot[d] = k == 0 ? a1 : a0;
-    A.S.wlen[d] = A.blen[2 * s] + A.blen[2 * s + 1] + a0 + a1;
+    A.S.wlen[d] = b0 + b1 + a0 + a1;
     A.S.status[d] = status_word(kLinked, round);
   } else {
     A.S.status[d] = status_word(kRootForever, round);

@@ -47,11 +47,19 @@ struct ReplayState {
   int* status;      // [M] kPending / kLinked / kRootForever, with the deciding round's tag
   int* parent;      // [M] link target (-1 = void) when kLinked
   long long* wlen;  // [M] length of W(node)
-  int* side;        // [M] dying side (0/1) of the node's cancellation
+  int* side;        // [M] side_word: dying side of the node's cancellation and what W(node) expands to
   int* csad;        // [M] saddle of the node's cancellation
   long long* cl_dy; // [M] chain length T_dying -> node at link time
   long long* cl_ot; // [M] chain length T_other -> parent at link time
 };
+
+// Side word of a linked node: the dying side k (bit 0), the number of
+// non-empty chains of W(node) (bits 1-2) and of its raw-arc segments (bits
+// 3-4), so counting a chain's expansion reads one word per node.
+__device__ __forceinline__ int side_word(int k, int n_chain, int n_base) { return k | (n_chain << 1) | (n_base << 3); }
+__device__ __forceinline__ int side_of(int w) { return w & 1; }
+__device__ __forceinline__ int chains_of(int w) { return (w >> 1) & 3; }
+__device__ __forceinline__ int bases_of(int w) { return (w >> 3) & 3; }
 
 // Root of x just before the replay step with key t, with the summed path
 // length; returns false when a node on the way is still undecided. Replay
@@ -246,21 +254,10 @@ __device__ __forceinline__ void seg_step(const EmitCtx& E, SegCursor& c) {
   if (--c.rem > 0) c.idx += flow_step((__ldg(E.flow + c.idx) >> (E.faces ? 4 : 0)) & 0xFu, c.Nx);
 }
 
-// Number of raw-arc segments W(d) contributes.
-__device__ __forceinline__ int w_base_count(const EmitCtx& E, int d) {
-  int k = E.S.side[d], s = E.S.csad[d];
-  return (E.blen[2 * s + k] > 0) + (E.blen[2 * s + 1 - k] > 0);
-}
-
-// Number of chain tasks W(d) produces (its two chains, when non-empty).
-__device__ __forceinline__ int w_task_count(const EmitCtx& E, int d) {
-  return (E.S.cl_dy[d] > 0) + (E.S.cl_ot[d] > 0);
-}
-
 // Expands W(d): queues its two chains at slot p and its two raw-arc segments
 // at base slot pb, advancing both.
 __device__ __forceinline__ void emit_w(const EmitCtx& E, int d, int rev, long long pos, int& p, int& pb) {
-  int k = E.S.side[d], o = 1 - k, s = E.S.csad[d];
+  int k = side_of(E.S.side[d]), o = 1 - k, s = E.S.csad[d];
   int Tk = E.t[2 * s + k], To = E.t[2 * s + o];
   long long la = E.S.cl_dy[d], lb = E.blen[2 * s + k], lc = E.blen[2 * s + o], ld = E.S.cl_ot[d];
   int R = E.S.parent[d];
@@ -295,8 +292,9 @@ __device__ __forceinline__ bool chain_expand_counts(const EmitCtx& E, int x, int
   *total = 0;
   while (z != stop && z >= 0) {
     tot += E.S.wlen[z];
-    nc += w_task_count(E, z);
-    nb += w_base_count(E, z);
+    const int w = E.S.side[z];  // counts stored at link time
+    nc += chains_of(w);
+    nb += bases_of(w);
     z = E.S.parent[z];
     if (++k > E.max_steps) {
       set_status(E.status, kStatusChainCap);
