@@ -44,8 +44,8 @@ enum Slot {
 };
 enum SideSlot {
   X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
-  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_CTIME, X_STAT, X_PAR, X_WLEN, X_SIDE,
-  X_CSAD, X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G1,
+  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_NODE,
+  X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G1,
   X_G2, X_GBASE, X_LAB, X_WX, X_WA, X_CENDS, kSideSlots
 };
 
@@ -518,16 +518,10 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   LAUNCH_CHECK("cancel_collect_kernel");
 
   ReplayState& R = S.R;
-  R.ctime = sget<unsigned long long>(ctx, si, X_CTIME, M + 1);
-  R.status = sget<int>(ctx, si, X_STAT, M + 1);
-  R.parent = sget<int>(ctx, si, X_PAR, M + 1);
-  R.wlen = sget<long long>(ctx, si, X_WLEN, M + 1);
-  R.side = sget<int>(ctx, si, X_SIDE, M + 1);
-  R.csad = sget<int>(ctx, si, X_CSAD, M + 1);
+  R.node = sget<ReplayNode>(ctx, si, X_NODE, M + 1);
   R.cl_dy = sget<long long>(ctx, si, X_CLDY, M + 1);
   R.cl_ot = sget<long long>(ctx, si, X_CLOT, M + 1);
-  LK(fill_u64_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.ctime, M + 1, kNever));
-  LK(fill_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.status, M + 1, kRootForever));
+  LK(replay_node_init_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.node, M + 1));
   LAUNCH_CHECK("replay init");
   ReplayArgs A{};
   A.n_cancel = S.C > 0 ? cnt + 3 : nullptr;

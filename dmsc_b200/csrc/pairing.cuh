@@ -47,16 +47,6 @@ __global__ void iota_kernel(int* __restrict__ a, int n) {
   if (i < n) a[i] = i;
 }
 
-__global__ void fill_u64_kernel(unsigned long long* __restrict__ a, long long n, unsigned long long v) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) a[i] = v;
-}
-
-__global__ void fill_kernel(int* __restrict__ a, long long n, int v) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) a[i] = v;
-}
-
 // Sweep-ordered edge list of one side for a batch. `asc` lists every image's
 // saddles in ascending (s_val, cell id), images in order; the face side sweeps
 // each image descending in the primal and ascending in the dual, the vertex

@@ -335,16 +335,17 @@ __device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r, int roun
     k = 1;
   if (k >= 0) {
     const long long b0 = A.blen[2 * s], b1 = A.blen[2 * s + 1];
-    A.S.parent[d] = k == 0 ? R1 : R0;
-    // the dying side, and what W(d) expands to: its non-empty chains and raw-arc segments
-    A.S.side[d] = side_word(k, (a0 > 0) + (a1 > 0), (b0 > 0) + (b1 > 0));
-    A.S.csad[d] = s;
     A.S.cl_dy[d] = k == 0 ? a0 : a1;
     A.S.cl_ot[d] = k == 0 ? a1 : a0;
-    A.S.wlen[d] = b0 + b1 + a0 + a1;
-    A.S.status[d] = status_word(kLinked, round);
+    A.S.node[d].wlen = b0 + b1 + a0 + a1;
+    // status, parent, the dying side with what W(d) expands to (its non-empty
+    // chains and raw-arc segments), and the saddle, in one store: no walk of
+    // this round reads a record whose status carries this round's tag
+    *reinterpret_cast<int4*>(&A.S.node[d].status) =
+        make_int4(status_word(kLinked, round), k == 0 ? R1 : R0,
+                  side_word(k, (a0 > 0) + (a1 > 0), (b0 > 0) + (b1 > 0)), s);
   } else {
-    A.S.status[d] = status_word(kRootForever, round);
+    A.S.node[d].status = status_word(kRootForever, round);
   }
   return false;
 }
@@ -360,8 +361,8 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
       A.act0[r] = (int)r;
       const int j = A.cj[r];
       int d = A.dying[j];
-      A.S.ctime[d] = A.key[r];
-      A.S.status[d] = kPending;
+      A.S.node[d].ctime = A.key[r];
+      A.S.node[d].status = kPending;
       A.wx[2 * r] = A.c1[j];
       A.wx[2 * r + 1] = A.c2[j];
       A.wa[2 * r] = 0;

@@ -42,16 +42,46 @@ enum : int { kPending = 0, kLinked = 1, kRootForever = 2 };
 __device__ __forceinline__ int status_kind(int st) { return st & 3; }
 __device__ __forceinline__ int status_word(int kind, int round) { return kind | ((round + 1) << 2); }
 
-struct ReplayState {
-  unsigned long long* ctime;  // [M] replay key of the cancellation killing the node, kNever if none
-  int* status;      // [M] kPending / kLinked / kRootForever, with the deciding round's tag
-  int* parent;      // [M] link target (-1 = void) when kLinked
-  long long* wlen;  // [M] length of W(node)
-  int* side;        // [M] side_word: dying side of the node's cancellation and what W(node) expands to
-  int* csad;        // [M] saddle of the node's cancellation
-  long long* cl_dy; // [M] chain length T_dying -> node at link time
-  long long* cl_ot; // [M] chain length T_other -> parent at link time
+// Everything a chain walk reads at one node, in one 32-byte sector, as two
+// 16-byte halves: (ctime, wlen) and (status, parent, side, csad).
+struct alignas(32) ReplayNode {
+  unsigned long long ctime;  // replay key of the cancellation killing the node, kNever if none
+  long long wlen;            // length of W(node)
+  int status;                // kPending / kLinked / kRootForever, with the deciding round's tag
+  int parent;                // link target (-1 = void) when kLinked
+  int side;                  // side_word: dying side of the node's cancellation and what W(node) expands to
+  int csad;                  // saddle of the node's cancellation
 };
+
+struct ReplayState {
+  ReplayNode* node;  // [M + 1]
+  long long* cl_dy;  // [M] chain length T_dying -> node at link time
+  long long* cl_ot;  // [M] chain length T_other -> parent at link time
+};
+
+// The halves of a node's record: through L2 inside the replay (other blocks
+// write records during the launch), plain loads after it.
+__device__ __forceinline__ longlong2 node_keylen_cg(const ReplayNode* n, int x) {
+  return __ldcg(reinterpret_cast<const longlong2*>(&n[x].ctime));
+}
+__device__ __forceinline__ int4 node_words_cg(const ReplayNode* n, int x) {
+  return __ldcg(reinterpret_cast<const int4*>(&n[x].status));
+}
+__device__ __forceinline__ longlong2 node_keylen(const ReplayNode* n, int x) {
+  return *reinterpret_cast<const longlong2*>(&n[x].ctime);
+}
+__device__ __forceinline__ int4 node_words(const ReplayNode* n, int x) {
+  return *reinterpret_cast<const int4*>(&n[x].status);
+}
+
+// Every node a root that is never cancelled, with tag 0 (a cancellation's
+// own key and kPending are set when the replay starts).
+__global__ void replay_node_init_kernel(ReplayNode* __restrict__ n, long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  *reinterpret_cast<longlong2*>(&n[i].ctime) = make_longlong2((long long)kNever, 0);
+  *reinterpret_cast<int4*>(&n[i].status) = make_int4(kRootForever, -1, 0, 0);
+}
 
 // Side word of a linked node: the dying side k (bit 0), the number of
 // non-empty chains of W(node) (bits 1-2) and of its raw-arc segments (bits
@@ -69,14 +99,15 @@ __device__ __forceinline__ bool walk_root(const ReplayState& S, int x, unsigned 
                                           long long* acc, int max_steps, unsigned* status) {
   long long a = 0;
   int steps = 0;
-  while (true) {
-    if (x < 0) break;
-    if (S.ctime[x] >= t) break;
-    int st = status_kind(S.status[x]);
+  while (x >= 0) {
+    const longlong2 kl = node_keylen(S.node, x);
+    const int4 w = node_words(S.node, x);
+    if ((unsigned long long)kl.x >= t) break;
+    const int st = status_kind(w.x);
     if (st == kPending) return false;
     if (st == kRootForever) break;
-    a += S.wlen[x];
-    x = S.parent[x];
+    a += kl.y;
+    x = w.y;
     if (++steps > max_steps) {
       set_status(status, kStatusChainCap);
       break;
@@ -99,15 +130,17 @@ __device__ __forceinline__ bool walk_resume(const ReplayState& S, int* x_io, uns
   bool done = true;
   while (true) {
     if (x < 0) break;
-    if (__ldcg(S.ctime + x) >= t) break;
-    const int st = __ldcg(S.status + x);
+    const longlong2 kl = node_keylen_cg(S.node, x);  // one sector: both halves issued together
+    const int4 w = node_words_cg(S.node, x);
+    if ((unsigned long long)kl.x >= t) break;
+    const int st = w.x;
     if (status_kind(st) == kPending || (st >> 2) > round) {  // undecided, or decided in this round
       done = false;
       break;
     }
     if (status_kind(st) == kRootForever) break;
-    a += __ldcg(S.wlen + x);
-    x = __ldcg(S.parent + x);
+    a += kl.y;
+    x = w.y;
     if (++steps > max_steps) {
       set_status(status, kStatusChainCap);
       break;
@@ -257,10 +290,11 @@ __device__ __forceinline__ void seg_step(const EmitCtx& E, SegCursor& c) {
 // Expands W(d): queues its two chains at slot p and its two raw-arc segments
 // at base slot pb, advancing both.
 __device__ __forceinline__ void emit_w(const EmitCtx& E, int d, int rev, long long pos, int& p, int& pb) {
-  int k = side_of(E.S.side[d]), o = 1 - k, s = E.S.csad[d];
+  const int4 nw = node_words(E.S.node, d);
+  int k = side_of(nw.z), o = 1 - k, s = nw.w;
   int Tk = E.t[2 * s + k], To = E.t[2 * s + o];
   long long la = E.S.cl_dy[d], lb = E.blen[2 * s + k], lc = E.blen[2 * s + o], ld = E.S.cl_ot[d];
-  int R = E.S.parent[d];
+  int R = nw.y;
   if (!rev) {
     // reverse(chain(Tk -> d)) + reverse(arc k) + arc o + chain(To -> R)
     if (la > 0) E.q_out[p++] = make_task(kTaskChain, 1, Tk, d, pos);
@@ -291,11 +325,12 @@ __device__ __forceinline__ bool chain_expand_counts(const EmitCtx& E, int x, int
   *n_base = 0;
   *total = 0;
   while (z != stop && z >= 0) {
-    tot += E.S.wlen[z];
-    const int w = E.S.side[z];  // counts stored at link time
-    nc += chains_of(w);
-    nb += bases_of(w);
-    z = E.S.parent[z];
+    const longlong2 kl = node_keylen(E.S.node, z);
+    const int4 w = node_words(E.S.node, z);
+    tot += kl.y;
+    nc += chains_of(w.z);  // counts stored at link time
+    nb += bases_of(w.z);
+    z = w.y;
     if (++k > E.max_steps) {
       set_status(E.status, kStatusChainCap);
       return false;
@@ -312,9 +347,9 @@ __device__ void chain_expand(const EmitCtx& E, int x, int stop, int rev, long lo
                              int pb) {
   long long off = 0;
   int k = 0;
-  for (int z = x; z != stop && z >= 0; z = E.S.parent[z]) {
+  for (int z = x; z != stop && z >= 0; z = E.S.node[z].parent) {
     if (++k > E.max_steps) break;
-    const long long w = E.S.wlen[z];
+    const long long w = E.S.node[z].wlen;
     emit_w(E, z, rev, rev ? pos + total - off - w : pos + off, p, pb);
     off += w;
   }
