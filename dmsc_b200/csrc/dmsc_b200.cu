@@ -37,7 +37,7 @@ namespace {
 
 enum Slot {
   S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
-  S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_MINBITS, S_MAXBITS, S_VMIN, S_VMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
+  S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_MINBITS, S_MAXBITS, S_VMIN, S_VMAX, S_KMIN, S_KMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
   S_ASC, S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
   S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX, S_SKEY32, S_SKEY32B,
   S_SIDE0,  // per-side slots start here, kSideSlots each
@@ -45,8 +45,8 @@ enum Slot {
 enum SideSlot {
   X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
   X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_NODE,
-  X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G1,
-  X_G2, X_GBASE, X_LAB, X_WX, X_WA, X_CENDS, kSideSlots
+  X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
+  X_GBASE, X_LAB, X_WX, X_WA, X_CENDS, kSideSlots
 };
 
 struct Buf {
@@ -74,6 +74,7 @@ struct Side {
   int* crit = nullptr;
   int* ext_img = nullptr;
   float* val = nullptr;
+  const int2* key = nullptr;  // (value bits, cell) per extremum
   int* t = nullptr;
   int* steps = nullptr;
   int* sweep = nullptr;
@@ -432,8 +433,7 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
   A.M = M;
   A.c1 = S.c1;
   A.c2 = S.c2;
-  A.g1 = sget<int>(ctx, si, X_G1, nsad);
-  A.g2 = sget<int>(ctx, si, X_G2, nsad);
+  A.g12 = sget<int2>(ctx, si, X_G12, nsad);
   A.dying = S.dying;
   A.link = sget<int>(ctx, si, X_LINK, M + 1);
   A.minedge = sget<unsigned>(ctx, si, X_MINE, M + 1);
@@ -442,8 +442,7 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
   A.roots0 = sget<int>(ctx, si, X_GRP, M + 1);
   A.roots1 = sget<int>(ctx, si, X_UF, M + 1);
   A.cnt = sget<int>(ctx, si, X_CNT, 8);
-  A.val = S.val;
-  A.cell = S.crit;
+  A.key = S.key;
   A.ext_img = S.ext_img;
   A.dual = ctx->I.dual;
   A.faces = S.faces;
@@ -721,6 +720,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   uint32_t* bmax = get<uint32_t>(ctx, S_MAXBITS, nseg);
   float* vmin = get<float>(ctx, S_VMIN, nmin);
   float* vmax = get<float>(ctx, S_VMAX, nmax);
+  int2* kmin = get<int2>(ctx, S_KMIN, nmin);  // (value bits, cell) records for the pairing
+  int2* kmax = get<int2>(ctx, S_KMAX, nmax);
   float* sval = get<float>(ctx, S_SVAL, nsad);
   // sort keys: (image id << 32) | orderable(s_val), or the 32-bit value key alone for one image
   unsigned long long* skey = B > 1 ? get<unsigned long long>(ctx, S_SKEY, nsad) : nullptr;
@@ -728,7 +729,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   ctx->crit_sad = csad;
   ctx->sad_img = isad;
   LK(compact_kernel<<<grid_for(nseg, 8), 256, 0, st>>>(I, img, nseg, mask, off[0], off[1], off[2], cmin, csad, cmax,
-                                                       imin, isad, imax, bmin, bmax, vmin, vmax, sval, skey, skey32));
+                                                       imin, isad, imax, bmin, bmax, vmin, vmax, kmin, kmax, sval, skey,
+                                                       skey32));
   LAUNCH_CHECK("compact_kernel");
   // per-image bases of the critical lists (B + 1 entries each)
   int* bases = get<int>(ctx, S_BASES, 9 * (size_t)(B + 1));
@@ -787,6 +789,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   V.ext_img = imin;
   F.val = vmax;
   V.val = vmin;
+  F.key = kmax;
+  V.key = kmin;
   F.t = tf;
   F.steps = lf;
   V.t = tv;

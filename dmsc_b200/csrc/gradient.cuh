@@ -460,7 +460,8 @@ __device__ __forceinline__ float cell_value_g(const float* __restrict__ img, int
 // contiguous slice in ascending cell-id order. Writes the three lists as
 // global cell ids, each critical cell's image, the per-segment bit masks of
 // the minima and maxima (an extremum's list rank is its segment's offset plus
-// the extrema before it in the mask), the extremum values and the saddle
+// the extrema before it in the mask), the extremum values (also as (value,
+// cell) records for the elder comparisons of the pairing) and the saddle
 // values with their sort keys (image id above the orderable value, so one
 // sort orders every image).
 static __global__ void __launch_bounds__(256) compact_kernel(
@@ -469,7 +470,8 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     int* __restrict__ crit_min, int* __restrict__ crit_sad, int* __restrict__ crit_max, int* __restrict__ min_img,
     int* __restrict__ sad_img, int* __restrict__ max_img, uint32_t* __restrict__ min_bits,
     uint32_t* __restrict__ max_bits,
-    float* __restrict__ min_val, float* __restrict__ max_val, float* __restrict__ sad_val,
+    float* __restrict__ min_val, float* __restrict__ max_val, int2* __restrict__ min_key, int2* __restrict__ max_key,
+    float* __restrict__ sad_val,
     unsigned long long* __restrict__ sad_key, uint32_t* __restrict__ sad_key32) {
   const int lane = threadIdx.x & 31;
   long long seg = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -504,13 +506,17 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     int p = off_min[seg] + __popc(bmin & lt);
     crit_min[p] = (int)(4 * gidx);
     min_img[p] = b;
-    min_val[p] = __ldg(img + (size_t)iy * W + ix);
+    const float v = __ldg(img + (size_t)iy * W + ix);
+    min_val[p] = v;
+    min_key[p] = make_int2(__float_as_int(v), (int)(4 * gidx));
   }
   if (m & 8u) {
     int p = off_max[seg] + __popc(bmax & lt);
     crit_max[p] = (int)(4 * gidx + 3);
     max_img[p] = b;
-    max_val[p] = dual ? cell_value_g<true>(img, 3, iy, ix, H, W) : cell_value_g<false>(img, 3, iy, ix, H, W);
+    const float v = dual ? cell_value_g<true>(img, 3, iy, ix, H, W) : cell_value_g<false>(img, 3, iy, ix, H, W);
+    max_val[p] = v;
+    max_key[p] = make_int2(__float_as_int(v), (int)(4 * gidx + 3));
   }
   int p = off_sad[seg] + excl;
 #pragma unroll

@@ -35,11 +35,13 @@ constexpr int kUndecided = -2;
 // older(a, b) for extremum dense indices of one image; `void_id` is older
 // than all. Older = smaller (value, cell) under value_less on the vertex side
 // in the primal and the face side in the dual, larger otherwise.
-__device__ __forceinline__ bool older(int a, int b, int void_id, const float* __restrict__ val,
-                                      const int* __restrict__ cell, bool older_less) {
+// `key[x]` = (value bits, cell) of extremum x, one 8-byte record per extremum.
+__device__ __forceinline__ bool older(int a, int b, int void_id, const int2* __restrict__ key, bool older_less) {
   if (a == void_id) return b != void_id;
   if (b == void_id) return false;
-  return older_less ? tie_lt(val[a], cell[a], val[b], cell[b]) : tie_lt(val[b], cell[b], val[a], cell[a]);
+  const int2 ka = key[a], kb = key[b];
+  const float va = __int_as_float(ka.x), vb = __int_as_float(kb.x);
+  return older_less ? tie_lt(va, ka.y, vb, kb.y) : tie_lt(vb, kb.y, va, ka.y);
 }
 
 __global__ void iota_kernel(int* __restrict__ a, int n) {

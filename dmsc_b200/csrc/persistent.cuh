@@ -92,8 +92,7 @@ struct PairArgs {
   int nsad, M;  // void group = M
   const int* c1;
   const int* c2;
-  int* g1;            // [nsad] group of each end, as of the saddle's last active round
-  int* g2;
+  int2* g12;          // [nsad] groups of the two ends, as of the saddle's last active round
   int* dying;
   int* link;          // [M+1] group union-find
   unsigned* minedge;  // [M+1]
@@ -102,8 +101,7 @@ struct PairArgs {
   int* roots0;        // live group roots (ping-pong), [M+1] each
   int* roots1;
   int* cnt;           // [0..2] rotating active counts, [3..5] rotating root counts
-  const float* val;
-  const int* cell;
+  const int2* key;       // [M] (value bits, cell) of each extremum
   const int* ext_img;    // [M] image of each extremum
   const uint8_t* dual;   // [B] orientation of each image
   bool faces;            // face side (maxima in the primal) or vertex side
@@ -142,14 +140,14 @@ __device__ __forceinline__ void pair_phase_a(const PairArgs& A, int r, long long
       ga = a < 0 ? M : a;
       gb = b < 0 ? M : b;
     } else {  // the ends' groups of the previous round, followed to their roots
-      ga = find_halving(A.link, A.g1[e]);
-      gb = find_halving(A.link, A.g2[e]);
+      const int2 g = A.g12[e];
+      ga = find_halving(A.link, g.x);
+      gb = find_halving(A.link, g.y);
     }
     if (ga == gb) {
       A.dying[e] = -1;
     } else {
-      A.g1[e] = ga;
-      A.g2[e] = gb;
+      A.g12[e] = make_int2(ga, gb);
       atomicMin(A.minedge + ga, (unsigned)e);  // result unused: a reduction
       atomicMin(A.minedge + gb, (unsigned)e);
       keep = true;
@@ -169,12 +167,13 @@ __device__ __forceinline__ void pair_phase_b1(const PairArgs& A, int r, long lon
   if (me != kNoEdge) {
     A.minedge[g] = kNoEdge;
     int e = (int)me;
-    int ga = A.g1[e], gb = A.g2[e];  // roots as of phase A
+    const int2 gg = A.g12[e];  // roots as of phase A
+    const int ga = gg.x, gb = gg.y;
     h = (ga == g) ? gb : ga;
     // g is an extremum of one image (the void never dies); older = value_less
     // order on the vertex side in the primal and the face side in the dual
     const bool du = g < M && A.dual[A.ext_img[g]];
-    if (older(h, g, M, A.val, A.cell, A.faces ? du : !du)) {
+    if (older(h, g, M, A.key, A.faces ? du : !du)) {
       A.dying[e] = g;
       A.link[g] = h;
     } else {
