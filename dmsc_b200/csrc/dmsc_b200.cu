@@ -45,7 +45,7 @@ enum Slot {
 enum SideSlot {
   X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
   X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_NODE,
-  X_CLDY, X_CLOT, X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
+  X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
   X_GBASE, X_LAB, X_WX, X_WA, X_CENDS, kSideSlots
 };
 
@@ -518,8 +518,6 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
 
   ReplayState& R = S.R;
   R.node = sget<ReplayNode>(ctx, si, X_NODE, M + 1);
-  R.cl_dy = sget<long long>(ctx, si, X_CLDY, M + 1);
-  R.cl_ot = sget<long long>(ctx, si, X_CLOT, M + 1);
   LK(replay_node_init_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.node, M + 1));
   LAUNCH_CHECK("replay init");
   ReplayArgs A{};

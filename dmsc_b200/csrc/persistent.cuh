@@ -334,8 +334,7 @@ __device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r, int roun
     k = 1;
   if (k >= 0) {
     const long long b0 = A.blen[2 * s], b1 = A.blen[2 * s + 1];
-    A.S.cl_dy[d] = k == 0 ? a0 : a1;
-    A.S.cl_ot[d] = k == 0 ? a1 : a0;
+    *reinterpret_cast<longlong2*>(&A.S.node[d].cl_dy) = make_longlong2(k == 0 ? a0 : a1, k == 0 ? a1 : a0);
     A.S.node[d].wlen = b0 + b1 + a0 + a1;
     // status, parent, the dying side with what W(d) expands to (its non-empty
     // chains and raw-arc segments), and the saddle, in one store: no walk of

@@ -42,21 +42,23 @@ enum : int { kPending = 0, kLinked = 1, kRootForever = 2 };
 __device__ __forceinline__ int status_kind(int st) { return st & 3; }
 __device__ __forceinline__ int status_word(int kind, int round) { return kind | ((round + 1) << 2); }
 
-// Everything a chain walk reads at one node, in one 32-byte sector, as two
-// 16-byte halves: (ctime, wlen) and (status, parent, side, csad).
-struct alignas(32) ReplayNode {
+// A replay node in one 64-byte line: everything a chain walk reads, in the
+// first 32-byte sector as two 16-byte halves, (ctime, wlen) and (status,
+// parent, side, csad); the two chain lengths the emission adds in the second.
+struct alignas(64) ReplayNode {
   unsigned long long ctime;  // replay key of the cancellation killing the node, kNever if none
   long long wlen;            // length of W(node)
   int status;                // kPending / kLinked / kRootForever, with the deciding round's tag
   int parent;                // link target (-1 = void) when kLinked
   int side;                  // side_word: dying side of the node's cancellation and what W(node) expands to
   int csad;                  // saddle of the node's cancellation
+  long long cl_dy;           // chain length T_dying -> node at link time
+  long long cl_ot;           // chain length T_other -> parent at link time
+  long long pad[2];
 };
 
 struct ReplayState {
   ReplayNode* node;  // [M + 1]
-  long long* cl_dy;  // [M] chain length T_dying -> node at link time
-  long long* cl_ot;  // [M] chain length T_other -> parent at link time
 };
 
 // The halves of a node's record: through L2 inside the replay (other blocks
@@ -293,7 +295,8 @@ __device__ __forceinline__ void emit_w(const EmitCtx& E, int d, int rev, long lo
   const int4 nw = node_words(E.S.node, d);
   int k = side_of(nw.z), o = 1 - k, s = nw.w;
   int Tk = E.t[2 * s + k], To = E.t[2 * s + o];
-  long long la = E.S.cl_dy[d], lb = E.blen[2 * s + k], lc = E.blen[2 * s + o], ld = E.S.cl_ot[d];
+  const longlong2 cl = *reinterpret_cast<const longlong2*>(&E.S.node[d].cl_dy);
+  long long la = cl.x, lb = E.blen[2 * s + k], lc = E.blen[2 * s + o], ld = cl.y;
   int R = nw.y;
   if (!rev) {
     // reverse(chain(Tk -> d)) + reverse(arc k) + arc o + chain(To -> R)
