@@ -337,8 +337,9 @@ __device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r, int roun
     *reinterpret_cast<longlong2*>(&A.S.node[d].cl_dy) = make_longlong2(k == 0 ? a0 : a1, k == 0 ? a1 : a0);
     A.S.node[d].wlen = b0 + b1 + a0 + a1;
     // status, parent, the dying side with what W(d) expands to (its non-empty
-    // chains and raw-arc segments), and the saddle, in one store: no walk of
-    // this round reads a record whose status carries this round's tag
+    // chains and raw-arc segments), and the saddle, in one store; a walk of
+    // this round uses no field of a record whose status carries this round's
+    // tag, so the order of these stores does not matter
     *reinterpret_cast<int4*>(&A.S.node[d].status) =
         make_int4(status_word(kLinked, round), k == 0 ? R1 : R0,
                   side_word(k, (a0 > 0) + (a1 > 0), (b0 > 0) + (b1 > 0)), s);
