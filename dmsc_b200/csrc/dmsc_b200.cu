@@ -443,7 +443,8 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
   A.roots1 = sget<int>(ctx, si, X_UF, M + 1);
   A.cnt = sget<int>(ctx, si, X_CNT, 8);
   A.key = S.key;
-  A.ext_img = S.ext_img;
+  A.idx_base = ctx->I.idx_base;
+  A.B = ctx->B;
   A.dual = ctx->I.dual;
   A.faces = S.faces;
   A.status = ctx->status;

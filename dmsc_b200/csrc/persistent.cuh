@@ -102,7 +102,8 @@ struct PairArgs {
   int* roots1;
   int* cnt;           // [0..2] rotating active counts, [3..5] rotating root counts
   const int2* key;       // [M] (value bits, cell) of each extremum
-  const int* ext_img;    // [M] image of each extremum
+  const int* idx_base;   // [B + 1] first global index of each image
+  int B;
   const uint8_t* dual;   // [B] orientation of each image
   bool faces;            // face side (maxima in the primal) or vertex side
   unsigned* status;
@@ -172,7 +173,8 @@ __device__ __forceinline__ void pair_phase_b1(const PairArgs& A, int r, long lon
     h = (ga == g) ? gb : ga;
     // g is an extremum of one image (the void never dies); older = value_less
     // order on the vertex side in the primal and the face side in the dual
-    const bool du = g < M && A.dual[A.ext_img[g]];
+    // (its image from its cell, in the record the comparison reads anyway)
+    const bool du = g < M && A.dual[find_image(A.idx_base, A.B, A.key[g].y >> 2)];
     if (older(h, g, M, A.key, A.faces ? du : !du)) {
       A.dying[e] = g;
       A.link[g] = h;
