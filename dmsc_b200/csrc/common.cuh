@@ -71,15 +71,6 @@ __device__ __forceinline__ int flow_step(unsigned code, int Nx) {
   return code == kFlowLeft ? -1 : code == kFlowRight ? 1 : code == kFlowUp ? -Nx : Nx;
 }
 
-// Vertex code of the vertex at index `idx` paired with edge cell `e`
-// (e = -1: none): the other end of the edge (cpu/arcs_topology.hxx:41-65).
-__device__ __forceinline__ unsigned vertex_flow(int e, int idx) {
-  if (e < 0) return kFlowNone;
-  int eidx = e >> 2;
-  if ((e & 3) == 1) return eidx == idx ? kFlowLeft : kFlowRight;  // H(y,x): (y,x-1); H(y,x+1): (y,x+1)
-  return eidx == idx ? kFlowUp : kFlowDown;                        // V(y,x): (y-1,x); V(y+1,x): (y+1,x)
-}
-
 // Face code of the face at index `idx` paired with edge cell `e`: the other
 // coface of the edge (cpu/arcs_topology.hxx:19-39).
 __device__ __forceinline__ unsigned face_flow(int e, int idx) {
@@ -87,31 +78,6 @@ __device__ __forceinline__ unsigned face_flow(int e, int idx) {
   int eidx = e >> 2;
   if ((e & 3) == 1) return eidx == idx ? kFlowDown : kFlowUp;  // H(fy,fx) -> F(fy+1,fx); H(fy-1,fx) -> F(fy-1,fx)
   return eidx == idx ? kFlowRight : kFlowLeft;                 // V(fy,fx) -> F(fy,fx+1); V(fy,fx-1) -> F(fy,fx-1)
-}
-
-// Successor of a face along its V-path: the other face of its paired edge
-// (cpu/arcs_topology.hxx:19-39). Both cofaces of an edge are always valid.
-__device__ __forceinline__ int next_face(int e, int curr, int Nx) {
-  int idx = e >> 2, t = e & 3;
-  int f1 = 3 + 4 * idx;
-  int f2 = (t == 1) ? 3 + 4 * (idx + Nx) : 3 + 4 * (idx + 1);
-  return (f1 == curr) ? f2 : f1;
-}
-
-// Successor of a vertex: the other vertex of its paired edge, or -1 off the
-// image (cpu/arcs_topology.hxx:41-65).
-__device__ __forceinline__ int next_vertex(int e, int curr, int H, int W, int Nx) {
-  int idx = e >> 2, t = e & 3;
-  int ey = idx / Nx, ex = idx - ey * Nx;
-  int v1 = -1, v2 = -1;
-  if (t == 1) {
-    if (ex - 1 >= 0) v1 = 4 * (idx - 1);
-    if (ex < W) v2 = 4 * idx;
-  } else {
-    if (ey - 1 >= 0) v1 = 4 * (idx - Nx);
-    if (ey < H) v2 = 4 * idx;
-  }
-  return (v1 == curr) ? v2 : v1;
 }
 
 // a - b with the NaN results of the x86 SSE subtraction the reference CPU
@@ -159,41 +125,12 @@ __device__ __forceinline__ int find_image(const int* __restrict__ base, int B, l
   return lo;
 }
 
-// Block-aggregated reservation of `cnt` consecutive slots per thread: one
-// global atomic per block, the warp totals scanned by warp 0. Every thread of
-// the block must call it (blockDim.x a multiple of 32, at most 1024). Returns
-// this thread's first slot.
-__device__ __forceinline__ int block_reserve(int* counter, int cnt) {
-  __shared__ int wsum[32], bbase_r;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  int x = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) wsum[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    const int s = lane < nw ? wsum[lane] : 0;
-    int incl = s;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    if (lane < nw) wsum[lane] = incl - s;
-    if (lane == 31) bbase_r = incl ? atomicAdd(counter, incl) : 0;  // block total
-  }
-  __syncthreads();
-  const int r = bbase_r + wsum[warp] + x - cnt;
-  __syncthreads();
-  return r;
-}
-
-// The same on two counters at once (n0 slots on c0 and n1 on c1 per thread),
-// with one set of barriers for both. A counter that receives no slots from
-// the block is not touched. p0 and p1 receive this thread's first slots.
+// Block-aggregated reservation of consecutive slots on two counters at once
+// (n0 slots on c0 and n1 on c1 per thread): one global atomic per counter and
+// block, the warp totals scanned by warp 0, one set of barriers for both. A
+// counter that receives no slots from the block is not touched. Every thread
+// of the block must call it (blockDim.x a multiple of 32, at most 1024). p0
+// and p1 receive this thread's first slots.
 __device__ __forceinline__ void block_reserve2(int* c0, int n0, int* c1, int n1, int& p0, int& p1) {
   __shared__ int wsum2[2][32], bbase2[2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;

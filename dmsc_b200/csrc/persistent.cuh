@@ -37,14 +37,6 @@ __device__ __forceinline__ int find_halving(int* link, int x) {
   }
 }
 
-__device__ __forceinline__ int warp_append(int* counter, bool take) {
-  unsigned b = __ballot_sync(0xffffffffu, take);
-  if (b == 0) return -1;
-  int lane = threadIdx.x & 31, leader = __ffs(b) - 1, base = 0;
-  if (lane == leader) base = atomicAdd(counter, __popc(b));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  return take ? base + __popc(b & ((1u << lane) - 1u)) : -1;
-}
 
 
 // Chunked processing with two output lists: each block takes contiguous
