@@ -15,7 +15,8 @@ N independent replicas (one field each, weak scaling), timed as the max over
 ranks.
 
 ``--impl reference`` times the reference's own CPU path (compiled from the
-reference sources into oracle/_ref, all host threads) on the same workload.
+reference sources into oracle/_ref/ordered with an order-preserving parallel
+TBB stand-in, all host threads) on the same workload.
 """
 
 from __future__ import annotations
@@ -109,23 +110,40 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # reference CPU path (oracle/_ref) -- checker and CPU baseline only
 # ---------------------------------------------------------------------------
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def load_reference():
-    ref_dir = os.path.join(ROOT, "oracle", "_ref")
-    if os.path.exists(os.path.join(ref_dir, "dmsc_cpu.so")):
-        sys.path.insert(0, ref_dir)
-        import dmsc_cpu
+    """The reference CPU path compiled from its sources: the build with the
+    order-preserving parallel TBB stand-in (oracle/_ref/ordered, all threads,
+    bit-identical to the single-thread order) when present, else the serial
+    stand-in build (oracle/_ref), else the C restatement (oracle/). Returns
+    (kind, shim, run)."""
+    for sub, shim in (("ordered", "ordered parallel TBB stand-in"), ("", "serial TBB stand-in")):
+        ref_dir = os.path.join(ROOT, "oracle", "_ref", sub) if sub else os.path.join(ROOT, "oracle", "_ref")
+        if os.path.exists(os.path.join(ref_dir, "dmsc_cpu.so")):
+            sys.path.insert(0, ref_dir)
+            import dmsc_cpu
 
-        def run(img, thr, dual):
-            r = dmsc_cpu.extract_dmsc(img, thr, True, dual, True, True, True, True)
-            return [r[i] for i in range(19)]
+            def run(img, thr, dual, geometry=True):
+                r = dmsc_cpu.extract_dmsc(img, thr, True, dual, geometry, geometry, True, True)
+                return [r[i] for i in range(19)]
 
-        return "reference", run
+            return "reference", shim, run
     from oracle import oracle
 
-    def run(img, thr, dual):
-        return list(oracle.run(img, thr, True, dual, True, True, True, True))
+    def run(img, thr, dual, geometry=True):
+        return list(oracle.run(img, thr, True, dual, geometry, geometry, True, True))
 
-    return "port", run
+    return "port", "C restatement, one thread", run
 
 
 def same_outputs(a, b):
@@ -141,31 +159,39 @@ def same_outputs(a, b):
     return True
 
 
-def cpu_baseline(img_cpu, gpu_outputs, budget_s=30.0):
-    """Reference CPU path on the same field (bounded sample), all host threads."""
-    kind, run = load_reference()
+def cpu_baseline(img_cpu, gpu_outputs):
+    """Reference CPU path on the same field: the four variants with all host
+    threads (timed, each checked bit for bit against the GPU's outputs of the
+    same variant) and one variant with one thread."""
+    kind, shim, run = load_reference()
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
     pix, t_tot, exact, done = 0, 0.0, True, []
-    for k, (dual, thr) in enumerate([VARIANTS[1], VARIANTS[2]]):
+    for dual, thr in VARIANTS:
         t0 = time.perf_counter()
         out = run(img_cpu, thr, dual)
         t_tot += time.perf_counter() - t0
         pix += img_cpu.numel()
         done.append(f"is_dual={dual},thr={thr}")
         g = gpu_outputs.get((dual, thr))
-        if g is not None:
-            exact = exact and same_outputs(g, out)
-        if t_tot > budget_s:
-            break
+        exact = exact and g is not None and same_outputs(g, out)
+    torch.set_num_threads(1)
+    t0 = time.perf_counter()
+    run(img_cpu, VARIANTS[1][1], VARIANTS[1][0])
+    t1 = time.perf_counter() - t0
+    torch.set_num_threads(threads)
     return {
         "value": pix / 1e6 / t_tot,
         "unit": UNIT,
         "cores": threads,
         "kind": kind,
+        "shim": shim,
+        "cpu_model": cpu_model(),
         "sample": f"{len(done)} full compute_dmsc calls on the same {img_cpu.shape[0]}x{img_cpu.shape[1]} field "
                   f"({'; '.join(done)}), torch threads={threads}",
         "seconds": t_tot,
+        "one_thread": {"value": img_cpu.numel() / 1e6 / t1, "unit": UNIT, "seconds": t1,
+                       "sample": f"one call (is_dual={VARIANTS[1][0]},thr={VARIANTS[1][1]}), torch threads=1"},
     }, exact
 
 
@@ -176,7 +202,7 @@ def reference_arm(args):
     from dmsc_b200.synthetic import field_4096_bumps
 
     size = args.size
-    kind, run = load_reference()
+    kind, shim, run = load_reference()
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
     img = field_4096_bumps(seed=SEED, size=size)
@@ -209,7 +235,8 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/i32",
         "data": "synthetic", "config": workload_config(size),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample_desc},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "shim": shim,
+                         "cpu_model": cpu_model(), "sample": sample_desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     })
 

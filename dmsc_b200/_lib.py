@@ -33,6 +33,8 @@ EXPORTS = (
     "dmsc_b200_launch_count",
     "dmsc_b200_loop_counts",
     "dmsc_b200_pairing_timeline",
+    "dmsc_b200_set_loop_caps",
+    "dmsc_b200_set_wait_timeout",
     "dmsc_b200_critical_cells_static",
 )
 
@@ -110,6 +112,10 @@ def load():
         lib.dmsc_b200_loop_counts.restype = ctypes.c_int
         lib.dmsc_b200_pairing_timeline.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
         lib.dmsc_b200_pairing_timeline.restype = ctypes.c_int
+        lib.dmsc_b200_set_loop_caps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.dmsc_b200_set_loop_caps.restype = ctypes.c_int
+        lib.dmsc_b200_set_wait_timeout.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        lib.dmsc_b200_set_wait_timeout.restype = ctypes.c_int
         lib.dmsc_b200_critical_cells_static.argtypes = [
             ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p,
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
@@ -155,6 +161,14 @@ class Context:
         names = ("pair_rounds_faces", "pair_rounds_vertices", "replay_rounds_faces", "replay_rounds_vertices",
                  "emit_levels_faces", "emit_levels_vertices")
         return {names[k]: int(buf[k]) for k in range(max(n, 0))}
+
+    def set_loop_caps(self, pair_rounds: int = 0, replay_rounds: int = 0, emit_levels: int = 0):
+        """Lowers the device loop bounds of the following calls (0 = normal)."""
+        self.check(self.lib.dmsc_b200_set_loop_caps(self.h, pair_rounds, replay_rounds, emit_levels),
+                   "dmsc_b200_set_loop_caps")
+
+    def set_wait_timeout(self, seconds: float):
+        self.check(self.lib.dmsc_b200_set_wait_timeout(self.h, float(seconds)), "dmsc_b200_set_wait_timeout")
 
     def timelines(self) -> dict:
         """Per-round / per-level durations (us) of the device loops of the last call."""

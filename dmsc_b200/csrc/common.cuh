@@ -30,6 +30,7 @@ enum : unsigned {
   kStatusChainCap = 4u,     // a replay chain walk exceeded its bound
   kStatusQueueOverflow = 8u,
   kStatusBadIndex = 16u,
+  kStatusFindCap = 32u,     // a union-find root search or union retry loop exceeded its bound
 };
 
 __host__ __device__ __forceinline__ int cell_id(int t, int y, int x, int Nx) { return t + 4 * (y * Nx + x); }

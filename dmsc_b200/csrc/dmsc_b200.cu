@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cub/cub.cuh>
 #include <cstdarg>
 #include <cstdio>
@@ -155,6 +156,11 @@ struct dmsc_b200_context {
   char* rb_h = nullptr;
   char* rb_d = nullptr;
   size_t rb_cap = 0;
+  // host wait deadline (seconds) and test-only loop caps (0 = the bounds
+  // that every input provably stays within)
+  double wait_timeout_s = 600.0;
+  int grad_shape = 1;  // gradient tile shape (index into kGradTY / kGradNT)
+  int cap_pair_rounds = 0, cap_replay_rounds = 0, cap_emit_levels = 0;
 };
 
 
@@ -224,6 +230,12 @@ void ck(dmsc_b200_context* c, cudaError_t e, const char* what) {
     __VA_ARGS__;      \
     ++ctx->launches;  \
   } while (0)
+
+// A loop bound lowered to a test-only cap (cap <= 0: the bound itself).
+int capped(long long bound, int cap) {
+  const long long b = cap > 0 && cap < bound ? cap : bound;
+  return (int)std::min<long long>(b, 2147483647LL);
+}
 
 template <class T>
 T* get(dmsc_b200_context* ctx, int slot, size_t n) {
@@ -310,13 +322,21 @@ void coop_launch(dmsc_b200_context* ctx, void (*kernel)(T), T args, cudaStream_t
 // Waits until the stream has drained by polling an event: the host thread
 // spins instead of sleeping in the driver, so the next launches follow the
 // readback without an operating-system wake-up delay (the few host round
-// trips of a call are on its critical path).
+// trips of a call are on its critical path). Gives up after the context's
+// wait deadline with DMSC_B200_ERR_CUDA; the work may still be running then,
+// so the context must be destroyed, not reused.
 void wait_stream(dmsc_b200_context* ctx, cudaStream_t st) {
   CK(cudaEventRecord(ctx->sync_ev, st));
-  while (true) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (unsigned k = 0;; ++k) {
     const cudaError_t e = cudaEventQuery(ctx->sync_ev);
     if (e == cudaSuccess) return;
     if (e != cudaErrorNotReady) CK(e);
+    if ((k & 15u) == 15u &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > ctx->wait_timeout_s) {
+      set_err(ctx, "device work did not finish within %.1f s", ctx->wait_timeout_s);
+      throw Fail{kErrCuda};
+    }
   }
 }
 
@@ -379,7 +399,7 @@ const long long* rb_ll(dmsc_b200_context* ctx) { return (const long long*)ctx->r
 
 // Error of a device status word (0: none).
 void raise_status(dmsc_b200_context* ctx, unsigned h) {
-  if (h & (kStatusWalkCap | kStatusRoundCap | kStatusChainCap)) {
+  if (h & (kStatusWalkCap | kStatusRoundCap | kStatusChainCap | kStatusFindCap)) {
     set_err(ctx, "a bounded device loop reached its cap (status 0x%x)", h);
     throw Fail{kErrIterationCap};
   }
@@ -448,7 +468,7 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
   A.dual = ctx->I.dual;
   A.faces = S.faces;
   A.status = ctx->status;
-  A.max_rounds = M + 2;
+  A.max_rounds = capped(M + 2, ctx->cap_pair_rounds);
   A.rounds = get<int>(ctx, S_STATS, 8) + 0 + si;
   A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline) + si * kTimeline;
   return A;
@@ -485,8 +505,8 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   S.ut = sget<int>(ctx, si, X_UT, M + 1);
   LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(uf, M + 1));
   if (nsad > 0)
-    LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(cends, ncanc, M, uf));
-  LK(ut_flatten_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, uf));
+    LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(cends, ncanc, M, uf, M + 2, ctx->status));
+  LK(ut_flatten_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, uf, M + 2, ctx->status));
   LK(ut_mark_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M, uf, S.alive, croot));
   if (M > 0) LK(ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.ut));
   LAUNCH_CHECK("thresholded union-find");
@@ -538,7 +558,7 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   A.wx = sget<int>(ctx, si, X_WX, 2 * (size_t)nsad);
   A.wa = sget<long long>(ctx, si, X_WA, 2 * (size_t)nsad);
   A.status = ctx->status;
-  A.max_rounds = nsad + 2;
+  A.max_rounds = capped(nsad + 2, ctx->cap_replay_rounds);
   A.rounds = get<int>(ctx, S_STATS, 8) + 2 + si;
   A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline) + (4 + si) * kTimeline;
   return A;
@@ -561,6 +581,26 @@ void replay_final(dmsc_b200_context* ctx, int si, Side& S, long long* total, cud
   incl_sum(ctx, S.plen, S.send, nsurv, st);
   LK(last_kernel<long long><<<1, 1, 0, st>>>(S.send, nsurv, total));
   LAUNCH_CHECK("final arcs");
+}
+
+// Gradient kernel of tile shape `shape` over `ntile` tiles of the batch.
+void launch_gradient(dmsc_b200_context* ctx, int shape, unsigned ntile, const Imgs& I, const float* img, int4* grad,
+                     uint8_t* mask, int* const* seg, uint8_t* flow, cudaStream_t st) {
+  switch (shape) {
+    case 0:
+      LK((gradient_batch_kernel<kGradTY[0], kGradNT[0]><<<ntile, kGradNT[0], 0, st>>>(I, img, grad, mask, seg[0], seg[1],
+                                                                                      seg[2], ctx->fifo_lut, flow)));
+      break;
+    case 1:
+      LK((gradient_batch_kernel<kGradTY[1], kGradNT[1]><<<ntile, kGradNT[1], 0, st>>>(I, img, grad, mask, seg[0], seg[1],
+                                                                                      seg[2], ctx->fifo_lut, flow)));
+      break;
+    default:
+      LK((gradient_batch_kernel<kGradTY[2], kGradNT[2]><<<ntile, kGradNT[2], 0, st>>>(I, img, grad, mask, seg[0], seg[1],
+                                                                                      seg[2], ctx->fifo_lut, flow)));
+      break;
+  }
+  LAUNCH_CHECK("gradient_batch_kernel");
 }
 
 // Number of bits needed for values 0 .. n-1 (at least 1).
@@ -600,6 +640,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   int* peaks_off = seg_base + (B + 1);
   int* basins_off = peaks_off + (B + 1);
   int* ltile_base = basins_off + (B + 1);
+  const int gshape = ctx->grad_shape;
+  const int gTY = kGradTY[gshape];
   long long nidx = 0, npx = 0, ntile = 0, nseg = 0, npk = 0, nbs = 0, nltile = 0;
   bool any_primal = false, any_dual = false;
   for (int b = 0; b < B; ++b) {
@@ -622,7 +664,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     basins_off[b] = (int)nbs;
     ltile_base[b] = (int)nltile;
     nltile += ((W + kLT) / kLT) * ((H + kLT) / kLT);
-    const long long ntx = (W + 1 + kTileX - 1) / kTileX, nty = (H + 1 + kTileY - 1) / kTileY;
+    const long long ntx = (W + 1 + kTileX - 1) / kTileX, nty = (H + 1 + gTY - 1) / gTY;
     nidx += (H + 1) * (W + 1);
     npx += H * W;
     ntile += ntx * nty;
@@ -693,9 +735,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   ctx->img = img;
   int* seg[3] = {get<int>(ctx, S_SEG0, nseg), get<int>(ctx, S_SEG1, nseg), get<int>(ctx, S_SEG2, nseg)};
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
-  LK(gradient_batch_kernel<<<(unsigned)ntile, kGradThreads, 0, st>>>(I, img, (int4*)grad, mask, seg[0], seg[1], seg[2],
-                                                                     ctx->fifo_lut, flow));
-  LAUNCH_CHECK("gradient_batch_kernel");
+  launch_gradient(ctx, gshape, (unsigned)ntile, I, img, (int4*)grad, mask, seg, flow, st);
   mark(ctx, 1, st);
   if (ret_grad) copy_out_async(ctx, ctx->host_grad, grad, 16 * (size_t)nidx, st);
   for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);
@@ -829,7 +869,13 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     LK(last_plus_kernel<int><<<1, 1, 0, st>>>(fpos, flag, nsad, tot));
     LK(copy2_kernel<<<1, 1, 0, st>>>(get<int>(ctx, S_NCANC, 4), tot + 1));
     LAUNCH_CHECK("survivors");
-    readback(ctx, st, tot, 3);
+    // the status word rides along: a capped pairing or union-find loop ends
+    // the call here, before the replay
+    rb_reserve(ctx, 4 * sizeof(long long));
+    rb_copy(ctx, st, 0, tot, 3 * sizeof(long long));
+    rb_copy(ctx, st, 3 * sizeof(long long), ctx->status, sizeof(unsigned));
+    wait_stream(ctx, st);
+    raise_status(ctx, *(const unsigned*)(ctx->rb_h + 3 * sizeof(long long)));
     ctx->nsurv = (int)rb_ll(ctx)[0];
     F.C = (int)rb_ll(ctx)[1];
     V.C = (int)rb_ll(ctx)[2];
@@ -1050,7 +1096,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   E.base_q = sget<int4>(ctx, si, X_QB, cap);
   E.base_cap = cap;
   E.n_base = nullptr;
-  A.max_levels = ctx->nsad + 4;
+  A.max_levels = capped(ctx->nsad + 4, ctx->cap_emit_levels);
   A.levels = get<int>(ctx, S_STATS, 8) + 4 + si;
   A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline) + (2 + si) * kTimeline;
   coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel");
@@ -1255,24 +1301,20 @@ int dmsc_b200_create(dmsc_b200_context** out, int device) {
   if (cudaEventCreateWithFlags(&c->sync_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking) != cudaSuccess) {
-    if (c->sync_ev) cudaEventDestroy(c->sync_ev);
-  if (c->copy_st) {
-    cudaStreamSynchronize(c->copy_st);
-    cudaStreamDestroy(c->copy_st);
-  }
-  if (c->copy_ev) cudaEventDestroy(c->copy_ev);
-    cudaFreeHost(c->pinned);
-    delete c;
+    dmsc_b200_destroy(c);
     return kErrCuda;
   }
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
   {
     std::vector<uint32_t> lut(kFifoTable);
     face_fifo_table(lut.data());
+    // the copy from pageable memory may return before the table has reached
+    // the device and orders only the legacy default stream: wait for it once
+    // here, so calls on any (non-blocking) stream see the whole table
     if (cudaMalloc(&c->fifo_lut, kFifoTable * sizeof(uint32_t)) != cudaSuccess ||
-        cudaMemcpy(c->fifo_lut, lut.data(), kFifoTable * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
-      cudaFreeHost(c->pinned);
-      delete c;
+        cudaMemcpy(c->fifo_lut, lut.data(), kFifoTable * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaDeviceSynchronize() != cudaSuccess) {
+      dmsc_b200_destroy(c);
       return kErrCuda;
     }
   }
@@ -1290,6 +1332,11 @@ void dmsc_b200_destroy(dmsc_b200_context* c) {
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->rb_h) cudaFreeHost(c->rb_h);
   if (c->sync_ev) cudaEventDestroy(c->sync_ev);
+  if (c->copy_st) {
+    cudaStreamSynchronize(c->copy_st);
+    cudaStreamDestroy(c->copy_st);
+  }
+  if (c->copy_ev) cudaEventDestroy(c->copy_ev);
   for (int k = 0; k < kStageMarks; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   delete c;
@@ -1434,6 +1481,20 @@ int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n) {
     return -1;
   for (int k = 0; k < 6 && k < n; ++k) out[k] = h[k];
   return 6;
+}
+
+int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_rounds, int emit_levels) {
+  if (!ctx || pair_rounds < 0 || replay_rounds < 0 || emit_levels < 0) return kErrInvalidArgument;
+  ctx->cap_pair_rounds = pair_rounds;
+  ctx->cap_replay_rounds = replay_rounds;
+  ctx->cap_emit_levels = emit_levels;
+  return kOk;
+}
+
+int dmsc_b200_set_wait_timeout(dmsc_b200_context* ctx, double seconds) {
+  if (!ctx || !(seconds > 0.0)) return kErrInvalidArgument;
+  ctx->wait_timeout_s = seconds;
+  return kOk;
 }
 
 }  // extern "C"

@@ -7,29 +7,33 @@
 //
 // Layout. The gradient array holds 4 int32 slots per index (y, x) of the
 // (H+1) x (W+1) index grid, i.e. 16 bytes per index; it is the grad_indices
-// output. One CTA owns a 32 x 64 tile of indices and writes it with one int4
-// store per index, so every warp writes 512 contiguous bytes per row. The
-// cells at a tile's indices are owned (have their highest vertex) in the
-// pixels of the tile plus one halo row above and one halo column to the left,
-// so the CTA evaluates the lower star of (64+1) x (32+1) pixels from a (64+3) x (32+3)
-// value tile in shared memory, one 32-bit pairing word per pixel, and every
-// index then gathers its four slots from the words of their owners. Slots of
+// output. One CTA owns a 32-column x TY-row tile of indices and writes it with
+// one int4 store per index, so every warp writes 512 contiguous bytes per row.
+// The cells at a tile's indices have their highest vertex in the tile's
+// pixels or in one halo row above / one halo column to the left, so the CTA
+// stages a (TY + 3) x 35 value window in shared memory and evaluates
+// (TY + 1) x 33 lower stars, one 32-bit pairing word per pixel:
+//   * the 32 main columns with one lane per column, each warp sliding down a
+//     run of consecutive rows with the 3 x 3 neighbourhood in registers
+//     (three new shared loads per pixel);
+//   * the halo column with one lane per row (32 lower stars per pass), so it
+//     costs 1/32 of a pass per row instead of a second pass.
+// Every index then gathers its four slots from the words of the pixels that
+// own them: (iy, ix), (iy, ix-1), (iy-1, ix) and (iy-1, ix-1). Slots of
 // invalid cells are -1.
 //
 // The same pass writes one criticality byte per index (bit t = slot t is an
-// unpaired valid cell) and per-(row, 32-column segment) counts of minima,
-// saddles and maxima; a scan over the segments in row-major order gives every
-// critical cell its position in the ascending-cell-id lists.
+// unpaired valid cell), the flow codes (common.cuh) and per-(row, 32-column
+// segment) counts of minima, saddles and maxima; a scan over the segments in
+// row-major order gives every critical cell its position in the
+// ascending-cell-id lists.
 #pragma once
 
 #include "common.cuh"
 
 namespace dmsc {
 
-constexpr int kTileX = 32;  // indices per tile row (one warp)
-constexpr int kTileY = 64;  // tile rows
-constexpr int kValX = kTileX + 3;
-constexpr int kValY = kTileY + 3;
+constexpr int kTileX = 32;  // indices per tile row (one warp) and per row segment
 
 // Face-edge pairing FIFO of one lower star (cpu/gradient.hxx:115-191) as a
 // pure function of eL (lower-star edge slots), fL (lower-star face slots) and
@@ -74,325 +78,340 @@ inline uint32_t face_fifo_entry(unsigned eL, unsigned fL, int best) {
   return (fpk << 16) | epk;
 }
 
-// Nibble value of a slot whose cell is not in this pixel's lower star (the
-// cell belongs to a neighbour, or does not exist).
-constexpr unsigned kNotMine = 14u;
-// Word of a pixel outside the image: it owns no cell.
-constexpr uint32_t kNoPixel = 0xEEEEEEEEu;
+// Pairing word of a pixel: 3-bit fields that describe every cell it owns
+// (the cells of its lower star) by the partner of that cell, relative to the
+// cell itself, so an index can combine the fields of its four possible owners
+// with ORs (a cell has exactly one owner; the others hold 0 there):
+//   bits 0-2   vertex: 0 = unpaired (or no pixel), 1..4 = paired with e0..e3,
+//              which is also the vertex's flow code (left, right, up, down);
+//   bits 3-14  edges e0..e3, 3 bits each: 0 = not owned, 1 = unpaired,
+//              2 = paired with its vertex at the lower coordinate (left end
+//              of an H edge, upper end of a V edge), 3 = with its vertex at
+//              the higher coordinate, 4 = with its coface at the lower
+//              coordinate (the face above an H edge, left of a V edge),
+//              5 = with its coface at the higher coordinate;
+//   bits 15-26 faces f0..f3, 3 bits each: 0 = not owned, 1 = unpaired,
+//              2..5 = paired with its left, right, upper, lower edge, i.e.
+//              its flow code + 1.
+// A pixel outside the image has word 0.
+constexpr int kWE0 = 3, kWE1 = 6, kWE2 = 9, kWE3 = 12, kWF0 = 15, kWF1 = 18, kWF2 = 21, kWF3 = 24;
 
-// All 16 x 16 x 5 entries, indexed ((eL << 4) | fL) * 5 + best + 1: the
-// pairing word of a pixel. Nibbles 0-3 describe edge slots 0-3 (4 = paired
-// with the vertex, 0..3 = paired with that face slot, 15 = critical, 14 = not
-// in the lower star), nibbles 4-7 face slots 0-3 (0..3 = paired with that
-// edge slot, 15 = critical, 14 = not in the lower star).
+// All 16 x 16 x 5 pairing words, indexed ((eL << 4) | fL) * 5 + best + 1,
+// built with face_fifo_entry (the reference's FIFO procedure).
 inline void face_fifo_table(uint32_t* out) {
+  // edge slot k paired with the pixel (its vertex): P is the right end of
+  // e0 = H(y,x), the left end of e1 = H(y,x+1), the lower end of e2 = V(y,x)
+  // and the upper end of e3 = V(y+1,x)
+  static const unsigned kEdgeVertex[4] = {3, 2, 3, 2};
+  // edge slot k paired with face slot f: lower (4) or higher (5) coface
+  static const unsigned kEdgeFace[4][4] = {{4, 0, 5, 0}, {0, 4, 0, 5}, {4, 5, 0, 0}, {0, 0, 4, 5}};
+  // face slot f paired with edge slot k: flow code of the face + 1
+  // (f0 = F(y,x): e0 = its lower edge (down), e2 = its right edge; f1 =
+  // F(y,x+1): e1 lower, e2 left; f2 = F(y+1,x): e0 upper, e3 right; f3 =
+  // F(y+1,x+1): e1 upper, e3 left)
+  static const unsigned kFaceEdge[4][4] = {
+      {kFlowDown + 1, 0, kFlowRight + 1, 0},
+      {0, kFlowDown + 1, kFlowLeft + 1, 0},
+      {kFlowUp + 1, 0, 0, kFlowRight + 1},
+      {0, kFlowUp + 1, 0, kFlowLeft + 1}};
   for (unsigned eL = 0; eL < 16; ++eL)
     for (unsigned fL = 0; fL < 16; ++fL)
       for (int b = -1; b < 4; ++b) {
-        uint32_t w = face_fifo_entry(eL, fL, b);
+        const uint32_t pk = face_fifo_entry(eL, fL, b);
+        uint32_t w = (uint32_t)(b + 1);
         for (int k = 0; k < 4; ++k) {
-          if (!((eL >> k) & 1u)) w = (w & ~(0xFu << (4 * k))) | (kNotMine << (4 * k));
-          if (!((fL >> k) & 1u)) w = (w & ~(0xFu << (16 + 4 * k))) | (kNotMine << (16 + 4 * k));
+          if (!((eL >> k) & 1u)) continue;
+          const unsigned n = (pk >> (4 * k)) & 0xFu;
+          const unsigned code = n == 15u ? 1u : n == 4u ? kEdgeVertex[k] : kEdgeFace[k][n];
+          w |= code << (3 + 3 * k);
+        }
+        for (int f = 0; f < 4; ++f) {
+          if (!((fL >> f) & 1u)) continue;
+          const unsigned n = (pk >> (16 + 4 * f)) & 0xFu;
+          const unsigned code = n == 15u ? 1u : kFaceEdge[f][n];
+          w |= code << (15 + 3 * f);
         }
         out[((eL << 4) | fL) * 5 + (b + 1)] = w;
       }
 }
 constexpr int kFifoTable = 16 * 16 * 5;
 
-// 16 warps; each thread evaluates about 4 of the (kTileY + 1) x (kTileX + 1)
-// lower stars of a tile and each warp writes kTileY / 16 of its rows, so one
-// CTA's global loads (all issued before their first use) are amortised over
-// 2048 indices.
-constexpr int kGradThreads = 512;
-constexpr int kGradWarps = kGradThreads / 32;
-
 // v_greater (cpu/cell_compare.hxx:23-31) orders pixels by (value, y*W+x),
-// flipped in the dual. gt(a, b) when a's linear id is known to be larger (a "after" b) or smaller:
-// the (value, id) tie rule then reduces to one float compare.
+// flipped in the dual. gt(a, b) when a's linear id is known to be larger (a
+// "after" b) or smaller: the (value, id) tie rule then reduces to one float
+// compare.
 //   primal: after -> !(a < b), before -> (b < a); dual: after -> (a < b), before -> !(b < a)
 template <bool DUAL>
-__device__ __forceinline__ bool gt_after(float a, float b) {
+__host__ __device__ __forceinline__ bool gt_after(float a, float b) {
   return DUAL ? (a < b) : !(a < b);
 }
 template <bool DUAL>
-__device__ __forceinline__ bool gt_before(float a, float b) {
+__host__ __device__ __forceinline__ bool gt_before(float a, float b) {
   return DUAL ? !(b < a) : (b < a);
 }
 
-// Lower star of pixel (y, x) and its pairing (cpu/gradient.hxx:48-192), all in
-// registers. The highest-vertex scans keep the reference's candidate order
-// (cpu/cell_compare.hxx:33-63), so ties and non-finite values resolve the same
-// way. Edge slots: e0 = H(y,x), e1 = H(y,x+1), e2 = V(y,x), e3 = V(y+1,x);
-// face slots: f0 = F(y,x), f1 = F(y,x+1), f2 = F(y+1,x), f3 = F(y+1,x+1).
-// Returns the pixel's pairing word (face_fifo_table).
-template <bool DUAL, bool INTERIOR = false>
-__device__ __forceinline__ uint32_t lower_star(const float (*sv)[kValX], int y, int x, int H, int W, int ty0, int tx0,
-                                               const uint32_t* __restrict__ fifo_lut) {
-  // 3x3 neighbourhood; r, c index the value tile (origin y0-2, x0-2)
-  const int r = y - (ty0 - 2), c = x - (tx0 - 2);
-  // INTERIOR: every neighbour of the pixel is in the image
-  const bool lv = INTERIOR || x >= 1, rv = INTERIOR || x + 1 < W, uv = INTERIOR || y >= 1, dv = INTERIOR || y + 1 < H;
-  // row-major linear order of the 3x3 neighbourhood: UL < U < UR < L < P < R < DL < D < DR
-  const float P = sv[r][c];
-  const float L = sv[r][c - 1], R = sv[r][c + 1];
-  const float U = sv[r - 1][c], D = sv[r + 1][c];
-  const float UL = sv[r - 1][c - 1], UR = sv[r - 1][c + 1];
-  const float DL = sv[r + 1][c - 1], DR = sv[r + 1][c + 1];
-#define GT_A(a, b) gt_after<DUAL>(a, b)   /* a after b */
-#define GT_B(a, b) gt_before<DUAL>(a, b)  /* a before b */
-
-  const bool p_gt_l = lv && GT_A(P, L);
-  const bool r_gt_p = rv && GT_A(R, P);
-  const bool p_gt_u = uv && GT_A(P, U);
-  const bool d_gt_p = dv && GT_A(D, P);
-
-  unsigned eL = 0, fL = 0;
-  if (!lv || p_gt_l) eL |= 1u;
-  if (!r_gt_p) eL |= 2u;
-  if (!uv || p_gt_u) eL |= 4u;
-  if (!d_gt_p) eL |= 8u;
-  {  // f0 = F(y,x): scan UL, U, L, then P (each later candidate is after the earlier ones)
-    bool p_top;
-    if (uv && lv) {
-      // best of UL, U, L
-      int b = GT_A(U, UL) ? 1 : 0;  // 0 = UL, 1 = U
-      float bv = b ? U : UL;
-      if (GT_A(L, bv)) {
-        bv = L;
-      }
-      p_top = GT_A(P, bv);
-    } else if (uv) {
-      p_top = GT_A(P, U);
-    } else if (lv) {
-      p_top = GT_A(P, L);
-    } else {
-      p_top = true;
-    }
-    if (p_top) fL |= 1u;
-  }
-  {  // f1 = F(y,x+1): scan U, UR, P, R
-    bool p_best;
-    if (uv) {
-      float bv = (rv && GT_A(UR, U)) ? UR : U;  // U, UR both before P
-      p_best = GT_A(P, bv);
-    } else {
-      p_best = true;
-    }
-    if (p_best && !r_gt_p) fL |= 2u;
-  }
-  {  // f2 = F(y+1,x): scan L, P, DL, D
-    bool p_best = !lv || p_gt_l;
-    if (p_best && dv && lv && GT_A(DL, P)) p_best = false;
-    if (p_best && d_gt_p) p_best = false;
-    if (p_best) fL |= 4u;
-  }
-  {  // f3 = F(y+1,x+1): scan P, R, D, DR
-    bool p_best = !r_gt_p && !d_gt_p && !(dv && rv && GT_A(DR, P));
-    if (p_best) fL |= 8u;
-  }
-
-  // vertex pairing: the lower-star edge whose other vertex is lowest
-  // (candidates visited L, R, U, D; "bo greater than the new one" decides)
+// Pairing word of pixel P from its 3 x 3 neighbourhood (cpu/gradient.hxx:48-192).
+// A cell is in P's lower star when P is its highest vertex; under the
+// (value, id) order, a strict total order on every field whose values are
+// numbers or all NaN, that is P being above each of the cell's other
+// vertices, so eight comparisons of P with its neighbours decide the eight
+// cells. The vertex pairs with the lower-star edge whose other vertex is
+// lowest, scanned L, R, U, D as the reference does; the face FIFO depends
+// only on (eL, fL, best) and is looked up. lv/rv/uv/dv: the neighbour exists.
+template <bool DUAL, bool INTERIOR>
+__host__ __device__ __forceinline__ uint32_t star_word(float UL, float U, float UR, float L, float P, float R, float DL, float D,
+                                              float DR, bool lv, bool rv, bool uv, bool dv,
+                                              const uint32_t* __restrict__ lut) {
+  if (INTERIOR) lv = rv = uv = dv = true;
+  const bool gL = gt_after<DUAL>(P, L), gU = gt_after<DUAL>(P, U);
+  const bool gUL = gt_after<DUAL>(P, UL), gUR = gt_after<DUAL>(P, UR);  // UR = (y-1, x+1) precedes P too
+  const bool gR = gt_before<DUAL>(P, R), gD = gt_before<DUAL>(P, D);
+  const bool gDL = gt_before<DUAL>(P, DL), gDR = gt_before<DUAL>(P, DR);
+  const bool e0 = !lv || gL, e1 = !rv || gR, e2 = !uv || gU, e3 = !dv || gD;
+  const bool f0 = e0 && e2 && (!(lv && uv) || gUL);
+  const bool f1 = e1 && e2 && (!(rv && uv) || gUR);
+  const bool f2 = e0 && e3 && (!(lv && dv) || gDL);
+  const bool f3 = e1 && e3 && (!(rv && dv) || gDR);
   int best = -1;
   float bo = 0.0f;
-  if ((eL & 1u) && lv) {
+  if (lv && gL) {
     best = 0;
     bo = L;
   }
-  if ((eL & 2u) && rv && (best < 0 || GT_B(bo, R))) {  // L before R
+  if (rv && gR && (best < 0 || gt_before<DUAL>(bo, R))) {  // L before R
     best = 1;
     bo = R;
   }
-  if ((eL & 4u) && uv && (best < 0 || GT_A(bo, U))) {  // L, R after U
+  if (uv && gU && (best < 0 || gt_after<DUAL>(bo, U))) {  // L, R after U
     best = 2;
     bo = U;
   }
-  if ((eL & 8u) && dv && (best < 0 || GT_B(bo, D))) {  // L, R, U before D
+  if (dv && gD && (best < 0 || gt_before<DUAL>(bo, D))) {  // L, R, U before D
     best = 3;
-    bo = D;
   }
-#undef GT_A
-#undef GT_B
-
-  // face pairing: the FIFO of cpu/gradient.hxx:115-191 depends only on the
-  // lower-star masks and the vertex-paired edge, so its result is looked up
-  // (face_fifo_table() builds the 1280 entries with the same procedure).
-  return __ldg(fifo_lut + (((eL << 4) | fL) * 5 + (best + 1)));
+  const unsigned eL = (unsigned)e0 | (unsigned)e1 << 1 | (unsigned)e2 << 2 | (unsigned)e3 << 3;
+  const unsigned fL = (unsigned)f0 | (unsigned)f1 << 1 | (unsigned)f2 << 2 | (unsigned)f3 << 3;
+#ifdef __CUDA_ARCH__
+  return __ldg(lut + (((eL << 4) | fL) * 5 + (best + 1)));
+#else
+  return lut[((eL << 4) | fL) * 5 + (best + 1)];
+#endif
 }
 
-// Pairing words of the (kTileY + 1) x (kTileX + 1) pixels whose lower stars
-// hold the cells of one 32 x kTileY index tile (origin pixel (y0 - 1, x0 - 1)).
-// INTERIOR: the tile's value window lies inside the image, so no bound is tested.
-template <bool DUAL, bool INTERIOR>
-__device__ __forceinline__ void gradient_tile(const float* __restrict__ img, int H, int W, int y0, int x0, int tid,
-                                              float (*sv)[kValX], uint32_t (*word)[kTileX + 1],
-                                              const uint32_t* __restrict__ fifo_lut) {
-  constexpr int kValN = kValY * kValX;
-  constexpr int kLoads = (kValN + kGradThreads - 1) / kGradThreads;
-  float v[kLoads];
-#pragma unroll
-  for (int k = 0; k < kLoads; ++k) {  // every load in flight before the first shared store
-    const int i = tid + k * kGradThreads;
-    const int r = i / kValX, c = i - r * kValX;
-    const int gy = y0 - 2 + r, gx = x0 - 2 + c;
-    v[k] = (i < kValN && (INTERIOR || (gy >= 0 && gy < H && gx >= 0 && gx < W))) ? __ldg(img + (size_t)gy * W + gx)
-                                                                                  : 0.0f;
+// Partner offsets of the gather (4 * index + offset = partner cell), per
+// image width; codes as in the pairing word:
+//   [0 + v]   vertex paired with e0..e3: H(y,x), H(y,x+1), V(y,x), V(y+1,x)
+//   [8 + c]   H edge H(y,x): left vertex, right vertex, face above, face below
+//   [16 + c]  V edge V(y,x): upper vertex, lower vertex, face left, face right
+//   [24 + c]  face F(y,x): left edge V(y,x-1), right V(y,x), upper H(y-1,x), lower H(y,x)
+__host__ __device__ __forceinline__ int gather_offset(int k, int Nx) {
+  switch (k) {
+    case 1: return 1;
+    case 2: return 5;
+    case 3: return 2;
+    case 4: return 4 * Nx + 2;
+    case 8 + 2: return -4;
+    case 8 + 3: return 0;
+    case 8 + 4: return 3;
+    case 8 + 5: return 4 * Nx + 3;
+    case 16 + 2: return -4 * Nx;
+    case 16 + 3: return 0;
+    case 16 + 4: return 3;
+    case 16 + 5: return 7;
+    case 24 + 2: return -2;
+    case 24 + 3: return 2;
+    case 24 + 4: return 1 - 4 * Nx;
+    case 24 + 5: return 1;
+    default: return 0;
   }
-#pragma unroll
-  for (int k = 0; k < kLoads; ++k) {
-    const int i = tid + k * kGradThreads;
-    if (i < kValN) (&sv[0][0])[i] = v[k];
-  }
-  __syncthreads();
-  constexpr int kWordN = (kTileY + 1) * (kTileX + 1);
-  for (int p = tid; p < kWordN; p += kGradThreads) {
-    const int r = p / (kTileX + 1), c = p - r * (kTileX + 1);
-    const int y = y0 - 1 + r, x = x0 - 1 + c;
-    uint32_t w = kNoPixel;
-    if (INTERIOR || (y >= 0 && y < H && x >= 0 && x < W)) w = lower_star<DUAL, INTERIOR>(sv, y, x, H, W, y0, x0, fifo_lut);
-    word[r][c] = w;
-  }
-  __syncthreads();
 }
 
-// Cell of edge slot k / face slot f of the pixel at index `b`.
-__device__ __forceinline__ int slot_edge_cell(int k, int b, int Nx) {
-  return (1 + (k >> 1)) + 4 * (b + (k == 3 ? Nx : 0) + (k == 1 ? 1 : 0));
+// Slots, criticality bits and flow code of the index b4 / 4 from the words of
+// the four pixels that may own its cells: P = (iy, ix), L = (iy, ix-1),
+// U = (iy-1, ix), UL = (iy-1, ix-1). `vin`: the index's vertex is a pixel.
+__host__ __device__ __forceinline__ void gather_index(uint32_t wP, uint32_t wL, uint32_t wU, uint32_t wUL, int b4,
+                                                      const int* off, bool vin, int4& g, unsigned& m,
+                                                      unsigned& fl) {
+  const unsigned v = wP & 7u;
+  const unsigned hc = ((wP >> kWE0) | (wL >> kWE1)) & 7u;
+  const unsigned vc = ((wP >> kWE2) | (wU >> kWE3)) & 7u;
+  const unsigned fc = ((wP >> kWF0) | (wL >> kWF1) | (wU >> kWF2) | (wUL >> kWF3)) & 7u;
+  g = make_int4(v ? b4 + off[v] : -1, hc >= 2u ? b4 + off[8 + hc] : -1, vc >= 2u ? b4 + off[16 + vc] : -1,
+                fc >= 2u ? b4 + off[24 + fc] : -1);
+  m = (unsigned)(v == 0u && vin) | (unsigned)(hc == 1u) << 1 | (unsigned)(vc == 1u) << 2 | (unsigned)(fc == 1u) << 3;
+  fl = v | ((fc - 1u) << 4);  // every index has its face, so fc >= 1
 }
-__device__ __forceinline__ int slot_face_cell(int f, int b, int Nx) { return 3 + 4 * (b + (f >> 1) * Nx + (f & 1)); }
 
-// Write-out of tile row `warp` by one warp. Index (iy, ix) gathers its four
-// slots from the pairing words of the pixels owning them: its vertex and
-// (when owned there) its H edge, V edge and face from pixel (iy, ix), else
-// the H edge from (iy, ix-1), the V edge from (iy-1, ix) and the face from
-// (iy, ix-1), (iy-1, ix) or (iy-1, ix-1). Coalesced int4 gradient stores at
-// global index base `gbase` (skipped when `grad` is null: the later stages
-// read only the mask and flow codes), criticality mask, flow codes and the
-// row segment's counts (segment id `seg`).
-template <bool INTERIOR>
-__device__ __forceinline__ void gradient_store_row(const uint32_t (*word)[kTileX + 1], int warp, int lane, int H,
-                                                   int W, int iy, int ix, long long gbase, int seg,
-                                                   int4* __restrict__ grad, uint8_t* __restrict__ crit_mask,
-                                                   uint8_t* __restrict__ flow, int* __restrict__ seg_min,
-                                                   int* __restrict__ seg_sad, int* __restrict__ seg_max) {
+template <int TY>
+struct GradSmem {
+  float v[TY + 3][35];         // pixel rows y0-2 .. y0+TY, columns x0-2 .. x0+32
+  uint32_t w[TY + 1][33];      // words of pixel rows y0-1 .. y0+TY-1, columns x0-1 .. x0+31
+  int off[32];                 // gather offsets of the tile's image
+};
+
+// One 32 x TY index tile at index origin (y0, x0) of an H x W image:
+// gradient, criticality, flow codes and row-segment counts. INTERIOR: the
+// value window [y0-2, y0+TY] x [x0-2, x0+32] lies inside the image, so no
+// bound is tested. `gbase`: global index of the image's index (0, 0);
+// `sbase`: its first row segment; `ntx`: its row segments per row.
+template <bool DUAL, bool INTERIOR, int TY, int NT>
+__device__ __forceinline__ void gradient_tile(GradSmem<TY>& S, const float* __restrict__ img, int H, int W, int y0,
+                                              int x0, long long gbase, int sbase, int ntx, int tx,
+                                              const uint32_t* __restrict__ lut, int4* __restrict__ grad,
+                                              uint8_t* __restrict__ crit_mask, uint8_t* __restrict__ flow,
+                                              int* __restrict__ seg_min, int* __restrict__ seg_sad,
+                                              int* __restrict__ seg_max) {
+  constexpr int NW = NT / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int Nx = W + 1;
-  const bool in = INTERIOR || ix <= W;
-  unsigned m = 0;
-  if (in) {
-    const uint32_t wP = word[warp + 1][lane + 1], wL = word[warp + 1][lane];
-    const uint32_t wU = word[warp][lane + 1], wUL = word[warp][lane];
-    const int b = iy * Nx + ix;  // image-local index: the cell ids written are local
-    // vertex: the edge slot of its own pixel marked 4
-    const unsigned e = wP & 0xFFFFu;
-    const int vk = ((e & 0xFu) == 4u) ? 0 : (((e >> 4) & 0xFu) == 4u) ? 1 : (((e >> 8) & 0xFu) == 4u) ? 2
-                 : (((e >> 12) & 0xFu) == 4u) ? 3 : -1;
-    const int s0 = vk >= 0 ? slot_edge_cell(vk, b, Nx) : -1;
-    // H edge (iy, ix): slot 0 of (iy, ix) or slot 1 of (iy, ix-1)
-    const unsigned h0 = wP & 0xFu;
-    const bool hown = h0 != kNotMine;
-    const unsigned hn = hown ? h0 : ((wL >> 4) & 0xFu);
-    const int hb = hown ? b : b - 1;
-    const int s1 = hn == 4u ? 4 * hb : (hn < 4u ? slot_face_cell((int)hn, hb, Nx) : -1);
-    // V edge (iy, ix): slot 2 of (iy, ix) or slot 3 of (iy-1, ix)
-    const unsigned v0 = (wP >> 8) & 0xFu;
-    const bool vown = v0 != kNotMine;
-    const unsigned vn = vown ? v0 : ((wU >> 12) & 0xFu);
-    const int vb = vown ? b : b - Nx;
-    const int s2 = vn == 4u ? 4 * vb : (vn < 4u ? slot_face_cell((int)vn, vb, Nx) : -1);
-    // face (iy, ix): face slot 0 of (iy, ix), 1 of (iy, ix-1), 2 of (iy-1, ix), 3 of (iy-1, ix-1)
-    const unsigned f0 = (wP >> 16) & 0xFu, f1 = (wL >> 20) & 0xFu, f2 = (wU >> 24) & 0xFu, f3 = wUL >> 28;
-    const unsigned fn = f0 != kNotMine ? f0 : f1 != kNotMine ? f1 : f2 != kNotMine ? f2 : f3;
-    const int fb = f0 != kNotMine ? b : f1 != kNotMine ? b - 1 : f2 != kNotMine ? b - Nx : b - Nx - 1;
-    const int s3 = fn < 4u ? slot_edge_cell((int)fn, fb, Nx) : -1;
-    const size_t gidx = (size_t)(gbase + b);
-    if (grad) grad[gidx] = make_int4(s0, s1, s2, s3);  // null when the gradient is not returned
-    if (vk < 0 && (INTERIOR || (iy < H && ix < W))) m |= 1u;
-    if (hn == 15u) m |= 2u;
-    if (vn == 15u) m |= 4u;
-    if (fn == 15u) m |= 8u;
-    crit_mask[gidx] = (uint8_t)m;
-    flow[gidx] = (uint8_t)((unsigned)(vk + 1) | (face_flow(s3, b) << 4));
+  if (threadIdx.x < 32) S.off[lane] = gather_offset(lane, Nx);
+  // ---- value window: rows by warp, 32 + 3 columns per row ----
+  for (int r = warp; r < TY + 3; r += NW) {
+    const int gy = y0 - 2 + r;
+    const float* row = img + (size_t)(INTERIOR ? gy : max(0, min(gy, H - 1))) * W;
+    const bool yin = INTERIOR || (gy >= 0 && gy < H);
+    const int gx = x0 - 2 + lane, gx2 = x0 + 30 + lane;
+    const float a = (INTERIOR || (yin && gx >= 0 && gx < W)) ? __ldg(row + gx) : 0.0f;
+    float b = 0.0f;
+    if (lane < 3 && (INTERIOR || (yin && gx2 < W))) b = __ldg(row + gx2);
+    S.v[r][lane] = a;
+    if (lane < 3) S.v[r][32 + lane] = b;
   }
-  unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
-  unsigned bs1 = __ballot_sync(0xffffffffu, m & 2u);
-  unsigned bs2 = __ballot_sync(0xffffffffu, m & 4u);
-  unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
-  if (lane == 0) {
-    seg_min[seg] = __popc(bmin);
-    seg_sad[seg] = __popc(bs1) + __popc(bs2);
-    seg_max[seg] = __popc(bmax);
+  __syncthreads();
+  // ---- pairing words ----
+  {  // main columns: lane -> column x0 + lane (word column lane + 1), a run of rows per warp
+    constexpr int kRun = (TY + 1 + NW - 1) / NW;
+    const int ra = warp * kRun, rb = min(TY + 1, ra + kRun);
+    const int x = x0 + lane, c = lane + 2;  // value column of the pixel
+    const bool xin = INTERIOR || x < W;
+    const bool lv = INTERIOR || x >= 1, rv = INTERIOR || x + 1 < W;
+    if (ra < rb) {
+      float u0 = S.v[ra][c - 1], u1 = S.v[ra][c], u2 = S.v[ra][c + 1];
+      float p0 = S.v[ra + 1][c - 1], p1 = S.v[ra + 1][c], p2 = S.v[ra + 1][c + 1];
+      for (int r = ra; r < rb; ++r) {
+        const float d0 = S.v[r + 2][c - 1], d1 = S.v[r + 2][c], d2 = S.v[r + 2][c + 1];
+        const int y = y0 - 1 + r;
+        uint32_t w = 0;
+        if (INTERIOR || (xin && y >= 0 && y < H))
+          w = star_word<DUAL, INTERIOR>(u0, u1, u2, p0, p1, p2, d0, d1, d2, lv, rv, INTERIOR || y >= 1,
+                                        INTERIOR || y + 1 < H, lut);
+        S.w[r][lane + 1] = w;
+        u0 = p0;
+        u1 = p1;
+        u2 = p2;
+        p0 = d0;
+        p1 = d1;
+        p2 = d2;
+      }
+    }
+  }
+  {  // halo column x0 - 1 (word column 0, value column 1): lane -> row
+    constexpr int kHaloPasses = (TY + 1 + 31) / 32;
+    if (warp < kHaloPasses) {
+      const int r = warp * 32 + lane;
+      if (r <= TY) {
+        const int y = y0 - 1 + r, x = x0 - 1;
+        uint32_t w = 0;
+        if (INTERIOR || (x >= 0 && x < W && y >= 0 && y < H))
+          w = star_word<DUAL, INTERIOR>(S.v[r][0], S.v[r][1], S.v[r][2], S.v[r + 1][0], S.v[r + 1][1], S.v[r + 1][2],
+                                        S.v[r + 2][0], S.v[r + 2][1], S.v[r + 2][2], INTERIOR || x >= 1,
+                                        INTERIOR || x + 1 < W, INTERIOR || y >= 1, INTERIOR || y + 1 < H, lut);
+        S.w[r][0] = w;
+      }
+    }
+  }
+  __syncthreads();
+  // ---- gather and stores: one index row per warp step ----
+  const int ix = x0 + lane;
+  const bool xok = INTERIOR || ix <= W;
+  for (int rr = warp; rr < TY; rr += NW) {
+    const int iy = y0 + rr;
+    if (!INTERIOR && iy > H) break;  // uniform per warp
+    unsigned m = 0;
+    if (xok) {
+      const uint32_t wP = S.w[rr + 1][lane + 1], wL = S.w[rr + 1][lane];
+      const uint32_t wU = S.w[rr][lane + 1], wUL = S.w[rr][lane];
+      const int b = iy * Nx + ix;  // image-local index: the cell ids written are local
+      const size_t gidx = (size_t)(gbase + b);
+      int4 g;
+      unsigned fl;
+      gather_index(wP, wL, wU, wUL, 4 * b, S.off, INTERIOR || (iy < H && ix < W), g, m, fl);
+      if (grad) grad[gidx] = g;  // null when the gradient is not returned
+      crit_mask[gidx] = (uint8_t)m;
+      flow[gidx] = (uint8_t)fl;
+    }
+    const unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
+    const unsigned bs1 = __ballot_sync(0xffffffffu, m & 2u);
+    const unsigned bs2 = __ballot_sync(0xffffffffu, m & 4u);
+    const unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
+    if (lane == 0) {
+      const int seg = sbase + iy * ntx + tx;
+      seg_min[seg] = __popc(bmin);
+      seg_sad[seg] = __popc(bs1) + __popc(bs2);
+      seg_max[seg] = __popc(bmax);
+    }
   }
 }
 
-// K1 (one image): gradient over one 32 x 64 index tile per CTA.
-template <bool DUAL>
-__global__ void __launch_bounds__(kGradThreads) gradient_kernel(const float* __restrict__ img, int H, int W,
-                                                               int4* __restrict__ grad,
-                                                               uint8_t* __restrict__ crit_mask,
-                                                               int* __restrict__ seg_min, int* __restrict__ seg_sad,
-                                                               int* __restrict__ seg_max,
-                                                               const uint32_t* __restrict__ fifo_lut,
-                                                               uint8_t* __restrict__ flow) {
-  __shared__ float sv[kValY][kValX];
-  __shared__ uint32_t word[kTileY + 1][kTileX + 1];
-  const int tid = threadIdx.x;
-  const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY;
-  gradient_tile<DUAL, false>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
-  const int warp = tid >> 5, lane = tid & 31;
-  for (int rr = warp; rr < kTileY; rr += kGradWarps) {
-    const int iy = y0 + rr, ix = x0 + lane;
-    if (iy > H) break;  // uniform per warp
-    gradient_store_row<false>(word, rr, lane, H, W, iy, ix, 0, iy * gridDim.x + blockIdx.x, grad, crit_mask, flow,
-                              seg_min, seg_sad, seg_max);
-  }
+// Tile shapes of the gradient kernels (index rows, threads): the tuner in
+// the host code picks one per call from these instantiations.
+constexpr int kGradShapes = 3;
+constexpr int kGradTY[kGradShapes] = {31, 63, 127};
+constexpr int kGradNT[kGradShapes] = {256, 256, 512};
+
+// K1 (one image): a 2-D grid of tiles, (ntx, nty).
+template <bool DUAL, int TY, int NT>
+__global__ void __launch_bounds__(NT) gradient_kernel(const float* __restrict__ img, int H, int W,
+                                                      int4* __restrict__ grad, uint8_t* __restrict__ crit_mask,
+                                                      int* __restrict__ seg_min, int* __restrict__ seg_sad,
+                                                      int* __restrict__ seg_max, const uint32_t* __restrict__ lut,
+                                                      uint8_t* __restrict__ flow) {
+  __shared__ GradSmem<TY> S;
+  const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * TY;
+  const bool interior = y0 >= 2 && x0 >= 2 && y0 + TY <= H - 1 && x0 + kTileX <= W - 1;
+  if (interior)
+    gradient_tile<DUAL, true, TY, NT>(S, img, H, W, y0, x0, 0, 0, gridDim.x, blockIdx.x, lut, grad, crit_mask, flow,
+                                      seg_min, seg_sad, seg_max);
+  else
+    gradient_tile<DUAL, false, TY, NT>(S, img, H, W, y0, x0, 0, 0, gridDim.x, blockIdx.x, lut, grad, crit_mask, flow,
+                                       seg_min, seg_sad, seg_max);
 }
 
 // K1 (batch): the tiles of every image of a batch in one 1-D grid; each CTA
-// finds its image from the tile bases.
-static __global__ void __launch_bounds__(kGradThreads) gradient_batch_kernel(Imgs I, const float* __restrict__ img_all,
-                                                                     int4* __restrict__ grad,
-                                                                     uint8_t* __restrict__ crit_mask,
-                                                                     int* __restrict__ seg_min,
-                                                                     int* __restrict__ seg_sad,
-                                                                     int* __restrict__ seg_max,
-                                                                     const uint32_t* __restrict__ fifo_lut,
-                                                                     uint8_t* __restrict__ flow) {
-  __shared__ float sv[kValY][kValX];
-  __shared__ uint32_t word[kTileY + 1][kTileX + 1];
-  const int tid = threadIdx.x;
+// finds its image from the tile bases (tiles of TY index rows).
+template <int TY, int NT>
+__global__ void __launch_bounds__(NT) gradient_batch_kernel(Imgs I, const float* __restrict__ img_all,
+                                                            int4* __restrict__ grad, uint8_t* __restrict__ crit_mask,
+                                                            int* __restrict__ seg_min, int* __restrict__ seg_sad,
+                                                            int* __restrict__ seg_max,
+                                                            const uint32_t* __restrict__ lut,
+                                                            uint8_t* __restrict__ flow) {
+  __shared__ GradSmem<TY> S;
   const int b = find_image(I.tile_base, I.B, blockIdx.x);
   const int H = I.H[b], W = I.W[b];
   const int ntx = (W + 1 + kTileX - 1) / kTileX;
   const int t = blockIdx.x - I.tile_base[b];
   const int ty = t / ntx, tx = t - ty * ntx;
-  const int x0 = tx * kTileX, y0 = ty * kTileY;
+  const int x0 = tx * kTileX, y0 = ty * TY;
   const float* img = img_all + I.px_base[b];
-  // tiles whose value window [y0-2, y0+kTileY] x [x0-2, x0+kTileX] lies inside
-  // the image (almost all of them) run without bound tests
-  const bool interior = y0 >= 2 && x0 >= 2 && y0 + kTileY <= H - 1 && x0 + kTileX <= W - 1;
-  if (I.dual[b]) {
-    if (interior)
-      gradient_tile<true, true>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
-    else
-      gradient_tile<true, false>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
-  } else {
-    if (interior)
-      gradient_tile<false, true>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
-    else
-      gradient_tile<false, false>(img, H, W, y0, x0, tid, sv, word, fifo_lut);
-  }
-  const int warp = tid >> 5, lane = tid & 31;
   const long long gbase = I.idx_base[b];
   const int sbase = I.seg_base[b];
-  for (int rr = warp; rr < kTileY; rr += kGradWarps) {
-    const int iy = y0 + rr, ix = x0 + lane;
-    if (iy > H) break;  // uniform per warp
+  // tiles whose value window lies inside the image (almost all) run without bound tests
+  const bool interior = y0 >= 2 && x0 >= 2 && y0 + TY <= H - 1 && x0 + kTileX <= W - 1;
+  if (I.dual[b]) {
     if (interior)
-      gradient_store_row<true>(word, rr, lane, H, W, iy, ix, gbase, sbase + iy * ntx + tx, grad, crit_mask, flow,
-                               seg_min, seg_sad, seg_max);
+      gradient_tile<true, true, TY, NT>(S, img, H, W, y0, x0, gbase, sbase, ntx, tx, lut, grad, crit_mask, flow,
+                                        seg_min, seg_sad, seg_max);
     else
-      gradient_store_row<false>(word, rr, lane, H, W, iy, ix, gbase, sbase + iy * ntx + tx, grad, crit_mask, flow,
-                                seg_min, seg_sad, seg_max);
+      gradient_tile<true, false, TY, NT>(S, img, H, W, y0, x0, gbase, sbase, ntx, tx, lut, grad, crit_mask, flow,
+                                         seg_min, seg_sad, seg_max);
+  } else {
+    if (interior)
+      gradient_tile<false, true, TY, NT>(S, img, H, W, y0, x0, gbase, sbase, ntx, tx, lut, grad, crit_mask, flow,
+                                         seg_min, seg_sad, seg_max);
+    else
+      gradient_tile<false, false, TY, NT>(S, img, H, W, y0, x0, gbase, sbase, ntx, tx, lut, grad, crit_mask, flow,
+                                          seg_min, seg_sad, seg_max);
   }
 }
 

@@ -31,7 +31,11 @@ namespace {
 using namespace dmsc;
 
 // 8 MiB: per image, 2 bytes per index (criticality mask and flow codes) plus
-// 6 ints per 32-index row segment (three counts, three offsets).
+// 6 ints per 32-index row segment (three counts, three offsets), each of the
+// eight parts rounded up to 256 bytes: about 2.75 bytes per index, so square
+// images up to 1743 x 1743 fit (1744 x 1744 needs 8,394,240 bytes). The
+// scratch check also keeps the segment count far below INT_MAX, which the
+// single-block scan relies on.
 constexpr size_t kStaticScratchBytes = 8u << 20;
 __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 __device__ uint32_t g_static_fifo_lut[kFifoTable];
@@ -60,6 +64,12 @@ int static_setup(int device, DeviceStatic** out) {
     face_fifo_table(lut.data());
     if (cudaMemcpyToSymbol(g_static_fifo_lut, lut.data(), kFifoTable * sizeof(uint32_t)) != cudaSuccess)
       return DMSC_B200_ERR_CUDA;
+    // A copy from pageable host memory may return before the table has
+    // reached the device, and it is ordered on the legacy default stream
+    // only; the caller's stream (possibly non-blocking) is not ordered after
+    // it. Waiting here, once per device, makes the table visible to every
+    // later launch on any stream.
+    if (cudaDeviceSynchronize() != cudaSuccess) return DMSC_B200_ERR_CUDA;
     d.ready = true;
   }
   *out = &d;
@@ -159,7 +169,7 @@ extern "C" int dmsc_b200_critical_cells_static(const float* image, int H, int W,
   // scratch layout: mask [nidx] | flow [nidx] | 6 x nseg ints, 256-byte aligned parts
   auto up = [](long long b) { return (b + 255) & ~255LL; };
   const long long need = up(nidx) + up(nidx) + 6 * up(nseg * 4);
-  if (need > (long long)kStaticScratchBytes) return DMSC_B200_ERR_TOO_LARGE;
+  if (need > (long long)kStaticScratchBytes) return DMSC_B200_ERR_TOO_LARGE;  // before any launch
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) return DMSC_B200_ERR_CUDA;
   DeviceStatic* d = nullptr;
@@ -181,14 +191,14 @@ extern "C" int dmsc_b200_critical_cells_static(const float* image, int H, int W,
     off[k] = (int*)p;
     p += up(nseg * 4);
   }
-  dim3 g1(nsegx, (H + 1 + kTileY - 1) / kTileY);
+  constexpr int TY = kGradTY[1], NT = kGradNT[1];
+  dim3 g1(nsegx, (H + 1 + TY - 1) / TY);
   if (flags & DMSC_B200_DUAL)
-    gradient_kernel<true><<<g1, kGradThreads, 0, st>>>(image, H, W, (int4*)grad_out, mask, seg[0], seg[1], seg[2],
-                                                       d->lut, flow);
+    gradient_kernel<true, TY, NT><<<g1, NT, 0, st>>>(image, H, W, (int4*)grad_out, mask, seg[0], seg[1], seg[2],
+                                                     d->lut, flow);
   else
-    gradient_kernel<false><<<g1, kGradThreads, 0, st>>>(image, H, W, (int4*)grad_out, mask, seg[0], seg[1], seg[2],
-                                                        d->lut, flow);
-  if (nseg > 2147483647LL) return DMSC_B200_ERR_TOO_LARGE;
+    gradient_kernel<false, TY, NT><<<g1, NT, 0, st>>>(image, H, W, (int4*)grad_out, mask, seg[0], seg[1], seg[2],
+                                                      d->lut, flow);
   static_scan3_kernel<<<1, 1024, 0, st>>>(seg[0], seg[1], seg[2], (int)nseg, off[0], off[1], off[2], counts_out);
   static_lists_kernel<<<(unsigned)((nseg + 7) / 8), 256, 0, st>>>(W, nsegx, nseg, mask, off[0], off[1], off[2],
                                                                   mins_out, saddles_out, maxes_out);

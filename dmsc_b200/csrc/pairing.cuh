@@ -117,11 +117,19 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
 
 // Thresholded union-find: lock-free union of the ends of every cancelled
 // saddle (link the larger root under the smaller), over the compact list of
-// cancelled edges written by persistence_kernel.
-__device__ __forceinline__ int uf_root(int* p, int x) {
-  while (true) {
+// cancelled edges written by persistence_kernel. Every link points to a
+// smaller index, so a root search takes at most n steps and every failed CAS
+// means another thread linked one of the two roots (at most n - 1 links
+// exist); both loops are capped at `cap` anyway, and a cap sets
+// kStatusFindCap and returns the node reached (a valid index).
+__device__ __forceinline__ int uf_root(int* p, int x, int cap, unsigned* status) {
+  for (int k = 0;; ++k) {
     int px = p[x];
     if (px == x) return x;
+    if (k >= cap) {
+      set_status(status, kStatusFindCap);
+      return x;
+    }
     int ppx = p[px];
     if (ppx != px) p[x] = ppx;  // path halving; benign race
     x = ppx;
@@ -129,15 +137,20 @@ __device__ __forceinline__ int uf_root(int* p, int x) {
 }
 
 __global__ void __launch_bounds__(256) ut_union_kernel(const int2* __restrict__ ends, const int* __restrict__ count,
-                                                       int void_id, int* __restrict__ p) {
+                                                       int void_id, int* __restrict__ p, int cap,
+                                                       unsigned* status) {
   const int n = *count;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
     const int2 e = ends[q];
     int a = e.x < 0 ? void_id : e.x;
     int b = e.y < 0 ? void_id : e.y;
-    while (true) {
-      a = uf_root(p, a);
-      b = uf_root(p, b);
+    for (int tries = 0;; ++tries) {
+      if (tries >= cap) {
+        set_status(status, kStatusFindCap);
+        break;
+      }
+      a = uf_root(p, a, cap, status);
+      b = uf_root(p, b, cap, status);
       if (a == b) break;
       if (a > b) {
         int t = a;
@@ -149,11 +162,17 @@ __global__ void __launch_bounds__(256) ut_union_kernel(const int2* __restrict__ 
   }
 }
 
-__global__ void ut_flatten_kernel(int n, int* __restrict__ p) {
+__global__ void ut_flatten_kernel(int n, int* __restrict__ p, int cap, unsigned* status) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= n) return;
   int r = x;
-  while (p[r] != r) r = p[r];
+  for (int k = 0; p[r] != r; ++k) {
+    if (k >= cap) {
+      set_status(status, kStatusFindCap);
+      break;
+    }
+    r = p[r];
+  }
   p[x] = r;
 }
 

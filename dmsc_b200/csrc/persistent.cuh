@@ -27,10 +27,18 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 constexpr int kTimeline = 64;  // timestamps kept per loop (round starts)
 
-__device__ __forceinline__ int find_halving(int* link, int x) {
-  while (true) {
+// Root of x in the pairing's group forest. A group links only under an
+// older group (ages strictly decrease along links), so a search visits at
+// most M + 1 nodes; the loop is capped at `cap` anyway and a cap sets
+// kStatusFindCap and returns the node reached (a valid group).
+__device__ __forceinline__ int find_halving(int* link, int x, int cap, unsigned* status) {
+  for (int k = 0;; ++k) {
     int p = link[x];
     if (p == x) return x;
+    if (k >= cap) {
+      set_status(status, kStatusFindCap);
+      return x;
+    }
     int pp = link[p];
     if (pp != p) link[x] = pp;  // path halving: replaces a pointer with an ancestor
     x = pp;
@@ -134,8 +142,8 @@ __device__ __forceinline__ void pair_phase_a(const PairArgs& A, int r, long long
       gb = b < 0 ? M : b;
     } else {  // the ends' groups of the previous round, followed to their roots
       const int2 g = A.g12[e];
-      ga = find_halving(A.link, g.x);
-      gb = find_halving(A.link, g.y);
+      ga = find_halving(A.link, g.x, M + 2, A.status);
+      gb = find_halving(A.link, g.y, M + 2, A.status);
     }
     if (ga == gb) {
       A.dying[e] = -1;
@@ -219,7 +227,13 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
     }
     if (n0 == 0 && n1 == 0) break;
     if (r >= max(P.s[0].max_rounds, P.s[1].max_rounds)) {
+      // every thread leaves here in the same round (the counters it read are
+      // the same); saddles still undecided become cycles, so the kernels
+      // that run before the host sees the status read valid extremum indices
       if (tid == 0) set_status(P.s[0].status, kStatusRoundCap);
+      for (int sd = 0; sd < 2; ++sd)
+        for (long long i = tid; i < P.s[sd].nsad; i += nth)
+          if (P.s[sd].dying[i] == kUndecided) P.s[sd].dying[i] = -1;
       break;
     }
     if (tid == 0) {
@@ -387,6 +401,15 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
     if (na == 0 && nb == 0) break;
     if (rd >= max(P.s[0].max_rounds, P.s[1].max_rounds)) {
       if (tid == 0) set_status(P.s[0].n_cancel ? P.s[0].status : P.s[1].status, kStatusRoundCap);
+      // the cancellations still pending are dropped (their dying nodes
+      // become roots), so the chain walks of the kernels that run before the
+      // host sees the status meet decided nodes only
+      for (long long i = tid; i < (long long)na + nb; i += nth) {
+        const ReplayArgs& A = i < na ? P.s[0] : P.s[1];
+        const long long k = i < na ? i : i - na;
+        const int r = ((rd & 1) ? A.act1 : A.act0)[k];
+        A.S.node[A.dying[A.cj[r]]].status = kRootForever;
+      }
       break;
     }
     if (tid == 0)
@@ -494,7 +517,7 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
       break;
     }
     if (lv >= A.max_levels || n > E.q_cap) {
-      if (tid == 0) set_status(E.status, kStatusQueueOverflow);
+      if (tid == 0) set_status(E.status, lv >= A.max_levels ? kStatusRoundCap : kStatusQueueOverflow);
       break;
     }
     const int4* in = (lv & 1) ? A.q1 : A.q0;

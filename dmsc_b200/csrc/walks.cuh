@@ -216,94 +216,55 @@ __device__ __forceinline__ int tile_label(const TileRanks& R, int j, const int* 
   return __ldg(lab + rank);
 }
 
-// In-tile resolution of a tile's cells for both sides. st[side][i] starts as
-// the cell's successor decoded once from its flow code: kDone | i for a
-// critical cell, kDone | kExit | i when the successor lies outside the tile,
-// else the successor's tile-local id. Pointer jumping in place
-// (st[i] = st[st[i]] for the cells not yet done; every value read is still a
-// position on the cell's path) doubles the distance covered per round, so a
-// path of n steps inside the tile resolves in about log2(n) rounds; then
-// st[i] = kDone | [kExit] | (the critical cell reached, or the path's last
-// cell in the tile).
-constexpr unsigned kDone = 0x8000u, kExit = 0x4000u, kCell = 0x0FFFu;
-
-template <int SHIFT>
-__device__ __forceinline__ uint16_t tile_succ(const uint8_t (*fl)[kLT], int r, int c) {
-  const unsigned code = ((unsigned)fl[r][c] >> SHIFT) & 0xFu;
-  const unsigned i = (unsigned)(r * kLT + c);
-  if (code == kFlowNone) return (uint16_t)(kDone | i);
-  const int nr = r + (code == kFlowUp ? -1 : code == kFlowDown ? 1 : 0);
-  const int nc = c + (code == kFlowLeft ? -1 : code == kFlowRight ? 1 : 0);
-  if ((unsigned)nr >= (unsigned)kLT || (unsigned)nc >= (unsigned)kLT) return (uint16_t)(kDone | kExit | i);
-  return (uint16_t)(nr * kLT + nc);
-}
+// In-tile resolution. Every (side, cell) of the tile has one 32-bit state:
+// pending (kPend | j: the cell's path continues at tile cell j) or final, an
+// entry: (label << 1) | 1 when the path ends at a critical cell of the tile
+// (label -1 encodes as all ones), or (border-map index of the cell the path
+// enters next, in the neighbouring tile) << 1. The states start at the cell's
+// successor (decoded once from its flow code); then every thread jumps its own
+// cells' pointers, st[i] = st[st[i]], without block barriers: each value read
+// is a state of a cell further along the same path (written by any thread, at
+// any time), so a pointer only moves toward the path's end and reaches it in
+// at most the path's length of jumps, about log2 of it when the cells ahead
+// jump too. Border-map indices and labels stay below 2^30, so the top two bits
+// tell a pending state apart.
+constexpr uint32_t kPend = 0x40000000u, kCellMask = 0x0FFFu;
+__device__ __forceinline__ bool st_pending(uint32_t v) { return (v >> 30) == 1u; }
 
 constexpr int kLabelThreads = 1024;
 constexpr int kTileCells = kLTN / kLabelThreads;  // 4 cells per thread: rows tid/64 + 16k
 
-// st[0] faces, st[1] vertices, for the sides whose flags are set.
-__device__ __forceinline__ void tile_resolve(const uint8_t (*fl)[kLT], uint16_t (*st)[kLTN], bool do_f, bool do_v,
-                                             unsigned* status) {
-  const int c = threadIdx.x % kLT, rb = threadIdx.x / kLT;
-  unsigned pending = 0;  // bit 2k + side
-#pragma unroll
-  for (int k = 0; k < kTileCells; ++k) {
-    const int r = rb + 16 * k, i = r * kLT + c;
-    if (do_f) {
-      const uint16_t v = tile_succ<4>(fl, r, c);
-      st[0][i] = v;
-      if (!(v & kDone)) pending |= 1u << (2 * k);
-    }
-    if (do_v) {
-      const uint16_t v = tile_succ<0>(fl, r, c);
-      st[1][i] = v;
-      if (!(v & kDone)) pending |= 2u << (2 * k);
-    }
-  }
-  int round = 0;
-  for (; round < 16; ++round) {
-    if (!__syncthreads_or(pending != 0)) break;
-#pragma unroll
-    for (int k = 0; k < kTileCells; ++k) {
-      const int i = (rb + 16 * k) * kLT + c;
-#pragma unroll
-      for (int sd = 0; sd < 2; ++sd) {
-        if (!((pending >> (2 * k + sd)) & 1u)) continue;
-        const unsigned w = st[sd][st[sd][i] & kCell];
-        st[sd][i] = (uint16_t)w;
-        if (w & kDone) pending &= ~(1u << (2 * k + sd));
-      }
-    }
-  }
-  if (round == 16 && pending) set_status(status, kStatusWalkCap);
-  __syncthreads();
-}
-
-// Border map entry or label of a resolved state: (label << 1) | 1 for a
-// critical cell in the tile, else (border-map index of the next tile's entry
-// cell) << 1. Tile `tile` of an image with `ntx` tiles per row.
+// Initial state of a cell of the tile (FACES: face side) at tile position
+// (r, c); the cell is in the image.
 template <bool FACES>
-__device__ __forceinline__ int state_entry(unsigned w, const uint8_t (*fl)[kLT], const TileRanks& R,
-                                           const int* __restrict__ lab, int tile, int ntx) {
-  const int j = (int)(w & kCell);
-  if (!(w & kExit)) return (int)(((unsigned)tile_label<FACES>(R, j, lab) << 1) | 1u);
-  const int r = j / kLT, c = j % kLT;
+__device__ __forceinline__ uint32_t tile_init(const uint8_t (*fl)[kLT], const TileRanks& R, const int* __restrict__ lab,
+                                              int r, int c, int tile, int ntx) {
   const unsigned code = ((unsigned)fl[r][c] >> (FACES ? 4 : 0)) & 0xFu;
-  int nt, nr = r, nc = c;
+  if (code == kFlowNone) return ((uint32_t)tile_label<FACES>(R, r * kLT + c, lab) << 1) | 1u;
+  int nr = r, nc = c, nt = tile;
   if (code == kFlowLeft) {
-    nt = tile - 1;
-    nc = kLT - 1;
+    if (--nc < 0) {
+      nt = tile - 1;
+      nc = kLT - 1;
+    }
   } else if (code == kFlowRight) {
-    nt = tile + 1;
-    nc = 0;
+    if (++nc == kLT) {
+      nt = tile + 1;
+      nc = 0;
+    }
   } else if (code == kFlowUp) {
-    nt = tile - ntx;
-    nr = kLT - 1;
+    if (--nr < 0) {
+      nt = tile - ntx;
+      nr = kLT - 1;
+    }
   } else {
-    nt = tile + ntx;
-    nr = 0;
+    if (++nr == kLT) {
+      nt = tile + ntx;
+      nr = 0;
+    }
   }
-  return (int)(((long long)nt * kPerim + perim_slot(nr, nc)) << 1);
+  if (nt != tile) return (uint32_t)(((long long)nt * kPerim + perim_slot(nr, nc)) << 1);
+  return kPend | (uint32_t)(nr * kLT + nc);
 }
 
 // Follows border-map entries to a label.
@@ -335,7 +296,7 @@ __global__ void __launch_bounds__(kLabelThreads, 2) label_tile_kernel(Imgs I, co
                                                                    int2* __restrict__ exits_f, int2* __restrict__ exits_v,
                                                                    int* __restrict__ n_exits, unsigned* status) {
   __shared__ uint8_t fl[kLT][kLT];
-  __shared__ uint16_t st[2][kLTN];
+  __shared__ uint32_t st[2][kLTN];
   __shared__ TileRanks R;
   const LabelTile g = label_tile_of(I, blockIdx.x);
   const bool d = I.dual[g.b];
@@ -346,9 +307,43 @@ __global__ void __launch_bounds__(kLabelThreads, 2) label_tile_kernel(Imgs I, co
   load_flow_tile(flow, g, fl, threadIdx.x, blockDim.x);
   __syncthreads();
   tile_ranks(fl, g, I, F.off, V.off, R);
-  tile_resolve(fl, st, F.perim != nullptr, V.perim != nullptr, status);
+  __syncthreads();
   const int c = threadIdx.x % kLT, rb = threadIdx.x / kLT;
   const int ntx = label_ntx(g);
+  const bool do_f = F.perim != nullptr, do_v = V.perim != nullptr;
+  // initial states; bit 2k + side of `pend`: the state of cell k is a pointer
+  unsigned pend = 0;
+#pragma unroll
+  for (int k = 0; k < kTileCells; ++k) {
+    const int r = rb + 16 * k, i = r * kLT + c;
+    const int y = g.y0 + r, x = g.x0 + c;
+    uint32_t a = 1u, b = 1u;  // cells outside the image: never reached, never written
+    if (do_f && y <= g.H && x <= g.W) a = tile_init<true>(fl, R, F.lab, r, c, blockIdx.x, ntx);
+    if (do_v && y < g.H && x < g.W) b = tile_init<false>(fl, R, V.lab, r, c, blockIdx.x, ntx);
+    st[0][i] = a;
+    st[1][i] = b;
+    pend |= (unsigned)st_pending(a) << (2 * k) | (unsigned)st_pending(b) << (2 * k + 1);
+  }
+  __syncthreads();
+  {  // barrier-free pointer jumping of this thread's pending cells (only this
+     // thread writes its cells' states; other threads read them at any time)
+    volatile uint32_t* vs = &st[0][0];
+    for (int it = 0; pend; ++it) {
+      if (it >= kLTN) {  // a path is at most kLTN cells long inside a tile
+        set_status(status, kStatusWalkCap);
+        break;
+      }
+#pragma unroll
+      for (int q = 0; q < 2 * kTileCells; ++q) {
+        if (!((pend >> q) & 1u)) continue;
+        const int side = (q & 1) * kLTN, i = side + (rb + 16 * (q >> 1)) * kLT + c;
+        const uint32_t w = vs[side + (vs[i] & kCellMask)];
+        vs[i] = w;
+        if (!st_pending(w)) pend &= ~(1u << q);
+      }
+    }
+  }
+  // this thread's own states are final now (read back from shared memory)
   const bool border_c = c == 0 || c == kLT - 1;
   // cells of this thread whose path leaves the tile, on a side whose labels
   // this image outputs: bit 2k (faces) and 2k + 1 (vertices); all of them are
@@ -356,29 +351,29 @@ __global__ void __launch_bounds__(kLabelThreads, 2) label_tile_kernel(Imgs I, co
   unsigned xm = 0;
 #pragma unroll
   for (int k = 0; k < kTileCells; ++k) {
-    const int r = rb + 16 * k, i = r * kLT + c;
-    const int y = g.y0 + r, x = g.x0 + c;
-    if (F.perim && of && y <= g.H && x <= g.W && (st[0][i] & kExit)) xm |= 1u << (2 * k);
-    if (V.perim && ov && y < g.H && x < g.W && (st[1][i] & kExit)) xm |= 2u << (2 * k);
+    const int y = g.y0 + rb + 16 * k, x = g.x0 + c;
+    const int i = (rb + 16 * k) * kLT + c;
+    if (do_f && of && y <= g.H && x <= g.W && !(st[0][i] & 1u)) xm |= 1u << (2 * k);
+    if (do_v && ov && y < g.H && x < g.W && !(st[1][i] & 1u)) xm |= 2u << (2 * k);
   }
   int pf, pv;
   block_reserve2(n_exits + 0, __popc(xm & 0x55u), n_exits + 1, __popc(xm & 0xAAu), pf, pv);
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < kTileCells; ++k) {
-    const int r = rb + 16 * k, i = r * kLT + c;
+    const int r = rb + 16 * k;
     const int y = g.y0 + r, x = g.x0 + c;
     const long long gidx = g.base + (long long)r * g.Nx + c;
     const bool border = border_c || r == 0 || r == kLT - 1;
     const long long po = (long long)blockIdx.x * kPerim + perim_slot(r, c);
-    if (F.perim && y <= g.H && x <= g.W) {
+    if (do_f && y <= g.H && x <= g.W) {
       // odd: (label << 1) | 1 of a path ending in the tile; even: exit entry
-      const int ef = state_entry<true>(st[0][i], fl, R, F.lab, blockIdx.x, ntx);
+      const int ef = (int)st[0][r * kLT + c];
       if (border) F.perim[po] = ef;
       if (of && (ef & 1)) of[(long long)y * g.Nx + x] = ef >> 1;
       if ((xm >> (2 * k)) & 1u) exits_f[pf++] = make_int2((int)gidx, ef);
     }
-    if (V.perim && y < g.H && x < g.W) {
-      const int ev = state_entry<false>(st[1][i], fl, R, V.lab, blockIdx.x, ntx);
+    if (do_v && y < g.H && x < g.W) {
+      const int ev = (int)st[1][r * kLT + c];
       if (border) V.perim[po] = ev;
       if (ov && (ev & 1)) ov[(long long)y * g.W + x] = ev >> 1;
       if ((xm >> (2 * k + 1)) & 1u) exits_v[pv++] = make_int2((int)gidx, ev);

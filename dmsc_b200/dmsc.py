@@ -93,25 +93,66 @@ class MSComplex:
     def offset_sad_pts_yx(self):
         return self.to_coordinates_yx(self.sad_pts)
 
-    def get_ridge(self, saddle_idx: int, split_arcs=False):
-        """CSR slice of one saddle's ridge (dmsc/dmsc.py:132-143)."""
-        start = self.ridge_offsets[saddle_idx]
-        end = self.ridge_offsets[saddle_idx + 1] if saddle_idx + 1 < len(self.ridge_offsets) else len(self.ridges)
-        pts = self.ridges[start:end]
+    # Host copies of the CSR offsets, read from the device once on first use
+    # (one transfer per array instead of one synchronisation per slice).
+    def _host_offsets(self, name: str) -> list:
+        cache = self.__dict__.setdefault("_host_cache", {})
+        if name not in cache:
+            cache[name] = getattr(self, name).tolist()
+        return cache[name]
+
+    def _arc(self, pts_name: str, off_name: str, aoff_name: str, saddle_idx: int, split_arcs: bool):
+        off = self._host_offsets(off_name)
+        pts = getattr(self, pts_name)
+        saddle_idx = int(saddle_idx)
+        start = off[saddle_idx]
+        end = off[saddle_idx + 1] if saddle_idx + 1 < len(off) else len(pts)
+        seg = pts[start:end]
         if split_arcs:
-            split = self.ridge_arc_offsets[saddle_idx]
-            return pts[: split - start], pts[split - start: end - start]
-        return pts
+            split = self._host_offsets(aoff_name)[saddle_idx]
+            return seg[: split - start], seg[split - start: end - start]
+        return seg
+
+    def get_ridge(self, saddle_idx: int, split_arcs=False):
+        """CSR slice of one saddle's ridge (dmsc/dmsc.py:132-143): the same
+        slices, as views of ``ridges``; the offsets are read once per complex,
+        so slicing does not synchronise with the device."""
+        return self._arc("ridges", "ridge_offsets", "ridge_arc_offsets", saddle_idx, split_arcs)
 
     def get_valley(self, saddle_idx: int, split_arcs=False):
-        """CSR slice of one saddle's valley (dmsc/dmsc.py:145-156)."""
-        start = self.valley_offsets[saddle_idx]
-        end = self.valley_offsets[saddle_idx + 1] if saddle_idx + 1 < len(self.valley_offsets) else len(self.valleys)
-        pts = self.valleys[start:end]
-        if split_arcs:
-            split = self.valley_arc_offsets[saddle_idx]
-            return pts[: split - start], pts[split - start: end - start]
-        return pts
+        """CSR slice of one saddle's valley (dmsc/dmsc.py:145-156); see get_ridge."""
+        return self._arc("valleys", "valley_offsets", "valley_arc_offsets", saddle_idx, split_arcs)
+
+    def _arcs(self, pts_name: str, off_name: str, aoff_name: str, saddle_idx):
+        pts, off, aoff = getattr(self, pts_name), getattr(self, off_name), getattr(self, aoff_name)
+        idx = torch.as_tensor(saddle_idx, dtype=torch.int64, device=off.device).reshape(-1)
+        n = len(off) - 1
+        if idx.numel() and n > 0:
+            idx = torch.where(idx < 0, idx + n, idx)
+        start = off[idx].to(torch.int64)
+        length = off[idx + 1].to(torch.int64) - start
+        new_off = torch.zeros(idx.numel() + 1, dtype=torch.int64, device=off.device)
+        torch.cumsum(length, 0, out=new_off[1:])
+        hl = self._host_offsets(off_name)
+        total = int(sum(hl[i + 1] - hl[i] for i in idx.tolist())) if idx.numel() else 0
+        # position of every output cell in `pts`: its arc's start + rank inside the arc
+        seg = torch.repeat_interleave(torch.arange(idx.numel(), device=off.device), length, output_size=total)
+        pos = start[seg] + torch.arange(total, device=off.device) - new_off[:-1][seg]
+        cells = pts[pos]
+        first = (aoff[idx].to(torch.int64) - start) + new_off[:-1]
+        return cells, new_off.to(torch.int32), first.to(torch.int32)
+
+    def get_ridges(self, saddle_idx):
+        """Ridges of many saddles at once (batched form of get_ridge):
+        ``(cells, offsets, arc_offsets)`` in CSR layout over the given saddle
+        indices, with ``cells[offsets[k]:offsets[k+1]] == get_ridge(i_k)`` and
+        ``arc_offsets[k]`` the end of its first arc. One gather on the
+        device."""
+        return self._arcs("ridges", "ridge_offsets", "ridge_arc_offsets", saddle_idx)
+
+    def get_valleys(self, saddle_idx):
+        """Valleys of many saddles at once (batched form of get_valley)."""
+        return self._arcs("valleys", "valley_offsets", "valley_arc_offsets", saddle_idx)
 
     def __iter__(self):
         # The 19 tensors in field order, as the reference's astuple-based

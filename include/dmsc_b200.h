@@ -212,25 +212,50 @@ int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n);
    pointer), returns the number written. */
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n);
 
+/* Failure handling (no counterpart in the reference). Every device loop of
+   the pipeline has a bound that no input reaches: pairing rounds (extrema of
+   a side + 2), replay rounds (saddles + 2), geometry expansion levels
+   (saddles + 4), union-find searches and retries (extrema + 2), V-path walks
+   (cells) and chain walks (saddles + 1). A loop that reaches its bound stops,
+   leaves the device state consistent (undecided saddles become cycles,
+   pending cancellations are dropped), sets a bit of a device status word,
+   and the call returns DMSC_B200_ERR_ITERATION_CAP at its next readback;
+   nothing traps. dmsc_b200_set_loop_caps() lowers the pairing-round,
+   replay-round and expansion-level bounds of the following calls to the given
+   values (0 = the normal bound) so that tests can make them run out; the
+   context stays usable after such an error. */
+int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_rounds, int emit_levels);
+
+/* Host waits inside a call poll an event; after `seconds` (default 600) they
+   give up with DMSC_B200_ERR_CUDA. Work may still be running on the device
+   then: destroy the context instead of reusing it. */
+int dmsc_b200_set_wait_timeout(dmsc_b200_context* ctx, double seconds);
+
 /* No counterpart in the reference. For callers that cannot allocate device
    memory at call time -- code running while a stream is captured into a CUDA
    graph, fixed-memory real-time hosts, or plugins whose framework hands out
    only input and output buffers -- this computes the discrete gradient
-   (grad_indices) and the ascending lists of critical minima (vertices),
-   saddles (edges) and maxima (faces) of one H x W image without allocating:
-   its scratch is a fixed 8 MiB static device array of the library (about
-   2 bytes per index (H+1)*(W+1) plus 24 bytes per 32-index row segment, so
-   up to roughly 1900 x 1900 images); larger images return
-   DMSC_B200_ERR_TOO_LARGE.
+   (grad_indices) and the ascending lists of critical vertices, edges and
+   faces of one H x W image without allocating. In the primal the critical
+   vertices are the minima and the critical faces the maxima; with
+   DMSC_B200_DUAL the roles swap (vertices are the maxima, faces the minima),
+   as in the reference's dual outputs. Its scratch is a fixed 8 MiB static
+   device array of the library: 2 bytes per index (H+1)*(W+1) plus 24 bytes
+   per 32-index row segment, each of its 8 parts rounded up to 256 bytes --
+   about 2.75 bytes per index, so square images up to 1743 x 1743 fit
+   (1744 x 1744 does not). Larger images return DMSC_B200_ERR_TOO_LARGE
+   before any buffer is touched.
    `grad_out`    : int32[4*(H+1)*(W+1)], 16-byte aligned.
-   `mins_out`    : int32[H*W] capacity; `saddles_out`: int32[H*(W+1)+(H+1)*W];
-   `maxes_out`   : int32[(H+1)*(W+1)]; `counts_out`: int32[3] = (#mins,
-                   #saddles, #maxima). All device pointers; only DMSC_B200_DUAL
-                   is read from `flags`.
-   The first call on a device looks up the static array's device address and
-   uploads a table; make it before any stream capture. Every call shares the
-   one scratch array (which keeps the last call's contents), so calls that
-   overlap on the GPU race: serialise them. */
+   `mins_out`    : critical vertices, int32[H*W] capacity;
+   `saddles_out` : critical edges, int32[H*(W+1)+(H+1)*W];
+   `maxes_out`   : critical faces, int32[(H+1)*(W+1)];
+   `counts_out`  : int32[3] = (#vertices, #edges, #faces). All device
+                   pointers; only DMSC_B200_DUAL is read from `flags`.
+   The first call on a device looks up the static array's device address,
+   uploads a table and waits for the device to finish (so any stream may make
+   it); make it before any stream capture. Every call shares the one scratch
+   array (which keeps the last call's contents), so calls that overlap on the
+   GPU race: serialise them. */
 int dmsc_b200_critical_cells_static(const float* image, int H, int W, unsigned flags, int32_t* grad_out,
                                     int32_t* mins_out, int32_t* saddles_out, int32_t* maxes_out,
                                     int32_t* counts_out, void* stream);

@@ -372,6 +372,7 @@ typedef struct {
   int N2;
   const int* base_len;
   int overflow;
+  int len_overflow; /* a merged path longer than INT32_MAX cells */
 } dag_t;
 
 /* MergePaths (cpu/arcs_simplification.hxx:378-392) */
@@ -385,7 +386,10 @@ static path_ref merge_paths(dag_t* g, path_ref p1, path_ref p2) {
   }
   int l1 = (p1.id < g->N2) ? g->base_len[p1.id] : g->nodes[p1.id - g->N2].total_len;
   int l2 = (p2.id < g->N2) ? g->base_len[p2.id] : g->nodes[p2.id - g->N2].total_len;
-  dag_node nd = {p1.id, p2.id, p1.fwd, p2.fwd, l1 + l2};
+  /* the reference sums these lengths in int (arcs_simplification.hxx:385);
+     a sum past INT32_MAX makes its offsets negative and the call fail */
+  if ((int64_t)l1 + l2 > 2147483647LL || l1 < 0 || l2 < 0) g->len_overflow = 1;
+  dag_node nd = {p1.id, p2.id, p1.fwd, p2.fwd, (int)(((int64_t)l1 + l2) & 0x7fffffff)};
   g->nodes[g->n] = nd;
   path_ref r = {(int)(g->n + g->N2), 1};
   g->n++;
@@ -476,7 +480,7 @@ typedef struct {
 
 typedef struct {
   field_out f[NF_ALL];
-  int status; /* 0 ok, 1 dag overflow, 2 invalid input, 3 sentinel saddle */
+  int status; /* 0 ok, 1 dag overflow, 2 invalid input, 3 sentinel saddle, 4 int32 geometry overflow */
   char msg[256];
 } oracle_result;
 
@@ -933,7 +937,7 @@ void* dmsc_oracle_run(const float* img, int H, int W, float thr, int flags) {
       }
       int64_t cap = 5LL * ncl;
       if (cap < (1LL << 18)) cap = 1LL << 18;
-      dag_t g = {(dag_node*)xmalloc(cap, sizeof(dag_node)), 0, cap, N2, base_len, 0};
+      dag_t g = {(dag_node*)xmalloc(cap, sizeof(dag_node)), 0, cap, N2, base_len, 0, 0};
       int32_t* dbgc = (int32_t*)xmalloc(3LL * ncl, sizeof(int32_t));
       if (traced) {
         int* co = (int*)xmalloc(ncl, sizeof(int));
@@ -1007,6 +1011,21 @@ void* dmsc_oracle_run(const float* img, int H, int W, float thr, int flags) {
       }
       for (int i = 0; i < N2; ++i) fin_off[i + 1] = fin_off[i] + fin_len[i];
       int64_t total = fin_off[N2];
+      const int geom_failed = g.len_overflow || total > 2147483647LL;
+      if (geom_failed) {
+        /* the reference's int32 prefix sums go negative here
+           (arcs_simplification.hxx:114, 140, 150-155) and it fails with
+           "Trying to create tensor with negative dimension"; stop the same
+           way, before allocating the arena */
+        R->status = 4;
+        snprintf(R->msg, sizeof R->msg, "arc geometry of %lld cells exceeds int32 offsets",
+                 (long long)(g.len_overflow ? -1 : total));
+        for (int i = 0; i < N2; ++i) {
+          fin_len[i] = 0;
+          fin_off[i + 1] = 0;
+        }
+        total = 0;
+      }
       int32_t* out = (int32_t*)xmalloc(total, sizeof(int32_t));
       const int32_t* old = side == 0 ? flat_max : flat_min;
       /* per-side alive is combined below, after both sides ran */
@@ -1035,7 +1054,7 @@ void* dmsc_oracle_run(const float* img, int H, int W, float thr, int flags) {
             A[a].target = parent[T];
             A[a].offset = (int)fin_off[2 * i + a];
             A[a].length = fin_len[2 * i + a];
-            write_geom(&g, fin_path[2 * i + a], out, fin_off[2 * i + a], old, base_off);
+            if (!geom_failed) write_geom(&g, fin_path[2 * i + a], out, fin_off[2 * i + a], old, base_off);
           }
         }
       }

@@ -231,3 +231,107 @@ def test_scatter_edge_cases():
     assert torch.equal(out.cpu().reshape(-1), exp)
     empty = scatter_pair_grads(plus[:0], minus[:0], g[:0], (3, 3))
     assert torch.equal(empty.cpu(), torch.zeros(3, 3))
+
+
+def _fd_check(loss_from_pairs, crop, h=1e-4):
+    """Gradient of ``loss_from_pairs(p, image, side, ppairs)`` through
+    persistence_pairs against FP64 central differences of the same function
+    evaluated on FP64 values of the pairs found at each perturbed field;
+    pixels whose pairing (or selected set) changes within the step are
+    skipped. Returns (max abs error on stable pixels, gradient scale,
+    fraction of stable pixels)."""
+    from dmsc_b200.autograd import persistence_pairs
+
+    x = crop.cuda().requires_grad_(True)
+    pp = persistence_pairs(x, -1.0)
+    loss_from_pairs(pp.persistence, pp.image, pp.side, pp.ppairs).sum().backward()
+    an = x.grad.double().cpu().reshape(-1)
+
+    def eval64(b32):
+        q = persistence_pairs(b32.cuda(), -1.0)
+        img, side, ppairs = q.image.cpu(), q.side.cpu(), q.ppairs.cpu()
+        plus, minus = q.plus_pixel.cpu().long(), q.minus_pixel.cpu().long()
+        ok = plus >= 0
+        flat = b32.double().reshape(b32.shape[0], -1)
+        p64 = torch.full((plus.numel(),), -1.0, dtype=torch.float64)
+        p64[ok] = flat[img[ok], plus[ok]] - flat[img[ok], minus[ok]]
+        L = loss_from_pairs(p64, img, side, ppairs, n_images=b32.shape[0])
+        # what the losses select: every pair, whether it is under the
+        # denoising cut, and the five most persistent pairs of each side
+        sig = [set() for _ in range(b32.shape[0])]
+        best = {}
+        for b, s, a, m, v in zip(img.tolist(), side.tolist(), plus.tolist(), minus.tolist(), p64.tolist()):
+            sig[b].add((s, a, m, v < 0.1))
+            best.setdefault((b, s), []).append((-v, a, m))
+        for (b, s), lst in best.items():
+            sig[b].add(("top", s, tuple((a, m) for _, a, m in sorted(lst)[:5])))
+        return L, sig
+
+    _, base_sig = eval64(crop.unsqueeze(0))
+    N = crop.numel()
+    fd = torch.zeros(N, dtype=torch.float64)
+    stable = torch.zeros(N, dtype=torch.bool)
+    chunk = 512
+    base64 = crop.double()
+    for s in range(0, N, chunk):
+        idx = torch.arange(s, min(N, s + chunk))
+        k = idx.numel()
+        b64 = base64.reshape(1, -1).repeat(2 * k, 1)
+        b64[torch.arange(k), idx] += h
+        b64[torch.arange(k, 2 * k), idx] -= h
+        b32 = b64.reshape(2 * k, *crop.shape).float()
+        L, sigs = eval64(b32)
+        b64 = b32.double().reshape(2 * k, -1)
+        steps = b64[torch.arange(k), idx] - b64[torch.arange(k, 2 * k), idx]
+        fd[idx] = (L[:k] - L[k:]) / steps
+        for j in range(k):
+            stable[idx[j]] = sigs[j] == base_sig[0] and sigs[k + j] == base_sig[0]
+    scale = an.abs().max()
+    return float((fd - an)[stable].abs().max()), float(scale), float(stable.float().mean())
+
+
+@pytest.mark.parametrize("name", ["denoise_min", "denoise_max", "betti_min", "betti_max", "segmentation"])
+def test_loss_library_fp64_finite_differences(name):
+    """Each loss of dmsc_b200.losses against FP64 central differences (step
+    1e-4) on a tie-free 48 x 48 crop, within 1e-5 of the gradient's scale."""
+    from dmsc_b200 import losses
+
+    fns = {
+        "denoise_min": lambda p, i, s, q, n_images=None: losses.denoising_loss_from_pairs(p, i, s, q, 0.1, "min",
+                                                                                            n_images),
+        "denoise_max": lambda p, i, s, q, n_images=None: losses.denoising_loss_from_pairs(p, i, s, q, 0.1, "max",
+                                                                                            n_images),
+        "betti_min": lambda p, i, s, q, n_images=None: losses.betti_loss_from_pairs(p, i, s, q, 3, "min", 1.0,
+                                                                                      n_images),
+        "betti_max": lambda p, i, s, q, n_images=None: losses.betti_loss_from_pairs(p, i, s, q, 2, "max", 0.5,
+                                                                                      n_images),
+        "segmentation": lambda p, i, s, q, n_images=None: (
+            losses.betti_loss_from_pairs(p, i, s, q, 3, "min", 1.0, n_images)
+            + losses.betti_loss_from_pairs(p, i, s, q, 2, "max", 1.0, n_images)),
+    }
+    field = tie_free_field(512, 512, seed=23, check=False)
+    crop = field[100:148, 260:308].contiguous()
+    assert torch.unique(crop).numel() == crop.numel()
+    err, scale, frac = _fd_check(fns[name], crop)
+    assert frac > 0.95
+    assert scale > 0
+    assert err <= 1e-5 * scale, (err, scale)
+
+
+def test_loss_library_public_forms_match_pairs():
+    """The image-level forms equal their *_from_pairs forms on one forward,
+    and segmentation_loss is the sum of the two side losses."""
+    from dmsc_b200 import losses
+    from dmsc_b200.autograd import persistence_pairs
+
+    x = torch.stack([tie_free_field(96, 96, seed=s, check=False) for s in (4, 5)]).cuda()
+    pp = persistence_pairs(x, -1.0)
+    a = losses.betti_loss(x, [2, 4], "min", reduction="none")
+    b = losses.betti_loss_from_pairs(pp.persistence, pp.image, pp.side, pp.ppairs, [2, 4], "min", 1.0, 2)
+    assert torch.equal(a, b)
+    s = losses.segmentation_loss(x, n_basins=[2, 4], n_peaks=3, reduction="none")
+    c = b + losses.betti_loss_from_pairs(pp.persistence, pp.image, pp.side, pp.ppairs, 3, "max", 1.0, 2)
+    assert torch.allclose(s, c)
+    d = losses.denoising_loss(x, 0.1, "both")
+    from dmsc_b200.autograd import topological_loss
+    assert torch.allclose(d, topological_loss(x, -1.0, 0.1))

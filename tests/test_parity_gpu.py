@@ -140,11 +140,62 @@ def test_too_large_raises():
         compute_dmsc(img, 0.0)
 
 
-def test_full_size_4096_primal(oracle_mod):
-    """The headline 4096 x 4096 bump workload, primal, threshold 0.05."""
+@pytest.mark.parametrize("dual,thr", [(False, 0.0), (False, 0.05), (True, 0.0), (True, 0.05)])
+def test_full_size_4096(oracle_mod, dual, thr):
+    """The headline 4096 x 4096 bump workload (2000 bumps, sigma U[4, 64],
+    N(0, 0.02^2) noise), all four (orientation, threshold) variants."""
     from dmsc_b200.synthetic import field_4096_bumps
 
-    img = field_4096_bumps(seed=1234, device="cuda")
-    got = gpu_run(img, 0.05, [True] * 5, False)
-    exp = oracle_mod.run(img.cpu(), 0.05, True, False, True, True, True, True)
+    img = field_4096_bumps(seed=1234)
+    got = gpu_run(img, thr, [True] * 5, dual)
+    exp = oracle_mod.run(img, thr, True, dual, True, True, True, True)
     assert diff_fields(got, exp) == []
+
+
+def test_uniform_2048(oracle_mod):
+    """i.i.d. U[0, 1) at 2048^2, the density of the 16384^2 worst case: at
+    threshold 0 every output bit for bit; at 0.5 the simplified ridges grow
+    past int32 offsets (7e9 cells already at 1024^2), where the reference's
+    offsets go negative and it fails, so the GPU must raise, and without arcs
+    every other output must match."""
+    from dmsc_b200.synthetic import field_uniform
+
+    img = field_uniform(2048, seed=99)
+    exp = oracle_mod.run(img, 0.0, True, False, True, True, True, True)
+    assert diff_fields(gpu_run(img, 0.0, [True] * 5, False), exp) == []
+    exp = oracle_mod.run(img, 0.5, True, False, False, False, True, True)
+    assert diff_fields(gpu_run(img, 0.5, [True, False, False, True, True], False), exp) == []
+    with pytest.raises(RuntimeError, match="exceeds int32 offsets"):
+        oracle_mod.run(img, 0.5, True, False, True, True, True, True)
+    with pytest.raises(RuntimeError, match="exceeds int32 offsets"):
+        gpu_run(img, 0.5, [True] * 5, False)
+    # the context stays usable after the overflow
+    assert diff_fields(gpu_run(img, 0.0, [True] * 5, False), oracle_mod.run(img, 0.0, True, False, True, True, True,
+                                                                          True)) == []
+
+
+def test_uniform_512_heavy_cancellation(oracle_mod):
+    """U[0, 1) at 512^2 and threshold 0.5: almost every pair cancels and the
+    ridges merge into 2.7e8 cells, just inside int32 offsets."""
+    from dmsc_b200.synthetic import field_uniform
+
+    img = field_uniform(512, seed=1234)
+    exp = oracle_mod.run(img, 0.5, True, False, True, True, True, True)
+    got = gpu_run(img, 0.5, [True] * 5, False)
+    assert diff_fields(got, exp) == []
+
+
+@pytest.mark.parametrize("dual", ["primal", "dual"])
+@pytest.mark.parametrize("flt,thr", [("raw", -1.0), ("flt", 0.15)])
+def test_reference_format_fixtures(dual, flt, thr):
+    """The regenerated fixtures in the reference's own torch.save format
+    (tests/golden/reference_format), every field bit for bit."""
+    import os
+
+    from dmsc_b200 import compute_dmsc
+
+    d = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_format")
+    img = torch.load(os.path.join(d, "landscape_32x32.pt"))
+    gt = torch.load(os.path.join(d, f"ms_st_{dual}_{flt}.pt"), weights_only=False)
+    ms = compute_dmsc(img.cuda(), thr, return_gradient=True, is_dual=dual == "dual")
+    assert diff_fields([getattr(ms, k) for k in FIELDS], [gt[k] for k in FIELDS]) == []

@@ -67,3 +67,66 @@ def test_static_rejects_oversize():
     d = ctypes.c_void_p(img.data_ptr())
     rc = lib.dmsc_b200_critical_cells_static(d, 4096, 4096, 0, d, d, d, d, d, None)
     assert rc == 2  # DMSC_B200_ERR_TOO_LARGE, before touching any buffer
+
+
+def test_static_largest_accepted_size():
+    """1743 x 1743 is the largest square image the 8 MiB scratch takes; its
+    scratch ends within a few KB of the array's end."""
+    from dmsc_b200 import _lib, extract_dmsc
+
+    lib = _lib.load()
+    img = torch.rand((1743, 1743), generator=torch.Generator().manual_seed(17)).cuda()
+    ref = extract_dmsc(img, -1.0, True, False, False, False, False, False)
+    for call in range(2):
+        grad, mins, sads, maxs = _static_call(lib, img, False)
+        assert torch.equal(grad, ref[10].cpu()), call
+        assert torch.equal(mins, ref[2].cpu()), call
+        assert torch.equal(maxs, ref[1].cpu()), call
+        assert torch.equal(sads, torch.sort(ref[3].cpu()).values), call
+
+
+def test_static_rejects_first_size_over():
+    from dmsc_b200 import _lib
+
+    lib = _lib.load()
+    img = torch.zeros((1744, 1744), device="cuda")
+    d = ctypes.c_void_p(img.data_ptr())
+    rc = lib.dmsc_b200_critical_cells_static(d, 1744, 1744, 0, d, d, d, d, d, None)
+    assert rc == 2  # DMSC_B200_ERR_TOO_LARGE
+
+
+_SIDE_STREAM_SCRIPT = r"""
+import sys
+sys.path.insert(0, {root!r})
+import torch
+from tests.test_zz_no_alloc import _static_call
+from dmsc_b200 import _lib, extract_dmsc
+from dmsc_b200.synthetic import field_256_bumps
+lib = _lib.load()
+img = field_256_bumps(seed=23).cuda()
+torch.cuda.synchronize()
+side = torch.cuda.Stream()
+with torch.cuda.stream(side):  # the first call of this process runs on a non-blocking side stream
+    grad, mins, sads, maxs = _static_call(lib, img, False)
+ref = extract_dmsc(img, -1.0, True, False, False, False, False, False)
+assert torch.equal(grad, ref[10].cpu())
+assert torch.equal(mins, ref[2].cpu()) and torch.equal(maxs, ref[1].cpu())
+assert torch.equal(sads, torch.sort(ref[3].cpu()).values)
+print("side-stream first call ok")
+"""
+
+
+def test_static_first_call_on_side_stream():
+    """The first call of a process sets up the static arrays (device address,
+    face-pairing table); it must be correct when made on a side stream that is
+    not ordered after the legacy default stream. Run in a fresh process so the
+    call really is the first."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _SIDE_STREAM_SCRIPT.format(root=root)], capture_output=True, text=True,
+                       timeout=300, cwd=root)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "side-stream first call ok" in r.stdout
