@@ -34,6 +34,9 @@ EXPORTS = (
     "dmsc_b200_loop_counts",
     "dmsc_b200_pairing_timeline",
     "dmsc_b200_set_loop_caps",
+    "dmsc_b200_set_tuning",
+    "dmsc_b200_get_tuning",
+    "dmsc_b200_tuning_limits",
     "dmsc_b200_set_wait_timeout",
     "dmsc_b200_critical_cells_static",
 )
@@ -49,6 +52,11 @@ class Sizes(ctypes.Structure):
         "max_pts", "min_pts", "sad_pts", "e_max_rows", "e_min_rows", "p_max", "p_min", "ppairs_max", "ppairs_min",
         "grad_indices", "peaks_h", "peaks_w", "ridges", "ridge_offsets", "ridge_arc_offsets", "basins_h", "basins_w",
         "valleys", "valley_offsets", "valley_arc_offsets")]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("grad_shape", "label_shape", "pair_blocks_per_sm",
+                                            "replay_blocks_per_sm", "emit_blocks_per_sm")]
 
 
 class Outputs(ctypes.Structure):
@@ -114,6 +122,12 @@ def load():
         lib.dmsc_b200_pairing_timeline.restype = ctypes.c_int
         lib.dmsc_b200_set_loop_caps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         lib.dmsc_b200_set_loop_caps.restype = ctypes.c_int
+        lib.dmsc_b200_set_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
+        lib.dmsc_b200_set_tuning.restype = ctypes.c_int
+        lib.dmsc_b200_get_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
+        lib.dmsc_b200_get_tuning.restype = ctypes.c_int
+        lib.dmsc_b200_tuning_limits.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        lib.dmsc_b200_tuning_limits.restype = ctypes.c_int
         lib.dmsc_b200_set_wait_timeout.argtypes = [ctypes.c_void_p, ctypes.c_double]
         lib.dmsc_b200_set_wait_timeout.restype = ctypes.c_int
         lib.dmsc_b200_critical_cells_static.argtypes = [
@@ -166,6 +180,24 @@ class Context:
         """Lowers the device loop bounds of the following calls (0 = normal)."""
         self.check(self.lib.dmsc_b200_set_loop_caps(self.h, pair_rounds, replay_rounds, emit_levels),
                    "dmsc_b200_set_loop_caps")
+
+    def set_tuning(self, **kw):
+        t = self.get_tuning()
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        self.check(self.lib.dmsc_b200_set_tuning(self.h, ctypes.byref(t)), "dmsc_b200_set_tuning")
+
+    def get_tuning(self) -> Tuning:
+        t = Tuning()
+        self.check(self.lib.dmsc_b200_get_tuning(self.h, ctypes.byref(t)), "dmsc_b200_get_tuning")
+        return t
+
+    def tuning_limits(self) -> dict:
+        buf = (ctypes.c_int * 5)()
+        if self.lib.dmsc_b200_tuning_limits(self.h, buf, 5) != 5:
+            raise RuntimeError("dmsc_b200_tuning_limits failed")
+        return dict(zip(("grad_shapes", "label_shapes", "pair_blocks_per_sm", "replay_blocks_per_sm",
+                         "emit_blocks_per_sm"), list(buf)))
 
     def set_wait_timeout(self, seconds: float):
         self.check(self.lib.dmsc_b200_set_wait_timeout(self.h, float(seconds)), "dmsc_b200_set_wait_timeout")

@@ -159,7 +159,12 @@ struct dmsc_b200_context {
   // host wait deadline (seconds) and test-only loop caps (0 = the bounds
   // that every input provably stays within)
   double wait_timeout_s = 600.0;
-  int grad_shape = 1;  // gradient tile shape (index into kGradTY / kGradNT)
+  // tuned launch shapes (dmsc_b200_set_tuning): gradient tile shape (index
+  // into kGradTY / kGradNT), label tile threads (index into kLabelNT), and
+  // the resident blocks per SM of the three persistent kernels (0 = all that fit)
+  int grad_shape = 1;
+  int label_shape = 0;
+  int pair_per_sm = 0, replay_per_sm = 0, emit_per_sm = 0;
   int cap_pair_rounds = 0, cap_replay_rounds = 0, cap_emit_levels = 0;
 };
 
@@ -307,13 +312,15 @@ void mark(dmsc_b200_context* ctx, int k, cudaStream_t st) {
 // Cooperative launch of a persistent kernel: as many blocks as can be
 // co-resident, so grid-wide barriers are safe.
 template <class T>
-void coop_launch(dmsc_b200_context* ctx, void (*kernel)(T), T args, cudaStream_t st, const char* name) {
+void coop_launch(dmsc_b200_context* ctx, void (*kernel)(T), T args, cudaStream_t st, const char* name,
+                 int per_cap = 0) {
   int per = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, 0));
   if (per < 1) {
     set_err(ctx, "%s cannot be made resident", name);
     throw Fail{kErrInternal};
   }
+  if (per_cap > 0 && per_cap < per) per = per_cap;
   void* a[] = {&args};
   CK(cudaLaunchCooperativeKernel((void*)kernel, dim3(per * ctx->num_sms), dim3(256), a, 0, st));
   ++ctx->launches;
@@ -478,7 +485,8 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
 void run_pairing(dmsc_b200_context* ctx, const int* asc, cudaStream_t st) {
   PairArgs2 P;
   for (int si = 0; si < 2; ++si) P.s[si] = pairing_args(ctx, si, ctx->side[si], asc, st);
-  if (ctx->nsad > 0) coop_launch(ctx, pairing_persistent_kernel, P, st, "pairing_persistent_kernel");
+  if (ctx->nsad > 0)
+    coop_launch(ctx, pairing_persistent_kernel, P, st, "pairing_persistent_kernel", ctx->pair_per_sm);
 }
 
 // Persistence, cancellation, thresholded union-find and output ranks of one side.
@@ -897,7 +905,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
         any = any || RA.s[si].n_cancel != nullptr;
       }
     }
-    if (any) coop_launch(ctx, replay_persistent_kernel, RA, st, "replay_persistent_kernel");
+    if (any) coop_launch(ctx, replay_persistent_kernel, RA, st, "replay_persistent_kernel", ctx->replay_per_sm);
     mark(ctx, 8, st);
     // geometry totals stay on the device (read back with the sizes)
     long long* tot = get<long long>(ctx, S_TOT, 8);
@@ -959,8 +967,12 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     int2* exv = V.groups ? get<int2>(ctx, S_EXV, nidx) : nullptr;
     int* nex = get<int>(ctx, S_NEX, 2);
     CK(cudaMemsetAsync(nex, 0, 2 * sizeof(int), st));
-    LK(label_tile_kernel<<<(unsigned)nltile, kLabelThreads, 0, st>>>(I, flow, LF, LV, OF, OV, exf, exv, nex,
-                                                                    ctx->status));
+    if (ctx->label_shape == 1)
+      LK((label_tile_kernel<kLabelNT[1]><<<(unsigned)nltile, kLabelNT[1], 0, st>>>(I, flow, LF, LV, OF, OV, exf, exv,
+                                                                                 nex, ctx->status)));
+    else
+      LK((label_tile_kernel<kLabelNT[0]><<<(unsigned)nltile, kLabelNT[0], 0, st>>>(I, flow, LF, LV, OF, OV, exf, exv,
+                                                                                 nex, ctx->status)));
     LAUNCH_CHECK("label_tile_kernel");
     int per = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, label_exit_kernel<true>, 256, 0));
@@ -1099,7 +1111,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   A.max_levels = capped(ctx->nsad + 4, ctx->cap_emit_levels);
   A.levels = get<int>(ctx, S_STATS, 8) + 4 + si;
   A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline) + (2 + si) * kTimeline;
-  coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel");
+  coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel", ctx->emit_per_sm);
   {
     int per = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel, 256, 0));
@@ -1489,6 +1501,41 @@ int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_
   ctx->cap_replay_rounds = replay_rounds;
   ctx->cap_emit_levels = emit_levels;
   return kOk;
+}
+
+int dmsc_b200_set_tuning(dmsc_b200_context* ctx, const dmsc_b200_tuning* t) {
+  if (!ctx || !t || t->grad_shape < 0 || t->grad_shape >= kGradShapes || t->label_shape < 0 ||
+      t->label_shape >= kLabelShapes || t->pair_blocks_per_sm < 0 || t->replay_blocks_per_sm < 0 ||
+      t->emit_blocks_per_sm < 0)
+    return kErrInvalidArgument;
+  ctx->grad_shape = t->grad_shape;
+  ctx->label_shape = t->label_shape;
+  ctx->pair_per_sm = t->pair_blocks_per_sm;
+  ctx->replay_per_sm = t->replay_blocks_per_sm;
+  ctx->emit_per_sm = t->emit_blocks_per_sm;
+  return kOk;
+}
+
+int dmsc_b200_get_tuning(const dmsc_b200_context* ctx, dmsc_b200_tuning* t) {
+  if (!ctx || !t) return kErrInvalidArgument;
+  t->grad_shape = ctx->grad_shape;
+  t->label_shape = ctx->label_shape;
+  t->pair_blocks_per_sm = ctx->pair_per_sm;
+  t->replay_blocks_per_sm = ctx->replay_per_sm;
+  t->emit_blocks_per_sm = ctx->emit_per_sm;
+  return kOk;
+}
+
+int dmsc_b200_tuning_limits(dmsc_b200_context* ctx, int* out, int n) {
+  if (!ctx || !out) return -1;
+  int v[5] = {kGradShapes, kLabelShapes, 0, 0, 0};
+  if (cudaSetDevice(ctx->device) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v[2], pairing_persistent_kernel, 256, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v[3], replay_persistent_kernel, 256, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v[4], emit_persistent_kernel, 256, 0) != cudaSuccess)
+    return -1;
+  for (int k = 0; k < 5 && k < n; ++k) out[k] = v[k];
+  return 5;
 }
 
 int dmsc_b200_set_wait_timeout(dmsc_b200_context* ctx, double seconds) {

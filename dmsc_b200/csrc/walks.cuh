@@ -231,8 +231,10 @@ __device__ __forceinline__ int tile_label(const TileRanks& R, int j, const int* 
 constexpr uint32_t kPend = 0x40000000u, kCellMask = 0x0FFFu;
 __device__ __forceinline__ bool st_pending(uint32_t v) { return (v >> 30) == 1u; }
 
-constexpr int kLabelThreads = 1024;
-constexpr int kTileCells = kLTN / kLabelThreads;  // 4 cells per thread: rows tid/64 + 16k
+// Threads per label tile (the tuner picks one): each thread owns column
+// tid % 64 of rows tid / 64 + (NT / 64) k, k < 4096 / NT.
+constexpr int kLabelShapes = 2;
+constexpr int kLabelNT[kLabelShapes] = {1024, 512};
 
 // Initial state of a cell of the tile (FACES: face side) at tile position
 // (r, c); the cell is in the image.
@@ -291,13 +293,15 @@ __device__ __forceinline__ int label_ntx(const LabelTile& g) { return (g.W + kLT
 // cells also get their border-map entries; a cell whose path leaves the tile
 // is appended to its side's exit list (global index, entry) and finished by
 // label_exit_kernel once every tile's border map is written.
-__global__ void __launch_bounds__(kLabelThreads, 2) label_tile_kernel(Imgs I, const uint8_t* __restrict__ flow,
+template <int NT>
+__global__ void __launch_bounds__(NT, 2048 / NT) label_tile_kernel(Imgs I, const uint8_t* __restrict__ flow,
                                                                    LabelSide F, LabelSide V, LabelOut OF, LabelOut OV,
                                                                    int2* __restrict__ exits_f, int2* __restrict__ exits_v,
                                                                    int* __restrict__ n_exits, unsigned* status) {
   __shared__ uint8_t fl[kLT][kLT];
   __shared__ uint32_t st[2][kLTN];
   __shared__ TileRanks R;
+  constexpr int kTileCells = kLTN / NT, kStep = NT / kLT;
   const LabelTile g = label_tile_of(I, blockIdx.x);
   const bool d = I.dual[g.b];
   int* of = d ? OF.dual : OF.primal;
@@ -315,7 +319,7 @@ __global__ void __launch_bounds__(kLabelThreads, 2) label_tile_kernel(Imgs I, co
   unsigned pend = 0;
 #pragma unroll
   for (int k = 0; k < kTileCells; ++k) {
-    const int r = rb + 16 * k, i = r * kLT + c;
+    const int r = rb + kStep * k, i = r * kLT + c;
     const int y = g.y0 + r, x = g.x0 + c;
     uint32_t a = 1u, b = 1u;  // cells outside the image: never reached, never written
     if (do_f && y <= g.H && x <= g.W) a = tile_init<true>(fl, R, F.lab, r, c, blockIdx.x, ntx);
@@ -336,7 +340,7 @@ __global__ void __launch_bounds__(kLabelThreads, 2) label_tile_kernel(Imgs I, co
 #pragma unroll
       for (int q = 0; q < 2 * kTileCells; ++q) {
         if (!((pend >> q) & 1u)) continue;
-        const int side = (q & 1) * kLTN, i = side + (rb + 16 * (q >> 1)) * kLT + c;
+        const int side = (q & 1) * kLTN, i = side + (rb + kStep * (q >> 1)) * kLT + c;
         const uint32_t w = vs[side + (vs[i] & kCellMask)];
         vs[i] = w;
         if (!st_pending(w)) pend &= ~(1u << q);
@@ -351,16 +355,16 @@ __global__ void __launch_bounds__(kLabelThreads, 2) label_tile_kernel(Imgs I, co
   unsigned xm = 0;
 #pragma unroll
   for (int k = 0; k < kTileCells; ++k) {
-    const int y = g.y0 + rb + 16 * k, x = g.x0 + c;
-    const int i = (rb + 16 * k) * kLT + c;
+    const int y = g.y0 + rb + kStep * k, x = g.x0 + c;
+    const int i = (rb + kStep * k) * kLT + c;
     if (do_f && of && y <= g.H && x <= g.W && !(st[0][i] & 1u)) xm |= 1u << (2 * k);
     if (do_v && ov && y < g.H && x < g.W && !(st[1][i] & 1u)) xm |= 2u << (2 * k);
   }
   int pf, pv;
-  block_reserve2(n_exits + 0, __popc(xm & 0x55u), n_exits + 1, __popc(xm & 0xAAu), pf, pv);
+  block_reserve2(n_exits + 0, __popc(xm & 0x55555555u), n_exits + 1, __popc(xm & 0xAAAAAAAAu), pf, pv);
 #pragma unroll
   for (int k = 0; k < kTileCells; ++k) {
-    const int r = rb + 16 * k;
+    const int r = rb + kStep * k;
     const int y = g.y0 + r, x = g.x0 + c;
     const long long gidx = g.base + (long long)r * g.Nx + c;
     const bool border = border_c || r == 0 || r == kLT - 1;

@@ -16,7 +16,7 @@ from dataclasses import dataclass, fields
 
 import torch
 
-from . import _lib
+from . import _lib, tuning
 
 
 @dataclass
@@ -216,6 +216,7 @@ def extract_single(img: torch.Tensor, persistence_threshold: float, flags: int, 
     H, W = int(img.shape[0]), int(img.shape[1])
     dev = img.device
     ctx = _lib.context(dev.index if dev.index is not None else torch.cuda.current_device())
+    tuning.apply(ctx, H * W)
     s = stream if stream is not None else torch.cuda.current_stream(dev)
     i32 = dict(dtype=torch.int32, device=dev)
     dual = bool(flags & _lib.DUAL)
@@ -296,6 +297,7 @@ def _batch_raw(images, thresholds, is_dual, flags: int, stream=None, flat=None, 
         flat = images[0].reshape(-1) if B == 1 else torch.cat([x.reshape(-1) for x in images])
     nidx = [(h + 1) * (w + 1) for h, w in zip(Hs, Ws)]
     npx = [h * w for h, w in zip(Hs, Ws)]
+    tuning.apply(ctx, sum(npx))
     pk_n = [p if d else n for p, n, d in zip(npx, nidx, duals)]
     bs_n = [n if d else p for p, n, d in zip(npx, nidx, duals)]
     grad = torch.empty(4 * sum(nidx), **i32) if flags & _lib.RETURN_GRADIENT else None

@@ -226,6 +226,34 @@ int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n);
    context stays usable after such an error. */
 int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_rounds, int emit_levels);
 
+/* Launch shapes (no counterpart in the reference, whose CPU path fixes its
+   blocking at compile time, cpu/gradient.hxx:15 DEFAULT_GRADIENT_BLOCK_SIZE
+   and cpu/cell_groups.hxx:9 CACHE_DEPTH). They change speed only, never an
+   output bit. The Python tuner (dmsc_b200.tuning) sweeps them on the
+   caller's data and sets the fastest per image-size class.
+   grad_shape   : gradient tile of 32 index columns x {31, 63, 127} rows
+                  (threads {256, 256, 512}), 0..2; default 1.
+   label_shape  : 64 x 64 label tiles with {1024, 512} threads, 0..1; default 0.
+   *_blocks_per_sm : resident blocks per SM of the pairing, replay and
+                  geometry-expansion persistent kernels; 0 = as many as fit
+                  (the default); larger values are clamped to what fits. */
+typedef struct {
+  int grad_shape;
+  int label_shape;
+  int pair_blocks_per_sm;
+  int replay_blocks_per_sm;
+  int emit_blocks_per_sm;
+} dmsc_b200_tuning;
+
+int dmsc_b200_set_tuning(dmsc_b200_context* ctx, const dmsc_b200_tuning* tuning);
+int dmsc_b200_get_tuning(const dmsc_b200_context* ctx, dmsc_b200_tuning* tuning);
+
+/* Choices of the tunables on this context's device (host pointer, up to `n`
+   values): number of gradient tile shapes, number of label tile shapes, and
+   the most blocks per SM of the pairing, replay and expansion kernels.
+   Returns the number written or -1. */
+int dmsc_b200_tuning_limits(dmsc_b200_context* ctx, int* out, int n);
+
 /* Host waits inside a call poll an event; after `seconds` (default 600) they
    give up with DMSC_B200_ERR_CUDA. Work may still be running on the device
    then: destroy the context instead of reusing it. */
