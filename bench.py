@@ -367,6 +367,8 @@ def b200_arm(args):
     batched = None if args.batch_images <= 0 else batched_section(args, dev, ctx, dist, world, rank)
     seg_only = segmentation_only_section(args, img, dev, ctx, dist, size)
     diff = None if args.no_diff else diff_section(args, dev, dist)
+    tune = tune_section(args, img, dev, size) if (not args.no_tune and world == 1) else None
+    c3 = c3_section(args, dev, ctx) if (args.c3_size > 0 and world == 1) else None
 
     if rank != 0:
         if dist:
@@ -409,6 +411,10 @@ def b200_arm(args):
     line["segmentation_only"] = seg_only
     if diff is not None:
         line["differentiation"] = diff
+    if tune is not None:
+        line["tuning"] = tune
+    if c3 is not None:
+        line["worst_case_uniform"] = c3
     if world == 1 and not args.no_cpu_baseline:
         cb, exact = cpu_baseline(img.cpu(), gpu_out)
         line["cpu_baseline"] = cb
@@ -604,6 +610,103 @@ def diff_section(args, dev, dist):
     }
 
 
+C3_DIGESTS = os.path.join(ROOT, "tests", "golden", "uniform16384_digests.json")
+
+
+def _digests(outs):
+    import hashlib
+
+    names = ("shape max_pts min_pts sad_pts e_max e_min p_max p_min ppairs_max ppairs_min grad_indices peaks ridges "
+             "ridge_offsets ridge_arc_offsets basins valleys valley_offsets valley_arc_offsets").split()
+    d = {}
+    for n, t in zip(names, outs):
+        a = t.contiguous().cpu().numpy()
+        d[n] = {"shape": list(a.shape), "dtype": str(a.dtype), "sha256": hashlib.sha256(a.tobytes()).hexdigest()}
+    return d
+
+
+def c3_section(args, dev, ctx):
+    """Worst-case critical-point density: one size x size i.i.d. U[0, 1)
+    float32 field (seed 1234, CPU generator), primal, thresholds 0 and 0.5.
+    At 0 every output is produced and checked against the digests of the
+    reference CPU path's outputs on the same field
+    (tests/golden/uniform16384_digests.json, made by
+    tests/golden/make_uniform_digests.py). At 0.5 almost every pair cancels
+    and the simplified arcs exceed int32 offsets, where the reference fails;
+    the full call must raise the same overflow, and the call without arcs
+    (gradient, lists, pairs, labels) is timed and checked. Device time by CUDA
+    events around whole calls, input resident in HBM."""
+    import hashlib
+
+    from dmsc_b200 import extract_dmsc
+    from dmsc_b200.synthetic import field_uniform
+
+    size = args.c3_size
+    img_cpu = field_uniform(size, seed=SEED)
+    in_sha = hashlib.sha256(img_cpu.numpy().tobytes()).hexdigest()
+    img = img_cpu.to(dev)
+    del img_cpu
+    ref = None
+    if os.path.exists(C3_DIGESTS):
+        with open(C3_DIGESTS) as f:
+            ref = json.load(f)
+        if ref.get("size") != size or ref.get("input_sha256") != in_sha:
+            ref = None
+    st = torch.cuda.current_stream(dev)
+    out = {"workload": f"{size}x{size} i.i.d. U[0,1) float32 (seed {SEED}), primal", "input_sha256": in_sha,
+           "runs": {}}
+    for thr, geom in ((0.0, True), (0.5, False), (0.5, True)):
+        ent = {}
+        try:
+            r = extract_dmsc(img, thr, True, False, geom, geom, True, True)  # warm-up (workspace growth)
+            del r
+            torch.cuda.synchronize()
+            times = []
+            for _ in range(2):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                r = extract_dmsc(img, thr, True, False, geom, geom, True, True)
+                e1.record(st)
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1))
+            ms = min(times)
+            ent.update({"ms_per_call": ms, "value": size * size / 1e6 / (ms / 1000.0), "unit": UNIT,
+                        "loops": ctx.loop_counts(),
+                        "sizes": {"max_pts": int(r[1].numel()), "min_pts": int(r[2].numel()),
+                                  "sad_pts": int(r[3].numel()), "ridges": int(r[12].numel()),
+                                  "valleys": int(r[16].numel())}})
+            free, total = torch.cuda.mem_get_info(dev)
+            ent["device_memory_used_gb"] = (total - free) / 1e9
+            rk = str(thr) if geom else f"{thr}_noarcs"
+            if ref is not None and rk in ref and "fields" in ref[rk]:
+                dg = _digests(r)
+                ent["bit_exact_vs_reference"] = all(dg[n] == ref[rk]["fields"][n] for n in dg)
+                ent["reference_seconds"] = ref[rk].get("seconds")
+            del r
+        except RuntimeError as e:
+            ent["error"] = str(e)
+            if ref is not None and "0.5" in ref and "error" in ref["0.5"]:
+                ent["reference_error"] = ref["0.5"]["error"]
+        out["runs"][f"thr={thr},arcs={geom}"] = ent
+        torch.cuda.empty_cache()
+    del img
+    torch.cuda.empty_cache()
+    return out
+
+
+def tune_section(args, img, dev, size):
+    """The launch-shape tuner (dmsc_b200.tuning) on this workload: one
+    variant (is_dual=False, threshold 0.05) of the field, median of 5 runs per
+    candidate; the report gives the default and tuned whole-call device times.
+    The choice stays cached for the rest of the run (the timed steps above
+    ran before it, with the default shapes)."""
+    from dmsc_b200 import compute_dmsc, tuning
+
+    rep = tuning.tune(lambda: compute_dmsc(img, 0.05), size * size, reps=5)
+    return {"workload": f"{size}x{size} field, is_dual=False, threshold 0.05", "choice": rep["choice"],
+            "default_ms": rep["default_ms"], "tuned_ms": rep["tuned_ms"], "stage_medians_ms": rep["stages"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -614,6 +717,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-images", type=int, default=512, help="uneven-batch images per GPU (0: skip)")
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiation workload")
+    ap.add_argument("--c3-size", type=int, default=16384, help="worst-case U[0,1) field size (0: skip)")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape tuner section")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

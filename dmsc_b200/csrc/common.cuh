@@ -61,9 +61,12 @@ __device__ __forceinline__ uint32_t orderable_key(float f) {
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-// Flow codes: one byte per index, the V-path successor of the vertex in the
-// low nibble and of the face in the high nibble: 0 = none (critical or no
-// cell), 1 = left (x-1), 2 = right (x+1), 3 = up (y-1), 4 = down (y+1).
+// Flow codes: one byte per index, the V-path successor of the vertex in
+// bits 0-2 and of the face in bits 4-6: 0 = none (critical or no cell),
+// 1 = left (x-1), 2 = right (x+1), 3 = up (y-1), 4 = down (y+1). Bits 3 and
+// 7 mark the index's H and V edge critical, so the byte also gives the
+// index's criticality: vertex (bits 0-2 zero, for a pixel), H edge, V edge,
+// face (bits 4-6 zero).
 // The gradient kernel writes them; every V-path walk uses them (17 MB at
 // 4096^2, resident in L2) instead of reading the 16 B/index gradient.
 enum : unsigned { kFlowNone = 0, kFlowLeft = 1, kFlowRight = 2, kFlowUp = 3, kFlowDown = 4 };

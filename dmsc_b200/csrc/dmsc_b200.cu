@@ -111,6 +111,7 @@ struct dmsc_b200_context {
   int device = 0;
   std::vector<Buf> bufs;
   Buf cub_tmp;
+  Buf cub_tmp_side;  // CUB scratch of the work queued on side_st
   long long* pinned = nullptr;  // host staging for readbacks and tables
   size_t pinned_cap = 0;
   std::string err;
@@ -149,6 +150,10 @@ struct dmsc_b200_context {
   bool host_fetch_set = false;
   bool copies_pending = false;
   cudaStream_t copy_st = nullptr;
+  // the second side's persistence, cancellation and rank kernels run on
+  // side_st, forked from and joined back to the call's stream
+  cudaStream_t side_st = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   cudaEvent_t copy_ev = nullptr;
   // readback area: pinned host memory mapped into the device address space;
   // a small kernel writes the values, so readbacks never queue behind bulk
@@ -263,14 +268,16 @@ T* sget(dmsc_b200_context* ctx, int side, int slot, size_t n) {
   return get<T>(ctx, S_SIDE0 + side * kSideSlots + slot, n);
 }
 
-void* cub_tmp(dmsc_b200_context* ctx, size_t bytes) {
-  if (ctx->cub_tmp.cap < bytes) {
-    if (ctx->cub_tmp.p) CK(cudaFree(ctx->cub_tmp.p));
+void* cub_tmp(dmsc_b200_context* ctx, size_t bytes, cudaStream_t st) {
+  Buf& b = (st && st == ctx->side_st) ? ctx->cub_tmp_side : ctx->cub_tmp;
+  if (b.cap < bytes) {
+    if (b.p) CK(cudaFree(b.p));
+    b.p = nullptr;
     size_t nb = bytes + bytes / 4 + 256;
-    CK(cudaMalloc(&ctx->cub_tmp.p, nb));
-    ctx->cub_tmp.cap = nb;
+    CK(cudaMalloc(&b.p, nb));
+    b.cap = nb;
   }
-  return ctx->cub_tmp.p;
+  return b.p;
 }
 
 template <class In, class Out>
@@ -278,7 +285,7 @@ void excl_sum(dmsc_b200_context* ctx, const In* in, Out* out, int n, cudaStream_
   if (n <= 0) return;
   size_t bytes = 0;
   CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, st));
-  void* tmp = cub_tmp(ctx, bytes);
+  void* tmp = cub_tmp(ctx, bytes, st);
   CK(cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, n, st));
   ++ctx->launches;
 }
@@ -288,7 +295,7 @@ void incl_sum(dmsc_b200_context* ctx, const In* in, Out* out, int n, cudaStream_
   if (n <= 0) return;
   size_t bytes = 0;
   CK(cub::DeviceScan::InclusiveSum(nullptr, bytes, in, out, n, st));
-  void* tmp = cub_tmp(ctx, bytes);
+  void* tmp = cub_tmp(ctx, bytes, st);
   CK(cub::DeviceScan::InclusiveSum(tmp, bytes, in, out, n, st));
   ++ctx->launches;
 }
@@ -299,7 +306,7 @@ void sort_pairs(dmsc_b200_context* ctx, const K* kin, K* kout, const int* vin, i
   if (n <= 0) return;
   size_t bytes = 0;
   CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, end_bit, st));
-  void* tmp = cub_tmp(ctx, bytes);
+  void* tmp = cub_tmp(ctx, bytes, st);
   CK(cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, n, 0, end_bit, st));
   ++ctx->launches;
 }
@@ -735,15 +742,14 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
 
   // ---- K1 gradient + criticality (all images, one grid) ----
   // the 16 B/index gradient is written only when returned; every later stage
-  // works from the mask and the flow codes
+  // works from the flow codes, which also carry the criticality bits
   int* grad = ret_grad ? grad_out : nullptr;
-  uint8_t* mask = get<uint8_t>(ctx, S_MASK, nidx);
   uint8_t* flow = get<uint8_t>(ctx, S_FLOW, nidx);
   ctx->flow = flow;
   ctx->img = img;
   int* seg[3] = {get<int>(ctx, S_SEG0, nseg), get<int>(ctx, S_SEG1, nseg), get<int>(ctx, S_SEG2, nseg)};
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
-  launch_gradient(ctx, gshape, (unsigned)ntile, I, img, (int4*)grad, mask, seg, flow, st);
+  launch_gradient(ctx, gshape, (unsigned)ntile, I, img, (int4*)grad, nullptr, seg, flow, st);
   mark(ctx, 1, st);
   if (ret_grad) copy_out_async(ctx, ctx->host_grad, grad, 16 * (size_t)nidx, st);
   for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);
@@ -775,7 +781,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   uint32_t* skey32 = B > 1 ? nullptr : get<uint32_t>(ctx, S_SKEY32, nsad);
   ctx->crit_sad = csad;
   ctx->sad_img = isad;
-  LK(compact_kernel<<<grid_for(nseg, 8), 256, 0, st>>>(I, img, nseg, mask, off[0], off[1], off[2], cmin, csad, cmax,
+  LK(compact_kernel<<<grid_for(nseg, 8), 256, 0, st>>>(I, img, nseg, flow, off[0], off[1], off[2], cmin, csad, cmax,
                                                        imin, isad, imax, bmin, bmax, vmin, vmax, kmin, kmax, sval, skey,
                                                        skey32));
   LAUNCH_CHECK("compact_kernel");
@@ -861,8 +867,15 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   CK(cudaMemsetAsync(canc, 0, nsad + 4, st));
   run_pairing(ctx, asc, st);
   mark(ctx, 5, st);
+  // the two sides' persistence, thresholded union-find and ranks are
+  // independent (disjoint buffers; their cancellation bits are ORed into the
+  // shared byte map with atomics): the vertex side runs on side_st
+  CK(cudaEventRecord(ctx->fork_ev, st));
+  CK(cudaStreamWaitEvent(ctx->side_st, ctx->fork_ev, 0));
   finish_pairing(ctx, 0, F, st);
-  finish_pairing(ctx, 1, V, st);
+  finish_pairing(ctx, 1, V, ctx->side_st);
+  CK(cudaEventRecord(ctx->join_ev, ctx->side_st));
+  CK(cudaStreamWaitEvent(st, ctx->join_ev, 0));
   mark(ctx, 6, st);
 
   // ---- surviving saddles in minima-sweep (vertex side) order ----
@@ -1312,7 +1325,10 @@ int dmsc_b200_create(dmsc_b200_context** out, int device) {
   c->pinned_cap = 64 * sizeof(long long);
   if (cudaEventCreateWithFlags(&c->sync_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->side_st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess) {
     dmsc_b200_destroy(c);
     return kErrCuda;
   }
@@ -1340,6 +1356,13 @@ void dmsc_b200_destroy(dmsc_b200_context* c) {
   for (auto& b : c->bufs)
     if (b.p) cudaFree(b.p);
   if (c->cub_tmp.p) cudaFree(c->cub_tmp.p);
+  if (c->cub_tmp_side.p) cudaFree(c->cub_tmp_side.p);
+  if (c->side_st) {
+    cudaStreamSynchronize(c->side_st);
+    cudaStreamDestroy(c->side_st);
+  }
+  if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  if (c->join_ev) cudaEventDestroy(c->join_ev);
   if (c->fifo_lut) cudaFree(c->fifo_lut);
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->rb_h) cudaFreeHost(c->rb_h);

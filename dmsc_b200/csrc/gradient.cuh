@@ -239,7 +239,8 @@ __host__ __device__ __forceinline__ void gather_index(uint32_t wP, uint32_t wL, 
   g = make_int4(v ? b4 + off[v] : -1, hc >= 2u ? b4 + off[8 + hc] : -1, vc >= 2u ? b4 + off[16 + vc] : -1,
                 fc >= 2u ? b4 + off[24 + fc] : -1);
   m = (unsigned)(v == 0u && vin) | (unsigned)(hc == 1u) << 1 | (unsigned)(vc == 1u) << 2 | (unsigned)(fc == 1u) << 3;
-  fl = v | ((fc - 1u) << 4);  // every index has its face, so fc >= 1
+  // every index has its face, so fc >= 1; bits 3 and 7: the H and V edge are critical
+  fl = v | (unsigned)(hc == 1u) << 3 | ((fc - 1u) << 4) | (unsigned)(vc == 1u) << 7;
 }
 
 template <int TY>
@@ -337,7 +338,7 @@ __device__ __forceinline__ void gradient_tile(GradSmem<TY>& S, const float* __re
       unsigned fl;
       gather_index(wP, wL, wU, wUL, 4 * b, S.off, INTERIOR || (iy < H && ix < W), g, m, fl);
       if (grad) grad[gidx] = g;  // null when the gradient is not returned
-      crit_mask[gidx] = (uint8_t)m;
+      if (crit_mask) crit_mask[gidx] = (uint8_t)m;  // null: the flow byte carries the same bits
       flow[gidx] = (uint8_t)fl;
     }
     const unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
@@ -473,6 +474,12 @@ __device__ __forceinline__ float cell_value_g(const float* __restrict__ img, int
   return bv;
 }
 
+// Criticality bits of an index (bit t: slot t is an unpaired valid cell) from
+// its flow byte; `vin`: the index's vertex is a pixel.
+__host__ __device__ __forceinline__ unsigned crit_bits(unsigned fl, bool vin) {
+  return (unsigned)((fl & 7u) == 0u && vin) | ((fl >> 2) & 2u) | ((fl >> 5) & 4u) | (unsigned)(((fl >> 4) & 7u) == 0u) << 3;
+}
+
 // K2: ordered compaction. One warp per (row, 32-column) segment of an image;
 // segment offsets are exclusive scans of the per-segment counts over the
 // whole batch (images in order, rows in order), so each image's lists are a
@@ -484,7 +491,7 @@ __device__ __forceinline__ float cell_value_g(const float* __restrict__ img, int
 // values with their sort keys (image id above the orderable value, so one
 // sort orders every image).
 static __global__ void __launch_bounds__(256) compact_kernel(
-    Imgs I, const float* __restrict__ img_all, long long nseg, const uint8_t* __restrict__ crit_mask,
+    Imgs I, const float* __restrict__ img_all, long long nseg, const uint8_t* __restrict__ flow,
     const int* __restrict__ off_min, const int* __restrict__ off_sad, const int* __restrict__ off_max,
     int* __restrict__ crit_min, int* __restrict__ crit_sad, int* __restrict__ crit_max, int* __restrict__ min_img,
     int* __restrict__ sad_img, int* __restrict__ max_img, uint32_t* __restrict__ min_bits,
@@ -505,7 +512,7 @@ static __global__ void __launch_bounds__(256) compact_kernel(
   unsigned m = 0;
   const long long gidx = (long long)I.idx_base[b] + (long long)iy * Nx + ix;
   const float* img = img_all + I.px_base[b];
-  if (ix <= W) m = crit_mask[gidx];
+  if (ix <= W) m = crit_bits(flow[gidx], iy < H && ix < W);
   unsigned lt = (1u << lane) - 1u;
   unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
   unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);

@@ -286,7 +286,7 @@ __device__ __forceinline__ void seg_start(const EmitCtx& E, int s, int j, int re
 __device__ __forceinline__ void seg_step(const EmitCtx& E, SegCursor& c) {
   *c.dst = (E.faces ? 3 : 0) + 4 * (c.idx - c.ibase);
   c.dst += c.step;
-  if (--c.rem > 0) c.idx += flow_step((__ldg(E.flow + c.idx) >> (E.faces ? 4 : 0)) & 0xFu, c.Nx);
+  if (--c.rem > 0) c.idx += flow_step((__ldg(E.flow + c.idx) >> (E.faces ? 4 : 0)) & 7u, c.Nx);
 }
 
 // Expands W(d): queues its two chains at slot p and its two raw-arc segments

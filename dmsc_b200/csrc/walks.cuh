@@ -45,7 +45,7 @@ __device__ __forceinline__ int flow_walk(const uint8_t* __restrict__ flow, int i
                                          long long* steps, unsigned* status) {
   long long n = 0;
   unsigned c;
-  while ((c = (__ldg(flow + idx) >> SHIFT) & 0xFu) != kFlowNone) {
+  while ((c = (__ldg(flow + idx) >> SHIFT) & 7u) != kFlowNone) {
     idx += flow_step(c, Nx);
     if (++n > cap) {
       set_status(status, kStatusWalkCap);
@@ -192,8 +192,8 @@ __device__ __forceinline__ void tile_ranks(const uint8_t (*fl)[kLT], const Label
     const int r = rs >> 1, sg = rs & 1;
     const int y = g.y0 + r, x = g.x0 + sg * 32 + lane;
     const unsigned code = fl[r][sg * 32 + lane];
-    const unsigned fb = __ballot_sync(0xffffffffu, y <= g.H && x <= g.W && (code >> 4) == kFlowNone);
-    const unsigned vb = __ballot_sync(0xffffffffu, y < g.H && x < g.W && (code & 0xFu) == kFlowNone);
+    const unsigned fb = __ballot_sync(0xffffffffu, y <= g.H && x <= g.W && ((code >> 4) & 7u) == kFlowNone);
+    const unsigned vb = __ballot_sync(0xffffffffu, y < g.H && x < g.W && (code & 7u) == kFlowNone);
     if (lane == 0) {
       R.fbits[r][sg] = fb;
       R.vbits[r][sg] = vb;
@@ -241,7 +241,7 @@ constexpr int kLabelNT[kLabelShapes] = {1024, 512};
 template <bool FACES>
 __device__ __forceinline__ uint32_t tile_init(const uint8_t (*fl)[kLT], const TileRanks& R, const int* __restrict__ lab,
                                               int r, int c, int tile, int ntx) {
-  const unsigned code = ((unsigned)fl[r][c] >> (FACES ? 4 : 0)) & 0xFu;
+  const unsigned code = ((unsigned)fl[r][c] >> (FACES ? 4 : 0)) & 7u;
   if (code == kFlowNone) return ((uint32_t)tile_label<FACES>(R, r * kLT + c, lab) << 1) | 1u;
   int nr = r, nc = c, nt = tile;
   if (code == kFlowLeft) {

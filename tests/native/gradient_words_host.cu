@@ -1,6 +1,6 @@
 // Host build of the gradient kernel's per-pixel and per-index functions
 // (dmsc_b200/csrc/gradient.cuh: face_fifo_table, star_word, gather_offset,
-// gather_index), for the CPU tests: the same code the device tiles run,
+// gather_index, crit_bits), for the CPU tests: the same code the device tiles run,
 // applied to a whole image in plain loops, so the word encoding and the
 // gather can be checked against the oracle without a GPU.
 #include <cstdint>
@@ -37,7 +37,9 @@ static void run(const float* img, int H, int W, int32_t* grad, uint8_t* mask, ui
       grad[4 * (size_t)b + 1] = g.y;
       grad[4 * (size_t)b + 2] = g.z;
       grad[4 * (size_t)b + 3] = g.w;
-      mask[b] = (uint8_t)m;
+      // the compaction reads these bits back from the flow byte: both forms must agree
+      const unsigned mb = crit_bits(fl, iy < H && ix < W);
+      mask[b] = (uint8_t)(mb == m ? mb : 0xFFu);
       flow[b] = (uint8_t)fl;
     }
 }

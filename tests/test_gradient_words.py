@@ -65,7 +65,8 @@ def _expected_mask_flow(grad, H, W):
                       0)
     eidx = s3 >> 2
     ffl = np.where(s3 < 0, 0, np.where((s3 & 3) == 1, np.where(eidx == b, 4, 3), np.where(eidx == b, 2, 1)))
-    return mask.reshape(-1), (vflow | (ffl << 4)).astype(np.uint8).reshape(-1)
+    fl = vflow | (crit[..., 1] << 3) | (ffl << 4) | (crit[..., 2] << 7)
+    return mask.reshape(-1), fl.astype(np.uint8).reshape(-1)
 
 
 def _fields(rng):
