@@ -63,10 +63,17 @@ struct ChunkLists {
   int buf[2][kChunk];
 };
 
-__device__ __forceinline__ long long chunk_size(long long n) {
-  const long long lanes = (long long)gridDim.x * 256;
+__device__ __forceinline__ long long chunk_size(long long n, int blocks) {
+  const long long lanes = (long long)blocks * 256;
   return 256LL * max(1LL, min((long long)kChunkPer, (n + lanes - 1) / lanes));
 }
+
+// Round loops whose active set has shrunk below kSoloItems finish in block 0
+// alone: the other blocks leave (all decide alike, from the same counters
+// read after the grid barrier that ended the previous round), and block 0
+// separates the remaining phases with block barriers instead of grid
+// barriers, which cost several microseconds each.
+constexpr long long kSoloItems = 4096;
 
 __device__ __forceinline__ void chunk_start(ChunkLists& L) {
   if (threadIdx.x < 2) L.n[threadIdx.x] = 0;
@@ -209,7 +216,7 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
     }
   }
   grid.sync();
-  bool done0 = false, done1 = false;
+  bool done0 = false, done1 = false, solo = false;
   for (int r = 0;; ++r) {
     const int n0 = *(volatile int*)(P.s[0].cnt + r % 3), n1 = *(volatile int*)(P.s[1].cnt + r % 3);
     // a side whose active list is empty is finished: its roots are not visited
@@ -226,16 +233,22 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
       }
     }
     if (n0 == 0 && n1 == 0) break;
+    if (!solo && (long long)n0 + n1 + nr0 + nr1 <= kSoloItems) {
+      solo = true;
+      if (blockIdx.x != 0) break;
+    }
     if (r >= max(P.s[0].max_rounds, P.s[1].max_rounds)) {
       // every thread leaves here in the same round (the counters it read are
       // the same); saddles still undecided become cycles, so the kernels
       // that run before the host sees the status read valid extremum indices
       if (tid == 0) set_status(P.s[0].status, kStatusRoundCap);
+      const long long t0 = solo ? threadIdx.x : tid, nt = solo ? blockDim.x : nth;
       for (int sd = 0; sd < 2; ++sd)
-        for (long long i = tid; i < P.s[sd].nsad; i += nth)
+        for (long long i = t0; i < P.s[sd].nsad; i += nt)
           if (P.s[sd].dying[i] == kUndecided) P.s[sd].dying[i] = -1;
       break;
     }
+    const int bid = solo ? 0 : (int)blockIdx.x, nblk = solo ? 1 : (int)gridDim.x;
     if (tid == 0) {
       for (int sd = 0; sd < 2; ++sd) {
         P.s[sd].cnt[(r + 2) % 3] = 0;
@@ -244,8 +257,8 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
     }
     // phase A over both sides' active saddles
     {
-      const long long n = (long long)n0 + n1, chunk = chunk_size(n);
-      for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
+      const long long n = (long long)n0 + n1, chunk = chunk_size(n, nblk);
+      for (long long c0 = (long long)bid * chunk; c0 < n; c0 += (long long)nblk * chunk) {
         chunk_start(L);
         for (long long i = c0 + threadIdx.x; i < min(n, c0 + chunk); i += 256) {
           bool keep;
@@ -262,11 +275,14 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
                     (r & 1) ? P.s[1].act0 : P.s[1].act1);
       }
     }
-    grid.sync();
+    if (solo)
+      __syncthreads();
+    else
+      grid.sync();
     // phase B1: live roots decide on their first outgoing saddle
     {
-      const long long n = (long long)nr0 + nr1, chunk = chunk_size(n);
-      for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
+      const long long n = (long long)nr0 + nr1, chunk = chunk_size(n, nblk);
+      for (long long c0 = (long long)bid * chunk; c0 < n; c0 += (long long)nblk * chunk) {
         chunk_start(L);
         for (long long k = c0 + threadIdx.x; k < min(n, c0 + chunk); k += 256) {
           bool live;
@@ -283,7 +299,10 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
                     P.s[1].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[1].roots0 : P.s[1].roots1);
       }
     }
-    grid.sync();
+    if (solo)
+      __syncthreads();
+    else
+      grid.sync();
   }
 }
 
@@ -382,7 +401,7 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
     }
   }
   grid.sync();
-  bool done0 = false, done1 = false;
+  bool done0 = false, done1 = false, solo = false;
   for (int rd = 0;; ++rd) {
     const int na = P.s[0].n_cancel ? *(volatile int*)(P.s[0].cnt + rd % 3) : 0;
     const int nb = P.s[1].n_cancel ? *(volatile int*)(P.s[1].cnt + rd % 3) : 0;
@@ -399,12 +418,17 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
     done0 = done0 || na == 0;
     done1 = done1 || nb == 0;
     if (na == 0 && nb == 0) break;
+    if (!solo && (long long)na + nb <= kSoloItems) {  // block 0 finishes alone (see kSoloItems)
+      solo = true;
+      if (blockIdx.x != 0) break;
+    }
+    const long long t0 = solo ? threadIdx.x : tid, nt = solo ? blockDim.x : nth;
     if (rd >= max(P.s[0].max_rounds, P.s[1].max_rounds)) {
       if (tid == 0) set_status(P.s[0].n_cancel ? P.s[0].status : P.s[1].status, kStatusRoundCap);
       // the cancellations still pending are dropped (their dying nodes
       // become roots), so the chain walks of the kernels that run before the
       // host sees the status meet decided nodes only
-      for (long long i = tid; i < (long long)na + nb; i += nth) {
+      for (long long i = t0; i < (long long)na + nb; i += nt) {
         const ReplayArgs& A = i < na ? P.s[0] : P.s[1];
         const long long k = i < na ? i : i - na;
         const int r = ((rd & 1) ? A.act1 : A.act0)[k];
@@ -417,8 +441,8 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
         if (P.s[sd].n_cancel) P.s[sd].cnt[(rd + 2) % 3] = 0;
     // grid-stride over both sides' pending cancellations (a cancellation
     // decided earlier in the same round is visible to later walks)
-    for (long long base = 0; base < (long long)na + nb; base += nth) {
-      const long long i = base + tid;
+    for (long long base = 0; base < (long long)na + nb; base += nt) {
+      const long long i = base + t0;
       bool k0 = false, k1 = false;
       int r0 = -1, r1 = -1;
       if (i < na) {
@@ -435,7 +459,10 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
       if (k0) ((rd & 1) ? P.s[0].act0 : P.s[0].act1)[p0] = r0;
       if (k1) ((rd & 1) ? P.s[1].act0 : P.s[1].act1)[p1] = r1;
     }
-    grid.sync();
+    if (solo)
+      __syncthreads();
+    else
+      grid.sync();
   }
 }
 
@@ -509,6 +536,7 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
     }
   }
   grid.sync();
+  bool solo = false;
   for (int lv = 0;; ++lv) {
     int n = *(volatile int*)(A.cnt + lv % 3);
     if (tid == 0 && A.timeline && lv < kTimeline - 2) A.timeline[lv] = global_ns();
@@ -520,12 +548,19 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
       if (tid == 0) set_status(E.status, lv >= A.max_levels ? kStatusRoundCap : kStatusQueueOverflow);
       break;
     }
+    // a level of at most one task per thread of a block finishes the
+    // expansion in block 0 alone (each task is one thread's work either way)
+    if (!solo && n <= 256) {
+      solo = true;
+      if (blockIdx.x != 0) break;
+    }
+    const long long t0 = solo ? threadIdx.x : tid, nt = solo ? blockDim.x : nth;
     const int4* in = (lv & 1) ? A.q1 : A.q0;
     E.q_out = (lv & 1) ? A.q0 : A.q1;
     E.n_out = A.cnt + (lv + 1) % 3;
     if (tid == 0) A.cnt[(lv + 2) % 3] = 0;
-    for (long long base = 0; base < n; base += nth) {
-      long long i = base + tid;
+    for (long long base = 0; base < n; base += nt) {
+      long long i = base + t0;
       int4 t = make_int4(-1, 0, 0, 0);
       int kind = -1, rev = 0, need = 0, nb = 0;
       long long total = 0;
@@ -543,7 +578,10 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
       }
       if (kind == kTaskChain) chain_expand(E, t.y, t.z, rev, t.w, total, p, pb);
     }
-    grid.sync();
+    if (solo)
+      __syncthreads();
+    else
+      grid.sync();
   }
 }
 
