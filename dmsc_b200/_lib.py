@@ -56,7 +56,7 @@ class Sizes(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("grad_shape", "label_shape", "pair_blocks_per_sm",
-                                            "replay_blocks_per_sm", "emit_blocks_per_sm")]
+                                            "replay_blocks_per_sm", "emit_blocks_per_sm", "seg_cursors")]
 
 
 class Outputs(ctypes.Structure):
@@ -193,11 +193,11 @@ class Context:
         return t
 
     def tuning_limits(self) -> dict:
-        buf = (ctypes.c_int * 5)()
-        if self.lib.dmsc_b200_tuning_limits(self.h, buf, 5) != 5:
+        buf = (ctypes.c_int * 6)()
+        if self.lib.dmsc_b200_tuning_limits(self.h, buf, 6) != 6:
             raise RuntimeError("dmsc_b200_tuning_limits failed")
         return dict(zip(("grad_shapes", "label_shapes", "pair_blocks_per_sm", "replay_blocks_per_sm",
-                         "emit_blocks_per_sm"), list(buf)))
+                         "emit_blocks_per_sm", "seg_cursors"), list(buf)))
 
     def set_wait_timeout(self, seconds: float):
         self.check(self.lib.dmsc_b200_set_wait_timeout(self.h, float(seconds)), "dmsc_b200_set_wait_timeout")

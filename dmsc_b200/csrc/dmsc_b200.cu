@@ -170,6 +170,7 @@ struct dmsc_b200_context {
   int grad_shape = 1;
   int label_shape = 0;
   int pair_per_sm = 0, replay_per_sm = 0, emit_per_sm = 0;
+  int seg_cursors = 2;  // raw-arc cursors per lane of the segment writer
   int cap_pair_rounds = 0, cap_replay_rounds = 0, cap_emit_levels = 0;
 };
 
@@ -1127,9 +1128,14 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel", ctx->emit_per_sm);
   {
     int per = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel, 256, 0));
     E.n_base = A.cnt + 3;
-    LK(emit_segments_kernel<<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3));
+    if (ctx->seg_cursors == 1) {
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel<1>, 256, 0));
+      LK(emit_segments_kernel<1><<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3));
+    } else {
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel<2>, 256, 0));
+      LK(emit_segments_kernel<2><<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3));
+    }
     LAUNCH_CHECK("emit_segments_kernel");
   }
 }
@@ -1529,8 +1535,9 @@ int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_
 int dmsc_b200_set_tuning(dmsc_b200_context* ctx, const dmsc_b200_tuning* t) {
   if (!ctx || !t || t->grad_shape < 0 || t->grad_shape >= kGradShapes || t->label_shape < 0 ||
       t->label_shape >= kLabelShapes || t->pair_blocks_per_sm < 0 || t->replay_blocks_per_sm < 0 ||
-      t->emit_blocks_per_sm < 0)
+      t->emit_blocks_per_sm < 0 || t->seg_cursors < 1 || t->seg_cursors > kSegCursorShapes)
     return kErrInvalidArgument;
+  ctx->seg_cursors = t->seg_cursors;
   ctx->grad_shape = t->grad_shape;
   ctx->label_shape = t->label_shape;
   ctx->pair_per_sm = t->pair_blocks_per_sm;
@@ -1546,19 +1553,20 @@ int dmsc_b200_get_tuning(const dmsc_b200_context* ctx, dmsc_b200_tuning* t) {
   t->pair_blocks_per_sm = ctx->pair_per_sm;
   t->replay_blocks_per_sm = ctx->replay_per_sm;
   t->emit_blocks_per_sm = ctx->emit_per_sm;
+  t->seg_cursors = ctx->seg_cursors;
   return kOk;
 }
 
 int dmsc_b200_tuning_limits(dmsc_b200_context* ctx, int* out, int n) {
   if (!ctx || !out) return -1;
-  int v[5] = {kGradShapes, kLabelShapes, 0, 0, 0};
+  int v[6] = {kGradShapes, kLabelShapes, 0, 0, 0, kSegCursorShapes};
   if (cudaSetDevice(ctx->device) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v[2], pairing_persistent_kernel, 256, 0) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v[3], replay_persistent_kernel, 256, 0) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v[4], emit_persistent_kernel, 256, 0) != cudaSuccess)
     return -1;
-  for (int k = 0; k < 5 && k < n; ++k) out[k] = v[k];
-  return 5;
+  for (int k = 0; k < 6 && k < n; ++k) out[k] = v[k];
+  return 6;
 }
 
 int dmsc_b200_set_wait_timeout(dmsc_b200_context* ctx, double seconds) {

@@ -590,35 +590,59 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
 // one instead of idling until the warp's longest is done: each warp owns
 // ranges of kSegRange consecutive segments (grid-stride over the ranges) and,
 // every kSegSteps cells, hands the next unstarted segments of its range to its
-// idle lanes by ballot (warp-local, no atomics).
+// idle cursors by ballot (warp-local, no atomics). Each lane drives NC
+// cursors whose flow-code loads are issued together, so a lane waits on NC
+// independent dependent-load chains at once instead of one.
 constexpr int kSegRange = 256;
 constexpr int kSegSteps = 8;
+constexpr int kSegCursorShapes = 2;  // NC = 1 or 2 (tuned)
 
+template <int NC>
 __global__ void __launch_bounds__(256) emit_segments_kernel(EmitCtx E, const int* __restrict__ count) {
   const long long nb = min((long long)*count, E.base_cap);
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const int shift = E.faces ? 4 : 0, type = E.faces ? 3 : 0;
   for (long long r0 = warp * kSegRange; r0 < nb; r0 += nwarps * kSegRange) {
     const long long r1 = min(nb, r0 + kSegRange);
     long long next = r0;  // first segment of the range not yet handed out (same in every lane)
-    SegCursor c;
-    c.rem = 0;
+    SegCursor c[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) c[q].rem = 0;
     while (true) {
-      const unsigned idle = __ballot_sync(0xffffffffu, c.rem <= 0);
-      if (c.rem <= 0) {
-        const long long my = next + __popc(idle & lt);
-        if (my < r1) {
-          const int4 t = E.base_q[my];
-          seg_start(E, t.y, t.z, (t.x >> 2) & 1, t.w, c);
+      bool busy = false;
+#pragma unroll
+      for (int q = 0; q < NC; ++q) {
+        const unsigned idle = __ballot_sync(0xffffffffu, c[q].rem <= 0);
+        if (c[q].rem <= 0) {
+          const long long my = next + __popc(idle & lt);
+          if (my < r1) {
+            const int4 t = E.base_q[my];
+            seg_start(E, t.y, t.z, (t.x >> 2) & 1, t.w, c[q]);
+          }
+        }
+        next += __popc(idle);
+        busy = busy || c[q].rem > 0;
+      }
+      if (next >= r1 && __ballot_sync(0xffffffffu, busy) == 0) break;
+#pragma unroll 1
+      for (int k = 0; k < kSegSteps; ++k) {
+        unsigned f[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {  // all loads first: independent chains overlap
+          f[q] = 0;
+          if (c[q].rem > 1) f[q] = __ldg(E.flow + c[q].idx);
+        }
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+          if (c[q].rem <= 0) continue;
+          *c[q].dst = type + 4 * (c[q].idx - c[q].ibase);
+          c[q].dst += c[q].step;
+          if (--c[q].rem > 0) c[q].idx += flow_step((f[q] >> shift) & 7u, c[q].Nx);
         }
       }
-      next += __popc(idle);
-      if (next >= r1 && __ballot_sync(0xffffffffu, c.rem > 0) == 0) break;
-#pragma unroll 1
-      for (int k = 0; k < kSegSteps; ++k)
-        if (c.rem > 0) seg_step(E, c);
     }
   }
 }

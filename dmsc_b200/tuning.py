@@ -11,7 +11,8 @@ changes an output bit:
   per thread in the barrier-free pointer jumping);
 * ``pair_blocks_per_sm``, ``replay_blocks_per_sm``, ``emit_blocks_per_sm``:
   resident blocks per SM of the three persistent round loops (0 = all that
-  fit); fewer blocks make each grid barrier cheaper, more hide more latency.
+  fit); fewer blocks make each grid barrier cheaper, more hide more latency;
+* ``seg_cursors``: raw-arc walks per lane of the segment writer (1 or 2).
 
 ``tune`` sweeps one tunable at a time on the caller's own input (coordinate
 descent in the order above), timing the stage that tunable affects with the
@@ -39,6 +40,7 @@ TUNABLES = (
     ("pair_blocks_per_sm", "pairing", lambda lim: _blocks(lim["pair_blocks_per_sm"])),
     ("replay_blocks_per_sm", "replay", lambda lim: _blocks(lim["replay_blocks_per_sm"])),
     ("emit_blocks_per_sm", "fetch_geometry", lambda lim: _blocks(lim["emit_blocks_per_sm"])),
+    ("seg_cursors", "fetch_geometry", lambda lim: list(range(2, lim["seg_cursors"] + 1)) + [1]),
 )
 
 _lock = threading.Lock()
@@ -48,7 +50,7 @@ _tuning = threading.local()  # set while tune() runs on this thread
 
 def _default_tuning() -> dict:
     return {"grad_shape": 1, "label_shape": 0, "pair_blocks_per_sm": 0, "replay_blocks_per_sm": 0,
-            "emit_blocks_per_sm": 0}
+            "emit_blocks_per_sm": 0, "seg_cursors": 2}
 
 
 def _blocks(most: int) -> list:

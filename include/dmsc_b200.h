@@ -236,22 +236,25 @@ int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_
    label_shape  : 64 x 64 label tiles with {1024, 512} threads, 0..1; default 0.
    *_blocks_per_sm : resident blocks per SM of the pairing, replay and
                   geometry-expansion persistent kernels; 0 = as many as fit
-                  (the default); larger values are clamped to what fits. */
+                  (the default); larger values are clamped to what fits.
+   seg_cursors  : raw-arc walks each lane of the segment writer drives at
+                  once, 1..2; default 2. */
 typedef struct {
   int grad_shape;
   int label_shape;
   int pair_blocks_per_sm;
   int replay_blocks_per_sm;
   int emit_blocks_per_sm;
+  int seg_cursors;
 } dmsc_b200_tuning;
 
 int dmsc_b200_set_tuning(dmsc_b200_context* ctx, const dmsc_b200_tuning* tuning);
 int dmsc_b200_get_tuning(const dmsc_b200_context* ctx, dmsc_b200_tuning* tuning);
 
 /* Choices of the tunables on this context's device (host pointer, up to `n`
-   values): number of gradient tile shapes, number of label tile shapes, and
-   the most blocks per SM of the pairing, replay and expansion kernels.
-   Returns the number written or -1. */
+   values): number of gradient tile shapes, number of label tile shapes, the
+   most blocks per SM of the pairing, replay and expansion kernels, and the
+   most segment-writer cursors per lane. Returns the number written or -1. */
 int dmsc_b200_tuning_limits(dmsc_b200_context* ctx, int* out, int n);
 
 /* Host waits inside a call poll an event; after `seconds` (default 600) they
