@@ -45,9 +45,9 @@ enum Slot {
 };
 enum SideSlot {
   X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
-  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_NODE,
+  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_UT, X_BLEN, X_CKEY, X_CVAL, X_NODE,
   X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
-  X_GBASE, X_LAB, X_WX, X_WA, X_CENDS, kSideSlots
+  X_GBASE, X_LAB, X_WX, X_WA, kSideSlots
 };
 
 struct Buf {
@@ -507,24 +507,19 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   CK(cudaMemsetAsync(S.alive, 1, M + 4, st));
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
   int* ncanc = get<int>(ctx, S_NCANC, 4) + si;
-  int2* cends = sget<int2>(ctx, si, X_CENDS, nsad);
   CK(cudaMemsetAsync(ncanc, 0, sizeof(int), st));
+  // thresholded union-find: the forest of cancelled deaths (pairing.cuh)
+  int* cparent = sget<int>(ctx, si, X_UF, M + 1);
+  S.ut = sget<int>(ctx, si, X_UT, M + 1);
+  LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(cparent, M + 1));
   if (nsad > 0) {
     LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(
         nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.sweep, S.dying, get<float>(ctx, S_SVAL, nsad), S.val,
-        S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.c1, S.c2, cends));
+        S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.c1, S.c2,
+        sget<int2>(ctx, si, X_G12, nsad), M, cparent));
     LAUNCH_CHECK("persistence_kernel");
   }
-  // thresholded union-find roots
-  int* uf = sget<int>(ctx, si, X_UF, M + 1);
-  int* croot = sget<int>(ctx, si, X_CROOT, M + 1);
-  S.ut = sget<int>(ctx, si, X_UT, M + 1);
-  LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(uf, M + 1));
-  if (nsad > 0)
-    LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(cends, ncanc, M, uf, M + 2, ctx->status));
-  LK(ut_flatten_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, uf, M + 2, ctx->status));
-  LK(ut_mark_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M, uf, S.alive, croot));
-  if (M > 0) LK(ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.ut));
+  if (M > 0) LK(ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, cparent, S.ut, M + 2, ctx->status));
   LAUNCH_CHECK("thresholded union-find");
   // batch-wide output rank of alive extrema
   int* alive_i = sget<int>(ctx, si, X_ALIVEI, M + 1);
