@@ -41,8 +41,8 @@ EXPORTS = (
     "dmsc_b200_critical_cells_static",
 )
 
-STAGES = ("gradient", "compaction", "saddle_sort", "saddle_walks", "pairing", "persistence_and_ranks", "survivors",
-          "replay", "final_arcs", "labels", "sizes", "fetch_lists", "fetch_geometry")
+STAGES = ("setup", "gradient", "compaction", "saddle_sort", "saddle_walks", "pairing", "persistence_and_ranks", "survivors",
+          "replay", "final_arcs", "label_setup", "labels", "sizes", "fetch_lists", "fetch_geometry")
 
 ERR_TOO_LARGE = 2
 

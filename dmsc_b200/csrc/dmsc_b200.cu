@@ -44,7 +44,7 @@ enum Slot {
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
-  X_SWEEP, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
+  X_SWEEP, X_RANK, X_DYINGL, X_G12L, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
   X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_UT, X_BLEN, X_CKEY, X_CVAL, X_NODE,
   X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
   X_GBASE, X_LAB, X_WX, X_WA, kSideSlots
@@ -105,7 +105,7 @@ struct Side {
 
 }  // namespace
 
-constexpr int kStageMarks = 16;
+constexpr int kStageMarks = 17;
 
 struct dmsc_b200_context {
   int device = 0;
@@ -458,18 +458,20 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
   S.c1 = sget<int>(ctx, si, X_C1, nsad);
   S.c2 = sget<int>(ctx, si, X_C2, nsad);
   S.dying = sget<int>(ctx, si, X_DYING, nsad);
+  int* rank = sget<int>(ctx, si, X_RANK, nsad);
   if (nsad > 0) {
     LK(sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, ctx->sad_img, ctx->bases.sad, ctx->I.dual,
-                                                             S.faces, S.t, S.sweep, S.c1, S.c2));
+                                                             S.faces, S.t, S.sweep, rank, S.c1, S.c2));
     LAUNCH_CHECK("sweep_edges_kernel");
   }
   PairArgs A;
   A.nsad = nsad;
   A.M = M;
-  A.c1 = S.c1;
-  A.c2 = S.c2;
-  A.g12 = sget<int2>(ctx, si, X_G12, nsad);
-  A.dying = S.dying;
+  A.t = S.t;
+  A.rank = rank;
+  A.sweep = S.sweep;
+  A.g12 = sget<int2>(ctx, si, X_G12L, nsad);
+  A.dying = sget<int>(ctx, si, X_DYINGL, nsad);
   A.link = sget<int>(ctx, si, X_LINK, M + 1);
   A.minedge = sget<unsigned>(ctx, si, X_MINE, M + 1);
   A.act0 = sget<int>(ctx, si, X_ACT0, nsad);
@@ -493,8 +495,15 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
 void run_pairing(dmsc_b200_context* ctx, const int* asc, cudaStream_t st) {
   PairArgs2 P;
   for (int si = 0; si < 2; ++si) P.s[si] = pairing_args(ctx, si, ctx->side[si], asc, st);
-  if (ctx->nsad > 0)
+  if (ctx->nsad > 0) {
     coop_launch(ctx, pairing_persistent_kernel, P, st, "pairing_persistent_kernel", ctx->pair_per_sm);
+    for (int si = 0; si < 2; ++si) {
+      Side& S = ctx->side[si];
+      LK(pair_to_sweep_kernel<<<grid_for(ctx->nsad, TB), TB, 0, st>>>(ctx->nsad, S.sweep, P.s[si].dying, P.s[si].g12,
+                                                                      S.dying, sget<int2>(ctx, si, X_G12, ctx->nsad)));
+    }
+    LAUNCH_CHECK("pair_to_sweep_kernel");
+  }
 }
 
 // Persistence, cancellation, thresholded union-find and output ranks of one side.
@@ -745,6 +754,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   ctx->img = img;
   int* seg[3] = {get<int>(ctx, S_SEG0, nseg), get<int>(ctx, S_SEG1, nseg), get<int>(ctx, S_SEG2, nseg)};
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
+  mark(ctx, 15, st);  // the gradient stage times the kernel alone
   launch_gradient(ctx, gshape, (unsigned)ntile, I, img, (int4*)grad, nullptr, seg, flow, st);
   mark(ctx, 1, st);
   if (ret_grad) copy_out_async(ctx, ctx->host_grad, grad, 16 * (size_t)nidx, st);
@@ -971,11 +981,12 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
       LK(label_map_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.ext_img, S.ut, S.to_out, BS.alive[si], lab));
     LAUNCH_CHECK("label_map_kernel");
   }
+  int* nex = get<int>(ctx, S_NEX, 2);
+  CK(cudaMemsetAsync(nex, 0, 2 * sizeof(int), st));
+  mark(ctx, 16, st);  // the labels stage times the label kernels alone
   if (F.groups || V.groups) {
     int2* exf = F.groups ? get<int2>(ctx, S_EXF, nidx) : nullptr;
     int2* exv = V.groups ? get<int2>(ctx, S_EXV, nidx) : nullptr;
-    int* nex = get<int>(ctx, S_NEX, 2);
-    CK(cudaMemsetAsync(nex, 0, 2 * sizeof(int), st));
     if (ctx->label_shape == 1)
       LK((label_tile_kernel<kLabelNT[1]><<<(unsigned)nltile, kLabelNT[1], 0, st>>>(I, flow, LF, LV, OF, OV, exf, exv,
                                                                                  nex, ctx->status)));
@@ -1485,9 +1496,10 @@ int dmsc_b200_set_profiling(dmsc_b200_context* ctx, int enable) {
 
 int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n) {
   if (!ctx || !ms || !ctx->profile) return -1;
-  // extract stages are marks 0..11, fetch stages marks 12..14
-  static const int from[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 13};
-  static const int to[] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 13, 14};
+  // extract stages are marks 0, 15, 1..9, 16, 10, 11 (15: just before the
+  // gradient kernel, 16: just before the label kernels), fetch stages 12..14
+  static const int from[] = {0, 15, 1, 2, 3, 4, 5, 6, 7, 8, 9, 16, 10, 12, 13};
+  static const int to[] = {15, 1, 2, 3, 4, 5, 6, 7, 8, 9, 16, 10, 11, 13, 14};
   const int ns = (int)(sizeof(from) / sizeof(from[0]));
   if (cudaEventSynchronize(ctx->ev[14]) != cudaSuccess) return -1;
   for (int k = 0; k < ns && k < n; ++k) {

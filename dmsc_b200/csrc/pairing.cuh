@@ -56,8 +56,8 @@ __global__ void iota_kernel(int* __restrict__ a, int n) {
 // sweep[q] with ends (t[2s], t[2s+1]); an image's edges stay contiguous.
 __global__ void sweep_edges_kernel(int nsad, const int* __restrict__ asc, const int* __restrict__ sad_img,
                                    const int* __restrict__ sad_base, const uint8_t* __restrict__ dual, bool faces,
-                                   const int* __restrict__ t, int* __restrict__ sweep, int* __restrict__ c1,
-                                   int* __restrict__ c2) {
+                                   const int* __restrict__ t, int* __restrict__ sweep, int* __restrict__ rank,
+                                   int* __restrict__ c1, int* __restrict__ c2) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nsad) return;
   int s = asc[p];
@@ -66,8 +66,23 @@ __global__ void sweep_edges_kernel(int nsad, const int* __restrict__ asc, const 
   bool rev = faces ? !dual[b] : dual[b];
   int q = rev ? base + n - 1 - (p - base) : p;
   sweep[q] = s;
+  rank[s] = q;  // sweep position of the saddle with list index s
   c1[q] = t[2 * s];
   c2[q] = t[2 * s + 1];
+}
+
+// The pairing works on saddles in list order (ascending cell id, so the
+// saddles a block handles touch extrema close to each other); its results go
+// back to sweep order for the later stages: dying[q] and the deciding groups
+// g12[q] of sweep position q.
+__global__ void pair_to_sweep_kernel(int nsad, const int* __restrict__ sweep, const int* __restrict__ dying_l,
+                                     const int2* __restrict__ g12_l, int* __restrict__ dying,
+                                     int2* __restrict__ g12) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nsad) return;
+  const int s = sweep[q];
+  dying[q] = dying_l[s];
+  g12[q] = g12_l[s];
 }
 
 // Persistence of each decided saddle and cancellation (persistence.hxx:82-104,

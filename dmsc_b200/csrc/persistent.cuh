@@ -97,8 +97,12 @@ __device__ __forceinline__ void chunk_flush(ChunkLists& L, int* cnt0, int* out0,
 // ---------------------------------------------------------------------------
 struct PairArgs {
   int nsad, M;  // void group = M
-  const int* c1;
-  const int* c2;
+  // saddles are indexed in list order (ascending cell id); `rank` gives a
+  // saddle's sweep position, which orders the saddles (the atomicMin key),
+  // and `sweep` maps a sweep position back to the saddle
+  const int* t;       // [2 nsad] extremum ends of each saddle (-1: void)
+  const int* rank;    // [nsad]
+  const int* sweep;   // [nsad]
   int2* g12;          // [nsad] groups of the two ends, as of the saddle's last active round
   int* dying;
   int* link;          // [M+1] group union-find
@@ -144,9 +148,9 @@ __device__ __forceinline__ void pair_phase_a(const PairArgs& A, int r, long long
   if (r == 0 || A.dying[e] == kUndecided) {
     int ga, gb;
     if (r == 0) {
-      int a = A.c1[e], b = A.c2[e];
-      ga = a < 0 ? M : a;
-      gb = b < 0 ? M : b;
+      const int2 ab = *reinterpret_cast<const int2*>(A.t + 2 * e);
+      ga = ab.x < 0 ? M : ab.x;
+      gb = ab.y < 0 ? M : ab.y;
     } else {  // the ends' groups of the previous round, followed to their roots
       const int2 g = A.g12[e];
       ga = find_halving(A.link, g.x, M + 2, A.status);
@@ -156,8 +160,9 @@ __device__ __forceinline__ void pair_phase_a(const PairArgs& A, int r, long long
       A.dying[e] = -1;
     } else {
       A.g12[e] = make_int2(ga, gb);
-      atomicMin(A.minedge + ga, (unsigned)e);  // result unused: a reduction
-      atomicMin(A.minedge + gb, (unsigned)e);
+      const unsigned rk = (unsigned)A.rank[e];
+      atomicMin(A.minedge + ga, rk);  // result unused: a reduction
+      atomicMin(A.minedge + gb, rk);
       keep = true;
     }
   }
@@ -174,7 +179,7 @@ __device__ __forceinline__ void pair_phase_b1(const PairArgs& A, int r, long lon
   unsigned me = A.minedge[g];
   if (me != kNoEdge) {
     A.minedge[g] = kNoEdge;
-    int e = (int)me;
+    const int e = A.sweep[me];  // the saddle at that sweep position
     const int2 gg = A.g12[e];  // roots as of phase A
     const int ga = gg.x, gb = gg.y;
     h = (ga == g) ? gb : ga;

@@ -4,7 +4,8 @@ The reference lists loss functions for topological segmentation as future
 work (readme.md, TODOs); it has no counterpart. Every loss here is a plain
 torch function of the persistence values returned by
 ``autograd.persistence_pairs``, so its gradient reaches the image through the
-deterministic pixel-pair scatter (no float atomics): repeated backward passes
+deterministic pixel-pair scatter (no float atomics), and per-image sums are
+segmented reductions in a fixed order: repeated forward and backward passes
 give identical bits. Each loss has a ``*_from_pairs`` form that takes the
 values and their metadata directly (any float dtype), which is also how the
 tests evaluate the same loss in FP64 for finite differences.
@@ -26,6 +27,16 @@ from .autograd import persistence_pairs
 _SIDES = {"min": (0,), "max": (1,), "both": (0, 1)}
 
 
+def _per_image_sum(term, image, B):
+    """Per-image sums in a fixed order (segmented reduction over the entries
+    grouped by image): deterministic bits, unlike a float index_add."""
+    if term.numel() == 0:
+        return torch.zeros(B, dtype=term.dtype, device=term.device)
+    order = torch.sort(image, stable=True).indices
+    lengths = torch.bincount(image, minlength=B)
+    return torch.segment_reduce(term[order], "sum", lengths=lengths, unsafe=True)
+
+
 def _side_mask(side_t, ppairs, p, side):
     if side not in _SIDES:
         raise ValueError(f"side must be one of {sorted(_SIDES)}, got {side!r}")
@@ -41,8 +52,7 @@ def denoising_loss_from_pairs(p, image, side_t, ppairs, max_persistence=0.1, sid
     persistence). Returns a [B] tensor."""
     B = int(n_images if n_images is not None else (int(image.max()) + 1 if image.numel() else 0))
     keep = _side_mask(side_t, ppairs, p, side) & (p < max_persistence)
-    out = torch.zeros(B, dtype=p.dtype, device=p.device)
-    return out.index_add(0, image, torch.where(keep, p * p, torch.zeros_like(p)))
+    return _per_image_sum(torch.where(keep, p * p, torch.zeros_like(p)), image, B)
 
 
 def _ranks_desc(p, image, mask):
@@ -82,7 +92,7 @@ def betti_loss_from_pairs(p, image, side_t, ppairs, n_regions, side="min", targe
     top = mask & (rank < (k[image] - 1))
     term = torch.where(top, (target - p) ** 2, p * p)
     term = torch.where(mask, term, torch.zeros_like(p))
-    return torch.zeros(B, dtype=p.dtype, device=p.device).index_add(0, image, term)
+    return _per_image_sum(term, image, B)
 
 
 def _pairs(img, persistence_threshold, is_dual):

@@ -189,10 +189,12 @@ const char* dmsc_b200_last_error(const dmsc_b200_context* ctx);
    When enabled, extract() and fetch() record a CUDA event on the call's stream
    at every stage boundary. dmsc_b200_stage_times() writes up to `n` stage
    durations in milliseconds of the last extract()+fetch() pair (host pointer)
-   and returns the number of stages: 0 gradient, 1 compaction, 2 saddle sort,
-   3 saddle walks, 4 pairing (both sides), 5 persistence, cancellation and
-   output ranks, 6 survivors, 7 replay (both sides), 8 final arcs, 9 labels,
-   10 sizes, 11 fetch lists, 12 fetch geometry. */
+   and returns the number of stages: 0 set-up (workspace clears, table
+   upload), 1 gradient (the kernel alone), 2 compaction, 3 saddle sort,
+   4 saddle walks, 5 pairing (both sides), 6 persistence, cancellation and
+   output ranks, 7 survivors, 8 replay (both sides), 9 final arcs, 10 label
+   set-up (per-extremum labels, bases), 11 labels (the label kernels alone),
+   12 sizes, 13 fetch lists, 14 fetch geometry. */
 int dmsc_b200_set_profiling(dmsc_b200_context* ctx, int enable);
 int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n);
 
