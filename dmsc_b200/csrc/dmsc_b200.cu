@@ -44,10 +44,10 @@ enum Slot {
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
-  X_SWEEP, X_RANK, X_DYINGL, X_G12L, X_C1, X_C2, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
-  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_UT, X_BLEN, X_CKEY, X_CVAL, X_NODE,
+  X_SWEEP, X_RANK, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
+  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_NODE,
   X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
-  X_GBASE, X_LAB, X_WX, X_WA, kSideSlots
+  X_GBASE, X_LAB, X_WX, X_WA, X_CENDS, kSideSlots
 };
 
 struct Buf {
@@ -79,8 +79,6 @@ struct Side {
   int* t = nullptr;
   int* steps = nullptr;
   int* sweep = nullptr;
-  int* c1 = nullptr;
-  int* c2 = nullptr;
   int* dying = nullptr;
   int* pair_dense = nullptr;
   float* pers = nullptr;
@@ -167,10 +165,10 @@ struct dmsc_b200_context {
   // tuned launch shapes (dmsc_b200_set_tuning): gradient tile shape (index
   // into kGradTY / kGradNT), label tile threads (index into kLabelNT), and
   // the resident blocks per SM of the three persistent kernels (0 = all that fit)
-  int grad_shape = 1;
-  int label_shape = 0;
+  int grad_shape = 2;
+  int label_shape = 1;
   int pair_per_sm = 0, replay_per_sm = 0, emit_per_sm = 0;
-  int seg_cursors = 2;  // raw-arc cursors per lane of the segment writer
+  int seg_cursors = 1;  // raw-arc cursors per lane of the segment writer
   int cap_pair_rounds = 0, cap_replay_rounds = 0, cap_emit_levels = 0;
 };
 
@@ -455,13 +453,11 @@ void* staging(dmsc_b200_context* ctx, size_t bytes) {
 PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, cudaStream_t st) {
   const int nsad = ctx->nsad, M = S.M;
   S.sweep = sget<int>(ctx, si, X_SWEEP, nsad);
-  S.c1 = sget<int>(ctx, si, X_C1, nsad);
-  S.c2 = sget<int>(ctx, si, X_C2, nsad);
-  S.dying = sget<int>(ctx, si, X_DYING, nsad);
+  S.dying = sget<int>(ctx, si, X_DYING, nsad);  // list order
   int* rank = sget<int>(ctx, si, X_RANK, nsad);
   if (nsad > 0) {
     LK(sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, ctx->sad_img, ctx->bases.sad, ctx->I.dual,
-                                                             S.faces, S.t, S.sweep, rank, S.c1, S.c2));
+                                                             S.faces, S.sweep, rank));
     LAUNCH_CHECK("sweep_edges_kernel");
   }
   PairArgs A;
@@ -470,8 +466,8 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
   A.t = S.t;
   A.rank = rank;
   A.sweep = S.sweep;
-  A.g12 = sget<int2>(ctx, si, X_G12L, nsad);
-  A.dying = sget<int>(ctx, si, X_DYINGL, nsad);
+  A.g12 = sget<int2>(ctx, si, X_G12, nsad);
+  A.dying = S.dying;
   A.link = sget<int>(ctx, si, X_LINK, M + 1);
   A.minedge = sget<unsigned>(ctx, si, X_MINE, M + 1);
   A.act0 = sget<int>(ctx, si, X_ACT0, nsad);
@@ -495,15 +491,8 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
 void run_pairing(dmsc_b200_context* ctx, const int* asc, cudaStream_t st) {
   PairArgs2 P;
   for (int si = 0; si < 2; ++si) P.s[si] = pairing_args(ctx, si, ctx->side[si], asc, st);
-  if (ctx->nsad > 0) {
+  if (ctx->nsad > 0)
     coop_launch(ctx, pairing_persistent_kernel, P, st, "pairing_persistent_kernel", ctx->pair_per_sm);
-    for (int si = 0; si < 2; ++si) {
-      Side& S = ctx->side[si];
-      LK(pair_to_sweep_kernel<<<grid_for(ctx->nsad, TB), TB, 0, st>>>(ctx->nsad, S.sweep, P.s[si].dying, P.s[si].g12,
-                                                                      S.dying, sget<int2>(ctx, si, X_G12, ctx->nsad)));
-    }
-    LAUNCH_CHECK("pair_to_sweep_kernel");
-  }
 }
 
 // Persistence, cancellation, thresholded union-find and output ranks of one side.
@@ -517,18 +506,23 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
   int* ncanc = get<int>(ctx, S_NCANC, 4) + si;
   CK(cudaMemsetAsync(ncanc, 0, sizeof(int), st));
-  // thresholded union-find: the forest of cancelled deaths (pairing.cuh)
-  int* cparent = sget<int>(ctx, si, X_UF, M + 1);
-  S.ut = sget<int>(ctx, si, X_UT, M + 1);
-  LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(cparent, M + 1));
+  int2* cends = sget<int2>(ctx, si, X_CENDS, nsad);
   if (nsad > 0) {
     LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(
         nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.sweep, S.dying, get<float>(ctx, S_SVAL, nsad), S.val,
-        S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.c1, S.c2,
-        sget<int2>(ctx, si, X_G12, nsad), M, cparent));
+        S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.t, cends));
     LAUNCH_CHECK("persistence_kernel");
   }
-  if (M > 0) LK(ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, cparent, S.ut, M + 2, ctx->status));
+  // thresholded union-find roots
+  int* uf = sget<int>(ctx, si, X_UF, M + 1);
+  int* croot = sget<int>(ctx, si, X_CROOT, M + 1);
+  S.ut = sget<int>(ctx, si, X_UT, M + 1);
+  LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(uf, M + 1));
+  if (nsad > 0)
+    LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(cends, ncanc, M, uf, M + 2, ctx->status));
+  LK(ut_flatten_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, uf, M + 2, ctx->status));
+  LK(ut_mark_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M, uf, S.alive, croot));
+  if (M > 0) LK(ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.ut));
   LAUNCH_CHECK("thresholded union-find");
   // batch-wide output rank of alive extrema
   int* alive_i = sget<int>(ctx, si, X_ALIVEI, M + 1);
@@ -567,8 +561,7 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   A.cj = cval;
   A.sweep = S.sweep;
   A.dying = S.dying;
-  A.c1 = S.c1;
-  A.c2 = S.c2;
+  A.t = S.t;
   A.blen = S.blen;
   A.S = R;
   A.max_steps = nsad + 1;

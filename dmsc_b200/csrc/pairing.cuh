@@ -56,8 +56,7 @@ __global__ void iota_kernel(int* __restrict__ a, int n) {
 // sweep[q] with ends (t[2s], t[2s+1]); an image's edges stay contiguous.
 __global__ void sweep_edges_kernel(int nsad, const int* __restrict__ asc, const int* __restrict__ sad_img,
                                    const int* __restrict__ sad_base, const uint8_t* __restrict__ dual, bool faces,
-                                   const int* __restrict__ t, int* __restrict__ sweep, int* __restrict__ rank,
-                                   int* __restrict__ c1, int* __restrict__ c2) {
+                                   int* __restrict__ sweep, int* __restrict__ rank) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nsad) return;
   int s = asc[p];
@@ -67,22 +66,6 @@ __global__ void sweep_edges_kernel(int nsad, const int* __restrict__ asc, const 
   int q = rev ? base + n - 1 - (p - base) : p;
   sweep[q] = s;
   rank[s] = q;  // sweep position of the saddle with list index s
-  c1[q] = t[2 * s];
-  c2[q] = t[2 * s + 1];
-}
-
-// The pairing works on saddles in list order (ascending cell id, so the
-// saddles a block handles touch extrema close to each other); its results go
-// back to sweep order for the later stages: dying[q] and the deciding groups
-// g12[q] of sweep position q.
-__global__ void pair_to_sweep_kernel(int nsad, const int* __restrict__ sweep, const int* __restrict__ dying_l,
-                                     const int2* __restrict__ g12_l, int* __restrict__ dying,
-                                     int2* __restrict__ g12) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nsad) return;
-  const int s = sweep[q];
-  dying[q] = dying_l[s];
-  g12[q] = g12_l[s];
 }
 
 // Persistence of each decided saddle and cancellation (persistence.hxx:82-104,
@@ -98,13 +81,12 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
                                                           int* __restrict__ pair_dense, float* __restrict__ pers,
                                                           uint8_t* __restrict__ cancelled, uint8_t sbit,
                                                           uint8_t* __restrict__ alive, int* __restrict__ n_cancel,
-                                                          const int* __restrict__ c1, const int* __restrict__ c2,
-                                                          const int2* __restrict__ g12, int void_id,
-                                                          int* __restrict__ cparent) {
+                                                          const int* __restrict__ t,
+                                                          int2* __restrict__ canc_ends) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   bool canc = false;
   if (j < nsad) {
-    int s = sweep[j], d = dying[j];
+    const int s = sweep[j], d = dying[s];
     if (d < 0) {
       pair_dense[s] = -1;
       pers[s] = -1.0f;
@@ -123,29 +105,25 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
         canc = true;
         atomicOr((unsigned*)(cancelled + (s & ~3)), (unsigned)sbit << (8 * (s & 3)));
         alive[d] = 0;
-        // the dying group hangs under the saddle's other end (g12: the two
-        // ends' groups when the saddle was decided; d is one of them)
-        const int other = g12[j].x == d ? c2[j] : c1[j];
-        cparent[d] = other < 0 ? void_id : other;
       }
     }
   }
-  block_append(n_cancel, canc);  // cancellation count (the replay runs only where it is not 0)
+  // cancelled edges' ends, compacted for the thresholded union-find
+  const int slot = block_append(n_cancel, canc);
+  if (canc) {
+    const int s = sweep[j];
+    canc_ends[slot] = make_int2(t[2 * s], t[2 * s + 1]);
+  }
 }
 
 // Thresholded union-find (the reference's uf_min / uf_max, persistence.hxx:
-// 90-104, 147-161): its components are those of the cancelled saddles, and
-// the reference's unite_from_root always hangs the dying end's root under the
-// surviving end's, so a component's root is its one member not killed by a
-// cancelled saddle, or the void. Here a cancelled death at saddle e hangs the
-// dying group's oldest member d under e's surviving end (persistence_kernel,
-// `cparent`); d and e's dying end lie in one component already, because every
-// earlier merge into d's group was cancelled too (swept earlier, so its saddle
-// value is not above e's, and its dying extremum is not older than d, so its
-// float persistence is not larger). Each extremum dies at most once, so
-// `cparent` is a forest whose roots are the surviving members; the root of x
-// is found with path halving (pointers only move to ancestors), capped at
-// `cap` steps (kStatusFindCap, then the node reached).
+// 90-104, 147-161): lock-free union of the ends of every cancelled saddle
+// (link the larger root under the smaller), over the compact list of
+// cancelled edges written by persistence_kernel. Every link points to a
+// smaller index, so a root search takes at most n steps and every failed CAS
+// means another thread linked one of the two roots (at most n - 1 links
+// exist); both loops are capped at `cap` anyway, and a cap sets
+// kStatusFindCap and returns the node reached (a valid index).
 __device__ __forceinline__ int uf_root(int* p, int x, int cap, unsigned* status) {
   for (int k = 0;; ++k) {
     int px = p[x];
@@ -160,13 +138,62 @@ __device__ __forceinline__ int uf_root(int* p, int x, int cap, unsigned* status)
   }
 }
 
-// ut[x] = the surviving member of x's component, -1 for the void's.
-__global__ void ut_root_kernel(int n_ext, int* __restrict__ cparent, int* __restrict__ ut, int cap,
-                               unsigned* status) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) ut_union_kernel(const int2* __restrict__ ends, const int* __restrict__ count,
+                                                       int void_id, int* __restrict__ p, int cap,
+                                                       unsigned* status) {
+  const int n = *count;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int2 e = ends[q];
+    int a = e.x < 0 ? void_id : e.x;
+    int b = e.y < 0 ? void_id : e.y;
+    for (int tries = 0;; ++tries) {
+      if (tries >= cap) {
+        set_status(status, kStatusFindCap);
+        break;
+      }
+      a = uf_root(p, a, cap, status);
+      b = uf_root(p, b, cap, status);
+      if (a == b) break;
+      if (a > b) {
+        int t = a;
+        a = b;
+        b = t;
+      }
+      if (atomicCAS(p + b, b, a) == b) break;
+    }
+  }
+}
+
+__global__ void ut_flatten_kernel(int n, int* __restrict__ p, int cap, unsigned* status) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n) return;
+  int r = x;
+  for (int k = 0; p[r] != r; ++k) {
+    if (k >= cap) {
+      set_status(status, kStatusFindCap);
+      break;
+    }
+    r = p[r];
+  }
+  p[x] = r;
+}
+
+// Component root = its alive member, or -1 for the void's component.
+__global__ void ut_mark_kernel(int n_ext, const int* __restrict__ p, const uint8_t* __restrict__ alive,
+                               int* __restrict__ comp_root) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x > n_ext) return;
+  if (x == n_ext)
+    comp_root[p[x]] = -1;
+  else if (alive[x])
+    comp_root[p[x]] = x;
+}
+
+__global__ void ut_root_kernel(int n_ext, const int* __restrict__ p, const int* __restrict__ comp_root,
+                               int* __restrict__ ut) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= n_ext) return;
-  const int r = uf_root(cparent, x, cap, status);
-  ut[x] = r == n_ext ? -1 : r;
+  ut[x] = comp_root[p[x]];
 }
 
 }  // namespace dmsc

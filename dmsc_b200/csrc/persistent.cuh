@@ -319,9 +319,8 @@ struct ReplayArgs {
   const unsigned long long* key;     // [C] replay key of each cancellation
   const int* cj;                     // [C] sweep index of each cancellation
   const int* sweep;
-  const int* dying;
-  const int* c1;
-  const int* c2;
+  const int* dying;  // [nsad] in saddle list order
+  const int* t;      // [2 nsad] extremum ends of each saddle, list order
   const long long* blen;
   ReplayState S;
   int max_steps;
@@ -346,7 +345,7 @@ struct ReplayArgs2 {
 __device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r, int round) {
   const unsigned long long t = A.key[r];
   int j = A.cj[r];
-  int d = A.dying[j], s = A.sweep[j];
+  const int s = A.sweep[j], d = A.dying[s];
   // both walks resume where the previous round left them
   int R0 = A.wx[2 * r], R1 = A.wx[2 * r + 1];
   long long a0 = A.wa[2 * r], a1 = A.wa[2 * r + 1];
@@ -391,11 +390,12 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
     for (long long r = tid; r < C; r += nth) {
       A.act0[r] = (int)r;
       const int j = A.cj[r];
-      int d = A.dying[j];
+      const int s = A.sweep[j];
+      int d = A.dying[s];
       A.S.node[d].ctime = A.key[r];
       A.S.node[d].status = kPending;
-      A.wx[2 * r] = A.c1[j];
-      A.wx[2 * r + 1] = A.c2[j];
+      A.wx[2 * r] = A.t[2 * s];
+      A.wx[2 * r + 1] = A.t[2 * s + 1];
       A.wa[2 * r] = 0;
       A.wa[2 * r + 1] = 0;
     }
@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
         const ReplayArgs& A = i < na ? P.s[0] : P.s[1];
         const long long k = i < na ? i : i - na;
         const int r = ((rd & 1) ? A.act1 : A.act0)[k];
-        A.S.node[A.dying[A.cj[r]]].status = kRootForever;
+        A.S.node[A.dying[A.sweep[A.cj[r]]]].status = kRootForever;
       }
       break;
     }

@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(256) cancel_collect_kernel(int nsad, const int
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   bool take = false;
   unsigned long long key = 0;
-  if (j < nsad && dying[j] >= 0) {
+  if (j < nsad && dying[sweep[j]] >= 0) {
     float p = pers[sweep[j]];
     if (p <= thr[sad_img[sweep[j]]]) {
       take = true;

@@ -40,7 +40,7 @@ TUNABLES = (
     ("pair_blocks_per_sm", "pairing", lambda lim: _blocks(lim["pair_blocks_per_sm"])),
     ("replay_blocks_per_sm", "replay", lambda lim: _blocks(lim["replay_blocks_per_sm"])),
     ("emit_blocks_per_sm", "fetch_geometry", lambda lim: _blocks(lim["emit_blocks_per_sm"])),
-    ("seg_cursors", "fetch_geometry", lambda lim: list(range(2, lim["seg_cursors"] + 1)) + [1]),
+    ("seg_cursors", "fetch_geometry", lambda lim: list(range(1, lim["seg_cursors"] + 1))),
 )
 
 _lock = threading.Lock()
@@ -49,8 +49,8 @@ _tuning = threading.local()  # set while tune() runs on this thread
 
 
 def _default_tuning() -> dict:
-    return {"grad_shape": 1, "label_shape": 0, "pair_blocks_per_sm": 0, "replay_blocks_per_sm": 0,
-            "emit_blocks_per_sm": 0, "seg_cursors": 2}
+    return {"grad_shape": 2, "label_shape": 1, "pair_blocks_per_sm": 0, "replay_blocks_per_sm": 0,
+            "emit_blocks_per_sm": 0, "seg_cursors": 1}
 
 
 def _blocks(most: int) -> list:

@@ -234,13 +234,13 @@ int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_
    output bit. The Python tuner (dmsc_b200.tuning) sweeps them on the
    caller's data and sets the fastest per image-size class.
    grad_shape   : gradient tile of 32 index columns x {31, 63, 127} rows
-                  (threads {256, 256, 512}), 0..2; default 1.
-   label_shape  : 64 x 64 label tiles with {1024, 512} threads, 0..1; default 0.
+                  (threads {256, 256, 512}), 0..2; default 2.
+   label_shape  : 64 x 64 label tiles with {1024, 512} threads, 0..1; default 1.
    *_blocks_per_sm : resident blocks per SM of the pairing, replay and
                   geometry-expansion persistent kernels; 0 = as many as fit
                   (the default); larger values are clamped to what fits.
    seg_cursors  : raw-arc walks each lane of the segment writer drives at
-                  once, 1..2; default 2. */
+                  once, 1..2; default 1. */
 typedef struct {
   int grad_shape;
   int label_shape;
