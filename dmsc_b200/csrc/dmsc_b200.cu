@@ -169,6 +169,7 @@ struct dmsc_b200_context {
   int label_shape = 1;
   int pair_per_sm = 0, replay_per_sm = 0, emit_per_sm = 0;
   int seg_cursors = 1;  // raw-arc cursors per lane of the segment writer
+  bool label_smem_set = false;  // dynamic shared memory limit raised for the label kernels
   int cap_pair_rounds = 0, cap_replay_rounds = 0, cap_emit_levels = 0;
 };
 
@@ -980,12 +981,18 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   if (F.groups || V.groups) {
     int2* exf = F.groups ? get<int2>(ctx, S_EXF, nidx) : nullptr;
     int2* exv = V.groups ? get<int2>(ctx, S_EXV, nidx) : nullptr;
+    constexpr int kLSm = (int)sizeof(LabelSmem);
+    if (!ctx->label_smem_set) {  // more than the 48 KB of static shared memory
+      CK(cudaFuncSetAttribute(label_tile_kernel<kLabelNT[0]>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLSm));
+      CK(cudaFuncSetAttribute(label_tile_kernel<kLabelNT[1]>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLSm));
+      ctx->label_smem_set = true;
+    }
     if (ctx->label_shape == 1)
-      LK((label_tile_kernel<kLabelNT[1]><<<(unsigned)nltile, kLabelNT[1], 0, st>>>(I, flow, LF, LV, OF, OV, exf, exv,
-                                                                                 nex, ctx->status)));
+      LK((label_tile_kernel<kLabelNT[1]><<<(unsigned)nltile, kLabelNT[1], kLSm, st>>>(I, flow, LF, LV, OF, OV, exf,
+                                                                                    exv, nex, ctx->status)));
     else
-      LK((label_tile_kernel<kLabelNT[0]><<<(unsigned)nltile, kLabelNT[0], 0, st>>>(I, flow, LF, LV, OF, OV, exf, exv,
-                                                                                 nex, ctx->status)));
+      LK((label_tile_kernel<kLabelNT[0]><<<(unsigned)nltile, kLabelNT[0], kLSm, st>>>(I, flow, LF, LV, OF, OV, exf,
+                                                                                    exv, nex, ctx->status)));
     LAUNCH_CHECK("label_tile_kernel");
     int per = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, label_exit_kernel<true>, 256, 0));

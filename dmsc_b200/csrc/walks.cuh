@@ -216,19 +216,24 @@ __device__ __forceinline__ int tile_label(const TileRanks& R, int j, const int* 
   return __ldg(lab + rank);
 }
 
-// In-tile resolution. Every (side, cell) of the tile has one 32-bit state:
-// pending (kPend | j: the cell's path continues at tile cell j) or final, an
-// entry: (label << 1) | 1 when the path ends at a critical cell of the tile
-// (label -1 encodes as all ones), or (border-map index of the cell the path
-// enters next, in the neighbouring tile) << 1. The states start at the cell's
-// successor (decoded once from its flow code); then every thread jumps its own
-// cells' pointers, st[i] = st[st[i]], without block barriers: each value read
-// is a state of a cell further along the same path (written by any thread, at
-// any time), so a pointer only moves toward the path's end and reaches it in
-// at most the path's length of jumps, about log2 of it when the cells ahead
-// jump too. Border-map indices and labels stay below 2^30, so the top two bits
-// tell a pending state apart.
+// In-tile resolution. Every (side, cell) of the tile has a 16-bit successor
+// and a 32-bit state. A terminal cell (critical, or whose successor lies
+// outside the tile) has successor kTerm | itself and a final state from the
+// start: the entry (label << 1) | 1 of its extremum (label -1 encodes as all
+// ones), or (border-map index of the cell its path enters next, in the
+// neighbouring tile) << 1. Every other cell walks its successors for up to
+// kWalk steps (paths are short: means of 3.2 steps for faces and 1.5 for
+// vertices on the bench field) and takes the state of the terminal cell it
+// reaches; a cell still walking after kWalk steps becomes pending (kPend | the
+// cell reached), and pending cells then jump their pointers,
+// state = state of the pointed-to cell, without block barriers: any state
+// read belongs to a cell further along the same path (written by any thread,
+// at any time), so a pointer only moves toward the path's end and gets there
+// in at most the path's length of jumps. Border-map indices and labels stay
+// below 2^30, so the top two bits tell a pending state apart.
 constexpr uint32_t kPend = 0x40000000u, kCellMask = 0x0FFFu;
+constexpr unsigned kTerm = 0x8000u;
+constexpr int kWalk = 8;
 __device__ __forceinline__ bool st_pending(uint32_t v) { return (v >> 30) == 1u; }
 
 // Threads per label tile (the tuner picks one): each thread owns column
@@ -236,13 +241,18 @@ __device__ __forceinline__ bool st_pending(uint32_t v) { return (v >> 30) == 1u;
 constexpr int kLabelShapes = 2;
 constexpr int kLabelNT[kLabelShapes] = {1024, 512};
 
-// Initial state of a cell of the tile (FACES: face side) at tile position
-// (r, c); the cell is in the image.
+// Successor of the cell at tile position (r, c) (FACES: face side; the cell
+// is in the image) and, for a terminal cell, its final state.
 template <bool FACES>
-__device__ __forceinline__ uint32_t tile_init(const uint8_t (*fl)[kLT], const TileRanks& R, const int* __restrict__ lab,
-                                              int r, int c, int tile, int ntx) {
+__device__ __forceinline__ uint16_t tile_step(const uint8_t (*fl)[kLT], const TileRanks& R,
+                                              const int* __restrict__ lab, int r, int c, int tile, int ntx,
+                                              uint32_t* final_state) {
   const unsigned code = ((unsigned)fl[r][c] >> (FACES ? 4 : 0)) & 7u;
-  if (code == kFlowNone) return ((uint32_t)tile_label<FACES>(R, r * kLT + c, lab) << 1) | 1u;
+  const int i = r * kLT + c;
+  if (code == kFlowNone) {
+    *final_state = ((uint32_t)tile_label<FACES>(R, i, lab) << 1) | 1u;
+    return (uint16_t)(kTerm | i);
+  }
   int nr = r, nc = c, nt = tile;
   if (code == kFlowLeft) {
     if (--nc < 0) {
@@ -265,8 +275,11 @@ __device__ __forceinline__ uint32_t tile_init(const uint8_t (*fl)[kLT], const Ti
       nr = 0;
     }
   }
-  if (nt != tile) return (uint32_t)(((long long)nt * kPerim + perim_slot(nr, nc)) << 1);
-  return kPend | (uint32_t)(nr * kLT + nc);
+  if (nt != tile) {
+    *final_state = (uint32_t)(((long long)nt * kPerim + perim_slot(nr, nc)) << 1);
+    return (uint16_t)(kTerm | i);
+  }
+  return (uint16_t)(nr * kLT + nc);
 }
 
 // Follows border-map entries to a label.
@@ -293,14 +306,25 @@ __device__ __forceinline__ int label_ntx(const LabelTile& g) { return (g.W + kLT
 // cells also get their border-map entries; a cell whose path leaves the tile
 // is appended to its side's exit list (global index, entry) and finished by
 // label_exit_kernel once every tile's border map is written.
+// Shared memory of a label tile (55 KB: dynamic shared memory).
+struct LabelSmem {
+  uint32_t st[2][kLTN];
+  uint16_t succ[2][kLTN];
+  uint8_t fl[kLT][kLT];
+  TileRanks R;
+};
+
 template <int NT>
 __global__ void __launch_bounds__(NT, 2048 / NT) label_tile_kernel(Imgs I, const uint8_t* __restrict__ flow,
                                                                    LabelSide F, LabelSide V, LabelOut OF, LabelOut OV,
                                                                    int2* __restrict__ exits_f, int2* __restrict__ exits_v,
                                                                    int* __restrict__ n_exits, unsigned* status) {
-  __shared__ uint8_t fl[kLT][kLT];
-  __shared__ uint32_t st[2][kLTN];
-  __shared__ TileRanks R;
+  extern __shared__ __align__(16) unsigned char label_smem[];
+  LabelSmem& SM = *reinterpret_cast<LabelSmem*>(label_smem);
+  uint8_t (*fl)[kLT] = SM.fl;
+  uint16_t (*succ)[kLTN] = SM.succ;
+  uint32_t (*st)[kLTN] = SM.st;
+  TileRanks& R = SM.R;
   constexpr int kTileCells = kLTN / NT, kStep = NT / kLT;
   const LabelTile g = label_tile_of(I, blockIdx.x);
   const bool d = I.dual[g.b];
@@ -315,18 +339,41 @@ __global__ void __launch_bounds__(NT, 2048 / NT) label_tile_kernel(Imgs I, const
   const int c = threadIdx.x % kLT, rb = threadIdx.x / kLT;
   const int ntx = label_ntx(g);
   const bool do_f = F.perim != nullptr, do_v = V.perim != nullptr;
-  // initial states; bit 2k + side of `pend`: the state of cell k is a pointer
-  unsigned pend = 0;
+  // successors; terminal cells get their final state (cells outside the
+  // image are terminal and never reached)
 #pragma unroll
   for (int k = 0; k < kTileCells; ++k) {
     const int r = rb + kStep * k, i = r * kLT + c;
     const int y = g.y0 + r, x = g.x0 + c;
-    uint32_t a = 1u, b = 1u;  // cells outside the image: never reached, never written
-    if (do_f && y <= g.H && x <= g.W) a = tile_init<true>(fl, R, F.lab, r, c, blockIdx.x, ntx);
-    if (do_v && y < g.H && x < g.W) b = tile_init<false>(fl, R, V.lab, r, c, blockIdx.x, ntx);
-    st[0][i] = a;
-    st[1][i] = b;
-    pend |= (unsigned)st_pending(a) << (2 * k) | (unsigned)st_pending(b) << (2 * k + 1);
+    uint32_t a = 1u, b = 1u;
+    uint16_t sa = (uint16_t)(kTerm | i), sb = sa;
+    if (do_f && y <= g.H && x <= g.W) sa = tile_step<true>(fl, R, F.lab, r, c, blockIdx.x, ntx, &a);
+    if (do_v && y < g.H && x < g.W) sb = tile_step<false>(fl, R, V.lab, r, c, blockIdx.x, ntx, &b);
+    succ[0][i] = sa;
+    succ[1][i] = sb;
+    if (sa & kTerm) st[0][i] = a;
+    if (sb & kTerm) st[1][i] = b;
+  }
+  __syncthreads();
+  // short walks to the terminal cell; bit 2k + side of `pend`: still walking
+  unsigned pend = 0;
+#pragma unroll
+  for (int q = 0; q < 2 * kTileCells; ++q) {
+    const int sd = q & 1, i = (rb + kStep * (q >> 1)) * kLT + c;
+    unsigned cur = succ[sd][i];
+    if (cur & kTerm) continue;
+    unsigned nx = succ[sd][cur];
+#pragma unroll 1
+    for (int w = 1; w < kWalk && !(nx & kTerm); ++w) {
+      cur = nx;
+      nx = succ[sd][cur];
+    }
+    if (nx & kTerm) {
+      st[sd][i] = st[sd][cur];  // cur is terminal: its state is final
+    } else {
+      st[sd][i] = kPend | cur;
+      pend |= 1u << q;
+    }
   }
   __syncthreads();
   {  // barrier-free pointer jumping of this thread's pending cells (only this
