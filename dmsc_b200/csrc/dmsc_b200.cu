@@ -45,7 +45,7 @@ enum Slot {
 };
 enum SideSlot {
   X_SWEEP, X_RANK, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
-  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_BLEN, X_CKEY, X_CVAL, X_NODE,
+  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_CKEY, X_CVAL, X_NODE,
   X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
   X_GBASE, X_LAB, X_WX, X_WA, X_CENDS, kSideSlots
 };
@@ -77,7 +77,6 @@ struct Side {
   float* val = nullptr;
   const int2* key = nullptr;  // (value bits, cell) per extremum
   int* t = nullptr;
-  int* steps = nullptr;
   int* sweep = nullptr;
   int* dying = nullptr;
   int* pair_dense = nullptr;
@@ -510,7 +509,7 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   int2* cends = sget<int2>(ctx, si, X_CENDS, nsad);
   if (nsad > 0) {
     LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(
-        nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.sweep, S.dying, get<float>(ctx, S_SVAL, nsad), S.val,
+        nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.dying, get<float>(ctx, S_SVAL, nsad), S.val,
         S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.t, cends));
     LAUNCH_CHECK("persistence_kernel");
   }
@@ -541,14 +540,12 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
 // with n_cancel == nullptr when the side has no cancellation to replay.
 ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   const int nsad = ctx->nsad, M = S.M;
-  S.blen = sget<long long>(ctx, si, X_BLEN, 2 * (size_t)nsad);
-  if (nsad > 0) LK(base_len_kernel<<<grid_for(2LL * nsad, TB), TB, 0, st>>>(2 * nsad, S.t, S.steps, S.blen));
   unsigned long long* ckey = sget<unsigned long long>(ctx, si, X_CKEY, nsad);
   int* cval = sget<int>(ctx, si, X_CVAL, nsad);
   int* cnt = sget<int>(ctx, si, X_CNT, 8);
   CK(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), st));
   if (nsad > 0)
-    LK(cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.sweep, S.dying, S.pers, ctx->I.thr,
+    LK(cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.dying, S.pers, ctx->I.thr,
                                                                ctx->sad_img, ctx->crit_sad, ckey, cval, cnt + 3));
   LAUNCH_CHECK("cancel_collect_kernel");
 
@@ -560,7 +557,6 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   A.n_cancel = S.C > 0 ? cnt + 3 : nullptr;
   A.key = ckey;
   A.cj = cval;
-  A.sweep = S.sweep;
   A.dying = S.dying;
   A.t = S.t;
   A.blen = S.blen;
@@ -817,9 +813,9 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
 
   // ---- K4 saddle walks ----
   int* tf = get<int>(ctx, S_TF, 2 * (size_t)nsad);
-  int* lf = get<int>(ctx, S_LF, 2 * (size_t)nsad);
+  long long* lf = get<long long>(ctx, S_LF, 2 * (size_t)nsad);  // raw-arc lengths (cells)
   int* tv = get<int>(ctx, S_TV, 2 * (size_t)nsad);
-  int* lv = get<int>(ctx, S_LV, 2 * (size_t)nsad);
+  long long* lv = get<long long>(ctx, S_LV, 2 * (size_t)nsad);
   if (nsad > 0) {
     LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(I, flow, nsad, csad, isad, off[2], bmax, off[0], bmin, tf,
                                                              lf, tv, lv,
@@ -845,9 +841,9 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   F.key = kmax;
   V.key = kmin;
   F.t = tf;
-  F.steps = lf;
+  F.blen = lf;
   V.t = tv;
-  V.steps = lv;
+  V.blen = lv;
   // faces: ridges/peaks in the primal, valleys/basins in the dual (workspace.hxx:322-362)
   F.arcs_primal = f_ridges;
   F.arcs_dual = f_valleys;

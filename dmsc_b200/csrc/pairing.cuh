@@ -74,7 +74,6 @@ __global__ void sweep_edges_kernel(int nsad, const int* __restrict__ asc, const 
 __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_side, const uint8_t* __restrict__ dual,
                                                           const float* __restrict__ thr,
                                                           const int* __restrict__ sad_img,
-                                                          const int* __restrict__ sweep,
                                                           const int* __restrict__ dying,
                                                           const float* __restrict__ sad_val,
                                                           const float* __restrict__ ext_val,
@@ -83,10 +82,11 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
                                                           uint8_t* __restrict__ alive, int* __restrict__ n_cancel,
                                                           const int* __restrict__ t,
                                                           int2* __restrict__ canc_ends) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  // saddles in list order: every per-saddle access is sequential
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
   bool canc = false;
-  if (j < nsad) {
-    const int s = sweep[j], d = dying[s];
+  if (s < nsad) {
+    const int d = dying[s];
     if (d < 0) {
       pair_dense[s] = -1;
       pers[s] = -1.0f;
@@ -110,10 +110,7 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
   }
   // cancelled edges' ends, compacted for the thresholded union-find
   const int slot = block_append(n_cancel, canc);
-  if (canc) {
-    const int s = sweep[j];
-    canc_ends[slot] = make_int2(t[2 * s], t[2 * s + 1]);
-  }
+  if (canc) canc_ends[slot] = make_int2(t[2 * s], t[2 * s + 1]);
 }
 
 // Thresholded union-find (the reference's uf_min / uf_max, persistence.hxx:

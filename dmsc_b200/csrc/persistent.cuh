@@ -317,8 +317,7 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
 struct ReplayArgs {
   const int* n_cancel;               // device count of cancellations
   const unsigned long long* key;     // [C] replay key of each cancellation
-  const int* cj;                     // [C] sweep index of each cancellation
-  const int* sweep;
+  const int* cj;                     // [C] saddle (list index) of each cancellation
   const int* dying;  // [nsad] in saddle list order
   const int* t;      // [2 nsad] extremum ends of each saddle, list order
   const long long* blen;
@@ -344,8 +343,7 @@ struct ReplayArgs2 {
 
 __device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r, int round) {
   const unsigned long long t = A.key[r];
-  int j = A.cj[r];
-  const int s = A.sweep[j], d = A.dying[s];
+  const int s = A.cj[r], d = A.dying[s];
   // both walks resume where the previous round left them
   int R0 = A.wx[2 * r], R1 = A.wx[2 * r + 1];
   long long a0 = A.wa[2 * r], a1 = A.wa[2 * r + 1];
@@ -389,8 +387,7 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
     const int C = *A.n_cancel;
     for (long long r = tid; r < C; r += nth) {
       A.act0[r] = (int)r;
-      const int j = A.cj[r];
-      const int s = A.sweep[j];
+      const int s = A.cj[r];
       int d = A.dying[s];
       A.S.node[d].ctime = A.key[r];
       A.S.node[d].status = kPending;
@@ -437,7 +434,7 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
         const ReplayArgs& A = i < na ? P.s[0] : P.s[1];
         const long long k = i < na ? i : i - na;
         const int r = ((rd & 1) ? A.act1 : A.act0)[k];
-        A.S.node[A.dying[A.sweep[A.cj[r]]]].status = kRootForever;
+        A.S.node[A.dying[A.cj[r]]].status = kRootForever;
       }
       break;
     }

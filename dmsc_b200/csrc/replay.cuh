@@ -157,38 +157,28 @@ __device__ __forceinline__ bool walk_resume(const ReplayState& S, int* x_io, uns
 // (CancelEvent::operator<, cpu/persistence_struct.hxx:16-21): (persistence,
 // saddle cell); a saddle is cancelled at most once per side, so the pair is
 // unique and the target cell never breaks a tie.
-__global__ void __launch_bounds__(256) cancel_collect_kernel(int nsad, const int* __restrict__ sweep,
-                                                             const int* __restrict__ dying,
+__global__ void __launch_bounds__(256) cancel_collect_kernel(int nsad, const int* __restrict__ dying,
                                                              const float* __restrict__ pers,
                                                              const float* __restrict__ thr,
                                                              const int* __restrict__ sad_img,
                                                              const int* __restrict__ crit_sad,
                                                              unsigned long long* __restrict__ keys,
                                                              int* __restrict__ vals, int* __restrict__ count) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;  // saddles in list order
   bool take = false;
   unsigned long long key = 0;
-  if (j < nsad && dying[sweep[j]] >= 0) {
-    float p = pers[sweep[j]];
-    if (p <= thr[sad_img[sweep[j]]]) {
+  if (s < nsad && dying[s] >= 0) {
+    float p = pers[s];
+    if (p <= thr[sad_img[s]]) {
       take = true;
-      key = ((unsigned long long)orderable_key(p) << 32) | (unsigned)crit_sad[sweep[j]];
+      key = ((unsigned long long)orderable_key(p) << 32) | (unsigned)crit_sad[s];
     }
   }
   int pos = block_append(count, take);
   if (take) {
     keys[pos] = key;
-    vals[pos] = j;
+    vals[pos] = s;
   }
-}
-
-// Base arc length in cells: steps + 1 for a valid arc, 0 otherwise
-// (cpu/arcs_geometry.hxx:35-49, 83-111).
-__global__ void base_len_kernel(int n2, const int* __restrict__ t, const int* __restrict__ steps,
-                                long long* __restrict__ blen) {
-  int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n2) return;
-  blen[a] = t[a] >= 0 ? (long long)steps[a] + 1 : 0;
 }
 
 // Final arcs of the surviving saddles: length and the chain root of each

@@ -76,8 +76,8 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
                                                           const uint32_t* __restrict__ max_bits,
                                                           const int* __restrict__ off_min,
                                                           const uint32_t* __restrict__ min_bits, int* __restrict__ tf,
-                                                          int* __restrict__ lf, int* __restrict__ tv,
-                                                          int* __restrict__ lv, long long cap, unsigned* status) {
+                                                          long long* __restrict__ lf, int* __restrict__ tv,
+                                                          long long* __restrict__ lv, long long cap, unsigned* status) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsad) return;
   const int b = sad_img[s];
@@ -87,20 +87,21 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
   for (int j = 0; j < 2; ++j) {
     long long steps;
     int end = flow_walk<4>(flow, face_start(sc, j, Nx) >> 2, Nx, cap, &steps, status);
-    tf[2 * s + j] = seg_rank(I, b, end, Nx, off_max, max_bits);
-    lf[2 * s + j] = (int)steps;
+    const int target = seg_rank(I, b, end, Nx, off_max, max_bits);
+    tf[2 * s + j] = target;
+    lf[2 * s + j] = target >= 0 ? steps + 1 : 0;  // cells of the raw arc, start and end included
   }
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
     int start = vertex_start(sc, j, H, W, Nx, I.idx_base[b]);
     long long steps = 0;
+    int target = -1;
     if (start >= 0) {
       int end = flow_walk<0>(flow, start >> 2, Nx, cap, &steps, status);
-      tv[2 * s + j] = seg_rank(I, b, end, Nx, off_min, min_bits);
-    } else {
-      tv[2 * s + j] = -1;
+      target = seg_rank(I, b, end, Nx, off_min, min_bits);
     }
-    lv[2 * s + j] = (int)steps;
+    tv[2 * s + j] = target;
+    lv[2 * s + j] = target >= 0 ? steps + 1 : 0;  // an arc that leaves the image is empty
   }
 }
 
