@@ -707,6 +707,23 @@ def tune_section(args, img, dev, size):
             "default_ms": rep["default_ms"], "tuned_ms": rep["tuned_ms"], "stage_medians_ms": rep["stages"]}
 
 
+def profile_workload(args):
+    """Workload for profiler captures (prints no measurement): the bump field
+    of --size generated on the host, one warm-up call of three variants, then
+    --profile-calls calls of (is_dual=False, threshold 0.05). A capture that
+    skips the launches of the warm-up calls sees exactly the timed calls."""
+    from dmsc_b200 import compute_dmsc
+    from dmsc_b200.synthetic import field_4096_bumps
+
+    img = field_4096_bumps(seed=SEED, size=args.size).cuda()
+    for d, t in ((False, 0.0), (True, 0.05), (False, 0.05)):
+        compute_dmsc(img, t, is_dual=d)
+    torch.cuda.synchronize()
+    for _ in range(args.profile_calls):
+        compute_dmsc(img, 0.05)
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -719,7 +736,12 @@ def main():
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiation workload")
     ap.add_argument("--c3-size", type=int, default=16384, help="worst-case U[0,1) field size (0: skip)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape tuner section")
+    ap.add_argument("--profile-calls", type=int, default=0,
+                    help="run the profiler workload (warm-up, then this many calls) and exit")
     args = ap.parse_args()
+    if args.profile_calls > 0:
+        profile_workload(args)
+        return
     if args.impl == "reference":
         reference_arm(args)
     else:
