@@ -710,8 +710,9 @@ def tune_section(args, img, dev, size):
 def profile_workload(args):
     """Workload for profiler captures (prints no measurement): the bump field
     of --size generated on the host, one warm-up call of three variants, then
-    --profile-calls calls of (is_dual=False, threshold 0.05). A capture that
-    skips the launches of the warm-up calls sees exactly the timed calls."""
+    --profile-calls calls of variant --profile-variant (default 1: is_dual=False,
+    threshold 0.05). A capture that skips the launches of the warm-up calls sees
+    exactly the profiled calls."""
     from dmsc_b200 import compute_dmsc
     from dmsc_b200.synthetic import field_4096_bumps
 
@@ -719,8 +720,9 @@ def profile_workload(args):
     for d, t in ((False, 0.0), (True, 0.05), (False, 0.05)):
         compute_dmsc(img, t, is_dual=d)
     torch.cuda.synchronize()
+    d, t = VARIANTS[args.profile_variant]
     for _ in range(args.profile_calls):
-        compute_dmsc(img, 0.05)
+        compute_dmsc(img, t, is_dual=d)
     torch.cuda.synchronize()
 
 
@@ -738,6 +740,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape tuner section")
     ap.add_argument("--profile-calls", type=int, default=0,
                     help="run the profiler workload (warm-up, then this many calls) and exit")
+    ap.add_argument("--profile-variant", type=int, default=1, choices=range(4),
+                    help="variant of the profiled calls (index into the bench's (is_dual, threshold) variants)")
     args = ap.parse_args()
     if args.profile_calls > 0:
         profile_workload(args)

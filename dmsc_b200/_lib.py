@@ -41,7 +41,7 @@ EXPORTS = (
     "dmsc_b200_critical_cells_static",
 )
 
-STAGES = ("setup", "gradient", "compaction", "saddle_sort", "saddle_walks", "pairing", "persistence_and_ranks", "survivors",
+STAGES = ("setup", "gradient", "compaction", "saddle_walks", "pairing", "persistence_and_ranks", "survivors",
           "replay", "final_arcs", "label_setup", "labels", "sizes", "fetch_lists", "fetch_geometry")
 
 ERR_TOO_LARGE = 2
@@ -56,7 +56,8 @@ class Sizes(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("grad_shape", "label_shape", "pair_blocks_per_sm",
-                                            "replay_blocks_per_sm", "emit_blocks_per_sm", "seg_cursors")]
+                                            "replay_blocks_per_sm", "emit_blocks_per_sm", "seg_cursors",
+                                            "pair_shape", "replay_shape", "emit_shape")]
 
 
 class Outputs(ctypes.Structure):
@@ -193,25 +194,28 @@ class Context:
         return t
 
     def tuning_limits(self) -> dict:
-        buf = (ctypes.c_int * 6)()
-        if self.lib.dmsc_b200_tuning_limits(self.h, buf, 6) != 6:
+        buf = (ctypes.c_int * 9)()
+        if self.lib.dmsc_b200_tuning_limits(self.h, buf, 9) != 9:
             raise RuntimeError("dmsc_b200_tuning_limits failed")
         return dict(zip(("grad_shapes", "label_shapes", "pair_blocks_per_sm", "replay_blocks_per_sm",
-                         "emit_blocks_per_sm", "seg_cursors"), list(buf)))
+                         "emit_blocks_per_sm", "seg_cursors", "pair_shapes", "replay_shapes", "emit_shapes"),
+                        list(buf)))
 
     def set_wait_timeout(self, seconds: float):
         self.check(self.lib.dmsc_b200_set_wait_timeout(self.h, float(seconds)), "dmsc_b200_set_wait_timeout")
 
-    def timelines(self) -> dict:
-        """Per-round / per-level durations (us) of the device loops of the last call."""
-        buf = (ctypes.c_longlong * 384)()
-        if self.lib.dmsc_b200_pairing_timeline(self.h, buf, 384) < 0:
+    def timelines(self, counts: bool = False) -> dict:
+        """Per-round / per-level durations (us) of the device loops of the last
+        call; with ``counts``, (durations, items per round) per loop."""
+        buf = (ctypes.c_longlong * 768)()
+        if self.lib.dmsc_b200_pairing_timeline(self.h, buf, 768) < 0:
             return {}
         out = {}
         for blk, name in enumerate(("pairing_faces", "pairing_vertices", "emit_faces", "emit_vertices",
                                     "replay_faces", "replay_vertices")):
             t = [x for x in (buf[blk * 64 + k] for k in range(64)) if x > 0]
-            out[name] = tuple((b - a) / 1000.0 for a, b in zip(t, t[1:]))
+            d = tuple((b - a) / 1000.0 for a, b in zip(t, t[1:]))
+            out[name] = (d, tuple(buf[384 + blk * 64 + k] for k in range(len(t)))) if counts else d
         return out
 
     def close(self):

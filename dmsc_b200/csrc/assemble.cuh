@@ -58,19 +58,67 @@ __global__ void points_kernel(int n, const uint8_t* __restrict__ alive, const in
   if (dst) dst[to_out_excl[x] - alive_base[b]] = cell[x] - 4 * I.idx_base[b];
 }
 
-// flag[j] = 1 when the saddle at minima-sweep position j survives both sides.
-__global__ void survivor_flag_kernel(int nsad, const int* __restrict__ sweep_min, const uint8_t* __restrict__ cancelled,
-                                     int* __restrict__ flag) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nsad) return;
-  flag[j] = cancelled[sweep_min[j]] == 0;
+// flag[s] = 1 when saddle s (list order) survives both sides.
+__global__ void survivor_flag_kernel(int nsad, const uint8_t* __restrict__ cancelled, int* __restrict__ flag) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsad) return;
+  flag[s] = cancelled[s] == 0;
 }
 
-__global__ void survivor_list_kernel(int nsad, const int* __restrict__ sweep_min, const int* __restrict__ flag,
-                                     const int* __restrict__ pos, int* __restrict__ surv_sad) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= nsad) return;
-  if (flag[j]) surv_sad[pos[j]] = sweep_min[j];
+// The survivors in list order with their sort keys ((image, s_val) order).
+template <class K>
+__global__ void survivor_gather_kernel(int nsad, const int* __restrict__ flag, const int* __restrict__ pos,
+                                       const K* __restrict__ key, K* __restrict__ key_out, int* __restrict__ idx_out) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsad || !flag[s]) return;
+  key_out[pos[s]] = key[s];
+  idx_out[pos[s]] = s;
+}
+
+// Surviving saddles in the vertex side's sweep order (arcs_topology.hxx:99-102):
+// `sorted` lists them by ascending (image, s_val, cell id); an image whose
+// vertex side sweeps descending (dual) takes its range reversed.
+__global__ void survivor_order_kernel(int n, const int* __restrict__ sorted, const int* __restrict__ sad_img,
+                                      const uint8_t* __restrict__ dual, const int* __restrict__ surv_base,
+                                      int* __restrict__ surv) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int s = sorted[p], b = sad_img[s];
+  int q = p;
+  if (dual[b]) {
+    const int base = surv_base[b], cnt = surv_base[b + 1] - base;
+    q = base + cnt - 1 - (p - base);
+  }
+  surv[q] = s;
+}
+
+// Per-survivor records gathered once in output (sweep) order, so the later
+// per-survivor kernels read them in order instead of gathering from the
+// list-ordered saddle arrays again: the image and cell of every survivor,
+// and per side its arc ends, raw-arc lengths and the record of its outputs
+// (out ranks of its ends' thresholded roots, persistence, out rank of its
+// pair's root; -1 for the void).
+__global__ void surv_common_kernel(int nsurv, const int* __restrict__ surv, const int* __restrict__ sad_img,
+                                   const int* __restrict__ crit_sad, int2* __restrict__ ic) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsurv) return;
+  const int s = surv[i];
+  ic[i] = make_int2(sad_img[s], crit_sad[s]);
+}
+
+__global__ void surv_side_kernel(int nsurv, const int* __restrict__ surv, const int* __restrict__ t,
+                                 const long long* __restrict__ blen, const float* __restrict__ pers,
+                                 const int* __restrict__ pair_dense, const int* __restrict__ rout,
+                                 int2* __restrict__ sv_t, longlong2* __restrict__ sv_len, int4* __restrict__ sv_rec) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsurv) return;
+  const int s = surv[i];
+  const int2 tt = *reinterpret_cast<const int2*>(t + 2 * s);
+  sv_t[i] = tt;
+  sv_len[i] = *reinterpret_cast<const longlong2*>(blen + 2 * s);
+  const int pd = pair_dense[s];
+  sv_rec[i] = make_int4(tt.x >= 0 ? rout[tt.x] : -1, tt.y >= 0 ? rout[tt.y] : -1, __float_as_int(pers[s]),
+                        pd >= 0 ? rout[pd] : -1);
 }
 
 // Per-image first positions (B + 1 entries, the last one the total):
@@ -102,64 +150,55 @@ __device__ __forceinline__ int visit(int q, bool reversed, const int* __restrict
   return base + n - 1 - (q - base);
 }
 
-// e rows of one survivor (cpu/workspace.hxx:175-195, 197-219): (0..2) ends
-// as batch-wide output ranks.
-__device__ __forceinline__ int erow_ends(int s, const int* __restrict__ t, const int* __restrict__ ut,
-                                         const int* __restrict__ to_out, int* o1, int* o2) {
-  int c1 = t[2 * s], c2 = t[2 * s + 1];
-  int r1 = c1 >= 0 ? ut[c1] : -1;
-  int r2 = c2 >= 0 ? ut[c2] : -1;
+// e rows of one survivor (cpu/workspace.hxx:175-195, 197-219) from the out
+// ranks of its ends' roots (-1: the void; a thresholded root is always an
+// alive extremum, so it always has an out rank): up to two ends.
+__device__ __forceinline__ int erow_ends(int r1, int r2, int* o1, int* o2) {
   int n = 0;
-  if (r1 != -1 && to_out[r1] != -1) {
-    *o1 = to_out[r1];
+  if (r1 != -1) {
+    *o1 = r1;
     n = 1;
   }
-  if (r1 != r2 && r2 != -1 && to_out[r2] != -1) {
+  if (r1 != r2 && r2 != -1) {
     if (n == 0)
-      *o1 = to_out[r2];
+      *o1 = r2;
     else
-      *o2 = to_out[r2];
+      *o2 = r2;
     n++;
   }
   return n;
 }
 
 __global__ void erow_count_kernel(int nsurv, bool reversed, const int* __restrict__ surv_base, int B,
-                                  const int* __restrict__ surv_sad, const int* __restrict__ t,
-                                  const int* __restrict__ ut, const int* __restrict__ to_out, int* __restrict__ cnt) {
+                                  const int4* __restrict__ sv_rec, int* __restrict__ cnt) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nsurv) return;
   int b;
-  int i = visit(q, reversed, surv_base, B, &b);
+  const int i = visit(q, reversed, surv_base, B, &b);
+  const int4 r = sv_rec[i];
   int a, c;
-  cnt[q] = erow_ends(surv_sad[i], t, ut, to_out, &a, &c);
+  cnt[q] = erow_ends(r.x, r.y, &a, &c);
 }
 
 // Per-survivor scalars and e rows of one side. `row_off` is the batch-wide
 // exclusive scan of the row counts in visiting order; `row_base[b]` its value
 // at image b's first survivor.
 __global__ void side_outputs_kernel(int nsurv, bool reversed, const int* __restrict__ surv_base, Imgs I,
-                                    const int* __restrict__ surv_sad, const int* __restrict__ t,
-                                    const int* __restrict__ ut, const int* __restrict__ to_out,
-                                    const int* __restrict__ alive_base, const float* __restrict__ pers,
-                                    const int* __restrict__ pair_dense, const int* __restrict__ row_off,
-                                    const int* __restrict__ row_base, RouteF P, Route PP, Route E) {
+                                    const int4* __restrict__ sv_rec, const int* __restrict__ alive_base,
+                                    const int* __restrict__ row_off, const int* __restrict__ row_base, RouteF P,
+                                    Route PP, Route E) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nsurv) return;
   int b;
   int i = visit(q, reversed, surv_base, I.B, &b);
   const bool d = I.dual[b];
   const int li = i - surv_base[b];
-  int s = surv_sad[i];
-  if (float* p = P.at(d, b)) p[li] = pers[s];
-  if (int* pp = PP.at(d, b)) {
-    int pd = pair_dense[s];
-    int r = pd >= 0 ? ut[pd] : -1;
-    pp[li] = r >= 0 ? to_out[r] - alive_base[b] : -1;
-  }
+  const int4 r = sv_rec[i];
+  if (float* p = P.at(d, b)) p[li] = __int_as_float(r.z);
+  if (int* pp = PP.at(d, b)) pp[li] = r.w >= 0 ? r.w - alive_base[b] : -1;
   if (int* e = E.at(d, b)) {
     int a = 0, c = 0;
-    int n = erow_ends(s, t, ut, to_out, &a, &c);
+    int n = erow_ends(r.x, r.y, &a, &c);
     int o = row_off[q] - row_base[b];
     if (n >= 1) {
       e[2 * o] = li;
@@ -172,14 +211,13 @@ __global__ void side_outputs_kernel(int nsurv, bool reversed, const int* __restr
   }
 }
 
-__global__ void sad_pts_kernel(int nsurv, const int* __restrict__ surv_sad, const int* __restrict__ crit_sad,
-                               const int* __restrict__ sad_img, const int* __restrict__ surv_base, Imgs I,
+__global__ void sad_pts_kernel(int nsurv, const int2* __restrict__ surv_ic, const int* __restrict__ surv_base, Imgs I,
                                int* __restrict__ out, const int* __restrict__ out_off) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsurv) return;
-  int s = surv_sad[i];
-  int b = sad_img[s];
-  out[out_off[b] + (i - surv_base[b])] = crit_sad[s] - 4 * I.idx_base[b];
+  const int2 ic = surv_ic[i];
+  const int b = ic.x;
+  out[out_off[b] + (i - surv_base[b])] = ic.y - 4 * I.idx_base[b];
 }
 
 __global__ void pair_len_kernel(int nsurv, const long long* __restrict__ arc_len, long long* __restrict__ out) {
@@ -200,13 +238,13 @@ __global__ void geom_base_kernel(int B, const int* __restrict__ surv_base, int n
 // Output position of every arc: the image's destination offset plus the
 // arc's position inside the image's geometry.
 __global__ void arc_pos_kernel(int nsurv, const long long* __restrict__ arc_len,
-                               const long long* __restrict__ saddle_end_incl, const int* __restrict__ surv_sad,
-                               const int* __restrict__ sad_img, const long long* __restrict__ gbase,
-                               const int* __restrict__ dst_off, long long* __restrict__ arc_pos) {
+                               const long long* __restrict__ saddle_end_incl, const int2* __restrict__ surv_ic,
+                               const long long* __restrict__ gbase, const int* __restrict__ dst_off,
+                               long long* __restrict__ arc_pos) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsurv) return;
   long long start = saddle_end_incl[i] - arc_len[2 * i] - arc_len[2 * i + 1];
-  const int b = sad_img[surv_sad[i]];
+  const int b = surv_ic[i].x;
   start += (long long)dst_off[b] - gbase[b];
   arc_pos[2 * i] = start;
   arc_pos[2 * i + 1] = start + arc_len[2 * i];

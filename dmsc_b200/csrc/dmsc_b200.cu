@@ -40,11 +40,11 @@ enum Slot {
   S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
   S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_MINBITS, S_MAXBITS, S_VMIN, S_VMAX, S_KMIN, S_KMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
   S_ASC, S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
-  S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX, S_SKEY32, S_SKEY32B,
+  S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX, S_SKEY32, S_SKEY32B, S_SKEYS, S_SURVIC,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
-  X_SWEEP, X_RANK, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
+  X_ROUT, X_SVT, X_SVL, X_SVR, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
   X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_CKEY, X_CVAL, X_NODE,
   X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
   X_GBASE, X_LAB, X_WX, X_WA, X_CENDS, kSideSlots
@@ -77,7 +77,10 @@ struct Side {
   float* val = nullptr;
   const int2* key = nullptr;  // (value bits, cell) per extremum
   int* t = nullptr;
-  int* sweep = nullptr;
+  int* rout = nullptr;              // [M] out rank of each extremum's thresholded root (-1: the void)
+  int2* sv_t = nullptr;             // [nsurv] per survivor (output order): arc ends
+  longlong2* sv_len = nullptr;      // raw-arc lengths
+  int4* sv_rec = nullptr;           // out ranks of the ends' roots, persistence, out rank of the pair's root
   int* dying = nullptr;
   int* pair_dense = nullptr;
   float* pers = nullptr;
@@ -127,6 +130,7 @@ struct dmsc_b200_context {
   int* crit_sad = nullptr;
   int* sad_img = nullptr;
   int* surv = nullptr;
+  int2* surv_ic = nullptr;  // [nsurv] image and cell of each survivor (output order)
   unsigned* status = nullptr;
   Side side[2];
   std::vector<dmsc_b200_sizes> sizes;
@@ -167,6 +171,9 @@ struct dmsc_b200_context {
   int grad_shape = 2;
   int label_shape = 1;
   int pair_per_sm = 0, replay_per_sm = 0, emit_per_sm = 0;
+  int pair_shape = 0;    // pairing items per thread batch: 0 -> 2, 1 -> 4
+  int replay_shape = 0;  // replay items per thread batch: 0 -> 1, 1 -> 2
+  int emit_shape = 0;    // expansion chain tasks per thread batch: 0 -> 1, 1 -> 2
   int seg_cursors = 1;  // raw-arc cursors per lane of the segment writer
   bool label_smem_set = false;  // dynamic shared memory limit raised for the label kernels
   int cap_pair_rounds = 0, cap_replay_rounds = 0, cap_emit_levels = 0;
@@ -450,26 +457,19 @@ void* staging(dmsc_b200_context* ctx, size_t bytes) {
 }
 
 // Sweep-ordered edges and the pairing arguments of one side (see pairing.cuh).
-PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, cudaStream_t st) {
+PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const float* sval) {
   const int nsad = ctx->nsad, M = S.M;
-  S.sweep = sget<int>(ctx, si, X_SWEEP, nsad);
   S.dying = sget<int>(ctx, si, X_DYING, nsad);  // list order
-  int* rank = sget<int>(ctx, si, X_RANK, nsad);
-  if (nsad > 0) {
-    LK(sweep_edges_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, asc, ctx->sad_img, ctx->bases.sad, ctx->I.dual,
-                                                             S.faces, S.sweep, rank));
-    LAUNCH_CHECK("sweep_edges_kernel");
-  }
   PairArgs A;
   A.nsad = nsad;
   A.M = M;
   A.t = S.t;
-  A.rank = rank;
-  A.sweep = S.sweep;
+  A.sval = sval;
+  A.sad_img = ctx->sad_img;
   A.g12 = sget<int2>(ctx, si, X_G12, nsad);
   A.dying = S.dying;
   A.link = sget<int>(ctx, si, X_LINK, M + 1);
-  A.minedge = sget<unsigned>(ctx, si, X_MINE, M + 1);
+  A.minedge = sget<unsigned long long>(ctx, si, X_MINE, M + 1);
   A.act0 = sget<int>(ctx, si, X_ACT0, nsad);
   A.act1 = sget<int>(ctx, si, X_ACT1, nsad);
   A.roots0 = sget<int>(ctx, si, X_GRP, M + 1);
@@ -483,16 +483,17 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const int* asc, c
   A.status = ctx->status;
   A.max_rounds = capped(M + 2, ctx->cap_pair_rounds);
   A.rounds = get<int>(ctx, S_STATS, 8) + 0 + si;
-  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline) + si * kTimeline;
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 12 * kTimeline) + si * kTimeline;
   return A;
 }
 
 // Both sides' pairing rounds in one cooperative launch.
-void run_pairing(dmsc_b200_context* ctx, const int* asc, cudaStream_t st) {
+void run_pairing(dmsc_b200_context* ctx, const float* sval, cudaStream_t st) {
   PairArgs2 P;
-  for (int si = 0; si < 2; ++si) P.s[si] = pairing_args(ctx, si, ctx->side[si], asc, st);
+  for (int si = 0; si < 2; ++si) P.s[si] = pairing_args(ctx, si, ctx->side[si], sval);
   if (ctx->nsad > 0)
-    coop_launch(ctx, pairing_persistent_kernel, P, st, "pairing_persistent_kernel", ctx->pair_per_sm);
+    coop_launch(ctx, ctx->pair_shape ? pairing_persistent_kernel<4, 4> : pairing_persistent_kernel<2, 5>, P, st,
+                "pairing_persistent_kernel", ctx->pair_per_sm);
 }
 
 // Persistence, cancellation, thresholded union-find and output ranks of one side.
@@ -507,10 +508,15 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   int* ncanc = get<int>(ctx, S_NCANC, 4) + si;
   CK(cudaMemsetAsync(ncanc, 0, sizeof(int), st));
   int2* cends = sget<int2>(ctx, si, X_CENDS, nsad);
+  // the replay's cancellation list (keys and saddles) comes out of the same
+  // pass when this side's arcs are simplified
+  unsigned long long* ckey = S.arcs ? sget<unsigned long long>(ctx, si, X_CKEY, nsad) : nullptr;
+  int* cval = S.arcs ? sget<int>(ctx, si, X_CVAL, nsad) : nullptr;
   if (nsad > 0) {
     LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(
         nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.dying, get<float>(ctx, S_SVAL, nsad), S.val,
-        S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.t, cends));
+        S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.t, cends, ctx->crit_sad, ckey,
+        cval));
     LAUNCH_CHECK("persistence_kernel");
   }
   // thresholded union-find roots
@@ -534,27 +540,26 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
     LK(to_out_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, S.alive, S.to_out_excl, S.to_out));
     LAUNCH_CHECK("to_out_kernel");
   }
+  S.rout = sget<int>(ctx, si, X_ROUT, M + 1);
+  if (M > 0) LK(root_out_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, S.ut, S.to_out, S.rout));
+  LAUNCH_CHECK("root_out_kernel");
 }
 
 // Replay inputs of one side (batch); returns the replay kernel's arguments,
 // with n_cancel == nullptr when the side has no cancellation to replay.
 ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   const int nsad = ctx->nsad, M = S.M;
+  // cancellations (keys, saddles, count) as the persistence pass listed them
   unsigned long long* ckey = sget<unsigned long long>(ctx, si, X_CKEY, nsad);
   int* cval = sget<int>(ctx, si, X_CVAL, nsad);
   int* cnt = sget<int>(ctx, si, X_CNT, 8);
-  CK(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), st));
-  if (nsad > 0)
-    LK(cancel_collect_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, S.dying, S.pers, ctx->I.thr,
-                                                               ctx->sad_img, ctx->crit_sad, ckey, cval, cnt + 3));
-  LAUNCH_CHECK("cancel_collect_kernel");
 
   ReplayState& R = S.R;
   R.node = sget<ReplayNode>(ctx, si, X_NODE, M + 1);
   LK(replay_node_init_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.node, M + 1));
   LAUNCH_CHECK("replay init");
   ReplayArgs A{};
-  A.n_cancel = S.C > 0 ? cnt + 3 : nullptr;
+  A.n_cancel = S.C > 0 ? get<int>(ctx, S_NCANC, 4) + si : nullptr;
   A.key = ckey;
   A.cj = cval;
   A.dying = S.dying;
@@ -570,7 +575,7 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   A.status = ctx->status;
   A.max_rounds = capped(nsad + 2, ctx->cap_replay_rounds);
   A.rounds = get<int>(ctx, S_STATS, 8) + 2 + si;
-  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline) + (4 + si) * kTimeline;
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 12 * kTimeline) + (4 + si) * kTimeline;
   return A;
 }
 
@@ -583,10 +588,9 @@ void replay_final(dmsc_b200_context* ctx, int si, Side& S, long long* total, cud
   S.arc_root = sget<int>(ctx, si, X_AROOT, 2 * (size_t)nsurv);
   S.plen = sget<long long>(ctx, si, X_PLEN, nsurv);
   S.send = sget<long long>(ctx, si, X_SEND, nsurv);
-  LK(final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->sad_img, ctx->I.dual,
-                                                                 S.arcs_primal, S.arcs_dual, S.t, S.blen, S.R,
-                                                                 ctx->nsad + 1, S.arc_len, S.arc_cl, S.arc_root,
-                                                                 ctx->status));
+  LK(final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv_ic, ctx->I.dual, S.arcs_primal,
+                                                                 S.arcs_dual, S.sv_t, S.sv_len, S.R, ctx->nsad + 1,
+                                                                 S.arc_len, S.arc_cl, S.arc_root, ctx->status));
   LK(pair_len_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.plen));
   incl_sum(ctx, S.plen, S.send, nsurv, st);
   LK(last_kernel<long long><<<1, 1, 0, st>>>(S.send, nsurv, total));
@@ -707,8 +711,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   mark(ctx, 0, st);
   CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
   CK(cudaMemsetAsync(get<int>(ctx, S_STATS, 8), 0, 8 * sizeof(int), st));
-  CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline), 0,
-                     6 * kTimeline * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, 12 * kTimeline), 0,
+                     12 * kTimeline * sizeof(unsigned long long), st));
   {  // upload the tables: 9 int arrays, then thr (float) and dual (u8)
     size_t ib = tab.size() * sizeof(int), fb = (size_t)B * sizeof(float);
     size_t total = ib + fb + B + 16;
@@ -798,19 +802,6 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   LAUNCH_CHECK("image_base_kernel");
   mark(ctx, 2, st);
 
-  // ---- saddle order: per image ascending (s_val, cell id) (arcs_topology.hxx:99-102) ----
-  int* iota = get<int>(ctx, S_IOTA, nsad);
-  int* asc = get<int>(ctx, S_ASC, nsad);
-
-  if (nsad > 0) {
-    LK(iota_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(iota, nsad));
-    if (B > 1)
-      sort_pairs(ctx, skey, get<unsigned long long>(ctx, S_SKEY2, nsad), iota, asc, nsad, st, 32 + bits_for(B));
-    else
-      sort_pairs(ctx, skey32, get<uint32_t>(ctx, S_SKEY32B, nsad), iota, asc, nsad, st, 32);
-  }
-  mark(ctx, 3, st);
-
   // ---- K4 saddle walks ----
   int* tf = get<int>(ctx, S_TF, 2 * (size_t)nsad);
   long long* lf = get<long long>(ctx, S_LF, 2 * (size_t)nsad);  // raw-arc lengths (cells)
@@ -861,7 +852,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
   mark(ctx, 4, st);
   CK(cudaMemsetAsync(canc, 0, nsad + 4, st));
-  run_pairing(ctx, asc, st);
+  run_pairing(ctx, sval, st);
   mark(ctx, 5, st);
   // the two sides' persistence, thresholded union-find and ranks are
   // independent (disjoint buffers; their cancellation bits are ORed into the
@@ -880,9 +871,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   ctx->surv = get<int>(ctx, S_SURV, nsad);
   ctx->nsurv = 0;
   if (nsad > 0) {
-    LK(survivor_flag_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, V.sweep, canc, flag));
+    LK(survivor_flag_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, canc, flag));
     excl_sum(ctx, flag, fpos, nsad, st);
-    LK(survivor_list_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(nsad, V.sweep, flag, fpos, ctx->surv));
     LK(last_plus_kernel<int><<<1, 1, 0, st>>>(fpos, flag, nsad, tot));
     LK(copy2_kernel<<<1, 1, 0, st>>>(get<int>(ctx, S_NCANC, 4), tot + 1));
     LAUNCH_CHECK("survivors");
@@ -900,6 +890,38 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   const int nsurv = ctx->nsurv;
   LK(image_base_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, BS.sad, nsad, fpos, nsurv, BS.surv));
   LAUNCH_CHECK("survivor bases");
+  if (nsurv > 0) {
+    // the survivors (list order) sorted by (image, s_val) with the list index
+    // as the stable tie-break, then each image's range in its vertex-side
+    // sweep direction (reversed for a dual image)
+    int* sidx = get<int>(ctx, S_IOTA, nsurv);
+    int* sorted = get<int>(ctx, S_ASC, nsurv);
+    if (B > 1) {
+      unsigned long long* k = get<unsigned long long>(ctx, S_SKEY2, nsurv);
+      LK(survivor_gather_kernel<unsigned long long><<<grid_for(nsad, TB), TB, 0, st>>>(nsad, flag, fpos, skey, k, sidx));
+      sort_pairs(ctx, k, get<unsigned long long>(ctx, S_SKEYS, nsurv), sidx, sorted, nsurv, st, 32 + bits_for(B));
+    } else {
+      uint32_t* k = get<uint32_t>(ctx, S_SKEY32B, nsurv);
+      LK(survivor_gather_kernel<uint32_t><<<grid_for(nsad, TB), TB, 0, st>>>(nsad, flag, fpos, skey32, k, sidx));
+      sort_pairs(ctx, k, get<uint32_t>(ctx, S_SKEYS, nsurv), sidx, sorted, nsurv, st, 32);
+    }
+    LK(survivor_order_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, sorted, ctx->sad_img, I.dual, BS.surv,
+                                                               ctx->surv));
+    LAUNCH_CHECK("survivor order");
+    // the survivors' records, gathered once in output order
+    ctx->surv_ic = get<int2>(ctx, S_SURVIC, nsurv);
+    LK(surv_common_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->sad_img, ctx->crit_sad,
+                                                            ctx->surv_ic));
+    for (int si = 0; si < 2; ++si) {
+      Side& S = ctx->side[si];
+      S.sv_t = sget<int2>(ctx, si, X_SVT, nsurv);
+      S.sv_len = sget<longlong2>(ctx, si, X_SVL, nsurv);
+      S.sv_rec = sget<int4>(ctx, si, X_SVR, nsurv);
+      LK(surv_side_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, S.t, S.blen, S.pers, S.pair_dense,
+                                                            S.rout, S.sv_t, S.sv_len, S.sv_rec));
+    }
+    LAUNCH_CHECK("survivor records");
+  }
   mark(ctx, 7, st);
 
   // ---- replay (both sides in one cooperative launch) + final arc lengths ----
@@ -914,7 +936,9 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
         any = any || RA.s[si].n_cancel != nullptr;
       }
     }
-    if (any) coop_launch(ctx, replay_persistent_kernel, RA, st, "replay_persistent_kernel", ctx->replay_per_sm);
+    if (any)
+      coop_launch(ctx, ctx->replay_shape ? replay_persistent_kernel<2, 3> : replay_persistent_kernel<1, 4>, RA, st,
+                  "replay_persistent_kernel", ctx->replay_per_sm);
     mark(ctx, 8, st);
     // geometry totals stay on the device (read back with the sizes)
     long long* tot = get<long long>(ctx, S_TOT, 8);
@@ -968,7 +992,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     L.lab = lab;
     L.perim = get<int>(ctx, S.faces ? S_PERF : S_PERV, (size_t)nltile * kPerim);
     if (S.M > 0)
-      LK(label_map_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.ext_img, S.ut, S.to_out, BS.alive[si], lab));
+      LK(label_map_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.ext_img, S.rout, BS.alive[si], lab));
     LAUNCH_CHECK("label_map_kernel");
   }
   int* nex = get<int>(ctx, S_NEX, 2);
@@ -1009,8 +1033,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     S.erow_off = sget<int>(ctx, si, X_EROWO, nsurv);
     long long* et = get<long long>(ctx, S_TOT, 8) + 6 + si;
     if (nsurv > 0) {
-      LK(erow_count_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, BS.surv, B, ctx->surv, S.t, S.ut,
-                                                               S.to_out, ec));
+      LK(erow_count_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, BS.surv, B, S.sv_rec, ec));
       excl_sum(ctx, ec, S.erow_off, nsurv, st);
       LK(last_plus_kernel<int><<<1, 1, 0, st>>>(S.erow_off, ec, nsurv, et));
     } else {
@@ -1093,8 +1116,8 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   LAUNCH_CHECK("arc_offsets_kernel");
   if (S.total <= 0 || (!flat_primal && !flat_dual)) return;
   long long* arc_pos = sget<long long>(ctx, si, X_APOS, 2 * (size_t)nsurv);
-  LK(arc_pos_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.send, ctx->surv, ctx->sad_img, S.gbase,
-                                                        dst_off, arc_pos));
+  LK(arc_pos_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.send, ctx->surv_ic, S.gbase, dst_off,
+                                                        arc_pos));
   long long cap = S.total;
   EmitArgs A;
   EmitCtx& E = A.E;
@@ -1108,13 +1131,13 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   E.S = S.R;
   E.out_primal = flat_primal;
   E.out_dual = flat_dual;
-  E.q_out = nullptr;
-  E.n_out = nullptr;
   E.q_cap = cap;
   E.max_steps = ctx->nsad + 1;
   E.status = ctx->status;
   A.nsurv = nsurv;
-  A.surv_sad = ctx->surv;
+  A.surv_ic = ctx->surv_ic;
+  A.sv_t = S.sv_t;
+  A.sv_len = S.sv_len;
   A.arc_pos = arc_pos;
   A.arc_cl = S.arc_cl;
   A.arc_root = S.arc_root;
@@ -1123,14 +1146,13 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   A.cnt = sget<int>(ctx, si, X_CNT, 8);
   E.base_q = sget<int4>(ctx, si, X_QB, cap);
   E.base_cap = cap;
-  E.n_base = nullptr;
   A.max_levels = capped(ctx->nsad + 4, ctx->cap_emit_levels);
   A.levels = get<int>(ctx, S_STATS, 8) + 4 + si;
-  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 6 * kTimeline) + (2 + si) * kTimeline;
-  coop_launch(ctx, emit_persistent_kernel, A, st, "emit_persistent_kernel", ctx->emit_per_sm);
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 12 * kTimeline) + (2 + si) * kTimeline;
+  coop_launch(ctx, ctx->emit_shape ? emit_persistent_kernel<2, 3> : emit_persistent_kernel<1, 5>, A, st,
+              "emit_persistent_kernel", ctx->emit_per_sm);
   {
     int per = 0;
-    E.n_base = A.cnt + 3;
     if (ctx->seg_cursors == 1) {
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel<1>, 256, 0));
       LK(emit_segments_kernel<1><<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3));
@@ -1198,8 +1220,8 @@ int fetch_batch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStr
                                                          S.ext_img, I, R));
   }
   if (nsurv > 0 && o->sad_pts)
-    LK(sad_pts_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->crit_sad, ctx->sad_img,
-                                                          ctx->bases.surv, I, o->sad_pts, ctx->bases.surv));
+    LK(sad_pts_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv_ic, ctx->bases.surv, I, o->sad_pts,
+                                                          ctx->bases.surv));
   LAUNCH_CHECK("point lists");
   // per-saddle scalars and e rows
   if (nsurv > 0) {
@@ -1208,9 +1230,9 @@ int fetch_batch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStr
       RouteF P{S.faces ? o->p_max : o->p_min, S.faces ? o->p_min : o->p_max, ctx->bases.surv};
       Route PP{S.faces ? o->ppairs_max : o->ppairs_min, S.faces ? o->ppairs_min : o->ppairs_max, ctx->bases.surv};
       Route E{S.faces ? o->e_max : o->e_min, S.faces ? o->e_min : o->e_max, rt_of(si == 0 ? R_E0 : R_E1)};
-      LK(side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(
-          nsurv, S.faces, ctx->bases.surv, I, ctx->surv, S.t, S.ut, S.to_out, ctx->bases.alive[si], S.pers,
-          S.pair_dense, S.erow_off, ctx->bases.erow[si], P, PP, E));
+      LK(side_outputs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, ctx->bases.surv, I, S.sv_rec,
+                                                                 ctx->bases.alive[si], S.erow_off,
+                                                                 ctx->bases.erow[si], P, PP, E));
     }
     LAUNCH_CHECK("side_outputs_kernel");
   }
@@ -1492,10 +1514,11 @@ int dmsc_b200_set_profiling(dmsc_b200_context* ctx, int enable) {
 
 int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n) {
   if (!ctx || !ms || !ctx->profile) return -1;
-  // extract stages are marks 0, 15, 1..9, 16, 10, 11 (15: just before the
-  // gradient kernel, 16: just before the label kernels), fetch stages 12..14
-  static const int from[] = {0, 15, 1, 2, 3, 4, 5, 6, 7, 8, 9, 16, 10, 12, 13};
-  static const int to[] = {15, 1, 2, 3, 4, 5, 6, 7, 8, 9, 16, 10, 11, 13, 14};
+  // extract stages are marks 0, 15, 1, 2, 4..9, 16, 10, 11 (15: just before
+  // the gradient kernel, 16: just before the label kernels; mark 3 is not
+  // recorded), fetch stages 12..14
+  static const int from[] = {0, 15, 1, 2, 4, 5, 6, 7, 8, 9, 16, 10, 12, 13};
+  static const int to[] = {15, 1, 2, 4, 5, 6, 7, 8, 9, 16, 10, 11, 13, 14};
   const int ns = (int)(sizeof(from) / sizeof(from[0]));
   if (cudaEventSynchronize(ctx->ev[14]) != cudaSuccess) return -1;
   for (int k = 0; k < ns && k < n; ++k) {
@@ -1510,7 +1533,7 @@ long long dmsc_b200_launch_count(const dmsc_b200_context* ctx) { return ctx ? ct
 
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n) {
   if (!ctx || !out || ctx->bufs.size() <= (size_t)S_TIMELINE || !ctx->bufs[S_TIMELINE].p) return -1;
-  int k = n < 6 * kTimeline ? n : 6 * kTimeline;
+  int k = n < 12 * kTimeline ? n : 12 * kTimeline;
   if (cudaSetDevice(ctx->device) != cudaSuccess ||
       cudaMemcpy(out, ctx->bufs[S_TIMELINE].p, k * sizeof(long long), cudaMemcpyDeviceToHost) != cudaSuccess)
     return -1;
@@ -1538,8 +1561,13 @@ int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_
 int dmsc_b200_set_tuning(dmsc_b200_context* ctx, const dmsc_b200_tuning* t) {
   if (!ctx || !t || t->grad_shape < 0 || t->grad_shape >= kGradShapes || t->label_shape < 0 ||
       t->label_shape >= kLabelShapes || t->pair_blocks_per_sm < 0 || t->replay_blocks_per_sm < 0 ||
-      t->emit_blocks_per_sm < 0 || t->seg_cursors < 1 || t->seg_cursors > kSegCursorShapes)
+      t->emit_blocks_per_sm < 0 || t->seg_cursors < 1 || t->seg_cursors > kSegCursorShapes || t->pair_shape < 0 ||
+      t->pair_shape >= kPairShapes || t->replay_shape < 0 || t->replay_shape >= kReplayShapes ||
+      t->emit_shape < 0 || t->emit_shape >= kEmitShapes)
     return kErrInvalidArgument;
+  ctx->emit_shape = t->emit_shape;
+  ctx->pair_shape = t->pair_shape;
+  ctx->replay_shape = t->replay_shape;
   ctx->seg_cursors = t->seg_cursors;
   ctx->grad_shape = t->grad_shape;
   ctx->label_shape = t->label_shape;
@@ -1557,19 +1585,28 @@ int dmsc_b200_get_tuning(const dmsc_b200_context* ctx, dmsc_b200_tuning* t) {
   t->replay_blocks_per_sm = ctx->replay_per_sm;
   t->emit_blocks_per_sm = ctx->emit_per_sm;
   t->seg_cursors = ctx->seg_cursors;
+  t->pair_shape = ctx->pair_shape;
+  t->replay_shape = ctx->replay_shape;
+  t->emit_shape = ctx->emit_shape;
   return kOk;
 }
 
 int dmsc_b200_tuning_limits(dmsc_b200_context* ctx, int* out, int n) {
   if (!ctx || !out) return -1;
-  int v[6] = {kGradShapes, kLabelShapes, 0, 0, 0, kSegCursorShapes};
+  int v[9] = {kGradShapes, kLabelShapes, 0, 0, 0, kSegCursorShapes, kPairShapes, kReplayShapes, kEmitShapes};
   if (cudaSetDevice(ctx->device) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v[2], pairing_persistent_kernel, 256, 0) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v[3], replay_persistent_kernel, 256, 0) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v[4], emit_persistent_kernel, 256, 0) != cudaSuccess)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &v[2], ctx->pair_shape ? pairing_persistent_kernel<4, 4> : pairing_persistent_kernel<2, 5>, 256, 0) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &v[3], ctx->replay_shape ? replay_persistent_kernel<2, 3> : replay_persistent_kernel<1, 4>, 256, 0) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &v[4], ctx->emit_shape ? emit_persistent_kernel<2, 3> : emit_persistent_kernel<1, 5>, 256, 0) !=
+          cudaSuccess)
     return -1;
-  for (int k = 0; k < 6 && k < n; ++k) out[k] = v[k];
-  return 6;
+  for (int k = 0; k < 9 && k < n; ++k) out[k] = v[k];
+  return 9;
 }
 
 int dmsc_b200_set_wait_timeout(dmsc_b200_context* ctx, double seconds) {

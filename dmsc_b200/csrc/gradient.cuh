@@ -417,61 +417,69 @@ __global__ void __launch_bounds__(NT) gradient_batch_kernel(Imgs I, const float*
 }
 
 // cell_value (cpu/cell_compare.hxx:82-87): value of the highest (dual: lowest)
-// vertex, chosen by (value, pixel id) with the reference scan order; the chosen
-// pixel's own value is returned, so -0.0 survives.
+// vertex, chosen by (value, pixel id) in the reference's scan order (each
+// candidate replaces the current choice when value_greater); the chosen
+// pixel's own value is returned, so -0.0 survives. `pick` adds one candidate.
 template <bool DUAL>
-__device__ __forceinline__ float cell_value_g(const float* __restrict__ img, int t, int y, int x, int H, int W) {
-  int cy[4], cx[4], n = 0;
-  if (t == 0) {
-    cy[n] = y;
-    cx[n++] = x;
-  } else if (t == 1) {
-    if (x - 1 >= 0) {
-      cy[n] = y;
-      cx[n++] = x - 1;
-    }
-    if (x < W) {
-      cy[n] = y;
-      cx[n++] = x;
-    }
-  } else if (t == 2) {
-    if (y - 1 >= 0) {
-      cy[n] = y - 1;
-      cx[n++] = x;
-    }
-    if (y < H) {
-      cy[n] = y;
-      cx[n++] = x;
-    }
-  } else {
-    if (y - 1 >= 0 && x - 1 >= 0) {
-      cy[n] = y - 1;
-      cx[n++] = x - 1;
-    }
-    if (y - 1 >= 0 && x < W) {
-      cy[n] = y - 1;
-      cx[n++] = x;
-    }
-    if (y < H && x - 1 >= 0) {
-      cy[n] = y;
-      cx[n++] = x - 1;
-    }
-    if (y < H && x < W) {
-      cy[n] = y;
-      cx[n++] = x;
-    }
+__device__ __forceinline__ void pick(bool& have, float& bv, int& bi, bool valid, float v, int id) {
+  if (valid && (!have || value_greater<DUAL>(v, id, bv, bi))) {
+    have = true;
+    bv = v;
+    bi = id;
   }
-  int b = cy[0] * W + cx[0];
-  float bv = __ldg(img + b);
-  for (int k = 1; k < n; ++k) {
-    int id = cy[k] * W + cx[k];
-    float v = __ldg(img + id);
-    if (value_greater<DUAL>(v, id, bv, b)) {
-      b = id;
-      bv = v;
-    }
+}
+
+// Values of the four cells of index (y, x) for a whole warp of consecutive
+// columns: every lane loads its pixel and the one above it, takes its left
+// neighbours' from the lane to its left (lane 0 loads them), and evaluates
+// the candidates of cpu/cell_compare.hxx:82-87 in the reference's order
+// (vertex (y-1, x-1), (y-1, x), (y, x-1), (y, x) among those in the image).
+// Every lane of the warp must call it.
+struct CellValues {
+  float v, h, e, f;  // vertex, H edge (t = 1), V edge (t = 2), face (t = 3)
+};
+
+template <bool DUAL>
+__device__ __forceinline__ CellValues warp_cell_values(const float* __restrict__ img, int y, int x, int H, int W,
+                                                       int lane) {
+  const bool in_x = x < W, in_xl = x >= 1 && x - 1 < W, up = y >= 1, here = y < H;
+  const float a = (here && in_x) ? __ldg(img + (size_t)y * W + x) : 0.f;
+  const float u = (up && in_x) ? __ldg(img + (size_t)(y - 1) * W + x) : 0.f;
+  float aL = __shfl_up_sync(0xffffffffu, a, 1), uL = __shfl_up_sync(0xffffffffu, u, 1);
+  if (lane == 0) {
+    aL = (here && in_xl) ? __ldg(img + (size_t)y * W + x - 1) : 0.f;
+    uL = (up && in_xl) ? __ldg(img + (size_t)(y - 1) * W + x - 1) : 0.f;
   }
-  return bv;
+  const int id = y * W + x, idu = id - W;
+  CellValues c;
+  c.v = a;
+  {
+    bool hv = false;
+    float bv = 0.f;
+    int bi = 0;
+    pick<DUAL>(hv, bv, bi, here && x >= 1, aL, id - 1);
+    pick<DUAL>(hv, bv, bi, here && in_x, a, id);
+    c.h = bv;
+  }
+  {
+    bool hv = false;
+    float bv = 0.f;
+    int bi = 0;
+    pick<DUAL>(hv, bv, bi, up && in_x, u, idu);
+    pick<DUAL>(hv, bv, bi, here && in_x, a, id);
+    c.e = bv;
+  }
+  {
+    bool hv = false;
+    float bv = 0.f;
+    int bi = 0;
+    pick<DUAL>(hv, bv, bi, up && x >= 1, uL, idu - 1);
+    pick<DUAL>(hv, bv, bi, up && in_x, u, idu);
+    pick<DUAL>(hv, bv, bi, here && x >= 1, aL, id - 1);
+    pick<DUAL>(hv, bv, bi, here && in_x, a, id);
+    c.f = bv;
+  }
+  return c;
 }
 
 // Criticality bits of an index (bit t: slot t is an unpaired valid cell) from
@@ -506,51 +514,46 @@ static __global__ void __launch_bounds__(256) compact_kernel(
   const int H = I.H[b], W = I.W[b], Nx = W + 1;
   const bool dual = I.dual[b];
   const int nsegx = (W + 1 + kTileX - 1) / kTileX;
-  const long long lseg = seg - I.seg_base[b];
-  int iy = (int)(lseg / nsegx), sx = (int)(lseg - (long long)iy * nsegx);
-  int ix = sx * kTileX + lane;
+  const int lseg = (int)(seg - I.seg_base[b]);  // an image has fewer than 2^31 / 4 indices
+  const int iy = lseg / nsegx, sx = lseg - iy * nsegx;
+  const int ix = sx * kTileX + lane;
   unsigned m = 0;
   const long long gidx = (long long)I.idx_base[b] + (long long)iy * Nx + ix;
   const float* img = img_all + I.px_base[b];
   if (ix <= W) m = crit_bits(flow[gidx], iy < H && ix < W);
-  unsigned lt = (1u << lane) - 1u;
-  unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
-  unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
+  const unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
+  const unsigned bh = __ballot_sync(0xffffffffu, m & 2u), bv = __ballot_sync(0xffffffffu, m & 4u);
   if (lane == 0) {
     min_bits[seg] = bmin;
     max_bits[seg] = bmax;
   }
-  int ns = ((m >> 1) & 1u) + ((m >> 2) & 1u);
-  int incl = ns;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += t;
-  }
-  int excl = incl - ns;
+  if ((bmin | bmax | bh | bv) == 0u) return;  // the whole warp leaves together
+  const CellValues cv = dual ? warp_cell_values<true>(img, iy, ix, H, W, lane)
+                             : warp_cell_values<false>(img, iy, ix, H, W, lane);
+  // saddles before this lane's: both edge kinds of the lanes below it
+  int p = off_sad[seg] + __popc(bh & lt) + __popc(bv & lt);
   if (m & 1u) {
-    int p = off_min[seg] + __popc(bmin & lt);
-    crit_min[p] = (int)(4 * gidx);
-    min_img[p] = b;
-    const float v = __ldg(img + (size_t)iy * W + ix);
-    min_val[p] = v;
-    min_key[p] = make_int2(__float_as_int(v), (int)(4 * gidx));
+    const int q = off_min[seg] + __popc(bmin & lt);
+    crit_min[q] = (int)(4 * gidx);
+    min_img[q] = b;
+    min_val[q] = cv.v;
+    min_key[q] = make_int2(__float_as_int(cv.v), (int)(4 * gidx));
   }
   if (m & 8u) {
-    int p = off_max[seg] + __popc(bmax & lt);
-    crit_max[p] = (int)(4 * gidx + 3);
-    max_img[p] = b;
-    const float v = dual ? cell_value_g<true>(img, 3, iy, ix, H, W) : cell_value_g<false>(img, 3, iy, ix, H, W);
-    max_val[p] = v;
-    max_key[p] = make_int2(__float_as_int(v), (int)(4 * gidx + 3));
+    const int q = off_max[seg] + __popc(bmax & lt);
+    crit_max[q] = (int)(4 * gidx + 3);
+    max_img[q] = b;
+    max_val[q] = cv.f;
+    max_key[q] = make_int2(__float_as_int(cv.f), (int)(4 * gidx + 3));
   }
-  int p = off_sad[seg] + excl;
 #pragma unroll
   for (int t = 1; t <= 2; ++t) {
     if (!(m & (1u << t))) continue;
+    const float v = t == 1 ? cv.h : cv.e;
     crit_sad[p] = (int)(4 * gidx + t);
     sad_img[p] = b;
-    float v = dual ? cell_value_g<true>(img, t, iy, ix, H, W) : cell_value_g<false>(img, t, iy, ix, H, W);
     sad_val[p] = v;
     if (sad_key32)  // one image: the image id is 0, a 32-bit key suffices
       sad_key32[p] = orderable_key(v);

@@ -29,7 +29,23 @@
 
 namespace dmsc {
 
-constexpr uint32_t kNoEdge = 0xFFFFFFFFu;
+constexpr unsigned long long kNoEdge = ~0ull;
+
+// Sweep key of saddle e (list index) on one side: the side sweeps its image's
+// saddles in ascending (s_val, cell id) order, or exactly the reverse (desc;
+// cpu/arcs_topology.hxx:99-102, 142). List indices ascend with the cell id
+// inside an image, so (orderable(s_val), e) orders the ascending sweep and
+// (~orderable(s_val), 0x7FFFFFFF - e) the descending one; both stay below
+// kNoEdge, and keys of one image never meet another image's.
+__device__ __forceinline__ unsigned long long sweep_key(float v, int e, bool desc) {
+  const uint32_t o = orderable_key(v);
+  return desc ? ((unsigned long long)(~o) << 32) | (uint32_t)(0x7FFFFFFF - e)
+              : ((unsigned long long)o << 32) | (uint32_t)e;
+}
+__device__ __forceinline__ int sweep_key_saddle(unsigned long long k, bool desc) {
+  const int lo = (int)(uint32_t)k;
+  return desc ? 0x7FFFFFFF - lo : lo;
+}
 constexpr int kUndecided = -2;
 
 // older(a, b) for extremum dense indices of one image; `void_id` is older
@@ -49,25 +65,6 @@ __global__ void iota_kernel(int* __restrict__ a, int n) {
   if (i < n) a[i] = i;
 }
 
-// Sweep-ordered edge list of one side for a batch. `asc` lists every image's
-// saddles in ascending (s_val, cell id), images in order; the face side sweeps
-// each image descending in the primal and ascending in the dual, the vertex
-// side the reverse (cpu/arcs_topology.hxx:99-102, 142). Edge q is saddle
-// sweep[q] with ends (t[2s], t[2s+1]); an image's edges stay contiguous.
-__global__ void sweep_edges_kernel(int nsad, const int* __restrict__ asc, const int* __restrict__ sad_img,
-                                   const int* __restrict__ sad_base, const uint8_t* __restrict__ dual, bool faces,
-                                   int* __restrict__ sweep, int* __restrict__ rank) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nsad) return;
-  int s = asc[p];
-  int b = sad_img[s];
-  int base = sad_base[b], n = sad_base[b + 1] - base;
-  bool rev = faces ? !dual[b] : dual[b];
-  int q = rev ? base + n - 1 - (p - base) : p;
-  sweep[q] = s;
-  rank[s] = q;  // sweep position of the saddle with list index s
-}
-
 // Persistence of each decided saddle and cancellation (persistence.hxx:82-104,
 // 139-161), with the saddle's image's orientation and threshold; `sbit` marks
 // the side in `cancelled`.
@@ -81,7 +78,10 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
                                                           uint8_t* __restrict__ cancelled, uint8_t sbit,
                                                           uint8_t* __restrict__ alive, int* __restrict__ n_cancel,
                                                           const int* __restrict__ t,
-                                                          int2* __restrict__ canc_ends) {
+                                                          int2* __restrict__ canc_ends,
+                                                          const int* __restrict__ crit_sad,
+                                                          unsigned long long* __restrict__ ckey,
+                                                          int* __restrict__ cval) {
   // saddles in list order: every per-saddle access is sequential
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   bool canc = false;
@@ -108,9 +108,19 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
       }
     }
   }
-  // cancelled edges' ends, compacted for the thresholded union-find
+  // cancelled edges' ends, compacted for the thresholded union-find, and (when
+  // the side's arcs are simplified) the same cancellations with their replay
+  // keys (CancelEvent::operator<, cpu/persistence_struct.hxx:16-21):
+  // (persistence, saddle cell); a saddle is cancelled at most once per side,
+  // so the pair is unique and the target cell never breaks a tie
   const int slot = block_append(n_cancel, canc);
-  if (canc) canc_ends[slot] = make_int2(t[2 * s], t[2 * s + 1]);
+  if (canc) {
+    canc_ends[slot] = make_int2(t[2 * s], t[2 * s + 1]);
+    if (ckey) {
+      ckey[slot] = ((unsigned long long)orderable_key(pers[s]) << 32) | (unsigned)crit_sad[s];
+      cval[slot] = s;
+    }
+  }
 }
 
 // Thresholded union-find (the reference's uf_min / uf_max, persistence.hxx:
@@ -184,6 +194,16 @@ __global__ void ut_mark_kernel(int n_ext, const int* __restrict__ p, const uint8
     comp_root[p[x]] = -1;
   else if (alive[x])
     comp_root[p[x]] = x;
+}
+
+// Out rank of each extremum's thresholded root (-1: the void's component);
+// a root is alive, so it always has one.
+__global__ void root_out_kernel(int n_ext, const int* __restrict__ ut, const int* __restrict__ to_out,
+                                int* __restrict__ rout) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_ext) return;
+  const int u = ut[x];
+  rout[x] = u >= 0 ? to_out[u] : -1;
 }
 
 __global__ void ut_root_kernel(int n_ext, const int* __restrict__ p, const int* __restrict__ comp_root,

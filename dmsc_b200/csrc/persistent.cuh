@@ -26,6 +26,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 constexpr int kTimeline = 64;  // timestamps kept per loop (round starts)
+// The timeline buffer holds 6 loops' round start times, then each round's
+// item count at the same position + kTimelineCounts.
+constexpr int kTimelineCounts = 6 * kTimeline;
 
 // Root of x in the pairing's group forest. A group links only under an
 // older group (ages strictly decrease along links), so a search visits at
@@ -68,12 +71,16 @@ __device__ __forceinline__ long long chunk_size(long long n, int blocks) {
   return 256LL * max(1LL, min((long long)kChunkPer, (n + lanes - 1) / lanes));
 }
 
-// Round loops whose active set has shrunk below kSoloItems finish in block 0
+// Round loops whose active set has shrunk below a threshold finish in block 0
 // alone: the other blocks leave (all decide alike, from the same counters
 // read after the grid barrier that ended the previous round), and block 0
 // separates the remaining phases with block barriers instead of grid
-// barriers, which cost several microseconds each.
-constexpr long long kSoloItems = 4096;
+// barriers, which cost several microseconds each. The pairing's items are
+// short (a few dependent loads each), so block 0 takes over while each of
+// its threads still has several; a replay item walks whole parent chains, so
+// the replay goes solo only at one item per thread.
+constexpr long long kPairSoloItems = 2048;
+constexpr long long kReplaySoloItems = 256;
 
 __device__ __forceinline__ void chunk_start(ChunkLists& L) {
   if (threadIdx.x < 2) L.n[threadIdx.x] = 0;
@@ -97,16 +104,16 @@ __device__ __forceinline__ void chunk_flush(ChunkLists& L, int* cnt0, int* out0,
 // ---------------------------------------------------------------------------
 struct PairArgs {
   int nsad, M;  // void group = M
-  // saddles are indexed in list order (ascending cell id); `rank` gives a
-  // saddle's sweep position, which orders the saddles (the atomicMin key),
-  // and `sweep` maps a sweep position back to the saddle
+  // saddles are indexed in list order (ascending cell id); a saddle's sweep
+  // key (sweep_key) orders the saddles of its image in this side's sweep
+  // and is the atomicMin key, so no sorted copy of the saddles is needed
   const int* t;       // [2 nsad] extremum ends of each saddle (-1: void)
-  const int* rank;    // [nsad]
-  const int* sweep;   // [nsad]
+  const float* sval;  // [nsad] saddle values
+  const int* sad_img; // [nsad] image of each saddle
   int2* g12;          // [nsad] groups of the two ends, as of the saddle's last active round
   int* dying;
-  int* link;          // [M+1] group union-find
-  unsigned* minedge;  // [M+1]
+  int* link;                    // [M+1] group union-find
+  unsigned long long* minedge;  // [M+1] smallest sweep key of the group's active saddles
   int* act0;          // active saddles (ping-pong)
   int* act1;
   int* roots0;        // live group roots (ping-pong), [M+1] each
@@ -138,65 +145,224 @@ struct PairArgs2 {
   PairArgs s[2];
 };
 
-__device__ __forceinline__ void pair_phase_a(const PairArgs& A, int r, long long i, int n, bool& keep, int& e) {
-  keep = false;
-  e = -1;
-  if (i < 0 || i >= n) return;
-  const int* in = (r & 1) ? A.act1 : A.act0;
-  const int M = A.M;
-  e = in[i];
-  if (r == 0 || A.dying[e] == kUndecided) {
-    int ga, gb;
+// Items a thread advances together in each phase (U): every load of a stage
+// is issued for all of them before any is used, so a thread waits on U
+// independent chains of dependent loads at once instead of one after the
+// other (the stores and atomics between items would otherwise keep the
+// compiler from overlapping them). Two shapes (tuned): U = 2 with 5 resident
+// blocks per SM (48 registers) and U = 4 with 4 (64 registers).
+constexpr int kPairShapes = 2;
+
+// Per-side fields picked by a flag (the parameter struct is only indexed
+// with constants, so it stays in the constant bank).
+#define PSIDE(f) (s1 ? P.s[1].f : P.s[0].f)
+
+// Phase A for the thread's items i0 + 256 u (u < U) below cend: side 0's
+// items come first (i < n0). Round 0 takes every saddle and keeps no list:
+// round 1 takes every saddle again and skips the decided ones. Later rounds
+// read the active list.
+template <int U>
+__device__ __forceinline__ void pair_batch_a(const PairArgs2& P, int r, long long i0, long long cend, int n0,
+                                             ChunkLists& L) {
+  int e[U], ga[U], gb[U];
+  float sv[U];
+  unsigned act = 0, s1m = 0, du = 0;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const long long i = i0 + 256LL * u;
+    e[u] = 0;
+    if (i < cend) {
+      const bool s1 = i >= n0;
+      const long long j = s1 ? i - n0 : i;
+      act |= 1u << u;
+      s1m |= (unsigned)s1 << u;
+      e[u] = r <= 1 ? (int)j : ((r & 1) ? PSIDE(act1) : PSIDE(act0))[j];
+    }
+  }
+  // the saddle's state, ends and key value, all issued together
+  int dy[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    dy[u] = kUndecided;
+    ga[u] = gb[u] = 0;
+    if (!((act >> u) & 1u)) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    const int M = PSIDE(M);
     if (r == 0) {
-      const int2 ab = *reinterpret_cast<const int2*>(A.t + 2 * e);
-      ga = ab.x < 0 ? M : ab.x;
-      gb = ab.y < 0 ? M : ab.y;
-    } else {  // the ends' groups of the previous round, followed to their roots
-      const int2 g = A.g12[e];
-      ga = find_halving(A.link, g.x, M + 2, A.status);
-      gb = find_halving(A.link, g.y, M + 2, A.status);
-    }
-    if (ga == gb) {
-      A.dying[e] = -1;
+      const int2 ab = *reinterpret_cast<const int2*>(PSIDE(t) + 2 * e[u]);
+      ga[u] = ab.x < 0 ? M : ab.x;
+      gb[u] = ab.y < 0 ? M : ab.y;
     } else {
-      A.g12[e] = make_int2(ga, gb);
-      const unsigned rk = (unsigned)A.rank[e];
-      atomicMin(A.minedge + ga, rk);  // result unused: a reduction
-      atomicMin(A.minedge + gb, rk);
-      keep = true;
+      dy[u] = PSIDE(dying)[e[u]];
+      const int2 g = PSIDE(g12)[e[u]];  // the ends' groups of the previous round
+      ga[u] = g.x;
+      gb[u] = g.y;
     }
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+    if (dy[u] != kUndecided) act &= ~(1u << u);
+  if (r > 0) {
+    // the groups' current roots: path-halving finds of all 2U ends in lockstep
+    unsigned live = 0;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if ((act >> u) & 1u) live |= 3u << (2 * u);
+    for (int it = 0; live; ++it) {
+      if (it > P.s[0].M + P.s[1].M + 2) {  // ages strictly decrease along links: never reached
+        set_status(P.s[0].status, kStatusFindCap);
+        break;
+      }
+      int pa[2 * U], pp[2 * U];
+#pragma unroll
+      for (int c = 0; c < 2 * U; ++c) {
+        const bool s1 = (s1m >> (c >> 1)) & 1u;
+        const int x = (c & 1) ? gb[c >> 1] : ga[c >> 1];
+        pa[c] = ((live >> c) & 1u) ? PSIDE(link)[x] : x;
+      }
+#pragma unroll
+      for (int c = 0; c < 2 * U; ++c) {
+        const bool s1 = (s1m >> (c >> 1)) & 1u;
+        const int x = (c & 1) ? gb[c >> 1] : ga[c >> 1];
+        if (pa[c] == x) live &= ~(1u << c);
+        pp[c] = ((live >> c) & 1u) ? PSIDE(link)[pa[c]] : pa[c];
+      }
+#pragma unroll
+      for (int c = 0; c < 2 * U; ++c) {
+        if (!((live >> c) & 1u)) continue;
+        const bool s1 = (s1m >> (c >> 1)) & 1u;
+        int& x = (c & 1) ? gb[c >> 1] : ga[c >> 1];
+        if (pp[c] == pa[c]) {  // pa is the root
+          live &= ~(1u << c);
+        } else {
+          PSIDE(link)[x] = pp[c];  // path halving: replaces a pointer with an ancestor
+        }
+        x = pp[c];
+      }
+    }
+  }
+  // key values (loaded after the finds: fewer registers live across them)
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    sv[u] = 0.f;
+    if (!((act >> u) & 1u) || ga[u] == gb[u]) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    sv[u] = PSIDE(sval)[e[u]];
+    const bool d = P.s[0].dual[P.s[0].B > 1 ? P.s[0].sad_img[e[u]] : 0];
+    du |= (unsigned)(s1 ? d : !d) << u;  // descending sweep: faces in the primal, vertices in the dual
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (!((act >> u) & 1u)) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    if (ga[u] == gb[u]) {
+      PSIDE(dying)[e[u]] = -1;
+      continue;
+    }
+    PSIDE(g12)[e[u]] = make_int2(ga[u], gb[u]);
+    const unsigned long long k = sweep_key(sv[u], e[u], (du >> u) & 1u);
+    atomicMin(PSIDE(minedge) + ga[u], k);  // result unused: a reduction
+    atomicMin(PSIDE(minedge) + gb[u], k);
+    if (r > 0) chunk_keep(L, s1, e[u]);
   }
 }
 
-__device__ __forceinline__ void pair_phase_b1(const PairArgs& A, int r, long long k, int nr, bool& live, int& g) {
-  live = false;
-  g = -1;
-  if (k < 0 || k >= nr) return;
-  const int* rin = (r & 1) ? A.roots1 : A.roots0;
-  const int M = A.M;
-  int h = -1;
-  g = rin[k];
-  unsigned me = A.minedge[g];
-  if (me != kNoEdge) {
-    A.minedge[g] = kNoEdge;
-    const int e = A.sweep[me];  // the saddle at that sweep position
-    const int2 gg = A.g12[e];  // roots as of phase A
-    const int ga = gg.x, gb = gg.y;
-    h = (ga == g) ? gb : ga;
-    // g is an extremum of one image (the void never dies); older = value_less
-    // order on the vertex side in the primal and the face side in the dual
-    // (its image from its cell, in the record the comparison reads anyway)
-    const bool du = g < M && A.dual[find_image(A.idx_base, A.B, A.key[g].y >> 2)];
-    if (older(h, g, M, A.key, A.faces ? du : !du)) {
-      A.dying[e] = g;
-      A.link[g] = h;
+// Phase B for the thread's live roots k0 + 256 u (u < U) below cend (side 0's
+// first, k < nr0; round 0 takes every group, in index order): each root with
+// an outgoing saddle decides there and a dying root links itself under the
+// other group's root; the void never dies; roots without outgoing saddles
+// leave the list.
+template <int U>
+__device__ __forceinline__ void pair_batch_b(const PairArgs2& P, int r, long long k0, long long cend, int nr0,
+                                             ChunkLists& L) {
+  int g[U];
+  unsigned act = 0, s1m = 0;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const long long k = k0 + 256LL * u;
+    g[u] = 0;
+    if (k < cend) {
+      const bool s1 = k >= nr0;
+      const long long j = s1 ? k - nr0 : k;
+      act |= 1u << u;
+      s1m |= (unsigned)s1 << u;
+      g[u] = r == 0 ? (int)j : ((r & 1) ? PSIDE(roots1) : PSIDE(roots0))[j];
+    }
+  }
+  unsigned long long me[U];
+  int2 kg[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    me[u] = kNoEdge;
+    kg[u] = make_int2(0, 0);
+    if (!((act >> u) & 1u)) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    me[u] = PSIDE(minedge)[g[u]];
+    if (g[u] < PSIDE(M)) kg[u] = PSIDE(key)[g[u]];
+  }
+  int e[U];
+  unsigned older_less = 0;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    e[u] = 0;
+    if (!((act >> u) & 1u)) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    if (me[u] == kNoEdge) {  // no outgoing saddle: leaves the list for good
+      act &= ~(1u << u);
+      continue;
+    }
+    PSIDE(minedge)[g[u]] = kNoEdge;
+    if (g[u] == PSIDE(M)) {  // the void is older than every group: it never dies
+      chunk_keep(L, s1, g[u]);
+      act &= ~(1u << u);
+      continue;
+    }
+    // g is an extremum of one image; its image (from its cell) gives the
+    // sweep direction of the key and the age order: value_less on the vertex
+    // side in the primal and the face side in the dual
+    const bool d = P.s[0].dual[find_image(P.s[0].idx_base, P.s[0].B, kg[u].y >> 2)];
+    e[u] = sweep_key_saddle(me[u], s1 ? d : !d);
+    older_less |= (unsigned)(s1 ? !d : d) << u;
+  }
+  int h[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    h[u] = 0;
+    if (!((act >> u) & 1u)) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    const int2 gg = PSIDE(g12)[e[u]];  // roots as of phase A
+    h[u] = gg.x == g[u] ? gg.y : gg.x;
+  }
+  int2 kh[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    kh[u] = make_int2(0, 0);
+    const bool s1 = (s1m >> u) & 1u;
+    if (((act >> u) & 1u) && h[u] < PSIDE(M)) kh[u] = PSIDE(key)[h[u]];
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (!((act >> u) & 1u)) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    // older(h, g): the void is older than any extremum; else (value, cell)
+    // under the side's order
+    bool dies = h[u] == PSIDE(M);
+    if (!dies) {
+      const float vh = __int_as_float(kh[u].x), vg = __int_as_float(kg[u].x);
+      dies = ((older_less >> u) & 1u) ? tie_lt(vh, kh[u].y, vg, kg[u].y) : tie_lt(vg, kg[u].y, vh, kh[u].y);
+    }
+    if (dies) {
+      PSIDE(dying)[e[u]] = g[u];
+      PSIDE(link)[g[u]] = h[u];
     } else {
-      live = true;
+      chunk_keep(L, s1, g[u]);
     }
   }
 }
+#undef PSIDE
 
-__global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P) {
+template <int U, int MINB>
+__global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2 P) {
   __shared__ ChunkLists L;
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
@@ -205,15 +371,11 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
     for (long long i = tid; i <= A.M; i += nth) {
       A.link[i] = (int)i;
       A.minedge[i] = kNoEdge;
-      A.roots0[i] = (int)i;
     }
-    for (long long i = tid; i < A.nsad; i += nth) {
-      A.act0[i] = (int)i;
-      A.dying[i] = kUndecided;
-    }
-    if (tid == 0) {
+    for (long long i = tid; i < A.nsad; i += nth) A.dying[i] = kUndecided;
+    if (tid == 0) {  // rounds 0 and 1 take every saddle, round 0 every group
       A.cnt[0] = A.nsad;
-      A.cnt[1] = 0;
+      A.cnt[1] = A.nsad;
       A.cnt[2] = 0;
       A.cnt[3] = A.M + 1;
       A.cnt[4] = 0;
@@ -232,13 +394,16 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
         const PairArgs& A = P.s[sd];
         const int n = sd ? n1 : n0;
         bool& done = sd ? done1 : done0;
-        if (A.timeline && r < kTimeline && !done) A.timeline[r] = global_ns();
+        if (A.timeline && r < kTimeline && !done) {
+          A.timeline[r] = global_ns();
+          A.timeline[kTimelineCounts + r] = n;
+        }
         if (n == 0 && !done && A.rounds) *A.rounds = r;
         done = done || n == 0;
       }
     }
     if (n0 == 0 && n1 == 0) break;
-    if (!solo && (long long)n0 + n1 + nr0 + nr1 <= kSoloItems) {
+    if (!solo && (long long)n0 + n1 + nr0 + nr1 <= kPairSoloItems) {
       solo = true;
       if (blockIdx.x != 0) break;
     }
@@ -260,46 +425,32 @@ __global__ void __launch_bounds__(256, 6) pairing_persistent_kernel(PairArgs2 P)
         P.s[sd].cnt[3 + (r + 2) % 3] = 0;
       }
     }
-    // phase A over both sides' active saddles
+    // phase A over both sides' active saddles (round 0 keeps no list)
     {
       const long long n = (long long)n0 + n1, chunk = chunk_size(n, nblk);
+      const bool lists = r > 0;
       for (long long c0 = (long long)bid * chunk; c0 < n; c0 += (long long)nblk * chunk) {
-        chunk_start(L);
-        for (long long i = c0 + threadIdx.x; i < min(n, c0 + chunk); i += 256) {
-          bool keep;
-          int v;
-          if (i < n0) {
-            pair_phase_a(P.s[0], r, i, n0, keep, v);
-            if (keep) chunk_keep(L, 0, v);
-          } else {
-            pair_phase_a(P.s[1], r, i - n0, n1, keep, v);
-            if (keep) chunk_keep(L, 1, v);
-          }
-        }
-        chunk_flush(L, P.s[0].cnt + (r + 1) % 3, (r & 1) ? P.s[0].act0 : P.s[0].act1, P.s[1].cnt + (r + 1) % 3,
-                    (r & 1) ? P.s[1].act0 : P.s[1].act1);
+        if (lists) chunk_start(L);
+        const long long cend = min(n, c0 + chunk);
+        for (long long i0 = c0 + threadIdx.x; i0 < cend; i0 += 256LL * U)
+          pair_batch_a<U>(P, r, i0, cend, n0, L);
+        if (lists)
+          chunk_flush(L, P.s[0].cnt + (r + 1) % 3, (r & 1) ? P.s[0].act0 : P.s[0].act1, P.s[1].cnt + (r + 1) % 3,
+                      (r & 1) ? P.s[1].act0 : P.s[1].act1);
       }
     }
     if (solo)
       __syncthreads();
     else
       grid.sync();
-    // phase B1: live roots decide on their first outgoing saddle
+    // phase B: live roots decide on their first outgoing saddle
     {
       const long long n = (long long)nr0 + nr1, chunk = chunk_size(n, nblk);
       for (long long c0 = (long long)bid * chunk; c0 < n; c0 += (long long)nblk * chunk) {
         chunk_start(L);
-        for (long long k = c0 + threadIdx.x; k < min(n, c0 + chunk); k += 256) {
-          bool live;
-          int g;
-          if (k < nr0) {
-            pair_phase_b1(P.s[0], r, k, nr0, live, g);
-            if (live) chunk_keep(L, 0, g);
-          } else {
-            pair_phase_b1(P.s[1], r, k - nr0, nr1, live, g);
-            if (live) chunk_keep(L, 1, g);
-          }
-        }
+        const long long cend = min(n, c0 + chunk);
+        for (long long k0 = c0 + threadIdx.x; k0 < cend; k0 += 256LL * U)
+          pair_batch_b<U>(P, r, k0, cend, nr0, L);
         chunk_flush(L, P.s[0].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[0].roots0 : P.s[0].roots1,
                     P.s[1].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[1].roots0 : P.s[1].roots1);
       }
@@ -341,44 +492,154 @@ struct ReplayArgs2 {
   ReplayArgs s[2];
 };
 
-__device__ __forceinline__ bool replay_step(const ReplayArgs& A, int r, int round) {
-  const unsigned long long t = A.key[r];
-  const int s = A.cj[r], d = A.dying[s];
-  // both walks resume where the previous round left them
-  int R0 = A.wx[2 * r], R1 = A.wx[2 * r + 1];
-  long long a0 = A.wa[2 * r], a1 = A.wa[2 * r + 1];
-  const bool ok0 = walk_resume(A.S, &R0, t, &a0, A.max_steps, A.status, round);
-  const bool ok1 = walk_resume(A.S, &R1, t, &a1, A.max_steps, A.status, round);
-  if (!(ok0 && ok1)) {  // still waiting on an earlier cancellation
-    A.wx[2 * r] = R0;
-    A.wx[2 * r + 1] = R1;
-    A.wa[2 * r] = a0;
-    A.wa[2 * r + 1] = a1;
-    return true;
+// One batch of a thread's pending cancellations, the items i0 + nt u (u < U)
+// below na + nb (side 0's first): both walks of every item resume where the
+// previous round left them and advance in lockstep (2U independent chains of
+// node loads at once); an item whose walks meet an undecided node keeps its
+// walk positions and stays pending, the others decide (link or skip). The
+// batch's pending items are appended to the next round's lists with one block
+// reservation.
+#define RSIDE(f) (s1 ? P.s[1].f : P.s[0].f)
+template <int U>
+__device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long long i0, long long nt, int na, int nb) {
+  int r[U];
+  unsigned act = 0, s1m = 0;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const long long i = i0 + nt * u;
+    r[u] = 0;
+    if (i < (long long)na + nb) {
+      const bool s1 = i >= na;
+      act |= 1u << u;
+      s1m |= (unsigned)s1 << u;
+      r[u] = ((rd & 1) ? RSIDE(act1) : RSIDE(act0))[s1 ? i - na : i];
+    }
   }
-  int k = -1;
-  if (R0 == d && R0 != R1)
-    k = 0;
-  else if (R1 == d && R0 != R1)
-    k = 1;
-  if (k >= 0) {
-    const long long b0 = A.blen[2 * s], b1 = A.blen[2 * s + 1];
-    *reinterpret_cast<longlong2*>(&A.S.node[d].cl_dy) = make_longlong2(k == 0 ? a0 : a1, k == 0 ? a1 : a0);
-    A.S.node[d].wlen = b0 + b1 + a0 + a1;
-    // status, parent, the dying side with what W(d) expands to (its non-empty
-    // chains and raw-arc segments), and the saddle, in one store; a walk of
-    // this round uses no field of a record whose status carries this round's
-    // tag, so the order of these stores does not matter
-    *reinterpret_cast<int4*>(&A.S.node[d].status) =
-        make_int4(status_word(kLinked, round), k == 0 ? R1 : R0,
-                  side_word(k, (a0 > 0) + (a1 > 0), (b0 > 0) + (b1 > 0)), s);
-  } else {
-    A.S.node[d].status = status_word(kRootForever, round);
+  unsigned long long tk[U];
+  int sd[U], x[2 * U];
+  long long a[2 * U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    tk[u] = 0;
+    sd[u] = 0;
+    x[2 * u] = x[2 * u + 1] = -1;
+    a[2 * u] = a[2 * u + 1] = 0;
+    if (!((act >> u) & 1u)) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    tk[u] = RSIDE(key)[r[u]];
+    sd[u] = RSIDE(cj)[r[u]];
+    const int2 w = *reinterpret_cast<const int2*>(RSIDE(wx) + 2 * r[u]);
+    const longlong2 aa = *reinterpret_cast<const longlong2*>(RSIDE(wa) + 2 * r[u]);
+    x[2 * u] = w.x;
+    x[2 * u + 1] = w.y;
+    a[2 * u] = aa.x;
+    a[2 * u + 1] = aa.y;
   }
-  return false;
+  int d[U];  // the dying node (issued before the walks, used after them)
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const bool s1 = (s1m >> u) & 1u;
+    d[u] = ((act >> u) & 1u) ? RSIDE(dying)[sd[u]] : 0;
+  }
+  // the walks (walk_resume, in lockstep): bit c of `live` is a walk still
+  // moving, bit c of `wait` one that met an undecided node
+  unsigned live = 0, wait = 0;
+#pragma unroll
+  for (int c = 0; c < 2 * U; ++c)
+    if (((act >> (c >> 1)) & 1u) && x[c] >= 0) live |= 1u << c;
+  // a chain is at most its side's node count long (a side without arcs takes
+  // no part and has no bound of its own)
+  const int cap = max(P.s[0].max_steps, P.s[1].max_steps);
+  for (int steps = 0; live; ++steps) {
+    if (steps > cap) {
+      set_status(P.s[0].status, kStatusChainCap);
+      break;
+    }
+    longlong2 kl[2 * U];
+    int2 w[2 * U];  // status, parent
+#pragma unroll
+    for (int c = 0; c < 2 * U; ++c) {
+      const bool s1 = (s1m >> (c >> 1)) & 1u;
+      if ((live >> c) & 1u) {  // one sector: both parts issued together
+        kl[c] = node_keylen_cg(RSIDE(S.node), x[c]);
+        w[c] = __ldcg(reinterpret_cast<const int2*>(&RSIDE(S.node)[x[c]].status));
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 2 * U; ++c) {
+      if (!((live >> c) & 1u)) continue;
+      if ((unsigned long long)kl[c].x >= tk[c >> 1]) {  // not linked before this step: the root
+        live &= ~(1u << c);
+        continue;
+      }
+      const int st = w[c].x;
+      if (status_kind(st) == kPending || (st >> 2) > rd) {  // undecided, or decided in this round
+        live &= ~(1u << c);
+        wait |= 1u << c;
+        continue;
+      }
+      if (status_kind(st) == kRootForever) {
+        live &= ~(1u << c);
+        continue;
+      }
+      a[c] += kl[c].y;
+      x[c] = w[c].y;
+      if (x[c] < 0) live &= ~(1u << c);
+    }
+  }
+  unsigned keep = 0;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (!((act >> u) & 1u)) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    if ((wait >> (2 * u)) & 3u) {  // still waiting on an earlier cancellation
+      keep |= 1u << u;
+      *reinterpret_cast<int2*>(RSIDE(wx) + 2 * r[u]) = make_int2(x[2 * u], x[2 * u + 1]);
+      *reinterpret_cast<longlong2*>(RSIDE(wa) + 2 * r[u]) = make_longlong2(a[2 * u], a[2 * u + 1]);
+      continue;
+    }
+    const int R0 = x[2 * u], R1 = x[2 * u + 1], dd = d[u], s = sd[u];
+    const long long a0 = a[2 * u], a1 = a[2 * u + 1];
+    int k = -1;
+    if (R0 == dd && R0 != R1)
+      k = 0;
+    else if (R1 == dd && R0 != R1)
+      k = 1;
+    ReplayNode* node = RSIDE(S.node);
+    if (k >= 0) {
+      const longlong2 bl = *reinterpret_cast<const longlong2*>(RSIDE(blen) + 2 * s);
+      *reinterpret_cast<longlong2*>(&node[dd].cl_dy) = make_longlong2(k == 0 ? a0 : a1, k == 0 ? a1 : a0);
+      node[dd].wlen = bl.x + bl.y + a0 + a1;
+      // status, parent, the dying side with what W(d) expands to (its
+      // non-empty chains and raw-arc segments), and the saddle, in one store;
+      // a walk of this round uses no field of a record whose status carries
+      // this round's tag, so the order of these stores does not matter
+      *reinterpret_cast<int4*>(&node[dd].status) =
+          make_int4(status_word(kLinked, rd), k == 0 ? R1 : R0,
+                    side_word(k, (a0 > 0) + (a1 > 0), (bl.x > 0) + (bl.y > 0)), s);
+    } else {
+      node[dd].status = status_word(kRootForever, rd);
+    }
+  }
+  // every thread of the block takes part in the reservation (a side without
+  // cancellations reserves nothing and its counter is not touched)
+  const int n0 = __popc(keep & ~s1m), n1 = __popc(keep & s1m);
+  int p0, p1;
+  block_reserve2(P.s[0].cnt + (rd + 1) % 3, n0, P.s[1].cnt + (rd + 1) % 3, n1, p0, p1);
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (!((keep >> u) & 1u)) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    ((rd & 1) ? RSIDE(act0) : RSIDE(act1))[s1 ? p1++ : p0++] = r[u];
+  }
 }
+#undef RSIDE
 
-__global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P) {
+// Replay shapes (tuned): U = 1 with 4 resident blocks per SM, U = 2 with 3.
+constexpr int kReplayShapes = 2;
+
+template <int U, int MINB>
+__global__ void __launch_bounds__(256, MINB) replay_persistent_kernel(ReplayArgs2 P) {
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
   for (int sd = 0; sd < 2; ++sd) {
@@ -409,18 +670,24 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
     const int nb = P.s[1].n_cancel ? *(volatile int*)(P.s[1].cnt + rd % 3) : 0;
     if (tid == 0) {
       if (P.s[0].n_cancel && !done0) {
-        if (P.s[0].timeline && rd < kTimeline) P.s[0].timeline[rd] = global_ns();
+        if (P.s[0].timeline && rd < kTimeline) {
+          P.s[0].timeline[rd] = global_ns();
+          P.s[0].timeline[kTimelineCounts + rd] = na;
+        }
         if (na == 0 && P.s[0].rounds) *P.s[0].rounds = rd;
       }
       if (P.s[1].n_cancel && !done1) {
-        if (P.s[1].timeline && rd < kTimeline) P.s[1].timeline[rd] = global_ns();
+        if (P.s[1].timeline && rd < kTimeline) {
+          P.s[1].timeline[rd] = global_ns();
+          P.s[1].timeline[kTimelineCounts + rd] = nb;
+        }
         if (nb == 0 && P.s[1].rounds) *P.s[1].rounds = rd;
       }
     }
     done0 = done0 || na == 0;
     done1 = done1 || nb == 0;
     if (na == 0 && nb == 0) break;
-    if (!solo && (long long)na + nb <= kSoloItems) {  // block 0 finishes alone (see kSoloItems)
+    if (!solo && (long long)na + nb <= kReplaySoloItems) {  // block 0 finishes alone
       solo = true;
       if (blockIdx.x != 0) break;
     }
@@ -441,26 +708,10 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
     if (tid == 0)
       for (int sd = 0; sd < 2; ++sd)
         if (P.s[sd].n_cancel) P.s[sd].cnt[(rd + 2) % 3] = 0;
-    // grid-stride over both sides' pending cancellations (a cancellation
-    // decided earlier in the same round is visible to later walks)
-    for (long long base = 0; base < (long long)na + nb; base += nt) {
-      const long long i = base + t0;
-      bool k0 = false, k1 = false;
-      int r0 = -1, r1 = -1;
-      if (i < na) {
-        r0 = ((rd & 1) ? P.s[0].act1 : P.s[0].act0)[i];
-        k0 = replay_step(P.s[0], r0, rd);
-      } else if (i < (long long)na + nb) {
-        r1 = ((rd & 1) ? P.s[1].act1 : P.s[1].act0)[i - na];
-        k1 = replay_step(P.s[1], r1, rd);
-      }
-      // every thread of the block takes part in the reservation (a side
-      // without cancellations reserves nothing and its counter is not touched)
-      int p0, p1;
-      block_reserve2(P.s[0].cnt + (rd + 1) % 3, k0 ? 1 : 0, P.s[1].cnt + (rd + 1) % 3, k1 ? 1 : 0, p0, p1);
-      if (k0) ((rd & 1) ? P.s[0].act0 : P.s[0].act1)[p0] = r0;
-      if (k1) ((rd & 1) ? P.s[1].act0 : P.s[1].act1)[p1] = r1;
-    }
+    // grid-stride over both sides' pending cancellations, U per thread at a
+    // time (a cancellation decided earlier in the same round is visible to
+    // later walks)
+    for (long long base = 0; base < (long long)na + nb; base += nt * U) replay_batch<U>(P, rd, base + t0, nt, na, nb);
     if (solo)
       __syncthreads();
     else
@@ -474,7 +725,9 @@ __global__ void __launch_bounds__(256, 5) replay_persistent_kernel(ReplayArgs2 P
 struct EmitArgs {
   EmitCtx E;
   int nsurv;
-  const int* surv_sad;
+  const int2* surv_ic;      // [nsurv] image and cell of each survivor (output order)
+  const int2* sv_t;         // [nsurv] this side's arc ends of each survivor
+  const longlong2* sv_len;  // [nsurv] this side's raw-arc lengths of each survivor
   const long long* arc_pos;
   const long long* arc_cl;
   const int* arc_root;
@@ -486,10 +739,154 @@ struct EmitArgs {
   unsigned long long* timeline;  // [kTimeline] level start times (ns), optional
 };
 
+// One batch of a thread's chain tasks at one expansion level, in[i0 + nt u]
+// (u < U) below n: the U chains are counted in lockstep (one node-record load
+// per chain and step), the batch reserves its chain tasks and raw-arc
+// segments with one block reservation, and the U chains are expanded in
+// lockstep: per step, every chain issues its node's loads, then the loads of
+// the node's saddle (arc ends and raw-arc lengths), then writes W(node)
+// (chain_expand / emit_w, replay.cuh).
+template <int U>
+__device__ __forceinline__ void emit_batch(const EmitCtx& E, int4* __restrict__ q_out, int* n_out, int* n_base,
+                                           const int4* __restrict__ in, long long i0, long long nt, long long n) {
+  int x[U], stop[U], z[U], nc[U], nb[U];
+  long long pos[U], tot[U];
+  unsigned act = 0, rev = 0;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const long long i = i0 + nt * u;
+    x[u] = stop[u] = -1;
+    pos[u] = 0;
+    if (i < n) {  // every queued task is a chain task
+      const int4 t = in[i];
+      if ((t.x & 3) == kTaskChain) {
+        act |= 1u << u;
+        rev |= (unsigned)((t.x >> 2) & 1) << u;
+        x[u] = t.y;
+        stop[u] = t.z;
+        pos[u] = t.w;
+      }
+    }
+    z[u] = x[u];
+    nc[u] = nb[u] = 0;
+    tot[u] = 0;
+  }
+  // counts and total length of each chain (chain_expand_counts)
+  unsigned live = 0;
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+    if (((act >> u) & 1u) && z[u] != stop[u] && z[u] >= 0) live |= 1u << u;
+  for (int k = 0; live; ++k) {
+    if (k > E.max_steps) {  // a chain is at most the side's node count long
+      set_status(E.status, kStatusChainCap);
+      act &= ~live;  // the capped tasks are dropped
+      break;
+    }
+    longlong2 kl[U];
+    int4 w[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if ((live >> u) & 1u) {
+        kl[u] = node_keylen(E.S.node, z[u]);
+        w[u] = node_words(E.S.node, z[u]);
+      }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if ((live >> u) & 1u) {
+        tot[u] += kl[u].y;
+        nc[u] += chains_of(w[u].z);  // counts stored at link time
+        nb[u] += bases_of(w[u].z);
+        z[u] = w[u].y;
+        if (z[u] == stop[u] || z[u] < 0) live &= ~(1u << u);
+      }
+  }
+  int need = 0, nbase = 0;
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+    if ((act >> u) & 1u) {
+      need += nc[u];
+      nbase += nb[u];
+    }
+  int p, pb;
+  block_reserve2(n_out, need, n_base, nbase, p, pb);
+  if (p + (long long)need > E.q_cap || pb + (long long)nbase > E.base_cap) {
+    set_status(E.status, kStatusQueueOverflow);
+    return;
+  }
+  // expansion: the slots of chain u follow those of the chains before it
+  int pc[U], pbc[U];
+  long long off[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    pc[u] = p;
+    pbc[u] = pb;
+    if ((act >> u) & 1u) {
+      p += nc[u];
+      pb += nb[u];
+    }
+    z[u] = x[u];
+    off[u] = 0;
+  }
+  live = 0;
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+    if (((act >> u) & 1u) && z[u] != stop[u] && z[u] >= 0) live |= 1u << u;
+  while (live) {
+    int4 w[U];
+    long long wl[U];
+    longlong2 cl[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if ((live >> u) & 1u) {
+        w[u] = node_words(E.S.node, z[u]);
+        wl[u] = E.S.node[z[u]].wlen;
+        cl[u] = *reinterpret_cast<const longlong2*>(&E.S.node[z[u]].cl_dy);
+      }
+    int2 tt[U];
+    longlong2 bl[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if ((live >> u) & 1u) {
+        const int s = w[u].w;
+        tt[u] = *reinterpret_cast<const int2*>(E.t + 2 * s);
+        bl[u] = *reinterpret_cast<const longlong2*>(E.blen + 2 * s);
+      }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!((live >> u) & 1u)) continue;
+      // W(z) = reverse(chain(Tk -> z)) + reverse(arc k) + arc o + chain(To -> R)
+      const int d = z[u], k = side_of(w[u].z), s = w[u].w, R = w[u].y;
+      const int Tk = k ? tt[u].y : tt[u].x, To = k ? tt[u].x : tt[u].y;
+      const long long la = cl[u].x, lb = k ? bl[u].y : bl[u].x, lc = k ? bl[u].x : bl[u].y, ld = cl[u].y;
+      const bool rv = (rev >> u) & 1u;
+      const long long at = rv ? pos[u] + tot[u] - off[u] - wl[u] : pos[u] + off[u];
+      int& q = pc[u];
+      int& qb = pbc[u];
+      if (!rv) {
+        if (la > 0) q_out[q++] = make_task(kTaskChain, 1, Tk, d, at);
+        if (lb > 0) E.base_q[qb++] = make_saddle_seg(s, k, 1, at + la);
+        if (lc > 0) E.base_q[qb++] = make_saddle_seg(s, 1 - k, 0, at + la + lb);
+        if (ld > 0) q_out[q++] = make_task(kTaskChain, 0, To, R, at + la + lb + lc);
+      } else {
+        if (ld > 0) q_out[q++] = make_task(kTaskChain, 1, To, R, at);
+        if (lc > 0) E.base_q[qb++] = make_saddle_seg(s, 1 - k, 1, at + ld);
+        if (lb > 0) E.base_q[qb++] = make_saddle_seg(s, k, 0, at + ld + lc);
+        if (la > 0) q_out[q++] = make_task(kTaskChain, 0, Tk, d, at + ld + lc + lb);
+      }
+      off[u] += wl[u];
+      z[u] = w[u].y;
+      if (z[u] == stop[u] || z[u] < 0) live &= ~(1u << u);
+    }
+  }
+}
+// Expansion shapes (tuned): U = 1 with 5 resident blocks per SM, U = 2 with 3.
+constexpr int kEmitShapes = 2;
+
 // Geometry of one side: breadth-first expansion of the chain and W tasks
 // (replay.cuh), collecting the raw-arc segments with their output positions,
 // then one parallel pass that walks and writes every segment.
-__global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
+template <int U, int MINB>
+__global__ void __launch_bounds__(256, MINB) emit_persistent_kernel(EmitArgs A) {
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
   if (tid == 0) {
@@ -499,8 +896,8 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
     A.cnt[3] = 0;
   }
   grid.sync();
-  EmitCtx E = A.E;
-  E.n_base = A.cnt + 3;
+  const EmitCtx& E = A.E;
+  int* const n_base = A.cnt + 3;
   // level 0: each surviving arc's own raw arc, then its chain
   for (long long base = 0; base < 2LL * A.nsurv; base += nth) {
     long long q = base + tid;
@@ -508,22 +905,25 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
     int4 task = make_int4(0, 0, 0, 0), btask = make_int4(0, 0, 0, 0);
     if (q < 2LL * A.nsurv) {
       int i = (int)(q >> 1), j = (int)(q & 1);
-      int s = A.surv_sad[i];
       // images whose output takes none of this side's arcs emit nothing
-      const int b = E.sad_img[s];
+      const int2 ic = A.surv_ic[i];
+      const int b = ic.x;
       const bool takes = (E.I.dual[b] ? E.out_dual : E.out_primal) != nullptr;
-      if (takes && E.t[2 * s + j] >= 0) {
-        long long pos = A.arc_pos[q];
-        seg = E.blen[2 * s + j] > 0;
-        btask = make_task(kTaskBase, 0, s, j, pos);
+      const int2 tt = A.sv_t[i];
+      const int T = j ? tt.y : tt.x;
+      if (takes && T >= 0) {
+        const longlong2 bl = A.sv_len[i];
+        const long long len = j ? bl.y : bl.x, pos = A.arc_pos[q];
+        seg = len > 0;
+        if (seg) btask = make_seg(arc_start_of_cell(E, ic.y, j, b), 0, len, pos, b);
         if (A.arc_cl[q] > 0) {
           push = true;
-          task = make_task(kTaskChain, 0, E.t[2 * s + j], A.arc_root[q], pos + E.blen[2 * s + j]);
+          task = make_task(kTaskChain, 0, T, A.arc_root[q], pos + len);
         }
       }
     }
     int p, pb;
-    block_reserve2(A.cnt, push ? 1 : 0, E.n_base, seg ? 1 : 0, p, pb);
+    block_reserve2(A.cnt, push ? 1 : 0, n_base, seg ? 1 : 0, p, pb);
     if (push) {
       if (p < E.q_cap)
         A.q0[p] = task;
@@ -541,7 +941,10 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
   bool solo = false;
   for (int lv = 0;; ++lv) {
     int n = *(volatile int*)(A.cnt + lv % 3);
-    if (tid == 0 && A.timeline && lv < kTimeline - 2) A.timeline[lv] = global_ns();
+    if (tid == 0 && A.timeline && lv < kTimeline - 2) {
+      A.timeline[lv] = global_ns();
+      A.timeline[kTimelineCounts + lv] = n;
+    }
     if (n == 0) {
       if (tid == 0 && A.levels) *A.levels = lv;
       break;
@@ -558,28 +961,10 @@ __global__ void __launch_bounds__(256) emit_persistent_kernel(EmitArgs A) {
     }
     const long long t0 = solo ? threadIdx.x : tid, nt = solo ? blockDim.x : nth;
     const int4* in = (lv & 1) ? A.q1 : A.q0;
-    E.q_out = (lv & 1) ? A.q0 : A.q1;
-    E.n_out = A.cnt + (lv + 1) % 3;
+    int4* q_out = (lv & 1) ? A.q0 : A.q1;
+    int* n_out = A.cnt + (lv + 1) % 3;
     if (tid == 0) A.cnt[(lv + 2) % 3] = 0;
-    for (long long base = 0; base < n; base += nt) {
-      long long i = base + t0;
-      int4 t = make_int4(-1, 0, 0, 0);
-      int kind = -1, rev = 0, need = 0, nb = 0;
-      long long total = 0;
-      if (i < n) {  // every queued task is a chain task
-        t = in[i];
-        kind = t.x & 3;
-        rev = (t.x >> 2) & 1;
-        if (kind == kTaskChain && !chain_expand_counts(E, t.y, t.z, &need, &nb, &total)) kind = -1;
-      }
-      int p, pb;
-      block_reserve2(E.n_out, need, E.n_base, nb, p, pb);
-      if (p + (long long)need > E.q_cap || pb + (long long)nb > E.base_cap) {
-        set_status(E.status, kStatusQueueOverflow);
-        kind = -1;
-      }
-      if (kind == kTaskChain) chain_expand(E, t.y, t.z, rev, t.w, total, p, pb);
-    }
+    for (long long base = 0; base < n; base += nt * U) emit_batch<U>(E, q_out, n_out, n_base, in, base + t0, nt, n);
     if (solo)
       __syncthreads();
     else
@@ -621,8 +1006,7 @@ __global__ void __launch_bounds__(256) emit_segments_kernel(EmitCtx E, const int
         if (c[q].rem <= 0) {
           const long long my = next + __popc(idle & lt);
           if (my < r1) {
-            const int4 t = E.base_q[my];
-            seg_start(E, t.y, t.z, (t.x >> 2) & 1, t.w, c[q]);
+            seg_start(E, E.base_q[my], c[q]);
           }
         }
         next += __popc(idle);

@@ -153,58 +153,31 @@ __device__ __forceinline__ bool walk_resume(const ReplayState& S, int* x_io, uns
   return done;
 }
 
-// Cancellations of one side, compacted in any order with their sort keys
-// (CancelEvent::operator<, cpu/persistence_struct.hxx:16-21): (persistence,
-// saddle cell); a saddle is cancelled at most once per side, so the pair is
-// unique and the target cell never breaks a tie.
-__global__ void __launch_bounds__(256) cancel_collect_kernel(int nsad, const int* __restrict__ dying,
-                                                             const float* __restrict__ pers,
-                                                             const float* __restrict__ thr,
-                                                             const int* __restrict__ sad_img,
-                                                             const int* __restrict__ crit_sad,
-                                                             unsigned long long* __restrict__ keys,
-                                                             int* __restrict__ vals, int* __restrict__ count) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;  // saddles in list order
-  bool take = false;
-  unsigned long long key = 0;
-  if (s < nsad && dying[s] >= 0) {
-    float p = pers[s];
-    if (p <= thr[sad_img[s]]) {
-      take = true;
-      key = ((unsigned long long)orderable_key(p) << 32) | (unsigned)crit_sad[s];
-    }
-  }
-  int pos = block_append(count, take);
-  if (take) {
-    keys[pos] = key;
-    vals[pos] = s;
-  }
-}
-
 // Final arcs of the surviving saddles: length and the chain root of each
-// (survivor i in output order, arc j). `surv_sad[i]` = dense saddle index.
-// Images whose output does not take this side's arcs (`arcs_primal` /
-// `arcs_dual` by orientation) get empty arcs.
-__global__ void final_arcs_kernel(int nsurv, const int* __restrict__ surv_sad, const int* __restrict__ sad_img,
-                                  const uint8_t* __restrict__ dual, bool arcs_primal, bool arcs_dual,
-                                  const int* __restrict__ t, const long long* __restrict__ blen, ReplayState S,
-                                  int max_steps, long long* __restrict__ arc_len, long long* __restrict__ arc_cl,
+// (survivor i in output order, arc j), from the survivors' gathered records
+// (image, arc ends, raw-arc lengths). Images whose output does not take this
+// side's arcs (`arcs_primal` / `arcs_dual` by orientation) get empty arcs.
+__global__ void final_arcs_kernel(int nsurv, const int2* __restrict__ surv_ic, const uint8_t* __restrict__ dual,
+                                  bool arcs_primal, bool arcs_dual, const int2* __restrict__ sv_t,
+                                  const longlong2* __restrict__ sv_len, ReplayState S, int max_steps,
+                                  long long* __restrict__ arc_len, long long* __restrict__ arc_cl,
                                   int* __restrict__ arc_root, unsigned* status) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= 2 * nsurv) return;
   int i = q >> 1, j = q & 1;
-  int s = surv_sad[i];
-  int T = t[2 * s + j];
-  if (T < 0 || !(dual[sad_img[s]] ? arcs_dual : arcs_primal)) {
+  const int2 tt = sv_t[i];
+  const int T = j ? tt.y : tt.x;
+  if (T < 0 || !(dual[surv_ic[i].x] ? arcs_dual : arcs_primal)) {
     arc_len[q] = 0;
     arc_cl[q] = 0;
     arc_root[q] = -1;
     return;
   }
+  const longlong2 bl = sv_len[i];
   int R;
   long long a;
   walk_root(S, T, kNever, &R, &a, max_steps, status);
-  arc_len[q] = blen[2 * s + j] + a;
+  arc_len[q] = (j ? bl.y : bl.x) + a;
   arc_cl[q] = a;
   arc_root[q] = R;
 }
@@ -212,9 +185,8 @@ __global__ void final_arcs_kernel(int nsurv, const int* __restrict__ surv_sad, c
 // ---------------------------------------------------------------------------
 // geometry emission
 // ---------------------------------------------------------------------------
-enum : int { kTaskBase = 0, kTaskChain = 2 };
-// task = {kind | dir << 2, a, b, pos}; base: a = saddle, b = arc;
-// chain: a = start node, b = stop node (-1 = void).
+enum : int { kTaskChain = 2 };
+// chain task = {kind | dir << 2, start node, stop node (-1 = void), pos}
 __device__ __forceinline__ int4 make_task(int kind, int rev, int a, int b, long long pos) {
   return make_int4(kind | (rev << 2), a, b, (int)pos);
 }
@@ -230,122 +202,76 @@ struct EmitCtx {
   ReplayState S;
   int* out_primal;  // destination of primal images' arcs of this side
   int* out_dual;    // destination of dual images' arcs
-  int4* q_out;
-  int* n_out;
   long long q_cap;
   int4* base_q;  // raw-arc segments, written after the expansion
-  int* n_base;
   long long base_cap;
   int max_steps;
   unsigned* status;
 };
 
-// A raw arc (s, j) being written by one lane: the V-path from its start cell,
-// `len` cells (cpu/arcs_geometry.hxx:83-111, 133-161), following the flow
-// codes. dst is the next output slot, step its stride (-1 for a reversed
-// arc), rem the cells left and idx the current index.
+// Raw-arc segment tasks come in two forms. A direct task carries everything
+// its writer needs, {start index | 1 << 30 | reversed << 31, cells, output
+// position, image}; the start index is the global index of the arc's first
+// cell (its face or vertex next to the saddle, cpu/arcs_geometry.hxx:74-81,
+// 124-131). Indices stay below 2^29 and a side's geometry below 2^31 cells
+// (checked by the host). A saddle task {reversed << 2, saddle, arc, output
+// position} leaves the look-ups to the writer: the chain expansion emits
+// those, so its walks along parent chains wait on no extra loads.
+constexpr int kSegDirect = 1 << 30;
+__device__ __forceinline__ int arc_start_of_cell(const EmitCtx& E, int sc, int j, int b) {
+  const int W = E.I.W[b], Nx = W + 1;
+  const int cell = E.faces ? face_start(sc, j, Nx) : vertex_start(sc, j, E.I.H[b], W, Nx, E.I.idx_base[b]);
+  return cell >> 2;
+}
+__device__ __forceinline__ int arc_start_index(const EmitCtx& E, int s, int j, int b) {
+  return arc_start_of_cell(E, E.crit_sad[s], j, b);
+}
+__device__ __forceinline__ int4 make_seg(int start, int rev, long long len, long long pos, int b) {
+  return make_int4(start | kSegDirect | (rev << 31), (int)len, (int)pos, b);
+}
+__device__ __forceinline__ int4 make_saddle_seg(int s, int j, int rev, long long pos) {
+  return make_int4(rev << 2, s, j, (int)pos);
+}
+
+// A raw arc being written by one lane: the V-path from its start cell, `len`
+// cells (cpu/arcs_geometry.hxx:83-111, 133-161), following the flow codes.
+// dst is the next output slot, step its stride (-1 for a reversed arc), rem
+// the cells left and idx the current index.
 struct SegCursor {
   int* dst;
   int step;
-  long long rem;
+  int rem;
   int idx, ibase, Nx;
 };
 
-// Starts raw arc (s, j) at output position pos; rem = 0 when it writes
-// nothing (no arc, or its image's output does not take this side's arcs).
-__device__ __forceinline__ void seg_start(const EmitCtx& E, int s, int j, int rev, long long pos, SegCursor& c) {
+// Starts the segment task t; rem = 0 when it writes nothing (its image's
+// output does not take this side's arcs).
+__device__ __forceinline__ void seg_start(const EmitCtx& E, const int4 t, SegCursor& c) {
   c.rem = 0;
-  const long long len = E.blen[2 * s + j];
-  if (len <= 0) return;
-  const int b = E.sad_img[s];
+  int b, idx, len, pos;
+  bool rev;
+  if (t.x & kSegDirect) {
+    b = t.w;
+    idx = t.x & (kSegDirect - 1);
+    len = t.y;
+    pos = t.z;
+    rev = (unsigned)t.x >> 31;
+  } else {
+    const int s = t.y, j = t.z;
+    len = (int)E.blen[2 * s + j];
+    b = E.sad_img[s];
+    idx = len > 0 ? arc_start_index(E, s, j, b) : 0;
+    pos = t.w;
+    rev = (t.x >> 2) & 1;
+  }
   int* out = E.I.dual[b] ? E.out_dual : E.out_primal;
-  if (!out) return;
-  const int W = E.I.W[b];
-  c.Nx = W + 1;
+  if (!out || len <= 0) return;
+  c.Nx = E.I.W[b] + 1;
   c.ibase = E.I.idx_base[b];
-  const int sc = E.crit_sad[s];
-  const int cell = E.faces ? face_start(sc, j, c.Nx) : vertex_start(sc, j, E.I.H[b], W, c.Nx, c.ibase);
-  c.idx = cell >> 2;
-  c.dst = out + (rev ? pos + len - 1 : pos);
+  c.idx = idx;
+  c.dst = out + (rev ? (long long)pos + len - 1 : (long long)pos);
   c.step = rev ? -1 : 1;
   c.rem = len;
-}
-
-// Writes the cursor's cell (image-local id: faces are type 3, vertices type 0)
-// and moves to the next one.
-__device__ __forceinline__ void seg_step(const EmitCtx& E, SegCursor& c) {
-  *c.dst = (E.faces ? 3 : 0) + 4 * (c.idx - c.ibase);
-  c.dst += c.step;
-  if (--c.rem > 0) c.idx += flow_step((__ldg(E.flow + c.idx) >> (E.faces ? 4 : 0)) & 7u, c.Nx);
-}
-
-// Expands W(d): queues its two chains at slot p and its two raw-arc segments
-// at base slot pb, advancing both.
-__device__ __forceinline__ void emit_w(const EmitCtx& E, int d, int rev, long long pos, int& p, int& pb) {
-  const int4 nw = node_words(E.S.node, d);
-  int k = side_of(nw.z), o = 1 - k, s = nw.w;
-  int Tk = E.t[2 * s + k], To = E.t[2 * s + o];
-  const longlong2 cl = *reinterpret_cast<const longlong2*>(&E.S.node[d].cl_dy);
-  long long la = cl.x, lb = E.blen[2 * s + k], lc = E.blen[2 * s + o], ld = cl.y;
-  int R = nw.y;
-  if (!rev) {
-    // reverse(chain(Tk -> d)) + reverse(arc k) + arc o + chain(To -> R)
-    if (la > 0) E.q_out[p++] = make_task(kTaskChain, 1, Tk, d, pos);
-    if (lb > 0) E.base_q[pb++] = make_task(kTaskBase, 1, s, k, pos + la);
-    if (lc > 0) E.base_q[pb++] = make_task(kTaskBase, 0, s, o, pos + la + lb);
-    if (ld > 0) E.q_out[p++] = make_task(kTaskChain, 0, To, R, pos + la + lb + lc);
-  } else {
-    if (ld > 0) E.q_out[p++] = make_task(kTaskChain, 1, To, R, pos);
-    if (lc > 0) E.base_q[pb++] = make_task(kTaskBase, 1, s, o, pos + ld);
-    if (lb > 0) E.base_q[pb++] = make_task(kTaskBase, 0, s, k, pos + ld + lc);
-    if (la > 0) E.q_out[p++] = make_task(kTaskChain, 0, Tk, d, pos + ld + lc + lb);
-  }
-}
-
-// A chain task expanded in one step: chain(x -> stop) is the concatenation
-// of W(z) for the nodes z on x's parent chain up to stop; every W(z) is
-// expanded in place (its raw-arc segments and its own two chains), so the
-// breadth-first expansion needs one level per chain depth instead of two.
-// Counts of the chain tasks and raw-arc segments the expansion writes, and
-// the chain's total length.
-// Returns false (with zero counts) when the chain exceeds its step cap; the
-// task is then dropped and the status reports the cap.
-__device__ __forceinline__ bool chain_expand_counts(const EmitCtx& E, int x, int stop, int* n_chain, int* n_base,
-                                                    long long* total) {
-  long long tot = 0;
-  int nc = 0, nb = 0, k = 0, z = x;
-  *n_chain = 0;
-  *n_base = 0;
-  *total = 0;
-  while (z != stop && z >= 0) {
-    const longlong2 kl = node_keylen(E.S.node, z);
-    const int4 w = node_words(E.S.node, z);
-    tot += kl.y;
-    nc += chains_of(w.z);  // counts stored at link time
-    nb += bases_of(w.z);
-    z = w.y;
-    if (++k > E.max_steps) {
-      set_status(E.status, kStatusChainCap);
-      return false;
-    }
-  }
-  *n_chain = nc;
-  *n_base = nb;
-  *total = tot;
-  return true;
-}
-
-// Writes the expansion counted by chain_expand_counts at slots p and pb.
-__device__ void chain_expand(const EmitCtx& E, int x, int stop, int rev, long long pos, long long total, int p,
-                             int pb) {
-  long long off = 0;
-  int k = 0;
-  for (int z = x; z != stop && z >= 0; z = E.S.node[z].parent) {
-    if (++k > E.max_steps) break;
-    const long long w = E.S.node[z].wlen;
-    emit_w(E, z, rev, rev ? pos + total - off - w : pos + off, p, pb);
-    off += w;
-  }
 }
 
 }  // namespace dmsc

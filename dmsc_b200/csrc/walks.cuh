@@ -109,13 +109,12 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
 // surviving extrema of its thresholded union-find root, or -1 when the root is
 // the void (cpu/cell_groups.hxx:128-146, 168-173). `alive_base[b]` is the
 // first output rank of image b's extrema.
-__global__ void label_map_kernel(int M, const int* __restrict__ ext_img, const int* __restrict__ ut_root,
-                                 const int* __restrict__ region, const int* __restrict__ alive_base,
-                                 int* __restrict__ lab) {
+__global__ void label_map_kernel(int M, const int* __restrict__ ext_img, const int* __restrict__ rout,
+                                 const int* __restrict__ alive_base, int* __restrict__ lab) {
   int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= M) return;
-  int u = ut_root[r];
-  lab[r] = u < 0 ? -1 : region[u] - alive_base[ext_img[r]];
+  const int o = rout[r];  // batch-wide out rank of the root (-1: the void)
+  lab[r] = o < 0 ? -1 : o - alive_base[ext_img[r]];
 }
 
 // Where the labels of one side go: image b's block of the output array picked

@@ -9,6 +9,12 @@ changes an output bit:
   (how much of the value window and its halo row each CTA stages);
 * ``label_shape``: 64 x 64 label tiles on 1024 or 512 threads (4 or 8 cells
   per thread in the barrier-free pointer jumping);
+* ``pair_shape``: pairing items each thread advances together (2 or 4,
+  with 5 or 4 resident blocks per SM);
+* ``replay_shape``: replay cancellations each thread advances together (1 or
+  2, with 4 or 3 resident blocks per SM);
+* ``emit_shape``: geometry-expansion chain tasks each thread advances
+  together (1 or 2, with 5 or 3 resident blocks per SM);
 * ``pair_blocks_per_sm``, ``replay_blocks_per_sm``, ``emit_blocks_per_sm``:
   resident blocks per SM of the three persistent round loops (0 = all that
   fit); fewer blocks make each grid barrier cheaper, more hide more latency;
@@ -37,8 +43,11 @@ from . import _lib
 TUNABLES = (
     ("grad_shape", "gradient", lambda lim: list(range(lim["grad_shapes"]))),
     ("label_shape", "labels", lambda lim: list(range(lim["label_shapes"]))),
+    ("pair_shape", "pairing", lambda lim: list(range(lim["pair_shapes"]))),
     ("pair_blocks_per_sm", "pairing", lambda lim: _blocks(lim["pair_blocks_per_sm"])),
+    ("replay_shape", "replay", lambda lim: list(range(lim["replay_shapes"]))),
     ("replay_blocks_per_sm", "replay", lambda lim: _blocks(lim["replay_blocks_per_sm"])),
+    ("emit_shape", "fetch_geometry", lambda lim: list(range(lim["emit_shapes"]))),
     ("emit_blocks_per_sm", "fetch_geometry", lambda lim: _blocks(lim["emit_blocks_per_sm"])),
     ("seg_cursors", "fetch_geometry", lambda lim: list(range(1, lim["seg_cursors"] + 1))),
 )
@@ -49,7 +58,8 @@ _tuning = threading.local()  # set while tune() runs on this thread
 
 
 def _default_tuning() -> dict:
-    return {"grad_shape": 2, "label_shape": 1, "pair_blocks_per_sm": 0, "replay_blocks_per_sm": 0,
+    return {"grad_shape": 2, "label_shape": 1, "pair_shape": 0, "pair_blocks_per_sm": 0, "replay_shape": 0,
+            "replay_blocks_per_sm": 0, "emit_shape": 0,
             "emit_blocks_per_sm": 0, "seg_cursors": 1}
 
 

@@ -190,11 +190,11 @@ const char* dmsc_b200_last_error(const dmsc_b200_context* ctx);
    at every stage boundary. dmsc_b200_stage_times() writes up to `n` stage
    durations in milliseconds of the last extract()+fetch() pair (host pointer)
    and returns the number of stages: 0 set-up (workspace clears, table
-   upload), 1 gradient (the kernel alone), 2 compaction, 3 saddle sort,
-   4 saddle walks, 5 pairing (both sides), 6 persistence, cancellation and
-   output ranks, 7 survivors, 8 replay (both sides), 9 final arcs, 10 label
-   set-up (per-extremum labels, bases), 11 labels (the label kernels alone),
-   12 sizes, 13 fetch lists, 14 fetch geometry. */
+   upload), 1 gradient (the kernel alone), 2 compaction, 3 saddle walks,
+   4 pairing (both sides), 5 persistence, cancellation and output ranks,
+   6 survivors (in sweep order), 7 replay (both sides), 8 final arcs, 9 label
+   set-up (per-extremum labels, bases), 10 labels (the label kernels alone),
+   11 sizes, 12 fetch lists, 13 fetch geometry. */
 int dmsc_b200_set_profiling(dmsc_b200_context* ctx, int enable);
 int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n);
 
@@ -210,7 +210,9 @@ int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n);
 /* Device loop timelines of the last call (ns, device global timer), six
    blocks of 64 slots: pairing round starts (faces, vertices), geometry
    expansion level starts (faces, vertices), then replay round starts (faces,
-   vertices). Unused slots are 0. Writes up to `n` values to `out` (host
+   vertices); then six more blocks in the same order with each round's item
+   count (active saddles, queued chain tasks, pending cancellations). Unused
+   slots are 0. Writes up to `n` (at most 768) values to `out` (host
    pointer), returns the number written. */
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n);
 
@@ -240,7 +242,14 @@ int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_
                   geometry-expansion persistent kernels; 0 = as many as fit
                   (the default); larger values are clamped to what fits.
    seg_cursors  : raw-arc walks each lane of the segment writer drives at
-                  once, 1..2; default 1. */
+                  once, 1..2; default 1.
+   pair_shape   : pairing items each thread advances together, {2, 4}
+                  (with {5, 4} resident blocks per SM), 0..1; default 0.
+   replay_shape : replay cancellations each thread advances together, {1, 2}
+                  (with {4, 3} resident blocks per SM), 0..1; default 0.
+   emit_shape   : geometry-expansion chain tasks each thread advances
+                  together, {1, 2} (with {5, 3} resident blocks per SM),
+                  0..1; default 0. */
 typedef struct {
   int grad_shape;
   int label_shape;
@@ -248,6 +257,9 @@ typedef struct {
   int replay_blocks_per_sm;
   int emit_blocks_per_sm;
   int seg_cursors;
+  int pair_shape;
+  int replay_shape;
+  int emit_shape;
 } dmsc_b200_tuning;
 
 int dmsc_b200_set_tuning(dmsc_b200_context* ctx, const dmsc_b200_tuning* tuning);
@@ -255,8 +267,10 @@ int dmsc_b200_get_tuning(const dmsc_b200_context* ctx, dmsc_b200_tuning* tuning)
 
 /* Choices of the tunables on this context's device (host pointer, up to `n`
    values): number of gradient tile shapes, number of label tile shapes, the
-   most blocks per SM of the pairing, replay and expansion kernels, and the
-   most segment-writer cursors per lane. Returns the number written or -1. */
+   most blocks per SM of the pairing and replay (in their current shapes)
+   and expansion kernels, the most segment-writer cursors per lane, and the
+   numbers of pairing, replay and expansion shapes. Returns the number
+   written or -1. */
 int dmsc_b200_tuning_limits(dmsc_b200_context* ctx, int* out, int n);
 
 /* Host waits inside a call poll an event; after `seconds` (default 600) they

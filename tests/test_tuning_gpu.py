@@ -1,5 +1,7 @@
 """Launch shapes change speed only: every gradient tile shape, label tile
-shape and persistent-kernel residency gives the same bits; the tuner runs,
+shape, pairing, replay and expansion batch shape and persistent-kernel
+residency gives the same
+bits; the tuner runs,
 reports and caches a choice that later calls of the size class use."""
 
 import itertools
@@ -23,13 +25,13 @@ def test_every_launch_shape_is_bit_identical():
     ref = {d: extract_dmsc(img, 0.05, True, d, True, True, True, True) for d in (False, True)}
     tuning._tuning.active = True  # keep the shapes set below for the calls
     try:
-        for g, lab, pb, sc in itertools.product(range(lim["grad_shapes"]), range(lim["label_shapes"]), (0, 1, 3),
-                                                range(1, lim["seg_cursors"] + 1)):
+        for g, lab, pb, sc, ps in itertools.product(range(lim["grad_shapes"]), range(lim["label_shapes"]), (0, 1, 3),
+                                                    range(1, lim["seg_cursors"] + 1), range(lim["pair_shapes"])):
             ctx.set_tuning(grad_shape=g, label_shape=lab, pair_blocks_per_sm=pb, replay_blocks_per_sm=pb,
-                           emit_blocks_per_sm=pb, seg_cursors=sc)
+                           emit_blocks_per_sm=pb, seg_cursors=sc, pair_shape=ps, replay_shape=ps, emit_shape=ps)
             for d in (False, True):
                 got = extract_dmsc(img, 0.05, True, d, True, True, True, True)
-                assert diff_fields(got, ref[d]) == [], (g, lab, pb, sc, d)
+                assert diff_fields(got, ref[d]) == [], (g, lab, pb, sc, ps, d)
     finally:
         tuning._tuning.active = False
         ctx.set_tuning(**tuning._default_tuning())
