@@ -207,8 +207,8 @@ class Context:
     def timelines(self, counts: bool = False) -> dict:
         """Per-round / per-level durations (us) of the device loops of the last
         call; with ``counts``, (durations, items per round) per loop."""
-        buf = (ctypes.c_longlong * 768)()
-        if self.lib.dmsc_b200_pairing_timeline(self.h, buf, 768) < 0:
+        buf = (ctypes.c_longlong * 896)()
+        if self.lib.dmsc_b200_pairing_timeline(self.h, buf, 896) < 0:
             return {}
         out = {}
         for blk, name in enumerate(("pairing_faces", "pairing_vertices", "emit_faces", "emit_vertices",
@@ -216,6 +216,9 @@ class Context:
             t = [x for x in (buf[blk * 64 + k] for k in range(64)) if x > 0]
             d = tuple((b - a) / 1000.0 for a, b in zip(t, t[1:]))
             out[name] = (d, tuple(buf[384 + blk * 64 + k] for k in range(len(t)))) if counts else d
+            if counts and blk < 2:  # pairing: phase A part of each round (us)
+                out[name + "_phase_a"] = (tuple((buf[768 + blk * 64 + k] - t[k]) / 1000.0
+                                                for k in range(len(t) - 1) if buf[768 + blk * 64 + k] > 0), ())
         return out
 
     def close(self):

@@ -31,6 +31,7 @@ enum : unsigned {
   kStatusQueueOverflow = 8u,
   kStatusBadIndex = 16u,
   kStatusFindCap = 32u,     // a union-find root search or union retry loop exceeded its bound
+  kStatusCopyWait = 64u,    // a bulk copy into shared memory did not complete within its time bound
 };
 
 __host__ __device__ __forceinline__ int cell_id(int t, int y, int x, int Nx) { return t + 4 * (y * Nx + x); }

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cub/cub.cuh>
+#include <cudaTypedefs.h>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -423,6 +424,10 @@ void raise_status(dmsc_b200_context* ctx, unsigned h) {
     set_err(ctx, "a bounded device loop reached its cap (status 0x%x)", h);
     throw Fail{kErrIterationCap};
   }
+  if (h & kStatusCopyWait) {
+    set_err(ctx, "a tensor copy into shared memory timed out (status 0x%x)", h);
+    throw Fail{kErrCuda};
+  }
   if (h & kStatusQueueOverflow) {
     set_err(ctx, "geometry work queue overflow (status 0x%x)", h);
     throw Fail{kErrOverflow};
@@ -483,7 +488,7 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const float* sval
   A.status = ctx->status;
   A.max_rounds = capped(M + 2, ctx->cap_pair_rounds);
   A.rounds = get<int>(ctx, S_STATS, 8) + 0 + si;
-  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 12 * kTimeline) + si * kTimeline;
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, kTimelineSlots) + si * kTimeline;
   return A;
 }
 
@@ -526,7 +531,8 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(uf, M + 1));
   if (nsad > 0)
     LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(cends, ncanc, M, uf, M + 2, ctx->status));
-  LK(ut_flatten_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M + 1, uf, M + 2, ctx->status));
+  LK(ut_flatten_kernel<<<grid_for((M + 1 + kUtBatch - 1) / kUtBatch, TB), TB, 0, st>>>(M + 1, uf, M + 2,
+                                                                                       ctx->status));
   LK(ut_mark_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M, uf, S.alive, croot));
   if (M > 0) LK(ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.ut));
   LAUNCH_CHECK("thresholded union-find");
@@ -556,8 +562,6 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
 
   ReplayState& R = S.R;
   R.node = sget<ReplayNode>(ctx, si, X_NODE, M + 1);
-  LK(replay_node_init_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(R.node, M + 1));
-  LAUNCH_CHECK("replay init");
   ReplayArgs A{};
   A.n_cancel = S.C > 0 ? get<int>(ctx, S_NCANC, 4) + si : nullptr;
   A.key = ckey;
@@ -565,6 +569,7 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   A.dying = S.dying;
   A.t = S.t;
   A.blen = S.blen;
+  A.alive = S.alive;
   A.S = R;
   A.max_steps = nsad + 1;
   A.act0 = sget<int>(ctx, si, X_ACT0, nsad);
@@ -575,7 +580,7 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   A.status = ctx->status;
   A.max_rounds = capped(nsad + 2, ctx->cap_replay_rounds);
   A.rounds = get<int>(ctx, S_STATS, 8) + 2 + si;
-  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 12 * kTimeline) + (4 + si) * kTimeline;
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, kTimelineSlots) + (4 + si) * kTimeline;
   return A;
 }
 
@@ -589,7 +594,8 @@ void replay_final(dmsc_b200_context* ctx, int si, Side& S, long long* total, cud
   S.plen = sget<long long>(ctx, si, X_PLEN, nsurv);
   S.send = sget<long long>(ctx, si, X_SEND, nsurv);
   LK(final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv_ic, ctx->I.dual, S.arcs_primal,
-                                                                 S.arcs_dual, S.sv_t, S.sv_len, S.R, ctx->nsad + 1,
+                                                                 S.arcs_dual, S.sv_t, S.sv_len, S.alive, S.R,
+                                                                 ctx->nsad + 1,
                                                                  S.arc_len, S.arc_cl, S.arc_root, ctx->status));
   LK(pair_len_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.plen));
   incl_sum(ctx, S.plen, S.send, nsurv, st);
@@ -597,15 +603,69 @@ void replay_final(dmsc_b200_context* ctx, int si, Side& S, long long* total, cud
   LAUNCH_CHECK("final arcs");
 }
 
-// Gradient kernel of tile shape `shape` over `ntile` tiles of the batch.
+// The driver's tensor-map encoder (through the runtime, so the library needs
+// no link against the driver library); null when unavailable.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The TMA-staged persistent gradient of one H x W image (tile TY x 32, NT
+// threads); false when it does not apply (rows not 16-byte multiples, an
+// unaligned buffer, no encoder), and the caller runs the batch kernel.
+template <int TY, int NT>
+bool launch_gradient_tma(dmsc_b200_context* ctx, int H, int W, bool dual, const float* img, int4* grad,
+                         int* const* seg, uint8_t* flow, cudaStream_t st) {
+  if (W % 4 != 0 || (reinterpret_cast<uintptr_t>(img) & 15u) != 0) return false;
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {(cuuint64_t)W, (cuuint64_t)H};
+  const cuuint64_t strides[1] = {(cuuint64_t)W * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)kTmaCols, (cuuint32_t)(TY + 3)};
+  const cuuint32_t estr[2] = {1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(img), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  auto kernel = dual ? gradient_tma_kernel<true, TY, NT> : gradient_tma_kernel<false, TY, NT>;
+  constexpr int kSmem = grad_tma_smem_bytes<TY>();
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+  int per = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, NT, kSmem));
+  const int ntx = (W + 1 + kTileX - 1) / kTileX, nty = (H + 1 + TY - 1) / TY;
+  const long long ntiles = (long long)ntx * nty;
+  const int grid = (int)std::min<long long>(ntiles, (long long)std::max(1, per) * ctx->num_sms);
+  LK((kernel<<<grid, NT, kSmem, st>>>(map, H, W, ntx, (int)ntiles, grad, flow, seg[0], seg[1], seg[2], ctx->fifo_lut,
+                                      ctx->status)));
+  LAUNCH_CHECK("gradient_tma_kernel");
+  return true;
+}
+
+// Gradient kernel of tile shape `shape` over `ntile` tiles of the batch (a
+// TMA shape on a one-image batch runs the persistent kernel when it applies).
 void launch_gradient(dmsc_b200_context* ctx, int shape, unsigned ntile, const Imgs& I, const float* img, int4* grad,
-                     uint8_t* mask, int* const* seg, uint8_t* flow, cudaStream_t st) {
-  switch (shape) {
-    case 0:
+                     uint8_t* mask, int* const* seg, uint8_t* flow, cudaStream_t st, int B, int H0, int W0,
+                     bool dual0) {
+  if (kGradTma[shape] && B == 1 && !mask) {
+    const bool done =
+        shape == 3 ? launch_gradient_tma<kGradTY[3], kGradNT[3]>(ctx, H0, W0, dual0, img, grad, seg, flow, st)
+                   : launch_gradient_tma<kGradTY[4], kGradNT[4]>(ctx, H0, W0, dual0, img, grad, seg, flow, st);
+    if (done) return;
+  }
+  switch (kGradTY[shape]) {
+    case kGradTY[0]:
       LK((gradient_batch_kernel<kGradTY[0], kGradNT[0]><<<ntile, kGradNT[0], 0, st>>>(I, img, grad, mask, seg[0], seg[1],
                                                                                       seg[2], ctx->fifo_lut, flow)));
       break;
-    case 1:
+    case kGradTY[1]:
       LK((gradient_batch_kernel<kGradTY[1], kGradNT[1]><<<ntile, kGradNT[1], 0, st>>>(I, img, grad, mask, seg[0], seg[1],
                                                                                       seg[2], ctx->fifo_lut, flow)));
       break;
@@ -711,8 +771,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   mark(ctx, 0, st);
   CK(cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st));
   CK(cudaMemsetAsync(get<int>(ctx, S_STATS, 8), 0, 8 * sizeof(int), st));
-  CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, 12 * kTimeline), 0,
-                     12 * kTimeline * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(get<unsigned long long>(ctx, S_TIMELINE, kTimelineSlots), 0,
+                     kTimelineSlots * sizeof(unsigned long long), st));
   {  // upload the tables: 9 int arrays, then thr (float) and dual (u8)
     size_t ib = tab.size() * sizeof(int), fb = (size_t)B * sizeof(float);
     size_t total = ib + fb + B + 16;
@@ -749,7 +809,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   int* seg[3] = {get<int>(ctx, S_SEG0, nseg), get<int>(ctx, S_SEG1, nseg), get<int>(ctx, S_SEG2, nseg)};
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
   mark(ctx, 15, st);  // the gradient stage times the kernel alone
-  launch_gradient(ctx, gshape, (unsigned)ntile, I, img, (int4*)grad, nullptr, seg, flow, st);
+  launch_gradient(ctx, gshape, (unsigned)ntile, I, img, (int4*)grad, nullptr, seg, flow, st, B, hH[0], hW[0],
+                  hdual[0] != 0);
   mark(ctx, 1, st);
   if (ret_grad) copy_out_async(ctx, ctx->host_grad, grad, 16 * (size_t)nidx, st);
   for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);
@@ -890,6 +951,11 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   const int nsurv = ctx->nsurv;
   LK(image_base_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, BS.sad, nsad, fpos, nsurv, BS.surv));
   LAUNCH_CHECK("survivor bases");
+  // the survivor order and records run on side_st, overlapping the replay
+  // and the labels (neither reads them); the final arcs wait for them
+  cudaStream_t ss = ctx->side_st;
+  CK(cudaEventRecord(ctx->fork_ev, st));
+  CK(cudaStreamWaitEvent(ss, ctx->fork_ev, 0));
   if (nsurv > 0) {
     // the survivors (list order) sorted by (image, s_val) with the list index
     // as the stable tie-break, then each image's range in its vertex-side
@@ -898,33 +964,34 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     int* sorted = get<int>(ctx, S_ASC, nsurv);
     if (B > 1) {
       unsigned long long* k = get<unsigned long long>(ctx, S_SKEY2, nsurv);
-      LK(survivor_gather_kernel<unsigned long long><<<grid_for(nsad, TB), TB, 0, st>>>(nsad, flag, fpos, skey, k, sidx));
-      sort_pairs(ctx, k, get<unsigned long long>(ctx, S_SKEYS, nsurv), sidx, sorted, nsurv, st, 32 + bits_for(B));
+      LK(survivor_gather_kernel<unsigned long long><<<grid_for(nsad, TB), TB, 0, ss>>>(nsad, flag, fpos, skey, k, sidx));
+      sort_pairs(ctx, k, get<unsigned long long>(ctx, S_SKEYS, nsurv), sidx, sorted, nsurv, ss, 32 + bits_for(B));
     } else {
       uint32_t* k = get<uint32_t>(ctx, S_SKEY32B, nsurv);
-      LK(survivor_gather_kernel<uint32_t><<<grid_for(nsad, TB), TB, 0, st>>>(nsad, flag, fpos, skey32, k, sidx));
-      sort_pairs(ctx, k, get<uint32_t>(ctx, S_SKEYS, nsurv), sidx, sorted, nsurv, st, 32);
+      LK(survivor_gather_kernel<uint32_t><<<grid_for(nsad, TB), TB, 0, ss>>>(nsad, flag, fpos, skey32, k, sidx));
+      sort_pairs(ctx, k, get<uint32_t>(ctx, S_SKEYS, nsurv), sidx, sorted, nsurv, ss, 32);
     }
-    LK(survivor_order_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, sorted, ctx->sad_img, I.dual, BS.surv,
+    LK(survivor_order_kernel<<<grid_for(nsurv, TB), TB, 0, ss>>>(nsurv, sorted, ctx->sad_img, I.dual, BS.surv,
                                                                ctx->surv));
     LAUNCH_CHECK("survivor order");
     // the survivors' records, gathered once in output order
     ctx->surv_ic = get<int2>(ctx, S_SURVIC, nsurv);
-    LK(surv_common_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, ctx->sad_img, ctx->crit_sad,
+    LK(surv_common_kernel<<<grid_for(nsurv, TB), TB, 0, ss>>>(nsurv, ctx->surv, ctx->sad_img, ctx->crit_sad,
                                                             ctx->surv_ic));
     for (int si = 0; si < 2; ++si) {
       Side& S = ctx->side[si];
       S.sv_t = sget<int2>(ctx, si, X_SVT, nsurv);
       S.sv_len = sget<longlong2>(ctx, si, X_SVL, nsurv);
       S.sv_rec = sget<int4>(ctx, si, X_SVR, nsurv);
-      LK(surv_side_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv, S.t, S.blen, S.pers, S.pair_dense,
+      LK(surv_side_kernel<<<grid_for(nsurv, TB), TB, 0, ss>>>(nsurv, ctx->surv, S.t, S.blen, S.pers, S.pair_dense,
                                                             S.rout, S.sv_t, S.sv_len, S.sv_rec));
     }
     LAUNCH_CHECK("survivor records");
   }
+  CK(cudaEventRecord(ctx->join_ev, ss));
   mark(ctx, 7, st);
 
-  // ---- replay (both sides in one cooperative launch) + final arc lengths ----
+  // ---- replay (both sides in one cooperative launch) ----
   {
     ReplayArgs2 RA{};
     bool any = false;
@@ -940,23 +1007,6 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
       coop_launch(ctx, ctx->replay_shape ? replay_persistent_kernel<2, 3> : replay_persistent_kernel<1, 4>, RA, st,
                   "replay_persistent_kernel", ctx->replay_per_sm);
     mark(ctx, 8, st);
-    // geometry totals stay on the device (read back with the sizes)
-    long long* tot = get<long long>(ctx, S_TOT, 8);
-    CK(cudaMemsetAsync(tot, 0, 2 * sizeof(long long), st));
-    for (int si = 0; si < 2; ++si) {
-      Side& S = ctx->side[si];
-      S.gbase = sget<long long>(ctx, si, X_GBASE, B + 1);
-      S.total = 0;
-      if (S.arcs && nsad > 0) {
-        if (nsurv > 0) replay_final(ctx, si, S, tot + si, st);
-        LK(geom_base_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, BS.surv, nsurv, S.send, S.plen, tot + si,
-                                                                  S.gbase));
-        LAUNCH_CHECK("geom_base_kernel");
-      } else {
-        CK(cudaMemsetAsync(S.gbase, 0, (B + 1) * sizeof(long long), st));
-      }
-    }
-    mark(ctx, 9, st);
   }
 
   // ---- labels (region id = rank among the image's alive extrema) ----
@@ -1025,6 +1075,28 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   if (f_peaks) copy_out_async(ctx, ctx->host_peaks, peaks_out, 4 * (size_t)npk, st);
   if (f_basins) copy_out_async(ctx, ctx->host_basins, basins_out, 4 * (size_t)nbs, st);
   ctx->host_grad = ctx->host_peaks = ctx->host_basins = nullptr;  // one extract only
+
+  // ---- final arc lengths (after the survivor records on side_st) ----
+  CK(cudaStreamWaitEvent(st, ctx->join_ev, 0));
+  {
+    // geometry totals stay on the device (read back with the sizes)
+    long long* tot = get<long long>(ctx, S_TOT, 8);
+    CK(cudaMemsetAsync(tot, 0, 2 * sizeof(long long), st));
+    for (int si = 0; si < 2; ++si) {
+      Side& S = ctx->side[si];
+      S.gbase = sget<long long>(ctx, si, X_GBASE, B + 1);
+      S.total = 0;
+      if (S.arcs && nsad > 0) {
+        if (nsurv > 0) replay_final(ctx, si, S, tot + si, st);
+        LK(geom_base_kernel<<<grid_for(B + 1LL, TB), TB, 0, st>>>(B, BS.surv, nsurv, S.send, S.plen, tot + si,
+                                                                  S.gbase));
+        LAUNCH_CHECK("geom_base_kernel");
+      } else {
+        CK(cudaMemsetAsync(S.gbase, 0, (B + 1) * sizeof(long long), st));
+      }
+    }
+    mark(ctx, 9, st);
+  }
 
   // ---- e rows ----
   for (int si = 0; si < 2; ++si) {
@@ -1135,10 +1207,11 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   E.max_steps = ctx->nsad + 1;
   E.status = ctx->status;
   A.nsurv = nsurv;
-  A.surv_ic = ctx->surv_ic;
-  A.sv_t = S.sv_t;
-  A.sv_len = S.sv_len;
-  A.arc_pos = arc_pos;
+  E.nvirt = 2 * nsurv;
+  E.surv_ic = ctx->surv_ic;
+  E.sv_t = S.sv_t;
+  E.sv_len = S.sv_len;
+  E.arc_pos = arc_pos;
   A.arc_cl = S.arc_cl;
   A.arc_root = S.arc_root;
   A.q0 = sget<int4>(ctx, si, X_Q0, cap);
@@ -1148,7 +1221,7 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   E.base_cap = cap;
   A.max_levels = capped(ctx->nsad + 4, ctx->cap_emit_levels);
   A.levels = get<int>(ctx, S_STATS, 8) + 4 + si;
-  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, 12 * kTimeline) + (2 + si) * kTimeline;
+  A.timeline = get<unsigned long long>(ctx, S_TIMELINE, kTimelineSlots) + (2 + si) * kTimeline;
   coop_launch(ctx, ctx->emit_shape ? emit_persistent_kernel<2, 3> : emit_persistent_kernel<1, 5>, A, st,
               "emit_persistent_kernel", ctx->emit_per_sm);
   {
@@ -1364,13 +1437,13 @@ int dmsc_b200_create(dmsc_b200_context** out, int device) {
   }
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
   {
-    std::vector<uint32_t> lut(kFifoTable);
-    face_fifo_table(lut.data());
+    std::vector<uint32_t> lut(kGradTable);
+    gradient_tables(lut.data());
     // the copy from pageable memory may return before the table has reached
     // the device and orders only the legacy default stream: wait for it once
     // here, so calls on any (non-blocking) stream see the whole table
-    if (cudaMalloc(&c->fifo_lut, kFifoTable * sizeof(uint32_t)) != cudaSuccess ||
-        cudaMemcpy(c->fifo_lut, lut.data(), kFifoTable * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+    if (cudaMalloc(&c->fifo_lut, kGradTable * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMemcpy(c->fifo_lut, lut.data(), kGradTable * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaDeviceSynchronize() != cudaSuccess) {
       dmsc_b200_destroy(c);
       return kErrCuda;
@@ -1514,10 +1587,11 @@ int dmsc_b200_set_profiling(dmsc_b200_context* ctx, int enable) {
 
 int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n) {
   if (!ctx || !ms || !ctx->profile) return -1;
-  // extract stages are marks 0, 15, 1, 2, 4..9, 16, 10, 11 (15: just before
-  // the gradient kernel, 16: just before the label kernels; mark 3 is not
-  // recorded), fetch stages 12..14
-  static const int from[] = {0, 15, 1, 2, 4, 5, 6, 7, 8, 9, 16, 10, 12, 13};
+  // extract stages are marks 0, 15, 1, 2, 4..8, 16, 10, 9, 11 in stream
+  // order (15: just before the gradient kernel, 16: just before the label
+  // kernels; the labels run before the final arcs; mark 3 is not recorded),
+  // fetch stages 12..14
+  static const int from[] = {0, 15, 1, 2, 4, 5, 6, 7, 10, 8, 16, 9, 12, 13};
   static const int to[] = {15, 1, 2, 4, 5, 6, 7, 8, 9, 16, 10, 11, 13, 14};
   const int ns = (int)(sizeof(from) / sizeof(from[0]));
   if (cudaEventSynchronize(ctx->ev[14]) != cudaSuccess) return -1;
@@ -1533,7 +1607,7 @@ long long dmsc_b200_launch_count(const dmsc_b200_context* ctx) { return ctx ? ct
 
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n) {
   if (!ctx || !out || ctx->bufs.size() <= (size_t)S_TIMELINE || !ctx->bufs[S_TIMELINE].p) return -1;
-  int k = n < 12 * kTimeline ? n : 12 * kTimeline;
+  int k = n < kTimelineSlots ? n : kTimelineSlots;
   if (cudaSetDevice(ctx->device) != cudaSuccess ||
       cudaMemcpy(out, ctx->bufs[S_TIMELINE].p, k * sizeof(long long), cudaMemcpyDeviceToHost) != cudaSuccess)
     return -1;

@@ -29,6 +29,8 @@
 // ascending-cell-id lists.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace dmsc {
@@ -136,6 +138,42 @@ inline void face_fifo_table(uint32_t* out) {
 }
 constexpr int kFifoTable = 16 * 16 * 5;
 
+// Pixels whose eight neighbours all exist (every pixel of an interior tile):
+// the word is a function of 14 comparisons, P against its eight neighbours
+// and the six pairs of its edge neighbours (L, R, U, D) that decide which
+// lower edge pairs with the vertex, so one lookup in a 2^14-entry table
+// replaces the scan. Entry bits: 0 L, 1 R, 2 U, 3 D, 4 UL, 5 UR, 6 DL, 7 DR
+// (P above that neighbour), 8 L above R, 9 L above U, 10 R above U, 11 L
+// above D, 12 R above D, 13 U above D (each under the (value, id) order, the
+// flipped one in the dual). The table follows the general path's rules
+// (star_word below) and is appended to the FIFO table.
+constexpr int kStarTable = 1 << 14;
+constexpr int kGradTable = kFifoTable + kStarTable;
+inline void gradient_tables(uint32_t* out) {
+  face_fifo_table(out);
+  for (unsigned idx = 0; idx < (unsigned)kStarTable; ++idx) {
+    auto bit = [&](int k) { return (idx >> k) & 1u; };
+    const unsigned eL = bit(0) | bit(1) << 1 | bit(2) << 2 | bit(3) << 3;
+    const unsigned fL = (bit(0) & bit(2) & bit(4)) | (bit(1) & bit(2) & bit(5)) << 1 | (bit(0) & bit(3) & bit(6)) << 2 |
+                        (bit(1) & bit(3) & bit(7)) << 3;
+    int best = -1, bo = -1;  // bo: 0 L, 1 R, 2 U
+    if (bit(0)) {
+      best = 0;
+      bo = 0;
+    }
+    if (bit(1) && (best < 0 || bit(8))) {
+      best = 1;
+      bo = 1;
+    }
+    if (bit(2) && (best < 0 || (bo == 0 ? bit(9) : bit(10)))) {
+      best = 2;
+      bo = 2;
+    }
+    if (bit(3) && (best < 0 || (bo == 0 ? bit(11) : bo == 1 ? bit(12) : bit(13)))) best = 3;
+    out[kFifoTable + idx] = out[((eL << 4) | fL) * 5 + best + 1];
+  }
+}
+
 // v_greater (cpu/cell_compare.hxx:23-31) orders pixels by (value, y*W+x),
 // flipped in the dual. gt(a, b) when a's linear id is known to be larger (a
 // "after" b) or smaller: the (value, id) tie rule then reduces to one float
@@ -162,7 +200,20 @@ template <bool DUAL, bool INTERIOR>
 __host__ __device__ __forceinline__ uint32_t star_word(float UL, float U, float UR, float L, float P, float R, float DL, float D,
                                               float DR, bool lv, bool rv, bool uv, bool dv,
                                               const uint32_t* __restrict__ lut) {
-  if (INTERIOR) lv = rv = uv = dv = true;
+  if (INTERIOR) {  // all neighbours exist: the 14-comparison table (gradient_tables)
+    const unsigned idx = (unsigned)gt_after<DUAL>(P, L) | (unsigned)gt_before<DUAL>(P, R) << 1 |
+                         (unsigned)gt_after<DUAL>(P, U) << 2 | (unsigned)gt_before<DUAL>(P, D) << 3 |
+                         (unsigned)gt_after<DUAL>(P, UL) << 4 | (unsigned)gt_after<DUAL>(P, UR) << 5 |
+                         (unsigned)gt_before<DUAL>(P, DL) << 6 | (unsigned)gt_before<DUAL>(P, DR) << 7 |
+                         (unsigned)gt_before<DUAL>(L, R) << 8 | (unsigned)gt_after<DUAL>(L, U) << 9 |
+                         (unsigned)gt_after<DUAL>(R, U) << 10 | (unsigned)gt_before<DUAL>(L, D) << 11 |
+                         (unsigned)gt_before<DUAL>(R, D) << 12 | (unsigned)gt_before<DUAL>(U, D) << 13;
+#ifdef __CUDA_ARCH__
+    return __ldg(lut + kFifoTable + idx);
+#else
+    return lut[kFifoTable + idx];
+#endif
+  }
   const bool gL = gt_after<DUAL>(P, L), gU = gt_after<DUAL>(P, U);
   const bool gUL = gt_after<DUAL>(P, UL), gUR = gt_after<DUAL>(P, UR);  // UR = (y-1, x+1) precedes P too
   const bool gR = gt_before<DUAL>(P, R), gD = gt_before<DUAL>(P, D);
@@ -254,7 +305,102 @@ struct GradSmem {
 // gradient, criticality, flow codes and row-segment counts. INTERIOR: the
 // value window [y0-2, y0+TY] x [x0-2, x0+32] lies inside the image, so no
 // bound is tested. `gbase`: global index of the image's index (0, 0);
-// `sbase`: its first row segment; `ntx`: its row segments per row.
+// `sbase`: its first row segment; `ntx`: its row segments per row. The tile
+// runs in three parts: the value window is staged in shared memory; the
+// pairing words of its pixels are computed from the window
+// (gradient_words: value of window row r, column c = pixel (y0 - 2 + r,
+// x0 - 2 + c) at V[r][c + VOFF]); every index gathers its slots from the
+// words (gradient_gather).
+template <bool DUAL, bool INTERIOR, int TY, int NT, int VC, int VOFF>
+__device__ __forceinline__ void gradient_words(const float (*V)[VC], uint32_t (*Wd)[33], int H, int W, int y0, int x0,
+                                               const uint32_t* __restrict__ lut) {
+  constexpr int NW = NT / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  {  // main columns: lane -> column x0 + lane (word column lane + 1), a run of rows per warp
+    constexpr int kRun = (TY + 1 + NW - 1) / NW;
+    const int ra = warp * kRun, rb = min(TY + 1, ra + kRun);
+    const int x = x0 + lane, c = lane + 2;  // value column of the pixel
+    const bool xin = INTERIOR || x < W;
+    const bool lv = INTERIOR || x >= 1, rv = INTERIOR || x + 1 < W;
+    if (ra < rb) {
+      float u0 = V[ra][c - 1 + VOFF], u1 = V[ra][c + VOFF], u2 = V[ra][c + 1 + VOFF];
+      float p0 = V[ra + 1][c - 1 + VOFF], p1 = V[ra + 1][c + VOFF], p2 = V[ra + 1][c + 1 + VOFF];
+      for (int r = ra; r < rb; ++r) {
+        const float d0 = V[r + 2][c - 1 + VOFF], d1 = V[r + 2][c + VOFF], d2 = V[r + 2][c + 1 + VOFF];
+        const int y = y0 - 1 + r;
+        uint32_t w = 0;
+        if (INTERIOR || (xin && y >= 0 && y < H))
+          w = star_word<DUAL, INTERIOR>(u0, u1, u2, p0, p1, p2, d0, d1, d2, lv, rv, INTERIOR || y >= 1,
+                                        INTERIOR || y + 1 < H, lut);
+        Wd[r][lane + 1] = w;
+        u0 = p0;
+        u1 = p1;
+        u2 = p2;
+        p0 = d0;
+        p1 = d1;
+        p2 = d2;
+      }
+    }
+  }
+  {  // halo column x0 - 1 (word column 0, value column 1): lane -> row
+    constexpr int kHaloPasses = (TY + 1 + 31) / 32;
+    if (warp < kHaloPasses) {
+      const int r = warp * 32 + lane;
+      if (r <= TY) {
+        const int y = y0 - 1 + r, x = x0 - 1;
+        uint32_t w = 0;
+        if (INTERIOR || (x >= 0 && x < W && y >= 0 && y < H))
+          w = star_word<DUAL, INTERIOR>(V[r][VOFF], V[r][1 + VOFF], V[r][2 + VOFF], V[r + 1][VOFF],
+                                        V[r + 1][1 + VOFF], V[r + 1][2 + VOFF], V[r + 2][VOFF], V[r + 2][1 + VOFF],
+                                        V[r + 2][2 + VOFF], INTERIOR || x >= 1, INTERIOR || x + 1 < W,
+                                        INTERIOR || y >= 1, INTERIOR || y + 1 < H, lut);
+        Wd[r][0] = w;
+      }
+    }
+  }
+}
+
+template <bool INTERIOR, int TY, int NT>
+__device__ __forceinline__ void gradient_gather(const uint32_t (*Wd)[33], const int* off, int H, int W, int y0, int x0,
+                                                long long gbase, int sbase, int ntx, int tx, int4* __restrict__ grad,
+                                                uint8_t* __restrict__ crit_mask, uint8_t* __restrict__ flow,
+                                                int* __restrict__ seg_min, int* __restrict__ seg_sad,
+                                                int* __restrict__ seg_max) {
+  constexpr int NW = NT / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int Nx = W + 1;
+  // ---- gather and stores: one index row per warp step ----
+  const int ix = x0 + lane;
+  const bool xok = INTERIOR || ix <= W;
+  for (int rr = warp; rr < TY; rr += NW) {
+    const int iy = y0 + rr;
+    if (!INTERIOR && iy > H) break;  // uniform per warp
+    unsigned m = 0;
+    if (xok) {
+      const uint32_t wP = Wd[rr + 1][lane + 1], wL = Wd[rr + 1][lane];
+      const uint32_t wU = Wd[rr][lane + 1], wUL = Wd[rr][lane];
+      const int b = iy * Nx + ix;  // image-local index: the cell ids written are local
+      const size_t gidx = (size_t)(gbase + b);
+      int4 g;
+      unsigned fl;
+      gather_index(wP, wL, wU, wUL, 4 * b, off, INTERIOR || (iy < H && ix < W), g, m, fl);
+      if (grad) grad[gidx] = g;  // null when the gradient is not returned
+      if (crit_mask) crit_mask[gidx] = (uint8_t)m;  // null: the flow byte carries the same bits
+      flow[gidx] = (uint8_t)fl;
+    }
+    // the segment's counts (at most 32, 64 and 32) packed in one warp sum
+    const unsigned cnt = __reduce_add_sync(
+        0xffffffffu, (m & 1u) | (((m >> 1) & 1u) + ((m >> 2) & 1u)) << 8 | ((m >> 3) & 1u) << 16);
+    if (lane == 0) {
+      const int seg = sbase + iy * ntx + tx;
+      seg_min[seg] = (int)(cnt & 0xFFu);
+      seg_sad[seg] = (int)((cnt >> 8) & 0xFFu);
+      seg_max[seg] = (int)(cnt >> 16);
+    }
+  }
+}
+
+
 template <bool DUAL, bool INTERIOR, int TY, int NT>
 __device__ __forceinline__ void gradient_tile(GradSmem<TY>& S, const float* __restrict__ img, int H, int W, int y0,
                                               int x0, long long gbase, int sbase, int ntx, int tx,
@@ -279,86 +425,159 @@ __device__ __forceinline__ void gradient_tile(GradSmem<TY>& S, const float* __re
     if (lane < 3) S.v[r][32 + lane] = b;
   }
   __syncthreads();
-  // ---- pairing words ----
-  {  // main columns: lane -> column x0 + lane (word column lane + 1), a run of rows per warp
-    constexpr int kRun = (TY + 1 + NW - 1) / NW;
-    const int ra = warp * kRun, rb = min(TY + 1, ra + kRun);
-    const int x = x0 + lane, c = lane + 2;  // value column of the pixel
-    const bool xin = INTERIOR || x < W;
-    const bool lv = INTERIOR || x >= 1, rv = INTERIOR || x + 1 < W;
-    if (ra < rb) {
-      float u0 = S.v[ra][c - 1], u1 = S.v[ra][c], u2 = S.v[ra][c + 1];
-      float p0 = S.v[ra + 1][c - 1], p1 = S.v[ra + 1][c], p2 = S.v[ra + 1][c + 1];
-      for (int r = ra; r < rb; ++r) {
-        const float d0 = S.v[r + 2][c - 1], d1 = S.v[r + 2][c], d2 = S.v[r + 2][c + 1];
-        const int y = y0 - 1 + r;
-        uint32_t w = 0;
-        if (INTERIOR || (xin && y >= 0 && y < H))
-          w = star_word<DUAL, INTERIOR>(u0, u1, u2, p0, p1, p2, d0, d1, d2, lv, rv, INTERIOR || y >= 1,
-                                        INTERIOR || y + 1 < H, lut);
-        S.w[r][lane + 1] = w;
-        u0 = p0;
-        u1 = p1;
-        u2 = p2;
-        p0 = d0;
-        p1 = d1;
-        p2 = d2;
-      }
-    }
-  }
-  {  // halo column x0 - 1 (word column 0, value column 1): lane -> row
-    constexpr int kHaloPasses = (TY + 1 + 31) / 32;
-    if (warp < kHaloPasses) {
-      const int r = warp * 32 + lane;
-      if (r <= TY) {
-        const int y = y0 - 1 + r, x = x0 - 1;
-        uint32_t w = 0;
-        if (INTERIOR || (x >= 0 && x < W && y >= 0 && y < H))
-          w = star_word<DUAL, INTERIOR>(S.v[r][0], S.v[r][1], S.v[r][2], S.v[r + 1][0], S.v[r + 1][1], S.v[r + 1][2],
-                                        S.v[r + 2][0], S.v[r + 2][1], S.v[r + 2][2], INTERIOR || x >= 1,
-                                        INTERIOR || x + 1 < W, INTERIOR || y >= 1, INTERIOR || y + 1 < H, lut);
-        S.w[r][0] = w;
-      }
-    }
-  }
+  gradient_words<DUAL, INTERIOR, TY, NT, 35, 0>(S.v, S.w, H, W, y0, x0, lut);
   __syncthreads();
-  // ---- gather and stores: one index row per warp step ----
-  const int ix = x0 + lane;
-  const bool xok = INTERIOR || ix <= W;
-  for (int rr = warp; rr < TY; rr += NW) {
-    const int iy = y0 + rr;
-    if (!INTERIOR && iy > H) break;  // uniform per warp
-    unsigned m = 0;
-    if (xok) {
-      const uint32_t wP = S.w[rr + 1][lane + 1], wL = S.w[rr + 1][lane];
-      const uint32_t wU = S.w[rr][lane + 1], wUL = S.w[rr][lane];
-      const int b = iy * Nx + ix;  // image-local index: the cell ids written are local
-      const size_t gidx = (size_t)(gbase + b);
-      int4 g;
-      unsigned fl;
-      gather_index(wP, wL, wU, wUL, 4 * b, S.off, INTERIOR || (iy < H && ix < W), g, m, fl);
-      if (grad) grad[gidx] = g;  // null when the gradient is not returned
-      if (crit_mask) crit_mask[gidx] = (uint8_t)m;  // null: the flow byte carries the same bits
-      flow[gidx] = (uint8_t)fl;
-    }
-    const unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
-    const unsigned bs1 = __ballot_sync(0xffffffffu, m & 2u);
-    const unsigned bs2 = __ballot_sync(0xffffffffu, m & 4u);
-    const unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
-    if (lane == 0) {
-      const int seg = sbase + iy * ntx + tx;
-      seg_min[seg] = __popc(bmin);
-      seg_sad[seg] = __popc(bs1) + __popc(bs2);
-      seg_max[seg] = __popc(bmax);
-    }
-  }
+  gradient_gather<INTERIOR, TY, NT>(S.w, S.off, H, W, y0, x0, gbase, sbase, ntx, tx, grad, crit_mask, flow, seg_min,
+                                    seg_sad, seg_max);
 }
 
 // Tile shapes of the gradient kernels (index rows, threads): the tuner in
-// the host code picks one per call from these instantiations.
-constexpr int kGradShapes = 3;
-constexpr int kGradTY[kGradShapes] = {31, 63, 127};
-constexpr int kGradNT[kGradShapes] = {256, 256, 512};
+// the host code picks one per call from these instantiations. Shapes 0-2 run
+// gradient_batch_kernel; shapes 3 and 4 run gradient_tma_kernel (one image
+// whose rows are 16-byte multiples in a 16-byte aligned buffer; otherwise
+// the batch kernel with the same tile).
+constexpr int kGradShapes = 5;
+constexpr int kGradTY[kGradShapes] = {31, 63, 127, 63, 127};
+constexpr int kGradNT[kGradShapes] = {256, 256, 512, 256, 512};
+constexpr bool kGradTma[kGradShapes] = {false, false, false, true, true};
+
+// ---------------------------------------------------------------------------
+// Persistent gradient with the value windows staged by the tensor-memory
+// accelerator: each CTA walks its tiles (tile blockIdx.x, then + gridDim.x,
+// ...) and, while it computes one tile, the next tile's window is already
+// being copied into the other half of a double buffer
+// (cp.async.bulk.tensor.2d with an mbarrier; no multicast, and the tensor
+// map covers this call's own image only). The copy box starts on a 16-byte
+// boundary: 40 columns x0-4 .. x0+35 and TY + 3 rows y0-2 .. y0+TY; parts of
+// the box outside the image read as zeros (the bounded path never uses them).
+// ---------------------------------------------------------------------------
+constexpr int kTmaCols = 40;
+
+template <int TY>
+struct alignas(128) GradTmaWindow {  // one copy destination, on a 128-byte boundary
+  float v[TY + 3][kTmaCols];
+};
+template <int TY>
+struct alignas(128) GradTmaSmem {
+  GradTmaWindow<TY> win[2];
+  uint32_t w[TY + 1][33];
+  int off[32];
+  unsigned long long bar[2];
+};
+// dynamic shared memory of the kernel: the struct plus room to align it
+template <int TY>
+constexpr int grad_tma_smem_bytes() {
+  return (int)sizeof(GradTmaSmem<TY>) + 128;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n"
+      ".reg .pred p;\n"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+// orders this CTA's earlier generic-proxy reads of shared memory before the
+// next bulk copy into it
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ unsigned long long grad_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait for phase `parity` of a copy barrier: false after `limit_ns`.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, uint32_t parity,
+                                                  unsigned long long limit_ns) {
+  const unsigned long long t0 = grad_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (grad_ns() - t0 > limit_ns) return false;
+  return true;
+}
+
+template <bool DUAL, int TY, int NT>
+__global__ void __launch_bounds__(NT) gradient_tma_kernel(const __grid_constant__ CUtensorMap map, int H, int W,
+                                                          int ntx, int ntiles, int4* __restrict__ grad,
+                                                          uint8_t* __restrict__ flow, int* __restrict__ seg_min,
+                                                          int* __restrict__ seg_sad, int* __restrict__ seg_max,
+                                                          const uint32_t* __restrict__ lut, unsigned* status) {
+  extern __shared__ __align__(128) unsigned char grad_tma_smem[];
+  // the copy destinations must sit on 128-byte boundaries: align the base
+  const uint32_t base = smem_u32(grad_tma_smem);
+  GradTmaSmem<TY>& S = *reinterpret_cast<GradTmaSmem<TY>*>(grad_tma_smem + (((base + 127u) & ~127u) - base));
+  constexpr uint32_t kBytes = (uint32_t)(TY + 3) * kTmaCols * sizeof(float);
+  constexpr unsigned long long kLimitNs = 1000000000ull;  // a copy takes microseconds
+  const int Nx = W + 1;
+  if (threadIdx.x < 32) S.off[threadIdx.x] = gather_offset(threadIdx.x, Nx);
+  if (threadIdx.x == 0) {
+    mbar_init(&S.bar[0], 1);
+    mbar_init(&S.bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  int t = blockIdx.x;
+  if (threadIdx.x == 0 && t < ntiles) {
+    const int ty = t / ntx, tx = t - ty * ntx;
+    mbar_arrive_expect_tx(&S.bar[0], kBytes);
+    tma_load_2d(&S.win[0].v[0][0], &map, tx * kTileX - 4, ty * TY - 2, &S.bar[0]);
+  }
+  for (int k = 0; t < ntiles; ++k, t += gridDim.x) {
+    const int b = k & 1;
+    const int tn = t + gridDim.x;
+    // the other buffer was last read before the barrier that ended the
+    // previous tile: the next tile's copy goes there now
+    if (threadIdx.x == 0 && tn < ntiles) {
+      const int ty = tn / ntx, tx = tn - ty * ntx;
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&S.bar[b ^ 1], kBytes);
+      tma_load_2d(&S.win[b ^ 1].v[0][0], &map, tx * kTileX - 4, ty * TY - 2, &S.bar[b ^ 1]);
+    }
+    const bool ok = mbar_wait_bounded(&S.bar[b], (uint32_t)(k >> 1) & 1u, kLimitNs);
+    if (__syncthreads_or(!ok)) {
+      // report, wait (bounded) for this CTA's copies still in flight, leave
+      if (threadIdx.x == 0) {
+        set_status(status, kStatusCopyWait);
+        mbar_wait_bounded(&S.bar[b], (uint32_t)(k >> 1) & 1u, kLimitNs);
+        if (tn < ntiles) mbar_wait_bounded(&S.bar[b ^ 1], (uint32_t)((k + 1) >> 1) & 1u, kLimitNs);
+      }
+      return;
+    }
+    const int ty = t / ntx, tx = t - ty * ntx, y0 = ty * TY, x0 = tx * kTileX;
+    const bool interior = y0 >= 2 && x0 >= 2 && y0 + TY <= H - 1 && x0 + kTileX <= W - 1;
+    if (interior)
+      gradient_words<DUAL, true, TY, NT, kTmaCols, 2>(S.win[b].v, S.w, H, W, y0, x0, lut);
+    else
+      gradient_words<DUAL, false, TY, NT, kTmaCols, 2>(S.win[b].v, S.w, H, W, y0, x0, lut);
+    __syncthreads();
+    if (interior)
+      gradient_gather<true, TY, NT>(S.w, S.off, H, W, y0, x0, 0, 0, ntx, tx, grad, nullptr, flow, seg_min, seg_sad,
+                                    seg_max);
+    else
+      gradient_gather<false, TY, NT>(S.w, S.off, H, W, y0, x0, 0, 0, ntx, tx, grad, nullptr, flow, seg_min, seg_sad,
+                                     seg_max);
+    __syncthreads();
+  }
+}
 
 // K1 (one image): a 2-D grid of tiles, (ntx, nty).
 template <bool DUAL, int TY, int NT>

@@ -38,7 +38,7 @@ using namespace dmsc;
 // single-block scan relies on.
 constexpr size_t kStaticScratchBytes = 8u << 20;
 __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
-__device__ uint32_t g_static_fifo_lut[kFifoTable];
+__device__ uint32_t g_static_fifo_lut[kGradTable];
 
 constexpr int kMaxDevices = 64;
 struct DeviceStatic {
@@ -60,9 +60,9 @@ int static_setup(int device, DeviceStatic** out) {
     d.scratch = (unsigned char*)p;
     if (cudaGetSymbolAddress(&p, g_static_fifo_lut) != cudaSuccess || !p) return DMSC_B200_ERR_CUDA;
     d.lut = (uint32_t*)p;
-    std::vector<uint32_t> lut(kFifoTable);
-    face_fifo_table(lut.data());
-    if (cudaMemcpyToSymbol(g_static_fifo_lut, lut.data(), kFifoTable * sizeof(uint32_t)) != cudaSuccess)
+    std::vector<uint32_t> lut(kGradTable);
+    gradient_tables(lut.data());
+    if (cudaMemcpyToSymbol(g_static_fifo_lut, lut.data(), kGradTable * sizeof(uint32_t)) != cudaSuccess)
       return DMSC_B200_ERR_CUDA;
     // A copy from pageable host memory may return before the table has
     // reached the device, and it is ordered on the legacy default stream

@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
   }
 }
 
+
 // Thresholded union-find (the reference's uf_min / uf_max, persistence.hxx:
 // 90-104, 147-161): lock-free union of the ends of every cancelled saddle
 // (link the larger root under the smaller), over the compact list of
@@ -130,7 +131,9 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
 // smaller index, so a root search takes at most n steps and every failed CAS
 // means another thread linked one of the two roots (at most n - 1 links
 // exist); both loops are capped at `cap` anyway, and a cap sets
-// kStatusFindCap and returns the node reached (a valid index).
+// kStatusFindCap and returns the node reached (a valid index). One edge per
+// thread: advancing 4 edges' searches in lockstep measured slower here (the
+// forest is deep while the unions run, and a thread waits for its longest).
 __device__ __forceinline__ int uf_root(int* p, int x, int cap, unsigned* status) {
   for (int k = 0;; ++k) {
     int px = p[x];
@@ -171,18 +174,39 @@ __global__ void __launch_bounds__(256) ut_union_kernel(const int2* __restrict__ 
   }
 }
 
+constexpr int kUtBatch = 4;
+
+// Every node's root, kUtBatch nodes per thread with their pointer chains
+// followed in lockstep (a written root is an ancestor for every reader).
 __global__ void ut_flatten_kernel(int n, int* __restrict__ p, int cap, unsigned* status) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= n) return;
-  int r = x;
-  for (int k = 0; p[r] != r; ++k) {
+  const long long nt = (long long)gridDim.x * blockDim.x;
+  const long long x0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int r[kUtBatch];
+  unsigned live = 0;
+#pragma unroll
+  for (int u = 0; u < kUtBatch; ++u) {
+    const long long x = x0 + nt * u;
+    r[u] = (int)x;
+    if (x < n) live |= 1u << u;
+  }
+  const unsigned own = live;
+  for (int k = 0; live; ++k) {
     if (k >= cap) {
       set_status(status, kStatusFindCap);
       break;
     }
-    r = p[r];
+    int pr[kUtBatch];
+#pragma unroll
+    for (int u = 0; u < kUtBatch; ++u) pr[u] = ((live >> u) & 1u) ? p[r[u]] : r[u];
+#pragma unroll
+    for (int u = 0; u < kUtBatch; ++u) {
+      if (pr[u] == r[u]) live &= ~(1u << u);
+      r[u] = pr[u];
+    }
   }
-  p[x] = r;
+#pragma unroll
+  for (int u = 0; u < kUtBatch; ++u)
+    if ((own >> u) & 1u) p[x0 + nt * u] = r[u];
 }
 
 // Component root = its alive member, or -1 for the void's component.

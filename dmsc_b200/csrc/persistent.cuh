@@ -27,8 +27,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 constexpr int kTimeline = 64;  // timestamps kept per loop (round starts)
 // The timeline buffer holds 6 loops' round start times, then each round's
-// item count at the same position + kTimelineCounts.
+// item count at the same position + kTimelineCounts, then the pairing's
+// phase-B start times (faces, vertices) at kTimelinePhaseB.
 constexpr int kTimelineCounts = 6 * kTimeline;
+constexpr int kTimelinePhaseB = 12 * kTimeline;
+constexpr int kTimelineSlots = 14 * kTimeline;
 
 // Root of x in the pairing's group forest. A group links only under an
 // older group (ages strictly decrease along links), so a search visits at
@@ -443,6 +446,9 @@ __global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2
       __syncthreads();
     else
       grid.sync();
+    if (tid == 0 && r < kTimeline)  // side sd's phase-B starts: block 12 + sd
+      for (int sd = 0; sd < 2; ++sd)
+        if (P.s[sd].timeline) P.s[sd].timeline[kTimelinePhaseB + r] = global_ns();
     // phase B: live roots decide on their first outgoing saddle
     {
       const long long n = (long long)nr0 + nr1, chunk = chunk_size(n, nblk);
@@ -472,6 +478,7 @@ struct ReplayArgs {
   const int* dying;  // [nsad] in saddle list order
   const int* t;      // [2 nsad] extremum ends of each saddle, list order
   const long long* blen;
+  const uint8_t* alive;  // [M] extrema that no cancellation kills (their records are never read)
   ReplayState S;
   int max_steps;
   int* act0;
@@ -512,7 +519,8 @@ __device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long 
       const bool s1 = i >= na;
       act |= 1u << u;
       s1m |= (unsigned)s1 << u;
-      r[u] = ((rd & 1) ? RSIDE(act1) : RSIDE(act0))[s1 ? i - na : i];
+      const long long j = s1 ? i - na : i;
+      r[u] = rd == 0 ? (int)j : ((rd & 1) ? RSIDE(act1) : RSIDE(act0))[j];
     }
   }
   unsigned long long tk[U];
@@ -528,12 +536,24 @@ __device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long 
     const bool s1 = (s1m >> u) & 1u;
     tk[u] = RSIDE(key)[r[u]];
     sd[u] = RSIDE(cj)[r[u]];
-    const int2 w = *reinterpret_cast<const int2*>(RSIDE(wx) + 2 * r[u]);
-    const longlong2 aa = *reinterpret_cast<const longlong2*>(RSIDE(wa) + 2 * r[u]);
-    x[2 * u] = w.x;
-    x[2 * u + 1] = w.y;
-    a[2 * u] = aa.x;
-    a[2 * u + 1] = aa.y;
+    if (rd > 0) {  // resume where the previous round left the walks
+      const int2 w = *reinterpret_cast<const int2*>(RSIDE(wx) + 2 * r[u]);
+      const longlong2 aa = *reinterpret_cast<const longlong2*>(RSIDE(wa) + 2 * r[u]);
+      x[2 * u] = w.x;
+      x[2 * u + 1] = w.y;
+      a[2 * u] = aa.x;
+      a[2 * u + 1] = aa.y;
+    }
+  }
+  if (rd == 0) {  // the walks start at the saddle's arc ends
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!((act >> u) & 1u)) continue;
+      const bool s1 = (s1m >> u) & 1u;
+      const int2 w = *reinterpret_cast<const int2*>(RSIDE(t) + 2 * sd[u]);
+      x[2 * u] = w.x;
+      x[2 * u + 1] = w.y;
+    }
   }
   int d[U];  // the dying node (issued before the walks, used after them)
 #pragma unroll
@@ -541,7 +561,9 @@ __device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long 
     const bool s1 = (s1m >> u) & 1u;
     d[u] = ((act >> u) & 1u) ? RSIDE(dying)[sd[u]] : 0;
   }
-  // the walks (walk_resume, in lockstep): bit c of `live` is a walk still
+  // the walks, resumed where the previous round left them and advanced in
+  // lockstep (the root as of the step's key, with the length summed on the
+  // way): bit c of `live` is a walk still
   // moving, bit c of `wait` one that met an undecided node
   unsigned live = 0, wait = 0;
 #pragma unroll
@@ -557,10 +579,12 @@ __device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long 
     }
     longlong2 kl[2 * U];
     int2 w[2 * U];  // status, parent
+    bool al[2 * U];
 #pragma unroll
     for (int c = 0; c < 2 * U; ++c) {
       const bool s1 = (s1m >> (c >> 1)) & 1u;
-      if ((live >> c) & 1u) {  // one sector: both parts issued together
+      if ((live >> c) & 1u) {  // the alive flag and the record's sector, issued together
+        al[c] = RSIDE(alive)[x[c]];
         kl[c] = node_keylen_cg(RSIDE(S.node), x[c]);
         w[c] = __ldcg(reinterpret_cast<const int2*>(&RSIDE(S.node)[x[c]].status));
       }
@@ -568,7 +592,9 @@ __device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long 
 #pragma unroll
     for (int c = 0; c < 2 * U; ++c) {
       if (!((live >> c) & 1u)) continue;
-      if ((unsigned long long)kl[c].x >= tk[c >> 1]) {  // not linked before this step: the root
+      // never cancelled (its record is not written), or not linked before
+      // this step: the root
+      if (al[c] || (unsigned long long)kl[c].x >= tk[c >> 1]) {
         live &= ~(1u << c);
         continue;
       }
@@ -646,16 +672,12 @@ __global__ void __launch_bounds__(256, MINB) replay_persistent_kernel(ReplayArgs
     const ReplayArgs& A = P.s[sd];
     if (!A.n_cancel) continue;
     const int C = *A.n_cancel;
+    // the killed nodes' keys; round 0 takes every cancellation with its
+    // walks starting at the saddle's arc ends (no list or walk state yet)
     for (long long r = tid; r < C; r += nth) {
-      A.act0[r] = (int)r;
-      const int s = A.cj[r];
-      int d = A.dying[s];
+      const int d = A.dying[A.cj[r]];
       A.S.node[d].ctime = A.key[r];
       A.S.node[d].status = kPending;
-      A.wx[2 * r] = A.t[2 * s];
-      A.wx[2 * r + 1] = A.t[2 * s + 1];
-      A.wa[2 * r] = 0;
-      A.wa[2 * r + 1] = 0;
     }
     if (tid == 0) {
       A.cnt[0] = C;
@@ -700,7 +722,7 @@ __global__ void __launch_bounds__(256, MINB) replay_persistent_kernel(ReplayArgs
       for (long long i = t0; i < (long long)na + nb; i += nt) {
         const ReplayArgs& A = i < na ? P.s[0] : P.s[1];
         const long long k = i < na ? i : i - na;
-        const int r = ((rd & 1) ? A.act1 : A.act0)[k];
+        const int r = rd == 0 ? (int)k : ((rd & 1) ? A.act1 : A.act0)[k];
         A.S.node[A.dying[A.cj[r]]].status = kRootForever;
       }
       break;
@@ -725,10 +747,6 @@ __global__ void __launch_bounds__(256, MINB) replay_persistent_kernel(ReplayArgs
 struct EmitArgs {
   EmitCtx E;
   int nsurv;
-  const int2* surv_ic;      // [nsurv] image and cell of each survivor (output order)
-  const int2* sv_t;         // [nsurv] this side's arc ends of each survivor
-  const longlong2* sv_len;  // [nsurv] this side's raw-arc lengths of each survivor
-  const long long* arc_pos;
   const long long* arc_cl;
   const int* arc_root;
   int4* q0;
@@ -898,41 +916,25 @@ __global__ void __launch_bounds__(256, MINB) emit_persistent_kernel(EmitArgs A) 
   grid.sync();
   const EmitCtx& E = A.E;
   int* const n_base = A.cnt + 3;
-  // level 0: each surviving arc's own raw arc, then its chain
+  // level 0: the chain of each surviving arc (its own raw arc is a segment
+  // item of the writer, read from the survivor records)
   for (long long base = 0; base < 2LL * A.nsurv; base += nth) {
-    long long q = base + tid;
-    bool push = false, seg = false;
-    int4 task = make_int4(0, 0, 0, 0), btask = make_int4(0, 0, 0, 0);
-    if (q < 2LL * A.nsurv) {
-      int i = (int)(q >> 1), j = (int)(q & 1);
-      // images whose output takes none of this side's arcs emit nothing
-      const int2 ic = A.surv_ic[i];
-      const int b = ic.x;
-      const bool takes = (E.I.dual[b] ? E.out_dual : E.out_primal) != nullptr;
-      const int2 tt = A.sv_t[i];
-      const int T = j ? tt.y : tt.x;
-      if (takes && T >= 0) {
-        const longlong2 bl = A.sv_len[i];
-        const long long len = j ? bl.y : bl.x, pos = A.arc_pos[q];
-        seg = len > 0;
-        if (seg) btask = make_seg(arc_start_of_cell(E, ic.y, j, b), 0, len, pos, b);
-        if (A.arc_cl[q] > 0) {
-          push = true;
-          task = make_task(kTaskChain, 0, T, A.arc_root[q], pos + len);
-        }
-      }
+    const long long q = base + tid;
+    bool push = false;
+    int4 task = make_int4(0, 0, 0, 0);
+    // a chain exists only on arcs that the image's output takes (arc_cl = 0 otherwise)
+    if (q < 2LL * A.nsurv && A.arc_cl[q] > 0) {
+      const int i = (int)(q >> 1), j = (int)(q & 1);
+      const int2 tt = E.sv_t[i];
+      const longlong2 bl = E.sv_len[i];
+      push = true;
+      task = make_task(kTaskChain, 0, j ? tt.y : tt.x, A.arc_root[q], E.arc_pos[q] + (j ? bl.y : bl.x));
     }
     int p, pb;
-    block_reserve2(A.cnt, push ? 1 : 0, n_base, seg ? 1 : 0, p, pb);
+    block_reserve2(A.cnt, push ? 1 : 0, n_base, 0, p, pb);
     if (push) {
       if (p < E.q_cap)
         A.q0[p] = task;
-      else
-        set_status(E.status, kStatusQueueOverflow);
-    }
-    if (seg) {
-      if (pb < E.base_cap)
-        E.base_q[pb] = btask;
       else
         set_status(E.status, kStatusQueueOverflow);
     }
@@ -986,7 +988,7 @@ constexpr int kSegCursorShapes = 2;  // NC = 1 or 2 (tuned)
 
 template <int NC>
 __global__ void __launch_bounds__(256) emit_segments_kernel(EmitCtx E, const int* __restrict__ count) {
-  const long long nb = min((long long)*count, E.base_cap);
+  const long long nb = E.nvirt + min((long long)*count, E.base_cap);
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1006,7 +1008,7 @@ __global__ void __launch_bounds__(256) emit_segments_kernel(EmitCtx E, const int
         if (c[q].rem <= 0) {
           const long long my = next + __popc(idle & lt);
           if (my < r1) {
-            seg_start(E, E.base_q[my], c[q]);
+            seg_start(E, my, c[q]);
           }
         }
         next += __popc(idle);

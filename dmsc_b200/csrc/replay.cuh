@@ -66,9 +66,6 @@ struct ReplayState {
 __device__ __forceinline__ longlong2 node_keylen_cg(const ReplayNode* n, int x) {
   return __ldcg(reinterpret_cast<const longlong2*>(&n[x].ctime));
 }
-__device__ __forceinline__ int4 node_words_cg(const ReplayNode* n, int x) {
-  return __ldcg(reinterpret_cast<const int4*>(&n[x].status));
-}
 __device__ __forceinline__ longlong2 node_keylen(const ReplayNode* n, int x) {
   return *reinterpret_cast<const longlong2*>(&n[x].ctime);
 }
@@ -76,15 +73,11 @@ __device__ __forceinline__ int4 node_words(const ReplayNode* n, int x) {
   return *reinterpret_cast<const int4*>(&n[x].status);
 }
 
-// Every node a root that is never cancelled, with tag 0 (a cancellation's
-// own key and kPending are set when the replay starts).
-__global__ void replay_node_init_kernel(ReplayNode* __restrict__ n, long long count) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  *reinterpret_cast<longlong2*>(&n[i].ctime) = make_longlong2((long long)kNever, 0);
-  *reinterpret_cast<int4*>(&n[i].status) = make_int4(kRootForever, -1, 0, 0);
-}
-
+// Node records are written only for the nodes a cancellation kills: the
+// replay sets their key and kPending when it starts, and their decision when
+// it is made. Every reader first checks the side's alive flags: an alive
+// extremum (no cancellation kills it) is a root forever and its record is
+// never read, so no pass initialises the records of the others.
 // Side word of a linked node: the dying side k (bit 0), the number of
 // non-empty chains of W(node) (bits 1-2) and of its raw-arc segments (bits
 // 3-4), so counting a chain's expansion reads one word per node.
@@ -97,11 +90,12 @@ __device__ __forceinline__ int bases_of(int w) { return (w >> 3) & 3; }
 // length; returns false when a node on the way is still undecided. Replay
 // steps are compared by their (persistence, saddle cell) keys, which are
 // unique, so no ranks are needed.
-__device__ __forceinline__ bool walk_root(const ReplayState& S, int x, unsigned long long t, int* root,
-                                          long long* acc, int max_steps, unsigned* status) {
+__device__ __forceinline__ bool walk_root(const ReplayState& S, const uint8_t* __restrict__ alive, int x,
+                                          unsigned long long t, int* root, long long* acc, int max_steps,
+                                          unsigned* status) {
   long long a = 0;
   int steps = 0;
-  while (x >= 0) {
+  while (x >= 0 && !alive[x]) {
     const longlong2 kl = node_keylen(S.node, x);
     const int4 w = node_words(S.node, x);
     if ((unsigned long long)kl.x >= t) break;
@@ -120,48 +114,15 @@ __device__ __forceinline__ bool walk_root(const ReplayState& S, int x, unsigned 
   return true;
 }
 
-// The same walk resumed from (*x, *acc) and left there: returns false, with
-// *x the first undecided node and *acc the length summed before it, when the
-// walk has to wait; the prefix already walked is final (decisions never
-// change), so a later round continues from that node.
-__device__ __forceinline__ bool walk_resume(const ReplayState& S, int* x_io, unsigned long long t, long long* acc_io,
-                                            int max_steps, unsigned* status, int round) {
-  int x = *x_io;
-  long long a = *acc_io;
-  int steps = 0;
-  bool done = true;
-  while (true) {
-    if (x < 0) break;
-    const longlong2 kl = node_keylen_cg(S.node, x);  // one sector: both halves issued together
-    const int4 w = node_words_cg(S.node, x);
-    if ((unsigned long long)kl.x >= t) break;
-    const int st = w.x;
-    if (status_kind(st) == kPending || (st >> 2) > round) {  // undecided, or decided in this round
-      done = false;
-      break;
-    }
-    if (status_kind(st) == kRootForever) break;
-    a += kl.y;
-    x = w.y;
-    if (++steps > max_steps) {
-      set_status(status, kStatusChainCap);
-      break;
-    }
-  }
-  *x_io = x;
-  *acc_io = a;
-  return done;
-}
-
 // Final arcs of the surviving saddles: length and the chain root of each
 // (survivor i in output order, arc j), from the survivors' gathered records
 // (image, arc ends, raw-arc lengths). Images whose output does not take this
 // side's arcs (`arcs_primal` / `arcs_dual` by orientation) get empty arcs.
 __global__ void final_arcs_kernel(int nsurv, const int2* __restrict__ surv_ic, const uint8_t* __restrict__ dual,
                                   bool arcs_primal, bool arcs_dual, const int2* __restrict__ sv_t,
-                                  const longlong2* __restrict__ sv_len, ReplayState S, int max_steps,
-                                  long long* __restrict__ arc_len, long long* __restrict__ arc_cl,
-                                  int* __restrict__ arc_root, unsigned* status) {
+                                  const longlong2* __restrict__ sv_len, const uint8_t* __restrict__ alive,
+                                  ReplayState S, int max_steps, long long* __restrict__ arc_len,
+                                  long long* __restrict__ arc_cl, int* __restrict__ arc_root, unsigned* status) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= 2 * nsurv) return;
   int i = q >> 1, j = q & 1;
@@ -174,9 +135,11 @@ __global__ void final_arcs_kernel(int nsurv, const int2* __restrict__ surv_ic, c
     return;
   }
   const longlong2 bl = sv_len[i];
-  int R;
-  long long a;
-  walk_root(S, T, kNever, &R, &a, max_steps, status);
+  // an extremum that no cancellation kills (alive) is its own final root;
+  // only the others walk their parent chains
+  int R = T;
+  long long a = 0;
+  if (!alive[T]) walk_root(S, alive, T, kNever, &R, &a, max_steps, status);
   arc_len[q] = (j ? bl.y : bl.x) + a;
   arc_cl[q] = a;
   arc_root[q] = R;
@@ -203,21 +166,21 @@ struct EmitCtx {
   int* out_primal;  // destination of primal images' arcs of this side
   int* out_dual;    // destination of dual images' arcs
   long long q_cap;
-  int4* base_q;  // raw-arc segments, written after the expansion
+  int4* base_q;  // raw-arc segments of the chain expansion
   long long base_cap;
+  // the survivors' own raw arcs (segment items 0 .. 2 nsurv - 1 of the
+  // writer, read from the survivor records instead of a task list)
+  int nvirt;                 // 2 nsurv
+  const int2* surv_ic;       // [nsurv] image and cell of each survivor (output order)
+  const int2* sv_t;          // [nsurv] this side's arc ends
+  const longlong2* sv_len;   // [nsurv] this side's raw-arc lengths
+  const long long* arc_pos;  // [2 nsurv] output position of each arc
   int max_steps;
   unsigned* status;
 };
 
-// Raw-arc segment tasks come in two forms. A direct task carries everything
-// its writer needs, {start index | 1 << 30 | reversed << 31, cells, output
-// position, image}; the start index is the global index of the arc's first
-// cell (its face or vertex next to the saddle, cpu/arcs_geometry.hxx:74-81,
-// 124-131). Indices stay below 2^29 and a side's geometry below 2^31 cells
-// (checked by the host). A saddle task {reversed << 2, saddle, arc, output
-// position} leaves the look-ups to the writer: the chain expansion emits
-// those, so its walks along parent chains wait on no extra loads.
-constexpr int kSegDirect = 1 << 30;
+// A raw-arc segment task of the chain expansion: {reversed << 2, saddle,
+// arc, output position}; its writer looks up the arc's start cell and length.
 __device__ __forceinline__ int arc_start_of_cell(const EmitCtx& E, int sc, int j, int b) {
   const int W = E.I.W[b], Nx = W + 1;
   const int cell = E.faces ? face_start(sc, j, Nx) : vertex_start(sc, j, E.I.H[b], W, Nx, E.I.idx_base[b]);
@@ -225,9 +188,6 @@ __device__ __forceinline__ int arc_start_of_cell(const EmitCtx& E, int sc, int j
 }
 __device__ __forceinline__ int arc_start_index(const EmitCtx& E, int s, int j, int b) {
   return arc_start_of_cell(E, E.crit_sad[s], j, b);
-}
-__device__ __forceinline__ int4 make_seg(int start, int rev, long long len, long long pos, int b) {
-  return make_int4(start | kSegDirect | (rev << 31), (int)len, (int)pos, b);
 }
 __device__ __forceinline__ int4 make_saddle_seg(int s, int j, int rev, long long pos) {
   return make_int4(rev << 2, s, j, (int)pos);
@@ -244,19 +204,27 @@ struct SegCursor {
   int idx, ibase, Nx;
 };
 
-// Starts the segment task t; rem = 0 when it writes nothing (its image's
+// Starts segment item q: q < nvirt is raw arc (q / 2, q % 2) of a survivor,
+// forward at its arc's output position; the others are the chain
+// expansion's tasks. rem = 0 when it writes nothing (no arc, or its image's
 // output does not take this side's arcs).
-__device__ __forceinline__ void seg_start(const EmitCtx& E, const int4 t, SegCursor& c) {
+__device__ __forceinline__ void seg_start(const EmitCtx& E, long long q, SegCursor& c) {
   c.rem = 0;
   int b, idx, len, pos;
   bool rev;
-  if (t.x & kSegDirect) {
-    b = t.w;
-    idx = t.x & (kSegDirect - 1);
-    len = t.y;
-    pos = t.z;
-    rev = (unsigned)t.x >> 31;
+  if (q < E.nvirt) {
+    const int i = (int)(q >> 1), j = (int)(q & 1);
+    const int2 tt = E.sv_t[i];
+    const longlong2 bl = E.sv_len[i];
+    len = (int)(j ? bl.y : bl.x);
+    if ((j ? tt.y : tt.x) < 0 || len <= 0) return;
+    const int2 ic = E.surv_ic[i];
+    b = ic.x;
+    idx = arc_start_of_cell(E, ic.y, j, b);
+    pos = (int)E.arc_pos[q];
+    rev = false;
   } else {
+    const int4 t = E.base_q[q - E.nvirt];
     const int s = t.y, j = t.z;
     len = (int)E.blen[2 * s + j];
     b = E.sad_img[s];

@@ -173,49 +173,6 @@ __device__ __forceinline__ int perim_slot(int r, int c) {
   return r == 0 ? c : r == kLT - 1 ? kLT + c : c == 0 ? 2 * kLT + r : 3 * kLT + r;
 }
 
-// Per tile: for each row and each of its two 32-cell segments, the bit mask
-// of the critical faces (maxima of the face side) and critical vertices, and
-// the segment's first rank in the batch-wide critical lists (the exclusive
-// scans of the compaction), so a critical cell's list rank is
-// off + popc(bits below it) and needs no index-sized map.
-struct TileRanks {
-  uint32_t fbits[kLT][2], vbits[kLT][2];
-  int foff[kLT][2], voff[kLT][2];
-};
-
-__device__ __forceinline__ void tile_ranks(const uint8_t (*fl)[kLT], const LabelTile& g, const Imgs& I,
-                                           const int* __restrict__ off_f, const int* __restrict__ off_v,
-                                           TileRanks& R) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int nsegx = (g.W + 32) / 32;  // 32-index row segments of the compaction: ceil((W + 1) / 32)
-  for (int rs = warp; rs < 2 * kLT; rs += nw) {
-    const int r = rs >> 1, sg = rs & 1;
-    const int y = g.y0 + r, x = g.x0 + sg * 32 + lane;
-    const unsigned code = fl[r][sg * 32 + lane];
-    const unsigned fb = __ballot_sync(0xffffffffu, y <= g.H && x <= g.W && ((code >> 4) & 7u) == kFlowNone);
-    const unsigned vb = __ballot_sync(0xffffffffu, y < g.H && x < g.W && (code & 7u) == kFlowNone);
-    if (lane == 0) {
-      R.fbits[r][sg] = fb;
-      R.vbits[r][sg] = vb;
-      const bool seg_in = y <= g.H && g.x0 + sg * 32 <= g.W;
-      const long long sid = (long long)I.seg_base[g.b] + (long long)y * nsegx + (g.x0 >> 5) + sg;
-      R.foff[r][sg] = (seg_in && off_f) ? __ldg(off_f + sid) : 0;
-      R.voff[r][sg] = (seg_in && off_v) ? __ldg(off_v + sid) : 0;
-    }
-  }
-}
-
-// Label of the critical cell at tile-local id j (FACES: a face of the face
-// side, else a vertex): lab[rank].
-template <bool FACES>
-__device__ __forceinline__ int tile_label(const TileRanks& R, int j, const int* __restrict__ lab) {
-  const int r = j / kLT, c = j % kLT, sg = c >> 5;
-  const uint32_t below = (1u << (c & 31)) - 1u;
-  const int rank = FACES ? R.foff[r][sg] + __popc(R.fbits[r][sg] & below)
-                         : R.voff[r][sg] + __popc(R.vbits[r][sg] & below);
-  return __ldg(lab + rank);
-}
-
 // In-tile resolution. Every (side, cell) of the tile has a 16-bit successor
 // and a 32-bit state. A terminal cell (critical, or whose successor lies
 // outside the tile) has successor kTerm | itself and a final state from the
@@ -241,45 +198,45 @@ __device__ __forceinline__ bool st_pending(uint32_t v) { return (v >> 30) == 1u;
 constexpr int kLabelShapes = 2;
 constexpr int kLabelNT[kLabelShapes] = {1024, 512};
 
-// Successor of the cell at tile position (r, c) (FACES: face side; the cell
-// is in the image) and, for a terminal cell, its final state.
-template <bool FACES>
-__device__ __forceinline__ uint16_t tile_step(const uint8_t (*fl)[kLT], const TileRanks& R,
-                                              const int* __restrict__ lab, int r, int c, int tile, int ntx,
-                                              uint32_t* final_state) {
-  const unsigned code = ((unsigned)fl[r][c] >> (FACES ? 4 : 0)) & 7u;
+// Successor set-up of one (row, 32-cell segment) item of a tile for both
+// sides, one lane per cell: a critical cell (terminal) takes the state
+// (label << 1) | 1 of its extremum, lab[rank], where rank is the segment's
+// first rank in the batch-wide critical list (the compaction's exclusive
+// scan) plus the critical cells before it in the segment (a ballot); a cell
+// whose successor lies in another tile (terminal) takes the border-map entry
+// of that cell; any other cell gets its successor's tile-local id. Cells
+// outside the image are terminal and never reached. `labf` / `labv`: the
+// labels loaded for this lane's critical cells (issued for a group of a
+// warp's items before any is used).
+__device__ __forceinline__ void tile_cell_setup(const uint8_t (*fl)[kLT], const LabelTile& g, int tile, int ntx,
+                                                int r, int c, bool do_f, bool do_v, bool critf, bool critv,
+                                                int labf, int labv, uint16_t (*succ)[kLTN], uint32_t (*st)[kLTN]) {
   const int i = r * kLT + c;
-  if (code == kFlowNone) {
-    *final_state = ((uint32_t)tile_label<FACES>(R, i, lab) << 1) | 1u;
-    return (uint16_t)(kTerm | i);
+  const unsigned code = fl[r][c];
+  const int y = g.y0 + r, x = g.x0 + c;
+#pragma unroll
+  for (int sd = 0; sd < 2; ++sd) {
+    const bool in = sd == 0 ? (do_f && y <= g.H && x <= g.W) : (do_v && y < g.H && x < g.W);
+    const unsigned k = sd == 0 ? (code >> 4) & 7u : code & 7u;
+    uint16_t sc = (uint16_t)(kTerm | i);
+    uint32_t state = 1u;
+    if (in) {
+      if (sd == 0 ? critf : critv) {
+        state = ((uint32_t)(sd == 0 ? labf : labv) << 1) | 1u;
+      } else {
+        const int dc = (k == kFlowRight) - (k == kFlowLeft), dr = (k == kFlowDown) - (k == kFlowUp);
+        const int nr = r + dr, nc = c + dc;
+        if ((unsigned)nr < (unsigned)kLT && (unsigned)nc < (unsigned)kLT) {
+          sc = (uint16_t)(nr * kLT + nc);
+        } else {  // enters the neighbouring tile at its border cell (nr, nc) mod 64
+          const int nt = tile + dc + dr * ntx;
+          state = (uint32_t)(((long long)nt * kPerim + perim_slot(nr & (kLT - 1), nc & (kLT - 1))) << 1);
+        }
+      }
+    }
+    succ[sd][i] = sc;
+    if (sc & kTerm) st[sd][i] = state;
   }
-  int nr = r, nc = c, nt = tile;
-  if (code == kFlowLeft) {
-    if (--nc < 0) {
-      nt = tile - 1;
-      nc = kLT - 1;
-    }
-  } else if (code == kFlowRight) {
-    if (++nc == kLT) {
-      nt = tile + 1;
-      nc = 0;
-    }
-  } else if (code == kFlowUp) {
-    if (--nr < 0) {
-      nt = tile - ntx;
-      nr = kLT - 1;
-    }
-  } else {
-    if (++nr == kLT) {
-      nt = tile + ntx;
-      nr = 0;
-    }
-  }
-  if (nt != tile) {
-    *final_state = (uint32_t)(((long long)nt * kPerim + perim_slot(nr, nc)) << 1);
-    return (uint16_t)(kTerm | i);
-  }
-  return (uint16_t)(nr * kLT + nc);
 }
 
 // Follows border-map entries to a label.
@@ -311,7 +268,6 @@ struct LabelSmem {
   uint32_t st[2][kLTN];
   uint16_t succ[2][kLTN];
   uint8_t fl[kLT][kLT];
-  TileRanks R;
 };
 
 template <int NT>
@@ -324,37 +280,64 @@ __global__ void __launch_bounds__(NT, 2048 / NT) label_tile_kernel(Imgs I, const
   uint8_t (*fl)[kLT] = SM.fl;
   uint16_t (*succ)[kLTN] = SM.succ;
   uint32_t (*st)[kLTN] = SM.st;
-  TileRanks& R = SM.R;
   constexpr int kTileCells = kLTN / NT, kStep = NT / kLT;
+  constexpr int NW = NT / 32, kItems = 2 * kLT / NW;  // (row, segment) items per warp
   const LabelTile g = label_tile_of(I, blockIdx.x);
   const bool d = I.dual[g.b];
   int* of = d ? OF.dual : OF.primal;
   int* ov = d ? OV.dual : OV.primal;
   if (of) of += (d ? OF.dual_off : OF.primal_off)[g.b];
   if (ov) ov += (d ? OV.dual_off : OV.primal_off)[g.b];
-  load_flow_tile(flow, g, fl, threadIdx.x, blockDim.x);
-  __syncthreads();
-  tile_ranks(fl, g, I, F.off, V.off, R);
-  __syncthreads();
-  const int c = threadIdx.x % kLT, rb = threadIdx.x / kLT;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int ntx = label_ntx(g);
   const bool do_f = F.perim != nullptr, do_v = V.perim != nullptr;
-  // successors; terminal cells get their final state (cells outside the
-  // image are terminal and never reached)
+  // the first ranks of this warp's items: lane k loads item k's (issued
+  // before the flow tile is waited for)
+  int offf = 0, offv = 0;
+  if (lane < kItems) {
+    const int rs = warp + NW * lane, r = rs >> 1, sg = rs & 1;
+    const int y = g.y0 + r;
+    if (y <= g.H && g.x0 + sg * 32 <= g.W) {
+      const int nsegx = (g.W + 32) / 32;  // 32-index row segments of the compaction: ceil((W + 1) / 32)
+      const long long sid = (long long)I.seg_base[g.b] + (long long)y * nsegx + (g.x0 >> 5) + sg;
+      if (do_f && F.off) offf = __ldg(F.off + sid);
+      if (do_v && V.off) offv = __ldg(V.off + sid);
+    }
+  }
+  load_flow_tile(flow, g, fl, threadIdx.x, blockDim.x);
+  __syncthreads();
+  {  // successors and terminal states, one warp per (row, segment) item, in
+     // groups of 4 items whose label loads are issued together
+    const unsigned lt = (1u << lane) - 1u;
+    constexpr int kGroup = kItems < 4 ? kItems : 4;
 #pragma unroll
-  for (int k = 0; k < kTileCells; ++k) {
-    const int r = rb + kStep * k, i = r * kLT + c;
-    const int y = g.y0 + r, x = g.x0 + c;
-    uint32_t a = 1u, b = 1u;
-    uint16_t sa = (uint16_t)(kTerm | i), sb = sa;
-    if (do_f && y <= g.H && x <= g.W) sa = tile_step<true>(fl, R, F.lab, r, c, blockIdx.x, ntx, &a);
-    if (do_v && y < g.H && x < g.W) sb = tile_step<false>(fl, R, V.lab, r, c, blockIdx.x, ntx, &b);
-    succ[0][i] = sa;
-    succ[1][i] = sb;
-    if (sa & kTerm) st[0][i] = a;
-    if (sb & kTerm) st[1][i] = b;
+    for (int k0 = 0; k0 < kItems; k0 += kGroup) {
+      int labf[kGroup], labv[kGroup];
+      unsigned cf = 0, cv = 0;  // bit k: this lane's cell of item k0 + k is critical
+#pragma unroll
+      for (int k = 0; k < kGroup; ++k) {  // ranks and label loads of the critical cells
+        const int rs = warp + NW * (k0 + k), r = rs >> 1, c = (rs & 1) * 32 + lane;
+        const int y = g.y0 + r, x = g.x0 + c;
+        const unsigned code = fl[r][c];
+        const bool fcrit = do_f && y <= g.H && x <= g.W && ((code >> 4) & 7u) == kFlowNone;
+        const bool vcrit = do_v && y < g.H && x < g.W && (code & 7u) == kFlowNone;
+        const unsigned fb = __ballot_sync(0xffffffffu, fcrit), vb = __ballot_sync(0xffffffffu, vcrit);
+        const int of0 = __shfl_sync(0xffffffffu, offf, k0 + k), ov0 = __shfl_sync(0xffffffffu, offv, k0 + k);
+        labf[k] = fcrit ? __ldg(F.lab + of0 + __popc(fb & lt)) : 0;
+        labv[k] = vcrit ? __ldg(V.lab + ov0 + __popc(vb & lt)) : 0;
+        cf |= (unsigned)fcrit << k;
+        cv |= (unsigned)vcrit << k;
+      }
+#pragma unroll
+      for (int k = 0; k < kGroup; ++k) {
+        const int rs = warp + NW * (k0 + k);
+        tile_cell_setup(fl, g, blockIdx.x, ntx, rs >> 1, (rs & 1) * 32 + lane, do_f, do_v, (cf >> k) & 1u,
+                        (cv >> k) & 1u, labf[k], labv[k], succ, st);
+      }
+    }
   }
   __syncthreads();
+  const int c = threadIdx.x % kLT, rb = threadIdx.x / kLT;
   // short walks to the terminal cell; bit 2k + side of `pend`: still walking
   unsigned pend = 0;
 #pragma unroll
@@ -394,41 +377,57 @@ __global__ void __launch_bounds__(NT, 2048 / NT) label_tile_kernel(Imgs I, const
       }
     }
   }
-  // this thread's own states are final now (read back from shared memory)
+  // this thread's own states are final now (read back from shared memory):
+  // labels of paths that end in the tile, border-map entries of the border
+  // cells, and a bit per cell whose path leaves the tile on a side whose
+  // labels this image outputs (bit 2k: faces, 2k + 1: vertices); those are
+  // reserved in the exit lists at once and written afterwards
   const bool border_c = c == 0 || c == kLT - 1;
-  // cells of this thread whose path leaves the tile, on a side whose labels
-  // this image outputs: bit 2k (faces) and 2k + 1 (vertices); all of them are
-  // reserved in the exit lists at once
+  const int x = g.x0 + c;
+  const bool fx = do_f && x <= g.W, vx = do_v && x < g.W;
   unsigned xm = 0;
+  {
+    int* ofr = of ? of + (g.y0 + rb) * g.Nx + x : nullptr;  // image-local outputs stay below 2^31
+    int* ovr = ov ? ov + (g.y0 + rb) * g.W + x : nullptr;
 #pragma unroll
-  for (int k = 0; k < kTileCells; ++k) {
-    const int y = g.y0 + rb + kStep * k, x = g.x0 + c;
-    const int i = (rb + kStep * k) * kLT + c;
-    if (do_f && of && y <= g.H && x <= g.W && !(st[0][i] & 1u)) xm |= 1u << (2 * k);
-    if (do_v && ov && y < g.H && x < g.W && !(st[1][i] & 1u)) xm |= 2u << (2 * k);
+    for (int k = 0; k < kTileCells; ++k) {
+      const int r = rb + kStep * k, y = g.y0 + r, i = r * kLT + c;
+      const bool border = border_c || r == 0 || r == kLT - 1;
+      if (fx && y <= g.H) {
+        // odd: (label << 1) | 1 of a path ending in the tile; even: exit entry
+        const uint32_t ef = st[0][i];
+        if (border) F.perim[blockIdx.x * kPerim + perim_slot(r, c)] = (int)ef;
+        if (ofr) {
+          if (ef & 1u)
+            ofr[k * kStep * g.Nx] = (int)ef >> 1;
+          else
+            xm |= 1u << (2 * k);
+        }
+      }
+      if (vx && y < g.H) {
+        const uint32_t ev = st[1][i];
+        if (border) V.perim[blockIdx.x * kPerim + perim_slot(r, c)] = (int)ev;
+        if (ovr) {
+          if (ev & 1u)
+            ovr[k * kStep * g.W] = (int)ev >> 1;
+          else
+            xm |= 2u << (2 * k);
+        }
+      }
+    }
   }
   int pf, pv;
   block_reserve2(n_exits + 0, __popc(xm & 0x55555555u), n_exits + 1, __popc(xm & 0xAAAAAAAAu), pf, pv);
-#pragma unroll
-  for (int k = 0; k < kTileCells; ++k) {
+  while (xm) {  // the few cells whose paths leave the tile
+    const int q = __ffs(xm) - 1, k = q >> 1, sd = q & 1;
+    xm &= xm - 1u;
     const int r = rb + kStep * k;
-    const int y = g.y0 + r, x = g.x0 + c;
-    const long long gidx = g.base + (long long)r * g.Nx + c;
-    const bool border = border_c || r == 0 || r == kLT - 1;
-    const long long po = (long long)blockIdx.x * kPerim + perim_slot(r, c);
-    if (do_f && y <= g.H && x <= g.W) {
-      // odd: (label << 1) | 1 of a path ending in the tile; even: exit entry
-      const int ef = (int)st[0][r * kLT + c];
-      if (border) F.perim[po] = ef;
-      if (of && (ef & 1)) of[(long long)y * g.Nx + x] = ef >> 1;
-      if ((xm >> (2 * k)) & 1u) exits_f[pf++] = make_int2((int)gidx, ef);
-    }
-    if (do_v && y < g.H && x < g.W) {
-      const int ev = (int)st[1][r * kLT + c];
-      if (border) V.perim[po] = ev;
-      if (ov && (ev & 1)) ov[(long long)y * g.W + x] = ev >> 1;
-      if ((xm >> (2 * k + 1)) & 1u) exits_v[pv++] = make_int2((int)gidx, ev);
-    }
+    const int gidx = (int)(g.base + (long long)r * g.Nx + c);  // global indices stay below 2^29
+    const int e = (int)st[sd][r * kLT + c];
+    if (sd == 0)
+      exits_f[pf++] = make_int2(gidx, e);
+    else
+      exits_v[pv++] = make_int2(gidx, e);
   }
 }
 

@@ -6,7 +6,9 @@ Tunables (``dmsc_b200_set_tuning`` in include/dmsc_b200.h), none of which
 changes an output bit:
 
 * ``grad_shape``: gradient tile of 32 index columns x 31, 63 or 127 rows
-  (how much of the value window and its halo row each CTA stages);
+  (how much of the value window and its halo row each CTA stages), or the
+  persistent kernel whose tile windows are staged by tensor-memory copies
+  (63 or 127 rows);
 * ``label_shape``: 64 x 64 label tiles on 1024 or 512 threads (4 or 8 cells
   per thread in the barrier-free pointer jumping);
 * ``pair_shape``: pairing items each thread advances together (2 or 4,

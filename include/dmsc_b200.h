@@ -192,9 +192,12 @@ const char* dmsc_b200_last_error(const dmsc_b200_context* ctx);
    and returns the number of stages: 0 set-up (workspace clears, table
    upload), 1 gradient (the kernel alone), 2 compaction, 3 saddle walks,
    4 pairing (both sides), 5 persistence, cancellation and output ranks,
-   6 survivors (in sweep order), 7 replay (both sides), 8 final arcs, 9 label
+   6 survivors (flags and counts), 7 replay (both sides), 8 final arcs, 9 label
    set-up (per-extremum labels, bases), 10 labels (the label kernels alone),
-   11 sizes, 12 fetch lists, 13 fetch geometry. */
+   11 sizes, 12 fetch lists, 13 fetch geometry. The survivors' sweep order
+   and records are computed on a second stream while the replay and the
+   labels run (the labels run before the final arcs); the final-arcs stage
+   includes the wait for them. */
 int dmsc_b200_set_profiling(dmsc_b200_context* ctx, int enable);
 int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n);
 
@@ -211,9 +214,10 @@ int dmsc_b200_loop_counts(dmsc_b200_context* ctx, int* out, int n);
    blocks of 64 slots: pairing round starts (faces, vertices), geometry
    expansion level starts (faces, vertices), then replay round starts (faces,
    vertices); then six more blocks in the same order with each round's item
-   count (active saddles, queued chain tasks, pending cancellations). Unused
-   slots are 0. Writes up to `n` (at most 768) values to `out` (host
-   pointer), returns the number written. */
+   count (active saddles, queued chain tasks, pending cancellations); then
+   the pairing's phase-B start times (faces, vertices). Unused slots are 0.
+   Writes up to `n` (at most 896) values to `out` (host pointer), returns the
+   number written. */
 int dmsc_b200_pairing_timeline(dmsc_b200_context* ctx, long long* out, int n);
 
 /* Failure handling (no counterpart in the reference). Every device loop of
@@ -235,8 +239,12 @@ int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_
    and cpu/cell_groups.hxx:9 CACHE_DEPTH). They change speed only, never an
    output bit. The Python tuner (dmsc_b200.tuning) sweeps them on the
    caller's data and sets the fastest per image-size class.
-   grad_shape   : gradient tile of 32 index columns x {31, 63, 127} rows
-                  (threads {256, 256, 512}), 0..2; default 2.
+   grad_shape   : gradient tile of 32 index columns x {31, 63, 127, 63, 127}
+                  rows (threads {256, 256, 512, 256, 512}), 0..4; shapes 3
+                  and 4 stage the value windows with tensor-memory copies in a
+                  persistent kernel (one image whose width is a multiple of 4
+                  in a 16-byte aligned buffer; others run shapes 1 and 2);
+                  default 2.
    label_shape  : 64 x 64 label tiles with {1024, 512} threads, 0..1; default 1.
    *_blocks_per_sm : resident blocks per SM of the pairing, replay and
                   geometry-expansion persistent kernels; 0 = as many as fit
