@@ -381,6 +381,8 @@ def b200_arm(args):
     grad_ms = stage_sum.get("gradient", 0.0) / args.steps
     achieved = grad_bytes / (grad_ms / 1000.0) / 1e9 if grad_ms > 0 else None
     traffic = ncu_traffic("gradient_kernel", size)
+    # shapes 3 and 4 run the TMA-staged persistent kernel on one image
+    grad_kernel = "gradient_tma_kernel" if ctx.get_tuning().grad_shape >= 3 else "gradient_batch_kernel"
     # segmentation (basins + peaks) kernels
     seg_bytes = 8.0 * (size + 1) ** 2 + 4.0 * size * size + 4.0 * (size + 1) ** 2
     lab_ms = stage_sum.get("labels", 0.0) / args.steps
@@ -393,7 +395,7 @@ def b200_arm(args):
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h // args.steps,
                 "timing": "host wall clock around K public-API calls from pinned host memory, max over ranks"},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "gradient_batch_kernel", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": grad_kernel, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "algorithmic_bytes": grad_bytes, "avg_ms": grad_ms,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"

@@ -169,7 +169,7 @@ struct dmsc_b200_context {
   // tuned launch shapes (dmsc_b200_set_tuning): gradient tile shape (index
   // into kGradTY / kGradNT), label tile threads (index into kLabelNT), and
   // the resident blocks per SM of the three persistent kernels (0 = all that fit)
-  int grad_shape = 2;
+  int grad_shape = 3;
   int label_shape = 1;
   int pair_per_sm = 0, replay_per_sm = 0, emit_per_sm = 0;
   int pair_shape = 0;    // pairing items per thread batch: 0 -> 2, 1 -> 4

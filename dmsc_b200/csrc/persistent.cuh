@@ -91,6 +91,13 @@ __device__ __forceinline__ void chunk_start(ChunkLists& L) {
 }
 
 __device__ __forceinline__ void chunk_keep(ChunkLists& L, int side, int v) { L.buf[side][atomicAdd(&L.n[side], 1)] = v; }
+// the same, counting only (no list is written)
+__device__ __forceinline__ void chunk_count(ChunkLists& L, int side) { atomicAdd(&L.n[side], 1); }
+__device__ __forceinline__ void chunk_flush_count(ChunkLists& L, int* cnt0, int* cnt1) {
+  __syncthreads();
+  if (threadIdx.x < 2 && L.n[threadIdx.x] > 0) atomicAdd(threadIdx.x == 0 ? cnt0 : cnt1, L.n[threadIdx.x]);
+  __syncthreads();
+}
 
 __device__ __forceinline__ void chunk_flush(ChunkLists& L, int* cnt0, int* out0, int* cnt1, int* out1) {
   const int t = threadIdx.x;
@@ -136,14 +143,15 @@ struct PairArgs {
 // Both sides' persistence pairing in one cooperative launch; each round
 // processes both sides' active saddles and live roots, so the two sides share
 // their grid barriers. Per round and side: (A) every active saddle finds its
-// ends' groups, cycles are decided, the rest reduce their sweep index into
-// both groups' minimum (no returned value needed) and stay active; (B1) every
+// ends' groups, cycles are decided, the rest reduce their sweep key into
+// both groups' minimum (no returned value needed) and stay active; (B) every
 // live root with an outgoing saddle decides whether it dies there, and a
-// root that dies links itself under the other group's root at once (phase B1
+// root that dies links itself under the other group's root at once (phase B
 // reads no link, and the next reader is the next round's phase A, behind the
 // round's barrier); the others stay live; roots without outgoing saddles
-// leave the list for good. Round 0 skips the lookups: all groups are single
-// extrema. A side whose active list is empty just idles.
+// leave for good. Round 0 skips the lookups: all groups are single extrema.
+// The first rounds scan every saddle and group instead of reading lists (see
+// the round loop). A side with no active saddle just idles.
 struct PairArgs2 {
   PairArgs s[2];
 };
@@ -161,12 +169,12 @@ constexpr int kPairShapes = 2;
 #define PSIDE(f) (s1 ? P.s[1].f : P.s[0].f)
 
 // Phase A for the thread's items i0 + 256 u (u < U) below cend: side 0's
-// items come first (i < n0). Round 0 takes every saddle and keeps no list:
-// round 1 takes every saddle again and skips the decided ones. Later rounds
-// read the active list.
+// items come first (i < n0). In a scan the items are the saddles themselves
+// (the decided ones are skipped), else the active list; the saddles that stay
+// active are appended to the next list (`lists`) or only counted.
 template <int U>
 __device__ __forceinline__ void pair_batch_a(const PairArgs2& P, int r, long long i0, long long cend, int n0,
-                                             ChunkLists& L) {
+                                             bool scan, bool lists, ChunkLists& L) {
   int e[U], ga[U], gb[U];
   float sv[U];
   unsigned act = 0, s1m = 0, du = 0;
@@ -179,7 +187,7 @@ __device__ __forceinline__ void pair_batch_a(const PairArgs2& P, int r, long lon
       const long long j = s1 ? i - n0 : i;
       act |= 1u << u;
       s1m |= (unsigned)s1 << u;
-      e[u] = r <= 1 ? (int)j : ((r & 1) ? PSIDE(act1) : PSIDE(act0))[j];
+      e[u] = scan ? (int)j : ((r & 1) ? PSIDE(act1) : PSIDE(act0))[j];
     }
   }
   // the saddle's state, ends and key value, all issued together
@@ -266,18 +274,22 @@ __device__ __forceinline__ void pair_batch_a(const PairArgs2& P, int r, long lon
     const unsigned long long k = sweep_key(sv[u], e[u], (du >> u) & 1u);
     atomicMin(PSIDE(minedge) + ga[u], k);  // result unused: a reduction
     atomicMin(PSIDE(minedge) + gb[u], k);
-    if (r > 0) chunk_keep(L, s1, e[u]);
+    if (lists)
+      chunk_keep(L, s1, e[u]);
+    else
+      chunk_count(L, s1);
   }
 }
 
 // Phase B for the thread's live roots k0 + 256 u (u < U) below cend (side 0's
-// first, k < nr0; round 0 takes every group, in index order): each root with
-// an outgoing saddle decides there and a dying root links itself under the
-// other group's root; the void never dies; roots without outgoing saddles
-// leave the list.
+// first, k < nr0; in a scan every group, in index order, and the groups
+// without an outgoing saddle are skipped): each root with an outgoing saddle
+// decides there and a dying root links itself under the other group's root;
+// the void never dies; roots without outgoing saddles leave for good. The
+// roots that stay live are listed when `lists` is set.
 template <int U>
 __device__ __forceinline__ void pair_batch_b(const PairArgs2& P, int r, long long k0, long long cend, int nr0,
-                                             ChunkLists& L) {
+                                             bool scan, bool lists, ChunkLists& L) {
   int g[U];
   unsigned act = 0, s1m = 0;
 #pragma unroll
@@ -289,7 +301,7 @@ __device__ __forceinline__ void pair_batch_b(const PairArgs2& P, int r, long lon
       const long long j = s1 ? k - nr0 : k;
       act |= 1u << u;
       s1m |= (unsigned)s1 << u;
-      g[u] = r == 0 ? (int)j : ((r & 1) ? PSIDE(roots1) : PSIDE(roots0))[j];
+      g[u] = scan ? (int)j : ((r & 1) ? PSIDE(roots1) : PSIDE(roots0))[j];
     }
   }
   unsigned long long me[U];
@@ -316,7 +328,7 @@ __device__ __forceinline__ void pair_batch_b(const PairArgs2& P, int r, long lon
     }
     PSIDE(minedge)[g[u]] = kNoEdge;
     if (g[u] == PSIDE(M)) {  // the void is older than every group: it never dies
-      chunk_keep(L, s1, g[u]);
+      if (lists) chunk_keep(L, s1, g[u]);
       act &= ~(1u << u);
       continue;
     }
@@ -357,7 +369,7 @@ __device__ __forceinline__ void pair_batch_b(const PairArgs2& P, int r, long lon
     if (dies) {
       PSIDE(dying)[e[u]] = g[u];
       PSIDE(link)[g[u]] = h[u];
-    } else {
+    } else if (lists) {
       chunk_keep(L, s1, g[u]);
     }
   }
@@ -376,9 +388,9 @@ __global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2
       A.minedge[i] = kNoEdge;
     }
     for (long long i = tid; i < A.nsad; i += nth) A.dying[i] = kUndecided;
-    if (tid == 0) {  // rounds 0 and 1 take every saddle, round 0 every group
+    if (tid == 0) {
       A.cnt[0] = A.nsad;
-      A.cnt[1] = A.nsad;
+      A.cnt[1] = 0;
       A.cnt[2] = 0;
       A.cnt[3] = A.M + 1;
       A.cnt[4] = 0;
@@ -387,11 +399,20 @@ __global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2
   }
   grid.sync();
   bool done0 = false, done1 = false, solo = false;
+  // While many saddles are active, a round scans every saddle (skipping the
+  // decided ones) and every group (skipping those without an outgoing
+  // saddle) instead of reading lists: a scan is a coalesced read, and no
+  // round spends its barriers and stores on writing lists that would hold
+  // most items anyway. The round in which the active saddles drop to an
+  // eighth of all saddles still scans but writes the lists, and the later
+  // rounds read them.
+  bool scan = true;
   for (int r = 0;; ++r) {
     const int n0 = *(volatile int*)(P.s[0].cnt + r % 3), n1 = *(volatile int*)(P.s[1].cnt + r % 3);
     // a side whose active list is empty is finished: its roots are not visited
-    const int nr0 = n0 ? *(volatile int*)(P.s[0].cnt + 3 + r % 3) : 0;
-    const int nr1 = n1 ? *(volatile int*)(P.s[1].cnt + 3 + r % 3) : 0;
+    const int nr0 = n0 && !scan ? *(volatile int*)(P.s[0].cnt + 3 + r % 3) : 0;
+    const int nr1 = n1 && !scan ? *(volatile int*)(P.s[1].cnt + 3 + r % 3) : 0;
+    const bool lists = !scan || 8LL * ((long long)n0 + n1) <= (long long)P.s[0].nsad + P.s[1].nsad;
     if (tid == 0) {
       for (int sd = 0; sd < 2; ++sd) {
         const PairArgs& A = P.s[sd];
@@ -406,7 +427,7 @@ __global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2
       }
     }
     if (n0 == 0 && n1 == 0) break;
-    if (!solo && (long long)n0 + n1 + nr0 + nr1 <= kPairSoloItems) {
+    if (!solo && !scan && (long long)n0 + n1 + nr0 + nr1 <= kPairSoloItems) {
       solo = true;
       if (blockIdx.x != 0) break;
     }
@@ -428,18 +449,20 @@ __global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2
         P.s[sd].cnt[3 + (r + 2) % 3] = 0;
       }
     }
-    // phase A over both sides' active saddles (round 0 keeps no list)
+    // phase A over both sides' active saddles (or every saddle in a scan)
     {
-      const long long n = (long long)n0 + n1, chunk = chunk_size(n, nblk);
-      const bool lists = r > 0;
+      const int na0 = scan ? P.s[0].nsad : n0, na1 = scan ? P.s[1].nsad : n1;
+      const long long n = (long long)na0 + na1, chunk = chunk_size(n, nblk);
       for (long long c0 = (long long)bid * chunk; c0 < n; c0 += (long long)nblk * chunk) {
-        if (lists) chunk_start(L);
+        chunk_start(L);
         const long long cend = min(n, c0 + chunk);
         for (long long i0 = c0 + threadIdx.x; i0 < cend; i0 += 256LL * U)
-          pair_batch_a<U>(P, r, i0, cend, n0, L);
+          pair_batch_a<U>(P, r, i0, cend, na0, scan, lists, L);
         if (lists)
           chunk_flush(L, P.s[0].cnt + (r + 1) % 3, (r & 1) ? P.s[0].act0 : P.s[0].act1, P.s[1].cnt + (r + 1) % 3,
                       (r & 1) ? P.s[1].act0 : P.s[1].act1);
+        else
+          chunk_flush_count(L, P.s[0].cnt + (r + 1) % 3, P.s[1].cnt + (r + 1) % 3);
       }
     }
     if (solo)
@@ -449,18 +472,22 @@ __global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2
     if (tid == 0 && r < kTimeline)  // side sd's phase-B starts: block 12 + sd
       for (int sd = 0; sd < 2; ++sd)
         if (P.s[sd].timeline) P.s[sd].timeline[kTimelinePhaseB + r] = global_ns();
-    // phase B: live roots decide on their first outgoing saddle
+    // phase B: live roots (or every group in a scan) decide on their first
+    // outgoing saddle
     {
-      const long long n = (long long)nr0 + nr1, chunk = chunk_size(n, nblk);
+      const int nb0 = scan ? P.s[0].M + 1 : nr0, nb1 = scan ? P.s[1].M + 1 : nr1;
+      const long long n = (long long)nb0 + nb1, chunk = chunk_size(n, nblk);
       for (long long c0 = (long long)bid * chunk; c0 < n; c0 += (long long)nblk * chunk) {
-        chunk_start(L);
+        if (lists) chunk_start(L);
         const long long cend = min(n, c0 + chunk);
         for (long long k0 = c0 + threadIdx.x; k0 < cend; k0 += 256LL * U)
-          pair_batch_b<U>(P, r, k0, cend, nr0, L);
-        chunk_flush(L, P.s[0].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[0].roots0 : P.s[0].roots1,
-                    P.s[1].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[1].roots0 : P.s[1].roots1);
+          pair_batch_b<U>(P, r, k0, cend, nb0, scan, lists, L);
+        if (lists)
+          chunk_flush(L, P.s[0].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[0].roots0 : P.s[0].roots1,
+                      P.s[1].cnt + 3 + (r + 1) % 3, (r & 1) ? P.s[1].roots0 : P.s[1].roots1);
       }
     }
+    scan = scan && !lists;
     if (solo)
       __syncthreads();
     else
@@ -634,7 +661,11 @@ __device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long 
     ReplayNode* node = RSIDE(S.node);
     if (k >= 0) {
       const longlong2 bl = *reinterpret_cast<const longlong2*>(RSIDE(blen) + 2 * s);
+      const int2 tt = *reinterpret_cast<const int2*>(RSIDE(t) + 2 * s);
       *reinterpret_cast<longlong2*>(&node[dd].cl_dy) = make_longlong2(k == 0 ? a0 : a1, k == 0 ? a1 : a0);
+      *reinterpret_cast<int4*>(&node[dd].t_dy) =
+          make_int4(k == 0 ? tt.x : tt.y, k == 0 ? tt.y : tt.x, (int)(k == 0 ? bl.x : bl.y),
+                    (int)(k == 0 ? bl.y : bl.x));
       node[dd].wlen = bl.x + bl.y + a0 + a1;
       // status, parent, the dying side with what W(d) expands to (its
       // non-empty chains and raw-arc segments), and the saddle, in one store;
@@ -850,45 +881,38 @@ __device__ __forceinline__ void emit_batch(const EmitCtx& E, int4* __restrict__ 
   for (int u = 0; u < U; ++u)
     if (((act >> u) & 1u) && z[u] != stop[u] && z[u] >= 0) live |= 1u << u;
   while (live) {
-    int4 w[U];
+    int4 w[U], te[U];  // (status, parent, side, saddle), (arc ends, raw-arc lengths)
     long long wl[U];
     longlong2 cl[U];
 #pragma unroll
     for (int u = 0; u < U; ++u)
-      if ((live >> u) & 1u) {
+      if ((live >> u) & 1u) {  // the node's two sectors, issued together
+        const ReplayNode* nd = E.S.node + z[u];
         w[u] = node_words(E.S.node, z[u]);
-        wl[u] = E.S.node[z[u]].wlen;
-        cl[u] = *reinterpret_cast<const longlong2*>(&E.S.node[z[u]].cl_dy);
-      }
-    int2 tt[U];
-    longlong2 bl[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      if ((live >> u) & 1u) {
-        const int s = w[u].w;
-        tt[u] = *reinterpret_cast<const int2*>(E.t + 2 * s);
-        bl[u] = *reinterpret_cast<const longlong2*>(E.blen + 2 * s);
+        wl[u] = nd->wlen;
+        cl[u] = *reinterpret_cast<const longlong2*>(&nd->cl_dy);
+        te[u] = *reinterpret_cast<const int4*>(&nd->t_dy);
       }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (!((live >> u) & 1u)) continue;
       // W(z) = reverse(chain(Tk -> z)) + reverse(arc k) + arc o + chain(To -> R)
       const int d = z[u], k = side_of(w[u].z), s = w[u].w, R = w[u].y;
-      const int Tk = k ? tt[u].y : tt[u].x, To = k ? tt[u].x : tt[u].y;
-      const long long la = cl[u].x, lb = k ? bl[u].y : bl[u].x, lc = k ? bl[u].x : bl[u].y, ld = cl[u].y;
+      const int Tk = te[u].x, To = te[u].y;
+      const long long la = cl[u].x, lb = te[u].z, lc = te[u].w, ld = cl[u].y;
       const bool rv = (rev >> u) & 1u;
       const long long at = rv ? pos[u] + tot[u] - off[u] - wl[u] : pos[u] + off[u];
       int& q = pc[u];
       int& qb = pbc[u];
       if (!rv) {
         if (la > 0) q_out[q++] = make_task(kTaskChain, 1, Tk, d, at);
-        if (lb > 0) E.base_q[qb++] = make_saddle_seg(s, k, 1, at + la);
-        if (lc > 0) E.base_q[qb++] = make_saddle_seg(s, 1 - k, 0, at + la + lb);
+        if (lb > 0) E.base_q[qb++] = make_saddle_seg(s, k, 1, lb, at + la);
+        if (lc > 0) E.base_q[qb++] = make_saddle_seg(s, 1 - k, 0, lc, at + la + lb);
         if (ld > 0) q_out[q++] = make_task(kTaskChain, 0, To, R, at + la + lb + lc);
       } else {
         if (ld > 0) q_out[q++] = make_task(kTaskChain, 1, To, R, at);
-        if (lc > 0) E.base_q[qb++] = make_saddle_seg(s, 1 - k, 1, at + ld);
-        if (lb > 0) E.base_q[qb++] = make_saddle_seg(s, k, 0, at + ld + lc);
+        if (lc > 0) E.base_q[qb++] = make_saddle_seg(s, 1 - k, 1, lc, at + ld);
+        if (lb > 0) E.base_q[qb++] = make_saddle_seg(s, k, 0, lb, at + ld + lc);
         if (la > 0) q_out[q++] = make_task(kTaskChain, 0, Tk, d, at + ld + lc + lb);
       }
       off[u] += wl[u];
@@ -930,13 +954,17 @@ __global__ void __launch_bounds__(256, MINB) emit_persistent_kernel(EmitArgs A) 
       push = true;
       task = make_task(kTaskChain, 0, j ? tt.y : tt.x, A.arc_root[q], E.arc_pos[q] + (j ? bl.y : bl.x));
     }
-    int p, pb;
-    block_reserve2(A.cnt, push ? 1 : 0, n_base, 0, p, pb);
-    if (push) {
-      if (p < E.q_cap)
-        A.q0[p] = task;
-      else
-        set_status(E.status, kStatusQueueOverflow);
+    // most arcs have no chain (at threshold 0 nearly all): a block reserves
+    // queue slots only when one of its threads has a task
+    if (__syncthreads_or(push)) {
+      int p, pb;
+      block_reserve2(A.cnt, push ? 1 : 0, n_base, 0, p, pb);
+      if (push) {
+        if (p < E.q_cap)
+          A.q0[p] = task;
+        else
+          set_status(E.status, kStatusQueueOverflow);
+      }
     }
   }
   grid.sync();
@@ -983,7 +1011,7 @@ __global__ void __launch_bounds__(256, MINB) emit_persistent_kernel(EmitArgs A) 
 // cursors whose flow-code loads are issued together, so a lane waits on NC
 // independent dependent-load chains at once instead of one.
 constexpr int kSegRange = 256;
-constexpr int kSegSteps = 8;
+constexpr int kSegSteps = 4;
 constexpr int kSegCursorShapes = 2;  // NC = 1 or 2 (tuned)
 
 template <int NC>

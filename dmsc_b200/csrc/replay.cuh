@@ -44,7 +44,10 @@ __device__ __forceinline__ int status_word(int kind, int round) { return kind | 
 
 // A replay node in one 64-byte line: everything a chain walk reads, in the
 // first 32-byte sector as two 16-byte halves, (ctime, wlen) and (status,
-// parent, side, csad); the two chain lengths the emission adds in the second.
+// parent, side, csad); in the second, what the emission needs to expand
+// W(node) without touching the saddle's arrays: the two chain lengths, the
+// saddle's arc ends on the dying and the other side and their raw-arc
+// lengths (written at link time).
 struct alignas(64) ReplayNode {
   unsigned long long ctime;  // replay key of the cancellation killing the node, kNever if none
   long long wlen;            // length of W(node)
@@ -54,8 +57,10 @@ struct alignas(64) ReplayNode {
   int csad;                  // saddle of the node's cancellation
   long long cl_dy;           // chain length T_dying -> node at link time
   long long cl_ot;           // chain length T_other -> parent at link time
-  long long pad[2];
+  int t_dy, t_ot;            // the saddle's arc ends on the dying and the other side
+  int len_dy, len_ot;        // their raw-arc lengths (cells; a side's geometry stays below 2^31)
 };
+static_assert(sizeof(ReplayNode) == 64, "one 64-byte line per node");
 
 struct ReplayState {
   ReplayNode* node;  // [M + 1]
@@ -179,8 +184,8 @@ struct EmitCtx {
   unsigned* status;
 };
 
-// A raw-arc segment task of the chain expansion: {reversed << 2, saddle,
-// arc, output position}; its writer looks up the arc's start cell and length.
+// A raw-arc segment task of the chain expansion: {reversed | arc << 1,
+// saddle, cells, output position}; its writer looks up the arc's start cell.
 __device__ __forceinline__ int arc_start_of_cell(const EmitCtx& E, int sc, int j, int b) {
   const int W = E.I.W[b], Nx = W + 1;
   const int cell = E.faces ? face_start(sc, j, Nx) : vertex_start(sc, j, E.I.H[b], W, Nx, E.I.idx_base[b]);
@@ -189,8 +194,8 @@ __device__ __forceinline__ int arc_start_of_cell(const EmitCtx& E, int sc, int j
 __device__ __forceinline__ int arc_start_index(const EmitCtx& E, int s, int j, int b) {
   return arc_start_of_cell(E, E.crit_sad[s], j, b);
 }
-__device__ __forceinline__ int4 make_saddle_seg(int s, int j, int rev, long long pos) {
-  return make_int4(rev << 2, s, j, (int)pos);
+__device__ __forceinline__ int4 make_saddle_seg(int s, int j, int rev, long long len, long long pos) {
+  return make_int4(rev | (j << 1), s, (int)len, (int)pos);
 }
 
 // A raw arc being written by one lane: the V-path from its start cell, `len`
@@ -225,12 +230,12 @@ __device__ __forceinline__ void seg_start(const EmitCtx& E, long long q, SegCurs
     rev = false;
   } else {
     const int4 t = E.base_q[q - E.nvirt];
-    const int s = t.y, j = t.z;
-    len = (int)E.blen[2 * s + j];
+    const int s = t.y, j = (t.x >> 1) & 1;
+    len = t.z;
     b = E.sad_img[s];
     idx = len > 0 ? arc_start_index(E, s, j, b) : 0;
     pos = t.w;
-    rev = (t.x >> 2) & 1;
+    rev = t.x & 1;
   }
   int* out = E.I.dual[b] ? E.out_dual : E.out_primal;
   if (!out || len <= 0) return;

@@ -60,7 +60,7 @@ _tuning = threading.local()  # set while tune() runs on this thread
 
 
 def _default_tuning() -> dict:
-    return {"grad_shape": 2, "label_shape": 1, "pair_shape": 0, "pair_blocks_per_sm": 0, "replay_shape": 0,
+    return {"grad_shape": 3, "label_shape": 1, "pair_shape": 0, "pair_blocks_per_sm": 0, "replay_shape": 0,
             "replay_blocks_per_sm": 0, "emit_shape": 0,
             "emit_blocks_per_sm": 0, "seg_cursors": 1}
 

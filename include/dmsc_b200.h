@@ -244,7 +244,7 @@ int dmsc_b200_set_loop_caps(dmsc_b200_context* ctx, int pair_rounds, int replay_
                   and 4 stage the value windows with tensor-memory copies in a
                   persistent kernel (one image whose width is a multiple of 4
                   in a 16-byte aligned buffer; others run shapes 1 and 2);
-                  default 2.
+                  default 3.
    label_shape  : 64 x 64 label tiles with {1024, 512} threads, 0..1; default 1.
    *_blocks_per_sm : resident blocks per SM of the pairing, replay and
                   geometry-expansion persistent kernels; 0 = as many as fit
