@@ -46,9 +46,9 @@ enum Slot {
 };
 enum SideSlot {
   X_ROUT, X_SVT, X_SVL, X_SVR, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
-  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_UT, X_CKEY, X_CVAL, X_NODE,
+  X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_CKEY, X_CVAL, X_NODE,
   X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
-  X_GBASE, X_LAB, X_WX, X_WA, X_CENDS, kSideSlots
+  X_GBASE, X_WX, X_WA, X_CENDS, kSideSlots
 };
 
 struct Buf {
@@ -88,7 +88,6 @@ struct Side {
   uint8_t* alive = nullptr;
   int* to_out_excl = nullptr;
   int* to_out = nullptr;
-  int* ut = nullptr;
   long long* blen = nullptr;
   ReplayState R{};
   int C = 0;
@@ -517,24 +516,23 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   // pass when this side's arcs are simplified
   unsigned long long* ckey = S.arcs ? sget<unsigned long long>(ctx, si, X_CKEY, nsad) : nullptr;
   int* cval = S.arcs ? sget<int>(ctx, si, X_CVAL, nsad) : nullptr;
+  ReplayNode* node = S.arcs ? sget<ReplayNode>(ctx, si, X_NODE, M + 1) : nullptr;
   if (nsad > 0) {
     LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(
         nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.dying, get<float>(ctx, S_SVAL, nsad), S.val,
         S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.t, cends, ctx->crit_sad, ckey,
-        cval));
+        cval, node));
     LAUNCH_CHECK("persistence_kernel");
   }
   // thresholded union-find roots
   int* uf = sget<int>(ctx, si, X_UF, M + 1);
   int* croot = sget<int>(ctx, si, X_CROOT, M + 1);
-  S.ut = sget<int>(ctx, si, X_UT, M + 1);
   LK(iota_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(uf, M + 1));
   if (nsad > 0)
     LK(ut_union_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(cends, ncanc, M, uf, M + 2, ctx->status));
   LK(ut_flatten_kernel<<<grid_for((M + 1 + kUtBatch - 1) / kUtBatch, TB), TB, 0, st>>>(M + 1, uf, M + 2,
                                                                                        ctx->status));
   LK(ut_mark_kernel<<<grid_for(M + 1, TB), TB, 0, st>>>(M, uf, S.alive, croot));
-  if (M > 0) LK(ut_root_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.ut));
   LAUNCH_CHECK("thresholded union-find");
   // batch-wide output rank of alive extrema
   int* alive_i = sget<int>(ctx, si, X_ALIVEI, M + 1);
@@ -547,7 +545,7 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
     LAUNCH_CHECK("to_out_kernel");
   }
   S.rout = sget<int>(ctx, si, X_ROUT, M + 1);
-  if (M > 0) LK(root_out_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, S.ut, S.to_out, S.rout));
+  if (M > 0) LK(root_out_kernel<<<grid_for(M, TB), TB, 0, st>>>(M, uf, croot, S.to_out, S.rout));
   LAUNCH_CHECK("root_out_kernel");
 }
 
@@ -1037,13 +1035,10 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
       O.dual_off = d_peaks_off;
     }
     LabelSide& L = S.faces ? LF : LV;
-    int* lab = sget<int>(ctx, si, X_LAB, S.M + 1);
     L.off = S.faces ? off[2] : off[0];
-    L.lab = lab;
+    L.rout = S.rout;
+    L.abase = BS.alive[si];
     L.perim = get<int>(ctx, S.faces ? S_PERF : S_PERV, (size_t)nltile * kPerim);
-    if (S.M > 0)
-      LK(label_map_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.ext_img, S.rout, BS.alive[si], lab));
-    LAUNCH_CHECK("label_map_kernel");
   }
   int* nex = get<int>(ctx, S_NEX, 2);
   CK(cudaMemsetAsync(nex, 0, 2 * sizeof(int), st));

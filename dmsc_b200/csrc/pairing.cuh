@@ -26,6 +26,7 @@
 #include <cuda/atomic>
 
 #include "common.cuh"
+#include "replay.cuh"
 
 namespace dmsc {
 
@@ -81,7 +82,7 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
                                                           int2* __restrict__ canc_ends,
                                                           const int* __restrict__ crit_sad,
                                                           unsigned long long* __restrict__ ckey,
-                                                          int* __restrict__ cval) {
+                                                          int* __restrict__ cval, ReplayNode* __restrict__ node) {
   // saddles in list order: every per-saddle access is sequential
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   bool canc = false;
@@ -117,8 +118,14 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
   if (canc) {
     canc_ends[slot] = make_int2(t[2 * s], t[2 * s + 1]);
     if (ckey) {
-      ckey[slot] = ((unsigned long long)orderable_key(pers[s]) << 32) | (unsigned)crit_sad[s];
+      const unsigned long long key = ((unsigned long long)orderable_key(pers[s]) << 32) | (unsigned)crit_sad[s];
+      ckey[slot] = key;
       cval[slot] = s;
+      // the killed extremum's replay record: its cancellation key, undecided
+      // (the other records are never read, see replay.cuh)
+      const int d = pair_dense[s];
+      node[d].ctime = key;
+      node[d].status = kPending;
     }
   }
 }
@@ -220,21 +227,15 @@ __global__ void ut_mark_kernel(int n_ext, const int* __restrict__ p, const uint8
     comp_root[p[x]] = x;
 }
 
-// Out rank of each extremum's thresholded root (-1: the void's component);
-// a root is alive, so it always has one.
-__global__ void root_out_kernel(int n_ext, const int* __restrict__ ut, const int* __restrict__ to_out,
-                                int* __restrict__ rout) {
+// Out rank of each extremum's thresholded root: the component's alive
+// member (comp_root of its flattened union-find root; -1 for the void's
+// component), which always has an out rank.
+__global__ void root_out_kernel(int n_ext, const int* __restrict__ p, const int* __restrict__ comp_root,
+                                const int* __restrict__ to_out, int* __restrict__ rout) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= n_ext) return;
-  const int u = ut[x];
+  const int u = comp_root[p[x]];
   rout[x] = u >= 0 ? to_out[u] : -1;
-}
-
-__global__ void ut_root_kernel(int n_ext, const int* __restrict__ p, const int* __restrict__ comp_root,
-                               int* __restrict__ ut) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= n_ext) return;
-  ut[x] = comp_root[p[x]];
 }
 
 }  // namespace dmsc

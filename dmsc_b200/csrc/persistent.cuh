@@ -150,7 +150,7 @@ struct PairArgs {
 // reads no link, and the next reader is the next round's phase A, behind the
 // round's barrier); the others stay live; roots without outgoing saddles
 // leave for good. Round 0 skips the lookups: all groups are single extrema.
-// The first rounds scan every saddle and group instead of reading lists (see
+// Rounds 0 and 1 scan every saddle and group instead of reading lists (see
 // the round loop). A side with no active saddle just idles.
 struct PairArgs2 {
   PairArgs s[2];
@@ -399,20 +399,19 @@ __global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2
   }
   grid.sync();
   bool done0 = false, done1 = false, solo = false;
-  // While many saddles are active, a round scans every saddle (skipping the
-  // decided ones) and every group (skipping those without an outgoing
-  // saddle) instead of reading lists: a scan is a coalesced read, and no
-  // round spends its barriers and stores on writing lists that would hold
-  // most items anyway. The round in which the active saddles drop to an
-  // eighth of all saddles still scans but writes the lists, and the later
-  // rounds read them.
+  // Round 0 takes every saddle and group and keeps no list (nearly all stay
+  // active); round 1 scans every saddle (skipping the decided ones) and every
+  // group (skipping those without an outgoing saddle) and writes the lists
+  // that the later rounds read. Scanning all items in later rounds too, while
+  // many are active, measured slower (1.58 against 1.28 ms at 4096^2: the
+  // decided items still cost their loads).
   bool scan = true;
   for (int r = 0;; ++r) {
     const int n0 = *(volatile int*)(P.s[0].cnt + r % 3), n1 = *(volatile int*)(P.s[1].cnt + r % 3);
     // a side whose active list is empty is finished: its roots are not visited
     const int nr0 = n0 && !scan ? *(volatile int*)(P.s[0].cnt + 3 + r % 3) : 0;
     const int nr1 = n1 && !scan ? *(volatile int*)(P.s[1].cnt + 3 + r % 3) : 0;
-    const bool lists = !scan || 8LL * ((long long)n0 + n1) <= (long long)P.s[0].nsad + P.s[1].nsad;
+    const bool lists = !scan || r >= 1;
     if (tid == 0) {
       for (int sd = 0; sd < 2; ++sd) {
         const PairArgs& A = P.s[sd];
@@ -703,13 +702,9 @@ __global__ void __launch_bounds__(256, MINB) replay_persistent_kernel(ReplayArgs
     const ReplayArgs& A = P.s[sd];
     if (!A.n_cancel) continue;
     const int C = *A.n_cancel;
-    // the killed nodes' keys; round 0 takes every cancellation with its
-    // walks starting at the saddle's arc ends (no list or walk state yet)
-    for (long long r = tid; r < C; r += nth) {
-      const int d = A.dying[A.cj[r]];
-      A.S.node[d].ctime = A.key[r];
-      A.S.node[d].status = kPending;
-    }
+    // the killed nodes' records hold their keys (written by the persistence
+    // pass); round 0 takes every cancellation with its walks starting at the
+    // saddle's arc ends (no list or walk state yet)
     if (tid == 0) {
       A.cnt[0] = C;
       A.cnt[1] = 0;
@@ -1010,7 +1005,7 @@ __global__ void __launch_bounds__(256, MINB) emit_persistent_kernel(EmitArgs A) 
 // idle cursors by ballot (warp-local, no atomics). Each lane drives NC
 // cursors whose flow-code loads are issued together, so a lane waits on NC
 // independent dependent-load chains at once instead of one.
-constexpr int kSegRange = 256;
+constexpr int kSegRange = 128;
 constexpr int kSegSteps = 4;
 constexpr int kSegCursorShapes = 2;  // NC = 1 or 2 (tuned)
 

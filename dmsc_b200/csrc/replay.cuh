@@ -79,8 +79,8 @@ __device__ __forceinline__ int4 node_words(const ReplayNode* n, int x) {
 }
 
 // Node records are written only for the nodes a cancellation kills: the
-// replay sets their key and kPending when it starts, and their decision when
-// it is made. Every reader first checks the side's alive flags: an alive
+// persistence pass sets their key and kPending, and the replay their decision
+// when it is made. Every reader first checks the side's alive flags: an alive
 // extremum (no cancellation kills it) is a root forever and its record is
 // never read, so no pass initialises the records of the others.
 // Side word of a linked node: the dying side k (bit 0), the number of

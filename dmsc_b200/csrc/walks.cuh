@@ -105,17 +105,6 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
   }
 }
 
-// Label of every extremum (batch-wide rank r): the rank among its image's
-// surviving extrema of its thresholded union-find root, or -1 when the root is
-// the void (cpu/cell_groups.hxx:128-146, 168-173). `alive_base[b]` is the
-// first output rank of image b's extrema.
-__global__ void label_map_kernel(int M, const int* __restrict__ ext_img, const int* __restrict__ rout,
-                                 const int* __restrict__ alive_base, int* __restrict__ lab) {
-  int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= M) return;
-  const int o = rout[r];  // batch-wide out rank of the root (-1: the void)
-  lab[r] = o < 0 ? -1 : o - alive_base[ext_img[r]];
-}
 
 // Where the labels of one side go: image b's block of the output array picked
 // by its orientation (faces are peaks in the primal, basins in the dual).
@@ -250,10 +239,16 @@ __device__ __forceinline__ int entry_label(int e, const int* __restrict__ perim,
 }
 
 struct LabelSide {
-  const int* off;  // segment offsets of this side's critical list (exclusive scan)
-  const int* lab;  // label per critical extremum (batch-wide rank)
-  int* perim;      // border map (nullptr: side not labelled)
+  const int* off;    // segment offsets of this side's critical list (exclusive scan)
+  const int* rout;   // per critical extremum (batch-wide rank): out rank of its thresholded root, -1 for the void
+  const int* abase;  // [B + 1] first out rank of each image's alive extrema
+  int* perim;        // border map (nullptr: side not labelled)
 };
+
+// Label of an extremum from its root's batch-wide out rank: the root's rank
+// among its image's surviving extrema, -1 for the void
+// (cpu/cell_groups.hxx:128-146, 168-173).
+__device__ __forceinline__ int region_label(int rout, int abase) { return rout < 0 ? -1 : rout - abase; }
 
 __device__ __forceinline__ int label_ntx(const LabelTile& g) { return (g.W + kLT) / kLT; }
 
@@ -294,6 +289,7 @@ __global__ void __launch_bounds__(NT, 2048 / NT) label_tile_kernel(Imgs I, const
   // the first ranks of this warp's items: lane k loads item k's (issued
   // before the flow tile is waited for)
   int offf = 0, offv = 0;
+  const int abf = do_f ? __ldg(F.abase + g.b) : 0, abv = do_v ? __ldg(V.abase + g.b) : 0;
   if (lane < kItems) {
     const int rs = warp + NW * lane, r = rs >> 1, sg = rs & 1;
     const int y = g.y0 + r;
@@ -323,8 +319,8 @@ __global__ void __launch_bounds__(NT, 2048 / NT) label_tile_kernel(Imgs I, const
         const bool vcrit = do_v && y < g.H && x < g.W && (code & 7u) == kFlowNone;
         const unsigned fb = __ballot_sync(0xffffffffu, fcrit), vb = __ballot_sync(0xffffffffu, vcrit);
         const int of0 = __shfl_sync(0xffffffffu, offf, k0 + k), ov0 = __shfl_sync(0xffffffffu, offv, k0 + k);
-        labf[k] = fcrit ? __ldg(F.lab + of0 + __popc(fb & lt)) : 0;
-        labv[k] = vcrit ? __ldg(V.lab + ov0 + __popc(vb & lt)) : 0;
+        labf[k] = fcrit ? region_label(__ldg(F.rout + of0 + __popc(fb & lt)), abf) : 0;
+        labv[k] = vcrit ? region_label(__ldg(V.rout + ov0 + __popc(vb & lt)), abv) : 0;
         cf |= (unsigned)fcrit << k;
         cv |= (unsigned)vcrit << k;
       }
