@@ -568,6 +568,7 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   A.t = S.t;
   A.blen = S.blen;
   A.alive = S.alive;
+  A.crit_sad = ctx->crit_sad;
   A.S = R;
   A.max_steps = nsad + 1;
   A.act0 = sget<int>(ctx, si, X_ACT0, nsad);
@@ -1189,12 +1190,8 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   EmitArgs A;
   EmitCtx& E = A.E;
   E.flow = ctx->flow;
-  E.crit_sad = ctx->crit_sad;
   E.I = ctx->I;
-  E.sad_img = ctx->sad_img;
   E.faces = S.faces;
-  E.t = S.t;
-  E.blen = S.blen;
   E.S = S.R;
   E.out_primal = flat_primal;
   E.out_dual = flat_dual;

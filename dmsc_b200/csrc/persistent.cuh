@@ -505,6 +505,7 @@ struct ReplayArgs {
   const int* t;      // [2 nsad] extremum ends of each saddle, list order
   const long long* blen;
   const uint8_t* alive;  // [M] extrema that no cancellation kills (their records are never read)
+  const int* crit_sad;   // [nsad] global cell id of each saddle
   ReplayState S;
   int max_steps;
   int* act0;
@@ -672,7 +673,7 @@ __device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long 
       // this round's tag, so the order of these stores does not matter
       *reinterpret_cast<int4*>(&node[dd].status) =
           make_int4(status_word(kLinked, rd), k == 0 ? R1 : R0,
-                    side_word(k, (a0 > 0) + (a1 > 0), (bl.x > 0) + (bl.y > 0)), s);
+                    side_word(k, (a0 > 0) + (a1 > 0), (bl.x > 0) + (bl.y > 0)), RSIDE(crit_sad)[s]);
     } else {
       node[dd].status = status_word(kRootForever, rd);
     }
@@ -892,7 +893,7 @@ __device__ __forceinline__ void emit_batch(const EmitCtx& E, int4* __restrict__ 
     for (int u = 0; u < U; ++u) {
       if (!((live >> u) & 1u)) continue;
       // W(z) = reverse(chain(Tk -> z)) + reverse(arc k) + arc o + chain(To -> R)
-      const int d = z[u], k = side_of(w[u].z), s = w[u].w, R = w[u].y;
+      const int d = z[u], k = side_of(w[u].z), s = w[u].w, R = w[u].y;  // s: the saddle's cell
       const int Tk = te[u].x, To = te[u].y;
       const long long la = cl[u].x, lb = te[u].z, lc = te[u].w, ld = cl[u].y;
       const bool rv = (rev >> u) & 1u;

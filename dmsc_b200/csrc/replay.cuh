@@ -44,7 +44,7 @@ __device__ __forceinline__ int status_word(int kind, int round) { return kind | 
 
 // A replay node in one 64-byte line: everything a chain walk reads, in the
 // first 32-byte sector as two 16-byte halves, (ctime, wlen) and (status,
-// parent, side, csad); in the second, what the emission needs to expand
+// parent, side, saddle cell); in the second, what the emission needs to expand
 // W(node) without touching the saddle's arrays: the two chain lengths, the
 // saddle's arc ends on the dying and the other side and their raw-arc
 // lengths (written at link time).
@@ -54,7 +54,7 @@ struct alignas(64) ReplayNode {
   int status;                // kPending / kLinked / kRootForever, with the deciding round's tag
   int parent;                // link target (-1 = void) when kLinked
   int side;                  // side_word: dying side of the node's cancellation and what W(node) expands to
-  int csad;                  // saddle of the node's cancellation
+  int scell;                 // global cell id of the saddle of the node's cancellation
   long long cl_dy;           // chain length T_dying -> node at link time
   long long cl_ot;           // chain length T_other -> parent at link time
   int t_dy, t_ot;            // the saddle's arc ends on the dying and the other side
@@ -161,12 +161,8 @@ __device__ __forceinline__ int4 make_task(int kind, int rev, int a, int b, long 
 
 struct EmitCtx {
   const uint8_t* flow;
-  const int* crit_sad;
   Imgs I;
-  const int* sad_img;
   bool faces;
-  const int* t;            // per arc target
-  const long long* blen;   // per arc length
   ReplayState S;
   int* out_primal;  // destination of primal images' arcs of this side
   int* out_dual;    // destination of dual images' arcs
@@ -185,17 +181,15 @@ struct EmitCtx {
 };
 
 // A raw-arc segment task of the chain expansion: {reversed | arc << 1,
-// saddle, cells, output position}; its writer looks up the arc's start cell.
+// saddle cell, cells, output position}: the writer finds the arc's start
+// cell from the saddle's cell with no further load.
 __device__ __forceinline__ int arc_start_of_cell(const EmitCtx& E, int sc, int j, int b) {
   const int W = E.I.W[b], Nx = W + 1;
   const int cell = E.faces ? face_start(sc, j, Nx) : vertex_start(sc, j, E.I.H[b], W, Nx, E.I.idx_base[b]);
   return cell >> 2;
 }
-__device__ __forceinline__ int arc_start_index(const EmitCtx& E, int s, int j, int b) {
-  return arc_start_of_cell(E, E.crit_sad[s], j, b);
-}
-__device__ __forceinline__ int4 make_saddle_seg(int s, int j, int rev, long long len, long long pos) {
-  return make_int4(rev | (j << 1), s, (int)len, (int)pos);
+__device__ __forceinline__ int4 make_saddle_seg(int scell, int j, int rev, long long len, long long pos) {
+  return make_int4(rev | (j << 1), scell, (int)len, (int)pos);
 }
 
 // A raw arc being written by one lane: the V-path from its start cell, `len`
@@ -230,10 +224,10 @@ __device__ __forceinline__ void seg_start(const EmitCtx& E, long long q, SegCurs
     rev = false;
   } else {
     const int4 t = E.base_q[q - E.nvirt];
-    const int s = t.y, j = (t.x >> 1) & 1;
+    const int j = (t.x >> 1) & 1;
     len = t.z;
-    b = E.sad_img[s];
-    idx = len > 0 ? arc_start_index(E, s, j, b) : 0;
+    b = find_image(E.I.idx_base, E.I.B, t.y >> 2);
+    idx = arc_start_of_cell(E, t.y, j, b);
     pos = t.w;
     rev = t.x & 1;
   }
