@@ -117,6 +117,24 @@ struct Imgs {
   const float* thr;
 };
 
+// The persistence pairing's starting state, written by the kernels that
+// produce its inputs instead of a pass of its own: the ordered compaction
+// sets every group's union-find link (itself) and smallest outgoing key
+// (none) as it lists the extrema, plus the void slots and the round
+// counters; the saddle walks then run the first round's saddle phase as they
+// find each arc's end (see pairing.cuh). Side 0 is the face side (maxima),
+// side 1 the vertex side (minima).
+struct PairStart {
+  int nsad;
+  int M[2];                        // extrema of each side; the void is group M
+  unsigned long long* minedge[2];  // [M + 1] smallest sweep key of each group's outgoing saddles
+  int* link[2];                    // [M + 1] group union-find
+  int* cnt[2];                     // [6] rotating active-saddle and live-root counters
+  int2* g12[2];                    // [nsad] groups of each saddle's two ends
+  int* dying[2];                   // [nsad] decision of each saddle
+  const float* sval;               // [nsad] saddle values
+};
+
 // Largest b with base[b] <= g (the image holding global item g).
 __device__ __forceinline__ int find_image(const int* __restrict__ base, int B, long long g) {
   int lo = 0, hi = B - 1;

@@ -467,7 +467,6 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const float* sval
   PairArgs A;
   A.nsad = nsad;
   A.M = M;
-  A.t = S.t;
   A.sval = sval;
   A.sad_img = ctx->sad_img;
   A.g12 = sget<int2>(ctx, si, X_G12, nsad);
@@ -841,9 +840,23 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   uint32_t* skey32 = B > 1 ? nullptr : get<uint32_t>(ctx, S_SKEY32, nsad);
   ctx->crit_sad = csad;
   ctx->sad_img = isad;
+  // the pairing's starting state (side 0: faces / maxima, side 1: vertices /
+  // minima), set up by the compaction and the saddle walks
+  PairStart ps;
+  ps.nsad = nsad;
+  ps.sval = sval;
+  for (int si = 0; si < 2; ++si) {
+    const int M = si ? nmin : nmax;
+    ps.M[si] = M;
+    ps.minedge[si] = sget<unsigned long long>(ctx, si, X_MINE, M + 1);
+    ps.link[si] = sget<int>(ctx, si, X_LINK, M + 1);
+    ps.cnt[si] = sget<int>(ctx, si, X_CNT, 8);
+    ps.g12[si] = sget<int2>(ctx, si, X_G12, nsad);
+    ps.dying[si] = sget<int>(ctx, si, X_DYING, nsad);
+  }
   LK(compact_kernel<<<grid_for(nseg, 8), 256, 0, st>>>(I, img, nseg, flow, off[0], off[1], off[2], cmin, csad, cmax,
                                                        imin, isad, imax, bmin, bmax, vmin, vmax, kmin, kmax, sval, skey,
-                                                       skey32));
+                                                       skey32, ps));
   LAUNCH_CHECK("compact_kernel");
   // per-image bases of the critical lists (B + 1 entries each)
   int* bases = get<int>(ctx, S_BASES, 9 * (size_t)(B + 1));
@@ -869,8 +882,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   long long* lv = get<long long>(ctx, S_LV, 2 * (size_t)nsad);
   if (nsad > 0) {
     LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(I, flow, nsad, csad, isad, off[2], bmax, off[0], bmin, tf,
-                                                             lf, tv, lv,
-                                                             ncells, ctx->status));
+                                                             lf, tv, lv, ncells, ps, ctx->status));
     LAUNCH_CHECK("saddle_walk_kernel");
   }
 

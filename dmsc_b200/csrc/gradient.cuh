@@ -716,7 +716,8 @@ __host__ __device__ __forceinline__ unsigned crit_bits(unsigned fl, bool vin) {
 // the extrema before it in the mask), the extremum values (also as (value,
 // cell) records for the elder comparisons of the pairing) and the saddle
 // values with their sort keys (image id above the orderable value, so one
-// sort orders every image).
+// sort orders every image); and the pairing's starting state of the groups
+// (PairStart).
 static __global__ void __launch_bounds__(256) compact_kernel(
     Imgs I, const float* __restrict__ img_all, long long nseg, const uint8_t* __restrict__ flow,
     const int* __restrict__ off_min, const int* __restrict__ off_sad, const int* __restrict__ off_max,
@@ -725,7 +726,7 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     uint32_t* __restrict__ max_bits,
     float* __restrict__ min_val, float* __restrict__ max_val, int2* __restrict__ min_key, int2* __restrict__ max_key,
     float* __restrict__ sad_val,
-    unsigned long long* __restrict__ sad_key, uint32_t* __restrict__ sad_key32) {
+    unsigned long long* __restrict__ sad_key, uint32_t* __restrict__ sad_key32, PairStart ps) {
   const int lane = threadIdx.x & 31;
   long long seg = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (seg >= nseg) return;
@@ -748,6 +749,20 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     min_bits[seg] = bmin;
     max_bits[seg] = bmax;
   }
+  if (seg == 0 && lane == 0) {  // the pairing's void groups and round counters
+#pragma unroll
+    for (int sd = 0; sd < 2; ++sd) {
+      ps.minedge[sd][ps.M[sd]] = ~0ull;
+      ps.link[sd][ps.M[sd]] = ps.M[sd];
+      int* c = ps.cnt[sd];
+      c[0] = ps.nsad;  // round 0 takes every saddle
+      c[1] = 0;        // the saddles still active after it (counted by the walks)
+      c[2] = 0;
+      c[3] = ps.M[sd] + 1;
+      c[4] = 0;
+      c[5] = 0;
+    }
+  }
   if ((bmin | bmax | bh | bv) == 0u) return;  // the whole warp leaves together
   const CellValues cv = dual ? warp_cell_values<true>(img, iy, ix, H, W, lane)
                              : warp_cell_values<false>(img, iy, ix, H, W, lane);
@@ -759,6 +774,8 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     min_img[q] = b;
     min_val[q] = cv.v;
     min_key[q] = make_int2(__float_as_int(cv.v), (int)(4 * gidx));
+    ps.minedge[1][q] = ~0ull;  // a single-extremum group without outgoing saddles yet
+    ps.link[1][q] = q;
   }
   if (m & 8u) {
     const int q = off_max[seg] + __popc(bmax & lt);
@@ -766,6 +783,8 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     max_img[q] = b;
     max_val[q] = cv.f;
     max_key[q] = make_int2(__float_as_int(cv.f), (int)(4 * gidx + 3));
+    ps.minedge[0][q] = ~0ull;
+    ps.link[0][q] = q;
   }
 #pragma unroll
   for (int t = 1; t <= 2; ++t) {

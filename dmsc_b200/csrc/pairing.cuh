@@ -61,6 +61,79 @@ __device__ __forceinline__ bool older(int a, int b, int void_id, const int2* __r
   return older_less ? tie_lt(va, ka.y, vb, kb.y) : tie_lt(vb, kb.y, va, ka.y);
 }
 
+// K4: per saddle, both face walks and the vertex walks. Writes per arc (2
+// per saddle and side) the dense target index (or -1) and the raw arc's cell
+// count; then runs the pairing's round-0 saddle phase for both sides (all
+// groups are still single extrema, so the ends are the groups): a saddle
+// whose two ends coincide is a cycle, the others record their ends' groups
+// and reduce their sweep key into both groups' minimum, and each block adds
+// the saddles that stay active to the side's round-1 counter.
+__global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t* __restrict__ flow, int nsad,
+                                                          const int* __restrict__ crit_sad,
+                                                          const int* __restrict__ sad_img,
+                                                          const int* __restrict__ off_max,
+                                                          const uint32_t* __restrict__ max_bits,
+                                                          const int* __restrict__ off_min,
+                                                          const uint32_t* __restrict__ min_bits, int* __restrict__ tf,
+                                                          long long* __restrict__ lf, int* __restrict__ tv,
+                                                          long long* __restrict__ lv, long long cap, PairStart ps,
+                                                          unsigned* status) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  int keep[2] = {0, 0};
+  if (s < nsad) {
+    const int b = sad_img[s];
+    const int H = I.H[b], W = I.W[b], Nx = W + 1;
+    const int sc = crit_sad[s];
+    int te[2][2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      long long steps;
+      const int end = flow_walk<4>(flow, face_start(sc, j, Nx) >> 2, Nx, cap, &steps, status);
+      const int target = seg_rank(I, b, end, Nx, off_max, max_bits);
+      tf[2 * s + j] = target;
+      lf[2 * s + j] = target >= 0 ? steps + 1 : 0;  // cells of the raw arc, start and end included
+      te[0][j] = target;
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int start = vertex_start(sc, j, H, W, Nx, I.idx_base[b]);
+      long long steps = 0;
+      int target = -1;
+      if (start >= 0) {
+        const int end = flow_walk<0>(flow, start >> 2, Nx, cap, &steps, status);
+        target = seg_rank(I, b, end, Nx, off_min, min_bits);
+      }
+      tv[2 * s + j] = target;
+      lv[2 * s + j] = target >= 0 ? steps + 1 : 0;  // an arc that leaves the image is empty
+      te[1][j] = target;
+    }
+    // round 0 of the pairing: descending sweep on the face side in the
+    // primal and the vertex side in the dual
+    const bool d = I.dual[b];
+    const float v = ps.sval[s];
+#pragma unroll
+    for (int sd = 0; sd < 2; ++sd) {
+      const int M = ps.M[sd];
+      const int ga = te[sd][0] < 0 ? M : te[sd][0], gb = te[sd][1] < 0 ? M : te[sd][1];
+      if (ga == gb) {
+        ps.dying[sd][s] = -1;
+        continue;
+      }
+      ps.dying[sd][s] = kUndecided;
+      ps.g12[sd][s] = make_int2(ga, gb);
+      const unsigned long long k = sweep_key(v, s, sd == 0 ? !d : d);
+      atomicMin(ps.minedge[sd] + ga, k);  // result unused: a reduction
+      atomicMin(ps.minedge[sd] + gb, k);
+      keep[sd] = 1;
+    }
+  }
+  const int c0 = __syncthreads_count(keep[0]), c1 = __syncthreads_count(keep[1]);
+  if (threadIdx.x == 0) {
+    if (c0) atomicAdd(ps.cnt[0] + 1, c0);
+    if (c1) atomicAdd(ps.cnt[1] + 1, c1);
+  }
+}
+
 __global__ void iota_kernel(int* __restrict__ a, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = i;

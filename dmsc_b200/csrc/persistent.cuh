@@ -117,7 +117,6 @@ struct PairArgs {
   // saddles are indexed in list order (ascending cell id); a saddle's sweep
   // key (sweep_key) orders the saddles of its image in this side's sweep
   // and is the atomicMin key, so no sorted copy of the saddles is needed
-  const int* t;       // [2 nsad] extremum ends of each saddle (-1: void)
   const float* sval;  // [nsad] saddle values
   const int* sad_img; // [nsad] image of each saddle
   int2* g12;          // [nsad] groups of the two ends, as of the saddle's last active round
@@ -149,9 +148,11 @@ struct PairArgs {
 // root that dies links itself under the other group's root at once (phase B
 // reads no link, and the next reader is the next round's phase A, behind the
 // round's barrier); the others stay live; roots without outgoing saddles
-// leave for good. Round 0 skips the lookups: all groups are single extrema.
-// Rounds 0 and 1 scan every saddle and group instead of reading lists (see
-// the round loop). A side with no active saddle just idles.
+// leave for good. Round 0's phase A runs in the saddle walks (all groups are
+// single extrema then, so it needs no lookups), which also leave the round
+// counters; the groups' union-find and minima are set up by the compaction
+// (PairStart). Rounds 0 and 1 scan every saddle and group instead of reading
+// lists (see the round loop). A side with no active saddle just idles.
 struct PairArgs2 {
   PairArgs s[2];
 };
@@ -198,22 +199,15 @@ __device__ __forceinline__ void pair_batch_a(const PairArgs2& P, int r, long lon
     ga[u] = gb[u] = 0;
     if (!((act >> u) & 1u)) continue;
     const bool s1 = (s1m >> u) & 1u;
-    const int M = PSIDE(M);
-    if (r == 0) {
-      const int2 ab = *reinterpret_cast<const int2*>(PSIDE(t) + 2 * e[u]);
-      ga[u] = ab.x < 0 ? M : ab.x;
-      gb[u] = ab.y < 0 ? M : ab.y;
-    } else {
-      dy[u] = PSIDE(dying)[e[u]];
-      const int2 g = PSIDE(g12)[e[u]];  // the ends' groups of the previous round
-      ga[u] = g.x;
-      gb[u] = g.y;
-    }
+    dy[u] = PSIDE(dying)[e[u]];
+    const int2 g = PSIDE(g12)[e[u]];  // the ends' groups of the previous round
+    ga[u] = g.x;
+    gb[u] = g.y;
   }
 #pragma unroll
   for (int u = 0; u < U; ++u)
     if (dy[u] != kUndecided) act &= ~(1u << u);
-  if (r > 0) {
+  {
     // the groups' current roots: path-halving finds of all 2U ends in lockstep
     unsigned live = 0;
 #pragma unroll
@@ -381,26 +375,10 @@ __global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2
   __shared__ ChunkLists L;
   cg::grid_group grid = cg::this_grid();
   const long long tid = grid.thread_rank(), nth = grid.size();
-  for (int sd = 0; sd < 2; ++sd) {
-    const PairArgs& A = P.s[sd];
-    for (long long i = tid; i <= A.M; i += nth) {
-      A.link[i] = (int)i;
-      A.minedge[i] = kNoEdge;
-    }
-    for (long long i = tid; i < A.nsad; i += nth) A.dying[i] = kUndecided;
-    if (tid == 0) {
-      A.cnt[0] = A.nsad;
-      A.cnt[1] = 0;
-      A.cnt[2] = 0;
-      A.cnt[3] = A.M + 1;
-      A.cnt[4] = 0;
-      A.cnt[5] = 0;
-    }
-  }
-  grid.sync();
   bool done0 = false, done1 = false, solo = false;
-  // Round 0 takes every saddle and group and keeps no list (nearly all stay
-  // active); round 1 scans every saddle (skipping the decided ones) and every
+  // Round 0 takes every group and keeps no list (nearly all stay live; its
+  // saddle phase ran in the saddle walks, which also counted the saddles
+  // that stay active); round 1 scans every saddle (skipping the decided ones) and every
   // group (skipping those without an outgoing saddle) and writes the lists
   // that the later rounds read. Scanning all items in later rounds too, while
   // many are active, measured slower (1.58 against 1.28 ms at 4096^2: the
@@ -448,8 +426,9 @@ __global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2
         P.s[sd].cnt[3 + (r + 2) % 3] = 0;
       }
     }
-    // phase A over both sides' active saddles (or every saddle in a scan)
-    {
+    // phase A over both sides' active saddles (or every saddle in a scan);
+    // round 0's ran in the saddle walks
+    if (r > 0) {
       const int na0 = scan ? P.s[0].nsad : n0, na1 = scan ? P.s[1].nsad : n1;
       const long long n = (long long)na0 + na1, chunk = chunk_size(n, nblk);
       for (long long c0 = (long long)bid * chunk; c0 < n; c0 += (long long)nblk * chunk) {
@@ -463,11 +442,11 @@ __global__ void __launch_bounds__(256, MINB) pairing_persistent_kernel(PairArgs2
         else
           chunk_flush_count(L, P.s[0].cnt + (r + 1) % 3, P.s[1].cnt + (r + 1) % 3);
       }
+      if (solo)
+        __syncthreads();
+      else
+        grid.sync();
     }
-    if (solo)
-      __syncthreads();
-    else
-      grid.sync();
     if (tid == 0 && r < kTimeline)  // side sd's phase-B starts: block 12 + sd
       for (int sd = 0; sd < 2; ++sd)
         if (P.s[sd].timeline) P.s[sd].timeline[kTimelinePhaseB + r] = global_ns();

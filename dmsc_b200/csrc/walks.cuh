@@ -67,45 +67,6 @@ __device__ __forceinline__ int seg_rank(const Imgs& I, int b, int g, int Nx, con
   return __ldg(off + seg) + __popc(__ldg(bits + seg) & ((1u << (x & 31)) - 1u));
 }
 
-// K4: per saddle, both face walks and the vertex walks. Writes per arc
-// (2 per saddle and side): dense target index (or -1) and step count.
-__global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t* __restrict__ flow, int nsad,
-                                                          const int* __restrict__ crit_sad,
-                                                          const int* __restrict__ sad_img,
-                                                          const int* __restrict__ off_max,
-                                                          const uint32_t* __restrict__ max_bits,
-                                                          const int* __restrict__ off_min,
-                                                          const uint32_t* __restrict__ min_bits, int* __restrict__ tf,
-                                                          long long* __restrict__ lf, int* __restrict__ tv,
-                                                          long long* __restrict__ lv, long long cap, unsigned* status) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsad) return;
-  const int b = sad_img[s];
-  const int H = I.H[b], W = I.W[b], Nx = W + 1;
-  int sc = crit_sad[s];
-#pragma unroll
-  for (int j = 0; j < 2; ++j) {
-    long long steps;
-    int end = flow_walk<4>(flow, face_start(sc, j, Nx) >> 2, Nx, cap, &steps, status);
-    const int target = seg_rank(I, b, end, Nx, off_max, max_bits);
-    tf[2 * s + j] = target;
-    lf[2 * s + j] = target >= 0 ? steps + 1 : 0;  // cells of the raw arc, start and end included
-  }
-#pragma unroll
-  for (int j = 0; j < 2; ++j) {
-    int start = vertex_start(sc, j, H, W, Nx, I.idx_base[b]);
-    long long steps = 0;
-    int target = -1;
-    if (start >= 0) {
-      int end = flow_walk<0>(flow, start >> 2, Nx, cap, &steps, status);
-      target = seg_rank(I, b, end, Nx, off_min, min_bits);
-    }
-    tv[2 * s + j] = target;
-    lv[2 * s + j] = target >= 0 ? steps + 1 : 0;  // an arc that leaves the image is empty
-  }
-}
-
-
 // Where the labels of one side go: image b's block of the output array picked
 // by its orientation (faces are peaks in the primal, basins in the dual).
 struct LabelOut {
