@@ -77,10 +77,13 @@ __global__ void survivor_gather_kernel(int nsad, const int* __restrict__ flag, c
 
 // Surviving saddles in the vertex side's sweep order (arcs_topology.hxx:99-102):
 // `sorted` lists them by ascending (image, s_val, cell id); an image whose
-// vertex side sweeps descending (dual) takes its range reversed.
+// vertex side sweeps descending (dual) takes its range reversed. Also
+// gathers each survivor's image and cell in output order (`ic`), so the
+// later per-survivor kernels read them in order.
 __global__ void survivor_order_kernel(int n, const int* __restrict__ sorted, const int* __restrict__ sad_img,
-                                      const uint8_t* __restrict__ dual, const int* __restrict__ surv_base,
-                                      int* __restrict__ surv) {
+                                      const int* __restrict__ crit_sad, const uint8_t* __restrict__ dual,
+                                      const int* __restrict__ surv_base, int* __restrict__ surv,
+                                      int2* __restrict__ ic) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const int s = sorted[p], b = sad_img[s];
@@ -90,22 +93,14 @@ __global__ void survivor_order_kernel(int n, const int* __restrict__ sorted, con
     q = base + cnt - 1 - (p - base);
   }
   surv[q] = s;
+  ic[q] = make_int2(b, crit_sad[s]);
 }
 
-// Per-survivor records gathered once in output (sweep) order, so the later
-// per-survivor kernels read them in order instead of gathering from the
-// list-ordered saddle arrays again: the image and cell of every survivor,
-// and per side its arc ends, raw-arc lengths and the record of its outputs
-// (out ranks of its ends' thresholded roots, persistence, out rank of its
-// pair's root; -1 for the void).
-__global__ void surv_common_kernel(int nsurv, const int* __restrict__ surv, const int* __restrict__ sad_img,
-                                   const int* __restrict__ crit_sad, int2* __restrict__ ic) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nsurv) return;
-  const int s = surv[i];
-  ic[i] = make_int2(sad_img[s], crit_sad[s]);
-}
-
+// Per-survivor records of one side gathered once in output (sweep) order, so
+// the later per-survivor kernels read them in order instead of gathering
+// from the list-ordered saddle arrays again: its arc ends, raw-arc lengths
+// and the record of its outputs (out ranks of its ends' thresholded roots,
+// persistence, out rank of its pair's root; -1 for the void).
 __global__ void surv_side_kernel(int nsurv, const int* __restrict__ surv, const int* __restrict__ t,
                                  const long long* __restrict__ blen, const float* __restrict__ pers,
                                  const int* __restrict__ pair_dense, const int* __restrict__ rout,
@@ -220,11 +215,6 @@ __global__ void sad_pts_kernel(int nsurv, const int2* __restrict__ surv_ic, cons
   out[out_off[b] + (i - surv_base[b])] = ic.y - 4 * I.idx_base[b];
 }
 
-__global__ void pair_len_kernel(int nsurv, const long long* __restrict__ arc_len, long long* __restrict__ out) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nsurv) out[i] = arc_len[2 * i] + arc_len[2 * i + 1];
-}
-
 // Geometry start of every image on one side (B + 1 entries).
 __global__ void geom_base_kernel(int B, const int* __restrict__ surv_base, int nsurv,
                                  const long long* __restrict__ saddle_end_incl, const long long* __restrict__ plen,
@@ -235,29 +225,18 @@ __global__ void geom_base_kernel(int B, const int* __restrict__ surv_base, int n
   gbase[b] = f < nsurv ? saddle_end_incl[f] - plen[f] : *total;
 }
 
-// Output position of every arc: the image's destination offset plus the
-// arc's position inside the image's geometry.
-__global__ void arc_pos_kernel(int nsurv, const long long* __restrict__ arc_len,
-                               const long long* __restrict__ saddle_end_incl, const int2* __restrict__ surv_ic,
-                               const long long* __restrict__ gbase, const int* __restrict__ dst_off,
-                               long long* __restrict__ arc_pos) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nsurv) return;
-  long long start = saddle_end_incl[i] - arc_len[2 * i] - arc_len[2 * i + 1];
-  const int b = surv_ic[i].x;
-  start += (long long)dst_off[b] - gbase[b];
-  arc_pos[2 * i] = start;
-  arc_pos[2 * i + 1] = start + arc_len[2 * i];
-}
-
 // CSR offsets of one side's arcs, per image (cpu/workspace.hxx:247-287):
 // offsets[0] = 0, offsets[k+1] = end of survivor k, arc_offsets[k] = end of
 // its first arc, image-local. `off_off[b]` / `arc_off[b]` place image b's
-// block (n_b + 1 and n_b entries) in the routed arrays.
+// block (n_b + 1 and n_b entries) in the routed arrays. With `arc_pos`, also
+// the output position of every arc for the geometry writer: the image's
+// destination offset (`dst_off`) plus the arc's position inside the image's
+// geometry.
 __global__ void arc_offsets_kernel(int nsurv, int B, const int* __restrict__ surv_base, const uint8_t* __restrict__ dual,
                                    const long long* __restrict__ arc_len,
                                    const long long* __restrict__ saddle_end_incl, const long long* __restrict__ gbase,
-                                   Route OFF, Route AOFF) {
+                                   Route OFF, Route AOFF, const int* __restrict__ dst_off,
+                                   long long* __restrict__ arc_pos) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsurv + B) return;
   if (i >= nsurv) {  // one leading zero per image
@@ -267,11 +246,16 @@ __global__ void arc_offsets_kernel(int nsurv, int B, const int* __restrict__ sur
   }
   int b = find_image(surv_base, B, i);
   const bool d = dual[b];
+  const longlong2 al = *reinterpret_cast<const longlong2*>(arc_len + 2 * i);
   long long end = saddle_end_incl[i] - gbase[b];
-  long long start = end - arc_len[2 * i] - arc_len[2 * i + 1];
+  long long start = end - al.x - al.y;
   int li = i - surv_base[b];
   if (int* o = OFF.at(d, b)) o[li + 1] = (int)end;
-  if (int* a = AOFF.at(d, b)) a[li] = (int)(start + arc_len[2 * i]);
+  if (int* a = AOFF.at(d, b)) a[li] = (int)(start + al.x);
+  if (arc_pos) {
+    const long long p = start + dst_off[b];
+    *reinterpret_cast<longlong2*>(arc_pos + 2 * i) = make_longlong2(p, p + al.x);
+  }
 }
 
 }  // namespace dmsc

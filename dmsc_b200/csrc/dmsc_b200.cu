@@ -591,11 +591,9 @@ void replay_final(dmsc_b200_context* ctx, int si, Side& S, long long* total, cud
   S.arc_root = sget<int>(ctx, si, X_AROOT, 2 * (size_t)nsurv);
   S.plen = sget<long long>(ctx, si, X_PLEN, nsurv);
   S.send = sget<long long>(ctx, si, X_SEND, nsurv);
-  LK(final_arcs_kernel<<<grid_for(2LL * nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv_ic, ctx->I.dual, S.arcs_primal,
-                                                                 S.arcs_dual, S.sv_t, S.sv_len, S.alive, S.R,
-                                                                 ctx->nsad + 1,
-                                                                 S.arc_len, S.arc_cl, S.arc_root, ctx->status));
-  LK(pair_len_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.plen));
+  LK(final_arcs_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, ctx->surv_ic, ctx->I.dual, S.arcs_primal,
+                                                           S.arcs_dual, S.sv_t, S.sv_len, S.alive, S.R, ctx->nsad + 1,
+                                                           S.arc_len, S.arc_cl, S.arc_root, S.plen, ctx->status));
   incl_sum(ctx, S.plen, S.send, nsurv, st);
   LK(last_kernel<long long><<<1, 1, 0, st>>>(S.send, nsurv, total));
   LAUNCH_CHECK("final arcs");
@@ -982,13 +980,11 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
       LK(survivor_gather_kernel<uint32_t><<<grid_for(nsad, TB), TB, 0, ss>>>(nsad, flag, fpos, skey32, k, sidx));
       sort_pairs(ctx, k, get<uint32_t>(ctx, S_SKEYS, nsurv), sidx, sorted, nsurv, ss, 32);
     }
-    LK(survivor_order_kernel<<<grid_for(nsurv, TB), TB, 0, ss>>>(nsurv, sorted, ctx->sad_img, I.dual, BS.surv,
-                                                               ctx->surv));
-    LAUNCH_CHECK("survivor order");
-    // the survivors' records, gathered once in output order
+    // the survivors in output order, with their records gathered once
     ctx->surv_ic = get<int2>(ctx, S_SURVIC, nsurv);
-    LK(surv_common_kernel<<<grid_for(nsurv, TB), TB, 0, ss>>>(nsurv, ctx->surv, ctx->sad_img, ctx->crit_sad,
-                                                            ctx->surv_ic));
+    LK(survivor_order_kernel<<<grid_for(nsurv, TB), TB, 0, ss>>>(nsurv, sorted, ctx->sad_img, ctx->crit_sad, I.dual,
+                                                               BS.surv, ctx->surv, ctx->surv_ic));
+    LAUNCH_CHECK("survivor order");
     for (int si = 0; si < 2; ++si) {
       Side& S = ctx->side[si];
       S.sv_t = sget<int2>(ctx, si, X_SVT, nsurv);
@@ -1187,17 +1183,13 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
 void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, int32_t* flat_dual, const int* dst_off,
                Route OFF, Route AOFF, cudaStream_t st) {
   const int nsurv = ctx->nsurv, B = ctx->B;
-  if (nsurv > 0)
-    LK(arc_offsets_kernel<<<grid_for(nsurv + (long long)B, TB), TB, 0, st>>>(
-        nsurv, B, ctx->bases.surv, ctx->I.dual, S.arc_len, S.send, S.gbase, OFF, AOFF));
-  else
-    LK(arc_offsets_kernel<<<grid_for((long long)B, TB), TB, 0, st>>>(0, B, ctx->bases.surv, ctx->I.dual, S.arc_len,
-                                                                     S.send, S.gbase, OFF, AOFF));
+  // the arcs' output positions only when geometry is written
+  const bool geom = S.total > 0 && (flat_primal || flat_dual);
+  long long* arc_pos = geom ? sget<long long>(ctx, si, X_APOS, 2 * (size_t)nsurv) : nullptr;
+  LK(arc_offsets_kernel<<<grid_for(nsurv + (long long)B, TB), TB, 0, st>>>(
+      nsurv, B, ctx->bases.surv, ctx->I.dual, S.arc_len, S.send, S.gbase, OFF, AOFF, dst_off, arc_pos));
   LAUNCH_CHECK("arc_offsets_kernel");
-  if (S.total <= 0 || (!flat_primal && !flat_dual)) return;
-  long long* arc_pos = sget<long long>(ctx, si, X_APOS, 2 * (size_t)nsurv);
-  LK(arc_pos_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.send, ctx->surv_ic, S.gbase, dst_off,
-                                                        arc_pos));
+  if (!geom) return;
   long long cap = S.total;
   EmitArgs A;
   EmitCtx& E = A.E;

@@ -120,34 +120,40 @@ __device__ __forceinline__ bool walk_root(const ReplayState& S, const uint8_t* _
 }
 
 // Final arcs of the surviving saddles: length and the chain root of each
-// (survivor i in output order, arc j), from the survivors' gathered records
-// (image, arc ends, raw-arc lengths). Images whose output does not take this
-// side's arcs (`arcs_primal` / `arcs_dual` by orientation) get empty arcs.
+// (survivor i in output order, arcs 0 and 1), and the survivor's total path
+// length, from the survivors' gathered records (image, arc ends, raw-arc
+// lengths). Images whose output does not take this side's arcs
+// (`arcs_primal` / `arcs_dual` by orientation) get empty arcs.
 __global__ void final_arcs_kernel(int nsurv, const int2* __restrict__ surv_ic, const uint8_t* __restrict__ dual,
                                   bool arcs_primal, bool arcs_dual, const int2* __restrict__ sv_t,
                                   const longlong2* __restrict__ sv_len, const uint8_t* __restrict__ alive,
                                   ReplayState S, int max_steps, long long* __restrict__ arc_len,
-                                  long long* __restrict__ arc_cl, int* __restrict__ arc_root, unsigned* status) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= 2 * nsurv) return;
-  int i = q >> 1, j = q & 1;
+                                  long long* __restrict__ arc_cl, int* __restrict__ arc_root,
+                                  long long* __restrict__ plen, unsigned* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsurv) return;
   const int2 tt = sv_t[i];
-  const int T = j ? tt.y : tt.x;
-  if (T < 0 || !(dual[surv_ic[i].x] ? arcs_dual : arcs_primal)) {
-    arc_len[q] = 0;
-    arc_cl[q] = 0;
-    arc_root[q] = -1;
-    return;
-  }
   const longlong2 bl = sv_len[i];
-  // an extremum that no cancellation kills (alive) is its own final root;
-  // only the others walk their parent chains
-  int R = T;
-  long long a = 0;
-  if (!alive[T]) walk_root(S, alive, T, kNever, &R, &a, max_steps, status);
-  arc_len[q] = (j ? bl.y : bl.x) + a;
-  arc_cl[q] = a;
-  arc_root[q] = R;
+  const bool take = dual[surv_ic[i].x] ? arcs_dual : arcs_primal;
+  long long len[2] = {0, 0}, cl[2] = {0, 0};
+  int root[2] = {-1, -1};
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int T = j ? tt.y : tt.x;
+    if (T < 0 || !take) continue;
+    // an extremum that no cancellation kills (alive) is its own final root;
+    // only the others walk their parent chains
+    int R = T;
+    long long a = 0;
+    if (!alive[T]) walk_root(S, alive, T, kNever, &R, &a, max_steps, status);
+    len[j] = (j ? bl.y : bl.x) + a;
+    cl[j] = a;
+    root[j] = R;
+  }
+  *reinterpret_cast<longlong2*>(arc_len + 2 * i) = make_longlong2(len[0], len[1]);
+  *reinterpret_cast<longlong2*>(arc_cl + 2 * i) = make_longlong2(cl[0], cl[1]);
+  *reinterpret_cast<int2*>(arc_root + 2 * i) = make_int2(root[0], root[1]);
+  plen[i] = len[0] + len[1];
 }
 
 // ---------------------------------------------------------------------------
