@@ -101,19 +101,17 @@ __global__ void survivor_order_kernel(int n, const int* __restrict__ sorted, con
 // from the list-ordered saddle arrays again: its arc ends, raw-arc lengths
 // and the record of its outputs (out ranks of its ends' thresholded roots,
 // persistence, out rank of its pair's root; -1 for the void).
-__global__ void surv_side_kernel(int nsurv, const int* __restrict__ surv, const int* __restrict__ t,
-                                 const long long* __restrict__ blen, const float* __restrict__ pers,
-                                 const int* __restrict__ pair_dense, const int* __restrict__ rout,
-                                 int2* __restrict__ sv_t, longlong2* __restrict__ sv_len, int4* __restrict__ sv_rec) {
+__global__ void surv_side_kernel(int nsurv, const int* __restrict__ surv, const int4* __restrict__ arc,
+                                 const int2* __restrict__ pp, const int* __restrict__ rout, int2* __restrict__ sv_t,
+                                 longlong2* __restrict__ sv_len, int4* __restrict__ sv_rec) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsurv) return;
   const int s = surv[i];
-  const int2 tt = *reinterpret_cast<const int2*>(t + 2 * s);
-  sv_t[i] = tt;
-  sv_len[i] = *reinterpret_cast<const longlong2*>(blen + 2 * s);
-  const int pd = pair_dense[s];
-  sv_rec[i] = make_int4(tt.x >= 0 ? rout[tt.x] : -1, tt.y >= 0 ? rout[tt.y] : -1, __float_as_int(pers[s]),
-                        pd >= 0 ? rout[pd] : -1);
+  const int4 a = arc[s];
+  const int2 pr = pp[s];
+  sv_t[i] = make_int2(a.x, a.y);
+  sv_len[i] = make_longlong2(a.z, a.w);
+  sv_rec[i] = make_int4(a.x >= 0 ? rout[a.x] : -1, a.y >= 0 ? rout[a.y] : -1, pr.y, pr.x >= 0 ? rout[pr.x] : -1);
 }
 
 // Per-image first positions (B + 1 entries, the last one the total):

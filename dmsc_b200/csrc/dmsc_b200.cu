@@ -40,12 +40,12 @@ namespace {
 enum Slot {
   S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
   S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_MINBITS, S_MAXBITS, S_VMIN, S_VMAX, S_KMIN, S_KMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
-  S_ASC, S_TF, S_LF, S_TV, S_LV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
+  S_ASC, S_ARCF, S_ARCV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
   S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX, S_SKEY32, S_SKEY32B, S_SKEYS, S_SURVIC,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
-  X_ROUT, X_SVT, X_SVL, X_SVR, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_PERS, X_ALIVE,
+  X_ROUT, X_SVT, X_SVL, X_SVR, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_ALIVE,
   X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_CKEY, X_CVAL, X_NODE,
   X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
   X_GBASE, X_WX, X_WA, X_CENDS, kSideSlots
@@ -77,18 +77,16 @@ struct Side {
   int* ext_img = nullptr;
   float* val = nullptr;
   const int2* key = nullptr;  // (value bits, cell) per extremum
-  int* t = nullptr;
+  int4* arc = nullptr;              // [nsad] per saddle (list order): arc ends and raw-arc cells
   int* rout = nullptr;              // [M] out rank of each extremum's thresholded root (-1: the void)
   int2* sv_t = nullptr;             // [nsurv] per survivor (output order): arc ends
   longlong2* sv_len = nullptr;      // raw-arc lengths
   int4* sv_rec = nullptr;           // out ranks of the ends' roots, persistence, out rank of the pair's root
   int* dying = nullptr;
-  int* pair_dense = nullptr;
-  float* pers = nullptr;
+  int2* pp = nullptr;               // [nsad] paired extremum (-1: none) and persistence bits
   uint8_t* alive = nullptr;
   int* to_out_excl = nullptr;
   int* to_out = nullptr;
-  long long* blen = nullptr;
   ReplayState R{};
   int C = 0;
   long long* arc_len = nullptr;
@@ -503,8 +501,7 @@ void run_pairing(dmsc_b200_context* ctx, const float* sval, cudaStream_t st) {
 void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   const int nsad = ctx->nsad, M = S.M;
   // persistence, cancellation, alive flags
-  S.pair_dense = sget<int>(ctx, si, X_PAIR, nsad);
-  S.pers = sget<float>(ctx, si, X_PERS, nsad);
+  S.pp = sget<int2>(ctx, si, X_PAIR, nsad);
   S.alive = sget<uint8_t>(ctx, si, X_ALIVE, M + 4);
   CK(cudaMemsetAsync(S.alive, 1, M + 4, st));
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
@@ -519,7 +516,7 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   if (nsad > 0) {
     LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(
         nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.dying, get<float>(ctx, S_SVAL, nsad), S.val,
-        S.pair_dense, S.pers, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.t, cends, ctx->crit_sad, ckey,
+        S.pp, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.arc, cends, ctx->crit_sad, ckey,
         cval, node));
     LAUNCH_CHECK("persistence_kernel");
   }
@@ -564,8 +561,7 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   A.key = ckey;
   A.cj = cval;
   A.dying = S.dying;
-  A.t = S.t;
-  A.blen = S.blen;
+  A.arc = S.arc;
   A.alive = S.alive;
   A.crit_sad = ctx->crit_sad;
   A.S = R;
@@ -874,13 +870,12 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   mark(ctx, 2, st);
 
   // ---- K4 saddle walks ----
-  int* tf = get<int>(ctx, S_TF, 2 * (size_t)nsad);
-  long long* lf = get<long long>(ctx, S_LF, 2 * (size_t)nsad);  // raw-arc lengths (cells)
-  int* tv = get<int>(ctx, S_TV, 2 * (size_t)nsad);
-  long long* lv = get<long long>(ctx, S_LV, 2 * (size_t)nsad);
+  // per saddle and side: arc ends and raw-arc lengths (cells)
+  int4* arc_f = get<int4>(ctx, S_ARCF, nsad);
+  int4* arc_v = get<int4>(ctx, S_ARCV, nsad);
   if (nsad > 0) {
-    LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(I, flow, nsad, csad, isad, off[2], bmax, off[0], bmin, tf,
-                                                             lf, tv, lv, ncells, ps, ctx->status));
+    LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(I, flow, nsad, csad, isad, off[2], bmax, off[0], bmin,
+                                                             arc_f, arc_v, ncells, ps, ctx->status));
     LAUNCH_CHECK("saddle_walk_kernel");
   }
 
@@ -901,10 +896,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   V.val = vmin;
   F.key = kmax;
   V.key = kmin;
-  F.t = tf;
-  F.blen = lf;
-  V.t = tv;
-  V.blen = lv;
+  F.arc = arc_f;
+  V.arc = arc_v;
   // faces: ridges/peaks in the primal, valleys/basins in the dual (workspace.hxx:322-362)
   F.arcs_primal = f_ridges;
   F.arcs_dual = f_valleys;
@@ -990,7 +983,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
       S.sv_t = sget<int2>(ctx, si, X_SVT, nsurv);
       S.sv_len = sget<longlong2>(ctx, si, X_SVL, nsurv);
       S.sv_rec = sget<int4>(ctx, si, X_SVR, nsurv);
-      LK(surv_side_kernel<<<grid_for(nsurv, TB), TB, 0, ss>>>(nsurv, ctx->surv, S.t, S.blen, S.pers, S.pair_dense,
+      LK(surv_side_kernel<<<grid_for(nsurv, TB), TB, 0, ss>>>(nsurv, ctx->surv, S.arc, S.pp,
                                                             S.rout, S.sv_t, S.sv_len, S.sv_rec));
     }
     LAUNCH_CHECK("survivor records");
@@ -1372,7 +1365,7 @@ int fetch_pair_pixels_impl(dmsc_b200_context* ctx, int32_t* plus_max, int32_t* m
     Route PLUS{S.faces ? plus_max : plus_min, S.faces ? plus_min : plus_max, ctx->bases.surv};
     Route MINUS{S.faces ? minus_max : minus_min, S.faces ? minus_min : minus_max, ctx->bases.surv};
     LK(pair_pixels_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, ctx->bases.surv, ctx->I, ctx->img,
-                                                              ctx->surv, ctx->crit_sad, S.pair_dense, S.crit, PLUS,
+                                                              ctx->surv, ctx->crit_sad, S.pp, S.crit, PLUS,
                                                               MINUS));
   }
   LAUNCH_CHECK("pair_pixels_kernel");

@@ -61,9 +61,9 @@ __device__ __forceinline__ bool older(int a, int b, int void_id, const int2* __r
   return older_less ? tie_lt(va, ka.y, vb, kb.y) : tie_lt(vb, kb.y, va, ka.y);
 }
 
-// K4: per saddle, both face walks and the vertex walks. Writes per arc (2
-// per saddle and side) the dense target index (or -1) and the raw arc's cell
-// count; then runs the pairing's round-0 saddle phase for both sides (all
+// K4: per saddle, both face walks and the vertex walks. Writes per saddle and
+// side one record {target 0, target 1, cells 0, cells 1}: each arc's dense
+// target index (or -1) and its raw arc's cell count; then runs the pairing's round-0 saddle phase for both sides (all
 // groups are still single extrema, so the ends are the groups): a saddle
 // whose two ends coincide is a cycle, the others record their ends' groups
 // and reduce their sweep key into both groups' minimum, and each block adds
@@ -74,25 +74,23 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
                                                           const int* __restrict__ off_max,
                                                           const uint32_t* __restrict__ max_bits,
                                                           const int* __restrict__ off_min,
-                                                          const uint32_t* __restrict__ min_bits, int* __restrict__ tf,
-                                                          long long* __restrict__ lf, int* __restrict__ tv,
-                                                          long long* __restrict__ lv, long long cap, PairStart ps,
-                                                          unsigned* status) {
+                                                          const uint32_t* __restrict__ min_bits,
+                                                          int4* __restrict__ arc_f, int4* __restrict__ arc_v,
+                                                          long long cap, PairStart ps, unsigned* status) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   int keep[2] = {0, 0};
   if (s < nsad) {
     const int b = sad_img[s];
     const int H = I.H[b], W = I.W[b], Nx = W + 1;
     const int sc = crit_sad[s];
-    int te[2][2];
+    int te[2][2], len[2][2];
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       long long steps;
       const int end = flow_walk<4>(flow, face_start(sc, j, Nx) >> 2, Nx, cap, &steps, status);
       const int target = seg_rank(I, b, end, Nx, off_max, max_bits);
-      tf[2 * s + j] = target;
-      lf[2 * s + j] = target >= 0 ? steps + 1 : 0;  // cells of the raw arc, start and end included
       te[0][j] = target;
+      len[0][j] = target >= 0 ? (int)steps + 1 : 0;  // cells of the raw arc, start and end included
     }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -103,10 +101,12 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
         const int end = flow_walk<0>(flow, start >> 2, Nx, cap, &steps, status);
         target = seg_rank(I, b, end, Nx, off_min, min_bits);
       }
-      tv[2 * s + j] = target;
-      lv[2 * s + j] = target >= 0 ? steps + 1 : 0;  // an arc that leaves the image is empty
       te[1][j] = target;
+      len[1][j] = target >= 0 ? (int)steps + 1 : 0;  // an arc that leaves the image is empty
     }
+    // a raw arc has fewer cells than the batch (cell ids are int32)
+    arc_f[s] = make_int4(te[0][0], te[0][1], len[0][0], len[0][1]);
+    arc_v[s] = make_int4(te[1][0], te[1][1], len[1][0], len[1][1]);
     // round 0 of the pairing: descending sweep on the face side in the
     // primal and the vertex side in the dual
     const bool d = I.dual[b];
@@ -140,18 +140,19 @@ __global__ void iota_kernel(int* __restrict__ a, int n) {
 }
 
 // Persistence of each decided saddle and cancellation (persistence.hxx:82-104,
-// 139-161), with the saddle's image's orientation and threshold; `sbit` marks
-// the side in `cancelled`.
+// 139-161), with the saddle's image's orientation and threshold: pp[s] =
+// (paired extremum or -1, persistence bits; -1 for a cycle); `sbit` marks the
+// side in `cancelled`.
 __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_side, const uint8_t* __restrict__ dual,
                                                           const float* __restrict__ thr,
                                                           const int* __restrict__ sad_img,
                                                           const int* __restrict__ dying,
                                                           const float* __restrict__ sad_val,
                                                           const float* __restrict__ ext_val,
-                                                          int* __restrict__ pair_dense, float* __restrict__ pers,
+                                                          int2* __restrict__ pp,
                                                           uint8_t* __restrict__ cancelled, uint8_t sbit,
                                                           uint8_t* __restrict__ alive, int* __restrict__ n_cancel,
-                                                          const int* __restrict__ t,
+                                                          const int4* __restrict__ arc,
                                                           int2* __restrict__ canc_ends,
                                                           const int* __restrict__ crit_sad,
                                                           unsigned long long* __restrict__ ckey,
@@ -159,28 +160,27 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
   // saddles in list order: every per-saddle access is sequential
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   bool canc = false;
+  int d = -1;
+  float p = -1.0f;
   if (s < nsad) {
-    const int d = dying[s];
+    d = dying[s];
     if (d < 0) {
-      pair_dense[s] = -1;
-      pers[s] = -1.0f;
+      d = -1;
     } else {
       const int b = sad_img[s];
       const bool du = dual[b];
       float sv = sad_val[s], ev = ext_val[d];
-      float p;
       if (min_side)
         p = du ? sub_like_host(ev, sv) : sub_like_host(sv, ev);
       else
         p = du ? sub_like_host(sv, ev) : sub_like_host(ev, sv);
-      pair_dense[s] = d;
-      pers[s] = p;
       if (p <= thr[b]) {
         canc = true;
         atomicOr((unsigned*)(cancelled + (s & ~3)), (unsigned)sbit << (8 * (s & 3)));
         alive[d] = 0;
       }
     }
+    pp[s] = make_int2(d, __float_as_int(p));
   }
   // cancelled edges' ends, compacted for the thresholded union-find, and (when
   // the side's arcs are simplified) the same cancellations with their replay
@@ -189,14 +189,14 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
   // so the pair is unique and the target cell never breaks a tie
   const int slot = block_append(n_cancel, canc);
   if (canc) {
-    canc_ends[slot] = make_int2(t[2 * s], t[2 * s + 1]);
+    const int4 a = arc[s];
+    canc_ends[slot] = make_int2(a.x, a.y);
     if (ckey) {
-      const unsigned long long key = ((unsigned long long)orderable_key(pers[s]) << 32) | (unsigned)crit_sad[s];
+      const unsigned long long key = ((unsigned long long)orderable_key(p) << 32) | (unsigned)crit_sad[s];
       ckey[slot] = key;
       cval[slot] = s;
       // the killed extremum's replay record: its cancellation key, undecided
       // (the other records are never read, see replay.cuh)
-      const int d = pair_dense[s];
       node[d].ctime = key;
       node[d].status = kPending;
     }

@@ -87,7 +87,7 @@ __device__ __forceinline__ int value_pixel(const float* __restrict__ img_all, co
 // primal and on the face side in the dual, extremum - saddle otherwise.
 __global__ void pair_pixels_kernel(int nsurv, bool faces, const int* __restrict__ surv_base, Imgs I,
                                    const float* __restrict__ img_all, const int* __restrict__ surv_sad,
-                                   const int* __restrict__ crit_sad, const int* __restrict__ pair_dense,
+                                   const int* __restrict__ crit_sad, const int2* __restrict__ pp,
                                    const int* __restrict__ ext_cell, Route PLUS, Route MINUS) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nsurv) return;
@@ -96,7 +96,7 @@ __global__ void pair_pixels_kernel(int nsurv, bool faces, const int* __restrict_
   const bool d = I.dual[b];
   const int li = i - surv_base[b];
   const int s = surv_sad[i];
-  const int e = pair_dense[s];
+  const int e = pp[s].x;
   int plus = -1, minus = -1;
   if (e >= 0) {
     const int sp = value_pixel(img_all, I, b, crit_sad[s]);

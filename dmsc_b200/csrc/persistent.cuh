@@ -481,8 +481,7 @@ struct ReplayArgs {
   const unsigned long long* key;     // [C] replay key of each cancellation
   const int* cj;                     // [C] saddle (list index) of each cancellation
   const int* dying;  // [nsad] in saddle list order
-  const int* t;      // [2 nsad] extremum ends of each saddle, list order
-  const long long* blen;
+  const int4* arc;   // [nsad] {end 0, end 1, raw-arc cells 0, raw-arc cells 1} of each saddle, list order
   const uint8_t* alive;  // [M] extrema that no cancellation kills (their records are never read)
   const int* crit_sad;   // [nsad] global cell id of each saddle
   ReplayState S;
@@ -556,7 +555,7 @@ __device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long 
     for (int u = 0; u < U; ++u) {
       if (!((act >> u) & 1u)) continue;
       const bool s1 = (s1m >> u) & 1u;
-      const int2 w = *reinterpret_cast<const int2*>(RSIDE(t) + 2 * sd[u]);
+      const int4 w = RSIDE(arc)[sd[u]];
       x[2 * u] = w.x;
       x[2 * u + 1] = w.y;
     }
@@ -639,8 +638,9 @@ __device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long 
       k = 1;
     ReplayNode* node = RSIDE(S.node);
     if (k >= 0) {
-      const longlong2 bl = *reinterpret_cast<const longlong2*>(RSIDE(blen) + 2 * s);
-      const int2 tt = *reinterpret_cast<const int2*>(RSIDE(t) + 2 * s);
+      const int4 ar = RSIDE(arc)[s];
+      const int2 tt = make_int2(ar.x, ar.y);
+      const longlong2 bl = make_longlong2(ar.z, ar.w);
       *reinterpret_cast<longlong2*>(&node[dd].cl_dy) = make_longlong2(k == 0 ? a0 : a1, k == 0 ? a1 : a0);
       *reinterpret_cast<int4*>(&node[dd].t_dy) =
           make_int4(k == 0 ? tt.x : tt.y, k == 0 ? tt.y : tt.x, (int)(k == 0 ? bl.x : bl.y),
@@ -916,30 +916,38 @@ __global__ void __launch_bounds__(256, MINB) emit_persistent_kernel(EmitArgs A) 
   const EmitCtx& E = A.E;
   int* const n_base = A.cnt + 3;
   // level 0: the chain of each surviving arc (its own raw arc is a segment
-  // item of the writer, read from the survivor records)
-  for (long long base = 0; base < 2LL * A.nsurv; base += nth) {
-    const long long q = base + tid;
-    bool push = false;
-    int4 task = make_int4(0, 0, 0, 0);
+  // item of the writer, read from the survivor records). A block takes
+  // kLevel0Arcs arcs per thread at a time: it counts their chains, reserves
+  // queue slots once for all of them and then writes the tasks, so the
+  // blocks queue on the shared counter once per 4096 arcs instead of once
+  // per 256 (each reservation waits on the atomic's return).
+  constexpr int kLevel0Arcs = 16;
+  const long long narcs = 2LL * A.nsurv, span = (long long)blockDim.x * kLevel0Arcs;
+  for (long long base = (long long)blockIdx.x * span; base < narcs; base += (long long)gridDim.x * span) {
     // a chain exists only on arcs that the image's output takes (arc_cl = 0 otherwise)
-    if (q < 2LL * A.nsurv && A.arc_cl[q] > 0) {
-      const int i = (int)(q >> 1), j = (int)(q & 1);
-      const int2 tt = E.sv_t[i];
-      const longlong2 bl = E.sv_len[i];
-      push = true;
-      task = make_task(kTaskChain, 0, j ? tt.y : tt.x, A.arc_root[q], E.arc_pos[q] + (j ? bl.y : bl.x));
+    int mine = 0;
+#pragma unroll
+    for (int k = 0; k < kLevel0Arcs; ++k) {
+      const long long q = base + (long long)k * blockDim.x + threadIdx.x;
+      mine += q < narcs && A.arc_cl[q] > 0;
     }
     // most arcs have no chain (at threshold 0 nearly all): a block reserves
     // queue slots only when one of its threads has a task
-    if (__syncthreads_or(push)) {
-      int p, pb;
-      block_reserve2(A.cnt, push ? 1 : 0, n_base, 0, p, pb);
-      if (push) {
-        if (p < E.q_cap)
-          A.q0[p] = task;
-        else
-          set_status(E.status, kStatusQueueOverflow);
-      }
+    if (!__syncthreads_or(mine > 0)) continue;
+    int p, pb;
+    block_reserve2(A.cnt, mine, n_base, 0, p, pb);
+    if (mine == 0) continue;
+    for (int k = 0; k < kLevel0Arcs; ++k) {
+      const long long q = base + (long long)k * blockDim.x + threadIdx.x;
+      if (q >= narcs || A.arc_cl[q] <= 0) continue;
+      const int i = (int)(q >> 1), j = (int)(q & 1);
+      const int2 tt = E.sv_t[i];
+      const longlong2 bl = E.sv_len[i];
+      if (p < E.q_cap)
+        A.q0[p] = make_task(kTaskChain, 0, j ? tt.y : tt.x, A.arc_root[q], E.arc_pos[q] + (j ? bl.y : bl.x));
+      else
+        set_status(E.status, kStatusQueueOverflow);
+      ++p;
     }
   }
   grid.sync();
