@@ -848,9 +848,9 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     ps.g12[si] = sget<int2>(ctx, si, X_G12, nsad);
     ps.dying[si] = sget<int>(ctx, si, X_DYING, nsad);
   }
-  LK(compact_kernel<<<grid_for(nseg, 8), 256, 0, st>>>(I, img, nseg, flow, off[0], off[1], off[2], cmin, csad, cmax,
-                                                       imin, isad, imax, bmin, bmax, vmin, vmax, kmin, kmax, sval, skey,
-                                                       skey32, ps));
+  LK(compact_kernel<<<grid_for(nseg, 8 * kCompactSegs), 256, 0, st>>>(
+      I, img, nseg, flow, off[0], off[1], off[2], cmin, csad, cmax, imin, isad, imax, bmin, bmax, vmin, vmax, kmin,
+      kmax, sval, skey, skey32, ps));
   LAUNCH_CHECK("compact_kernel");
   // per-image bases of the critical lists (B + 1 entries each)
   int* bases = get<int>(ctx, S_BASES, 9 * (size_t)(B + 1));

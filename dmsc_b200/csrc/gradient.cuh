@@ -658,16 +658,34 @@ struct CellValues {
   float v, h, e, f;  // vertex, H edge (t = 1), V edge (t = 2), face (t = 3)
 };
 
-template <bool DUAL>
-__device__ __forceinline__ CellValues warp_cell_values(const float* __restrict__ img, int y, int x, int H, int W,
-                                                       int lane) {
+// The four pixel values an index's cells need: its own (y, x), the one above
+// and their left neighbours (0 outside the image).
+struct CellPixels {
+  float a, u, aL, uL;
+};
+
+// The loads of the cell values: every lane loads its pixel and the one above
+// it; lane 0 also loads its left neighbours (the other lanes take theirs from
+// the lane to their left in cell_values_of).
+__device__ __forceinline__ CellPixels warp_cell_loads(const float* __restrict__ img, int y, int x, int H, int W,
+                                                      int lane) {
   const bool in_x = x < W, in_xl = x >= 1 && x - 1 < W, up = y >= 1, here = y < H;
-  const float a = (here && in_x) ? __ldg(img + (size_t)y * W + x) : 0.f;
-  const float u = (up && in_x) ? __ldg(img + (size_t)(y - 1) * W + x) : 0.f;
+  CellPixels c;
+  c.a = (here && in_x) ? __ldg(img + (size_t)y * W + x) : 0.f;
+  c.u = (up && in_x) ? __ldg(img + (size_t)(y - 1) * W + x) : 0.f;
+  c.aL = (lane == 0 && here && in_xl) ? __ldg(img + (size_t)y * W + x - 1) : 0.f;
+  c.uL = (lane == 0 && up && in_xl) ? __ldg(img + (size_t)(y - 1) * W + x - 1) : 0.f;
+  return c;
+}
+
+template <bool DUAL>
+__device__ __forceinline__ CellValues cell_values_of(CellPixels px, int y, int x, int H, int W, int lane) {
+  const bool in_x = x < W, up = y >= 1, here = y < H;
+  const float a = px.a, u = px.u;
   float aL = __shfl_up_sync(0xffffffffu, a, 1), uL = __shfl_up_sync(0xffffffffu, u, 1);
   if (lane == 0) {
-    aL = (here && in_xl) ? __ldg(img + (size_t)y * W + x - 1) : 0.f;
-    uL = (up && in_xl) ? __ldg(img + (size_t)(y - 1) * W + x - 1) : 0.f;
+    aL = px.aL;
+    uL = px.uL;
   }
   const int id = y * W + x, idu = id - W;
   CellValues c;
@@ -707,17 +725,22 @@ __host__ __device__ __forceinline__ unsigned crit_bits(unsigned fl, bool vin) {
   return (unsigned)((fl & 7u) == 0u && vin) | ((fl >> 2) & 2u) | ((fl >> 5) & 4u) | (unsigned)(((fl >> 4) & 7u) == 0u) << 3;
 }
 
-// K2: ordered compaction. One warp per (row, 32-column) segment of an image;
-// segment offsets are exclusive scans of the per-segment counts over the
-// whole batch (images in order, rows in order), so each image's lists are a
-// contiguous slice in ascending cell-id order. Writes the three lists as
-// global cell ids, each critical cell's image, the per-segment bit masks of
-// the minima and maxima (an extremum's list rank is its segment's offset plus
-// the extrema before it in the mask), the extremum values (also as (value,
-// cell) records for the elder comparisons of the pairing) and the saddle
-// values with their sort keys (image id above the orderable value, so one
-// sort orders every image); and the pairing's starting state of the groups
+// K2: ordered compaction. One warp per (row, 32-column) segment of an image,
+// kCompactSegs consecutive segments per warp with every load of all of them
+// (flow bytes, pixel values, list offsets) issued before any is used, so a
+// warp waits on one round of loads instead of three per segment; segment
+// offsets are exclusive scans of the per-segment counts over the whole batch
+// (images in order, rows in order), so each image's lists are a contiguous
+// slice in ascending cell-id order. Writes the three lists as global cell
+// ids, each critical cell's image, the per-segment bit masks of the minima
+// and maxima (an extremum's list rank is its segment's offset plus the
+// extrema before it in the mask), the extremum values (also as (value, cell)
+// records for the elder comparisons of the pairing) and the saddle values
+// with their sort keys (image id above the orderable value, so one sort
+// orders every image); and the pairing's starting state of the groups
 // (PairStart).
+constexpr int kCompactSegs = 2;
+
 static __global__ void __launch_bounds__(256) compact_kernel(
     Imgs I, const float* __restrict__ img_all, long long nseg, const uint8_t* __restrict__ flow,
     const int* __restrict__ off_min, const int* __restrict__ off_sad, const int* __restrict__ off_max,
@@ -727,29 +750,11 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     float* __restrict__ min_val, float* __restrict__ max_val, int2* __restrict__ min_key, int2* __restrict__ max_key,
     float* __restrict__ sad_val,
     unsigned long long* __restrict__ sad_key, uint32_t* __restrict__ sad_key32, PairStart ps) {
+  constexpr int K = kCompactSegs;
   const int lane = threadIdx.x & 31;
-  long long seg = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (seg >= nseg) return;
-  const int b = find_image(I.seg_base, I.B, seg);
-  const int H = I.H[b], W = I.W[b], Nx = W + 1;
-  const bool dual = I.dual[b];
-  const int nsegx = (W + 1 + kTileX - 1) / kTileX;
-  const int lseg = (int)(seg - I.seg_base[b]);  // an image has fewer than 2^31 / 4 indices
-  const int iy = lseg / nsegx, sx = lseg - iy * nsegx;
-  const int ix = sx * kTileX + lane;
-  unsigned m = 0;
-  const long long gidx = (long long)I.idx_base[b] + (long long)iy * Nx + ix;
-  const float* img = img_all + I.px_base[b];
-  if (ix <= W) m = crit_bits(flow[gidx], iy < H && ix < W);
-  const unsigned lt = (1u << lane) - 1u;
-  const unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
-  const unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
-  const unsigned bh = __ballot_sync(0xffffffffu, m & 2u), bv = __ballot_sync(0xffffffffu, m & 4u);
-  if (lane == 0) {
-    min_bits[seg] = bmin;
-    max_bits[seg] = bmax;
-  }
-  if (seg == 0 && lane == 0) {  // the pairing's void groups and round counters
+  const long long seg0 = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * K;
+  if (seg0 >= nseg) return;
+  if (seg0 == 0 && lane == 0) {  // the pairing's void groups and round counters
 #pragma unroll
     for (int sd = 0; sd < 2; ++sd) {
       ps.minedge[sd][ps.M[sd]] = ~0ull;
@@ -763,41 +768,82 @@ static __global__ void __launch_bounds__(256) compact_kernel(
       c[5] = 0;
     }
   }
-  if ((bmin | bmax | bh | bv) == 0u) return;  // the whole warp leaves together
-  const CellValues cv = dual ? warp_cell_values<true>(img, iy, ix, H, W, lane)
-                             : warp_cell_values<false>(img, iy, ix, H, W, lane);
-  // saddles before this lane's: both edge kinds of the lanes below it
-  int p = off_sad[seg] + __popc(bh & lt) + __popc(bv & lt);
-  if (m & 1u) {
-    const int q = off_min[seg] + __popc(bmin & lt);
-    crit_min[q] = (int)(4 * gidx);
-    min_img[q] = b;
-    min_val[q] = cv.v;
-    min_key[q] = make_int2(__float_as_int(cv.v), (int)(4 * gidx));
-    ps.minedge[1][q] = ~0ull;  // a single-extremum group without outgoing saddles yet
-    ps.link[1][q] = q;
-  }
-  if (m & 8u) {
-    const int q = off_max[seg] + __popc(bmax & lt);
-    crit_max[q] = (int)(4 * gidx + 3);
-    max_img[q] = b;
-    max_val[q] = cv.f;
-    max_key[q] = make_int2(__float_as_int(cv.f), (int)(4 * gidx + 3));
-    ps.minedge[0][q] = ~0ull;
-    ps.link[0][q] = q;
+  const unsigned lt = (1u << lane) - 1u;
+  int b[K], iy[K], ix[K], o_min[K], o_sad[K], o_max[K];
+  unsigned fl[K];
+  CellPixels px[K];
+  // every load of the warp's segments first
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const long long seg = seg0 + k;
+    b[k] = 0;
+    iy[k] = ix[k] = 0;
+    fl[k] = 0;
+    o_min[k] = o_sad[k] = o_max[k] = 0;
+    px[k] = CellPixels{0.f, 0.f, 0.f, 0.f};
+    if (seg >= nseg) continue;  // warp-uniform
+    b[k] = find_image(I.seg_base, I.B, seg);
+    const int H = I.H[b[k]], W = I.W[b[k]], Nx = W + 1;
+    const int nsegx = (W + 1 + kTileX - 1) / kTileX;
+    const int lseg = (int)(seg - I.seg_base[b[k]]);  // an image has fewer than 2^31 / 4 indices
+    iy[k] = lseg / nsegx;
+    ix[k] = (lseg - iy[k] * nsegx) * kTileX + lane;
+    if (ix[k] <= W) fl[k] = flow[(long long)I.idx_base[b[k]] + (long long)iy[k] * Nx + ix[k]];
+    px[k] = warp_cell_loads(img_all + I.px_base[b[k]], iy[k], ix[k], H, W, lane);
+    o_min[k] = off_min[seg];
+    o_sad[k] = off_sad[seg];
+    o_max[k] = off_max[seg];
   }
 #pragma unroll
-  for (int t = 1; t <= 2; ++t) {
-    if (!(m & (1u << t))) continue;
-    const float v = t == 1 ? cv.h : cv.e;
-    crit_sad[p] = (int)(4 * gidx + t);
-    sad_img[p] = b;
-    sad_val[p] = v;
-    if (sad_key32)  // one image: the image id is 0, a 32-bit key suffices
-      sad_key32[p] = orderable_key(v);
-    else
-      sad_key[p] = ((unsigned long long)b << 32) | orderable_key(v);
-    p++;
+  for (int k = 0; k < K; ++k) {
+    const long long seg = seg0 + k;
+    if (seg >= nseg) break;  // warp-uniform
+    const int bk = b[k], H = I.H[bk], W = I.W[bk], Nx = W + 1;
+    const long long gidx = (long long)I.idx_base[bk] + (long long)iy[k] * Nx + ix[k];
+    const unsigned m = ix[k] <= W ? crit_bits(fl[k], iy[k] < H && ix[k] < W) : 0u;
+    const unsigned bmin = __ballot_sync(0xffffffffu, m & 1u);
+    const unsigned bmax = __ballot_sync(0xffffffffu, m & 8u);
+    const unsigned bh = __ballot_sync(0xffffffffu, m & 2u), bv = __ballot_sync(0xffffffffu, m & 4u);
+    if (lane == 0) {
+      min_bits[seg] = bmin;
+      max_bits[seg] = bmax;
+    }
+    if ((bmin | bmax | bh | bv) == 0u) continue;  // the whole warp together
+    const CellValues cv = I.dual[bk] ? cell_values_of<true>(px[k], iy[k], ix[k], H, W, lane)
+                                     : cell_values_of<false>(px[k], iy[k], ix[k], H, W, lane);
+    // saddles before this lane's: both edge kinds of the lanes below it
+    int p = o_sad[k] + __popc(bh & lt) + __popc(bv & lt);
+    if (m & 1u) {
+      const int q = o_min[k] + __popc(bmin & lt);
+      crit_min[q] = (int)(4 * gidx);
+      min_img[q] = bk;
+      min_val[q] = cv.v;
+      min_key[q] = make_int2(__float_as_int(cv.v), (int)(4 * gidx));
+      ps.minedge[1][q] = ~0ull;  // a single-extremum group without outgoing saddles yet
+      ps.link[1][q] = q;
+    }
+    if (m & 8u) {
+      const int q = o_max[k] + __popc(bmax & lt);
+      crit_max[q] = (int)(4 * gidx + 3);
+      max_img[q] = bk;
+      max_val[q] = cv.f;
+      max_key[q] = make_int2(__float_as_int(cv.f), (int)(4 * gidx + 3));
+      ps.minedge[0][q] = ~0ull;
+      ps.link[0][q] = q;
+    }
+#pragma unroll
+    for (int t = 1; t <= 2; ++t) {
+      if (!(m & (1u << t))) continue;
+      const float v = t == 1 ? cv.h : cv.e;
+      crit_sad[p] = (int)(4 * gidx + t);
+      sad_img[p] = bk;
+      sad_val[p] = v;
+      if (sad_key32)  // one image: the image id is 0, a 32-bit key suffices
+        sad_key32[p] = orderable_key(v);
+      else
+        sad_key[p] = ((unsigned long long)bk << 32) | orderable_key(v);
+      p++;
+    }
   }
 }
 
