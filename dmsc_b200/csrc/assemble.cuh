@@ -49,13 +49,13 @@ __global__ void to_out_kernel(int n, const uint8_t* __restrict__ alive, const in
 
 // Surviving extrema, image-local cell ids, into the routed point lists.
 __global__ void points_kernel(int n, const uint8_t* __restrict__ alive, const int* __restrict__ to_out_excl,
-                              const int* __restrict__ alive_base, const int* __restrict__ cell,
+                              const int* __restrict__ alive_base, const int2* __restrict__ key,
                               const int* __restrict__ ext_img, Imgs I, Route R) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= n || !alive[x]) return;
   int b = ext_img[x];
   int* dst = R.at(I.dual[b], b);
-  if (dst) dst[to_out_excl[x] - alive_base[b]] = cell[x] - 4 * I.idx_base[b];
+  if (dst) dst[to_out_excl[x] - alive_base[b]] = key[x].y - 4 * I.idx_base[b];
 }
 
 // flag[s] = 1 when saddle s (list order) survives both sides.
@@ -65,13 +65,17 @@ __global__ void survivor_flag_kernel(int nsad, const uint8_t* __restrict__ cance
   flag[s] = cancelled[s] == 0;
 }
 
-// The survivors in list order with their sort keys ((image, s_val) order).
+// The survivors in list order with their sort keys ((image, s_val) order:
+// the image id above the orderable value, so one sort orders every image;
+// a 32-bit key of the value alone for one image).
 template <class K>
 __global__ void survivor_gather_kernel(int nsad, const int* __restrict__ flag, const int* __restrict__ pos,
-                                       const K* __restrict__ key, K* __restrict__ key_out, int* __restrict__ idx_out) {
+                                       const float* __restrict__ sval, const int* __restrict__ sad_img,
+                                       K* __restrict__ key_out, int* __restrict__ idx_out) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsad || !flag[s]) return;
-  key_out[pos[s]] = key[s];
+  const uint32_t o = orderable_key(sval[s]);
+  key_out[pos[s]] = sizeof(K) > 4 ? (K)(((unsigned long long)sad_img[s] << 32) | o) : (K)o;
   idx_out[pos[s]] = s;
 }
 

@@ -39,9 +39,9 @@ namespace {
 
 enum Slot {
   S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
-  S_CMIN, S_CSAD, S_CMAX, S_IMIN, S_ISAD, S_IMAX, S_MINBITS, S_MAXBITS, S_VMIN, S_VMAX, S_KMIN, S_KMAX, S_SVAL, S_SKEY, S_SKEY2, S_IOTA,
+  S_CSAD, S_IMIN, S_ISAD, S_IMAX, S_MINBITS, S_MAXBITS, S_KMIN, S_KMAX, S_SVAL, S_SKEY2, S_IOTA,
   S_ASC, S_ARCF, S_ARCV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
-  S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX, S_SKEY32, S_SKEY32B, S_SKEYS, S_SURVIC,
+  S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX, S_SKEY32B, S_SKEYS, S_SURVIC,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
@@ -73,10 +73,8 @@ struct Side {
   bool groups = false;  // some image takes this side's labels
   bool arcs_primal = false, arcs_dual = false;      // by orientation
   bool groups_primal = false, groups_dual = false;
-  int* crit = nullptr;
   int* ext_img = nullptr;
-  float* val = nullptr;
-  const int2* key = nullptr;  // (value bits, cell) per extremum
+  const int2* key = nullptr;  // (value bits, global cell id) per extremum, list order
   int4* arc = nullptr;              // [nsad] per saddle (list order): arc ends and raw-arc cells
   int* rout = nullptr;              // [M] out rank of each extremum's thresholded root (-1: the void)
   int2* sv_t = nullptr;             // [nsurv] per survivor (output order): arc ends
@@ -459,15 +457,13 @@ void* staging(dmsc_b200_context* ctx, size_t bytes) {
 }
 
 // Sweep-ordered edges and the pairing arguments of one side (see pairing.cuh).
-PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const float* sval) {
+PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S) {
   const int nsad = ctx->nsad, M = S.M;
   S.dying = sget<int>(ctx, si, X_DYING, nsad);  // list order
   PairArgs A;
   A.nsad = nsad;
   A.M = M;
-  A.sval = sval;
-  A.sad_img = ctx->sad_img;
-  A.g12 = sget<int2>(ctx, si, X_G12, nsad);
+  A.rec = sget<int4>(ctx, si, X_G12, nsad);
   A.dying = S.dying;
   A.link = sget<int>(ctx, si, X_LINK, M + 1);
   A.minedge = sget<unsigned long long>(ctx, si, X_MINE, M + 1);
@@ -489,9 +485,9 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S, const float* sval
 }
 
 // Both sides' pairing rounds in one cooperative launch.
-void run_pairing(dmsc_b200_context* ctx, const float* sval, cudaStream_t st) {
+void run_pairing(dmsc_b200_context* ctx, cudaStream_t st) {
   PairArgs2 P;
-  for (int si = 0; si < 2; ++si) P.s[si] = pairing_args(ctx, si, ctx->side[si], sval);
+  for (int si = 0; si < 2; ++si) P.s[si] = pairing_args(ctx, si, ctx->side[si]);
   if (ctx->nsad > 0)
     coop_launch(ctx, ctx->pair_shape ? pairing_persistent_kernel<4, 4> : pairing_persistent_kernel<2, 5>, P, st,
                 "pairing_persistent_kernel", ctx->pair_per_sm);
@@ -515,7 +511,7 @@ void finish_pairing(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
   ReplayNode* node = S.arcs ? sget<ReplayNode>(ctx, si, X_NODE, M + 1) : nullptr;
   if (nsad > 0) {
     LK(persistence_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(
-        nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.dying, get<float>(ctx, S_SVAL, nsad), S.val,
+        nsad, !S.faces, ctx->I.dual, ctx->I.thr, ctx->sad_img, S.dying, get<float>(ctx, S_SVAL, nsad), S.key,
         S.pp, canc, (uint8_t)(S.faces ? 1 : 2), S.alive, ncanc, S.arc, cends, ctx->crit_sad, ckey,
         cval, node));
     LAUNCH_CHECK("persistence_kernel");
@@ -816,22 +812,15 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   ctx->nmax = nmax;
 
   // ---- K2 ordered compaction ----
-  int* cmin = get<int>(ctx, S_CMIN, nmin);
   int* csad = get<int>(ctx, S_CSAD, nsad);
-  int* cmax = get<int>(ctx, S_CMAX, nmax);
   int* imin = get<int>(ctx, S_IMIN, nmin);
   int* isad = get<int>(ctx, S_ISAD, nsad);
   int* imax = get<int>(ctx, S_IMAX, nmax);
   uint32_t* bmin = get<uint32_t>(ctx, S_MINBITS, nseg);  // per-segment bit masks of the extrema
   uint32_t* bmax = get<uint32_t>(ctx, S_MAXBITS, nseg);
-  float* vmin = get<float>(ctx, S_VMIN, nmin);
-  float* vmax = get<float>(ctx, S_VMAX, nmax);
-  int2* kmin = get<int2>(ctx, S_KMIN, nmin);  // (value bits, cell) records for the pairing
+  int2* kmin = get<int2>(ctx, S_KMIN, nmin);  // (value bits, cell): the extremum lists
   int2* kmax = get<int2>(ctx, S_KMAX, nmax);
   float* sval = get<float>(ctx, S_SVAL, nsad);
-  // sort keys: (image id << 32) | orderable(s_val), or the 32-bit value key alone for one image
-  unsigned long long* skey = B > 1 ? get<unsigned long long>(ctx, S_SKEY, nsad) : nullptr;
-  uint32_t* skey32 = B > 1 ? nullptr : get<uint32_t>(ctx, S_SKEY32, nsad);
   ctx->crit_sad = csad;
   ctx->sad_img = isad;
   // the pairing's starting state (side 0: faces / maxima, side 1: vertices /
@@ -845,12 +834,11 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     ps.minedge[si] = sget<unsigned long long>(ctx, si, X_MINE, M + 1);
     ps.link[si] = sget<int>(ctx, si, X_LINK, M + 1);
     ps.cnt[si] = sget<int>(ctx, si, X_CNT, 8);
-    ps.g12[si] = sget<int2>(ctx, si, X_G12, nsad);
+    ps.rec[si] = sget<int4>(ctx, si, X_G12, nsad);
     ps.dying[si] = sget<int>(ctx, si, X_DYING, nsad);
   }
   LK(compact_kernel<<<grid_for(nseg, 8 * kCompactSegs), 256, 0, st>>>(
-      I, img, nseg, flow, off[0], off[1], off[2], cmin, csad, cmax, imin, isad, imax, bmin, bmax, vmin, vmax, kmin,
-      kmax, sval, skey, skey32, ps));
+      I, img, nseg, flow, off[0], off[1], off[2], csad, imin, isad, imax, bmin, bmax, kmin, kmax, sval, ps));
   LAUNCH_CHECK("compact_kernel");
   // per-image bases of the critical lists (B + 1 entries each)
   int* bases = get<int>(ctx, S_BASES, 9 * (size_t)(B + 1));
@@ -888,12 +876,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   V.faces = false;
   F.M = nmax;
   V.M = nmin;
-  F.crit = cmax;
-  V.crit = cmin;
   F.ext_img = imax;
   V.ext_img = imin;
-  F.val = vmax;
-  V.val = vmin;
   F.key = kmax;
   V.key = kmin;
   F.arc = arc_f;
@@ -915,7 +899,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   uint8_t* canc = get<uint8_t>(ctx, S_CANC, nsad + 4);
   mark(ctx, 4, st);
   CK(cudaMemsetAsync(canc, 0, nsad + 4, st));
-  run_pairing(ctx, sval, st);
+  run_pairing(ctx, st);
   mark(ctx, 5, st);
   // the two sides' persistence, thresholded union-find and ranks are
   // independent (disjoint buffers; their cancellation bits are ORed into the
@@ -966,11 +950,13 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     int* sorted = get<int>(ctx, S_ASC, nsurv);
     if (B > 1) {
       unsigned long long* k = get<unsigned long long>(ctx, S_SKEY2, nsurv);
-      LK(survivor_gather_kernel<unsigned long long><<<grid_for(nsad, TB), TB, 0, ss>>>(nsad, flag, fpos, skey, k, sidx));
+      LK(survivor_gather_kernel<unsigned long long><<<grid_for(nsad, TB), TB, 0, ss>>>(
+          nsad, flag, fpos, get<float>(ctx, S_SVAL, nsad), ctx->sad_img, k, sidx));
       sort_pairs(ctx, k, get<unsigned long long>(ctx, S_SKEYS, nsurv), sidx, sorted, nsurv, ss, 32 + bits_for(B));
     } else {
       uint32_t* k = get<uint32_t>(ctx, S_SKEY32B, nsurv);
-      LK(survivor_gather_kernel<uint32_t><<<grid_for(nsad, TB), TB, 0, ss>>>(nsad, flag, fpos, skey32, k, sidx));
+      LK(survivor_gather_kernel<uint32_t><<<grid_for(nsad, TB), TB, 0, ss>>>(
+          nsad, flag, fpos, get<float>(ctx, S_SVAL, nsad), ctx->sad_img, k, sidx));
       sort_pairs(ctx, k, get<uint32_t>(ctx, S_SKEYS, nsurv), sidx, sorted, nsurv, ss, 32);
     }
     // the survivors in output order, with their records gathered once
@@ -1278,7 +1264,7 @@ int fetch_batch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStr
     Side& S = ctx->side[si];
     Route R{S.faces ? o->max_pts : o->min_pts, S.faces ? o->min_pts : o->max_pts, rt_of(si == 0 ? R_PTS0 : R_PTS1)};
     if (S.M > 0)
-      LK(points_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.alive, S.to_out_excl, ctx->bases.alive[si], S.crit,
+      LK(points_kernel<<<grid_for(S.M, TB), TB, 0, st>>>(S.M, S.alive, S.to_out_excl, ctx->bases.alive[si], S.key,
                                                          S.ext_img, I, R));
   }
   if (nsurv > 0 && o->sad_pts)
@@ -1365,7 +1351,7 @@ int fetch_pair_pixels_impl(dmsc_b200_context* ctx, int32_t* plus_max, int32_t* m
     Route PLUS{S.faces ? plus_max : plus_min, S.faces ? plus_min : plus_max, ctx->bases.surv};
     Route MINUS{S.faces ? minus_max : minus_min, S.faces ? minus_min : minus_max, ctx->bases.surv};
     LK(pair_pixels_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.faces, ctx->bases.surv, ctx->I, ctx->img,
-                                                              ctx->surv, ctx->crit_sad, S.pp, S.crit, PLUS,
+                                                              ctx->surv, ctx->crit_sad, S.pp, S.key, PLUS,
                                                               MINUS));
   }
   LAUNCH_CHECK("pair_pixels_kernel");

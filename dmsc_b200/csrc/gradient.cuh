@@ -731,25 +731,21 @@ __host__ __device__ __forceinline__ unsigned crit_bits(unsigned fl, bool vin) {
 // warp waits on one round of loads instead of three per segment; segment
 // offsets are exclusive scans of the per-segment counts over the whole batch
 // (images in order, rows in order), so each image's lists are a contiguous
-// slice in ascending cell-id order. Writes the three lists as global cell
-// ids, each critical cell's image, the per-segment bit masks of the minima
-// and maxima (an extremum's list rank is its segment's offset plus the
-// extrema before it in the mask), the extremum values (also as (value, cell)
-// records for the elder comparisons of the pairing) and the saddle values
-// with their sort keys (image id above the orderable value, so one sort
-// orders every image); and the pairing's starting state of the groups
-// (PairStart).
+// slice in ascending cell-id order. Writes the saddle list as global cell
+// ids with each saddle's image and value; each extremum's image and its
+// (value bits, global cell id) record (the extremum lists, read by the
+// elder comparisons of the pairing, the persistence pass and the outputs);
+// the per-segment bit masks of the minima and maxima (an extremum's list
+// rank is its segment's offset plus the extrema before it in the mask); and
+// the pairing's starting state of the groups (PairStart).
 constexpr int kCompactSegs = 2;
 
 static __global__ void __launch_bounds__(256) compact_kernel(
     Imgs I, const float* __restrict__ img_all, long long nseg, const uint8_t* __restrict__ flow,
     const int* __restrict__ off_min, const int* __restrict__ off_sad, const int* __restrict__ off_max,
-    int* __restrict__ crit_min, int* __restrict__ crit_sad, int* __restrict__ crit_max, int* __restrict__ min_img,
-    int* __restrict__ sad_img, int* __restrict__ max_img, uint32_t* __restrict__ min_bits,
-    uint32_t* __restrict__ max_bits,
-    float* __restrict__ min_val, float* __restrict__ max_val, int2* __restrict__ min_key, int2* __restrict__ max_key,
-    float* __restrict__ sad_val,
-    unsigned long long* __restrict__ sad_key, uint32_t* __restrict__ sad_key32, PairStart ps) {
+    int* __restrict__ crit_sad, int* __restrict__ min_img, int* __restrict__ sad_img, int* __restrict__ max_img,
+    uint32_t* __restrict__ min_bits, uint32_t* __restrict__ max_bits, int2* __restrict__ min_key,
+    int2* __restrict__ max_key, float* __restrict__ sad_val, PairStart ps) {
   constexpr int K = kCompactSegs;
   const int lane = threadIdx.x & 31;
   const long long seg0 = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * K;
@@ -815,18 +811,14 @@ static __global__ void __launch_bounds__(256) compact_kernel(
     int p = o_sad[k] + __popc(bh & lt) + __popc(bv & lt);
     if (m & 1u) {
       const int q = o_min[k] + __popc(bmin & lt);
-      crit_min[q] = (int)(4 * gidx);
       min_img[q] = bk;
-      min_val[q] = cv.v;
       min_key[q] = make_int2(__float_as_int(cv.v), (int)(4 * gidx));
       ps.minedge[1][q] = ~0ull;  // a single-extremum group without outgoing saddles yet
       ps.link[1][q] = q;
     }
     if (m & 8u) {
       const int q = o_max[k] + __popc(bmax & lt);
-      crit_max[q] = (int)(4 * gidx + 3);
       max_img[q] = bk;
-      max_val[q] = cv.f;
       max_key[q] = make_int2(__float_as_int(cv.f), (int)(4 * gidx + 3));
       ps.minedge[0][q] = ~0ull;
       ps.link[0][q] = q;
@@ -838,10 +830,6 @@ static __global__ void __launch_bounds__(256) compact_kernel(
       crit_sad[p] = (int)(4 * gidx + t);
       sad_img[p] = bk;
       sad_val[p] = v;
-      if (sad_key32)  // one image: the image id is 0, a 32-bit key suffices
-        sad_key32[p] = orderable_key(v);
-      else
-        sad_key[p] = ((unsigned long long)bk << 32) | orderable_key(v);
       p++;
     }
   }

@@ -67,7 +67,9 @@ __device__ __forceinline__ bool older(int a, int b, int void_id, const int2* __r
 // groups are still single extrema, so the ends are the groups): a saddle
 // whose two ends coincide is a cycle, the others record their ends' groups
 // and reduce their sweep key into both groups' minimum, and each block adds
-// the saddles that stay active to the side's round-1 counter.
+// the saddles that stay active to the side's round-1 counter. A saddle's
+// pairing record holds its ends' groups and its sweep key, so the later
+// rounds read one 16-byte record per saddle and need no value lookups.
 __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t* __restrict__ flow, int nsad,
                                                           const int* __restrict__ crit_sad,
                                                           const int* __restrict__ sad_img,
@@ -120,8 +122,8 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
         continue;
       }
       ps.dying[sd][s] = kUndecided;
-      ps.g12[sd][s] = make_int2(ga, gb);
       const unsigned long long k = sweep_key(v, s, sd == 0 ? !d : d);
+      ps.rec[sd][s] = make_int4(ga, gb, (int)(unsigned)k, (int)(unsigned)(k >> 32));
       atomicMin(ps.minedge[sd] + ga, k);  // result unused: a reduction
       atomicMin(ps.minedge[sd] + gb, k);
       keep[sd] = 1;
@@ -148,7 +150,7 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
                                                           const int* __restrict__ sad_img,
                                                           const int* __restrict__ dying,
                                                           const float* __restrict__ sad_val,
-                                                          const float* __restrict__ ext_val,
+                                                          const int2* __restrict__ ext_key,
                                                           int2* __restrict__ pp,
                                                           uint8_t* __restrict__ cancelled, uint8_t sbit,
                                                           uint8_t* __restrict__ alive, int* __restrict__ n_cancel,
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(256) persistence_kernel(int nsad, bool min_sid
     } else {
       const int b = sad_img[s];
       const bool du = dual[b];
-      float sv = sad_val[s], ev = ext_val[d];
+      float sv = sad_val[s], ev = __int_as_float(ext_key[d].x);
       if (min_side)
         p = du ? sub_like_host(ev, sv) : sub_like_host(sv, ev);
       else

@@ -88,7 +88,7 @@ __device__ __forceinline__ int value_pixel(const float* __restrict__ img_all, co
 __global__ void pair_pixels_kernel(int nsurv, bool faces, const int* __restrict__ surv_base, Imgs I,
                                    const float* __restrict__ img_all, const int* __restrict__ surv_sad,
                                    const int* __restrict__ crit_sad, const int2* __restrict__ pp,
-                                   const int* __restrict__ ext_cell, Route PLUS, Route MINUS) {
+                                   const int2* __restrict__ ext_key, Route PLUS, Route MINUS) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nsurv) return;
   int b;
@@ -100,7 +100,7 @@ __global__ void pair_pixels_kernel(int nsurv, bool faces, const int* __restrict_
   int plus = -1, minus = -1;
   if (e >= 0) {
     const int sp = value_pixel(img_all, I, b, crit_sad[s]);
-    const int ep = value_pixel(img_all, I, b, ext_cell[e]);
+    const int ep = value_pixel(img_all, I, b, ext_key[e].y);
     const bool saddle_plus = (!faces) != d;
     plus = saddle_plus ? sp : ep;
     minus = saddle_plus ? ep : sp;
