@@ -130,9 +130,9 @@ struct PairStart {
   unsigned long long* minedge[2];  // [M + 1] smallest sweep key of each group's outgoing saddles
   int* link[2];                    // [M + 1] group union-find
   int* cnt[2];                     // [6] rotating active-saddle and live-root counters
-  int4* rec[2];                    // [nsad] each saddle's {group of end 0, group of end 1, sweep key (lo, hi)}
+  int2* g12[2];                    // [nsad] groups of each saddle's two ends
   int* dying[2];                   // [nsad] decision of each saddle
-  const float* sval;               // [nsad] saddle values (for the sweep keys)
+  const float* sval;               // [nsad] saddle values
 };
 
 // Largest b with base[b] <= g (the image holding global item g).

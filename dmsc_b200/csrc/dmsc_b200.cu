@@ -463,7 +463,9 @@ PairArgs pairing_args(dmsc_b200_context* ctx, int si, Side& S) {
   PairArgs A;
   A.nsad = nsad;
   A.M = M;
-  A.rec = sget<int4>(ctx, si, X_G12, nsad);
+  A.sval = get<float>(ctx, S_SVAL, nsad);
+  A.sad_img = ctx->sad_img;
+  A.g12 = sget<int2>(ctx, si, X_G12, nsad);
   A.dying = S.dying;
   A.link = sget<int>(ctx, si, X_LINK, M + 1);
   A.minedge = sget<unsigned long long>(ctx, si, X_MINE, M + 1);
@@ -834,7 +836,7 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     ps.minedge[si] = sget<unsigned long long>(ctx, si, X_MINE, M + 1);
     ps.link[si] = sget<int>(ctx, si, X_LINK, M + 1);
     ps.cnt[si] = sget<int>(ctx, si, X_CNT, 8);
-    ps.rec[si] = sget<int4>(ctx, si, X_G12, nsad);
+    ps.g12[si] = sget<int2>(ctx, si, X_G12, nsad);
     ps.dying[si] = sget<int>(ctx, si, X_DYING, nsad);
   }
   LK(compact_kernel<<<grid_for(nseg, 8 * kCompactSegs), 256, 0, st>>>(

@@ -67,9 +67,7 @@ __device__ __forceinline__ bool older(int a, int b, int void_id, const int2* __r
 // groups are still single extrema, so the ends are the groups): a saddle
 // whose two ends coincide is a cycle, the others record their ends' groups
 // and reduce their sweep key into both groups' minimum, and each block adds
-// the saddles that stay active to the side's round-1 counter. A saddle's
-// pairing record holds its ends' groups and its sweep key, so the later
-// rounds read one 16-byte record per saddle and need no value lookups.
+// the saddles that stay active to the side's round-1 counter.
 __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t* __restrict__ flow, int nsad,
                                                           const int* __restrict__ crit_sad,
                                                           const int* __restrict__ sad_img,
@@ -122,8 +120,8 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
         continue;
       }
       ps.dying[sd][s] = kUndecided;
+      ps.g12[sd][s] = make_int2(ga, gb);
       const unsigned long long k = sweep_key(v, s, sd == 0 ? !d : d);
-      ps.rec[sd][s] = make_int4(ga, gb, (int)(unsigned)k, (int)(unsigned)(k >> 32));
       atomicMin(ps.minedge[sd] + ga, k);  // result unused: a reduction
       atomicMin(ps.minedge[sd] + gb, k);
       keep[sd] = 1;

@@ -117,9 +117,9 @@ struct PairArgs {
   // saddles are indexed in list order (ascending cell id); a saddle's sweep
   // key (sweep_key) orders the saddles of its image in this side's sweep
   // and is the atomicMin key, so no sorted copy of the saddles is needed
-  // [nsad] groups of the two ends, as of the saddle's last active round, and
-  // the saddle's sweep key (lo, hi), written by the saddle walks
-  int4* rec;
+  const float* sval;  // [nsad] saddle values
+  const int* sad_img; // [nsad] image of each saddle
+  int2* g12;          // [nsad] groups of the two ends, as of the saddle's last active round
   int* dying;
   int* link;                    // [M+1] group union-find
   unsigned long long* minedge;  // [M+1] smallest sweep key of the group's active saddles
@@ -177,7 +177,8 @@ template <int U>
 __device__ __forceinline__ void pair_batch_a(const PairArgs2& P, int r, long long i0, long long cend, int n0,
                                              bool scan, bool lists, ChunkLists& L) {
   int e[U], ga[U], gb[U];
-  unsigned act = 0, s1m = 0;
+  float sv[U];
+  unsigned act = 0, s1m = 0, du = 0;
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     const long long i = i0 + 256LL * u;
@@ -190,21 +191,18 @@ __device__ __forceinline__ void pair_batch_a(const PairArgs2& P, int r, long lon
       e[u] = scan ? (int)j : ((r & 1) ? PSIDE(act1) : PSIDE(act0))[j];
     }
   }
-  // the saddle's state, ends and sweep key, all issued together
+  // the saddle's state, ends and key value, all issued together
   int dy[U];
-  unsigned long long kk[U];
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     dy[u] = kUndecided;
     ga[u] = gb[u] = 0;
-    kk[u] = 0;
     if (!((act >> u) & 1u)) continue;
     const bool s1 = (s1m >> u) & 1u;
     dy[u] = PSIDE(dying)[e[u]];
-    const int4 g = PSIDE(rec)[e[u]];  // the ends' groups of the previous round, the key
+    const int2 g = PSIDE(g12)[e[u]];  // the ends' groups of the previous round
     ga[u] = g.x;
     gb[u] = g.y;
-    kk[u] = ((unsigned long long)(unsigned)g.w << 32) | (unsigned)g.z;
   }
 #pragma unroll
   for (int u = 0; u < U; ++u)
@@ -248,6 +246,16 @@ __device__ __forceinline__ void pair_batch_a(const PairArgs2& P, int r, long lon
       }
     }
   }
+  // key values (loaded after the finds: fewer registers live across them)
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    sv[u] = 0.f;
+    if (!((act >> u) & 1u) || ga[u] == gb[u]) continue;
+    const bool s1 = (s1m >> u) & 1u;
+    sv[u] = PSIDE(sval)[e[u]];
+    const bool d = P.s[0].dual[P.s[0].B > 1 ? P.s[0].sad_img[e[u]] : 0];
+    du |= (unsigned)(s1 ? d : !d) << u;  // descending sweep: faces in the primal, vertices in the dual
+  }
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     if (!((act >> u) & 1u)) continue;
@@ -256,9 +264,10 @@ __device__ __forceinline__ void pair_batch_a(const PairArgs2& P, int r, long lon
       PSIDE(dying)[e[u]] = -1;
       continue;
     }
-    *reinterpret_cast<int2*>(PSIDE(rec) + e[u]) = make_int2(ga[u], gb[u]);
-    atomicMin(PSIDE(minedge) + ga[u], kk[u]);  // result unused: a reduction
-    atomicMin(PSIDE(minedge) + gb[u], kk[u]);
+    PSIDE(g12)[e[u]] = make_int2(ga[u], gb[u]);
+    const unsigned long long k = sweep_key(sv[u], e[u], (du >> u) & 1u);
+    atomicMin(PSIDE(minedge) + ga[u], k);  // result unused: a reduction
+    atomicMin(PSIDE(minedge) + gb[u], k);
     if (lists)
       chunk_keep(L, s1, e[u]);
     else
@@ -330,7 +339,7 @@ __device__ __forceinline__ void pair_batch_b(const PairArgs2& P, int r, long lon
     h[u] = 0;
     if (!((act >> u) & 1u)) continue;
     const bool s1 = (s1m >> u) & 1u;
-    const int2 gg = *reinterpret_cast<const int2*>(PSIDE(rec) + e[u]);  // roots as of phase A
+    const int2 gg = PSIDE(g12)[e[u]];  // roots as of phase A
     h[u] = gg.x == g[u] ? gg.y : gg.x;
   }
   int2 kh[U];
