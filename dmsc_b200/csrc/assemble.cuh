@@ -102,22 +102,19 @@ __global__ void survivor_order_kernel(int n, const int* __restrict__ sorted, con
 
 // Per-survivor records of one side gathered once in output (sweep) order, so
 // the later per-survivor kernels read them in order instead of gathering
-// from the list-ordered saddle arrays again: its arc ends, raw-arc lengths,
-// raw-arc path words and the record of its outputs (out ranks of its ends' thresholded roots,
+// from the list-ordered saddle arrays again: its arc ends, raw-arc lengths
+// and the record of its outputs (out ranks of its ends' thresholded roots,
 // persistence, out rank of its pair's root; -1 for the void).
 __global__ void surv_side_kernel(int nsurv, const int* __restrict__ surv, const int4* __restrict__ arc,
-                                 const ulonglong2* __restrict__ path, const int2* __restrict__ pp,
-                                 const int* __restrict__ rout, int2* __restrict__ sv_t, longlong2* __restrict__ sv_len,
-                                 ulonglong2* __restrict__ sv_path, int4* __restrict__ sv_rec) {
+                                 const int2* __restrict__ pp, const int* __restrict__ rout, int2* __restrict__ sv_t,
+                                 longlong2* __restrict__ sv_len, int4* __restrict__ sv_rec) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsurv) return;
   const int s = surv[i];
   const int4 a = arc[s];
   const int2 pr = pp[s];
-  const ulonglong2 pw = path[s];
   sv_t[i] = make_int2(a.x, a.y);
   sv_len[i] = make_longlong2(a.z, a.w);
-  sv_path[i] = pw;
   sv_rec[i] = make_int4(a.x >= 0 ? rout[a.x] : -1, a.y >= 0 ? rout[a.y] : -1, pr.y, pr.x >= 0 ? rout[pr.x] : -1);
 }
 

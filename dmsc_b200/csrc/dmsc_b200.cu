@@ -40,12 +40,12 @@ namespace {
 enum Slot {
   S_MASK, S_FLOW, S_SEG0, S_SEG1, S_SEG2, S_OFF0, S_OFF1, S_OFF2, S_TOT, S_TAB, S_BASES,
   S_CSAD, S_IMIN, S_ISAD, S_IMAX, S_MINBITS, S_MAXBITS, S_KMIN, S_KMAX, S_SVAL, S_SKEY2, S_IOTA,
-  S_ASC, S_ARCF, S_ARCV, S_PATHF, S_PATHV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
+  S_ASC, S_ARCF, S_ARCV, S_CANC, S_FLAG, S_FPOS, S_SURV, S_STATUS, S_NCANC, S_STATS, S_TIMELINE, S_ROUTE,
   S_BKEY, S_BIDX, S_BKEY2, S_BIDX2, S_PERF, S_PERV, S_EXF, S_EXV, S_NEX, S_SKEY32B, S_SKEYS, S_SURVIC,
   S_SIDE0,  // per-side slots start here, kSideSlots each
 };
 enum SideSlot {
-  X_ROUT, X_SVT, X_SVL, X_SVP, X_SVR, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_ALIVE,
+  X_ROUT, X_SVT, X_SVL, X_SVR, X_DYING, X_GRP, X_LINK, X_MINE, X_ACT0, X_ACT1, X_CNT, X_PAIR, X_ALIVE,
   X_ALIVEI, X_TOOUTX, X_TOOUT, X_UF, X_CROOT, X_CKEY, X_CVAL, X_NODE,
   X_ALEN, X_ACL, X_AROOT, X_PLEN, X_SEND, X_APOS, X_EROWC, X_EROWO, X_Q0, X_Q1, X_QB, X_G12,
   X_GBASE, X_WX, X_WA, X_CENDS, kSideSlots
@@ -76,11 +76,9 @@ struct Side {
   int* ext_img = nullptr;
   const int2* key = nullptr;  // (value bits, global cell id) per extremum, list order
   int4* arc = nullptr;              // [nsad] per saddle (list order): arc ends and raw-arc cells
-  const ulonglong2* path = nullptr; // [nsad] per saddle (list order): the two raw arcs' path words
   int* rout = nullptr;              // [M] out rank of each extremum's thresholded root (-1: the void)
   int2* sv_t = nullptr;             // [nsurv] per survivor (output order): arc ends
   longlong2* sv_len = nullptr;      // raw-arc lengths
-  ulonglong2* sv_path = nullptr;    // raw-arc path words
   int4* sv_rec = nullptr;           // out ranks of the ends' roots, persistence, out rank of the pair's root
   int* dying = nullptr;
   int2* pp = nullptr;               // [nsad] paired extremum (-1: none) and persistence bits
@@ -563,6 +561,7 @@ ReplayArgs replay_prepare(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t 
   A.dying = S.dying;
   A.arc = S.arc;
   A.alive = S.alive;
+  A.crit_sad = ctx->crit_sad;
   A.S = R;
   A.max_steps = nsad + 1;
   A.act0 = sget<int>(ctx, si, X_ACT0, nsad);
@@ -864,13 +863,9 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   // per saddle and side: arc ends and raw-arc lengths (cells)
   int4* arc_f = get<int4>(ctx, S_ARCF, nsad);
   int4* arc_v = get<int4>(ctx, S_ARCV, nsad);
-  // per saddle and side: the two raw arcs' path words (first 32 step directions)
-  ulonglong2* path_f = get<ulonglong2>(ctx, S_PATHF, nsad);
-  ulonglong2* path_v = get<ulonglong2>(ctx, S_PATHV, nsad);
   if (nsad > 0) {
     LK(saddle_walk_kernel<<<grid_for(nsad, TB), TB, 0, st>>>(I, flow, nsad, csad, isad, off[2], bmax, off[0], bmin,
-                                                             arc_f, arc_v, path_f, path_v, ncells, ps,
-                                                             ctx->status));
+                                                             arc_f, arc_v, ncells, ps, ctx->status));
     LAUNCH_CHECK("saddle_walk_kernel");
   }
 
@@ -889,8 +884,6 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   V.key = kmin;
   F.arc = arc_f;
   V.arc = arc_v;
-  F.path = path_f;
-  V.path = path_v;
   // faces: ridges/peaks in the primal, valleys/basins in the dual (workspace.hxx:322-362)
   F.arcs_primal = f_ridges;
   F.arcs_dual = f_valleys;
@@ -978,9 +971,8 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
       S.sv_t = sget<int2>(ctx, si, X_SVT, nsurv);
       S.sv_len = sget<longlong2>(ctx, si, X_SVL, nsurv);
       S.sv_rec = sget<int4>(ctx, si, X_SVR, nsurv);
-      S.sv_path = sget<ulonglong2>(ctx, si, X_SVP, nsurv);
-      LK(surv_side_kernel<<<grid_for(nsurv, TB), TB, 0, ss>>>(nsurv, ctx->surv, S.arc, S.path, S.pp, S.rout,
-                                                            S.sv_t, S.sv_len, S.sv_path, S.sv_rec));
+      LK(surv_side_kernel<<<grid_for(nsurv, TB), TB, 0, ss>>>(nsurv, ctx->surv, S.arc, S.pp,
+                                                            S.rout, S.sv_t, S.sv_len, S.sv_rec));
     }
     LAUNCH_CHECK("survivor records");
   }
@@ -1183,9 +1175,6 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   EmitArgs A;
   EmitCtx& E = A.E;
   E.flow = ctx->flow;
-  E.crit_sad = ctx->crit_sad;
-  E.path = S.path;
-  E.sv_path = S.sv_path;
   E.I = ctx->I;
   E.faces = S.faces;
   E.S = S.R;

@@ -63,8 +63,7 @@ __device__ __forceinline__ bool older(int a, int b, int void_id, const int2* __r
 
 // K4: per saddle, both face walks and the vertex walks. Writes per saddle and
 // side one record {target 0, target 1, cells 0, cells 1}: each arc's dense
-// target index (or -1) and its raw arc's cell count, and the two arcs' path
-// words (walks.cuh); then runs the pairing's round-0 saddle phase for both sides (all
+// target index (or -1) and its raw arc's cell count; then runs the pairing's round-0 saddle phase for both sides (all
 // groups are still single extrema, so the ends are the groups): a saddle
 // whose two ends coincide is a cycle, the others record their ends' groups
 // and reduce their sweep key into both groups' minimum, and each block adds
@@ -77,9 +76,7 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
                                                           const int* __restrict__ off_min,
                                                           const uint32_t* __restrict__ min_bits,
                                                           int4* __restrict__ arc_f, int4* __restrict__ arc_v,
-                                                          ulonglong2* __restrict__ path_f,
-                                                          ulonglong2* __restrict__ path_v, long long cap,
-                                                          PairStart ps, unsigned* status) {
+                                                          long long cap, PairStart ps, unsigned* status) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   int keep[2] = {0, 0};
   if (s < nsad) {
@@ -87,11 +84,10 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
     const int H = I.H[b], W = I.W[b], Nx = W + 1;
     const int sc = crit_sad[s];
     int te[2][2], len[2][2];
-    unsigned long long pw[2][2];
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       long long steps;
-      const int end = flow_walk<4>(flow, face_start(sc, j, Nx) >> 2, Nx, cap, &steps, &pw[0][j], status);
+      const int end = flow_walk<4>(flow, face_start(sc, j, Nx) >> 2, Nx, cap, &steps, status);
       const int target = seg_rank(I, b, end, Nx, off_max, max_bits);
       te[0][j] = target;
       len[0][j] = target >= 0 ? (int)steps + 1 : 0;  // cells of the raw arc, start and end included
@@ -101,9 +97,8 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
       const int start = vertex_start(sc, j, H, W, Nx, I.idx_base[b]);
       long long steps = 0;
       int target = -1;
-      pw[1][j] = 0;
       if (start >= 0) {
-        const int end = flow_walk<0>(flow, start >> 2, Nx, cap, &steps, &pw[1][j], status);
+        const int end = flow_walk<0>(flow, start >> 2, Nx, cap, &steps, status);
         target = seg_rank(I, b, end, Nx, off_min, min_bits);
       }
       te[1][j] = target;
@@ -112,8 +107,6 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
     // a raw arc has fewer cells than the batch (cell ids are int32)
     arc_f[s] = make_int4(te[0][0], te[0][1], len[0][0], len[0][1]);
     arc_v[s] = make_int4(te[1][0], te[1][1], len[1][0], len[1][1]);
-    path_f[s] = make_ulonglong2(pw[0][0], pw[0][1]);
-    path_v[s] = make_ulonglong2(pw[1][0], pw[1][1]);
     // round 0 of the pairing: descending sweep on the face side in the
     // primal and the vertex side in the dual
     const bool d = I.dual[b];

@@ -483,6 +483,7 @@ struct ReplayArgs {
   const int* dying;  // [nsad] in saddle list order
   const int4* arc;   // [nsad] {end 0, end 1, raw-arc cells 0, raw-arc cells 1} of each saddle, list order
   const uint8_t* alive;  // [M] extrema that no cancellation kills (their records are never read)
+  const int* crit_sad;   // [nsad] global cell id of each saddle
   ReplayState S;
   int max_steps;
   int* act0;
@@ -651,7 +652,7 @@ __device__ __forceinline__ void replay_batch(const ReplayArgs2& P, int rd, long 
       // this round's tag, so the order of these stores does not matter
       *reinterpret_cast<int4*>(&node[dd].status) =
           make_int4(status_word(kLinked, rd), k == 0 ? R1 : R0,
-                    side_word(k, (a0 > 0) + (a1 > 0), (bl.x > 0) + (bl.y > 0)), s);
+                    side_word(k, (a0 > 0) + (a1 > 0), (bl.x > 0) + (bl.y > 0)), RSIDE(crit_sad)[s]);
     } else {
       node[dd].status = status_word(kRootForever, rd);
     }
@@ -871,7 +872,7 @@ __device__ __forceinline__ void emit_batch(const EmitCtx& E, int4* __restrict__ 
     for (int u = 0; u < U; ++u) {
       if (!((live >> u) & 1u)) continue;
       // W(z) = reverse(chain(Tk -> z)) + reverse(arc k) + arc o + chain(To -> R)
-      const int d = z[u], k = side_of(w[u].z), s = w[u].w, R = w[u].y;  // s: the saddle (list index)
+      const int d = z[u], k = side_of(w[u].z), s = w[u].w, R = w[u].y;  // s: the saddle's cell
       const int Tk = te[u].x, To = te[u].y;
       const long long la = cl[u].x, lb = te[u].z, lc = te[u].w, ld = cl[u].y;
       const bool rv = (rev >> u) & 1u;
@@ -1031,20 +1032,14 @@ __global__ void __launch_bounds__(256) emit_segments_kernel(EmitCtx E, const int
 #pragma unroll
         for (int q = 0; q < NC; ++q) {  // all loads first: independent chains overlap
           f[q] = 0;
-          // the first kPathSteps steps come from the path word, no load
-          if (c[q].rem > 1 && c[q].n >= kPathSteps) f[q] = __ldg(E.flow + c[q].idx);
+          if (c[q].rem > 1) f[q] = __ldg(E.flow + c[q].idx);
         }
 #pragma unroll
         for (int q = 0; q < NC; ++q) {
           if (c[q].rem <= 0) continue;
           *c[q].dst = type + 4 * (c[q].idx - c[q].ibase);
           c[q].dst += c[q].step;
-          if (--c[q].rem > 0) {
-            const unsigned code = c[q].n < kPathSteps ? (unsigned)(c[q].pw >> (2 * c[q].n)) % 4u + 1u
-                                                      : (f[q] >> shift) & 7u;
-            c[q].idx += flow_step(code, c[q].Nx);
-            ++c[q].n;
-          }
+          if (--c[q].rem > 0) c[q].idx += flow_step((f[q] >> shift) & 7u, c[q].Nx);
         }
       }
     }

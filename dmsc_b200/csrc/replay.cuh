@@ -44,7 +44,7 @@ __device__ __forceinline__ int status_word(int kind, int round) { return kind | 
 
 // A replay node in one 64-byte line: everything a chain walk reads, in the
 // first 32-byte sector as two 16-byte halves, (ctime, wlen) and (status,
-// parent, side, saddle); in the second, what the emission needs to expand
+// parent, side, saddle cell); in the second, what the emission needs to expand
 // W(node) without touching the saddle's arrays: the two chain lengths, the
 // saddle's arc ends on the dying and the other side and their raw-arc
 // lengths (written at link time).
@@ -54,7 +54,7 @@ struct alignas(64) ReplayNode {
   int status;                // kPending / kLinked / kRootForever, with the deciding round's tag
   int parent;                // link target (-1 = void) when kLinked
   int side;                  // side_word: dying side of the node's cancellation and what W(node) expands to
-  int csad;                  // saddle (list index) of the node's cancellation
+  int scell;                 // global cell id of the saddle of the node's cancellation
   long long cl_dy;           // chain length T_dying -> node at link time
   long long cl_ot;           // chain length T_other -> parent at link time
   int t_dy, t_ot;            // the saddle's arc ends on the dying and the other side
@@ -167,8 +167,6 @@ __device__ __forceinline__ int4 make_task(int kind, int rev, int a, int b, long 
 
 struct EmitCtx {
   const uint8_t* flow;
-  const int* crit_sad;      // [nsad] global cell id of each saddle
-  const ulonglong2* path;   // [nsad] the path words of each saddle's two raw arcs (this side)
   Imgs I;
   bool faces;
   ReplayState S;
@@ -183,36 +181,32 @@ struct EmitCtx {
   const int2* surv_ic;       // [nsurv] image and cell of each survivor (output order)
   const int2* sv_t;          // [nsurv] this side's arc ends
   const longlong2* sv_len;   // [nsurv] this side's raw-arc lengths
-  const ulonglong2* sv_path; // [nsurv] this side's raw-arc path words
   const long long* arc_pos;  // [2 nsurv] output position of each arc
   int max_steps;
   unsigned* status;
 };
 
 // A raw-arc segment task of the chain expansion: {reversed | arc << 1,
-// saddle (list index), cells, output position}: the writer loads the
-// saddle's cell and the arc's path word together and derives the rest.
+// saddle cell, cells, output position}: the writer finds the arc's start
+// cell from the saddle's cell with no further load.
 __device__ __forceinline__ int arc_start_of_cell(const EmitCtx& E, int sc, int j, int b) {
   const int W = E.I.W[b], Nx = W + 1;
   const int cell = E.faces ? face_start(sc, j, Nx) : vertex_start(sc, j, E.I.H[b], W, Nx, E.I.idx_base[b]);
   return cell >> 2;
 }
-__device__ __forceinline__ int4 make_saddle_seg(int s, int j, int rev, long long len, long long pos) {
-  return make_int4(rev | (j << 1), s, (int)len, (int)pos);
+__device__ __forceinline__ int4 make_saddle_seg(int scell, int j, int rev, long long len, long long pos) {
+  return make_int4(rev | (j << 1), scell, (int)len, (int)pos);
 }
 
 // A raw arc being written by one lane: the V-path from its start cell, `len`
-// cells (cpu/arcs_geometry.hxx:83-111, 133-161): its first kPathSteps steps
-// from the arc's path word, any further ones from the flow codes. dst is the
-// next output slot, step its stride (-1 for a reversed arc), rem the cells
-// left, idx the current index and n the steps taken.
+// cells (cpu/arcs_geometry.hxx:83-111, 133-161), following the flow codes.
+// dst is the next output slot, step its stride (-1 for a reversed arc), rem
+// the cells left and idx the current index.
 struct SegCursor {
   int* dst;
   int step;
   int rem;
   int idx, ibase, Nx;
-  int n;
-  unsigned long long pw;
 };
 
 // Starts segment item q: q < nvirt is raw arc (q / 2, q % 2) of a survivor,
@@ -230,23 +224,18 @@ __device__ __forceinline__ void seg_start(const EmitCtx& E, long long q, SegCurs
     len = (int)(j ? bl.y : bl.x);
     if ((j ? tt.y : tt.x) < 0 || len <= 0) return;
     const int2 ic = E.surv_ic[i];
-    const ulonglong2 pw = E.sv_path[i];
     b = ic.x;
     idx = arc_start_of_cell(E, ic.y, j, b);
     pos = (int)E.arc_pos[q];
     rev = false;
-    c.pw = j ? pw.y : pw.x;
   } else {
     const int4 t = E.base_q[q - E.nvirt];
     const int j = (t.x >> 1) & 1;
-    const int sc = E.crit_sad[t.y];
-    const ulonglong2 pw = E.path[t.y];
     len = t.z;
-    b = find_image(E.I.idx_base, E.I.B, sc >> 2);
-    idx = arc_start_of_cell(E, sc, j, b);
+    b = find_image(E.I.idx_base, E.I.B, t.y >> 2);
+    idx = arc_start_of_cell(E, t.y, j, b);
     pos = t.w;
     rev = t.x & 1;
-    c.pw = j ? pw.y : pw.x;
   }
   int* out = E.I.dual[b] ? E.out_dual : E.out_primal;
   if (!out || len <= 0) return;
@@ -256,7 +245,6 @@ __device__ __forceinline__ void seg_start(const EmitCtx& E, long long q, SegCurs
   c.dst = out + (rev ? (long long)pos + len - 1 : (long long)pos);
   c.step = rev ? -1 : 1;
   c.rem = len;
-  c.n = 0;
 }
 
 }  // namespace dmsc

@@ -38,30 +38,21 @@ __device__ __forceinline__ int vertex_start(int s_cell, int j, int H, int W, int
   return j < n ? v[j] : -1;
 }
 
-// A raw arc's path word: the directions (flow code - 1: left, right, up,
-// down) of its first kPathSteps steps, two bits each from the low end, so
-// its cells follow from its start index with no flow-code load.
-constexpr int kPathSteps = 32;
-
 // Walks from index `idx` along the flow codes (nibble shift 0 = vertices,
-// 4 = faces) to the index of the critical cell; counts the steps and records
-// the path word.
+// 4 = faces) to the index of the critical cell; counts the steps.
 template <int SHIFT>
 __device__ __forceinline__ int flow_walk(const uint8_t* __restrict__ flow, int idx, int Nx, long long cap,
-                                         long long* steps, unsigned long long* path, unsigned* status) {
+                                         long long* steps, unsigned* status) {
   long long n = 0;
-  unsigned long long pw = 0;
   unsigned c;
   while ((c = (__ldg(flow + idx) >> SHIFT) & 7u) != kFlowNone) {
     idx += flow_step(c, Nx);
-    if (n < kPathSteps) pw |= (unsigned long long)(c - 1u) << (2 * n);
     if (++n > cap) {
       set_status(status, kStatusWalkCap);
       break;
     }
   }
   *steps = n;
-  *path = pw;
   return idx;
 }
 
