@@ -23,6 +23,7 @@ EXPORTS = (
     "dmsc_b200_fetch",
     "dmsc_b200_set_host_outputs",
     "dmsc_b200_set_host_fetch_outputs",
+    "dmsc_b200_set_host_input",
     "dmsc_b200_extract_batch",
     "dmsc_b200_fetch_pair_pixels",
     "dmsc_b200_scatter_pair_grads",
@@ -94,6 +95,8 @@ def load():
         lib.dmsc_b200_fetch.restype = ctypes.c_int
         lib.dmsc_b200_set_host_outputs.argtypes = [ctypes.c_void_p] * 4
         lib.dmsc_b200_set_host_outputs.restype = ctypes.c_int
+        lib.dmsc_b200_set_host_input.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.dmsc_b200_set_host_input.restype = ctypes.c_int
         lib.dmsc_b200_set_host_fetch_outputs.argtypes = [ctypes.c_void_p, ctypes.POINTER(Outputs)]
         lib.dmsc_b200_set_host_fetch_outputs.restype = ctypes.c_int
         lib.dmsc_b200_extract_batch.argtypes = [

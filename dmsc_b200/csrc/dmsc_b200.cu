@@ -102,6 +102,7 @@ struct Side {
 }  // namespace
 
 constexpr int kStageMarks = 17;
+constexpr int kInBands = 8;  // row bands of an image uploaded from a host source
 
 struct dmsc_b200_context {
   int device = 0;
@@ -152,6 +153,11 @@ struct dmsc_b200_context {
   cudaStream_t side_st = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   cudaEvent_t copy_ev = nullptr;
+  // pinned host source of the next extract's image (dmsc_b200_set_host_input),
+  // uploaded in bands of rows on in_st; in_ev[k]: band k's rows have arrived
+  const float* host_img = nullptr;
+  cudaStream_t in_st = nullptr;
+  cudaEvent_t in_ev[kInBands] = {};
   // readback area: pinned host memory mapped into the device address space;
   // a small kernel writes the values, so readbacks never queue behind bulk
   // device-to-host copies on the copy engines
@@ -378,6 +384,7 @@ void join_copies(dmsc_b200_context* ctx, cudaStream_t st) {
 // written after the call returns, and forget the registered destinations.
 void abandon_copies(dmsc_b200_context* ctx) {
   if (ctx->copy_st) cudaStreamSynchronize(ctx->copy_st);
+  if (ctx->in_st) cudaStreamSynchronize(ctx->in_st);  // uploads from a host image source
   ctx->copies_pending = false;
   ctx->host_grad = ctx->host_peaks = ctx->host_basins = nullptr;
   ctx->host_fetch_set = false;
@@ -610,9 +617,15 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // The TMA-staged persistent gradient of one H x W image (tile TY x 32, NT
 // threads); false when it does not apply (rows not 16-byte multiples, an
 // unaligned buffer, no encoder), and the caller runs the batch kernel.
+// With a host source (`host_img`, pinned) the image is uploaded into `img`
+// in kInBands bands of rows on in_st, and each band of tile rows is launched
+// as soon as the rows its value windows read have arrived; with a host
+// gradient destination (`host_grad`), each band's gradient rows are copied
+// back as soon as the band is done, so the upload overlaps the downloads.
 template <int TY, int NT>
 bool launch_gradient_tma(dmsc_b200_context* ctx, int H, int W, bool dual, const float* img, int4* grad,
-                         int* const* seg, uint8_t* flow, cudaStream_t st) {
+                         int* const* seg, uint8_t* flow, cudaStream_t st, const float* host_img,
+                         int32_t* host_grad) {
   if (W % 4 != 0 || (reinterpret_cast<uintptr_t>(img) & 15u) != 0) return false;
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   if (!enc) return false;
@@ -632,24 +645,64 @@ bool launch_gradient_tma(dmsc_b200_context* ctx, int H, int W, bool dual, const 
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, NT, kSmem));
   const int ntx = (W + 1 + kTileX - 1) / kTileX, nty = (H + 1 + TY - 1) / TY;
   const long long ntiles = (long long)ntx * nty;
-  const int grid = (int)std::min<long long>(ntiles, (long long)std::max(1, per) * ctx->num_sms);
-  LK((kernel<<<grid, NT, kSmem, st>>>(map, H, W, ntx, (int)ntiles, grad, flow, seg[0], seg[1], seg[2], ctx->fifo_lut,
-                                      ctx->status)));
-  LAUNCH_CHECK("gradient_tma_kernel");
+  const long long resident = (long long)std::max(1, per) * ctx->num_sms;
+  auto launch = [&](long long t0, long long t1) {  // tiles [t0, t1): whole tile rows
+    const int grid = (int)std::min<long long>(t1 - t0, resident);
+    LK((kernel<<<grid, NT, kSmem, st>>>(map, H, W, ntx, (int)t0, (int)t1, grad, flow, seg[0], seg[1], seg[2],
+                                        ctx->fifo_lut, ctx->status)));
+    LAUNCH_CHECK("gradient_tma_kernel");
+  };
+  if (!host_img) {
+    launch(0, ntiles);
+    if (host_grad && grad) copy_out_async(ctx, host_grad, grad, 16 * (size_t)(H + 1) * (W + 1), st);
+    return true;
+  }
+  // the device buffer's earlier users on st come first
+  CK(cudaEventRecord(ctx->in_ev[0], st));
+  CK(cudaStreamWaitEvent(ctx->in_st, ctx->in_ev[0], 0));
+  float* dimg = const_cast<float*>(img);
+  const int nb = std::min(kInBands, nty);
+  long long rows_in = 0;
+  for (int k = 0; k < nb; ++k) {
+    const long long r0 = (long long)nty * k / nb, r1 = (long long)nty * (k + 1) / nb;  // tile rows
+    // a tile's value window reads image rows y0 - 2 .. y0 + TY (y0 = its
+    // first index row); rows outside the image read as zero fill
+    const long long need = std::min<long long>(H, r1 * TY + 1);
+    if (need > rows_in)
+      CK(cudaMemcpyAsync(dimg + rows_in * W, host_img + rows_in * W, (size_t)(need - rows_in) * W * sizeof(float),
+                         cudaMemcpyHostToDevice, ctx->in_st));
+    rows_in = std::max(rows_in, need);
+    CK(cudaEventRecord(ctx->in_ev[k], ctx->in_st));
+    CK(cudaStreamWaitEvent(st, ctx->in_ev[k], 0));
+    launch(r0 * ntx, r1 * ntx);
+    if (host_grad && grad) {  // the band's index rows r0 TY .. min(H + 1, r1 TY) - 1
+      const long long i0 = r0 * TY, i1 = std::min<long long>(H + 1, r1 * TY);
+      if (i1 > i0)
+        copy_out_async(ctx, host_grad + i0 * (W + 1) * 4, grad + i0 * (W + 1), 16 * (size_t)(i1 - i0) * (W + 1), st);
+    }
+  }
   return true;
 }
 
 // Gradient kernel of tile shape `shape` over `ntile` tiles of the batch (a
-// TMA shape on a one-image batch runs the persistent kernel when it applies).
-void launch_gradient(dmsc_b200_context* ctx, int shape, unsigned ntile, const Imgs& I, const float* img, int4* grad,
+// TMA shape on a one-image batch runs the persistent kernel when it applies),
+// with the image's upload from `host_img` (one image; nullptr: the image is
+// on the device); true when it also issued the gradient's copy to
+// `host_grad` (the persistent kernel copies it band by band), false when
+// the caller copies it after the kernel.
+bool launch_gradient(dmsc_b200_context* ctx, int shape, unsigned ntile, const Imgs& I, const float* img, int4* grad,
                      uint8_t* mask, int* const* seg, uint8_t* flow, cudaStream_t st, int B, int H0, int W0,
-                     bool dual0) {
+                     bool dual0, const float* host_img, int32_t* host_grad) {
   if (kGradTma[shape] && B == 1 && !mask) {
-    const bool done =
-        shape == 3 ? launch_gradient_tma<kGradTY[3], kGradNT[3]>(ctx, H0, W0, dual0, img, grad, seg, flow, st)
-                   : launch_gradient_tma<kGradTY[4], kGradNT[4]>(ctx, H0, W0, dual0, img, grad, seg, flow, st);
-    if (done) return;
+    const bool done = shape == 3 ? launch_gradient_tma<kGradTY[3], kGradNT[3]>(ctx, H0, W0, dual0, img, grad, seg,
+                                                                                flow, st, host_img, host_grad)
+                                 : launch_gradient_tma<kGradTY[4], kGradNT[4]>(ctx, H0, W0, dual0, img, grad, seg,
+                                                                                flow, st, host_img, host_grad);
+    if (done) return true;
   }
+  if (host_img)  // the whole image first
+    CK(cudaMemcpyAsync(const_cast<float*>(img), host_img, (size_t)H0 * W0 * sizeof(float), cudaMemcpyHostToDevice,
+                       st));
   switch (kGradTY[shape]) {
     case kGradTY[0]:
       LK((gradient_batch_kernel<kGradTY[0], kGradNT[0]><<<ntile, kGradNT[0], 0, st>>>(I, img, grad, mask, seg[0], seg[1],
@@ -665,6 +718,7 @@ void launch_gradient(dmsc_b200_context* ctx, int shape, unsigned ntile, const Im
       break;
   }
   LAUNCH_CHECK("gradient_batch_kernel");
+  return false;
 }
 
 // Number of bits needed for values 0 .. n-1 (at least 1).
@@ -678,6 +732,12 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
                        const float* hthr, const unsigned char* hdual, unsigned flags, int32_t* grad_out,
                        int32_t* peaks_out, int32_t* basins_out, dmsc_b200_sizes* sizes_out, cudaStream_t st) {
   ctx->valid = false;
+  const float* host_img = ctx->host_img;  // the registration covers this call only
+  ctx->host_img = nullptr;
+  if (host_img && B != 1) {
+    set_err(ctx, "a host image source takes one image");
+    return kErrInvalidArgument;
+  }
   if (!img || B <= 0 || !hH || !hW || !hthr || !hdual || !sizes_out) {
     set_err(ctx, "invalid argument");
     return kErrInvalidArgument;
@@ -799,10 +859,11 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   int* seg[3] = {get<int>(ctx, S_SEG0, nseg), get<int>(ctx, S_SEG1, nseg), get<int>(ctx, S_SEG2, nseg)};
   int* off[3] = {get<int>(ctx, S_OFF0, nseg), get<int>(ctx, S_OFF1, nseg), get<int>(ctx, S_OFF2, nseg)};
   mark(ctx, 15, st);  // the gradient stage times the kernel alone
-  launch_gradient(ctx, gshape, (unsigned)ntile, I, img, (int4*)grad, nullptr, seg, flow, st, B, hH[0], hW[0],
-                  hdual[0] != 0);
+  const bool grad_copied = launch_gradient(ctx, gshape, (unsigned)ntile, I, img, (int4*)grad, nullptr, seg, flow, st,
+                                           B, hH[0], hW[0], hdual[0] != 0, host_img,
+                                           ret_grad ? ctx->host_grad : nullptr);
   mark(ctx, 1, st);
-  if (ret_grad) copy_out_async(ctx, ctx->host_grad, grad, 16 * (size_t)nidx, st);
+  if (ret_grad && !grad_copied) copy_out_async(ctx, ctx->host_grad, grad, 16 * (size_t)nidx, st);
   for (int k = 0; k < 3; ++k) excl_sum(ctx, seg[k], off[k], (int)nseg, st);
   long long* tot = get<long long>(ctx, S_TOT, 8);
   LK(totals3_kernel<<<1, 1, 0, st>>>(off[0], seg[0], off[1], seg[1], off[2], seg[2], nseg, tot));
@@ -1408,10 +1469,16 @@ int dmsc_b200_create(dmsc_b200_context** out, int device) {
       cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->side_st, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->in_st, cudaStreamNonBlocking) != cudaSuccess) {
     dmsc_b200_destroy(c);
     return kErrCuda;
   }
+  for (int k = 0; k < kInBands; ++k)
+    if (cudaEventCreateWithFlags(&c->in_ev[k], cudaEventDisableTiming) != cudaSuccess) {
+      dmsc_b200_destroy(c);
+      return kErrCuda;
+    }
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
   {
     std::vector<uint32_t> lut(kGradTable);
@@ -1452,6 +1519,12 @@ void dmsc_b200_destroy(dmsc_b200_context* c) {
     cudaStreamDestroy(c->copy_st);
   }
   if (c->copy_ev) cudaEventDestroy(c->copy_ev);
+  if (c->in_st) {
+    cudaStreamSynchronize(c->in_st);
+    cudaStreamDestroy(c->in_st);
+  }
+  for (int k = 0; k < kInBands; ++k)
+    if (c->in_ev[k]) cudaEventDestroy(c->in_ev[k]);
   for (int k = 0; k < kStageMarks; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   delete c;
@@ -1491,6 +1564,12 @@ int dmsc_b200_set_host_fetch_outputs(dmsc_b200_context* ctx, const dmsc_b200_out
   return kOk;
 }
 
+int dmsc_b200_set_host_input(dmsc_b200_context* ctx, const float* host_image) {
+  if (!ctx) return kErrInvalidArgument;
+  ctx->host_img = host_image;
+  return kOk;
+}
+
 int dmsc_b200_set_host_outputs(dmsc_b200_context* ctx, int32_t* grad_host, int32_t* peaks_host,
                                int32_t* basins_host) {
   if (!ctx) return kErrInvalidArgument;
@@ -1505,6 +1584,11 @@ int dmsc_b200_extract_batch(dmsc_b200_context* ctx, const float* images, int B, 
                             int32_t* peaks_out, int32_t* basins_out, dmsc_b200_sizes* sizes, void* stream) {
   if (!ctx) return kErrInvalidArgument;
   ctx->err.clear();
+  if (ctx->host_img) {  // a host image source covers one single-image extract only
+    ctx->host_img = nullptr;
+    set_err(ctx, "dmsc_b200_set_host_input applies to dmsc_b200_extract only");
+    return kErrInvalidArgument;
+  }
   try {
     return extract_batch_impl(ctx, B, images, H, W, thresholds, is_dual, flags, grad_out, peaks_out, basins_out,
                               sizes, (cudaStream_t)stream);

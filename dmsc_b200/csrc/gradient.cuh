@@ -517,7 +517,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, uint3
 
 template <bool DUAL, int TY, int NT>
 __global__ void __launch_bounds__(NT) gradient_tma_kernel(const __grid_constant__ CUtensorMap map, int H, int W,
-                                                          int ntx, int ntiles, int4* __restrict__ grad,
+                                                          int ntx, int tile0, int ntiles, int4* __restrict__ grad,
                                                           uint8_t* __restrict__ flow, int* __restrict__ seg_min,
                                                           int* __restrict__ seg_sad, int* __restrict__ seg_max,
                                                           const uint32_t* __restrict__ lut, unsigned* status) {
@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(NT) gradient_tma_kernel(const __grid_constant_
     mbar_fence_init();
   }
   __syncthreads();
-  int t = blockIdx.x;
+  int t = tile0 + blockIdx.x;  // tiles tile0 .. ntiles - 1 (a band of tile rows, or all)
   if (threadIdx.x == 0 && t < ntiles) {
     const int ty = t / ntx, tx = t - ty * ntx;
     mbar_arrive_expect_tx(&S.bar[0], kBytes);

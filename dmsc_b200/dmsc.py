@@ -206,13 +206,16 @@ def _host_like(t):
 
 
 def extract_single(img: torch.Tensor, persistence_threshold: float, flags: int, stream=None,
-                   host_fixed: bool = False) -> tuple:
+                   host_fixed: bool = False, host_src: torch.Tensor | None = None) -> tuple:
     """One contiguous float32 [H, W] CUDA image through both C-ABI phases;
     returns the 19 output tensors on the image's device (shape on the CPU).
     With ``host_fixed`` the gradient and label maps are returned in pinned
     host tensors that the library fills while the rest of the call runs
     (``dmsc_b200_set_host_outputs``); they are complete once the stream has
-    passed the call."""
+    passed the call. With ``host_src`` (a pinned host copy of the image)
+    ``img`` is only the device destination: the library uploads the image
+    itself, overlapped with the gradient (``dmsc_b200_set_host_input``);
+    ``host_src`` must stay unchanged until the stream has passed the call."""
     H, W = int(img.shape[0]), int(img.shape[1])
     dev = img.device
     ctx = _lib.context(dev.index if dev.index is not None else torch.cuda.current_device())
@@ -228,6 +231,8 @@ def extract_single(img: torch.Tensor, persistence_threshold: float, flags: int, 
         hg, hp, hb = _host_like(grad), _host_like(peaks), _host_like(basins)
         ctx.check(ctx.lib.dmsc_b200_set_host_outputs(ctx.h, _ptr(hg), _ptr(hp), _ptr(hb)),
                   "dmsc_b200_set_host_outputs")
+    if host_src is not None:
+        ctx.check(ctx.lib.dmsc_b200_set_host_input(ctx.h, _ptr(host_src)), "dmsc_b200_set_host_input")
     sz = _lib.Sizes()
     rc = ctx.lib.dmsc_b200_extract(ctx.h, ctypes.c_void_p(img.data_ptr()), H, W, ctypes.c_float(persistence_threshold),
                                    flags, _ptr(grad), _ptr(peaks), _ptr(basins), ctypes.byref(sz),
@@ -417,13 +422,21 @@ def extract_dmsc(scalar_field, persistence_threshold, return_gradient=False, is_
         raise RuntimeError("dmsc_b200 requires a CUDA device; there is no CPU compute path")
     on_cpu = scalar_field.device.type != "cuda"
     flags = _flags(return_gradient, is_dual, trace_max_arcs, trace_min_arcs, trace_max_groups, trace_min_groups)
+    host_src = None
     if on_cpu:
-        x = scalar_field.contiguous().to("cuda", non_blocking=True)
+        xh = scalar_field.contiguous()
+        if xh.dim() == 2 and xh.is_pinned():
+            # the library uploads the pinned image in bands of rows, each
+            # band's gradient starting as soon as its rows have arrived
+            host_src = xh
+            x = torch.empty(xh.shape, dtype=torch.float32, device="cuda")
+        else:
+            x = xh.to("cuda", non_blocking=True)
     else:
         x = scalar_field.contiguous()
     with torch.cuda.device(x.device):
         if x.dim() == 2:
-            res = extract_single(x, persistence_threshold, flags, host_fixed=on_cpu)
+            res = extract_single(x, persistence_threshold, flags, host_fixed=on_cpu, host_src=host_src)
             return _to_host(res) if on_cpu else res
         n = x.shape[0]
         return _extract_many(list(x.unbind(0)), [persistence_threshold] * n, [is_dual] * n, flags, on_cpu)

@@ -133,6 +133,20 @@ int dmsc_b200_set_host_outputs(dmsc_b200_context* ctx, int32_t* grad_host, int32
    has passed that fetch. The registration covers one fetch call. */
 int dmsc_b200_set_host_fetch_outputs(dmsc_b200_context* ctx, const dmsc_b200_outputs* host);
 
+/* Optional host source of the image of the next dmsc_b200_extract() on this
+   context (no counterpart in the reference, whose CUDA path takes a device
+   tensor): `host_image` is a pinned host buffer of H x W float32 values. The
+   extract copies it into its `image` argument, which is then a device
+   buffer of H x W floats that the call only writes, in bands of rows on an
+   internal stream, and starts each band's gradient tiles (and, with
+   dmsc_b200_set_host_outputs, the copy of their gradient back to the host)
+   as soon as the rows they read have arrived, so the upload overlaps the
+   downloads. `host_image` must stay unchanged until the caller's stream has
+   passed the extract. NULL clears it; the registration covers one extract
+   call and is not allowed before dmsc_b200_extract_batch (returns
+   DMSC_B200_ERR_INVALID_ARGUMENT there). */
+int dmsc_b200_set_host_input(dmsc_b200_context* ctx, const float* host_image);
+
 /* Phase 1 for a batch of B images of independent sizes, thresholds and
    orientations, computed together (one pass of every stage over the union
    of the images). Replaces the reference's per-image loop over a 3-D batch

@@ -113,6 +113,32 @@ def test_cpu_input_returns_cpu_outputs(oracle_mod):
     assert diff_fields(list(ms), exp) == []
 
 
+@pytest.mark.parametrize("shape", [(1000, 1024), (333, 518), (40, 64)])
+@pytest.mark.parametrize("dual", [False, True])
+def test_pinned_cpu_input_uploaded_in_bands(shape, dual):
+    """A pinned CPU image is uploaded by the library in bands of rows that
+    overlap the gradient (dmsc_b200_set_host_input): every output equals the
+    call on the same image already on the device. Widths that are multiples
+    of 4 take the banded persistent gradient (1000 rows: 8 bands; 40 rows:
+    fewer tile rows than bands); 518 columns take the one-copy fallback."""
+    from dmsc_b200 import compute_dmsc
+    from dmsc_b200.synthetic import field_256_bumps
+
+    g = torch.Generator().manual_seed(5)
+    base = field_256_bumps(seed=11)
+    img = torch.nn.functional.interpolate(base[None, None], size=shape, mode="bilinear", align_corners=False)[0, 0]
+    img = (img + 0.01 * torch.randn(shape, generator=g)).contiguous()
+    host = img.pin_memory()
+    assert host.is_pinned()
+    exp = compute_dmsc(img.cuda(), 0.02, is_dual=dual)
+    got = compute_dmsc(host, 0.02, is_dual=dual)
+    assert all(t.device.type == "cpu" for t in got)
+    assert diff_fields(list(got), [t.cpu() for t in exp]) == []
+    # the registration covers one call: the next device call is unaffected
+    again = compute_dmsc(img.cuda(), 0.02, is_dual=dual)
+    assert diff_fields([t.cpu() for t in again], [t.cpu() for t in exp]) == []
+
+
 def test_output_devices():
     from dmsc_b200 import compute_dmsc
 
