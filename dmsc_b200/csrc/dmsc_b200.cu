@@ -1004,6 +1004,28 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
   // and the labels (neither reads them); the final arcs wait for them
   cudaStream_t ss = ctx->side_st;
   CK(cudaEventRecord(ctx->fork_ev, st));
+  mark(ctx, 7, st);
+
+  // ---- replay (both sides in one cooperative launch) ----
+  {
+    ReplayArgs2 RA{};
+    bool any = false;
+    for (int si = 0; si < 2; ++si) {
+      Side& S = ctx->side[si];
+      RA.s[si].status = ctx->status;
+      if (S.arcs && nsad > 0) {
+        RA.s[si] = replay_prepare(ctx, si, S, st);
+        any = any || RA.s[si].n_cancel != nullptr;
+      }
+    }
+    if (any)
+      coop_launch(ctx, ctx->replay_shape ? replay_persistent_kernel<2, 3> : replay_persistent_kernel<1, 4>, RA, st,
+                  "replay_persistent_kernel", ctx->replay_per_sm);
+    mark(ctx, 8, st);
+  }
+
+  // the survivors' side-stream work is enqueued after the replay's launch,
+  // so the device starts the replay while the host sets up the sort
   CK(cudaStreamWaitEvent(ss, ctx->fork_ev, 0));
   if (nsurv > 0) {
     // the survivors (list order) sorted by (image, s_val) with the list index
@@ -1038,25 +1060,6 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
     LAUNCH_CHECK("survivor records");
   }
   CK(cudaEventRecord(ctx->join_ev, ss));
-  mark(ctx, 7, st);
-
-  // ---- replay (both sides in one cooperative launch) ----
-  {
-    ReplayArgs2 RA{};
-    bool any = false;
-    for (int si = 0; si < 2; ++si) {
-      Side& S = ctx->side[si];
-      RA.s[si].status = ctx->status;
-      if (S.arcs && nsad > 0) {
-        RA.s[si] = replay_prepare(ctx, si, S, st);
-        any = any || RA.s[si].n_cancel != nullptr;
-      }
-    }
-    if (any)
-      coop_launch(ctx, ctx->replay_shape ? replay_persistent_kernel<2, 3> : replay_persistent_kernel<1, 4>, RA, st,
-                  "replay_persistent_kernel", ctx->replay_per_sm);
-    mark(ctx, 8, st);
-  }
 
   // ---- labels (region id = rank among the image's alive extrema) ----
   LabelOut OF{}, OV{};
