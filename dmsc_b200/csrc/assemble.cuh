@@ -227,18 +227,26 @@ __global__ void geom_base_kernel(int B, const int* __restrict__ surv_base, int n
   gbase[b] = f < nsurv ? saddle_end_incl[f] - plen[f] : *total;
 }
 
+// Image-local output position of every arc (its start inside its image's
+// geometry of this side), for the geometry expansion and writer.
+__global__ void arc_pos_kernel(int nsurv, const long long* __restrict__ arc_len,
+                               const long long* __restrict__ saddle_end_incl, const int2* __restrict__ surv_ic,
+                               const long long* __restrict__ gbase, long long* __restrict__ arc_pos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsurv) return;
+  const longlong2 al = *reinterpret_cast<const longlong2*>(arc_len + 2 * i);
+  const long long start = saddle_end_incl[i] - gbase[surv_ic[i].x] - al.x - al.y;
+  *reinterpret_cast<longlong2*>(arc_pos + 2 * i) = make_longlong2(start, start + al.x);
+}
+
 // CSR offsets of one side's arcs, per image (cpu/workspace.hxx:247-287):
 // offsets[0] = 0, offsets[k+1] = end of survivor k, arc_offsets[k] = end of
 // its first arc, image-local. `off_off[b]` / `arc_off[b]` place image b's
-// block (n_b + 1 and n_b entries) in the routed arrays. With `arc_pos`, also
-// the output position of every arc for the geometry writer: the image's
-// destination offset (`dst_off`) plus the arc's position inside the image's
-// geometry.
+// block (n_b + 1 and n_b entries) in the routed arrays.
 __global__ void arc_offsets_kernel(int nsurv, int B, const int* __restrict__ surv_base, const uint8_t* __restrict__ dual,
                                    const long long* __restrict__ arc_len,
                                    const long long* __restrict__ saddle_end_incl, const long long* __restrict__ gbase,
-                                   Route OFF, Route AOFF, const int* __restrict__ dst_off,
-                                   long long* __restrict__ arc_pos) {
+                                   Route OFF, Route AOFF) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsurv + B) return;
   if (i >= nsurv) {  // one leading zero per image
@@ -254,10 +262,6 @@ __global__ void arc_offsets_kernel(int nsurv, int B, const int* __restrict__ sur
   int li = i - surv_base[b];
   if (int* o = OFF.at(d, b)) o[li + 1] = (int)end;
   if (int* a = AOFF.at(d, b)) a[li] = (int)(start + al.x);
-  if (arc_pos) {
-    const long long p = start + dst_off[b];
-    *reinterpret_cast<longlong2*>(arc_pos + 2 * i) = make_longlong2(p, p + al.x);
-  }
 }
 
 }  // namespace dmsc

@@ -101,7 +101,7 @@ struct Side {
 
 }  // namespace
 
-constexpr int kStageMarks = 17;
+constexpr int kStageMarks = 19;
 constexpr int kInBands = 8;  // row bands of an image uploaded from a host source
 
 struct dmsc_b200_context {
@@ -138,6 +138,10 @@ struct dmsc_b200_context {
   uint32_t* fifo_lut = nullptr;  // face-pairing FIFO table (device)
   int num_sms = 0;
   cudaEvent_t ev[kStageMarks] = {};
+  // each side's geometry expansion, launched at the end of extract; the
+  // writer in fetch reads its segment list (expanded: launched this call)
+  EmitArgs emit[2] = {};
+  bool expanded[2] = {false, false};
   cudaEvent_t sync_ev = nullptr;   // polled by wait_stream
   // host destinations of the fixed-size outputs for the next extract (copied
   // on copy_st as soon as each is produced; see dmsc_b200_set_host_outputs)
@@ -728,6 +732,8 @@ int bits_for(int n) {
   return b;
 }
 
+void emit_expand(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st);
+
 int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const int* hH, const int* hW,
                        const float* hthr, const unsigned char* hdual, unsigned flags, int32_t* grad_out,
                        int32_t* peaks_out, int32_t* basins_out, dmsc_b200_sizes* sizes_out, cudaStream_t st) {
@@ -1220,30 +1226,34 @@ int extract_batch_impl(dmsc_b200_context* ctx, int B, const float* img, const in
       sizes_out[b] = z;
     }
   }
+  // the geometry's chain expansion needs no output buffer: it runs now,
+  // while the caller allocates the outputs of the fetch
+  mark(ctx, 17, st);
+  for (int si = 0; si < 2; ++si) emit_expand(ctx, si, ctx->side[si], st);
+  mark(ctx, 18, st);
   ctx->valid = true;
   return kOk;
 }
 
-// Geometry of one side: positions, CSR offsets and the expansion kernels.
-void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, int32_t* flat_dual, const int* dst_off,
-               Route OFF, Route AOFF, cudaStream_t st) {
-  const int nsurv = ctx->nsurv, B = ctx->B;
-  // the arcs' output positions only when geometry is written
-  const bool geom = S.total > 0 && (flat_primal || flat_dual);
-  long long* arc_pos = geom ? sget<long long>(ctx, si, X_APOS, 2 * (size_t)nsurv) : nullptr;
-  LK(arc_offsets_kernel<<<grid_for(nsurv + (long long)B, TB), TB, 0, st>>>(
-      nsurv, B, ctx->bases.surv, ctx->I.dual, S.arc_len, S.send, S.gbase, OFF, AOFF, dst_off, arc_pos));
-  LAUNCH_CHECK("arc_offsets_kernel");
-  if (!geom) return;
-  long long cap = S.total;
-  EmitArgs A;
+// Geometry of one side, first half (end of extract, before the caller has
+// allocated the outputs): the arcs' image-local positions and the
+// breadth-first chain expansion into the segment list. The writer runs in
+// fetch (emit_write); the device runs this while the host allocates.
+void emit_expand(dmsc_b200_context* ctx, int si, Side& S, cudaStream_t st) {
+  const int nsurv = ctx->nsurv;
+  ctx->expanded[si] = false;
+  if (!S.arcs || S.total <= 0 || nsurv <= 0) return;
+  long long* arc_pos = sget<long long>(ctx, si, X_APOS, 2 * (size_t)nsurv);
+  LK(arc_pos_kernel<<<grid_for(nsurv, TB), TB, 0, st>>>(nsurv, S.arc_len, S.send, ctx->surv_ic, S.gbase, arc_pos));
+  LAUNCH_CHECK("arc_pos_kernel");
+  const long long cap = S.total;
+  EmitArgs& A = ctx->emit[si];
+  A = EmitArgs{};
   EmitCtx& E = A.E;
   E.flow = ctx->flow;
   E.I = ctx->I;
   E.faces = S.faces;
   E.S = S.R;
-  E.out_primal = flat_primal;
-  E.out_dual = flat_dual;
   E.q_cap = cap;
   E.max_steps = ctx->nsad + 1;
   E.status = ctx->status;
@@ -1265,17 +1275,33 @@ void emit_side(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, in
   A.timeline = get<unsigned long long>(ctx, S_TIMELINE, kTimelineSlots) + (2 + si) * kTimeline;
   coop_launch(ctx, ctx->emit_shape ? emit_persistent_kernel<2, 3> : emit_persistent_kernel<1, 5>, A, st,
               "emit_persistent_kernel", ctx->emit_per_sm);
-  {
-    int per = 0;
-    if (ctx->seg_cursors == 1) {
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel<1>, 256, 0));
-      LK(emit_segments_kernel<1><<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3));
-    } else {
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel<2>, 256, 0));
-      LK(emit_segments_kernel<2><<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3));
-    }
-    LAUNCH_CHECK("emit_segments_kernel");
+  ctx->expanded[si] = true;
+}
+
+// Geometry of one side, second half (fetch): the CSR offsets and the writer
+// of every raw-arc segment into the caller's arrays (`dst_off[b]`: image b's
+// start in its destination).
+void emit_write(dmsc_b200_context* ctx, int si, Side& S, int32_t* flat_primal, int32_t* flat_dual, const int* dst_off,
+                Route OFF, Route AOFF, cudaStream_t st) {
+  const int nsurv = ctx->nsurv, B = ctx->B;
+  LK(arc_offsets_kernel<<<grid_for(nsurv + (long long)B, TB), TB, 0, st>>>(nsurv, B, ctx->bases.surv, ctx->I.dual,
+                                                                           S.arc_len, S.send, S.gbase, OFF, AOFF));
+  LAUNCH_CHECK("arc_offsets_kernel");
+  if (!ctx->expanded[si] || (!flat_primal && !flat_dual)) return;
+  EmitArgs& A = ctx->emit[si];
+  EmitCtx E = A.E;
+  E.out_primal = flat_primal;
+  E.out_dual = flat_dual;
+  E.dst_off = dst_off;
+  int per = 0;
+  if (ctx->seg_cursors == 1) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel<1>, 256, 0));
+    LK(emit_segments_kernel<1><<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3));
+  } else {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emit_segments_kernel<2>, 256, 0));
+    LK(emit_segments_kernel<2><<<dim3(per * ctx->num_sms * 4), 256, 0, st>>>(E, A.cnt + 3));
   }
+  LAUNCH_CHECK("emit_segments_kernel");
 }
 
 int fetch_batch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStream_t st) {
@@ -1390,7 +1416,7 @@ int fetch_batch_impl(dmsc_b200_context* ctx, const dmsc_b200_outputs* o, cudaStr
       OFF.dual = nullptr;
       AOFF.dual = nullptr;
     }
-    emit_side(ctx, si, S, gp, gd, rt_of(si == 0 ? R_G0 : R_G1), OFF, AOFF, st);
+    emit_write(ctx, si, S, gp, gd, rt_of(si == 0 ? R_G0 : R_G1), OFF, AOFF, st);
   }
   mark(ctx, 14, st);
   if (ctx->host_fetch_set)
@@ -1654,7 +1680,8 @@ int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n) {
   // extract stages are marks 0, 15, 1, 2, 4..8, 16, 10, 9, 11 in stream
   // order (15: just before the gradient kernel, 16: just before the label
   // kernels; the labels run before the final arcs; mark 3 is not recorded),
-  // fetch stages 12..14
+  // fetch stages 12..14; the geometry stage adds the expansion at the end of
+  // extract (marks 17, 18) to the writer in fetch (13, 14)
   static const int from[] = {0, 15, 1, 2, 4, 5, 6, 7, 10, 8, 16, 9, 12, 13};
   static const int to[] = {15, 1, 2, 4, 5, 6, 7, 8, 9, 16, 10, 11, 13, 14};
   const int ns = (int)(sizeof(from) / sizeof(from[0]));
@@ -1662,6 +1689,10 @@ int dmsc_b200_stage_times(dmsc_b200_context* ctx, float* ms, int n) {
   for (int k = 0; k < ns && k < n; ++k) {
     float t = 0.f;
     if (cudaEventElapsedTime(&t, ctx->ev[from[k]], ctx->ev[to[k]]) != cudaSuccess) t = -1.f;
+    if (k == ns - 1 && t >= 0.f) {
+      float e = 0.f;
+      if (cudaEventElapsedTime(&e, ctx->ev[17], ctx->ev[18]) == cudaSuccess) t += e;
+    }
     ms[k] = t;
   }
   return ns;

@@ -172,6 +172,7 @@ struct EmitCtx {
   ReplayState S;
   int* out_primal;  // destination of primal images' arcs of this side
   int* out_dual;    // destination of dual images' arcs
+  const int* dst_off;  // [B] start of each image's geometry in its destination (positions are image-local)
   long long q_cap;
   int4* base_q;  // raw-arc segments of the chain expansion
   long long base_cap;
@@ -181,7 +182,7 @@ struct EmitCtx {
   const int2* surv_ic;       // [nsurv] image and cell of each survivor (output order)
   const int2* sv_t;          // [nsurv] this side's arc ends
   const longlong2* sv_len;   // [nsurv] this side's raw-arc lengths
-  const long long* arc_pos;  // [2 nsurv] output position of each arc
+  const long long* arc_pos;  // [2 nsurv] image-local output position of each arc
   int max_steps;
   unsigned* status;
 };
@@ -242,7 +243,7 @@ __device__ __forceinline__ void seg_start(const EmitCtx& E, long long q, SegCurs
   c.Nx = E.I.W[b] + 1;
   c.ibase = E.I.idx_base[b];
   c.idx = idx;
-  c.dst = out + (rev ? (long long)pos + len - 1 : (long long)pos);
+  c.dst = out + E.dst_off[b] + (rev ? (long long)pos + len - 1 : (long long)pos);
   c.step = rev ? -1 : 1;
   c.rem = len;
 }

@@ -208,7 +208,9 @@ const char* dmsc_b200_last_error(const dmsc_b200_context* ctx);
    4 pairing (both sides), 5 persistence, cancellation and output ranks,
    6 survivors (flags and counts), 7 replay (both sides), 8 final arcs, 9 label
    set-up (per-extremum labels, bases), 10 labels (the label kernels alone),
-   11 sizes, 12 fetch lists, 13 fetch geometry. The survivors' sweep order
+   11 sizes, 12 fetch lists, 13 geometry (the chain expansion, which runs at
+   the end of extract() while the caller allocates the outputs, plus the
+   writer in fetch()). The survivors' sweep order
    and records are computed on a second stream while the replay and the
    labels run (the labels run before the final arcs); the final-arcs stage
    includes the wait for them. */
