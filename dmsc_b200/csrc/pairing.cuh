@@ -68,12 +68,6 @@ __device__ __forceinline__ bool older(int a, int b, int void_id, const int2* __r
 // whose two ends coincide is a cycle, the others record their ends' groups
 // and reduce their sweep key into both groups' minimum, and each block adds
 // the saddles that stay active to the side's round-1 counter.
-// The walks of a warp's 32 saddles (4 each: both face walks, then both
-// vertex walks) are handed out to its lanes as they finish, every
-// kWalkWindow steps: a warp then runs about the mean of its 128 walk
-// lengths per lane instead of, for each of the 4 walks, its longest one.
-constexpr int kWalkWindow = 4;
-
 __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t* __restrict__ flow, int nsad,
                                                           const int* __restrict__ crit_sad,
                                                           const int* __restrict__ sad_img,
@@ -83,85 +77,34 @@ __global__ void __launch_bounds__(256) saddle_walk_kernel(Imgs I, const uint8_t*
                                                           const uint32_t* __restrict__ min_bits,
                                                           int4* __restrict__ arc_f, int4* __restrict__ arc_v,
                                                           long long cap, PairStart ps, unsigned* status) {
-  __shared__ int w_start[8][128];  // start index of walk q = 32 j + lane (-1: no walk)
-  __shared__ int w_nx[8][32];      // row pitch of each lane's image
-  __shared__ int2 w_res[8][128];   // (end index, steps) of walk q
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned lt = (1u << lane) - 1u;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = s < nsad;
-  int b = 0, Nx = 1, sc = 0;
-  if (valid) {
-    b = sad_img[s];
-    const int H = I.H[b], W = I.W[b];
-    Nx = W + 1;
-    sc = crit_sad[s];
-    w_start[warp][lane] = face_start(sc, 0, Nx) >> 2;
-    w_start[warp][32 + lane] = face_start(sc, 1, Nx) >> 2;
-    const int v0 = vertex_start(sc, 0, H, W, Nx, I.idx_base[b]);
-    const int v1 = vertex_start(sc, 1, H, W, Nx, I.idx_base[b]);
-    w_start[warp][64 + lane] = v0 >= 0 ? v0 >> 2 : -1;
-    w_start[warp][96 + lane] = v1 >= 0 ? v1 >> 2 : -1;
-  } else {
-#pragma unroll
-    for (int j = 0; j < 4; ++j) w_start[warp][32 * j + lane] = -1;
-  }
-  w_nx[warp][lane] = Nx;
-  __syncwarp();
-  {
-    int q = -1, idx = 0, n = 0, step_nx = 1;
-    unsigned shift = 0;
-    int next = 0;  // first walk of the warp not yet handed out (same in every lane)
-    while (true) {
-      const unsigned idle = __ballot_sync(0xffffffffu, q < 0);
-      if (q < 0) {
-        const int my = next + __popc(idle & lt);
-        if (my < 128) {
-          const int st = w_start[warp][my];
-          if (st < 0) {
-            w_res[warp][my] = make_int2(-1, 0);  // an arc that leaves the image: no walk
-          } else {
-            q = my;
-            idx = st;
-            n = 0;
-            shift = my < 64 ? 4u : 0u;  // faces, then vertices
-            step_nx = w_nx[warp][my & 31];
-          }
-        }
-      }
-      next += __popc(idle);
-      if (next >= 128 && __ballot_sync(0xffffffffu, q >= 0) == 0) break;
-#pragma unroll 1
-      for (int k = 0; k < kWalkWindow && q >= 0; ++k) {
-        const unsigned c = (__ldg(flow + idx) >> shift) & 7u;
-        if (c == kFlowNone) {
-          w_res[warp][q] = make_int2(idx, n);
-          q = -1;
-        } else {
-          idx += flow_step(c, step_nx);
-          if (++n > cap) {
-            set_status(status, kStatusWalkCap);
-            w_res[warp][q] = make_int2(idx, n);
-            q = -1;
-          }
-        }
-      }
-    }
-  }
-  __syncwarp();
   int keep[2] = {0, 0};
-  if (valid) {
+  if (s < nsad) {
+    const int b = sad_img[s];
+    const int H = I.H[b], W = I.W[b], Nx = W + 1;
+    const int sc = crit_sad[s];
     int te[2][2], len[2][2];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int2 r = w_res[warp][32 * j + lane];
-      const int sd = j >> 1, jj = j & 1;
-      const int target = r.x < 0 ? -1 : seg_rank(I, b, r.x, Nx, sd ? off_min : off_max, sd ? min_bits : max_bits);
-      te[sd][jj] = target;
-      // cells of the raw arc, start and end included; an arc that leaves
-      // the image is empty (a raw arc has fewer cells than the batch)
-      len[sd][jj] = target >= 0 ? r.y + 1 : 0;
+    for (int j = 0; j < 2; ++j) {
+      long long steps;
+      const int end = flow_walk<4>(flow, face_start(sc, j, Nx) >> 2, Nx, cap, &steps, status);
+      const int target = seg_rank(I, b, end, Nx, off_max, max_bits);
+      te[0][j] = target;
+      len[0][j] = target >= 0 ? (int)steps + 1 : 0;  // cells of the raw arc, start and end included
     }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int start = vertex_start(sc, j, H, W, Nx, I.idx_base[b]);
+      long long steps = 0;
+      int target = -1;
+      if (start >= 0) {
+        const int end = flow_walk<0>(flow, start >> 2, Nx, cap, &steps, status);
+        target = seg_rank(I, b, end, Nx, off_min, min_bits);
+      }
+      te[1][j] = target;
+      len[1][j] = target >= 0 ? (int)steps + 1 : 0;  // an arc that leaves the image is empty
+    }
+    // a raw arc has fewer cells than the batch (cell ids are int32)
     arc_f[s] = make_int4(te[0][0], te[0][1], len[0][0], len[0][1]);
     arc_v[s] = make_int4(te[1][0], te[1][1], len[1][0], len[1][1]);
     // round 0 of the pairing: descending sweep on the face side in the
